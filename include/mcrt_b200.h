@@ -1,0 +1,264 @@
+/*
+ * mcrt_b200.h -- C ABI of the B200 Monte Carlo photon-packet engine.
+ *
+ * The engine replaces the per-packet loop of the Fortran routine
+ *   subroutine disk(converge,iter,i1)          newdisktherm_5_fuv.f90:1-663
+ * (emission -> propagate -> tauint cell walk -> scatter / absorb+reemit ->
+ * peel-off -> SED and image tallies), the rank reduction of its tallies
+ * (newdisktherm_5_fuv.f90:520-604) and the Lucy temperature update
+ *   subroutine tfinal(nphot,iter,converge)     tfinal_5_test1.f90:1-447
+ *   function   dusttemp(...)                   dusttemp_5.f90:8-152
+ * One GPU replaces all MPI ranks.  The Fortran driver keeps building the
+ * model (gridset, dustinit, atmosinit) and writing FITS output; it hands the
+ * module arrays it already owns to this library through the structs below.
+ *
+ * Conventions at the boundary are the reference's own:
+ *   - arrays are Fortran column-major with the reference's dimensions,
+ *     e.g. densarr(nrg,ntg,npg,ndg+2) is passed as a flat pointer whose
+ *     element (ir,it,ip,id) (1-based) sits at
+ *     (ir-1) + nrg*((it-1) + ntg*((ip-1) + npg*(id-1)));
+ *   - lengths are in stellar radii, frequencies in eV (lambda[um] = 1.2398/nu),
+ *     temperatures in the reference's "eV units" (Kelvin / 11605);
+ *   - Fortran LOGICAL arrays are passed as int32 (0 = .false.).
+ * All pointers are caller-owned; the library copies inputs to the GPU on
+ * upload and copies tallies out on download and keeps no host pointer after
+ * a call returns.  Errors are return codes, never process exits; a message is
+ * available from mcrt_last_error().  A context is bound to one CUDA device
+ * and is not re-entrant (one host thread per context).
+ */
+#ifndef MCRT_B200_H
+#define MCRT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---- */
+#define MCRT_OK               0
+#define MCRT_ERR_ARG          1   /* bad argument / inconsistent sizes          */
+#define MCRT_ERR_CUDA         2   /* CUDA runtime error (message has details)    */
+#define MCRT_ERR_UNSUPPORTED  3   /* model feature outside the built scope       */
+#define MCRT_ERR_GEOM         4   /* packets lost to a geometry failure          */
+#define MCRT_ERR_TIMEOUT      5   /* device watchdog ended a launch              */
+#define MCRT_ERR_STATE        6   /* call order violated (e.g. run before upload)*/
+
+/* ---- fixed reference dimensions ---- */
+#define MCRT_NDG2   10    /* ndg+2 density components per cell, grid_mod_5.f90:15 */
+#define MCRT_NO      8    /* SED components, tts_mod_5.f90:30                      */
+#define MCRT_IZMAX 145    /* zeta-series terms of bbfreq, random.f90:12            */
+
+/* ---- arithmetic of the transport kernels ---- */
+#define MCRT_PREC_FP64   0   /* everything in FP64 (event-for-event with the oracle) */
+#define MCRT_PREC_MIXED  1   /* FP32 walk/scatter, FP64 radial roots, tau sums, tallies */
+
+/*
+ * Run configuration: the scalars of tts_mod/grid_mod/dust_mod/spot_mod that
+ * the packet loop reads.  Field names follow the reference's variables.
+ */
+typedef struct mcrt_config {
+  /* grid wall counts (grid_mod_5.f90:10); cells are (nrg-1)x(ntg-1)x(npg-1) */
+  int32_t nrg, ntg, npg;
+  /* dust tables (dust_mod_5.f90:7-16): species, table lengths */
+  int32_t nopac, nlammax, nT, nnu;
+  /* stellar atmosphere CDF length (atmos_interp_mod.f90:5) */
+  int32_t nhnu;
+  /* SED / peel-off / image binning (tts_mod_5.f90:19-62) */
+  int32_t nfreq, nmu, nph, nap, npeel, nxhst;
+  /* switches */
+  int32_t output_imcube;     /* image_m_* cube on (IMCUBE=YES)                */
+  int32_t partial_peeloff;   /* tts_mod_5.f90:34                              */
+  int32_t limb;              /* 0 uniform, 1 Eddington limb darkening         */
+  int32_t iplanckst;         /* 1: star emits a Planck spectrum               */
+  int32_t idust;             /* 0 Rayleigh, 1 dustmat phase matrix (setup.f90:152) */
+  int32_t ilucy;             /* must be 1: Lucy reemission (emit_common_2.f90:59) */
+  int32_t iffuv;             /* FUV mean-intensity tally and FUV-only packets */
+  int32_t ispot, nspot;      /* hot spots (spot_mod.f90)                       */
+  int32_t pad0;
+  /* physics scalars */
+  double rstar;              /* stellar radius [Rsun]                          */
+  double tstar;              /* stellar temperature [K/11605]                  */
+  double tstarave;           /* tstarave [K/11605] (dusttemp normalisation)    */
+  double tshock;             /* hot-spot temperature [K/11605]                 */
+  double fspot;              /* hot-spot area fraction                         */
+  double accfrac, accfrac2;  /* disk-accretion and hot-spot packet fractions   */
+  double isrf_frac;          /* external-illumination packet fraction          */
+  double rddust;             /* disk inner dust radius [R*] (point-source switch) */
+  double rmaxi;              /* image half size [R*]                           */
+  double numin, lnurat;      /* SED frequency grid: numin [eV], log(numax/numin) */
+  double autors;             /* AU -> R* (setup.f90:45)                        */
+  double ifuv_ori;           /* FUV packet energy (newdisktherm_5_fuv.f90:206) */
+  /* spot geometry (spotset.f90) */
+  double cspot1, sspot1, scspot1, ssspot1;
+  double cspot2, sspot2, scspot2, ssspot2;
+  double csprad;
+} mcrt_config;
+
+/*
+ * Spherical-polar grid and per-cell model (grid_mod_5.f90:29-63, gridset).
+ */
+typedef struct mcrt_grid {
+  const double  *rarr, *r2arr;                          /* [nrg]            */
+  const double  *thetarr, *costarr, *sintarr, *tan2arr; /* [ntg]; tan2arr=-1 flags theta=90 */
+  const double  *phiarr, *aarr, *barr;                  /* [npg]            */
+  const double  *densarr;     /* [nrg,ntg,npg,10] g/cm^3                    */
+  const int32_t *findopac;    /* [nrg,ntg,npg,10] opacity species, 1-based  */
+  const int32_t *diffus;      /* [nrg,ntg,npg] LOGICAL                      */
+  const int32_t *diffdir;     /* [nrg,ntg,npg]                              */
+  const double  *tdust;       /* [nrg,ntg,npg] [K/11605]                    */
+  const double  *vcell;       /* [nrg,ntg,npg] cm^3                         */
+  const double  *ravearr;     /* [nrg-1] (accretion emission)               */
+  const double  *Ldint;       /* [nrg-1] accretion luminosity CDF           */
+  const double  *hdisk;       /* [nrg-1] disk scale height                  */
+} mcrt_grid;
+
+/*
+ * Dust, atmosphere and observer tables (dust_mod_5.f90, atmos_interp_mod.f90,
+ * tts_mod_5.f90:36-47, setup.f90:115-195).
+ */
+typedef struct mcrt_tables {
+  const int32_t *nlambda;                     /* [nopac]                     */
+  const double  *nudust, *kappad, *adust, *gdust, *pldust; /* [nlammax,nopac] */
+  const double  *kappav;                      /* [nopac]                     */
+  const double  *kapint;                      /* [nT,nnu,nopac] normalised   */
+  const double  *lTint, *Tint;                /* [nT]                        */
+  const double  *nuint;                       /* [nnu]                       */
+  const double  *kappap, *kappar;             /* [nT,nopac]                  */
+  const double  *atmosnu, *hnuint, *lognu, *loghnu;        /* [nhnu]         */
+  const double  *aperture2;                   /* [nap] squared apertures     */
+  const double  *u;                           /* [nmu] SED cos(theta) bins   */
+  const double  *coste_arr, *sinte_arr, *cospe_arr, *sinpe_arr; /* [npeel]   */
+  const double  *limb_prob;                   /* [100] Eddington CDF (samptabl.f90:1-23), limb=1 only */
+} mcrt_tables;
+
+/*
+ * Tallies of one iteration (caller-owned; any pointer may be NULL to skip it).
+ * Types and shapes are the reference's (tts_mod_5.f90, grid_mod_5.f90).
+ */
+typedef struct mcrt_tallies {
+  int32_t *nabs, *dbig, *dsg, *killed;        /* [nrg,ntg,npg]               */
+  double  *dtauabs, *fuvmean;                 /* [nrg,ntg,npg]               */
+  float   *si, *sq, *su, *sv, *si2, *sq2, *su2, *sv2, *nums, *aveinc; /* [nfreq,nmu,nph,nap,8] */
+  float   *ti, *tq, *tu, *tv, *ti2, *tq2, *tu2, *tv2, *numt;          /* [nfreq,npeel,nap,8]    */
+  float   *image_m_i, *image_m_q, *image_m_u, *image_m_v;             /* [npeel,nxhst,nxhst,nfreq] */
+  double  *scalars;   /* [MCRT_NSCALARS], see MCRT_S_* below                 */
+  int64_t *counters;  /* [MCRT_NCOUNTERS], see MCRT_C_* below                */
+} mcrt_tallies;
+
+/* scalars[] of one iteration (the reference's module scalars) */
+#define MCRT_S_FLUX     0   /* flux   (propagate_5_fuv.f90:265)  */
+#define MCRT_S_SFLUX    1   /* sflux                             */
+#define MCRT_S_NSCAT    2   /* nscat                             */
+#define MCRT_S_TOT      3   /* tot    (propagate_5_fuv.f90:72)   */
+#define MCRT_S_SCOUNT   4   /* scount (propagate_5_fuv.f90:320)  */
+#define MCRT_S_DSCOUNT  5   /* dscount                           */
+#define MCRT_S_AFLUX    6   /* aflux  (tauint_3d_2_fuv.f90:185)  */
+#define MCRT_S_ABFLUX   7   /* abflux (propagate_5_fuv.f90:210)  */
+#define MCRT_NSCALARS   8
+
+/* counters[] (device-side work statistics, not reference outputs) */
+#define MCRT_C_PACKETS       0  /* packets run                          */
+#define MCRT_C_CROSSINGS     1  /* cell crossings of the transport walk */
+#define MCRT_C_INTERACTIONS  2  /* scatterings + absorptions            */
+#define MCRT_C_SCATTERS      3
+#define MCRT_C_PEELS         4  /* peel-off walks started               */
+#define MCRT_C_PEEL_CROSS    5  /* cell crossings of peel-off walks     */
+#define MCRT_C_PEEL_BINNED   6  /* peel-offs that reached an image/SED  */
+#define MCRT_C_GEOM_FAIL     7  /* packets dropped: no wall found       */
+#define MCRT_C_RESETS        8  /* testgrid random re-locations         */
+#define MCRT_C_KILLED        9  /* packets killed after 10000 events    */
+#define MCRT_C_EXITED       10  /* packets that left the grid           */
+#define MCRT_C_STARHITS     11  /* packets absorbed + re-emitted by the star */
+#define MCRT_NCOUNTERS      16
+
+/* Per-packet summary used by the parity tests (event-for-event checks). */
+typedef struct mcrt_packet_log {
+  int64_t  iphot;
+  int32_t  nscat, nabs, ncross, nstar;   /* event counts                  */
+  int32_t  status;                        /* 0 exited, 1 killed, 2 fuv-drop, 3 geometry failure */
+  int32_t  ir, it, ip;                    /* last cell                      */
+  int32_t  ndraws;                        /* random numbers consumed        */
+  int32_t  iflag, i_orig, pad;
+  double   nub, cost, phi, sip, sqp, sup, svp, xp, yp, zp;
+} mcrt_packet_log;
+
+typedef struct mcrt_ctx mcrt_ctx;
+
+/* Create a context on CUDA device `device` for the sizes in *cfg.
+ * Replaces the rank set-up of newtts.f90:36-207 for the packet engine. */
+int mcrt_create(const mcrt_config *cfg, int device, mcrt_ctx **out);
+
+/* Upload the grid/model arrays that gridset fills every iteration
+ * (newdisktherm_5_fuv.f90:89 -> gridset_5_model13new.f90). */
+int mcrt_upload_grid(mcrt_ctx *ctx, const mcrt_grid *grid);
+
+/* Upload dust, atmosphere and observer tables (dustinit dust_5.f90:345-504,
+ * atmosinit starbarb_2.f90:3-122, setup.f90:115-195). */
+int mcrt_upload_tables(mcrt_ctx *ctx, const mcrt_tables *tab);
+
+/* Select FP64 or mixed-precision transport (MCRT_PREC_*). */
+int mcrt_set_precision(mcrt_ctx *ctx, int32_t mode);
+
+/* Zero the tallies of one iteration (initarr_2_new.f90:79-119). */
+int mcrt_reset_tallies(mcrt_ctx *ctx);
+
+/* Run packets iphot_lo..iphot_hi (1-based, inclusive) of an iteration of
+ * np packets: the loop `do iphot=1,np` of newdisktherm_5_fuv.f90:220-491.
+ * Packet iphot of iteration iter draws from block (iter-1)*np + iphot-1
+ * of L'Ecuyer-Cote generator `generator` seeded by (seed1,seed2) as
+ * user_set_all does (user_set_generator.f90:250-273,
+ * ecuyer_cote_mod.f90:297-395); blocks are 2^30 draws apart.
+ * ipeel=1 peels each emission/interaction off to every inclination.
+ * Tallies accumulate on the device until mcrt_reset_tallies. */
+int mcrt_run_iteration(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo,
+                       int64_t iphot_hi, int32_t iter, int32_t ipeel,
+                       int32_t seed1, int32_t seed2, int32_t generator);
+
+/* Copy the tallies to caller-owned arrays (the reduced values of
+ * newdisktherm_5_fuv.f90:520-604 for a single GPU). */
+int mcrt_download_tallies(mcrt_ctx *ctx, mcrt_tallies *out);
+
+/* Add a tally set from another process into this context's device tallies
+ * (the summing half of MPI_ALLREDUCE for multi-process runs). */
+int mcrt_accumulate_tallies(mcrt_ctx *ctx, const mcrt_tallies *in);
+
+/* Lucy temperature update on the device: tfinal(nphot,iter,converge)
+ * (tfinal_5_test1.f90:1-447) with dusttemp (dusttemp_5.f90:8-152).
+ * tdave [nrg,ntg,npg] is read (previous iteration) and overwritten.
+ * *converge is 0 ('no') or 1 ('yes') on entry and may be set to 1.
+ * sig[0..2] receive the three convergence statistics of tfinal_5_test1.f90:346-348. */
+int mcrt_update_temperature(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
+                            double *tdave, int32_t *converge, double *sig);
+
+/* Parity support: record a mcrt_packet_log for the first `max_packets`
+ * packets of the next mcrt_run_iteration (0 disables). */
+int mcrt_enable_packet_log(mcrt_ctx *ctx, int64_t max_packets);
+int mcrt_download_packet_log(mcrt_ctx *ctx, mcrt_packet_log *out, int64_t n);
+
+/* Device time of the last mcrt_run_iteration's transport kernels [ms]. */
+int mcrt_last_kernel_ms(mcrt_ctx *ctx, double *ms);
+
+/* Measurement support: record CUDA event `slot` (0..15) on the context's
+ * stream, and the device time between two recorded events [ms]. */
+int mcrt_mark(mcrt_ctx *ctx, int32_t slot);
+int mcrt_elapsed_ms(mcrt_ctx *ctx, int32_t slot_a, int32_t slot_b, double *ms);
+
+/* Overwrite a 256 MiB device buffer on the context's stream so that the next
+ * launch starts with a cold L2 (timing hygiene between benchmark steps). */
+int mcrt_flush_l2(mcrt_ctx *ctx);
+
+/* Block until all work queued on the context's stream has finished. */
+int mcrt_synchronize(mcrt_ctx *ctx);
+
+const char *mcrt_last_error(mcrt_ctx *ctx);
+void mcrt_destroy(mcrt_ctx *ctx);
+
+/* Library version string. */
+const char *mcrt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCRT_B200_H */

@@ -1,0 +1,94 @@
+"""Python handle on the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/_build/libmcrt_oracle.so (built by oracle/Makefile) and runs the
+FP64 restatement of the reference's packet loop on host threads.  Only the
+tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of bench.py use it,
+always as the checker or the baseline, never as the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from src3_mpi_cfitsio_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libmcrt_oracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        lib.oracle_run.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
+                                   C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                   C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                   C.POINTER(abi.Tallies), C.POINTER(abi.PacketLog), C.c_int64]
+        lib.oracle_run.restype = C.c_int
+        lib.oracle_rng.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+        lib.oracle_inczeta.argtypes = [C.POINTER(C.c_double)]
+        lib.oracle_tfinal.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
+                                      C.POINTER(C.c_double), C.c_int32, C.c_int32,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        lib.oracle_tfinal.restype = C.c_int
+        _lib = lib
+    return _lib
+
+
+def run(bundle: abi.Bundle, np_total: int, lo: int = 1, hi: int | None = None, *, ipeel: int = 1,
+        iteration: int = 1, seeds=(12345678, 87654321), generator: int = 1,
+        threads: int | None = None, nlog: int = 0, images: bool = True):
+    """Run packets lo..hi of an np_total-packet iteration; returns (tallies, log)."""
+    lib = load()
+    hi = np_total if hi is None else hi
+    threads = threads or os.cpu_count() or 1
+    tal = abi.TallyArrays(bundle.config, images=images)
+    log = abi.packet_log_array(nlog) if nlog > 0 else None
+    rc = lib.oracle_run(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables),
+                        np_total, lo, hi, iteration, ipeel, seeds[0], seeds[1], generator, threads,
+                        C.byref(tal.struct), log, nlog)
+    if rc != 0:
+        raise RuntimeError(f"oracle_run failed with code {rc}")
+    return tal, log
+
+
+def rng(seed1: int, seed2: int, generator: int, block: int, n: int):
+    lib = load()
+    out = np.zeros(n, np.float64)
+    seeds = np.zeros(2, np.int32)
+    lib.oracle_rng(seed1, seed2, generator, block, n, out.ctypes.data_as(C.POINTER(C.c_double)),
+                   seeds.ctypes.data_as(C.POINTER(C.c_int32)))
+    return out, seeds
+
+
+def inczeta():
+    out = np.zeros(145, np.float64)
+    load().oracle_inczeta(out.ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def tfinal(bundle: abi.Bundle, dtauabs: np.ndarray, nphot: int, iteration: int, tdave: np.ndarray):
+    lib = load()
+    td = np.ascontiguousarray(tdave, dtype=np.float64).copy()
+    da = np.ascontiguousarray(dtauabs, dtype=np.float64)
+    conv = C.c_int32(0)
+    sig = np.zeros(3, np.float64)
+    rc = lib.oracle_tfinal(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables),
+                           da.ctypes.data_as(C.POINTER(C.c_double)), nphot, iteration,
+                           td.ctypes.data_as(C.POINTER(C.c_double)), C.byref(conv),
+                           sig.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle_tfinal failed with code {rc}")
+    return td, sig

@@ -1,0 +1,725 @@
+// mcrt_b200.cu -- C ABI of the B200 photon-packet engine (include/mcrt_b200.h).
+//
+// Host side: one context per device holds the model in the transport layout
+// of mcrt_device.cuh, the FP64 device tallies, and launches the transport
+// kernels (mcrt_fp64.cu / mcrt_mixed.cu) and the Lucy temperature kernels
+// below.  Nothing here falls back to the CPU: every call that cannot run on
+// the GPU returns an error code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mcrt_device.cuh"
+
+namespace mcrt {
+// transport launchers (mcrt_fp64.cu, mcrt_mixed.cu)
+cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t s);
+cudaError_t launch_transport_mixed(const LaunchParams& p, int grid, cudaStream_t s);
+int transport_fp64_blocks_per_sm();
+int transport_mixed_blocks_per_sm();
+}  // namespace mcrt
+
+using namespace mcrt;
+
+struct mcrt_ctx {
+  mcrt_config cfg{};
+  int device = 0;
+  int nsm = 148;
+  int precision = MCRT_PREC_FP64;
+  bool have_grid = false, have_tables = false;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  int64_t ncell = 0, nsed = 0, npsed = 0, nimg = 0;
+  DevModel dm{};
+  DevTallies dt{};
+  std::vector<void*> allocs;         // device buffers owned by the context
+  // model buffers
+  double *d_walls = nullptr;
+  CellRec *d_cells = nullptr;
+  double *d_tdust = nullptr, *d_vcell = nullptr;
+  double *d_dens_thermal = nullptr;   // [ncell] density of the thermal component (tfinal)
+  int32_t *d_idust3 = nullptr;        // [ncell] its opacity species (0 = none)
+  int32_t *d_diffus = nullptr;
+  // tables
+  int32_t *d_nlambda = nullptr;
+  double *d_tabs = nullptr;
+  int64_t *d_jump = nullptr;
+  // tallies
+  void *d_tally = nullptr;
+  size_t tally_bytes = 0;
+  unsigned long long *d_next = nullptr;
+  int32_t *d_err = nullptr;
+  mcrt_packet_log *d_log = nullptr;
+  int64_t nlog = 0;
+  double prev_sig = -1.0;
+  cudaEvent_t marks[16] = {};
+  void *d_flush = nullptr;
+  int64_t off_Tint = 0, off_kappap = 0;   // offsets of Tint/kappap in d_tabs (tfinal)
+  std::vector<double> h_rarr;
+};
+
+namespace {
+
+int fail(mcrt_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+int dalloc(mcrt_ctx* ctx, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "cudaMalloc(%zu): %s", n * sizeof(T), cudaGetErrorString(e));
+  ctx->allocs.push_back(q);
+  *p = (T*)q;
+  return MCRT_OK;
+}
+
+void dfree(mcrt_ctx* ctx, void* p) {
+  if (!p) return;
+  auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), p);
+  if (it != ctx->allocs.end()) ctx->allocs.erase(it);
+  cudaFree(p);
+}
+
+int64_t mulmod_h(int64_t a, int64_t b, int64_t m) {
+  return (int64_t)(((unsigned __int128)a * (unsigned __int128)b) % (unsigned __int128)m);
+}
+
+void zetainit_h(double* inczeta) {   // random.f90:227-245
+  for (int i = 0; i < MCRT_IZMAX; ++i) inczeta[i] = 0.0;
+  for (int j = MCRT_IZMAX; j >= 1; --j) {
+    double temp = 1.0 / (double)(j * j * j * j);
+    for (int i = MCRT_IZMAX; i >= j; --i) inczeta[i - 1] += temp;
+  }
+}
+
+const bool kIsSg[MCRT_NDG2] = {false, false, false, false, true, true, true, true, false, false};  // grid_mod_5.f90:20
+
+}  // namespace
+
+// ---------------------------------------------------------------- tfinal --
+namespace mcrt {
+
+__device__ __forceinline__ double p4(double x) { double x2 = x * x; return x2 * x2; }
+
+// dusttemp (dusttemp_5.f90:8-152) for a zero velocity field
+__device__ double dusttemp_dev(const double* Tint, const double* kp, int nT, double kv, double na, int nphot,
+                               double mcell, double rstar, double tstar) {
+  const double Tmax = 199999.0, T01 = 0.1 / 11605.0;
+  double Td = T01;
+  if (!(mcell > 0.0)) return Td;
+  double abs_ = p4(tstar) * (na * 3.1415926535897932384626433 * rstar * rstar) / ((double)nphot * kv);
+  abs_ = abs_ * (6.9598e10 * 6.9598e10) / p4(mcell);
+  if (na == 0.0) return T01;
+  double minkap = p4(Tint[0]) * kp[0], maxkap = minkap;
+  int mini = 1, maxi = 1;
+  for (int i = 1; i <= nT; ++i) {
+    const double k = p4(Tint[i - 1]) * kp[i - 1];
+    if (minkap > k) { minkap = k; mini = i; }
+    if (maxkap < k) { maxkap = k; maxi = i; }
+  }
+  if (maxkap < abs_) Td = fmax(fmin(Tint[maxi - 1], Tmax / 11605.0), T01);
+  if (minkap > abs_) Td = fmax(fmin(Tint[mini - 1], Tmax / 11605.0), T01);
+  if (mini < maxi) {
+    for (int i = mini; i <= maxi - 1; ++i) {
+      const double kl = p4(Tint[i - 1]) * kp[i - 1], ku = p4(Tint[i]) * kp[i];
+      if (kl < abs_ && ku >= abs_) {
+        const double Tl = Tint[i - 1], Tu = Tint[i];
+        Td = Tl + (Tu - Tl) / (ku - kl) * (abs_ - kl);
+        return fmax(fmin(Td, Tmax / 11605.0), T01);
+      }
+    }
+  } else {
+    for (int i = maxi; i <= mini - 1; ++i) {
+      const double kl = p4(Tint[i - 1]) * kp[i - 1], ku = p4(Tint[i]) * kp[i];
+      if (kl > abs_ && ku <= abs_) {
+        const double Tl = Tint[i - 1], Tu = Tint[i];
+        Td = Tl + (Tu - Tl) / (ku - kl) * (abs_ - kl);
+        return fmax(fmin(Td, Tmax / 11605.0), T01);
+      }
+    }
+  }
+  return Td;
+}
+
+struct TfinalArgs {
+  int nrg, ntg, npg, nT, nphot, maxii;
+  double rstar, tstar;
+  const double *Tint, *kappap, *kappav, *dtauabs, *vcell, *dens, *tdust;
+  const int32_t *idust3, *diffus;
+  const double *told;   // tdave of the previous iteration
+  double *tnew;         // scratch: new upper-hemisphere values
+  double *tdave;        // result
+};
+
+// tfinal_5_test1.f90:206-256: upper-hemisphere cells of phi slice 1.  The
+// thermal component of the cell (id) fixes the species; the mirror cell
+// ntg-it contributes its density of the same component (zero if absent).
+__global__ void tfinal_cells(TfinalArgs a) {
+  const int nu = (a.ntg - 1) / 2;
+  const int64_t n = (int64_t)(a.nrg - 1) * nu;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % (a.nrg - 1)) + 1;
+    const int it = (int)(k / (a.nrg - 1)) + 1;
+    const int itm = a.ntg - it;
+    const int64_t c = (ir - 1) + (int64_t)a.nrg * (it - 1);
+    const int64_t cm = (ir - 1) + (int64_t)a.nrg * (itm - 1);
+    double td = 0.1 / 11605.0;
+    const int sp = a.idust3[c];
+    if (sp > 0) {
+      if (!a.diffus[c]) {
+        const double dm = (a.idust3[cm] == sp) ? a.dens[cm] : 0.0;
+        const double m1 = pow(a.dens[c] * a.vcell[c], 0.25);
+        const double m2 = pow(dm * a.vcell[c], 0.25);
+        const double* kp = a.kappap + (int64_t)a.nT * (sp - 1);
+        const double t1 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[c], a.nphot, m1, a.rstar, a.tstar);
+        const double t2 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[cm], a.nphot, m2, a.rstar, a.tstar);
+        td = (t1 + t2) / 2.0;
+      } else {
+        td = (a.tdust[c] + a.tdust[cm]) / 2.0;
+      }
+      if (td * 11605.0 >= 199999.0) td = 199999.0 / 11605.0;
+    }
+    a.tnew[c] = td;
+  }
+}
+
+// tfinal_5_test1.f90:267-293: mirror to the lower hemisphere and the other
+// phi slices, then the average over passes 11..20 (all passes give the same
+// value for a zero velocity field; the sum is formed term by term as in the
+// reference).  Cells outside the loops keep their previous value.
+__global__ void tfinal_mirror(TfinalArgs a) {
+  const int64_t n = (int64_t)a.nrg * a.ntg * a.npg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1;
+    const int it = (int)((k / a.nrg) % a.ntg) + 1;
+    const int ip = (int)(k / ((int64_t)a.nrg * a.ntg)) + 1;
+    double v = a.told[k];
+    if (ir <= a.nrg - 1 && it <= a.ntg - 1 && (ip == 1 || (a.npg > 2 && ip <= a.npg - 1))) {
+      const int src_it = (it >= (a.ntg + 1) / 2) ? a.ntg - it : it;
+      v = a.tnew[(ir - 1) + (int64_t)a.nrg * (src_it - 1)];
+    }
+    if (a.maxii > 10) {
+      double acc = 0.0;
+      for (int i = 0; i < a.maxii - 10; ++i) acc += v;
+      v = acc / (double)(a.maxii - 10);
+    }
+    a.tdave[k] = v;
+  }
+}
+
+// gridset_5_model13new.f90:1855-1866: tdust for the next iteration
+__global__ void tdust_from_tdave(int64_t n, const double* tdave, const int32_t* diffus, const int32_t* idust3,
+                                 const CellRec* cells, double* tdust) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    double t = diffus[k] ? 0.1 / 11605.0 : tdave[k];
+    if (cell_n(cells[k].meta) == 0) t = 0.1 / 11605.0;
+    tdust[k] = t;
+  }
+}
+
+__global__ void to_float(const double* src, float* dst, int64_t n) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    dst[k] = (float)src[k];
+}
+
+}  // namespace mcrt
+
+// ------------------------------------------------------------------ API --
+extern "C" {
+
+const char* mcrt_version(void) { return "mcrt-b200 1.0 (sm_100a)"; }
+
+const char* mcrt_last_error(mcrt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
+  mcrt_ctx* ctx = nullptr;
+  if (!cfg || !out) return MCRT_ERR_ARG;
+  *out = nullptr;
+  if (cfg->nrg < 3 || cfg->ntg < 2 || cfg->npg < 2 || cfg->nopac < 1 || cfg->nfreq < 1 || cfg->nmu < 1 ||
+      cfg->nph < 1 || cfg->nap < 1 || cfg->npeel < 0 || cfg->nxhst < 1 || cfg->nT < 2 || cfg->nnu < 2 ||
+      cfg->nhnu < 2 || cfg->nlammax < 1)
+    return MCRT_ERR_ARG;
+  ctx = new mcrt_ctx();
+  ctx->cfg = *cfg;
+  ctx->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device));
+  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&ctx->ev0));
+  CK(cudaEventCreate(&ctx->ev1));
+  const mcrt_config& c = *cfg;
+  ctx->ncell = (int64_t)c.nrg * c.ntg * c.npg;
+  ctx->nsed = (int64_t)c.nfreq * c.nmu * c.nph * c.nap * MCRT_NO;
+  ctx->npsed = (int64_t)c.nfreq * c.npeel * c.nap * MCRT_NO;
+  ctx->nimg = c.output_imcube ? (int64_t)c.npeel * c.nxhst * c.nxhst * c.nfreq : 0;
+  // one tally allocation: cell ints, cell doubles, SED, peeled SED, images, scalars, counters
+  const int64_t n_int = 4 * ctx->ncell;
+  const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + MCRT_NSCALARS;
+  ctx->tally_bytes = (size_t)n_dbl * 8 + (size_t)MCRT_NCOUNTERS * 8 + (size_t)((n_int * 4 + 7) / 8) * 8;
+  int rc = dalloc(ctx, (char**)&ctx->d_tally, ctx->tally_bytes);
+  if (rc) { *out = ctx; return rc; }
+  char* base = (char*)ctx->d_tally;
+  double* d = (double*)base;
+  DevTallies& t = ctx->dt;
+  t.dtauabs = d; d += ctx->ncell;
+  t.fuvmean = d; d += ctx->ncell;
+  t.sed = d; d += 10 * ctx->nsed;
+  t.psed = d; d += 9 * ctx->npsed;
+  t.img = d; d += 4 * ctx->nimg;
+  t.scal = d; d += MCRT_NSCALARS;
+  t.cnt = (unsigned long long*)d;
+  int32_t* ip = (int32_t*)(t.cnt + MCRT_NCOUNTERS);
+  t.nabs = ip; ip += ctx->ncell;
+  t.dbig = ip; ip += ctx->ncell;
+  t.dsg = ip; ip += ctx->ncell;
+  t.killed = ip;
+  if ((rc = dalloc(ctx, &ctx->d_next, 1))) { *out = ctx; return rc; }
+  if ((rc = dalloc(ctx, &ctx->d_err, 4))) { *out = ctx; return rc; }
+  CK(cudaMemset(ctx->d_tally, 0, ctx->tally_bytes));
+  *out = ctx;
+  return MCRT_OK;
+}
+
+void mcrt_destroy(mcrt_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (auto& e : ctx->marks) if (e) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int mcrt_set_precision(mcrt_ctx* ctx, int32_t mode) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (mode != MCRT_PREC_FP64 && mode != MCRT_PREC_MIXED) return fail(ctx, MCRT_ERR_ARG, "unknown precision %d", mode);
+  ctx->precision = mode;
+  return MCRT_OK;
+}
+
+int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
+  if (!ctx || !g) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const mcrt_config& c = ctx->cfg;
+  const int nrg = c.nrg, ntg = c.ntg, npg = c.npg;
+  const int64_t ncell = ctx->ncell;
+  if (!g->rarr || !g->r2arr || !g->thetarr || !g->costarr || !g->tan2arr || !g->phiarr || !g->aarr || !g->barr ||
+      !g->densarr || !g->findopac || !g->diffus || !g->tdust || !g->vcell)
+    return fail(ctx, MCRT_ERR_ARG, "mcrt_upload_grid: missing array");
+  // transport layout: one CellRec per cell with the non-zero components
+  std::vector<CellRec> cells(ncell);
+  std::vector<int> slot_species;
+  std::vector<double> dens_th(ncell, 0.0);
+  std::vector<int32_t> idust3(ncell, 0), diffus(ncell, 0);
+  for (int64_t k = 0; k < ncell; ++k) {
+    CellRec& r = cells[k];
+    std::memset(&r, 0, sizeof r);
+    int n = 0;
+    int nth = 0;
+    for (int id = 1; id <= MCRT_NDG2; ++id) {
+      const double rho = g->densarr[k + ncell * (id - 1)];
+      if (!(rho > 0.0)) continue;
+      const int sp = g->findopac[k + ncell * (id - 1)];
+      if (id > 8) return fail(ctx, MCRT_ERR_UNSUPPORTED, "gas-opacity component %d is outside the built scope", id);
+      if (kIsSg[id - 1]) return fail(ctx, MCRT_ERR_UNSUPPORTED, "small-grain component %d needs rep_draine (out of scope)", id);
+      if (sp != id) return fail(ctx, MCRT_ERR_UNSUPPORTED, "findopac(.,%d)=%d: dust components must map to their own species", id, sp);
+      if (sp < 1 || sp > c.nopac) return fail(ctx, MCRT_ERR_ARG, "findopac out of range");
+      if (n >= kMaxComp) return fail(ctx, MCRT_ERR_UNSUPPORTED, "more than %d non-zero density components in a cell", kMaxComp);
+      int s = -1;
+      for (size_t q = 0; q < slot_species.size(); ++q) if (slot_species[q] == sp) s = (int)q;
+      if (s < 0) {
+        if ((int)slot_species.size() >= kMaxSlot) return fail(ctx, MCRT_ERR_UNSUPPORTED, "more than %d opacity species", kMaxSlot);
+        slot_species.push_back(sp);
+        s = (int)slot_species.size() - 1;
+      }
+      r.rho[n] = rho;
+      r.meta |= (uint32_t)s << (2 + 7 * n);
+      r.meta |= (uint32_t)(id - 1) << (5 + 7 * n);
+      ++n;
+      if (!kIsSg[id - 1]) { ++nth; dens_th[k] = rho; idust3[k] = id; }
+    }
+    r.meta |= (uint32_t)n;
+    if (nth > 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "cell with %d thermal components (tfinal allows one)", nth);
+    diffus[k] = g->diffus[k] ? 1 : 0;
+    if (diffus[k]) return fail(ctx, MCRT_ERR_UNSUPPORTED, "diffusion cells (emit_common_2.f90:83-381) are outside the built scope");
+    r.flags = (uint32_t)diffus[k];
+  }
+  if (slot_species.empty()) slot_species.push_back(1);
+  // walls: rarr r2arr | thetarr costarr tan2arr | phiarr aarr barr, each
+  // padded by one element.  The reference reads one past the last wall when a
+  // peel-off steps to ir=nrg or a walk reaches it=ntg before testgrid
+  // (testgrid.f90:92-93, peeloff_3d_2_test.f90:119-121); the pad makes those
+  // reads defined: a sphere at 4 r2arr(nrg), a cone beyond the south pole.
+  std::vector<double> walls;
+  auto addp = [&](const double* a, int n, double pad) { walls.insert(walls.end(), a, a + n); walls.push_back(pad); };
+  addp(g->rarr, nrg, 2.0 * g->rarr[nrg - 1]);
+  addp(g->r2arr, nrg, 4.0 * g->r2arr[nrg - 1]);
+  addp(g->thetarr, ntg, g->thetarr[ntg - 1]);
+  addp(g->costarr, ntg, g->costarr[ntg - 1] - 1.0);
+  addp(g->tan2arr, ntg, 0.0);
+  addp(g->phiarr, npg, g->phiarr[npg - 1]);
+  addp(g->aarr, npg, g->aarr[npg - 1]);
+  addp(g->barr, npg, g->barr[npg - 1]);
+  ctx->h_rarr.assign(g->rarr, g->rarr + nrg);
+  if (!ctx->have_grid) {
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->d_walls, walls.size()))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_cells, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_tdust, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_vcell, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_dens_thermal, 2 * ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_idust3, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_diffus, ncell))) return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->d_walls, walls.data(), walls.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_cells, cells.data(), ncell * sizeof(CellRec), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_tdust, g->tdust, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_vcell, g->vcell, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_dens_thermal, dens_th.data(), ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_idust3, idust3.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_diffus, diffus.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  DevModel& m = ctx->dm;
+  const double* w = ctx->d_walls;
+  m.rarr = w; w += nrg + 1;
+  m.r2arr = w; w += nrg + 1;
+  m.thetarr = w; w += ntg + 1;
+  m.costarr = w; w += ntg + 1;
+  m.tan2arr = w; w += ntg + 1;
+  m.phiarr = w; w += npg + 1;
+  m.aarr = w; w += npg + 1;
+  m.barr = w;
+  m.cells = ctx->d_cells;
+  m.tdust = ctx->d_tdust;
+  m.vcell = ctx->d_vcell;
+  m.nslot = (int)slot_species.size();
+  for (int s = 0; s < kMaxSlot; ++s) m.slot_species[s] = s < m.nslot ? slot_species[s] : 1;
+  ctx->have_grid = true;
+  return MCRT_OK;
+}
+
+int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
+  if (!ctx || !t) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const mcrt_config& c = ctx->cfg;
+  if (!t->nlambda || !t->nudust || !t->kappad || !t->adust || !t->gdust || !t->pldust || !t->kappav || !t->kapint ||
+      !t->lTint || !t->Tint || !t->nuint || !t->kappap || !t->atmosnu || !t->hnuint || !t->lognu || !t->loghnu ||
+      !t->aperture2 || !t->u || (c.npeel > 0 && (!t->coste_arr || !t->sinte_arr || !t->cospe_arr || !t->sinpe_arr)))
+    return fail(ctx, MCRT_ERR_ARG, "mcrt_upload_tables: missing array");
+  if (c.limb != 0 && !t->limb_prob) return fail(ctx, MCRT_ERR_ARG, "limb=1 needs limb_prob");
+  for (int i = 0; i < c.nopac; ++i)
+    if (t->nlambda[i] < 2 || t->nlambda[i] > c.nlammax) return fail(ctx, MCRT_ERR_ARG, "nlambda(%d) out of range", i + 1);
+  const int64_t nl = (int64_t)c.nlammax * c.nopac;
+  const int64_t nk = (int64_t)c.nT * c.nnu * c.nopac;
+  std::vector<double> tab;
+  std::vector<int64_t> off;
+  auto add = [&](const double* p, int64_t n) { off.push_back((int64_t)tab.size()); tab.insert(tab.end(), p, p + n); };
+  std::vector<double> sini(c.nmu), inczeta(MCRT_IZMAX), zero(c.npeel > 0 ? 0 : 1, 0.0);
+  for (int i = 0; i < c.nmu; ++i) sini[i] = std::sqrt(1.0 - t->u[i] * t->u[i]);
+  zetainit_h(inczeta.data());
+  std::vector<double> limb(100, 0.0);
+  if (t->limb_prob) limb.assign(t->limb_prob, t->limb_prob + 100);
+  add(t->nudust, nl); add(t->kappad, nl); add(t->adust, nl); add(t->gdust, nl); add(t->pldust, nl);   // 0-4
+  add(t->kappav, c.nopac); add(t->kapint, nk); add(t->lTint, c.nT); add(t->nuint, c.nnu);              // 5-8
+  add(t->atmosnu, c.nhnu); add(t->hnuint, c.nhnu); add(t->lognu, c.nhnu); add(t->loghnu, c.nhnu);      // 9-12
+  add(limb.data(), 100); add(inczeta.data(), MCRT_IZMAX);                                              // 13-14
+  add(t->aperture2, c.nap); add(t->u, c.nmu); add(sini.data(), c.nmu);                                 // 15-17
+  const int np = std::max(c.npeel, 1);
+  std::vector<double> pz(np, 0.0);
+  add(c.npeel ? t->coste_arr : pz.data(), np); add(c.npeel ? t->sinte_arr : pz.data(), np);            // 18-19
+  add(c.npeel ? t->cospe_arr : pz.data(), np); add(c.npeel ? t->sinpe_arr : pz.data(), np);            // 20-21
+  add(t->Tint, c.nT); add(t->kappap, (int64_t)c.nT * c.nopac);                                          // 22-23
+  // jump tables a^(2^30 * 2^k)
+  std::vector<int64_t> jump(128);
+  int64_t j1 = 1033780774, j2 = 1494757890;   // a1w, a2w (ecuyer_cote_mod.f90:14-15)
+  for (int k = 0; k < 64; ++k) {
+    jump[k] = j1;
+    jump[64 + k] = j2;
+    j1 = mulmod_h(j1, j1, 2147483563);
+    j2 = mulmod_h(j2, j2, 2147483399);
+  }
+  int rc;
+  if (ctx->have_tables) { dfree(ctx, ctx->d_tabs); dfree(ctx, ctx->d_nlambda); dfree(ctx, ctx->d_jump); }
+  if ((rc = dalloc(ctx, &ctx->d_tabs, tab.size()))) return rc;
+  if ((rc = dalloc(ctx, &ctx->d_nlambda, c.nopac))) return rc;
+  if ((rc = dalloc(ctx, &ctx->d_jump, 128))) return rc;
+  CK(cudaMemcpyAsync(ctx->d_tabs, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_nlambda, t->nlambda, c.nopac * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_jump, jump.data(), 128 * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  DevModel& m = ctx->dm;
+  const double* b = ctx->d_tabs;
+  m.nudust = b + off[0]; m.kappad = b + off[1]; m.adust = b + off[2]; m.gdust = b + off[3]; m.pldust = b + off[4];
+  m.kappav = b + off[5]; m.kapint = b + off[6]; m.lTint = b + off[7]; m.nuint = b + off[8];
+  m.atmosnu = b + off[9]; m.hnuint = b + off[10]; m.lognu = b + off[11]; m.loghnu = b + off[12];
+  m.limb_prob = b + off[13]; m.inczeta = b + off[14];
+  m.aperture2 = b + off[15]; m.u = b + off[16]; m.sini = b + off[17];
+  m.coste = b + off[18]; m.sinte = b + off[19]; m.cospe = b + off[20]; m.sinpe = b + off[21];
+  m.nlambda = ctx->d_nlambda;
+  m.jump1 = ctx->d_jump;
+  m.jump2 = ctx->d_jump + 64;
+  ctx->have_tables = true;
+  ctx->off_Tint = off[22];
+  ctx->off_kappap = off[23];
+  return MCRT_OK;
+}
+
+int mcrt_reset_tallies(mcrt_ctx* ctx) {
+  if (!ctx) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d_tally, 0, ctx->tally_bytes, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_enable_packet_log(mcrt_ctx* ctx, int64_t max_packets) {
+  if (!ctx || max_packets < 0) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (ctx->d_log) { dfree(ctx, ctx->d_log); ctx->d_log = nullptr; }
+  ctx->nlog = max_packets;
+  if (max_packets > 0) {
+    int rc = dalloc(ctx, &ctx->d_log, (size_t)max_packets);
+    if (rc) return rc;
+    CK(cudaMemset(ctx->d_log, 0, (size_t)max_packets * sizeof(mcrt_packet_log)));
+  }
+  return MCRT_OK;
+}
+
+int mcrt_download_packet_log(mcrt_ctx* ctx, mcrt_packet_log* out, int64_t n) {
+  if (!ctx || !out || n < 0 || n > ctx->nlog) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpy(out, ctx->d_log, (size_t)n * sizeof(mcrt_packet_log), cudaMemcpyDeviceToHost));
+  return MCRT_OK;
+}
+
+int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
+                       int32_t seed1, int32_t seed2, int32_t generator) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range %lld..%lld of %lld", (long long)lo, (long long)hi, (long long)np);
+  if (generator < 1 || generator > 32) return fail(ctx, MCRT_ERR_ARG, "generator %d not in 1..32", generator);
+  if (seed1 < 1 || seed1 >= 2147483563 || seed2 < 1 || seed2 >= 2147483399) return fail(ctx, MCRT_ERR_ARG, "seeds out of range");
+  const mcrt_config& c = ctx->cfg;
+  if (c.ilucy != 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "ilucy=0 (Bjorkman-Wood) stops in the reference (emit_common_2.f90:59-61)");
+  CK(cudaSetDevice(ctx->device));
+  // packet split (newdisktherm_5_fuv.f90:158-191)
+  int64_t npout = (int64_t)(c.isrf_frac * (double)np);
+  double rn = c.isrf_frac * (double)np;
+  if (rn - (double)npout > 0.5) npout++;
+  int64_t ns = (int64_t)((double)np * (1.0 - c.accfrac - c.isrf_frac));
+  rn = (double)(float)np * (1.0 - c.accfrac - c.isrf_frac);
+  if (rn - (double)ns > 0.5) ns++;
+  int64_t npacc = (int64_t)((double)np * c.accfrac);
+  int64_t npaccstar = (int64_t)(c.accfrac2 * (double)np);
+  const int64_t nsum = ns + npacc + npout;
+  if (nsum != np) ns = ns + np - nsum;
+  if (npacc > 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "disk-accretion packets (initpacc) are outside the built scope");
+  if (npout > 0) return fail(ctx, MCRT_ERR_UNSUPPORTED, "external-illumination packets (initpout) are outside the built scope");
+  // generator seeds (set_all_seeds)
+  int64_t g1 = seed1, g2 = seed2;
+  for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }
+  LaunchParams P{};
+  P.m = ctx->dm;
+  DevModel& m = P.m;
+  m.nrg = c.nrg; m.ntg = c.ntg; m.npg = c.npg; m.nopac = c.nopac; m.nlammax = c.nlammax; m.nT = c.nT; m.nnu = c.nnu;
+  m.nhnu = c.nhnu; m.nfreq = c.nfreq; m.nmu = c.nmu; m.nph = c.nph; m.nap = c.nap; m.npeel = c.npeel; m.nxhst = c.nxhst;
+  m.output_imcube = c.output_imcube; m.partial_peeloff = c.partial_peeloff; m.limb = c.limb; m.iplanckst = c.iplanckst;
+  m.idust = c.idust; m.iffuv = c.iffuv; m.ispot = c.ispot; m.nspot = c.nspot;
+  m.ncell = ctx->ncell; m.nsed = ctx->nsed; m.npsed = ctx->npsed; m.nimg = ctx->nimg;
+  m.rstar = c.rstar; m.rmincgs = c.rstar * 6.9598e10; m.tstar = c.tstar; m.tshock = c.tshock; m.fspot = c.fspot;
+  m.rmaxi = c.rmaxi; m.fractxh = 2.0 * c.rmaxi / (double)c.nxhst; m.numin = c.numin; m.lnurat = c.lnurat;
+  m.ifuv_ori = c.ifuv_ori;
+  m.cspot1 = c.cspot1; m.sspot1 = c.sspot1; m.scspot1 = c.scspot1; m.ssspot1 = c.ssspot1;
+  m.cspot2 = c.cspot2; m.sspot2 = c.sspot2; m.scspot2 = c.scspot2; m.ssspot2 = c.ssspot2; m.csprad = c.csprad;
+  P.t = ctx->dt;
+  P.np = np; P.lo = lo; P.hi = hi;
+  if (iter < 1) return fail(ctx, MCRT_ERR_ARG, "iter must be >= 1");
+  P.block0 = (int64_t)(iter - 1) * np;
+  P.ns = ns; P.npacc = npacc; P.npaccstar = npaccstar;
+  P.ipeel = ipeel ? 1 : 0;
+  P.ips = (c.rddust > 100.0) ? 1 : 0;
+  P.g1 = (int32_t)g1; P.g2 = (int32_t)g2;
+  P.next = ctx->d_next;
+  P.log = ctx->d_log;
+  P.nlog = ctx->nlog;
+  P.err = ctx->d_err;
+  CK(cudaMemsetAsync(ctx->d_next, 0, sizeof(unsigned long long), ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_err, 0, 4 * sizeof(int32_t), ctx->stream));
+  const int64_t npk = hi - lo + 1;
+  int per_sm = ctx->precision == MCRT_PREC_FP64 ? transport_fp64_blocks_per_sm() : transport_mixed_blocks_per_sm();
+  int64_t want = (npk + kTransportBlock - 1) / kTransportBlock;
+  int grid = (int)std::min<int64_t>((int64_t)ctx->nsm * std::max(per_sm, 1), std::max<int64_t>(want, 1));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  cudaError_t e = ctx->precision == MCRT_PREC_FP64 ? launch_transport_fp64(P, grid, ctx->stream)
+                                                    : launch_transport_mixed(P, grid, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->last_ms = ms;
+  CK(cudaGetLastError());
+  return MCRT_OK;
+}
+
+int mcrt_mark(mcrt_ctx* ctx, int32_t slot) {
+  if (!ctx || slot < 0 || slot >= 16) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->marks[slot]) CK(cudaEventCreate(&ctx->marks[slot]));
+  CK(cudaEventRecord(ctx->marks[slot], ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_elapsed_ms(mcrt_ctx* ctx, int32_t a, int32_t b, double* ms) {
+  if (!ctx || !ms || a < 0 || a >= 16 || b < 0 || b >= 16 || !ctx->marks[a] || !ctx->marks[b]) return MCRT_ERR_ARG;
+  CK(cudaEventSynchronize(ctx->marks[b]));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, ctx->marks[a], ctx->marks[b]));
+  *ms = f;
+  return MCRT_OK;
+}
+
+int mcrt_flush_l2(mcrt_ctx* ctx) {
+  if (!ctx) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)256 << 20;
+  if (!ctx->d_flush) { int rc = dalloc(ctx, (char**)&ctx->d_flush, bytes); if (rc) return rc; }
+  CK(cudaMemsetAsync(ctx->d_flush, ctx->marks[15] ? 1 : 0, bytes, ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_synchronize(mcrt_ctx* ctx) {
+  if (!ctx) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_last_kernel_ms(mcrt_ctx* ctx, double* ms) {
+  if (!ctx || !ms) return MCRT_ERR_ARG;
+  *ms = ctx->last_ms;
+  return MCRT_OK;
+}
+
+int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
+  if (!ctx || !out) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const DevTallies& t = ctx->dt;
+  const int64_t nc = ctx->ncell;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (!dst) return MCRT_OK;
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return MCRT_OK;
+  };
+  int rc;
+  if ((rc = cp(out->nabs, t.nabs, nc * 4)) || (rc = cp(out->dbig, t.dbig, nc * 4)) || (rc = cp(out->dsg, t.dsg, nc * 4)) ||
+      (rc = cp(out->killed, t.killed, nc * 4)) || (rc = cp(out->dtauabs, t.dtauabs, nc * 8)) ||
+      (rc = cp(out->fuvmean, t.fuvmean, nc * 8)) || (rc = cp(out->scalars, t.scal, MCRT_NSCALARS * 8)) ||
+      (rc = cp(out->counters, t.cnt, MCRT_NCOUNTERS * 8)))
+    return rc;
+  // FP64 device sums -> the reference's REAL arrays
+  float* sed[10] = {out->si, out->sq, out->su, out->sv, out->si2, out->sq2, out->su2, out->sv2, out->nums, out->aveinc};
+  float* ps[9] = {out->ti, out->tq, out->tu, out->tv, out->ti2, out->tq2, out->tu2, out->tv2, out->numt};
+  float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
+  int64_t nmax = std::max(ctx->nsed, std::max(ctx->npsed, ctx->nimg));
+  float* d_f = nullptr;
+  if ((rc = dalloc(ctx, &d_f, nmax))) return rc;
+  std::vector<std::pair<float*, std::pair<const double*, int64_t>>> jobs;
+  for (int k = 0; k < 10; ++k) jobs.push_back({sed[k], {t.sed + k * ctx->nsed, ctx->nsed}});
+  for (int k = 0; k < 9; ++k) jobs.push_back({ps[k], {t.psed + k * ctx->npsed, ctx->npsed}});
+  for (int k = 0; k < 4; ++k) jobs.push_back({im[k], {t.img + k * ctx->nimg, ctx->nimg}});
+  for (auto& j : jobs) {
+    if (!j.first || j.second.second == 0) continue;
+    const int64_t n = j.second.second;
+    to_float<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, ctx->stream>>>(j.second.first, d_f, n);
+    if ((rc = cp(j.first, d_f, n * 4))) { dfree(ctx, d_f); return rc; }
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_f);
+  return MCRT_OK;
+}
+
+int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
+  (void)in;
+  return fail(ctx, MCRT_ERR_UNSUPPORTED, "mcrt_accumulate_tallies: use the device-side all-reduce path");
+}
+
+int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* tdave, int32_t* converge, double* sig) {
+  if (!ctx || !tdave || !converge) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (nphot < 1) return fail(ctx, MCRT_ERR_ARG, "nphot must be positive");
+  CK(cudaSetDevice(ctx->device));
+  const mcrt_config& c = ctx->cfg;
+  const int64_t nc = ctx->ncell;
+  double* d_td = nullptr;
+  int rc;
+  if ((rc = dalloc(ctx, &d_td, 3 * nc))) return rc;
+  CK(cudaMemcpyAsync(d_td, tdave, nc * 8, cudaMemcpyHostToDevice, ctx->stream));
+  TfinalArgs a{};
+  a.nrg = c.nrg; a.ntg = c.ntg; a.npg = c.npg; a.nT = c.nT; a.nphot = nphot; a.maxii = iter > 3 ? 20 : 1;
+  a.rstar = c.rstar; a.tstar = c.tstarave;
+  a.Tint = ctx->d_tabs + ctx->off_Tint;
+  a.kappap = ctx->d_tabs + ctx->off_kappap;
+  a.kappav = ctx->dm.kappav;
+  a.dtauabs = ctx->dt.dtauabs; a.vcell = ctx->d_vcell; a.dens = ctx->d_dens_thermal; a.tdust = ctx->d_tdust;
+  a.idust3 = ctx->d_idust3; a.diffus = ctx->d_diffus;
+  a.told = d_td; a.tnew = d_td + nc; a.tdave = d_td + 2 * nc;
+  std::vector<double> old(tdave, tdave + nc);
+  tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
+  tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
+  tdust_from_tdave<<<512, 256, 0, ctx->stream>>>(nc, a.tdave, ctx->d_diffus, ctx->d_idust3, ctx->d_cells, ctx->d_tdust);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(tdave, a.tdave, nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, d_td);
+  // convergence statistics (tfinal_5_test1.f90:307-348)
+  const double T01 = 0.1 / 11605.0;
+  double s[3] = {0, 0, 0}, s2[3] = {0, 0, 0};
+  int64_t n[3] = {0, 0, 0};
+  for (int ir = 1; ir <= c.nrg - 1; ++ir) {
+    for (int it = 1; it <= (c.ntg - 1) / 2; ++it) {
+      const int64_t k = (ir - 1) + (int64_t)c.nrg * (it - 1);
+      const double told = old[k], tnew = tdave[k];
+      const double d = (tnew - told) / tnew;
+      if (tnew != told && tnew > T01 && told > T01) { s[0] += std::fabs(d); s2[0] += d * d; n[0]++; }
+      if (tnew > T01 && told > T01) { s[1] += std::fabs(d); s2[1] += d * d; n[1]++; }
+      if (ctx->h_rarr[ir - 1] / c.autors < 5.0 && tnew > T01 && told > T01) { s[2] += std::fabs(d); s2[2] += d * d; n[2]++; }
+    }
+  }
+  double sg[3];
+  for (int k = 0; k < 3; ++k) {
+    const double av = s[k] / (double)n[k], av2 = s2[k] / (double)n[k];
+    sg[k] = std::sqrt(av2 - av * av);
+    if (sig) sig[k] = sg[k];
+  }
+  // convergence when sigma changes by less than 25% between iterations
+  if (*converge == 0 && ctx->prev_sig > 0.0 && std::fabs(ctx->prev_sig - sg[0]) / sg[0] < 0.25) *converge = 1;
+  ctx->prev_sig = sg[0];
+  return MCRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// mcrt_device.cuh -- device-side data layout of the B200 photon-packet engine.
+//
+// The model lives in HBM in a transport-friendly layout built once per
+// upload by the host (mcrt_b200.cu):
+//   * walls (rarr/r2arr/costarr/tan2arr/phiarr/aarr/barr) as plain FP64
+//     vectors (a few KB, L1/L2 resident);
+//   * one CellRec per cell (Fortran linear order over nrg x ntg x npg) with
+//     the non-zero density components of densarr(ir,it,ip,1:10) in id order
+//     and their opacity-species slot (findopac mapped to a compact slot of
+//     the species the model actually references), so a crossing reads one
+//     32-byte record instead of 10 strided densarr/findopac pairs;
+//   * per-species dust tables (nudust, kappad, adust, gdust, pldust) and the
+//     normalised emissivity CDFs kapint(nT,nnu,species).
+// Tallies are FP64 on the device (the reference's REAL tallies are produced
+// by the download) and are updated with atomics.
+#pragma once
+#include <cstdint>
+
+#include "../../include/mcrt_b200.h"
+
+namespace mcrt {
+
+constexpr int kMaxComp = 3;   // non-zero density components per cell
+constexpr int kMaxSlot = 8;   // distinct opacity species referenced by the grid
+constexpr int kTransportBlock = 128;  // threads per transport block
+
+struct __align__(16) CellRec {
+  double rho[kMaxComp];       // densarr of the non-zero components, id order
+  uint32_t meta;              // bits 0-1: n; per comp k: slot (3 bits) at 2+7k, id-1 (4 bits) at 5+7k
+  uint32_t flags;             // bit 0: diffus
+};
+static_assert(sizeof(CellRec) == 32, "CellRec must stay 32 bytes");
+
+__host__ __device__ inline int cell_n(uint32_t meta) { return (int)(meta & 3u); }
+__host__ __device__ inline int cell_slot(uint32_t meta, int k) { return (int)((meta >> (2 + 7 * k)) & 7u); }
+__host__ __device__ inline int cell_id(uint32_t meta, int k) { return (int)((meta >> (5 + 7 * k)) & 15u) + 1; }
+
+struct DevTallies {
+  int32_t *nabs, *dbig, *dsg, *killed;     // [ncell]
+  double *dtauabs, *fuvmean;               // [ncell]
+  double *sed;                             // [10][nsed]
+  double *psed;                            // [9][npsed]
+  double *img;                             // [4][nimg]
+  double *scal;                            // [MCRT_NSCALARS]
+  unsigned long long *cnt;                 // [MCRT_NCOUNTERS]
+};
+
+struct DevModel {
+  // sizes
+  int nrg, ntg, npg, nopac, nlammax, nT, nnu, nhnu;
+  int nfreq, nmu, nph, nap, npeel, nxhst;
+  int nslot;
+  int output_imcube, partial_peeloff, limb, iplanckst, idust, iffuv, ispot, nspot;
+  int64_t ncell, nsed, npsed, nimg;
+  // scalars
+  double rstar, rmincgs, tstar, tshock, fspot, rmaxi, fractxh, numin, lnurat, ifuv_ori;
+  double cspot1, sspot1, scspot1, ssspot1, cspot2, sspot2, scspot2, ssspot2, csprad;
+  // walls
+  const double *rarr, *r2arr, *thetarr, *costarr, *tan2arr, *phiarr, *aarr, *barr;
+  // cells
+  const CellRec *cells;
+  const double *tdust, *vcell;
+  // species: slot -> species (1-based) and the species tables
+  int slot_species[kMaxSlot];
+  const int32_t *nlambda;
+  const double *nudust, *kappad, *adust, *gdust, *pldust, *kappav;
+  const double *kapint, *lTint, *nuint;
+  // star
+  const double *atmosnu, *hnuint, *lognu, *loghnu, *limb_prob;
+  const double *inczeta;                     // [MCRT_IZMAX]
+  // observer
+  const double *aperture2, *u, *sini, *coste, *sinte, *cospe, *sinpe;
+  // random-number jump tables: a^(2^30 * 2^k) mod m, k = 0..63
+  const int64_t *jump1, *jump2;
+};
+
+struct LaunchParams {
+  DevModel m;
+  DevTallies t;
+  int64_t np, lo, hi;           // iteration size and this launch's packet range
+  int64_t block0;               // first random block of the iteration: (iter-1)*np
+  int64_t ns, npacc, npaccstar; // packet split (newdisktherm_5_fuv.f90:158-191)
+  int32_t ipeel, ips;
+  int32_t g1, g2;               // generator initial seeds
+  unsigned long long *next;     // dynamic packet counter
+  mcrt_packet_log *log;
+  int64_t nlog;
+  int32_t *err;                 // device error flags
+};
+
+}  // namespace mcrt

@@ -1,0 +1,20 @@
+// mcrt_fp64.cu -- FP64 transport build.  Compiled with --fmad=false so that
+// every FP64 add/multiply is a separate IEEE operation, as in the oracle.
+#include <cuda_runtime.h>
+
+#include "mcrt_transport.cuh"
+
+namespace mcrt {
+
+cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t s) {
+  transport_fp64<<<grid, kBlock, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+int transport_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_fp64, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+}  // namespace mcrt

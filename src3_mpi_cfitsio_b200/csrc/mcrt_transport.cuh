@@ -1,0 +1,1091 @@
+// mcrt_transport.cuh -- FP64 photon-packet transport kernel for sm_100a.
+//
+// One persistent kernel runs the whole packet life of the reference's loop
+// `do iphot=1,np` (newdisktherm_5_fuv.f90:220-491): emission, the cell walk
+// (tauint_3d_2_fuv.f90:5-210), interactions (propagate_5_fuv.f90:76-218),
+// peel-off walks (peeloff_3d_2_test.f90:7-347) and the exit binning
+// (propagate_5_fuv.f90:231-320).  Threads fetch packets from a global counter,
+// so a lane whose packet leaves the grid early starts the next packet instead
+// of idling behind a long-lived one.
+//
+// The arithmetic is written in the reference's operation order; compiled
+// with --fmad=false the FP64 kernel performs the same IEEE operations as the
+// CPU oracle, and differs from it only by the last-place behaviour of the
+// transcendental functions (log, exp, sin, cos, acos, atan2, pow).
+//
+// Per-thread opacity state (kapd, albedo, g, pl of the species slots the
+// model references) lives in shared memory, indexed [slot][thread], so the
+// data-dependent slot lookups of a crossing do not spill to local memory.
+#pragma once
+#include "mcrt_device.cuh"
+
+namespace mcrt {
+
+constexpr double PI = 3.1415926535897932384626433;
+constexpr double R2P = 2.0 * PI;
+constexpr double RSOL = 6.9598e10;
+constexpr double HUGE_D = 1.7976931348623157e308;
+constexpr int kBlock = kTransportBlock;
+// watchdog: a packet is killed after this many interactions in total (the
+// reference only kills after 10000 in one cell, propagate_5_fuv.f90:208-213)
+constexpr int64_t kMaxEvents = 100000000;
+
+// --------------------------------------------------------------- RNG ----
+struct Rng {
+  int32_t s1, s2;
+  int32_t ndraws;
+  // random_large_integer (ecuyer_cote_mod.f90:252-293), Schrage steps
+  __device__ __forceinline__ double ran() {
+    int32_t k = s1 / 53668;
+    s1 = 40014 * (s1 - k * 53668) - k * 12211;
+    if (s1 < 0) s1 += 2147483563;
+    k = s2 / 52774;
+    s2 = 40692 * (s2 - k * 52774) - k * 3791;
+    if (s2 < 0) s2 += 2147483399;
+    int32_t z = s1 - s2;
+    if (z < 1) z += 2147483562;
+    ++ndraws;
+    return (double)z * 4.656613057e-10;
+  }
+};
+
+__device__ __forceinline__ int64_t mulmod(int64_t a, int64_t b, int64_t m) {
+  return (int64_t)(((unsigned long long)a * (unsigned long long)b) % (unsigned long long)m);
+}
+
+// Block `b` of the generator seeded (g1,g2): a^(b*2^30) * g mod m via the
+// precomputed squares a^(2^30*2^k) (reinitialize_current_generator(1) b times).
+__device__ __forceinline__ Rng rng_block(const DevModel& m, int32_t g1, int32_t g2, int64_t b) {
+  int64_t r1 = g1, r2 = g2;
+  for (int k = 0; b != 0; ++k, b >>= 1) {
+    if (b & 1) {
+      r1 = mulmod(r1, m.jump1[k], 2147483563);
+      r2 = mulmod(r2, m.jump2[k], 2147483399);
+    }
+  }
+  Rng r;
+  r.s1 = (int32_t)r1;
+  r.s2 = (int32_t)r2;
+  r.ndraws = 0;
+  return r;
+}
+
+// ------------------------------------------------------------ helpers ---
+__device__ __forceinline__ double chk(double x) { return x > 1.0 ? 1.0 : (x < -1.0 ? -1.0 : x); }
+
+// locate (nr_2.f:131-154), 1-based result
+__device__ __forceinline__ int locate(const double* xx, int n, double x) {
+  int jl = 0, ju = n + 1;
+  const bool asc = xx[n - 1] > xx[0];
+  while (ju - jl > 1) {
+    int jm = (ju + jl) >> 1;
+    if (asc == (x > xx[jm - 1])) jl = jm; else ju = jm;
+  }
+  if (jl == 0 && x == xx[0]) jl = 1;
+  return jl;
+}
+
+// closest_wall.f90 selector
+struct Walls {
+  double tn1, tp1, tp2;
+  int ip1, ip2;
+  __device__ __forceinline__ void reset() { tn1 = -HUGE_D; tp1 = HUGE_D; tp2 = HUGE_D; ip1 = 0; ip2 = 0; }
+  __device__ __forceinline__ void insert(double t, int i) {
+    if (t < 0.0) {
+      if (t > tn1) tn1 = t;
+    } else if (t < tp1) {
+      tp2 = tp1; ip2 = ip1; tp1 = t; ip1 = i;
+    } else if (t < tp2) {
+      tp2 = t; ip2 = i;
+    }
+  }
+  __device__ __forceinline__ void next(bool on_wall, double& t, int& i) const {
+    if (on_wall && !(fabs(tn1) < fabs(tp1))) { t = tp2; i = ip2; }
+    else { t = tp1; i = ip1; }
+  }
+};
+
+// Shared per-thread species state: S[q][slot][tid]
+struct SpecState {
+  double* base;
+  int tid;
+  __device__ __forceinline__ double& kapd(int s) const { return base[(0 * kMaxSlot + s) * kBlock + tid]; }
+  __device__ __forceinline__ double& alb(int s) const { return base[(1 * kMaxSlot + s) * kBlock + tid]; }
+  __device__ __forceinline__ double& g(int s) const { return base[(2 * kMaxSlot + s) * kBlock + tid]; }
+  __device__ __forceinline__ double& pl(int s) const { return base[(3 * kMaxSlot + s) * kBlock + tid]; }
+  __device__ __forceinline__ double& kap(int s) const { return base[(4 * kMaxSlot + s) * kBlock + tid]; }
+};
+
+enum KapdOrder { KAPD_DISK = 0, KAPD_PROPAGATE = 1, KAPD_TAUINT = 2 };
+
+struct Packet {
+  const DevModel& m;
+  const DevTallies& T;
+  SpecState sp;
+  Rng rng;
+  double xp, yp, zp, rsq, rtot, ux, uy, uz, tau;
+  double cost, sint, cosp, sinp, phi, sip, sqp, sup, svp, nub, ifuv;
+  double cosb, sinb, lp;
+  int ir, it, ip;
+  bool on_wall;
+  int iflag, i_orig, exitflag;
+  int nscat, nabsev, ncross, nstar;
+  unsigned long long c_cross, c_peel, c_pcross, c_pbin, c_reset;
+
+  __device__ Packet(const DevModel& mm, const DevTallies& tt, double* sbase)
+      : m(mm), T(tt) {
+    sp.base = sbase;
+    sp.tid = threadIdx.x;
+    c_cross = c_peel = c_pcross = c_pbin = c_reset = 0;
+  }
+
+  __device__ __forceinline__ double ran() { return rng.ran(); }
+
+  // opacset (dust_5.f90:9-109) for the referenced species, then kapd with
+  // the association order of the calling site.
+  __device__ void opacset(double nu, int order) {
+    for (int s = 0; s < m.nslot; ++s) {
+      const int id = m.slot_species[s] - 1;
+      const int nl = m.nlammax;
+      const double* nud = m.nudust + (int64_t)nl * id;
+      const int n = m.nlambda[id];
+      int a, b;
+      double f;
+      if (nu >= __ldg(nud)) { a = 0; b = 0; f = 0.0; }
+      else if (nu <= __ldg(nud + n - 1)) { a = n - 1; b = n - 1; f = 0.0; }
+      else {
+        int i0 = 1, i1 = n;
+        while (i1 - i0 > 1) {
+          int i = (i1 + i0) >> 1;
+          if (nu <= __ldg(nud + i - 1)) i0 = i; else i1 = i;
+        }
+        a = i1 - 1; b = i0 - 1;
+        f = (nu - __ldg(nud + a)) / (__ldg(nud + b) - __ldg(nud + a));
+      }
+      const double* kd = m.kappad + (int64_t)nl * id;
+      const double* ad = m.adust + (int64_t)nl * id;
+      const double* gd = m.gdust + (int64_t)nl * id;
+      const double* pd = m.pldust + (int64_t)nl * id;
+      double kap, alb, gg, pll;
+      if (a == b) {
+        kap = __ldg(kd + a); alb = __ldg(ad + a); gg = __ldg(gd + a); pll = __ldg(pd + a);
+      } else {
+        const double fm1 = 1.0 - f;
+        gg = fm1 * __ldg(gd + a) + f * __ldg(gd + b);
+        pll = fm1 * __ldg(pd + a) + f * __ldg(pd + b);
+        kap = fm1 * __ldg(kd + a) + f * __ldg(kd + b);
+        alb = fm1 * __ldg(ad + a) + f * __ldg(ad + b);
+      }
+      const double kv = __ldg(m.kappav + id);
+      double kd_;
+      if (order == KAPD_DISK) kd_ = kap * m.rmincgs * kv;
+      else if (order == KAPD_PROPAGATE) kd_ = kap * m.rstar * RSOL * kv;
+      else kd_ = kap * RSOL * m.rstar * kv;
+      sp.kapd(s) = kd_;
+      sp.alb(s) = alb;
+      sp.g(s) = gg;
+      sp.pl(s) = pll;
+      sp.kap(s) = kap;
+    }
+  }
+
+  __device__ __forceinline__ static bool is_fuv(double nu) { return nu <= 13.6 && nu >= 6.0; }
+
+  // ------------------------------------------------------ frequencies
+  __device__ double bbfreq(double teff) {          // random.f90:197-225
+    double z0 = __ldg(m.inczeta + MCRT_IZMAX - 1) * ran();
+    double z1 = ran(), z2 = ran(), z3 = ran(), z4 = ran();
+    int i = 1;
+    while (z0 > __ldg(m.inczeta + i - 1)) ++i;
+    return -log(z1 * z2 * z3 * z4) * teff / (double)i;
+  }
+  __device__ double atmosfreq() {                  // starbarb_2.f90:124-153
+    double xi = ran();
+    int i = locate(m.hnuint, m.nhnu, xi);
+    i = min(max(i, 1), m.nhnu - 1);   // a CDF that does not span [0,1) cannot index outside the table
+    if (i > 1) {
+      double logatm = m.lognu[i - 1] + (m.lognu[i] - m.lognu[i - 1]) / (m.loghnu[i] - m.loghnu[i - 1]) *
+                                           (log10(xi) - m.loghnu[i - 1]);
+      return pow(10.0, logatm);
+    }
+    return m.atmosnu[i - 1] + (m.atmosnu[i] - m.atmosnu[i - 1]) / (m.hnuint[i] - m.hnuint[i - 1]) * (xi - m.hnuint[i - 1]);
+  }
+  __device__ double lucydustfreq(double T0, int idust2) {   // lucydustfreq_2_test.f90:19-160
+    const int nT = m.nT, nnu = m.nnu;
+    const double Tmax = 199999.0;
+    if (T0 >= Tmax / 11605.0) return bbfreq(T0);
+    double lT0 = log(T0);
+    double xi = ran();
+    const double l1 = __ldg(m.lTint), ln = __ldg(m.lTint + nT - 1);
+    int j = (int)((double)(nT - 1) * (lT0 - l1) / (ln - l1)) + 1;
+    j = min(max(j, 1), nT - 1);
+    double f = (lT0 - __ldg(m.lTint + j - 1)) / (__ldg(m.lTint + j) - __ldg(m.lTint + j - 1));
+    if (f < 0.0) f = 0.0;
+    if (f > 1.0) f = 1.0;
+    const double* K = m.kapint + (int64_t)nT * nnu * (idust2 - 1);
+    auto kap = [&](int jj, int ii) { return __ldg(K + (jj - 1) + (int64_t)nT * (ii - 1)); };
+    int i0 = 1, i1 = nnu;
+    double P0 = (1.0 - f) * kap(j, i0) + f * kap(j + 1, i0);
+    if (xi < P0) {
+      if (P0 > 0.0) return T0 * xi * __ldg(m.nuint) / P0;
+      return T0 * __ldg(m.nuint);
+    }
+    double P1 = (1.0 - f) * kap(j, i1) + f * kap(j + 1, i1);
+    if (P1 > 1.0) P1 = 1.0;
+    if (xi >= P1) {
+      if (P1 < 1.0 && xi < 1.0) return T0 * __ldg(m.nuint + nnu - 1) * (1.0 - P1) / (1.0 - xi);
+      return T0 * __ldg(m.nuint + nnu - 1);
+    }
+    while (i1 - i0 > 1) {
+      int i = (i0 + i1) >> 1;
+      double P = (1.0 - f) * kap(j, i) + f * kap(j + 1, i);
+      if (P > 1.0) P = 1.0;
+      if (P < P0) { P0 = P; i0 = i; }
+      if (P > P1) { P1 = P; i1 = 1; }
+      if (P > xi) { i1 = i; P1 = P; } else { i0 = i; P0 = P; }
+    }
+    if (xi < P0) f = 0.0;
+    else if (xi > P1) f = 1.0;
+    else if (P0 <= 0.0) f = 0.5;
+    else if (P1 <= 0.0 || xi <= 0.0) { }
+    else f = log(xi / P0) / log(P1 / P0);
+    return T0 * __ldg(m.nuint + i0 - 1) * pow(__ldg(m.nuint + i1 - 1) / __ldg(m.nuint + i0 - 1), f);
+  }
+
+  // ---------------------------------------------------------- emission
+  __device__ void initp_sample() {                 // initp_common.f90:1-29
+    if (m.limb == 0) {
+      cost = sqrt(ran());
+    } else {                                       // samptabl.f90:29-65
+      double xr = ran();
+      int n = min(max(locate(m.limb_prob, 100, xr), 1), 99);
+      const double delmu = 1.0 / 100.0;
+      double xmu1 = delmu * (double)(n + 1);
+      cost = xmu1 - (m.limb_prob[n] - xr) / (m.limb_prob[n] - m.limb_prob[n - 1]) * delmu;
+    }
+    sint = sqrt(1.0 - cost * cost);
+    phi = R2P * ran();
+    cosp = cos(phi);
+    sinp = sin(phi);
+  }
+  __device__ void initp_transform() {              // initp_common.f90:31-94
+    if (fabs(cosb) < 0.9999999) {
+      double costi = cost * cosb - sint * sinb * cosp;
+      if (fabs(costi) > 1.0) {
+        if (costi > 1.0) costi = 1.0;
+        if (cost < -1.0) costi = -1.0;
+      }
+      double sinti = sqrt(1.0 - costi * costi);
+      double phinew;
+      if (sinti > 0.0000001) {
+        double cospn = (cost - costi * cosb) / (sinti * sinb);
+        if (fabs(cospn) > 1.0) cospn = (cospn < 0.0) ? -1.0 : 1.0;
+        if (phi < PI) {
+          phinew = acos(cospn);
+          if (phinew > PI) phinew = PI;
+        } else {
+          phinew = R2P - acos(cospn);
+          if (phinew < PI) phinew = PI;
+        }
+      } else {
+        phinew = 0.0;
+      }
+      phi = phinew;
+      cost = costi;
+      sint = sinti;
+    } else if (cosb < 0.0) {
+      cost = -cost;
+    }
+    phi = phi + lp;
+    if (phi > R2P) phi = phi - R2P;
+    if (phi < 0.0) phi = phi + R2P;
+    sinp = sin(phi);
+    cosp = cos(phi);
+  }
+  __device__ void initpspot(int ispotph) {         // initpspot.f90:3-175
+    sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+    for (;;) {
+      for (;;) {
+        double xr = ran();
+        cosb = 1.0 - 2.0 * xr;
+        sinb = sqrt(1.0 - cosb * cosb);
+        if (cosb != 0.0 && fabs(cosb) < 1.0) break;
+      }
+      lp = R2P * ran();
+      if (m.ispot == 1) {
+        double cphi = cos(lp), sphi = sin(lp);
+        double dotsp1 = m.scspot1 * sinb * cphi + m.ssspot1 * sinb * sphi + m.cspot1 * cosb;
+        double dotsp2 = m.scspot2 * sinb * cphi + m.ssspot2 * sinb * sphi + m.cspot2 * cosb;
+        if (m.nspot == 1) {
+          if (ispotph == 1 && dotsp1 < m.csprad) continue;
+        } else {
+          if (ispotph == 1 && dotsp1 < m.csprad && dotsp2 < m.csprad) continue;
+        }
+        if (m.fspot < 1.0) {
+          double dellon = (lp < PI) ? lp : R2P - lp;
+          double costhp = m.cspot1 * cosb + m.sspot1 * sinb * cos(dellon);
+          if (costhp > m.csprad) ispotph = 1;
+          if (m.nspot == 2) {
+            dellon = (lp < PI) ? PI - lp : lp - PI;
+            costhp = m.cspot2 * cosb + m.sspot2 * sinb * cos(dellon);
+            if (costhp > m.csprad) ispotph = 1;
+          }
+        }
+      }
+      break;
+    }
+    initp_sample();
+    initp_transform();
+    if (m.fspot == 1.0) nub = (m.iplanckst == 0) ? atmosfreq() : bbfreq(m.tshock);
+    else if (ispotph == 0) nub = (m.iplanckst == 0) ? atmosfreq() : bbfreq(m.tstar);
+    else nub = bbfreq(m.tshock);
+  }
+  __device__ void initp_ps(int ispotph) {          // initp_ps (initp_common.f90 family)
+    sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+    for (;;) {
+      double xr = ran();
+      cosb = chk(1.0 - 2.0 * xr);
+      sinb = chk(sqrt(1.0 - cosb * cosb));
+      if (cosb != 0.0) break;
+    }
+    cost = cosb;
+    sint = sinb;
+    lp = R2P * ran();
+    phi = lp;
+    sinp = chk(sin(phi));
+    cosp = chk(cos(phi));
+    if (ispotph == 0) nub = (m.iplanckst == 0) ? atmosfreq() : bbfreq(m.tstar);
+    else nub = bbfreq(m.tshock);
+  }
+  __device__ void initpabs() {                     // initpabs.f90:1-44
+    sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+    cosb = zp / rtot;
+    sinb = sqrt(1.0 - cosb * cosb);
+    lp = atan2(yp, xp);
+    initp_sample();
+    initp_transform();
+    ux = sint * cosp;
+    uy = sint * sinp;
+    uz = cost;
+    nub = atmosfreq();
+  }
+
+  // -------------------------------------------------------------- grid
+  // testgrid.f90:1-128.  For npg == 2 the phi checks can never fire
+  // (phi in [0,2pi) against phiarr = [0,2pi]), so atan2 is only evaluated
+  // when a re-location needs it.
+  __device__ void testgrid(double& x, double& y, double& z, double& rs, double& rt, int& r, int& t, int& p, bool& onw) {
+    const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
+    const double tol = 1.0e-4;
+    const double* r2 = m.r2arr;
+    const double* ca = m.costarr;
+    const double* pa = m.phiarr;
+    double cb = chk(z / rt);
+    const bool need_phi = npg > 2;
+    double ph = 0.0;
+    if (need_phi) {
+      ph = atan2(y, x);
+      if (ph < 0.0) ph = ph + R2P;
+    }
+    bool reset = false;
+    if ((rs - __ldg(r2)) / (__ldg(r2 + 1) - __ldg(r2)) < -tol ||
+        (rs - __ldg(r2 + nrg - 2)) / (__ldg(r2 + nrg - 1) - __ldg(r2 + nrg - 2)) > 1.0 + tol) {
+      const double third = (double)(1.0f / 3.0f);
+      const double r1 = m.rarr[0], rn = m.rarr[nrg - 1];
+      rt = pow(ran() * (pow(rn, 3.0) - pow(r1, 3.0)) + pow(r1, 3.0), third);
+      reset = true;
+    }
+    if ((cb - __ldg(ca)) / (__ldg(ca + 1) - __ldg(ca)) < -tol ||
+        (cb - __ldg(ca + ntg - 2)) / (__ldg(ca + ntg - 1) - __ldg(ca + ntg - 2)) > 1.0 + tol) {
+      cb = ran() * (__ldg(ca + ntg - 1) - __ldg(ca)) + __ldg(ca);
+      reset = true;
+    }
+    if (need_phi && ((ph - pa[0]) / (pa[1] - pa[0]) < -tol || (ph - pa[npg - 2]) / (pa[npg - 1] - pa[npg - 2]) > 1.0 + tol)) {
+      ph = ran() * (pa[npg - 1] - pa[0]) + pa[0];
+      reset = true;
+    }
+    if (reset) {
+      if (!need_phi) {
+        ph = atan2(y, x);
+        if (ph < 0.0) ph = ph + R2P;
+      }
+      double s = sqrt(1.0 - cb * cb);
+      x = rt * s * cos(ph);
+      y = rt * s * sin(ph);
+      z = rt * cb;
+      rs = rt * rt;
+      onw = false;
+      ++c_reset;
+    }
+    if (r < 1 || r > nrg) r = locate(r2, nrg, rs);
+    if (t < 1 || t > ntg) t = locate(ca, ntg, cb);
+    if (p < 1 || p > npg) {
+      if (!need_phi) { ph = atan2(y, x); if (ph < 0.0) ph = ph + R2P; }
+      p = locate(pa, npg, ph);
+    }
+    const double rfrac = (rs - __ldg(r2 + r - 1)) / (__ldg(r2 + r) - __ldg(r2 + r - 1));
+    const double tfrac = (cb - __ldg(ca + t - 1)) / (__ldg(ca + t) - __ldg(ca + t - 1));
+    bool phierr = false;
+    if (need_phi) {
+      const double pfrac = (ph - pa[p - 1]) / (pa[p] - pa[p - 1]);
+      if (pfrac < -tol || pfrac > 1.0 + tol) {
+        double d1 = ph - pa[p - 1];
+        if (d1 > PI) d1 -= R2P;
+        if (d1 < -PI) d1 += R2P;
+        double d2 = ph - pa[p];
+        if (d2 > PI) d2 -= R2P;
+        if (d2 < -PI) d2 += R2P;
+        phierr = fabs(d1) > tol && fabs(d2) > tol;
+      }
+    }
+    if (rfrac < -tol || rfrac > 1.0 + tol) r = locate(r2, nrg, rs);
+    if (tfrac < -tol || tfrac > 1.0 + tol) t = locate(ca, ntg, cb);
+    if (phierr) p = locate(pa, npg, ph);
+  }
+
+  // radface / thetaface / phiface (radface.f90, thetaface.f90, phiface.f90)
+  __device__ __forceinline__ void faces(Walls& w, double vx, double vy, double vz, double x, double y, double z,
+                                        int r, int t, int p) const {
+    const double bb = 2.0 * (x * vx + y * vy + vz * z);
+    const double rr = x * x + y * y + z * z;
+    double cc = rr - __ldg(m.r2arr + r - 1);
+    double descr = bb * bb - 4.0 * cc;
+    if (descr > 0.0) {
+      descr = sqrt(descr);
+      w.insert((-bb + descr) * 0.5, 1);
+      w.insert((-bb - descr) * 0.5, 1);
+    }
+    cc = rr - __ldg(m.r2arr + r);
+    descr = bb * bb - 4.0 * cc;
+    if (descr > 0.0) {
+      descr = sqrt(descr);
+      w.insert((-bb + descr) * 0.5, 2);
+      w.insert((-bb - descr) * 0.5, 2);
+    }
+    if (m.ntg > 2) {
+      const double t1 = __ldg(m.tan2arr + t - 1), t2 = __ldg(m.tan2arr + t);
+      const double tmp1 = x * vx + y * vy, tmp2 = vx * vx + vy * vy, tmp3 = x * x + y * y;
+      double ta, tb;
+      int i1, i2;
+      if (t2 < t1) { ta = t2; tb = t1; i1 = 4; i2 = 3; }
+      else { ta = t1; tb = t2; i1 = 3; i2 = 4; }
+      if (ta < 0.0) {
+        if (vz != 0.0) w.insert(-z / vz, i1);
+      } else {
+        const double b2 = 2.0 * (tmp1 - ta * vz * z);
+        const double aa = tmp2 - ta * vz * vz;
+        const double c2 = tmp3 - z * z * ta;
+        if (fabs(aa) > 1.0e-10) {
+          double d = b2 * b2 - 4.0 * aa * c2;
+          if (d > 0.0 && ta != 0.0) {
+            d = sqrt(d);
+            w.insert((-b2 + d) * 0.5 / aa, i1);
+            w.insert((-b2 - d) * 0.5 / aa, i1);
+          }
+        } else if (fabs(b2) > 1.0e-10) {
+          w.insert(-c2 / b2, i1);
+        }
+      }
+      const double b2 = 2.0 * (tmp1 - tb * vz * z);
+      const double aa = tmp2 - tb * vz * vz;
+      const double c2 = tmp3 - z * z * tb;
+      if (fabs(aa) > 1.0e-10) {
+        double d = b2 * b2 - 4.0 * aa * c2;
+        if (d > 0.0 && tb != 0.0) {
+          d = sqrt(d);
+          w.insert((-b2 + d) * 0.5 / aa, i2);
+          w.insert((-b2 - d) * 0.5 / aa, i2);
+        }
+      } else if (fabs(b2) > 1.0e-10) {
+        w.insert(-c2 / b2, i2);
+      }
+    }
+    if (m.npg > 2 && m.ntg > 2) {
+      const double A1 = __ldg(m.aarr + p - 1), B1 = __ldg(m.barr + p - 1);
+      const double A2 = __ldg(m.aarr + p), B2 = __ldg(m.barr + p);
+      const double d1 = (A1 * vx + B1 * vy + 0.0 * vz);
+      if (d1 != 0.0) w.insert(-(A1 * x + B1 * y + 0.0 * z + 0.0) / d1, 5);
+      const double d2 = (A2 * vx + B2 * vy + 0.0 * vz);
+      if (d2 != 0.0) w.insert(-(A2 * x + B2 * y + 0.0 * z + 0.0) / d2, 6);
+    }
+  }
+
+  __device__ __forceinline__ int64_t cidx(int r, int t, int p) const {
+    return (int64_t)(r - 1) + (int64_t)m.nrg * ((t - 1) + (int64_t)m.ntg * (p - 1));
+  }
+
+  __device__ __forceinline__ double cell_opac(const CellRec& c) const {   // tauint_3d_2_fuv.f90:59-65
+    const int n = cell_n(c.meta);
+    double opac = 0.0;
+    for (int k = 0; k < n; ++k) opac = opac + sp.kapd(cell_slot(c.meta, k)) * c.rho[k];
+    return opac;
+  }
+
+  __device__ __forceinline__ void tally_abs(int64_t ci, const CellRec& c, double len) {  // tauint_3d_2_fuv.f90:83-98
+    const int n = cell_n(c.meta);
+    double add = 0.0;
+    bool any = false;
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      if (id >= 5 && id <= 8) continue;     // is_sg
+      const int s = cell_slot(c.meta, k);
+      const double v = len * sp.kapd(s) * c.rho[k] * (1.0 - sp.alb(s));
+      add = any ? add + v : v;
+      any = true;
+    }
+    if (any) atomicAdd(T.dtauabs + ci, add);
+    if (m.iffuv) atomicAdd(T.fuvmean + ci, len * (m.rstar * RSOL) * ifuv / __ldg(m.vcell + ci));
+  }
+
+  __device__ __forceinline__ void step_index(int iface, int& r, int& t, int& p) const {
+    switch (iface) {
+      case 1: r = r - 1; break;
+      case 2: r = r + 1; break;
+      case 3: t = t - 1; break;
+      case 4: t = t + 1; break;
+      case 5: p = p - 1; break;
+      default: p = p + 1; break;
+    }
+    if (p == 0) p = m.npg - 1;
+    if (p == m.npg) p = 1;
+  }
+
+  // tauint_3d_2_fuv.f90:5-210.  false = geometry failure.
+  __device__ bool tauint() {
+    double tsum = 0.0;
+    for (int guard = 0; guard < 50000000; ++guard) {
+      testgrid(xp, yp, zp, rsq, rtot, ir, it, ip, on_wall);
+      Walls w;
+      w.reset();
+      faces(w, ux, uy, uz, xp, yp, zp, ir, it, ip);
+      double dt;
+      int iface;
+      w.next(on_wall, dt, iface);
+      if (dt < 0.0 || dt == HUGE_D || iface < 1 || iface > 6) return false;
+      const int64_t ci = cidx(ir, it, ip);
+      const CellRec c = m.cells[ci];
+      const double opac = cell_opac(c);
+      const double dtau = opac * dt;
+      if (tsum + dtau > tau) {
+        const double ds = (tau - tsum) / opac;
+        tally_abs(ci, c, ds);
+        xp = xp + ds * ux;
+        yp = yp + ds * uy;
+        zp = zp + ds * uz;
+        rsq = xp * xp + yp * yp + zp * zp;
+        rtot = sqrt(rsq);
+        on_wall = false;
+        return true;
+      }
+      tally_abs(ci, c, dt);
+      step_index(iface, ir, it, ip);
+      xp = xp + dt * ux;
+      yp = yp + dt * uy;
+      zp = zp + dt * uz;
+      on_wall = true;
+      rsq = xp * xp + yp * yp + zp * zp;
+      rtot = sqrt(rsq);
+      tsum = tsum + dtau;
+      ++ncross;
+      ++c_cross;
+      if (ir == m.nrg) { exitflag = 1; return true; }
+      if (ir == 0) {
+        atomicAdd(T.scal + MCRT_S_AFLUX, 1.0);
+        ++nstar;
+        rtot = sqrt(rsq);
+        initpabs();
+        opacset(nub, KAPD_TAUINT);
+        ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;
+        i_orig = 1;
+        iflag = 0;
+        ir = 1;
+        tsum = 0.0;
+      }
+    }
+    return false;
+  }
+
+  // ------------------------------------------------------- scattering
+  __device__ __forceinline__ void dustmat(double bmu, double cosb2, int s, double& p1, double& p2, double& p3) const {
+    const double gg = sp.g(s);
+    const double g2 = gg * gg;
+    const double temp = (g2 + 1.0) - (2.0 * gg) * bmu;
+    p1 = 1.5 * (1.0 - g2) / (2.0 + g2) * (1.0 + cosb2) / (temp * sqrt(temp));
+    p2 = -sp.pl(s) * p1 * (1.0 - cosb2) / (1.0 + cosb2);
+    p3 = p1 * 2.0 * bmu / (1.0 + cosb2);
+  }
+
+  // Rotation/phase-matrix product shared by stokes and stokespeel
+  // (stokes.f90:183-216 and :284-317; stokespeel.f90:193-210, :293-309).
+  struct Mat { double a11, a12, a13, a21, a22, a23, a31, a32, a33, a43, a44; };
+
+  __device__ void stokes(int s) {                  // stokes.f90:1-340 (p4 = 0)
+    const double costp = cost, sintp = sint, phip = phi;
+    const double gg = sp.g(s);
+    const double g2 = gg * gg;
+    double peak;
+    {
+      double temp = (gg > 0.0) ? (g2 + 1.0) - (2.0 * gg) : (g2 + 1.0) + (2.0 * gg);
+      peak = 1.5 * (1.0 - g2) / (2.0 + g2) * 2.0 / temp / sqrt(temp);
+      peak = peak * 1.01;
+    }
+    double bmu, cosb2, sinbt, p1, p2, p3, a, ci, si_, c2i, s2i;
+    bool upper;
+    for (;;) {
+      bmu = 1.0 - 2.0 * ran();
+      cosb2 = bmu * bmu;
+      if (m.idust == 0) {
+        p1 = 0.75 * (1.0 + cosb2); p2 = 0.75 * (cosb2 - 1.0) * 1.0; p3 = 0.75 * (2.0 * bmu);
+        peak = 1.501;
+      } else {
+        dustmat(bmu, cosb2, s, p1, p2, p3);
+      }
+      sinbt = sqrt(1.0 - cosb2);
+      const double ri1 = R2P * ran();
+      upper = ri1 > PI;
+      const double ang = upper ? R2P - ri1 : ri1;
+      ci = cos(ang);
+      si_ = sin(ang);
+      s2i = 2.0 * si_ * ci;
+      c2i = 2.0 * ci * ci - 1.0;
+      const double a12 = p2 * c2i;
+      const double a13 = upper ? p2 * s2i : -p2 * s2i;
+      const double rprob = (p1 * sip + a12 * sqp + a13 * sup) / sip;
+      if (rprob > peak) peak = rprob;
+      if (peak * ran() > rprob) continue;
+      a = rprob;
+      break;
+    }
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) {
+      si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0;
+      cost = -costp; sint = sintp;
+    } else {
+      cost = costp * bmu + sintp * sinbt * ci;
+      if (fabs(cost) < 1.0) {
+        sint = fabs(sqrt(1.0 - cost * cost));
+        sini2 = si_ * sintp / sint;
+        const double bott = sint * sinbt;
+        cosi2 = costp / bott - cost * bmu / bott;
+      } else {
+        sint = 0.0; sini2 = 0.0;
+        if (cost >= 1.0) cosi2 = -1.0;
+        if (cost <= -1.0) cosi2 = 1.0;
+      }
+    }
+    double cosdph = upper ? -cosi2 * ci + sini2 * si_ * bmu : -ci * cosi2 + si_ * sini2 * bmu;
+    if (fabs(cosdph) > 1.0) cosdph = (cosdph > 1.0) ? 1.0 : -1.0;
+    phi = upper ? phip + acos(cosdph) : phip - acos(cosdph);
+    if (phi > R2P) phi = phi - R2P;
+    if (phi < 0.0) phi = phi + R2P;
+    const double sin2i2 = 2.0 * sini2 * cosi2, cos2i2 = 2.0 * cosi2 * cosi2 - 1.0;
+    const double sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const double sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    // p4 = 0 in dustmat and the Rayleigh branch, so a24=a34=a42=a43=0
+    double a11 = p1, a12 = p2 * c2i, a13, a21 = p2 * cos2i2, a22 = p1 * cos2 - p3 * sin2, a23, a31, a32;
+    const double a33 = -p1 * sin2 + p3 * cos2, a44 = p3;
+    if (upper) {
+      a13 = p2 * s2i;
+      a23 = p1 * cos2sin1 + p3 * sin2cos1;
+      a31 = -p2 * sin2i2;
+      a32 = -p1 * sin2cos1 - p3 * cos2sin1;
+    } else {
+      a13 = -p2 * s2i;
+      a23 = -p1 * cos2sin1 - p3 * sin2cos1;
+      a31 = p2 * sin2i2;
+      a32 = p1 * sin2cos1 + p3 * cos2sin1;
+    }
+    const double a24 = 0.0 * sin2i2, a34 = 0.0 * cos2i2, a42 = 0.0 * s2i, a43 = 0.0 * c2i;
+    const double nsi = (a11 * sip + a12 * sqp + a13 * sup) / a;
+    const double nsq = (a21 * sip + a22 * sqp + a23 * sup + a24 * svp) / a;
+    const double nsu = (a31 * sip + a32 * sqp + a33 * sup + a34 * svp) / a;
+    const double nsv = (a42 * sqp + a43 * sup + a44 * svp) / a;
+    sip = nsi; sqp = nsq; sup = nsu; svp = nsv;
+    cosp = cos(phi);
+    sinp = sin(phi);
+  }
+
+  // stokespeel.f90:1-328 (no normalisation), sign conventions as stokes
+  __device__ void stokespeel(double& qi, double& qq, double& qu, double& qv, double cst, double snt, double ri1,
+                             double bmu, double costp, double sintp, int s) const {
+    double p1, p2, p3;
+    const double cosb2 = bmu * bmu;
+    if (m.idust == 0) {
+      p1 = 0.75 * (1.0 + cosb2); p2 = 0.75 * (cosb2 - 1.0) * 1.0; p3 = 0.75 * (2.0 * bmu);
+    } else {
+      dustmat(bmu, cosb2, s, p1, p2, p3);
+    }
+    const double sinbt = sqrt(1.0 - cosb2);
+    const bool upper = ri1 > PI;
+    const double ang = upper ? R2P - ri1 : ri1;
+    double ci = cos(ang), si_ = sin(ang);
+    const double s2i = 2.0 * si_ * ci, c2i = 2.0 * ci * ci - 1.0;
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) { si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0; }
+    else if (fabs(cst) < 1.0) {
+      sini2 = si_ * sintp / snt;
+      const double bott = snt * sinbt;
+      cosi2 = costp / bott - cst * bmu / bott;
+    } else {
+      sini2 = 0.0;
+      if (cst >= 1.0) cosi2 = -1.0;
+      if (cst <= -1.0) cosi2 = 1.0;
+    }
+    const double sin2i2 = 2.0 * sini2 * cosi2, cos2i2 = 2.0 * cosi2 * cosi2 - 1.0;
+    const double sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const double sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    double a13, a23, a31, a32;
+    const double a11 = p1, a12 = p2 * c2i, a21 = p2 * cos2i2, a22 = p1 * cos2 - p3 * sin2;
+    const double a33 = -p1 * sin2 + p3 * cos2, a44 = p3;
+    if (upper) {
+      a13 = p2 * s2i; a23 = p1 * cos2sin1 + p3 * sin2cos1; a31 = -p2 * sin2i2; a32 = -p1 * sin2cos1 - p3 * cos2sin1;
+    } else {
+      a13 = -p2 * s2i; a23 = -p1 * cos2sin1 - p3 * sin2cos1; a31 = p2 * sin2i2; a32 = p1 * sin2cos1 + p3 * cos2sin1;
+    }
+    const double a24 = 0.0 * sin2i2, a34 = 0.0 * cos2i2, a42 = 0.0 * s2i, a43 = 0.0 * c2i;
+    const double ni = (a11 * qi + a12 * qq + a13 * qu);
+    const double nq = (a21 * qi + a22 * qq + a23 * qu + a24 * qv);
+    const double nu_ = (a31 * qi + a32 * qq + a33 * qu + a34 * qv);
+    const double nv = (a42 * qq + a43 * qu + a44 * qv);
+    qi = ni; qq = nq; qu = nu_; qv = nv;
+  }
+
+  __device__ __forceinline__ int freq_bin(double nu) const {
+    const double v = (double)m.nfreq * log(nu / m.numin) / m.lnurat;
+    int ib;
+    if (!(v > -2.0e9)) ib = 0;
+    else if (v > 2.0e9) ib = m.nfreq;
+    else ib = (int)v + 1;
+    return min(max(ib, 1), m.nfreq);
+  }
+
+  // ------------------------------------------------------- peel-off
+  // peeloff_3d_2_test.f90:7-347 for one direction
+  __device__ void peeloff(double s_i, int r, int t, int p, int idust2, int peelid) {
+    ++c_peel;
+    bool onw = on_wall;
+    double x1 = xp, y1 = yp, z1 = zp, rs1 = rsq, rt1 = rtot;
+    const double cospe = __ldg(m.cospe + peelid - 1), sinpe = __ldg(m.sinpe + peelid - 1);
+    const double coste = __ldg(m.coste + peelid - 1), sinte = __ldg(m.sinte + peelid - 1);
+    const double ux1 = sinte * cospe, uy1 = sinte * sinpe, uz1 = coste;
+    if (onw) {
+      const bool inner = fabs(rs1 - __ldg(m.r2arr + r - 1)) < fabs(rs1 - __ldg(m.r2arr + r));
+      const bool outwards = ux1 * x1 + uy1 * y1 + uz1 * z1 > 0.0;
+      if (inner && !outwards) {
+        if (r == 1) return;
+        r = r - 1;
+      }
+      if (!inner && outwards) r = r + 1;
+    }
+    double tsum = 0.0;
+    for (int guard = 0;; ++guard) {
+      if (guard > 10000000) return;
+      testgrid(x1, y1, z1, rs1, rt1, r, t, p, onw);
+      Walls w;
+      w.reset();
+      faces(w, ux1, uy1, uz1, x1, y1, z1, r, t, p);
+      double dt;
+      int iface;
+      w.next(onw, dt, iface);
+      if (dt == HUGE_D || iface < 1 || iface > 6) return;
+      const CellRec c = m.cells[cidx(r, t, p)];
+      tsum = tsum + cell_opac(c) * dt;
+      if (tsum > 25.0) return;
+      step_index(iface, r, t, p);
+      x1 = x1 + dt * ux1;
+      y1 = y1 + dt * uy1;
+      z1 = z1 + dt * uz1;
+      onw = true;
+      rs1 = x1 * x1 + y1 * y1 + z1 * z1;
+      rt1 = sqrt(rs1);
+      ++c_pcross;
+      if (r == m.nrg) break;
+      if (r == 0) return;
+    }
+    ++c_pbin;
+    const double factor = exp(-tsum);
+    double qi = s_i * factor, qq = sqp * factor, qu = sup * factor, qv = svp * factor;
+    if (iflag == 1) {
+      // findangle3.f90 with phi2 = phie = 0 (reapar_4_test1.f90:425)
+      double costnew = cost * coste + (sint * sinte * (cosp * cospe + sinp * sinpe));
+      costnew = chk(costnew);
+      const double sintnew = sqrt(1.0 - costnew * costnew);
+      double ri1 = 0.0;
+      if (sint > 1.0e-8 && sintnew > 1.0e-8) {
+        double cosx = (coste - (cost * costnew)) / (sint * sintnew);
+        cosx = chk(cosx);
+        const double x = acos(cosx);
+        if (0.0 > phi) ri1 = (0.0 - phi > PI) ? x : R2P - x;
+        else ri1 = (phi - 0.0 > PI) ? R2P - x : x;
+      }
+      // species of the final walk cell, as the reference indexes findopac
+      int sslot = 0;
+      const CellRec cf = m.cells[cidx(r, t, p)];
+      const int n = cell_n(cf.meta);
+      bool found = false;
+      for (int k = 0; k < n; ++k)
+        if (cell_id(cf.meta, k) == idust2) { sslot = cell_slot(cf.meta, k); found = true; }
+      if (!found) sslot = idust2slot(idust2);
+      stokespeel(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, sslot);
+    }
+    const double yimage = z1 * sinte - y1 * coste * sinpe - x1 * coste * cospe;
+    const double ximage = y1 * cospe - x1 * sinpe;
+    const double vx = (ximage + m.rmaxi) / m.fractxh, vy = (yimage + m.rmaxi) / m.fractxh;
+    const double rho2 = ximage * ximage + yimage * yimage;
+    const int inub = freq_bin(nub);
+    if (m.output_imcube && vx > -1.0e9 && vx < 1.0e9 && vy > -1.0e9 && vy < 1.0e9) {
+      const int ix = (int)vx + 1, iy = (int)vy + 1;
+      if (ix <= m.nxhst && iy <= m.nxhst && ix > 0 && iy > 0) {
+        const int64_t k = (int64_t)(peelid - 1) + (int64_t)m.npeel * ((ix - 1) + (int64_t)m.nxhst * ((iy - 1) + (int64_t)m.nxhst * (inub - 1)));
+        atomicAdd(T.img + k, qi);
+        atomicAdd(T.img + m.nimg + k, qq);
+        atomicAdd(T.img + 2 * m.nimg + k, qu);
+        atomicAdd(T.img + 3 * m.nimg + k, qv);
+      }
+    }
+    const int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
+    const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
+    for (int ia = 1; ia <= m.nap; ++ia) {
+      if (rho2 < __ldg(m.aperture2 + ia - 1)) {
+        for (int k = 0; k < 3; ++k) {
+          const int64_t e = (inub - 1) + (int64_t)m.nfreq * ((peelid - 1) + (int64_t)m.npeel * ((ia - 1) + (int64_t)m.nap * (indx[k] - 1)));
+          double* P = T.psed + e;
+          atomicAdd(P, qi); atomicAdd(P + m.npsed, qq); atomicAdd(P + 2 * m.npsed, qu); atomicAdd(P + 3 * m.npsed, qv);
+          atomicAdd(P + 4 * m.npsed, qi * qi); atomicAdd(P + 5 * m.npsed, qq * qq);
+          atomicAdd(P + 6 * m.npsed, qu * qu); atomicAdd(P + 7 * m.npsed, qv * qv);
+          atomicAdd(P + 8 * m.npsed, 1.0);
+        }
+      }
+    }
+  }
+
+  // slot of a species id whose component is absent in the lookup cell
+  __device__ __forceinline__ int idust2slot(int idust2) const {
+    for (int s = 0; s < m.nslot; ++s)
+      if (m.slot_species[s] == idust2) return s;
+    return 0;
+  }
+
+  // select_dust_2.f90 with mask = is_any; returns component index k (or -1)
+  __device__ int select_dust(const CellRec& c) {
+    const double xran = ran();
+    const int n = cell_n(c.meta);
+    int nn = 0, kk = -1;
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      if (!(id >= 5 && id <= 8)) { ++nn; kk = k; }
+    }
+    if (nn == 1) return kk;
+    double opac = 0.0;
+    for (int k = 0; k < n; ++k) opac = opac + sp.kapd(cell_slot(c.meta, k)) * c.rho[k];
+    if (opac == 0.0) return -1;
+    double frac = 0.0;
+    for (int k = 0; k < n; ++k) {
+      frac = frac + sp.kapd(cell_slot(c.meta, k)) * c.rho[k] / opac;
+      if (xran <= frac + 1.0e-10) return k;
+    }
+    return -1;
+  }
+
+  // ------------------------------------------------------------ packet
+  __device__ int run(int64_t iphot, const LaunchParams& P) {
+    on_wall = false;
+    nscat = nabsev = ncross = nstar = 0;
+    if (iphot < P.npacc || iphot > P.npacc + P.ns) return 3;   // rejected at launch
+    if (iphot < P.npacc + P.npaccstar) {
+      if (P.ips == 0) initpspot(1); else initp_ps(1);
+      if (ran() < 0.5) nub = 1.2398 / 0.06 + ran() * (1.2398 / 0.015 - 1.2398 / 0.06);
+    } else {
+      if (P.ips == 0) initpspot(0); else initp_ps(0);
+    }
+    i_orig = 1;
+    opacset(nub, KAPD_DISK);
+    const double coslp = cos(lp), sinlp = sin(lp);
+    const double rmin = m.rarr[0];
+    zp = cosb * rmin;
+    const double rp = sinb * rmin;
+    xp = rp * coslp;
+    yp = rp * sinlp;
+    rsq = zp * zp + rp * rp;
+    rtot = sqrt(rsq);
+    ux = sint * cosp;
+    uy = sint * sinp;
+    uz = cost;
+    iflag = 0;
+    ir = 1;
+    on_wall = true;
+    it = locate(m.thetarr, m.ntg, acos(cosb));
+    ip = locate(m.phiarr, m.npg, lp);
+    if (P.ipeel == 1 && !m.partial_peeloff) {
+      for (int peelid = 1; peelid <= m.npeel; ++peelid) {
+        if (P.ips == 0) {
+          const double coste = __ldg(m.coste + peelid - 1), sinte = __ldg(m.sinte + peelid - 1);
+          const double cospe = __ldg(m.cospe + peelid - 1), sinpe = __ldg(m.sinpe + peelid - 1);
+          const double cosnorm = cosb * coste + (sinb * sinte * (cospe * coslp + sinpe * sinlp));
+          const double sipnew = (m.limb == 0) ? 4.0 * sip * cosnorm : 12.0 / 5.0 * sip * (cosnorm + cosnorm * cosnorm);
+          if (cosnorm > 0.0) peeloff(sipnew, ir, it, ip, 0, peelid);
+        } else {
+          peeloff(sip * 2.0, ir, it, ip, 0, peelid);
+        }
+      }
+    }
+    ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;
+    return propagate(P);
+  }
+
+  // propagate_5_fuv.f90:1-326
+  __device__ int propagate(const LaunchParams& P) {
+    double xpold = xp, ypold = yp, zpold = zp;
+    iflag = 0;
+    exitflag = 0;
+    int iscat = 0, iint = 0;
+    int64_t nev = 0;
+    tau = -log(ran());
+    if (!tauint()) return 3;
+    if (exitflag != 1) {
+      CellRec c = m.cells[cidx(ir, it, ip)];
+      int k = select_dust(c);
+      if (k < 0) return 3;
+      atomicAdd(T.scal + MCRT_S_TOT, 1.0);
+      for (;;) {
+        const int slot = cell_slot(c.meta, k);
+        const int idust2 = cell_id(c.meta, k);
+        if (ran() <= sp.alb(slot)) {               // scattered
+          iflag = 1;
+          ++iscat;
+          ++iint;
+          ++nscat;
+          if (P.ipeel == 1)
+            for (int peelid = 1; peelid <= m.npeel; ++peelid) peeloff(sip, ir, it, ip, idust2, peelid);
+          stokes(slot);
+        } else {                                    // absorbed + re-emitted
+          ++nabsev;
+          const int64_t ci = cidx(ir, it, ip);
+          if (idust2 >= 5 && idust2 <= 8) atomicAdd(T.dsg + ci, 1); else atomicAdd(T.dbig + ci, 1);
+          if (idust2 == 1 || idust2 == 2 || idust2 == 5 || idust2 == 6 || idust2 == 9) i_orig = 2;
+          else if (idust2 == 3 || idust2 == 7) i_orig = 3;
+          else i_orig = 4;
+          if (!(c.flags & 1u)) atomicAdd(T.nabs + ci, 1);
+          const double tave = __ldg(m.tdust + ci);
+          sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90
+          cost = 1.0 - 2.0 * ran();
+          sint = sqrt(1.0 - cost * cost);
+          phi = R2P * ran();
+          cosp = cos(phi);
+          sinp = sin(phi);
+          nub = lucydustfreq(tave, m.slot_species[slot]);
+          uy = sint * sinp;
+          ux = sint * cosp;
+          uz = cost;
+          iflag = 0;
+          opacset(nub, KAPD_PROPAGATE);
+          ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;
+          if (P.ipeel == 1 && !m.partial_peeloff)
+            for (int peelid = 1; peelid <= m.npeel; ++peelid) peeloff(sip, ir, it, ip, idust2, peelid);
+          ++iint;
+        }
+        tau = -log(ran());
+        xpold = xp; ypold = yp; zpold = zp;
+        ux = sint * cosp;
+        uy = sint * sinp;
+        uz = cost;
+        const int pr = ir, pt = it, pp = ip;
+        if (!tauint()) return 3;
+        if (exitflag == 1) break;
+        if (ir != pr || it != pt || ip != pp) iint = 0;
+        if (m.iffuv && !is_fuv(nub)) return 2;
+        if (iint > 10000 || ++nev > kMaxEvents) {
+          atomicAdd(T.killed + cidx(ir, it, ip), 1);
+          atomicAdd(T.scal + MCRT_S_ABFLUX, 1.0);
+          return 1;
+        }
+        c = m.cells[cidx(ir, it, ip)];
+        k = select_dust(c);
+        if (k < 0) return 3;
+      }
+    }
+    // exit binning (propagate_5_fuv.f90:231-320)
+    int itb = (int)((double)m.nmu * (1.0 - cost) / 2.0) + 1;
+    itb = min(max(itb, 1), m.nmu);
+    if (phi < 0.0) phi = phi + R2P;
+    int ipb = (int)((double)m.nph * phi / R2P) + 1;
+    ipb = min(max(ipb, 1), m.nph);
+    const double ub = __ldg(m.u + itb - 1);
+    const double sini = __ldg(m.sini + itb - 1);
+    const double x = ypold * cosp - xpold * sinp;
+    const double y = zpold * sini - ypold * ub * sinp - xpold * ub * cosp;
+    const double rho2 = x * x + y * y;
+    if (rho2 < __ldg(m.aperture2 + m.nap - 1) * 1.0001) {
+      atomicAdd(T.scal + MCRT_S_FLUX, 1.0);
+      if (iflag == 1) {
+        atomicAdd(T.scal + MCRT_S_SFLUX, 1.0);
+        atomicAdd(T.scal + MCRT_S_NSCAT, (double)iscat);
+      }
+    }
+    const int inub = freq_bin(nub);
+    const int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
+    const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
+    for (int ia = 1; ia <= m.nap; ++ia) {
+      if (rho2 < __ldg(m.aperture2 + ia - 1) && !(iflag == 0 && i_orig == 5)) {
+        for (int kk = 0; kk < 3; ++kk) {
+          const int64_t e = (inub - 1) + (int64_t)m.nfreq * ((itb - 1) + (int64_t)m.nmu * ((ipb - 1) + (int64_t)m.nph * ((ia - 1) + (int64_t)m.nap * (indx[kk] - 1))));
+          double* S = T.sed + e;
+          const int64_t ns = m.nsed;
+          atomicAdd(S, sip); atomicAdd(S + ns, sqp); atomicAdd(S + 2 * ns, sup); atomicAdd(S + 3 * ns, svp);
+          atomicAdd(S + 4 * ns, sip * sip); atomicAdd(S + 5 * ns, sqp * sqp);
+          atomicAdd(S + 6 * ns, sup * sup); atomicAdd(S + 7 * ns, svp * svp);
+          atomicAdd(S + 8 * ns, 1.0); atomicAdd(S + 9 * ns, fabs(cost));
+        }
+      }
+    }
+    if (iflag == 1) atomicAdd(T.scal + MCRT_S_SCOUNT, 1.0);
+    return 0;
+  }
+};
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Persistent transport kernel: every thread fetches packets until the
+// launch's range is exhausted.
+__global__ void __launch_bounds__(kBlock) transport_fp64(LaunchParams P) {
+  __shared__ double spec[5 * kMaxSlot * kBlock];
+  Packet pk(P.m, P.t, spec);
+  const int64_t n = P.hi - P.lo + 1;
+  unsigned long long c_pkt = 0, c_int = 0, c_sca = 0, c_geo = 0, c_kil = 0, c_exit = 0, c_star = 0;
+  for (;;) {
+    const unsigned long long k = atomicAdd(P.next, 1ull);
+    if ((int64_t)k >= n) break;
+    const int64_t iphot = P.lo + (int64_t)k;
+    pk.rng = rng_block(P.m, P.g1, P.g2, P.block0 + iphot - 1);
+    const int st = pk.run(iphot, P);
+    ++c_pkt;
+    c_int += pk.nscat + pk.nabsev;
+    c_sca += pk.nscat;
+    c_star += pk.nstar;
+    if (st == 3) ++c_geo;
+    if (st == 1) ++c_kil;
+    if (st == 0) ++c_exit;
+    if (P.log && (int64_t)k < P.nlog) {
+      mcrt_packet_log& L = P.log[k];
+      L.iphot = iphot; L.nscat = pk.nscat; L.nabs = pk.nabsev; L.ncross = pk.ncross; L.nstar = pk.nstar;
+      L.status = st; L.ir = 0; L.it = 0; L.ip = 0; L.ndraws = pk.rng.ndraws;
+      L.iflag = pk.iflag; L.i_orig = pk.i_orig; L.pad = 0;
+      L.nub = pk.nub; L.cost = pk.cost; L.phi = pk.phi; L.sip = pk.sip; L.sqp = pk.sqp; L.sup = pk.sup; L.svp = pk.svp;
+      L.xp = pk.xp; L.yp = pk.yp; L.zp = pk.zp;
+    }
+  }
+  // warp-aggregated statistics
+  unsigned long long v[12] = {c_pkt, pk.c_cross, c_int, c_sca, pk.c_peel, pk.c_pcross, pk.c_pbin, c_geo,
+                              pk.c_reset, c_kil, c_exit, c_star};
+  for (int i = 0; i < 12; ++i) {
+    unsigned long long s = warp_sum(v[i]);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(P.t.cnt + i, s);
+  }
+}
+
+}  // namespace mcrt

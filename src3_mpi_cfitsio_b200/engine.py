@@ -1,0 +1,205 @@
+"""Host-side mirror of the reference's ``disk`` / Lucy-iteration interface.
+
+``Engine`` drives the CUDA engine through its C ABI (``libmcrt_b200.so``,
+include/mcrt_b200.h) exactly as the Fortran driver would through
+``iso_c_binding``:
+
+* ``Engine.disk(converge, iteration, i1)`` is ``subroutine disk``
+  (newdisktherm_5_fuv.f90:1-663): reset tallies, run the packet loop on the
+  GPU, download the reduced tallies, update the dust temperature (``tfinal``)
+  and return the new ``converge`` flag;
+* ``lucy_iterations`` is the temperature loop of newtts.f90:225-256.
+
+There is no CPU path: if the library cannot be loaded or a call fails, a
+``MCRTError`` is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmcrt_b200.so")
+_lib = None
+
+
+class MCRTError(RuntimeError):
+    pass
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the engine library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MCRTError(f"engine library not built: {path} (run __graft_entry__.build())")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    lib.mcrt_create.argtypes = [P(abi.Config), C.c_int, P(C.c_void_p)]
+    lib.mcrt_upload_grid.argtypes = [C.c_void_p, P(abi.Grid)]
+    lib.mcrt_upload_tables.argtypes = [C.c_void_p, P(abi.Tables)]
+    lib.mcrt_set_precision.argtypes = [C.c_void_p, C.c_int32]
+    lib.mcrt_reset_tallies.argtypes = [C.c_void_p]
+    lib.mcrt_run_iteration.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32]
+    lib.mcrt_download_tallies.argtypes = [C.c_void_p, P(abi.Tallies)]
+    lib.mcrt_accumulate_tallies.argtypes = [C.c_void_p, P(abi.Tallies)]
+    lib.mcrt_update_temperature.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double), P(C.c_int32),
+                                            P(C.c_double)]
+    lib.mcrt_enable_packet_log.argtypes = [C.c_void_p, C.c_int64]
+    lib.mcrt_download_packet_log.argtypes = [C.c_void_p, P(abi.PacketLog), C.c_int64]
+    lib.mcrt_last_kernel_ms.argtypes = [C.c_void_p, P(C.c_double)]
+    lib.mcrt_mark.argtypes = [C.c_void_p, C.c_int32]
+    lib.mcrt_elapsed_ms.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]
+    lib.mcrt_flush_l2.argtypes = [C.c_void_p]
+    lib.mcrt_synchronize.argtypes = [C.c_void_p]
+    lib.mcrt_last_error.argtypes = [C.c_void_p]
+    lib.mcrt_last_error.restype = C.c_char_p
+    lib.mcrt_destroy.argtypes = [C.c_void_p]
+    lib.mcrt_destroy.restype = None
+    lib.mcrt_version.restype = C.c_char_p
+    for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision",
+                 "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
+                 "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
+                 "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_mark", "mcrt_elapsed_ms",
+                 "mcrt_flush_l2", "mcrt_synchronize"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+class Engine:
+    """One GPU context holding one model (the state ``disk`` reads)."""
+
+    def __init__(self, model, device: int = 0, precision: str = "fp64"):
+        self.lib = load_library()
+        self.model = model
+        self.bundle = abi.Bundle(model)
+        self.cfg = self.bundle.config
+        ctx = C.c_void_p()
+        self._check(self.lib.mcrt_create(C.byref(self.cfg), device, C.byref(ctx)), ctx)
+        self.ctx = ctx
+        self.set_precision(precision)
+        self.upload_grid()
+        self.upload_tables()
+        self.tdave = model.grid["tdust"].copy()
+        self.sig = np.full(3, np.nan)
+
+    # ------------------------------------------------------------ plumbing
+    def _check(self, rc, ctx=None):
+        if rc != 0:
+            c = ctx if ctx is not None else self.ctx
+            msg = self.lib.mcrt_last_error(c).decode() if c else ""
+            raise MCRTError(f"mcrt call failed (code {rc}): {msg}")
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.mcrt_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, precision: str):
+        mode = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}[precision]
+        self._check(self.lib.mcrt_set_precision(self.ctx, mode))
+        self.precision = precision
+
+    def upload_grid(self):
+        self.bundle = abi.Bundle(self.model)
+        self._check(self.lib.mcrt_upload_grid(self.ctx, C.byref(self.bundle.grid)))
+
+    def upload_tables(self):
+        self._check(self.lib.mcrt_upload_tables(self.ctx, C.byref(self.bundle.tables)))
+
+    def reset_tallies(self):
+        self._check(self.lib.mcrt_reset_tallies(self.ctx))
+
+    def run(self, np_total: int, lo: int = 1, hi: int | None = None, *, iteration: int = 1, ipeel: int = 1,
+            seeds=(12345678, 87654321), generator: int = 1):
+        hi = np_total if hi is None else hi
+        self._check(self.lib.mcrt_run_iteration(self.ctx, np_total, lo, hi, iteration, ipeel,
+                                                seeds[0], seeds[1], generator))
+
+    def kernel_ms(self) -> float:
+        v = C.c_double()
+        self._check(self.lib.mcrt_last_kernel_ms(self.ctx, C.byref(v)))
+        return v.value
+
+    def mark(self, slot: int):
+        self._check(self.lib.mcrt_mark(self.ctx, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = C.c_double()
+        self._check(self.lib.mcrt_elapsed_ms(self.ctx, a, b, C.byref(v)))
+        return v.value
+
+    def flush_l2(self):
+        self._check(self.lib.mcrt_flush_l2(self.ctx))
+
+    def synchronize(self):
+        self._check(self.lib.mcrt_synchronize(self.ctx))
+
+    def download(self, images: bool = True) -> abi.TallyArrays:
+        tal = abi.TallyArrays(self.cfg, images=images)
+        self._check(self.lib.mcrt_download_tallies(self.ctx, C.byref(tal.struct)))
+        return tal
+
+    def enable_packet_log(self, n: int):
+        self._check(self.lib.mcrt_enable_packet_log(self.ctx, n))
+
+    def packet_log(self, n: int):
+        log = abi.packet_log_array(n)
+        self._check(self.lib.mcrt_download_packet_log(self.ctx, log, n))
+        return log
+
+    def update_temperature(self, nphot: int, iteration: int, converge: int = 0):
+        td = np.ascontiguousarray(self.tdave, dtype=np.float64).copy()
+        conv = C.c_int32(converge)
+        sig = np.zeros(3, np.float64)
+        self._check(self.lib.mcrt_update_temperature(self.ctx, nphot, iteration,
+                                                     td.ctypes.data_as(C.POINTER(C.c_double)), C.byref(conv),
+                                                     sig.ctypes.data_as(C.POINTER(C.c_double))))
+        self.tdave = td
+        self.sig = sig
+        return td, bool(conv.value), sig
+
+    # --------------------------------------------------- reference interface
+    def disk(self, converge: str, iteration: int, i1: int, np_total: int, *, ipeel: int = 0,
+             generator: int = 1):
+        """``subroutine disk(converge,iter,i1)`` for one GPU.
+
+        Runs np_total packets (the packet loop), leaves the reduced tallies in
+        ``self.tallies`` and updates the temperature with ``tfinal``;
+        returns the new ``converge`` ('yes'/'no').
+        """
+        self.reset_tallies()
+        self.run(np_total, iteration=iteration, ipeel=ipeel, seeds=(12345678 - i1 if i1 else 12345678, 87654321),
+                 generator=generator)
+        self.tallies = self.download(images=bool(ipeel))
+        _, conv, _ = self.update_temperature(np_total, iteration, 1 if converge == "yes" else 0)
+        return "yes" if conv else "no"
+
+
+def lucy_iterations(engine: Engine, np_total: int, n_iter: int, n_iter_min: int = 0):
+    """The Lucy loop of newtts.f90:225-256 (no peel-off during iterations)."""
+    converge = "no"
+    it = 0
+    history = []
+    while converge == "no":
+        it += 1
+        converge = engine.disk(converge, it, 0, np_total, ipeel=0)
+        history.append(engine.sig.copy())
+        if it < n_iter_min:
+            converge = "no"
+        if it >= n_iter:
+            converge = "yes"
+    return it, history

@@ -1,0 +1,485 @@
+"""Synthetic young-star models in the reference's array layout.
+
+The reference builds its model on the host before every call of ``disk``:
+walls and densities in ``gridset`` (gridset_5_model13new.f90), dust tables in
+``dustinit``/``setemiss`` (dust_5.f90:345-699) and the stellar CDF in
+``atmosinit`` (starbarb_2.f90:3-122).  Those routines stay outside the packet
+engine; this module produces the same arrays from the analytic recipes the
+benchmark workloads name, so that the engine and its oracle can be driven
+without the reference's missing parameter files:
+
+* walls: wall 1 is the stellar surface, wall 2 the dust inner radius, then
+  log-spaced walls to ``rmax``; theta walls keep the reference convention of an
+  odd wall count with a theta=90 deg wall flagged by ``tan2arr=-1``
+  (gridset_5_model13new.f90:722-750, thetaface.f90:33-53);
+* disk: Whitney flared disk normalised to its mass (setup_wave.f90:60-88),
+  rho = rho0 (1-sqrt(R*/w)) (R*/w)^a exp(-z^2/2h^2), h = z1 w^b;
+* envelope: Ulrich rotating infall (densenv.f90:37-43, envset.f90:157-160,
+  zerod.f90) with the ambient floor; polynomial bipolar cavity
+  (densenv.f90:76-90, envset.f90:182-189); disk cells clear the envelope and
+  cavity components (gridset_5_model13new.f90:1217-1224);
+* dust: kappa = kappa0 (lambda/1um)^-1.5 on 100 log wavelengths 0.1-3000 um,
+  albedo 0.5->0 and g 0.6->0 linear in log lambda, pmax 0.5; normalised to
+  0.55 um like dustinit (dust_5.f90:457-464); kapint/kappap/kappar follow the
+  setemiss integrals (dust_5.f90:507-699) with Gauss-Legendre quadrature in
+  place of Numerical Recipes' qsimp;
+* star: Planck atmosphere CDF as atmosinit builds it with CPLANCKST=YES.
+
+All arrays are returned flattened in Fortran (column-major) order.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+# constants.f90
+PI = 3.1415926535897932384626433
+R2P = 2.0 * PI
+RSOL = 6.9598e10
+MSOL = 1.989e33
+GN = 6.67428e-8
+SIGT = 5.670400e-5
+KB = 1.3806503e-16
+MH = 1.67262158e-24
+
+NDG2 = 10
+NO = 8
+
+
+@dataclasses.dataclass
+class Workload:
+    """Parameters of one model; defaults are the 2-D reference workload."""
+    # grid (wall counts, Fortran nrg/ntg/npg)
+    nrg: int = 101
+    ntg: int = 99
+    npg: int = 2
+    # star
+    rstar: float = 2.0            # Rsun
+    tstar_k: float = 4000.0       # K
+    # geometry [AU]
+    rddust_au: float = 0.1
+    rmax_au: float = 5000.0
+    rmaxd_au: float = 200.0
+    # disk
+    massd: float = 0.01           # Msun
+    a_exp: float = 2.25
+    b_exp: float = 1.25
+    h100_au: float = 10.0
+    # envelope
+    rate: float = 1.0e-6          # Msun/yr
+    rc_au: float = 100.0
+    massc: float = 0.5            # Msun
+    rhoamb: float = 1.67e-20
+    # cavity
+    thet1_deg: float = 20.0
+    ex1: float = 1.5
+    rhoconst1: float = 1.67e-19
+    # dust law
+    kappa0: float = 100.0         # cm^2/g at 1 um
+    nlambda: int = 100
+    # SEDs / images
+    nfreq: int = 100
+    nmu: int = 10
+    nph: int = 1
+    nap: int = 1
+    npeel: int = 10
+    nxhst: int = 101
+    rmaxi_au: float = 5000.0
+    aperture_au: float = 5000.0
+    # theta-wall clustering toward the equator
+    theta_power: float = 2.0
+    # multiplicative clump field (3-D fractal models); None for smooth models
+    clump_seed: int | None = None
+    clump_dim: float = 2.6
+    clump_mass_frac: float = 0.5
+
+
+class Model:
+    """A complete engine input: config scalars plus grid and table arrays."""
+
+    def __init__(self, w: Workload):
+        self.w = w
+        self.config: dict = {}
+        self.grid: dict = {}
+        self.tables: dict = {}
+        self._build()
+
+    # ------------------------------------------------------------------ walls
+    def _walls(self):
+        w = self.w
+        autors = 214.94 / w.rstar                      # setup.f90:45
+        rddust = w.rddust_au * autors
+        rmax = w.rmax_au * autors
+        nrg, ntg, npg = w.nrg, w.ntg, w.npg
+        if ntg % 2 == 0:
+            raise ValueError("ntg must be odd (theta=90 wall), grid_mod_5.f90:6")
+        rarr = np.empty(nrg)
+        rarr[0] = 1.0                                  # stellar surface
+        rarr[1] = rddust
+        rarr[2:] = rddust * (rmax / rddust) ** (np.arange(1, nrg - 1) / (nrg - 2))
+        rarr[-1] = rmax
+        r2arr = rarr * rarr
+
+        nttmp = (ntg + 1) // 2
+        tmpth = 0.5 * PI * (np.arange(nttmp) / (nttmp - 1)) ** w.theta_power
+        thetarr = np.empty(ntg)
+        for it in range(2, nttmp):                     # gridset_5_model13new.f90:722-725
+            thetarr[nttmp + 1 - it - 1] = 0.5 * PI - tmpth[it - 1]
+            thetarr[nttmp - 1 + it - 1] = 0.5 * PI + tmpth[it - 1]
+        thetarr[0] = 0.0
+        thetarr[nttmp - 1] = 0.5 * PI
+        thetarr[ntg - 1] = PI
+        costarr = np.cos(thetarr)
+        sintarr = np.sin(thetarr)
+        tan2arr = np.tan(thetarr) ** 2
+        costarr[0], sintarr[0], tan2arr[0] = 1.0, 0.0, 0.0
+        costarr[-1], sintarr[-1], tan2arr[-1] = -1.0, 0.0, 0.0
+        costarr[nttmp - 1], sintarr[nttmp - 1], tan2arr[nttmp - 1] = 0.0, 1.0, -1.0
+
+        dp = R2P / (npg - 1)
+        phiarr = dp * np.arange(npg)
+        aarr = np.sin(phiarr)
+        barr = -np.cos(phiarr)
+        return autors, rddust, rmax, rarr, r2arr, thetarr, costarr, sintarr, tan2arr, phiarr, aarr, barr
+
+    # ------------------------------------------------------------- densities
+    @staticmethod
+    def _ulrich_mu0(mu, rx):
+        """Root of mu0^3 + (rx-1) mu0 - rx mu = 0 in [0,1] (zerod.f90)."""
+        a2 = rx - 1.0
+        a3 = -rx * mu
+        q = (-3.0 * a2) / 9.0
+        r = (27.0 * a3) / 54.0
+        q3 = q ** 3
+        out = np.empty_like(mu)
+        three = (q3 - r * r) >= 0.0
+        if np.any(three):
+            qq, rr, qq3 = q[three], r[three], q3[three]
+            qh = np.sqrt(qq)
+            th = np.arccos(np.clip(rr / np.sqrt(qq3), -1.0, 1.0))
+            roots = np.stack([-2.0 * qh * np.cos(th / 3.0),
+                              -2.0 * qh * np.cos((th + 2.0 * PI) / 3.0),
+                              -2.0 * qh * np.cos((th + 4.0 * PI) / 3.0)])
+            roots = np.where(roots > 0.0, roots, np.inf)
+            out[three] = np.min(roots, axis=0)
+        one = ~three
+        if np.any(one):
+            rr, qq, qq3 = r[one], q[one], q3[one]
+            fac = np.sqrt(rr * rr - qq3) + np.abs(rr)
+            f3 = fac ** (1.0 / 3.0)
+            out[one] = -np.sign(rr) * (f3 + qq / f3)
+        return np.clip(out, 1e-12, 1.0)
+
+    def _densities(self, autors, rddust, rmax, rarr, thetarr, npg):
+        w = self.w
+        nr, nt, npc = w.nrg - 1, w.ntg - 1, npg - 1
+        rave = 0.5 * (rarr[:-1] + rarr[1:])
+        thave = 0.5 * (thetarr[:-1] + thetarr[1:])
+        rad = rave[:, None]
+        th = thave[None, :]
+        sina = np.sin(th)
+        cosa = np.abs(np.cos(th))
+        wcyl = rad * sina
+        zp = rad * cosa
+        rmincgs = w.rstar * RSOL
+
+        # disk (setup.f90:96-99 R100 scale height, setup_wave.f90:60-88)
+        rmaxd = w.rmaxd_au * autors
+        z1 = w.h100_au * autors / (100.0 * autors) ** w.b_exp
+        p = w.b_exp - w.a_exp
+        const = R2P ** 1.5 * rmincgs ** 2 * (rmincgs * z1)
+        rmind = rddust
+        rho0 = w.massd * MSOL / const / (
+            1.0 / (p + 2.0) * (rmaxd ** (p + 2.0) - rmind ** (p + 2.0))
+            - 1.0 / (p + 1.5) * (rmaxd ** (p + 1.5) - rmind ** (p + 1.5)))
+        h = z1 * wcyl ** w.b_exp
+        with np.errstate(invalid="ignore", divide="ignore"):
+            rho_d = rho0 * (1.0 - np.sqrt(1.0 / wcyl)) * wcyl ** (-w.a_exp) * np.exp(-0.5 * (zp / h) ** 2)
+        rho_d = np.where((rad > rddust) & (wcyl <= rmaxd) & (wcyl > 1.0), rho_d, 0.0)
+        rho_d = np.where(rho_d > 1e-300, rho_d, 0.0)
+
+        # Ulrich envelope (envset.f90:157-160, densenv.f90:37-43)
+        rc = w.rc_au * autors
+        rdcgs = rc * rmincgs
+        cst = 1.0 / 3.15576e7 * math.sqrt(MSOL) / (4.0 * PI) / math.sqrt(GN)
+        rhoe0 = cst * w.rate / math.sqrt(w.massc) / rdcgs ** 1.5
+        rmine = rddust
+        mu = zp / rad
+        rx = np.broadcast_to(rad / rc, mu.shape).copy()
+        mu0 = self._ulrich_mu0(np.broadcast_to(mu, rx.shape).copy(), rx)
+        factor = 1.0 / ((mu / mu0) + 2.0 * mu0 ** 2 / rx)
+        rho_e = rhoe0 * rx ** (-1.5) * factor / np.sqrt(1.0 + mu / mu0)
+        rho_e = np.where(rad > rmine, np.maximum(rho_e, w.rhoamb), 0.0)
+
+        # polynomial cavity (envset.f90:182-189, densenv.f90:76-90)
+        r1max = rmax * math.tan(w.thet1_deg * PI / 180.0)
+        c1e = rmax / r1max ** w.ex1
+        zup = c1e * wcyl ** w.ex1
+        inhole = zp > zup
+        rho_c = np.where(inhole & (rad > rmine) & (rad < rmax), w.rhoconst1, 0.0)
+        rho_e = np.where(inhole | (rad >= rmax), 0.0, rho_e)
+
+        if w.clump_seed is not None:
+            fac = self._clump_field(nr, nt, max(npc, 1))
+            rho_e = rho_e[:, :, None] * fac
+            rho_c = np.broadcast_to(rho_c[:, :, None], fac.shape)
+            rho_d = np.broadcast_to(rho_d[:, :, None], fac.shape)
+        else:
+            rho_e = np.broadcast_to(rho_e[:, :, None], (nr, nt, npc))
+            rho_c = np.broadcast_to(rho_c[:, :, None], (nr, nt, npc))
+            rho_d = np.broadcast_to(rho_d[:, :, None], (nr, nt, npc))
+
+        # the disk owns a cell where it is denser than the envelope+cavity gas;
+        # there the other components are cleared (gridset_5_model13new.f90:1217-1224)
+        rho_d = np.where(rho_d > rho_e + rho_c, rho_d, 0.0)
+        disk = rho_d > 0.0
+        dens = np.zeros((w.nrg, w.ntg, npg, NDG2))
+        dens[:nr, :nt, :npc, 1] = rho_d                      # id 2: disk grains
+        dens[:nr, :nt, :npc, 2] = np.where(disk, 0.0, rho_e)  # id 3: envelope
+        dens[:nr, :nt, :npc, 3] = np.where(disk, 0.0, rho_c)  # id 4: cavity
+        # vcell (gridset_5_model13new.f90:1147-1150)
+        dr3 = rarr[1:] ** 3 - rarr[:-1] ** 3
+        dcost = np.cos(thetarr[1:]) - np.cos(thetarr[:-1])
+        vcell = np.zeros((w.nrg, w.ntg, npg))
+        vcell[:nr, :nt, :npc] = (-(dr3[:, None] * dcost[None, :]) * (R2P / npc) / 3.0
+                                 * rmincgs ** 3)[:, :, None]
+        return rave, dens, vcell
+
+    def _clump_field(self, nr, nt, npc):
+        """Seeded hierarchical clump multiplier with mean 1 (fractal_sph.f90 style)."""
+        w = self.w
+        rng = np.random.default_rng(w.clump_seed)
+        field = np.zeros((nr, nt, npc))
+        # hierarchical cascade: each level places children around parents
+        nlev = 4
+        nchild = max(2, int(round(2.0 ** w.clump_dim)))
+        pts = rng.random((nchild, 3))
+        for _ in range(nlev - 1):
+            scale = 0.5 ** (_ + 1)
+            kids = pts[:, None, :] + scale * (rng.random((pts.shape[0], nchild, 3)) - 0.5)
+            pts = np.mod(kids.reshape(-1, 3), 1.0)
+        ix = np.minimum((pts[:, 0] * nr).astype(int), nr - 1)
+        iy = np.minimum((pts[:, 1] * nt).astype(int), nt - 1)
+        iz = np.minimum((pts[:, 2] * npc).astype(int), npc - 1)
+        np.add.at(field, (ix, iy, iz), 1.0)
+        field /= field.mean()
+        f = w.clump_mass_frac
+        return (1.0 - f) + f * field
+
+    # --------------------------------------------------------------- tables
+    def _dust(self):
+        w = self.w
+        lam_um = np.logspace(math.log10(0.1), math.log10(3000.0), w.nlambda)
+        s = (np.log10(lam_um) - np.log10(0.1)) / (np.log10(3000.0) - np.log10(0.1))
+        kap = w.kappa0 * lam_um ** -1.5
+        alb = 0.5 * (1.0 - s)
+        gg = 0.6 * (1.0 - s)
+        pl = np.full_like(lam_um, 0.5)
+        lamdust = 10000.0 * lam_um                     # dust_5.f90:427
+        nudust = 12398.0 / lamdust                     # dust_5.f90:428
+        kapd = kap.copy()
+        kapd[0] = 0.00001 * kapd[0]                    # dust_5.f90:445
+        iv = int(np.max(np.nonzero(lam_um <= 0.55)[0]))
+        f = (5500.0 - lamdust[iv]) / (lamdust[iv + 1] - lamdust[iv])
+        kappav1 = (1.0 - f) * kapd[iv] + f * kapd[iv + 1]
+        kapd = kapd / kappav1
+        return nudust, kapd, alb, gg, pl, kappav1
+
+    @staticmethod
+    def _opac_interp(nu, nudust, tab):
+        """opacset interpolation (dust_5.f90:21-60) vectorised over nu."""
+        nu = np.asarray(nu, dtype=float)
+        n = nudust.size
+        out = np.empty_like(nu)
+        hi = nu >= nudust[0]
+        lo = nu <= nudust[n - 1]
+        mid = ~(hi | lo)
+        out[hi] = tab[0]
+        out[lo] = tab[n - 1]
+        if np.any(mid):
+            x = nu[mid]
+            # nudust decreasing; i0 = last index with x <= nudust(i0)
+            i0 = np.searchsorted(-nudust, -x, side="right") - 1
+            i0 = np.clip(i0, 0, n - 2)
+            i1 = i0 + 1
+            ff = (x - nudust[i1]) / (nudust[i0] - nudust[i1])
+            out[mid] = (1.0 - ff) * tab[i1] + ff * tab[i0]
+        return out
+
+    def _emission_tables(self, nudust, kapd, alb, nT=500, nnu=513):
+        tmin, tmax = 0.1, 200000.0
+        lTint = np.log(tmin / 11605.0) + np.arange(nT) * math.log(tmax / tmin) / (nT - 1)
+        Tint = np.exp(lTint)
+        numax = 32.0
+        numin = numax / 1024.0
+        nuint = numin + np.arange(nnu) * (numax - numin) / (nnu - 1)
+        norm = 0.1539897
+        gx, gw = np.polynomial.legendre.leggauss(12)
+        gx = 0.5 * (gx + 1.0)
+        gw = 0.5 * gw
+        kapint = np.zeros((nT, nnu))
+        kappar = np.zeros(nT)
+        kappa_abs = (1.0 - alb) * kapd
+        for i in range(nT):
+            T = Tint[i]
+            nu1_all = nuint * T
+            nu0_all = np.concatenate(([0.0], nu1_all[:-1]))
+            chi = self._opac_interp(np.concatenate(([0.0], nu1_all)), nudust, kapd)
+            kab = self._opac_interp(np.concatenate(([0.0], nu1_all)), nudust, kappa_abs)
+            chi0, chi1 = chi[:-1], chi[1:]
+            k0, k1 = kab[:-1], kab[1:]
+            dnu = nu1_all - nu0_all
+            dx = dnu / T
+            nu = nu0_all[:, None] + gx[None, :] * dnu[:, None]
+            x = nu / T
+            with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+                bx = np.where(x > 0, norm * x ** 3 / np.expm1(x), 0.0)
+                dbx = np.where(x > 0, -norm * x ** 4 / (4.0 * np.expm1(x) * np.expm1(-x)), 0.0)
+            bx = np.nan_to_num(bx)
+            dbx = np.nan_to_num(dbx)
+            ff = gx[None, :]
+            kb = ((1.0 - ff) * k0[:, None] + ff * k1[:, None]) * bx
+            cdb = dbx / ((1.0 - ff) * chi0[:, None] + ff * chi1[:, None])
+            seg = (kb * gw[None, :]).sum(axis=1)
+            segc = (cdb * gw[None, :]).sum(axis=1)
+            ok = (nu0_all / T) < 50.0
+            seg = np.where(ok, seg, 0.0)
+            segc = np.where(ok, segc, 0.0)
+            kapint[i] = np.cumsum(dx * seg)
+            kappar[i] = 1.0 / np.sum(dx * segc)
+        kappap = kapint[:, -1].copy()
+        kapint = kapint / kapint[:, -1:]
+        kapint[:, -1] = 1.0
+        return lTint, Tint, nuint, kapint, kappap, kappar
+
+    def _atmosphere(self, tstar_ev, nhnu=2000):
+        lam = np.logspace(math.log10(0.05), math.log10(1000.0), nhnu)   # file order: increasing lambda
+        winv = (1.0 / lam)[::-1]                                        # starbarb_2.f90:69-72
+        nu = 1.2398 * lam ** -1
+        x = nu / tstar_ev
+        with np.errstate(over="ignore"):
+            f = 0.1539897 * x ** 3 / np.expm1(x)                       # mathsubs.f90:4-22
+        f = f[::-1]
+        atmosnu = 1.2398 * winv
+        hnuint = np.zeros(nhnu)
+        hnuint[1:] = np.cumsum(0.5 * (f[1:] + f[:-1]) * (winv[1:] - winv[:-1]))
+        hnuint = hnuint / hnuint[-1]
+        lognu = np.log10(atmosnu)
+        with np.errstate(divide="ignore"):
+            loghnu = np.where(hnuint > 0, np.log10(np.maximum(hnuint, 1e-300)), 0.0)
+        loghnu[0] = 0.0
+        return atmosnu, hnuint, lognu, loghnu
+
+    # ---------------------------------------------------------------- build
+    def _build(self):
+        w = self.w
+        (autors, rddust, rmax, rarr, r2arr, thetarr, costarr, sintarr, tan2arr,
+         phiarr, aarr, barr) = self._walls()
+        rave, dens, vcell = self._densities(autors, rddust, rmax, rarr, thetarr, w.npg)
+        nrg, ntg, npg = w.nrg, w.ntg, w.npg
+        findopac = np.zeros((nrg, ntg, npg, NDG2), dtype=np.int32)
+        for idd in range(NDG2):
+            findopac[..., idd] = idd + 1 if idd < 8 else 1       # findopacid_5.f90:97
+        tstar = w.tstar_k / 11605.0
+        tdust = np.full((nrg, ntg, npg), 0.1 / 11605.0)
+        diffus = np.zeros((nrg, ntg, npg), dtype=np.int32)
+        diffdir = np.zeros((nrg, ntg, npg), dtype=np.int32)
+
+        nudust, kapd, alb, gg, pl, kappav1 = self._dust()
+        nopac = 8
+        nl = nudust.size
+        lTint, Tint, nuint, kapint1, kappap1, kappar1 = self._emission_tables(nudust, kapd, alb)
+        nT, nnu = lTint.size, nuint.size
+        rep = lambda a: np.repeat(a[..., None], nopac, axis=-1)
+        atmosnu, hnuint, lognu, loghnu = self._atmosphere(tstar)
+
+        numin = 1.2398 / 5000.0                       # setup.f90:36-41
+        numax = 1.2398 / 0.01
+        nmu = w.nmu
+        dmu = 2.0 / nmu
+        u = 1.0 - dmu * (np.arange(1, nmu + 1) - 0.5)  # initarr_2_new.f90:22-26
+        thete = np.linspace(5.0, 86.0, w.npeel) if w.npeel > 1 else np.array([45.0])
+        thete_rad = thete * R2P / 360.0
+        phie = np.zeros(w.npeel)
+        aperture2 = (w.aperture_au * autors) ** 2 * np.ones(w.nap)
+
+        xmu = np.arange(1, 101) / 100.0               # samptabl.f90:1-23
+        prob = 0.5 * (xmu ** 3 + xmu ** 2)
+        prob[0] = 0.0
+
+        self.config = dict(
+            nrg=nrg, ntg=ntg, npg=npg, nopac=nopac, nlammax=nl, nT=nT, nnu=nnu,
+            nhnu=atmosnu.size, nfreq=w.nfreq, nmu=nmu, nph=w.nph, nap=w.nap,
+            npeel=w.npeel, nxhst=w.nxhst, output_imcube=1, partial_peeloff=0,
+            limb=0, iplanckst=1, idust=1, ilucy=1, iffuv=0, ispot=0, nspot=1,
+            rstar=w.rstar, tstar=tstar, tstarave=tstar, tshock=tstar, fspot=0.0,
+            accfrac=0.0, accfrac2=0.0, isrf_frac=0.0, rddust=rddust,
+            rmaxi=w.rmaxi_au * autors, numin=numin, lnurat=math.log(numax / numin),
+            autors=autors,
+            ifuv_ori=SIGT * (tstar * 11605.0) ** 4 * 4.0 * PI * (w.rstar * RSOL) ** 2,
+        )
+        F = lambda a: np.asfortranarray(a).ravel(order="F")
+        self.grid = dict(
+            rarr=rarr, r2arr=r2arr, thetarr=thetarr, costarr=costarr, sintarr=sintarr,
+            tan2arr=tan2arr, phiarr=phiarr, aarr=aarr, barr=barr,
+            densarr=F(dens), findopac=F(findopac), diffus=F(diffus), diffdir=F(diffdir),
+            tdust=F(tdust), vcell=F(vcell), ravearr=rave,
+            Ldint=np.linspace(1.0 / (nrg - 1), 1.0, nrg - 1),
+            hdisk=np.zeros(nrg - 1),
+        )
+        self.tables = dict(
+            nlambda=np.full(nopac, nl, dtype=np.int32),
+            nudust=F(rep(nudust)), kappad=F(rep(kapd)), adust=F(rep(alb)),
+            gdust=F(rep(gg)), pldust=F(rep(pl)),
+            kappav=np.full(nopac, kappav1),
+            kapint=F(rep(kapint1)), lTint=lTint, Tint=Tint, nuint=nuint,
+            kappap=F(rep(kappap1)), kappar=F(rep(kappar1)),
+            atmosnu=atmosnu, hnuint=hnuint, lognu=lognu, loghnu=loghnu,
+            aperture2=aperture2, u=u,
+            coste_arr=np.cos(thete_rad), sinte_arr=np.sin(thete_rad),
+            cospe_arr=np.cos(phie), sinpe_arr=np.sin(phie),
+            limb_prob=prob,
+        )
+        self.ncells = (nrg - 1) * (ntg - 1) * (npg - 1)
+
+    # convenience views (reference shapes)
+    def dens4(self):
+        w = self.w
+        return self.grid["densarr"].reshape((w.nrg, w.ntg, w.npg, NDG2), order="F")
+
+
+def reference_2d(**over) -> Model:
+    """2-D disk+envelope+cavity workload (nr=100, ntheta=99, nphi=1)."""
+    return Model(Workload(**over))
+
+
+def small_2d(**over) -> Model:
+    """A reduced grid of the same model for quick oracle comparisons."""
+    kw = dict(nrg=31, ntg=21, npg=2, nfreq=20, nmu=4, nph=1, npeel=3, nxhst=21)
+    kw.update(over)
+    return Model(Workload(**kw))
+
+
+def clumpy_3d(**over) -> Model:
+    """3-D clumpy model: nr=200, ntheta=199, nphi=64 cells."""
+    kw = dict(nrg=201, ntg=199, npg=65, nph=1, npeel=20, nfreq=20, nxhst=201,
+              clump_seed=31944)
+    kw.update(over)
+    return Model(Workload(**kw))
+
+
+def warm(m: Model, t1au_k: float = 300.0, q: float = 0.5) -> Model:
+    """Give the dust a power-law temperature T = t1au (r/1AU)^-q (cells with
+    dust only), a stand-in for a converged Lucy temperature in tests."""
+    w = m.w
+    autors = m.config["autors"]
+    rave = 0.5 * (m.grid["rarr"][:-1] + m.grid["rarr"][1:])
+    T = np.full((w.nrg, w.ntg, w.npg), 0.1 / 11605.0)
+    tr = np.clip(t1au_k * (rave / autors) ** (-q), 2.0, 1500.0) / 11605.0
+    T[:-1, :, :] = tr[:, None, None]
+    has = m.dens4().sum(axis=-1) > 0
+    T = np.where(has, T, 0.1 / 11605.0)
+    m.grid["tdust"] = np.asfortranarray(T).ravel(order="F")
+    return m

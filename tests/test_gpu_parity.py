@@ -1,0 +1,139 @@
+"""FP64 engine (CUDA, through the C ABI) against the CPU oracle.
+
+Event-for-event: the same packets draw the same random numbers, take the
+same scatter/absorb decisions and end in the same state; the FP64 kernel is
+built without FMA contraction, so packets can only part company through a
+last-place difference of a transcendental function flipping a comparison.
+Tallies: integer tallies agree up to such packets; FP64 sums agree to
+1e-9 relative (atomic order); the REAL outputs to float rounding.
+"""
+import numpy as np
+import pytest
+
+from src3_mpi_cfitsio_b200 import abi, model
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(m, precision="fp64"):
+    from src3_mpi_cfitsio_b200.engine import Engine
+    return Engine(m, precision=precision)
+
+
+def _same_packets(g, o):
+    same = ((g["ndraws"] == o["ndraws"]) & (g["nscat"] == o["nscat"]) & (g["nabs"] == o["nabs"]) &
+            (g["status"] == o["status"]) & (g["ncross"] == o["ncross"]) & (g["nstar"] == o["nstar"]))
+    close = np.isclose(g["nub"], o["nub"], rtol=1e-9, atol=0) & np.isclose(g["sip"], o["sip"], rtol=1e-9, atol=1e-12)
+    return same, same & close
+
+
+@pytest.fixture(scope="module")
+def warm_small():
+    return model.warm(model.small_2d())
+
+
+@pytest.mark.parametrize("ipeel", [0, 1])
+def test_fp64_event_for_event(warm_small, oracle_mod, ipeel):
+    n = 3000 if ipeel else 20000
+    eng = _engine(warm_small)
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=ipeel)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    tg = eng.download()
+    to, lo = oracle_mod.run(abi.Bundle(warm_small), n, ipeel=ipeel, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    assert (g["iphot"] == np.arange(1, n + 1)).all()
+    same, exact = _same_packets(g, o)
+    assert same.mean() >= 0.995, same.mean()
+    assert exact.mean() >= 0.995, exact.mean()
+    assert (g["nscat"] + g["nabs"]).sum() > n // 5      # the model interacts
+    # integer tallies: identical up to the few packets that parted company
+    for k in ("nabs", "dbig", "killed"):
+        assert abs(int(tg[k].sum()) - int(to[k].sum())) <= max(2, int(0.01 * to[k].sum())), k
+    # FP64 cell tally
+    da, db = tg["dtauabs"], to["dtauabs"]
+    assert np.allclose(da.sum(), db.sum(), rtol=2e-3)
+    cg, co = tg.counters(), to.counters()
+    assert cg["packets"] == co["packets"] == n
+    assert abs(cg["crossings"] - co["crossings"]) <= 0.01 * co["crossings"]
+    # SEDs (REAL): total flux per frequency bin
+    for k in ("si", "nums", "sq"):
+        a = tg.shaped(k)[..., 0].sum(axis=(1, 2, 3))
+        b = to.shaped(k)[..., 0].sum(axis=(1, 2, 3))
+        assert np.allclose(a, b, rtol=2e-2, atol=2e-3 * np.abs(b).max() + 1e-6), k
+    if ipeel:
+        for k in ("ti", "tq", "numt"):
+            a, b = tg[k].astype(np.float64), to[k].astype(np.float64)
+            assert np.allclose(a.sum(), b.sum(), rtol=1e-2), k
+        ia, ib = tg["image_m_i"].astype(np.float64), to["image_m_i"].astype(np.float64)
+        assert np.allclose(ia.sum(), ib.sum(), rtol=1e-2)
+        assert np.abs(ia - ib).max() <= 2e-2 * ib.max()
+    eng.close()
+
+
+def test_exact_subset_bitwise(warm_small, oracle_mod):
+    """Packets that never touch a transcendental tie end bit-identical in
+    their integer state and within 1e-12 in their FP64 state."""
+    n = 2000
+    eng = _engine(warm_small)
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    _, lo = oracle_mod.run(abi.Bundle(warm_small), n, ipeel=0, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    same, _ = _same_packets(g, o)
+    for k in ("xp", "yp", "zp", "cost", "phi", "nub"):
+        rel = np.abs(g[k][same] - o[k][same]) / np.maximum(np.abs(o[k][same]), 1e-300)
+        assert np.median(rel) < 1e-13 and np.quantile(rel, 0.99) < 1e-9, k
+    eng.close()
+
+
+def test_tfinal_matches_oracle(warm_small, oracle_mod):
+    """Device tfinal/dusttemp against the oracle on the same dtauabs."""
+    n = 20000
+    eng = _engine(warm_small)
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    tg = eng.download(images=False)
+    for it in (1, 4):
+        eng.tdave = warm_small.grid["tdust"].copy()
+        td_g, _, sig_g = eng.update_temperature(n, it)
+        td_o, sig_o = oracle_mod.tfinal(abi.Bundle(warm_small), tg["dtauabs"], n, it, warm_small.grid["tdust"])
+        assert np.allclose(td_g, td_o, rtol=1e-12, atol=0), np.abs(td_g - td_o).max()
+        assert np.allclose(sig_g, sig_o, rtol=1e-9, equal_nan=True)
+    eng.close()
+
+
+def test_multi_launch_sharding(warm_small):
+    """Packet ranges are independent: two launches over halves of the range
+    give the tallies of one launch over all of it (the per-rank split of the
+    MPI run, newtts.f90:139)."""
+    n = 4000
+    eng = _engine(warm_small)
+    eng.reset_tallies()
+    eng.run(n, ipeel=1)
+    a = eng.download()
+    eng.reset_tallies()
+    eng.run(n, 1, n // 2, ipeel=1)
+    eng.run(n, n // 2 + 1, n, ipeel=1)
+    b = eng.download()
+    for k in ("nabs", "dbig", "killed"):
+        assert (a[k] == b[k]).all(), k
+    assert np.allclose(a["dtauabs"], b["dtauabs"], rtol=1e-12, atol=1e-300)
+    for k in ("si", "ti", "image_m_i"):
+        assert np.allclose(a[k], b[k], rtol=1e-5, atol=1e-6 * max(1e-30, np.abs(a[k]).max())), k
+    eng.close()
+
+
+def test_errors_are_reported_not_fatal(warm_small):
+    from src3_mpi_cfitsio_b200.engine import MCRTError
+    eng = _engine(warm_small)
+    with pytest.raises(MCRTError):
+        eng.run(100, 50, 200)          # range beyond np
+    with pytest.raises(MCRTError):
+        eng.run(100, generator=40)     # generator outside 1..32
+    eng.run(100)                        # context still usable
+    assert eng.download(images=False).counters()["packets"] == 100
+    eng.close()

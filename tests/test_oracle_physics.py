@@ -1,0 +1,70 @@
+"""Known-answer tests of the CPU oracle (the checker the GPU tests use)."""
+import numpy as np
+import pytest
+
+from src3_mpi_cfitsio_b200 import abi, model
+
+
+def _empty(m):
+    m.grid["densarr"] = np.zeros_like(m.grid["densarr"])
+    return m
+
+
+def test_unobscured_star(oracle_mod):
+    """Empty grid: every packet escapes once; the direct peel-off weight
+    4 mu (limb=0, newdisktherm_5_fuv.f90:382-390) integrates to one packet
+    per packet for every inclination."""
+    m = _empty(model.small_2d())
+    b = abi.Bundle(m)
+    n = 20000
+    tal, log = oracle_mod.run(b, n, threads=4, nlog=n)
+    L = abi.packet_log_to_numpy(log)
+    assert (L["status"] == 0).all()
+    assert (L["nscat"] == 0).all() and (L["nabs"] == 0).all()
+    s = tal.scalars()
+    assert s["flux"] == n and s["tot"] == 0
+    nums = tal.shaped("nums")
+    assert nums[..., 0].sum() == n            # total component
+    assert nums[..., 1].sum() == n            # stellar origin (1 + i_orig)
+    assert nums[..., 5].sum() == n            # direct (5 + i_inter)
+    ti = tal.shaped("ti")[:, :, 0, 0].sum(axis=0)   # per inclination
+    assert np.allclose(ti / n, 1.0, atol=0.03), ti / n
+
+
+def test_planck_spectrum(oracle_mod):
+    """bbfreq samples B_nu(T*) (random.f90:197-225): the exit frequencies of
+    an empty grid follow the Planck distribution."""
+    m = _empty(model.small_2d())
+    b = abi.Bundle(m)
+    n = 40000
+    _, log = oracle_mod.run(b, n, ipeel=0, threads=4, nlog=n)
+    x = abi.packet_log_to_numpy(log)["nub"] / m.config["tstar"]   # h nu / k T
+    # mean of x under x^3/(e^x-1): 4 zeta(5)/zeta(4) = 3.8322 (sd 2.2 -> 4 sigma = 0.045)
+    assert abs(x.mean() - 3.8322) < 0.045
+    # fraction below x=1: 15/pi^4 * int_0^1 x^3/(e^x-1) dx = 0.034618
+    assert abs((x < 1.0).mean() - 0.034618) < 0.004
+
+
+def test_packet_conservation(oracle_mod, small_model):
+    """Each packet ends exactly once: exited + killed + dropped = np."""
+    b = abi.Bundle(small_model)
+    n = 3000
+    tal, log = oracle_mod.run(b, n, threads=4, nlog=n)
+    c = tal.counters()
+    st = abi.packet_log_to_numpy(log)["status"]
+    assert c["packets"] == n
+    assert c["exited"] + c["killed"] + c["geom_fail"] + (st == 2).sum() == n
+    assert c["geom_fail"] == 0
+    # SED: every exited packet lands in the total component once
+    assert tal.shaped("nums")[..., 0].sum() == c["exited"]
+
+
+def test_polarisation_bound(oracle_mod, small_model):
+    """Q^2+U^2+V^2 <= I^2 after scattering (propagate_5_fuv.f90:92-109)."""
+    b = abi.Bundle(small_model)
+    n = 3000
+    _, log = oracle_mod.run(b, n, ipeel=0, threads=4, nlog=n)
+    L = abi.packet_log_to_numpy(log)
+    p2 = L["sqp"] ** 2 + L["sup"] ** 2 + L["svp"] ** 2
+    assert np.all(p2 <= L["sip"] ** 2 * (1 + 1e-9))
+    assert (L["nscat"] > 0).sum() > 10
