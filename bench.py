@@ -1,0 +1,320 @@
+"""Benchmark: photon packets/s of the B200 engine on the 2-D young-star model.
+
+Workload (the configuration the headline metric is quoted on): the 2-D disk +
+Ulrich envelope + bipolar cavity model (nr=100 x ntheta=99 x nphi=1 cells,
+4000 K / 2 Rsun star, Mdisk=0.01 Msun, 100 log wavelengths 0.1-3000 um),
+run as Lucy iterations of the reference's ``disk`` routine.  One step is one
+iteration: the packet loop over ``--packets`` packets per GPU (emission, cell
+walk, scattering, absorption + Lucy reemission, exit binning) plus the
+device temperature update (``tfinal``).  Inputs are synthetic (seeded
+generator, no reference parameter files exist here).
+
+value : packets/s of the whole job (all ranks), device-timed between CUDA
+        events on the engine's stream, max over ranks;
+e2e   : the same through the public C ABI with host buffers: grid upload
+        (host->device), iteration, tally + temperature download
+        (device->host) inside the timed region.
+
+``--impl reference`` times the CPU restatement of the reference's packet
+loop (the oracle; the Fortran itself cannot be built here) on all host
+cores for a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "photon packets/s (1 B200): mixed vs FP64 plain at equal SED error; grad time"
+UNIT = "packets/s"
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "_fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            if self._stop.is_set():
+                break
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+
+    def summary(self):
+        import statistics
+        sm = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) >= 7:
+                for k, n in enumerate(names):
+                    if s[3 + k].lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def build_model(args):
+    """The 2-D workload with the reference's default diffusion treatment of
+    the optically thick disk interior (DIFFUSION=YES, tts_mod_5.f90:33)."""
+    from src3_mpi_cfitsio_b200 import model
+    m = model.warm(model.reference_2d())
+    return model.with_diffusion(m)
+
+
+def algorithmic_bytes(c: dict) -> float:
+    """Algorithmic bytes of one transport launch: 16 B per walk crossing
+    (density + species record 8 B, FP64 dtauabs update 8 B), 8 B per
+    peel-off crossing, 64 B per interaction (opacity row 32 B + packet
+    state 32 B), 16 B per SED / peel-off bin (4 x FP32 Stokes)."""
+    return (16.0 * c["crossings"] + 8.0 * c["peel_cross"] + 64.0 * c["interactions"] +
+            16.0 * (c["exited"] + c["peel_binned"]))
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+
+    from src3_mpi_cfitsio_b200 import abi
+    from src3_mpi_cfitsio_b200.engine import Engine
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    m = build_model(args)
+    eng = Engine(m, device=dev, precision=args.precision)
+    P = args.packets
+    np_total = P * world
+    lo, hi = rank * P + 1, (rank + 1) * P
+    dist = world > 1
+    if dist:
+        import torch
+        import torch.distributed as tdist
+
+    def reduce_cells(tal):
+        if not dist:
+            return tal
+        for k in ("dtauabs",):
+            t = torch.from_numpy(tal[k]).cuda(dev)
+            tdist.all_reduce(t)
+            tal.arrays[k][:] = t.cpu().numpy()
+        return tal
+
+    def step(it):
+        eng.reset_tallies()
+        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+        eng.update_temperature(np_total, it)
+
+    # warm-up iterations (also converge the temperature a little)
+    for w in range(args.warmup):
+        step(w + 1)
+    eng.synchronize()
+    if dist:
+        tdist.barrier()
+    counters = {}
+    kernel_ms = []
+    with Clocks(dev) as clk:
+        eng.flush_l2()
+        eng.mark(0)
+        for s in range(args.steps):
+            it = args.warmup + s + 1
+            eng.reset_tallies()
+            eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+            kernel_ms.append(eng.kernel_ms())
+            eng.update_temperature(np_total, it)
+            if s + 1 < args.steps:
+                eng.flush_l2()
+        eng.mark(1)
+        eng.synchronize()
+        ms = eng.elapsed_ms(0, 1)
+    tal = eng.download(images=False)
+    counters = tal.counters()
+    flush_ms = 0.0
+    if args.steps > 1:
+        eng.mark(2)
+        eng.flush_l2()
+        eng.mark(3)
+        flush_ms = eng.elapsed_ms(2, 3) * (args.steps - 1)
+    ms_steps = ms - flush_ms
+    if dist:
+        t = torch.tensor([ms_steps], dtype=torch.float64, device=f"cuda:{dev}")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms_steps = float(t.item())
+    value = np_total * args.steps / (ms_steps / 1e3)
+
+    # ---- end-to-end through the public API with host buffers
+    e2e_steps = max(1, min(args.steps, 3))
+    eng.synchronize()
+    h2d = 0
+    for name in ("densarr", "findopac", "diffus", "tdust", "vcell"):
+        h2d += m.grid[name].nbytes
+    t0 = time.perf_counter()
+    eng.mark(4)
+    for s in range(e2e_steps):
+        it = args.warmup + args.steps + s + 1
+        eng.upload_grid()
+        eng.reset_tallies()
+        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+        tl = eng.download(images=bool(args.ipeel))
+        reduce_cells(tl)
+        td, _, _ = eng.update_temperature(np_total, it)
+    eng.mark(5)
+    eng.synchronize()
+    e2e_ms = eng.elapsed_ms(4, 5)
+    wall_e2e = time.perf_counter() - t0
+    d2h = sum(a.nbytes for k, a in tl.arrays.items()) + td.nbytes
+    e2e_ms = max(e2e_ms, wall_e2e * 1e3)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = np_total * e2e_steps / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (transport)
+    per_launch = {k: v / args.steps for k, v in counters.items()}   # tallies of the last step only
+    per_launch = counters
+    kms = kernel_ms[-1]
+    abytes = algorithmic_bytes(per_launch)
+    achieved = abytes / (kms / 1e3) / 1e9
+    peaks = _peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    out = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms_steps / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+        dtype="f64" if args.precision == "fp64" else "f32+f64",
+        data="synthetic (seeded model generator; no reference parameter files)",
+        config={"workload": "2-D disk+envelope+cavity, nr=100 ntheta=99 nphi=1, Lucy iteration",
+                "packets_per_gpu": P, "packets_total": np_total, "peel_off": bool(args.ipeel),
+                "precision": args.precision, "l2": "flushed between steps (256 MiB write)",
+                "parallelism": f"packet shards x{world}"},
+        e2e={"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                  "frac": achieved / peak, "traffic": None,
+                  "peak_source": "measured" if not peaks.get("_fallback") else "fallback",
+                  "kernel": "transport_fp64" if args.precision == "fp64" else "transport_mixed",
+                  "kernel_ms": kms, "algorithmic_bytes": abytes},
+        gpu_launches=4 * args.steps,
+        clocks=clk.summary(),
+        counters=counters,
+    )
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args, m)
+    eng.close()
+    return out
+
+
+def cpu_baseline(args, m=None, sample=None):
+    """The oracle (CPU restatement of the reference loop) on all host cores."""
+    from oracle import oracle
+    from src3_mpi_cfitsio_b200 import abi
+    if m is None:
+        m = build_model(args)
+    b = abi.Bundle(m)
+    cores = os.cpu_count() or 1
+    n = sample or args.cpu_sample
+    oracle.run(b, min(n, 2000), ipeel=args.ipeel, threads=cores)      # warm caches
+    t0 = time.perf_counter()
+    tal, _ = oracle.run(b, n, ipeel=args.ipeel, threads=cores, iteration=2)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} packets of one Lucy iteration of the same model, {cores} host threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle
+    from src3_mpi_cfitsio_b200 import abi
+    m = build_model(args)
+    b = abi.Bundle(m)
+    cores = os.cpu_count() or 1
+    n = args.cpu_sample
+    for w in range(args.warmup):
+        oracle.run(b, min(n, 5000), ipeel=args.ipeel, threads=cores, iteration=w + 1)
+    times = []
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.run(b, n, ipeel=args.ipeel, threads=cores, iteration=args.warmup + s + 1)
+        times.append(time.perf_counter() - t0)
+    v = n * args.steps / sum(times)
+    return dict(metric=METRIC, value=v, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1e3 * sum(times) / args.steps, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                config={"workload": "2-D disk+envelope+cavity, nr=100 ntheta=99 nphi=1, Lucy iteration",
+                        "packets_per_step": n, "peel_off": bool(args.ipeel)},
+                cpu_baseline={"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                              "sample": f"{n} packets per step, {cores} host threads"},
+                e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--packets", type=int, default=1_000_000)
+    ap.add_argument("--ipeel", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        tdist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    out = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world)
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -183,10 +183,18 @@ struct Model {
     padv(thetarr, g->thetarr, ntg, g->thetarr[ntg - 1]);
     padv(costarr, g->costarr, ntg, g->costarr[ntg - 1] - 1.0);
     padv(tan2arr, g->tan2arr, ntg, 0.0);
+    padv(sintarr, g->sintarr, ntg, 0.0);
     padv(phiarr, g->phiarr, npg, g->phiarr[npg - 1]);
     padv(aarr, g->aarr, npg, g->aarr[npg - 1]);
     padv(barr, g->barr, npg, g->barr[npg - 1]);
   }
+
+  // Diffusion surface bookkeeping (emit_common_2.f90:201-372): the number of
+  // diffusion absorptions so far at each surface cell; the k-th one heats the
+  // cell to T^4 = T0^4 + k dT^4, the recursion of emit_common_2.f90:260-272.
+  std::atomic<int32_t>* ndiff = nullptr;
+  double nphot_diff = 1.0;
+  std::vector<double> sintarr;
 
   int64_t cidx(int ir, int it, int ip) const {
     return (int64_t)(ir - 1) + (int64_t)nrg * ((it - 1) + (int64_t)ntg * (ip - 1));
@@ -248,7 +256,7 @@ struct Packet {
   // opacset outputs (dust_mod) and kapd (opacin_mod) for all species
   std::vector<double> kappa, albedo, g, pl, g2, onemg2, g2p1, twog, kapd;
   // statistics
-  int32_t nscat = 0, nabsev = 0, ncross = 0, nstar = 0;
+  int32_t nscat = 0, nabsev = 0, ncross = 0, nstar = 0, ndiffev = 0;
 
   double ran() { return rng.ran(); }
 
@@ -1030,6 +1038,100 @@ struct Packet {
     for (int peelid = 1; peelid <= m->c.npeel; ++peelid) peeloff(s_i, ir, it, ip, idust2, peelid);
   }
 
+  // isotrp.f90:1-36
+  void isotrp(double sux, double suy, double suz, double& vx, double& vy, double& vz) {
+    double r2 = 2.0, mur = 0.0, x = 0.0, y = 0.0, z = 0.0;
+    while (r2 * r2 > std::fabs(mur)) {
+      x = ran(); x = x + x - 1.0;
+      y = ran(); y = y + y - 1.0;
+      z = ran(); z = z + z - 1.0;
+      mur = x * sux + y * suy + z * suz;
+      r2 = x * x + y * y + z * z;
+    }
+    double r = std::sqrt(r2);
+    if (mur < 0.0) r = -r;
+    vx = x / r; vy = y / r; vz = z / r;
+  }
+
+  // select_dust with mask = is_thermal (emit_common_2.f90:346)
+  int select_thermal(int ir, int it, int ip) {
+    double xran = ran();
+    int nn = 0, idust2 = 0;
+    for (int id = 1; id <= MCRT_NDG2; ++id)
+      if (!m->is_sg[id - 1] && m->dens(ir, it, ip, id) > 0.0) { ++nn; idust2 = id; }
+    if (nn == 1) return idust2;
+    double opac = 0.0;
+    for (int id = 1; id <= MCRT_NDG2; ++id)
+      if (!m->is_sg[id - 1]) opac = opac + kapd[m->fopac(ir, it, ip, id) - 1] * m->dens(ir, it, ip, id);
+    if (opac == 0.0) return 0;
+    double frac = 0.0;
+    for (int id = 1; id <= MCRT_NDG2; ++id) {
+      if (m->is_sg[id - 1]) continue;
+      frac = frac + kapd[m->fopac(ir, it, ip, id) - 1] * m->dens(ir, it, ip, id) / opac;
+      if (xran <= frac + 1.0e-10) return id;
+    }
+    return 0;
+  }
+
+  // emit_common_2.f90:201-372, vertical diffusion (|diffdir| = 2) without
+  // accretion photons (nacc = 0).  Moves the packet to the diffusion
+  // surface, heats the surface cell and emits isotropically from it.
+  // Returns false on a geometry failure.  ir/it/idust2 are updated like the
+  // reference's by-reference arguments.
+  bool emit_diffusion(int& ir, int& it, int& ip, int& idust2) {
+    const mcrt_grid* g = m->g;
+    const double Tmax = 199999.0;
+    const int dd = g->diffdir[m->cidx(ir, it, ip)];
+    if (dd == -2) {
+      while (it >= 1 && g->diffus[m->cidx(ir, it, ip)]) it = it - 1;
+      if (it < 1) return false;
+      it = it + 1;
+    } else {
+      while (it <= m->ntg - 1 && g->diffus[m->cidx(ir, it, ip)]) it = it + 1;
+      if (it > m->ntg - 1) return false;
+    }
+    cosb = zp / rtot;
+    sinb = std::sqrt(1.0 - cosb * cosb);
+    const double cosbnew = 1.00001 * m->costarr[it - 1];
+    const double sinbnew = std::sqrt(1.0 - cosbnew * cosbnew);
+    xp = xp * sinbnew / sinb;
+    yp = yp * sinbnew / sinb;
+    zp = rtot * cosbnew;
+    const double mu0 = m->costarr[it - 1], sth = m->sintarr[it - 1];
+    double sux, suy, suz;
+    if (mu0 > 0.0) { sux = -mu0 * xp / sth / rtot; suy = -mu0 * yp / sth / rtot; suz = sth; }
+    else { sux = mu0 * xp / sth / rtot; suy = mu0 * yp / sth / rtot; suz = -sth; }
+    isotrp(sux, suy, suz, ux, uy, uz);
+    cost = uz;
+    sint = std::sqrt(1.0 - cost * cost);
+    cosp = ux / sint;
+    sinp = uy / sint;
+    phi = std::atan2(sinp, cosp);
+    if (m->costarr[it - 1] < 0.0) it = it - 1;
+    const double dA = PI * sth * (m->rarr[ir] * m->rarr[ir] - m->rarr[ir - 1] * m->rarr[ir - 1]);
+    double T4s = m->c.tstar * m->c.tstar;
+    T4s = T4s * T4s;
+    const int64_t cs = m->cidx(ir, it, ip);
+    int nth = 0;
+    for (int id = 1; id <= MCRT_NDG2; ++id) if (!m->is_sg[id - 1] && m->dens(ir, it, ip, id) > 0.0) ++nth;
+    if (nth == 0) return false;
+    const int32_t k = m->ndiff[cs].fetch_add(nth) + nth;
+    double T4d = g->tdust[cs] * g->tdust[cs];
+    T4d = T4d * T4d;
+    const double T4 = T4d + (double)k * (4.0 * PI * T4s / (m->nphot_diff * dA));
+    const double tsurf = std::min(Tmax / 11605.0, std::pow(T4, 0.25));
+    idust2 = select_thermal(ir, it, ip);
+    if (idust2 == 0) return false;
+    double T4b = tsurf * tsurf;
+    T4b = T4b * T4b;
+    const double T4eff = 0.0;   // 4 pi T4s nacc/(dA nphot) with nacc = 0
+    const double mu = ux * sux + uy * suy + uz * suz;
+    const double T = std::min(std::pow(T4b + 0.75 * mu * T4eff, 0.25), Tmax / 11605.0);
+    nub = bbfreq(T);
+    if (g->diffdir[cs] == -2) it = it - 1; else it = it + 1;
+    return true;
+  }
+
   // select_dust_2.f90:1-84 with mask = is_any; returns 1-based id or 0
   int select_dust(int ir, int it, int ip) {
     double xran = ran();
@@ -1140,19 +1242,25 @@ struct Packet {
           else if (idust2 == 3 || idust2 == 7) i_orig = 3;
           else i_orig = 4;
           if (!m->g->diffus[cc]) T->nabs[cc]++;
-          // emit_common, non-diffusion thermal branch (emit_common_2.f90:52-81)
-          double tave = m->g->tdust[cc];
-          // reemit.f90
-          sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
-          cost = 1.0 - 2.0 * ran();
-          sint = std::sqrt(1.0 - cost * cost);
-          phi = R2P * ran();
-          cosp = std::cos(phi);
-          sinp = std::sin(phi);
-          nub = lucydustfreq(tave, m->fopac(ir, it, ip, idust2));
-          uy = sint * sinp;
-          ux = sint * cosp;
-          uz = cost;
+          if (!m->g->diffus[cc]) {
+            // emit_common, non-diffusion thermal branch (emit_common_2.f90:52-81)
+            double tave = m->g->tdust[cc];
+            // reemit.f90
+            sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+            cost = 1.0 - 2.0 * ran();
+            sint = std::sqrt(1.0 - cost * cost);
+            phi = R2P * ran();
+            cosp = std::cos(phi);
+            sinp = std::sin(phi);
+            nub = lucydustfreq(tave, m->fopac(ir, it, ip, idust2));
+            uy = sint * sinp;
+            ux = sint * cosp;
+            uz = cost;
+          } else {
+            ++ndiffev;
+            if (!emit_diffusion(ir, it, ip, idust2)) return 3;
+            ii[1] = it;
+          }
           iflag = 0;
           opacset(nub);
           ifuv = is_fuv(nub) ? c.ifuv_ori : 0.0;
@@ -1237,7 +1345,7 @@ extern "C" {
 int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables* tab, int64_t np,
                int64_t iphot_lo, int64_t iphot_hi, int32_t iter, int32_t ipeel, int32_t seed1,
                int32_t seed2, int32_t generator, int32_t nthreads, mcrt_tallies* out,
-               mcrt_packet_log* log, int64_t nlog) {
+               mcrt_packet_log* log, int64_t nlog, double* tdust_out) {
   if (iter < 1) return MCRT_ERR_ARG;
   const int64_t block0 = (int64_t)(iter - 1) * np;
   Model m;
@@ -1252,7 +1360,11 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   m.rmincgs = cfg->rstar * RSOL;
   m.pad_walls();
   if (cfg->ilucy != 1) return MCRT_ERR_UNSUPPORTED;
-  for (int64_t c = 0; c < m.ncell; ++c) if (grid->diffus[c]) return MCRT_ERR_UNSUPPORTED;
+  for (int64_t c = 0; c < m.ncell; ++c)
+    if (grid->diffus[c] && (grid->diffdir[c] != 2 && grid->diffdir[c] != -2)) return MCRT_ERR_UNSUPPORTED;
+  std::vector<std::atomic<int32_t>> ndiff(m.ncell);
+  for (auto& a : ndiff) a.store(0);
+  m.ndiff = ndiff.data();
 
   // packet split (newdisktherm_5_fuv.f90:158-191)
   int64_t npout = (int64_t)(cfg->isrf_frac * (double)np);
@@ -1266,6 +1378,8 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   int64_t nsum = ns + npacc + npout;
   if (nsum != np) ns = ns + np - nsum;
   if (npacc > 1 || npout > 0) return MCRT_ERR_UNSUPPORTED;
+  // emit_common receives nphot = ns of the (rank's) run; a shard uses its share
+  m.nphot_diff = (double)ns * (double)(iphot_hi - iphot_lo + 1) / (double)np;
   int ips = (cfg->rddust > 100.0) ? 1 : 0;
 
   const int64_t nsed = (int64_t)cfg->nfreq * cfg->nmu * cfg->nph * cfg->nap * MCRT_NO;
@@ -1290,7 +1404,7 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
       int64_t hi = std::min(lo + chunk - 1, iphot_hi);
       for (int64_t iphot = lo; iphot <= hi; ++iphot) {
         p.rng = stream(seed1, seed2, generator, block0 + iphot - 1);
-        p.nscat = p.nabsev = p.ncross = p.nstar = 0;
+        p.nscat = p.nabsev = p.ncross = p.nstar = p.ndiffev = 0;
         int st = p.run(iphot, np, ns, npacc, npaccstar, ips);
         T.cnt[MCRT_C_PACKETS]++;
         if (st == 3) T.cnt[MCRT_C_GEOM_FAIL]++;
@@ -1299,7 +1413,7 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
           mcrt_packet_log& L = log[li];
           L.iphot = iphot; L.nscat = p.nscat; L.nabs = p.nabsev; L.ncross = p.ncross; L.nstar = p.nstar;
           L.status = st; L.ir = 0; L.it = 0; L.ip = 0; L.ndraws = (int32_t)p.rng.ndraws;
-          L.iflag = p.iflag; L.i_orig = p.i_orig; L.pad = 0;
+          L.iflag = p.iflag; L.i_orig = p.i_orig; L.pad = p.ndiffev;
           L.nub = p.nub; L.cost = p.cost; L.phi = p.phi; L.sip = p.sip; L.sqp = p.sqp; L.sup = p.sup; L.svp = p.svp;
           L.xp = p.xp; L.yp = p.yp; L.zp = p.zp;
         }
@@ -1333,6 +1447,49 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
     for (int k = 0; k < 4; ++k) put(im[k], img.im[k]);
     if (out->scalars) for (int k = 0; k < MCRT_NSCALARS; ++k) out->scalars[k] = S.scal[k];
     if (out->counters) for (int k = 0; k < MCRT_NCOUNTERS; ++k) out->counters[k] = S.cnt[k];
+  }
+  // End-of-iteration tdust of the diffusion cells (emit_common_2.f90:260-339,
+  // nacc = 0): the surface cell of a column with N diffusion absorptions
+  // holds min(Tmax,(T0^4+N dT^4)^(1/4)); interior cells whose neighbour
+  // toward the surface holds a thermal component take the same value.
+  if (tdust_out) {
+    const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
+    auto thermal = [&](int r, int t, int p) {
+      for (int id = 1; id <= MCRT_NDG2; ++id) if (!m.is_sg[id - 1] && m.dens(r, t, p, id) > 0.0) return true;
+      return false;
+    };
+    for (int ip = 1; ip <= npg; ++ip)
+      for (int it = 1; it <= ntg; ++it)
+        for (int ir = 1; ir <= nrg; ++ir) {
+          const int64_t c = m.cidx(ir, it, ip);
+          double t = grid->tdust[c];
+          if (grid->diffus[c]) {
+            const int dd = grid->diffdir[c];
+            int is = it, iwall;
+            if (dd == -2) { while (is - 1 >= 1 && grid->diffus[m.cidx(ir, is - 1, ip)]) --is; iwall = is; }
+            else { while (is + 1 <= ntg - 1 && grid->diffus[m.cidx(ir, is + 1, ip)]) ++is; iwall = is + 1; }
+            const int64_t cs = m.cidx(ir, is, ip);
+            const int32_t N = ndiff[cs].load();
+            bool gets = false;
+            if (N > 0) {
+              if (is == it) gets = thermal(ir, is, ip);
+              else if (dd == -2) gets = thermal(ir, it - 1, ip);
+              else gets = thermal(ir, it + 1, ip);
+            }
+            if (gets) {
+              const double sth = m.sintarr[iwall - 1];
+              const double dA = PI * sth * (m.rarr[ir] * m.rarr[ir] - m.rarr[ir - 1] * m.rarr[ir - 1]);
+              double T4s = cfg->tstar * cfg->tstar;
+              T4s = T4s * T4s;
+              const double t0 = grid->tdust[cs];
+              double T4d = t0 * t0;
+              T4d = T4d * T4d;
+              const double T4 = T4d + (double)N * (4.0 * PI * T4s / (m.nphot_diff * dA));
+              t = std::min(199999.0 / 11605.0, std::pow(T4, 0.25));
+            }
+          }
+          tdust_out[c] = t;
+        }
   }
   return MCRT_OK;
 }
@@ -1413,7 +1570,9 @@ static double dusttemp(const mcrt_config* c, const mcrt_tables* t, double na, in
 // tfinal (tfinal_5_test1.f90:1-447) for axisymmetric models, zero velocity
 // field (divvarr = vrarr = vthetarr = 0, so the gradient terms vanish).
 int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t, const double* dtauabs,
-                  int32_t nphot, int32_t iter, double* tdave, int32_t* converge, double* sig_out) {
+                  const double* tdust_now, int32_t nphot, int32_t iter, double* tdave, int32_t* converge,
+                  double* sig_out) {
+  if (!tdust_now) tdust_now = g->tdust;
   const int nrg = c->nrg, ntg = c->ntg, npg = c->npg;
   const int64_t ncell = (int64_t)nrg * ntg * npg;
   auto ci = [&](int ir, int it, int ip) { return (int64_t)(ir - 1) + (int64_t)nrg * ((it - 1) + (int64_t)ntg * (ip - 1)); };
@@ -1441,7 +1600,7 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
               (void)KB; (void)MHY; (void)SIGT;
               td = (t1 + t2) / 2.0;
             } else {
-              td = (g->tdust[ci(ir, it, ip)] + g->tdust[ci(ir, itm, ip)]) / 2.0;
+              td = (tdust_now[ci(ir, it, ip)] + tdust_now[ci(ir, itm, ip)]) / 2.0;
             }
             if (td * 11605.0 >= Tmax) td = Tmax / 11605.0;
           }

@@ -34,13 +34,14 @@ def load():
         lib.oracle_run.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
                                    C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, C.c_int32, C.c_int32,
-                                   C.POINTER(abi.Tallies), C.POINTER(abi.PacketLog), C.c_int64]
+                                   C.POINTER(abi.Tallies), C.POINTER(abi.PacketLog), C.c_int64,
+                                   C.POINTER(C.c_double)]
         lib.oracle_run.restype = C.c_int
         lib.oracle_rng.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.oracle_inczeta.argtypes = [C.POINTER(C.c_double)]
         lib.oracle_tfinal.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
-                                      C.POINTER(C.c_double), C.c_int32, C.c_int32,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32, C.c_int32,
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.oracle_tfinal.restype = C.c_int
         _lib = lib
@@ -56,9 +57,11 @@ def run(bundle: abi.Bundle, np_total: int, lo: int = 1, hi: int | None = None, *
     threads = threads or os.cpu_count() or 1
     tal = abi.TallyArrays(bundle.config, images=images)
     log = abi.packet_log_array(nlog) if nlog > 0 else None
+    c = bundle.config
+    tal.tdust = np.zeros(c.nrg * c.ntg * c.npg, np.float64)
     rc = lib.oracle_run(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables),
                         np_total, lo, hi, iteration, ipeel, seeds[0], seeds[1], generator, threads,
-                        C.byref(tal.struct), log, nlog)
+                        C.byref(tal.struct), log, nlog, tal.tdust.ctypes.data_as(C.POINTER(C.c_double)))
     if rc != 0:
         raise RuntimeError(f"oracle_run failed with code {rc}")
     return tal, log
@@ -79,14 +82,17 @@ def inczeta():
     return out
 
 
-def tfinal(bundle: abi.Bundle, dtauabs: np.ndarray, nphot: int, iteration: int, tdave: np.ndarray):
+def tfinal(bundle: abi.Bundle, dtauabs: np.ndarray, nphot: int, iteration: int, tdave: np.ndarray,
+           tdust_now: np.ndarray | None = None):
     lib = load()
     td = np.ascontiguousarray(tdave, dtype=np.float64).copy()
     da = np.ascontiguousarray(dtauabs, dtype=np.float64)
+    tn = None if tdust_now is None else np.ascontiguousarray(tdust_now, dtype=np.float64)
     conv = C.c_int32(0)
     sig = np.zeros(3, np.float64)
     rc = lib.oracle_tfinal(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables),
-                           da.ctypes.data_as(C.POINTER(C.c_double)), nphot, iteration,
+                           da.ctypes.data_as(C.POINTER(C.c_double)),
+                           None if tn is None else tn.ctypes.data_as(C.POINTER(C.c_double)), nphot, iteration,
                            td.ctypes.data_as(C.POINTER(C.c_double)), C.byref(conv),
                            sig.ctypes.data_as(C.POINTER(C.c_double)))
     if rc != 0:

@@ -21,6 +21,8 @@ namespace mcrt {
 // transport launchers (mcrt_fp64.cu, mcrt_mixed.cu)
 cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t s);
 cudaError_t launch_transport_mixed(const LaunchParams& p, int grid, cudaStream_t s);
+cudaError_t launch_diffusion_finalize(const DevModel& m, const int32_t* ndiff, const double* tdust0, double* tdust,
+                                      double nphot, cudaStream_t s);
 int transport_fp64_blocks_per_sm();
 int transport_mixed_blocks_per_sm();
 }  // namespace mcrt
@@ -45,6 +47,8 @@ struct mcrt_ctx {
   double *d_walls = nullptr;
   CellRec *d_cells = nullptr;
   double *d_tdust = nullptr, *d_vcell = nullptr;
+  double *d_tdust0 = nullptr;         // tdust at the start of the iteration (read by the transport)
+  double last_nphot_diff = 1.0;
   double *d_dens_thermal = nullptr;   // [ncell] density of the thermal component (tfinal)
   int32_t *d_idust3 = nullptr;        // [ncell] its opacity species (0 = none)
   int32_t *d_diffus = nullptr;
@@ -274,7 +278,7 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   ctx->npsed = (int64_t)c.nfreq * c.npeel * c.nap * MCRT_NO;
   ctx->nimg = c.output_imcube ? (int64_t)c.npeel * c.nxhst * c.nxhst * c.nfreq : 0;
   // one tally allocation: cell ints, cell doubles, SED, peeled SED, images, scalars, counters
-  const int64_t n_int = 4 * ctx->ncell;
+  const int64_t n_int = 5 * ctx->ncell;
   const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + MCRT_NSCALARS;
   ctx->tally_bytes = (size_t)n_dbl * 8 + (size_t)MCRT_NCOUNTERS * 8 + (size_t)((n_int * 4 + 7) / 8) * 8;
   int rc = dalloc(ctx, (char**)&ctx->d_tally, ctx->tally_bytes);
@@ -293,7 +297,8 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   t.nabs = ip; ip += ctx->ncell;
   t.dbig = ip; ip += ctx->ncell;
   t.dsg = ip; ip += ctx->ncell;
-  t.killed = ip;
+  t.killed = ip; ip += ctx->ncell;
+  t.ndiff = ip;
   if ((rc = dalloc(ctx, &ctx->d_next, 1))) { *out = ctx; return rc; }
   if ((rc = dalloc(ctx, &ctx->d_err, 4))) { *out = ctx; return rc; }
   CK(cudaMemset(ctx->d_tally, 0, ctx->tally_bytes));
@@ -327,7 +332,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   const int nrg = c.nrg, ntg = c.ntg, npg = c.npg;
   const int64_t ncell = ctx->ncell;
   if (!g->rarr || !g->r2arr || !g->thetarr || !g->costarr || !g->tan2arr || !g->phiarr || !g->aarr || !g->barr ||
-      !g->densarr || !g->findopac || !g->diffus || !g->tdust || !g->vcell)
+      !g->densarr || !g->findopac || !g->diffus || !g->tdust || !g->vcell || !g->sintarr)
     return fail(ctx, MCRT_ERR_ARG, "mcrt_upload_grid: missing array");
   // transport layout: one CellRec per cell with the non-zero components
   std::vector<CellRec> cells(ncell);
@@ -364,8 +369,12 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     r.meta |= (uint32_t)n;
     if (nth > 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "cell with %d thermal components (tfinal allows one)", nth);
     diffus[k] = g->diffus[k] ? 1 : 0;
-    if (diffus[k]) return fail(ctx, MCRT_ERR_UNSUPPORTED, "diffusion cells (emit_common_2.f90:83-381) are outside the built scope");
-    r.flags = (uint32_t)diffus[k];
+    const int dd = g->diffdir ? g->diffdir[k] : 0;
+    if (diffus[k] && dd != 2 && dd != -2)
+      return fail(ctx, MCRT_ERR_UNSUPPORTED, "radial/phi diffusion (diffdir=%d, emit_common_2.f90:91-199,374) is outside the built scope", dd);
+    if (diffus[k] && nth == 0) return fail(ctx, MCRT_ERR_ARG, "diffusion cell without a thermal component");
+    if (dd < -8 || dd > 7) return fail(ctx, MCRT_ERR_ARG, "diffdir out of range");
+    r.flags = (uint32_t)diffus[k] | ((uint32_t)(dd + 8) << 1) | (nth > 0 ? 32u : 0u);
   }
   if (slot_species.empty()) slot_species.push_back(1);
   // walls: rarr r2arr | thetarr costarr tan2arr | phiarr aarr barr, each
@@ -380,6 +389,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   addp(g->thetarr, ntg, g->thetarr[ntg - 1]);
   addp(g->costarr, ntg, g->costarr[ntg - 1] - 1.0);
   addp(g->tan2arr, ntg, 0.0);
+  addp(g->sintarr ? g->sintarr : g->tan2arr, ntg, 0.0);
   addp(g->phiarr, npg, g->phiarr[npg - 1]);
   addp(g->aarr, npg, g->aarr[npg - 1]);
   addp(g->barr, npg, g->barr[npg - 1]);
@@ -389,6 +399,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     if ((rc = dalloc(ctx, &ctx->d_walls, walls.size()))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_cells, ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_tdust, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_tdust0, ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_vcell, ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_dens_thermal, 2 * ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_idust3, ncell))) return rc;
@@ -397,6 +408,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   CK(cudaMemcpyAsync(ctx->d_walls, walls.data(), walls.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_cells, cells.data(), ncell * sizeof(CellRec), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_tdust, g->tdust, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_tdust0, g->tdust, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_vcell, g->vcell, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_dens_thermal, dens_th.data(), ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_idust3, idust3.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -409,11 +421,12 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   m.thetarr = w; w += ntg + 1;
   m.costarr = w; w += ntg + 1;
   m.tan2arr = w; w += ntg + 1;
+  m.sintarr = w; w += ntg + 1;
   m.phiarr = w; w += npg + 1;
   m.aarr = w; w += npg + 1;
   m.barr = w;
   m.cells = ctx->d_cells;
-  m.tdust = ctx->d_tdust;
+  m.tdust = ctx->d_tdust0;
   m.vcell = ctx->d_vcell;
   m.nslot = (int)slot_species.size();
   for (int s = 0; s < kMaxSlot; ++s) m.slot_species[s] = s < m.nslot ? slot_species[s] : 1;
@@ -560,6 +573,8 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   P.block0 = (int64_t)(iter - 1) * np;
   P.ns = ns; P.npacc = npacc; P.npaccstar = npaccstar;
   P.ipeel = ipeel ? 1 : 0;
+  P.nphot_diff = (double)ns * (double)(hi - lo + 1) / (double)np;
+  ctx->last_nphot_diff = P.nphot_diff;
   P.ips = (c.rddust > 100.0) ? 1 : 0;
   P.g1 = (int32_t)g1; P.g2 = (int32_t)g2;
   P.next = ctx->d_next;
@@ -577,6 +592,8 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
                                                     : launch_transport_mixed(P, grid, ctx->stream);
   if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  e = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion finalize: %s", cudaGetErrorString(e));
   CK(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
@@ -692,6 +709,7 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
   tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
   tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
   tdust_from_tdave<<<512, 256, 0, ctx->stream>>>(nc, a.tdave, ctx->d_diffus, ctx->d_idust3, ctx->d_cells, ctx->d_tdust);
+  CK(cudaMemcpyAsync(ctx->d_tdust0, ctx->d_tdust, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(tdave, a.tdave, nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

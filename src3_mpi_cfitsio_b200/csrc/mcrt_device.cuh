@@ -27,13 +27,16 @@ constexpr int kTransportBlock = 128;  // threads per transport block
 struct __align__(16) CellRec {
   double rho[kMaxComp];       // densarr of the non-zero components, id order
   uint32_t meta;              // bits 0-1: n; per comp k: slot (3 bits) at 2+7k, id-1 (4 bits) at 5+7k
-  uint32_t flags;             // bit 0: diffus
+  uint32_t flags;             // bit 0: diffus; bits 1-4: diffdir+8; bit 5: has a thermal component
 };
 static_assert(sizeof(CellRec) == 32, "CellRec must stay 32 bytes");
 
 __host__ __device__ inline int cell_n(uint32_t meta) { return (int)(meta & 3u); }
 __host__ __device__ inline int cell_slot(uint32_t meta, int k) { return (int)((meta >> (2 + 7 * k)) & 7u); }
 __host__ __device__ inline int cell_id(uint32_t meta, int k) { return (int)((meta >> (5 + 7 * k)) & 15u) + 1; }
+__host__ __device__ inline bool cell_diffus(uint32_t flags) { return (flags & 1u) != 0; }
+__host__ __device__ inline int cell_diffdir(uint32_t flags) { return (int)((flags >> 1) & 15u) - 8; }
+__host__ __device__ inline bool cell_thermal(uint32_t flags) { return (flags & 32u) != 0; }
 
 struct DevTallies {
   int32_t *nabs, *dbig, *dsg, *killed;     // [ncell]
@@ -43,6 +46,7 @@ struct DevTallies {
   double *img;                             // [4][nimg]
   double *scal;                            // [MCRT_NSCALARS]
   unsigned long long *cnt;                 // [MCRT_NCOUNTERS]
+  int32_t *ndiff;                          // [ncell] diffusion absorptions per surface cell
 };
 
 struct DevModel {
@@ -56,10 +60,10 @@ struct DevModel {
   double rstar, rmincgs, tstar, tshock, fspot, rmaxi, fractxh, numin, lnurat, ifuv_ori;
   double cspot1, sspot1, scspot1, ssspot1, cspot2, sspot2, scspot2, ssspot2, csprad;
   // walls
-  const double *rarr, *r2arr, *thetarr, *costarr, *tan2arr, *phiarr, *aarr, *barr;
+  const double *rarr, *r2arr, *thetarr, *costarr, *tan2arr, *phiarr, *aarr, *barr, *sintarr;
   // cells
   const CellRec *cells;
-  const double *tdust, *vcell;
+  const double *tdust, *vcell;              // tdust: start-of-iteration values
   // species: slot -> species (1-based) and the species tables
   int slot_species[kMaxSlot];
   const int32_t *nlambda;
@@ -81,6 +85,7 @@ struct LaunchParams {
   int64_t block0;               // first random block of the iteration: (iter-1)*np
   int64_t ns, npacc, npaccstar; // packet split (newdisktherm_5_fuv.f90:158-191)
   int32_t ipeel, ips;
+  double nphot_diff;            // nphot of emit_common's surface heating (ns of this shard)
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter
   mcrt_packet_log *log;

@@ -11,6 +11,12 @@ cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t 
   return cudaGetLastError();
 }
 
+cudaError_t launch_diffusion_finalize(const DevModel& m, const int32_t* ndiff, const double* tdust0, double* tdust,
+                                      double nphot, cudaStream_t s) {
+  diffusion_finalize<<<256, 256, 0, s>>>(m, ndiff, tdust0, tdust, nphot);
+  return cudaGetLastError();
+}
+
 int transport_fp64_blocks_per_sm() {
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_fp64, kBlock, 0) != cudaSuccess) return 1;

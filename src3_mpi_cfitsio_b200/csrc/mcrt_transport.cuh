@@ -129,7 +129,7 @@ struct Packet {
   int ir, it, ip;
   bool on_wall;
   int iflag, i_orig, exitflag;
-  int nscat, nabsev, ncross, nstar;
+  int nscat, nabsev, ncross, nstar, ndiffev;
   unsigned long long c_cross, c_peel, c_pcross, c_pbin, c_reset;
 
   __device__ Packet(const DevModel& mm, const DevTallies& tt, double* sbase)
@@ -861,6 +861,106 @@ struct Packet {
     }
   }
 
+  // isotrp.f90:1-36
+  __device__ void isotrp(double sux, double suy, double suz) {
+    double r2 = 2.0, mur = 0.0, x = 0.0, y = 0.0, z = 0.0;
+    while (r2 * r2 > fabs(mur)) {
+      x = ran(); x = x + x - 1.0;
+      y = ran(); y = y + y - 1.0;
+      z = ran(); z = z + z - 1.0;
+      mur = x * sux + y * suy + z * suz;
+      r2 = x * x + y * y + z * z;
+    }
+    double r = sqrt(r2);
+    if (mur < 0.0) r = -r;
+    ux = x / r; uy = y / r; uz = z / r;
+  }
+
+  // select_dust with mask = is_thermal (emit_common_2.f90:346)
+  __device__ int select_thermal(const CellRec& c) {
+    const double xran = ran();
+    const int n = cell_n(c.meta);
+    int nn = 0, kk = -1;
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      if (!(id >= 5 && id <= 8)) { ++nn; kk = k; }
+    }
+    if (nn == 1) return kk;
+    double opac = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      if (!(id >= 5 && id <= 8)) opac = opac + sp.kapd(cell_slot(c.meta, k)) * c.rho[k];
+    }
+    if (opac == 0.0) return -1;
+    double frac = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      if (id >= 5 && id <= 8) continue;
+      frac = frac + sp.kapd(cell_slot(c.meta, k)) * c.rho[k] / opac;
+      if (xran <= frac + 1.0e-10) return k;
+    }
+    return -1;
+  }
+
+  // emit_common_2.f90:201-372, vertical diffusion (|diffdir| = 2) without
+  // accretion photons (nacc = 0): move the packet to the diffusion surface,
+  // heat the surface cell and emit isotropically from it.  The k-th
+  // diffusion absorption at a surface cell (atomic counter) heats it to
+  // T^4 = T0^4 + k dT^4, the reference's recursion of :260-272.
+  __device__ bool emit_diffusion(const LaunchParams& P) {
+    const double Tmax = 199999.0;
+    const int dd = cell_diffdir(m.cells[cidx(ir, it, ip)].flags);
+    if (dd == -2) {
+      while (it >= 1 && cell_diffus(m.cells[cidx(ir, it, ip)].flags)) it = it - 1;
+      if (it < 1) return false;
+      it = it + 1;
+    } else {
+      while (it <= m.ntg - 1 && cell_diffus(m.cells[cidx(ir, it, ip)].flags)) it = it + 1;
+      if (it > m.ntg - 1) return false;
+    }
+    cosb = zp / rtot;
+    sinb = sqrt(1.0 - cosb * cosb);
+    const double cosbnew = 1.00001 * m.costarr[it - 1];
+    const double sinbnew = sqrt(1.0 - cosbnew * cosbnew);
+    xp = xp * sinbnew / sinb;
+    yp = yp * sinbnew / sinb;
+    zp = rtot * cosbnew;
+    const double mu0 = m.costarr[it - 1], sth = m.sintarr[it - 1];
+    double sux, suy, suz;
+    if (mu0 > 0.0) { sux = -mu0 * xp / sth / rtot; suy = -mu0 * yp / sth / rtot; suz = sth; }
+    else { sux = mu0 * xp / sth / rtot; suy = mu0 * yp / sth / rtot; suz = -sth; }
+    isotrp(sux, suy, suz);
+    cost = uz;
+    sint = sqrt(1.0 - cost * cost);
+    cosp = ux / sint;
+    sinp = uy / sint;
+    phi = atan2(sinp, cosp);
+    if (m.costarr[it - 1] < 0.0) it = it - 1;
+    const double dA = PI * sth * (m.rarr[ir] * m.rarr[ir] - m.rarr[ir - 1] * m.rarr[ir - 1]);
+    double T4s = m.tstar * m.tstar;
+    T4s = T4s * T4s;
+    const int64_t cs = cidx(ir, it, ip);
+    const CellRec c = m.cells[cs];
+    int nth = 0;
+    for (int k = 0; k < cell_n(c.meta); ++k) { const int id = cell_id(c.meta, k); if (!(id >= 5 && id <= 8)) ++nth; }
+    if (nth == 0) return false;
+    const int32_t k = atomicAdd(T.ndiff + cs, nth) + nth;
+    const double t0 = __ldg(m.tdust + cs);
+    double T4d = t0 * t0;
+    T4d = T4d * T4d;
+    const double T4 = T4d + (double)k * (4.0 * PI * T4s / (P.nphot_diff * dA));
+    const double tsurf = fmin(Tmax / 11605.0, pow(T4, 0.25));
+    if (select_thermal(c) < 0) return false;
+    double T4b = tsurf * tsurf;
+    T4b = T4b * T4b;
+    const double T4eff = 0.0;
+    const double mu = ux * sux + uy * suy + uz * suz;
+    const double T = fmin(pow(T4b + 0.75 * mu * T4eff, 0.25), Tmax / 11605.0);
+    nub = bbfreq(T);
+    if (cell_diffdir(c.flags) == -2) it = it - 1; else it = it + 1;
+    return true;
+  }
+
   // slot of a species id whose component is absent in the lookup cell
   __device__ __forceinline__ int idust2slot(int idust2) const {
     for (int s = 0; s < m.nslot; ++s)
@@ -892,7 +992,7 @@ struct Packet {
   // ------------------------------------------------------------ packet
   __device__ int run(int64_t iphot, const LaunchParams& P) {
     on_wall = false;
-    nscat = nabsev = ncross = nstar = 0;
+    nscat = nabsev = ncross = nstar = ndiffev = 0;
     if (iphot < P.npacc || iphot > P.npacc + P.ns) return 3;   // rejected at launch
     if (iphot < P.npacc + P.npaccstar) {
       if (P.ips == 0) initpspot(1); else initp_ps(1);
@@ -967,18 +1067,23 @@ struct Packet {
           if (idust2 == 1 || idust2 == 2 || idust2 == 5 || idust2 == 6 || idust2 == 9) i_orig = 2;
           else if (idust2 == 3 || idust2 == 7) i_orig = 3;
           else i_orig = 4;
-          if (!(c.flags & 1u)) atomicAdd(T.nabs + ci, 1);
-          const double tave = __ldg(m.tdust + ci);
-          sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90
-          cost = 1.0 - 2.0 * ran();
-          sint = sqrt(1.0 - cost * cost);
-          phi = R2P * ran();
-          cosp = cos(phi);
-          sinp = sin(phi);
-          nub = lucydustfreq(tave, m.slot_species[slot]);
-          uy = sint * sinp;
-          ux = sint * cosp;
-          uz = cost;
+          if (!cell_diffus(c.flags)) {
+            atomicAdd(T.nabs + ci, 1);
+            const double tave = __ldg(m.tdust + ci);
+            sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90
+            cost = 1.0 - 2.0 * ran();
+            sint = sqrt(1.0 - cost * cost);
+            phi = R2P * ran();
+            cosp = cos(phi);
+            sinp = sin(phi);
+            nub = lucydustfreq(tave, m.slot_species[slot]);
+            uy = sint * sinp;
+            ux = sint * cosp;
+            uz = cost;
+          } else {
+            ++ndiffev;
+            if (!emit_diffusion(P)) return 3;
+          }
           iflag = 0;
           opacset(nub, KAPD_PROPAGATE);
           ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;
@@ -1074,7 +1179,7 @@ __global__ void __launch_bounds__(kBlock) transport_fp64(LaunchParams P) {
       mcrt_packet_log& L = P.log[k];
       L.iphot = iphot; L.nscat = pk.nscat; L.nabs = pk.nabsev; L.ncross = pk.ncross; L.nstar = pk.nstar;
       L.status = st; L.ir = 0; L.it = 0; L.ip = 0; L.ndraws = pk.rng.ndraws;
-      L.iflag = pk.iflag; L.i_orig = pk.i_orig; L.pad = 0;
+      L.iflag = pk.iflag; L.i_orig = pk.i_orig; L.pad = pk.ndiffev;
       L.nub = pk.nub; L.cost = pk.cost; L.phi = pk.phi; L.sip = pk.sip; L.sqp = pk.sqp; L.sup = pk.sup; L.svp = pk.svp;
       L.xp = pk.xp; L.yp = pk.yp; L.zp = pk.zp;
     }
@@ -1085,6 +1190,55 @@ __global__ void __launch_bounds__(kBlock) transport_fp64(LaunchParams P) {
   for (int i = 0; i < 12; ++i) {
     unsigned long long s = warp_sum(v[i]);
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(P.t.cnt + i, s);
+  }
+}
+
+// End-of-iteration dust temperature of the diffusion cells: the state the
+// reference's per-packet updates leave behind (emit_common_2.f90:260-339 with
+// nacc = 0): the surface cell of a column that saw N diffusion absorptions
+// holds min(Tmax, (T0^4 + N dT^4)^(1/4)); the interior cells whose
+// neighbour toward the surface holds a thermal component take that value.
+__global__ void diffusion_finalize(DevModel m, const int32_t* ndiff, const double* tdust0, double* tdust,
+                                   double nphot) {
+  const int64_t n = (int64_t)m.nrg * m.ntg * m.npg;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    double t = tdust0[c];
+    const uint32_t fl = m.cells[c].flags;
+    if (cell_diffus(fl)) {
+      const int ir = (int)(c % m.nrg) + 1;
+      const int it = (int)((c / m.nrg) % m.ntg) + 1;
+      const int ip = (int)(c / ((int64_t)m.nrg * m.ntg)) + 1;
+      auto ci = [&](int r, int tt, int p) { return (int64_t)(r - 1) + (int64_t)m.nrg * ((tt - 1) + (int64_t)m.ntg * (p - 1)); };
+      const int dd = cell_diffdir(fl);
+      int is = it, iwall;
+      if (dd == -2) {
+        while (is - 1 >= 1 && cell_diffus(m.cells[ci(ir, is - 1, ip)].flags)) --is;
+        iwall = is;
+      } else {
+        while (is + 1 <= m.ntg - 1 && cell_diffus(m.cells[ci(ir, is + 1, ip)].flags)) ++is;
+        iwall = is + 1;
+      }
+      const int64_t cs = ci(ir, is, ip);
+      const int32_t N = ndiff[cs];
+      bool gets = false;
+      if (N > 0) {
+        if (is == it) gets = cell_thermal(m.cells[cs].flags);
+        else if (dd == -2) gets = cell_thermal(m.cells[ci(ir, it - 1, ip)].flags);
+        else gets = cell_thermal(m.cells[ci(ir, it + 1, ip)].flags);
+      }
+      if (gets) {
+        const double sth = m.sintarr[iwall - 1];
+        const double dA = PI * sth * (m.rarr[ir] * m.rarr[ir] - m.rarr[ir - 1] * m.rarr[ir - 1]);
+        double T4s = m.tstar * m.tstar;
+        T4s = T4s * T4s;
+        const double t0 = tdust0[cs];
+        double T4d = t0 * t0;
+        T4d = T4d * T4d;
+        const double T4 = T4d + (double)N * (4.0 * PI * T4s / (nphot * dA));
+        t = fmin(199999.0 / 11605.0, pow(T4, 0.25));
+      }
+    }
+    tdust[c] = t;
   }
 }
 

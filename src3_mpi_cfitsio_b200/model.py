@@ -90,6 +90,12 @@ class Workload:
     aperture_au: float = 5000.0
     # theta-wall clustering toward the equator
     theta_power: float = 2.0
+    # inner-rim refinement (gridset_5_model13new.f90:437-493): number of walls
+    # spent between the dust rim and rim_top_au, the first cell holding a
+    # midplane Rosseland optical depth of rim_tau
+    rim_walls: int = 20
+    rim_top_au: float = 0.15
+    rim_tau: float = 0.5
     # multiplicative clump field (3-D fractal models); None for smooth models
     clump_seed: int | None = None
     clump_dim: float = 2.6
@@ -118,7 +124,12 @@ class Model:
         rarr = np.empty(nrg)
         rarr[0] = 1.0                                  # stellar surface
         rarr[1] = rddust
-        rarr[2:] = rddust * (rmax / rddust) ** (np.arange(1, nrg - 1) / (nrg - 2))
+        nf = self._rim_walls(autors, rddust) if (w.rim_walls > 0 and w.massd > 0) else np.empty(0)
+        nfw = nf.size
+        rarr[2:2 + nfw] = nf
+        r0 = rarr[1 + nfw]
+        nlog = nrg - 2 - nfw
+        rarr[2 + nfw:] = r0 * (rmax / r0) ** (np.arange(1, nlog + 1) / nlog)
         rarr[-1] = rmax
         r2arr = rarr * rarr
 
@@ -143,6 +154,63 @@ class Model:
         aarr = np.sin(phiarr)
         barr = -np.cos(phiarr)
         return autors, rddust, rmax, rarr, r2arr, thetarr, costarr, sintarr, tan2arr, phiarr, aarr, barr
+
+    def _rim_walls(self, autors, rddust):
+        """Walls resolving the optically thick disk rim: the first cell holds a
+        midplane Rosseland depth rim_tau (tauw of gridset_5_model13new.f90:437-
+        446), then the spacing ratio grows geometrically (rfac <- rfac**gamma,
+        :465-469) so that rim_walls walls reach rim_top_au."""
+        w = self.w
+        rmincgs = w.rstar * RSOL
+        rmaxd = w.rmaxd_au * autors
+        z1 = w.h100_au * autors / (100.0 * autors) ** w.b_exp
+        p = w.b_exp - w.a_exp
+        const = R2P ** 1.5 * rmincgs ** 2 * (rmincgs * z1)
+        rho0 = w.massd * MSOL / const / (
+            1.0 / (p + 2.0) * (rmaxd ** (p + 2.0) - rddust ** (p + 2.0))
+            - 1.0 / (p + 1.5) * (rmaxd ** (p + 1.5) - rddust ** (p + 1.5)))
+        # Rosseland mean of the dust law at 1400 K relative to V (dust_5.f90:465)
+        lam = np.logspace(-1, np.log10(3000.0), 4000)
+        x = 1.4388e4 / (lam * 1400.0)
+        dB = x ** 5 * np.exp(x) / np.expm1(x) ** 2 / lam ** 0   # dB/dT shape in nu
+        nu = 1.0 / lam
+        kap = (lam / 0.55) ** -1.5
+        wgt = dB * np.gradient(nu)
+        chir = np.sum(np.abs(wgt)) / np.sum(np.abs(wgt) / kap)
+        kV = w.kappa0 * 0.55 ** -1.5
+        # cumulative midplane tau_R from the rim
+        rr = rddust * (1.0 + np.logspace(-12, np.log10(w.rim_top_au / w.rddust_au - 1.0 + 1e-12), 20000))
+        rho = rho0 * (1.0 - np.sqrt(1.0 / rr)) * rr ** (-w.a_exp)
+        dtau = kV * chir * rho * rmincgs
+        tau = np.concatenate(([0.0], np.cumsum(0.5 * (dtau[1:] + dtau[:-1]) * np.diff(rr))))
+        tau = tau - tau[0]
+        r1 = float(np.interp(w.rim_tau, tau, rr))
+        rtop = w.rim_top_au * autors
+        n = w.rim_walls
+        f1 = r1 / rddust
+        # rfac_k = f1**(gamma**k); find gamma so that wall n reaches rtop
+        def top(gam):
+            r = rddust
+            f = f1
+            for _ in range(n):
+                r = r * f
+                f = f ** gam
+            return r
+        lo, hi = 1.0, 3.0
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            if top(mid) > rtop:
+                hi = mid
+            else:
+                lo = mid
+        gam = lo
+        walls = []
+        r, f = rddust, f1
+        for _ in range(n):
+            r = r * f
+            f = f ** gam
+            walls.append(r)
+        return np.array(walls)
 
     # ------------------------------------------------------------- densities
     @staticmethod
@@ -427,7 +495,7 @@ class Model:
             densarr=F(dens), findopac=F(findopac), diffus=F(diffus), diffdir=F(diffdir),
             tdust=F(tdust), vcell=F(vcell), ravearr=rave,
             Ldint=np.linspace(1.0 / (nrg - 1), 1.0, nrg - 1),
-            hdisk=np.zeros(nrg - 1),
+            hdisk=(w.h100_au * autors / (100.0 * autors) ** w.b_exp) * rave ** w.b_exp,
         )
         self.tables = dict(
             nlambda=np.full(nopac, nl, dtype=np.int32),
@@ -457,7 +525,7 @@ def reference_2d(**over) -> Model:
 
 def small_2d(**over) -> Model:
     """A reduced grid of the same model for quick oracle comparisons."""
-    kw = dict(nrg=31, ntg=21, npg=2, nfreq=20, nmu=4, nph=1, npeel=3, nxhst=21)
+    kw = dict(nrg=31, ntg=21, npg=2, nfreq=20, nmu=4, nph=1, npeel=3, nxhst=21, rim_walls=8)
     kw.update(over)
     return Model(Workload(**kw))
 
@@ -483,3 +551,95 @@ def warm(m: Model, t1au_k: float = 300.0, q: float = 0.5) -> Model:
     T = np.where(has, T, 0.1 / 11605.0)
     m.grid["tdust"] = np.asfortranarray(T).ravel(order="F")
     return m
+
+
+def _chiR(tables, T, species):
+    """chiR (dust_5.f90:112-141): Rosseland table interpolated in log T."""
+    lTint = tables["lTint"]
+    nT = lTint.size
+    kr = tables["kappar"].reshape((nT, -1), order="F")[:, species - 1]
+    lT = math.log(T)
+    k = int((nT - 1) * (lT - lTint[0]) / (lTint[-1] - lTint[0])) + 1
+    k = min(max(k, 1), nT - 1)
+    f = (lT - lTint[k - 1]) / (lTint[k] - lTint[k - 1])
+    return (1.0 - f) * kr[k - 1] + f * kr[k]
+
+
+def setdiffus(m: Model, tdave: np.ndarray, iteration: int) -> Model:
+    """Flag the optically thick disk interior for the diffusion treatment.
+
+    Restates setdiffus (setdiffus_5.f90:1-132): for every radius inside the
+    disk, march from each theta cell toward the pole accumulating the
+    Rosseland optical depth; cells whose photon mean free path to tau=1 is
+    below h/20 become diffusion cells with diffdir=-2 (upper hemisphere),
+    mirrored with diffdir=+2 below the midplane.  kapd is taken at its V-band
+    value kappav*R*, the value setup_wave.f90:50 leaves in it.
+    """
+    w = m.w
+    nrg, ntg, npg = w.nrg, w.ntg, w.npg
+    dens = m.dens4()
+    td = np.asarray(tdave).reshape((nrg, ntg, npg), order="F")
+    rarr, thetarr = m.grid["rarr"], m.grid["thetarr"]
+    autors = m.config["autors"]
+    rmaxd = w.rmaxd_au * autors
+    hdisk = m.grid["hdisk"]
+    kv = m.tables["kappav"]
+    rmincgs = w.rstar * RSOL
+    fo = m.grid["findopac"].reshape((nrg, ntg, npg, NDG2), order="F")
+    diffus = np.zeros((nrg, ntg, npg), dtype=np.int32)
+    diffdir = np.zeros((nrg, ntg, npg), dtype=np.int32)
+    thermal = [True, True, True, True, False, False, False, False, True, True]
+    if w.massd > 0.0:
+        nr0 = 1 if m.config["rddust"] == rarr[0] else 3
+        ir = nr0
+        rad = rarr[ir - 1]
+        while rad < rmaxd and ir <= nrg - 1:
+            zmr = hdisk[ir - 1]
+            for it in range((ntg - 1) // 2, 1, -1):
+                tau = 0.0
+                tau1 = 0.0
+                itt = it
+                while tau < 1.0 and itt > 1:
+                    dt = thetarr[itt] - thetarr[itt - 1]
+                    tau1 = tau
+                    tt = td[ir - 1, itt - 1, 0]
+                    if iteration < 2:
+                        tt = max(tt, 50.0 / 11605.0)
+                    for idd in range(NDG2):
+                        if thermal[idd] and dens[ir - 1, itt - 1, 0, idd] > 0.0:
+                            sp = int(fo[ir - 1, itt - 1, 0, idd])
+                            tau += (kv[sp - 1] * rmincgs) * _chiR(m.tables, tt, sp) * \
+                                dens[ir - 1, itt - 1, 0, idd] * dt * rad
+                    itt -= 1
+                if tau > 1.0:
+                    lmfp1 = rad * (thetarr[itt + 1] - thetarr[itt]) / (tau - tau1) * (1.0 - tau1)
+                else:
+                    lmfp1 = rad * (thetarr[itt + 1] - thetarr[itt])
+                lmfp = rad * (thetarr[it] - thetarr[itt + 1]) + lmfp1
+                if tau >= 1.0 and lmfp < zmr / 20.0:
+                    diffus[ir - 1, it - 1:(ntg - 1) // 2, 0] = 1
+                    diffdir[ir - 1, it - 1:(ntg - 1) // 2, 0] = -2
+            ir += 1
+            rad = rarr[ir - 1]
+        for it in range((ntg + 1) // 2, ntg):
+            diffus[:nrg - 1, it - 1, 0] = diffus[:nrg - 1, ntg - it - 1, 0]
+            diffdir[:nrg - 1, it - 1, 0] = -diffdir[:nrg - 1, ntg - it - 1, 0]
+        if npg > 2:
+            diffus[:nrg - 1, :ntg - 1, 1:npg - 1] = diffus[:nrg - 1, :ntg - 1, :1]
+            diffdir[:nrg - 1, :ntg - 1, 1:npg - 1] = diffdir[:nrg - 1, :ntg - 1, :1]
+    # cells without a thermal component cannot diffuse
+    has_th = (dens[..., [0, 1, 2, 3, 8, 9]] > 0).any(axis=-1)
+    diffus = np.where(has_th, diffus, 0)
+    diffdir = np.where(has_th, diffdir, 0)
+    m.grid["diffus"] = np.asfortranarray(diffus).ravel(order="F")
+    m.grid["diffdir"] = np.asfortranarray(diffdir).ravel(order="F")
+    # gridset_5_model13new.f90:1855-1866: tdust of diffusion cells restarts at 0.1 K
+    T = np.where(diffus > 0, 0.1 / 11605.0, td)
+    T = np.where(dens.sum(axis=-1) > 0, T, 0.1 / 11605.0)
+    m.grid["tdust"] = np.asfortranarray(T).ravel(order="F")
+    return m
+
+
+def with_diffusion(m: Model, iteration: int = 2) -> Model:
+    """setdiffus on the model's current temperature."""
+    return setdiffus(m, m.grid["tdust"].copy(), iteration)

@@ -137,3 +137,38 @@ def test_errors_are_reported_not_fatal(warm_small):
     eng.run(100)                        # context still usable
     assert eng.download(images=False).counters()["packets"] == 100
     eng.close()
+
+
+@pytest.fixture(scope="module")
+def diffusion_small():
+    return model.with_diffusion(model.warm(model.small_2d()))
+
+
+def test_diffusion_statistical_and_pre_diffusion_exact(diffusion_small, oracle_mod):
+    """Diffusion (emit_common_2.f90:201-372): packets that never reach a
+    diffusion cell stay event-for-event equal; the ones that do depend on
+    the order in which diffusion absorptions heat the surface cell, so the
+    ensemble is compared within Monte Carlo error."""
+    m = diffusion_small
+    n = 20000
+    eng = _engine(m)
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    tg = eng.download(images=False)
+    to, lo = oracle_mod.run(abi.Bundle(m), n, ipeel=0, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    nodiff = (g["pad"] == 0) & (o["pad"] == 0)
+    assert g["pad"].sum() > 20 and o["pad"].sum() > 20       # the diffusion branch runs
+    same, exact = _same_packets(g, o)
+    assert exact[nodiff].mean() >= 0.995
+    # diffusion events: same count up to Monte Carlo noise
+    dg, do = g["pad"].sum(), o["pad"].sum()
+    assert abs(dg - do) <= 5 * np.sqrt(do) + 5
+    assert (g["status"] == 3).sum() == 0
+    # SED of the ensemble
+    a = tg.shaped("nums")[..., 0].sum(axis=(1, 2, 3))
+    b = to.shaped("nums")[..., 0].sum(axis=(1, 2, 3))
+    assert np.all(np.abs(a - b) <= 5 * np.sqrt(np.maximum(b, 1)) + 5)
+    eng.close()
