@@ -49,6 +49,10 @@ extern "C" {
 #define MCRT_NO      8    /* SED components, tts_mod_5.f90:30                      */
 #define MCRT_IZMAX 145    /* zeta-series terms of bbfreq, random.f90:12            */
 
+/* ---- scheduling of the transport kernels ---- */
+#define MCRT_SCHED_PACKET  0   /* one thread runs one packet start to finish         */
+#define MCRT_SCHED_WARP    1   /* lanes step rays in lockstep, events run in batches */
+
 /* ---- arithmetic of the transport kernels ---- */
 #define MCRT_PREC_FP64   0   /* everything in FP64 (event-for-event with the oracle) */
 #define MCRT_PREC_MIXED  1   /* FP32 walk/scatter, FP64 radial roots, tau sums, tallies */
@@ -199,6 +203,12 @@ int mcrt_upload_tables(mcrt_ctx *ctx, const mcrt_tables *tab);
 
 /* Select FP64 or mixed-precision transport (MCRT_PREC_*). */
 int mcrt_set_precision(mcrt_ctx *ctx, int32_t mode);
+
+/* Select the kernel schedule (MCRT_SCHED_*; default MCRT_SCHED_WARP) and,
+ * for the warp schedule, how many lanes of a warp must wait for an event
+ * before the warp stops stepping rays to run them (1..32, default 16).
+ * Results do not depend on either choice. */
+int mcrt_set_schedule(mcrt_ctx *ctx, int32_t schedule, int32_t event_batch);
 
 /* Zero the tallies of one iteration (initarr_2_new.f90:79-119). */
 int mcrt_reset_tallies(mcrt_ctx *ctx);

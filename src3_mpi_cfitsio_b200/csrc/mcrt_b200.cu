@@ -24,6 +24,8 @@ cudaError_t launch_transport_mixed(const LaunchParams& p, int grid, cudaStream_t
 cudaError_t launch_diffusion_finalize(const DevModel& m, const int32_t* ndiff, const double* tdust0, double* tdust,
                                       double nphot, cudaStream_t s);
 int transport_fp64_blocks_per_sm();
+cudaError_t launch_transport_sched_fp64(const LaunchParams& p, int grid, cudaStream_t s);
+int transport_sched_fp64_blocks_per_sm();
 int transport_mixed_blocks_per_sm();
 }  // namespace mcrt
 
@@ -34,6 +36,8 @@ struct mcrt_ctx {
   int device = 0;
   int nsm = 148;
   int precision = MCRT_PREC_FP64;
+  int schedule = MCRT_SCHED_WARP;
+  int event_batch = 16;
   bool have_grid = false, have_tables = false;
   std::string err;
   cudaStream_t stream = nullptr;
@@ -325,6 +329,15 @@ int mcrt_set_precision(mcrt_ctx* ctx, int32_t mode) {
   return MCRT_OK;
 }
 
+int mcrt_set_schedule(mcrt_ctx* ctx, int32_t schedule, int32_t event_batch) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (schedule != MCRT_SCHED_PACKET && schedule != MCRT_SCHED_WARP) return fail(ctx, MCRT_ERR_ARG, "unknown schedule %d", schedule);
+  if (event_batch < 1 || event_batch > 32) return fail(ctx, MCRT_ERR_ARG, "event_batch must be 1..32");
+  ctx->schedule = schedule;
+  ctx->event_batch = event_batch;
+  return MCRT_OK;
+}
+
 int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   if (!ctx || !g) return MCRT_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
@@ -584,12 +597,16 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   CK(cudaMemsetAsync(ctx->d_next, 0, sizeof(unsigned long long), ctx->stream));
   CK(cudaMemsetAsync(ctx->d_err, 0, 4 * sizeof(int32_t), ctx->stream));
   const int64_t npk = hi - lo + 1;
-  int per_sm = ctx->precision == MCRT_PREC_FP64 ? transport_fp64_blocks_per_sm() : transport_mixed_blocks_per_sm();
+  P.event_batch = ctx->event_batch;
+  const bool warp = ctx->schedule == MCRT_SCHED_WARP;
+  int per_sm = ctx->precision == MCRT_PREC_FP64 ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
+                                                : transport_mixed_blocks_per_sm();
   int64_t want = (npk + kTransportBlock - 1) / kTransportBlock;
   int grid = (int)std::min<int64_t>((int64_t)ctx->nsm * std::max(per_sm, 1), std::max<int64_t>(want, 1));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  cudaError_t e = ctx->precision == MCRT_PREC_FP64 ? launch_transport_fp64(P, grid, ctx->stream)
-                                                    : launch_transport_mixed(P, grid, ctx->stream);
+  cudaError_t e = ctx->precision == MCRT_PREC_FP64
+                      ? (warp ? launch_transport_sched_fp64(P, grid, ctx->stream) : launch_transport_fp64(P, grid, ctx->stream))
+                      : launch_transport_mixed(P, grid, ctx->stream);
   if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   e = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);

@@ -85,6 +85,8 @@ struct LaunchParams {
   int64_t block0;               // first random block of the iteration: (iter-1)*np
   int64_t ns, npacc, npaccstar; // packet split (newdisktherm_5_fuv.f90:158-191)
   int32_t ipeel, ips;
+  int32_t event_batch;          // warp scheduler: lanes that must wait before events run
+  int32_t pad_;
   double nphot_diff;            // nphot of emit_common's surface heating (ns of this shard)
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter

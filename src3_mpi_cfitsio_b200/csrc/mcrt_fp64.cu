@@ -2,13 +2,24 @@
 // every FP64 add/multiply is a separate IEEE operation, as in the oracle.
 #include <cuda_runtime.h>
 
-#include "mcrt_transport.cuh"
+#include "mcrt_sched.cuh"
 
 namespace mcrt {
 
 cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t s) {
   transport_fp64<<<grid, kBlock, 0, s>>>(p);
   return cudaGetLastError();
+}
+
+cudaError_t launch_transport_sched_fp64(const LaunchParams& p, int grid, cudaStream_t s) {
+  transport_sched<<<grid, kBlock, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+int transport_sched_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_sched, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
 }
 
 cudaError_t launch_diffusion_finalize(const DevModel& m, const int32_t* ndiff, const double* tdust0, double* tdust,

@@ -44,6 +44,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_upload_grid.argtypes = [C.c_void_p, P(abi.Grid)]
     lib.mcrt_upload_tables.argtypes = [C.c_void_p, P(abi.Tables)]
     lib.mcrt_set_precision.argtypes = [C.c_void_p, C.c_int32]
+    lib.mcrt_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     lib.mcrt_reset_tallies.argtypes = [C.c_void_p]
     lib.mcrt_run_iteration.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32, C.c_int32]
@@ -63,7 +64,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.argtypes = [C.c_void_p]
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
-    for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision",
+    for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision", "mcrt_set_schedule",
                  "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_mark", "mcrt_elapsed_ms",
@@ -112,6 +113,11 @@ class Engine:
         mode = {"fp64": abi.PREC_FP64, "mixed": abi.PREC_MIXED}[precision]
         self._check(self.lib.mcrt_set_precision(self.ctx, mode))
         self.precision = precision
+
+    def set_schedule(self, schedule: str = "warp", event_batch: int = 16):
+        mode = {"packet": 0, "warp": 1}[schedule]
+        self._check(self.lib.mcrt_set_schedule(self.ctx, mode, event_batch))
+        self.schedule = schedule
 
     def upload_grid(self):
         self.bundle = abi.Bundle(self.model)

@@ -172,3 +172,22 @@ def test_diffusion_statistical_and_pre_diffusion_exact(diffusion_small, oracle_m
     b = to.shaped("nums")[..., 0].sum(axis=(1, 2, 3))
     assert np.all(np.abs(a - b) <= 5 * np.sqrt(np.maximum(b, 1)) + 5)
     eng.close()
+
+
+@pytest.mark.parametrize("batch", [1, 12, 32])
+def test_schedules_agree_bitwise(warm_small, batch):
+    """The warp-scheduled kernel reorders work across lanes, never within a
+    packet: its packet logs equal the per-thread kernel's bit for bit."""
+    n = 3000
+    logs = []
+    for sched in ("packet", "warp"):
+        eng = _engine(warm_small)
+        eng.set_schedule(sched, batch)
+        eng.enable_packet_log(n)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        logs.append(abi.packet_log_to_numpy(eng.packet_log(n)))
+        eng.close()
+    a, b = logs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
