@@ -241,6 +241,20 @@ int mcrt_accumulate_tallies(mcrt_ctx *ctx, const mcrt_tallies *in);
 int mcrt_update_temperature(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
                             double *tdave, int32_t *converge, double *sig);
 
+/* Allocation-free variant of mcrt_update_temperature (no counterpart in the
+ * reference).  For callers that cannot allocate device memory while they
+ * run, e.g. a Fortran driver stepping the Lucy loop inside a memory pool it
+ * sized up front, or code that must not trigger cudaMalloc's implicit device
+ * synchronisation between iterations.  Same inputs, outputs and result as
+ * mcrt_update_temperature (sig to summation order), but the scratch lives in
+ * a fixed 12 MiB device array inside the library, so models are limited to
+ * nrg*ntg*npg <= 524288 cells (larger ones return MCRT_ERR_ARG).  The first
+ * call on each device looks the array up and should come before any stream
+ * capture.  All calls in the process share the array: calls that overlap on
+ * a GPU (two contexts on one device, or two host threads) race. */
+int mcrt_update_temperature_noalloc(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
+                                    double *tdave, int32_t *converge, double *sig);
+
 /* Parity support: record a mcrt_packet_log for the first `max_packets`
  * packets of the next mcrt_run_iteration (0 disables). */
 int mcrt_enable_packet_log(mcrt_ctx *ctx, int64_t max_packets);

@@ -246,6 +246,38 @@ __global__ void tdust_from_tdave(int64_t n, const double* tdave, const int32_t* 
   }
 }
 
+// Convergence sums of tfinal_5_test1.f90:307-332 accumulated on the device:
+// out[0..2] sums of |dT/T|, out[3..5] sums of (dT/T)^2, out[6..8] counts.
+__global__ void tfinal_stats(int nrg, int ntg, const double* told, const double* tnew, const double* rarr,
+                             double autors, double* out) {
+  const int nu = (ntg - 1) / 2;
+  const int64_t n = (int64_t)(nrg - 1) * nu;
+  const double T01 = 0.1 / 11605.0;
+  double a[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % (nrg - 1)) + 1;
+    const int it = (int)(k / (nrg - 1)) + 1;
+    const int64_t c = (ir - 1) + (int64_t)nrg * (it - 1);
+    const double to = told[c], tn = tnew[c];
+    const double d = (tn - to) / tn;
+    if (tn != to && tn > T01 && to > T01) { a[0] += fabs(d); a[3] += d * d; a[6] += 1.0; }
+    if (tn > T01 && to > T01) { a[1] += fabs(d); a[4] += d * d; a[7] += 1.0; }
+    if (rarr[ir - 1] / autors < 5.0 && tn > T01 && to > T01) { a[2] += fabs(d); a[5] += d * d; a[8] += 1.0; }
+  }
+  for (int i = 0; i < 9; ++i) {
+    double v = a[i];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(out + i, v);
+  }
+}
+
+// Scratch of mcrt_update_temperature_noalloc: previous field, new upper
+// hemisphere, result, and the nine convergence sums.  A file-scope device
+// array, so that entry point needs no allocation; every process that loads
+// the library holds it (3*524288+16 doubles, 12 MiB) on each device it uses.
+constexpr int64_t kNoAllocMaxCells = 524288;
+static __device__ __align__(256) double g_tfinal_scratch[3 * kNoAllocMaxCells + 16];
+
 __global__ void to_float(const double* src, float* dst, int64_t n) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
     dst[k] = (float)src[k];
@@ -752,6 +784,64 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
     if (sig) sig[k] = sg[k];
   }
   // convergence when sigma changes by less than 25% between iterations
+  if (*converge == 0 && ctx->prev_sig > 0.0 && std::fabs(ctx->prev_sig - sg[0]) / sg[0] < 0.25) *converge = 1;
+  ctx->prev_sig = sg[0];
+  return MCRT_OK;
+}
+
+// Allocation-free temperature update.  The device address of the
+// file-scope scratch array is looked up once per device (with that device
+// current) on the first call made on it; that first call must therefore not
+// be made while a stream is being captured.
+int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* tdave, int32_t* converge,
+                                    double* sig) {
+  static double* scratch_of_device[64] = {};
+  if (!ctx || !tdave || !converge) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (nphot < 1) return fail(ctx, MCRT_ERR_ARG, "nphot must be positive");
+  const mcrt_config& c = ctx->cfg;
+  const int64_t nc = ctx->ncell;
+  if (nc > kNoAllocMaxCells)
+    return fail(ctx, MCRT_ERR_ARG, "mcrt_update_temperature_noalloc: %lld cells exceed its fixed scratch of %lld cells",
+                (long long)nc, (long long)kNoAllocMaxCells);
+  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, MCRT_ERR_ARG, "device index out of range");
+  CK(cudaSetDevice(ctx->device));
+  double* base = scratch_of_device[ctx->device];
+  if (!base) {
+    CK(cudaGetSymbolAddress((void**)&base, g_tfinal_scratch));
+    scratch_of_device[ctx->device] = base;
+  }
+  double* d_told = base;
+  double* d_tnew = base + kNoAllocMaxCells;
+  double* d_res = base + 2 * kNoAllocMaxCells;
+  double* d_stats = base + 3 * kNoAllocMaxCells;
+  CK(cudaMemcpyAsync(d_told, tdave, nc * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(d_stats, 0, 9 * sizeof(double), ctx->stream));
+  TfinalArgs a{};
+  a.nrg = c.nrg; a.ntg = c.ntg; a.npg = c.npg; a.nT = c.nT; a.nphot = nphot; a.maxii = iter > 3 ? 20 : 1;
+  a.rstar = c.rstar; a.tstar = c.tstarave;
+  a.Tint = ctx->d_tabs + ctx->off_Tint;
+  a.kappap = ctx->d_tabs + ctx->off_kappap;
+  a.kappav = ctx->dm.kappav;
+  a.dtauabs = ctx->dt.dtauabs; a.vcell = ctx->d_vcell; a.dens = ctx->d_dens_thermal; a.tdust = ctx->d_tdust;
+  a.idust3 = ctx->d_idust3; a.diffus = ctx->d_diffus;
+  a.told = d_told; a.tnew = d_tnew; a.tdave = d_res;
+  tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
+  tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
+  tfinal_stats<<<128, 256, 0, ctx->stream>>>(c.nrg, c.ntg, d_told, d_res, ctx->dm.rarr, c.autors, d_stats);
+  tdust_from_tdave<<<512, 256, 0, ctx->stream>>>(nc, d_res, ctx->d_diffus, ctx->d_idust3, ctx->d_cells, ctx->d_tdust);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->d_tdust0, ctx->d_tdust, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(tdave, d_res, nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  double st[9];
+  CK(cudaMemcpyAsync(st, d_stats, 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double sg[3];
+  for (int k = 0; k < 3; ++k) {
+    const double av = st[k] / st[6 + k], av2 = st[3 + k] / st[6 + k];
+    sg[k] = std::sqrt(av2 - av * av);
+    if (sig) sig[k] = sg[k];
+  }
   if (*converge == 0 && ctx->prev_sig > 0.0 && std::fabs(ctx->prev_sig - sg[0]) / sg[0] < 0.25) *converge = 1;
   ctx->prev_sig = sg[0];
   return MCRT_OK;
