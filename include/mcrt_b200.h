@@ -174,6 +174,8 @@ typedef struct mcrt_tallies {
 #define MCRT_C_KILLED        9  /* packets killed after 10000 events    */
 #define MCRT_C_EXITED       10  /* packets that left the grid           */
 #define MCRT_C_STARHITS     11  /* packets absorbed + re-emitted by the star */
+#define MCRT_C_PEEL_RESETS  12  /* testgrid re-locations inside queued peel-off walks */
+#define MCRT_C_PEEL_JOBS    13  /* peel-off jobs queued for the peel-off kernel */
 #define MCRT_NCOUNTERS      16
 
 /* Per-packet summary used by the parity tests (event-for-event checks). */

@@ -26,12 +26,15 @@ def nvcc() -> str:
     return cand if os.path.exists(cand) else "nvcc"
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(LIBDIR, exist_ok=True)
+def build(verbose: bool = False, ptxas_info: bool = False, out: str = LIB, defines=()) -> str:
+    """Compile the library to `out`; `defines` are extra -D macros
+    (compile-time tuning knobs of the kernels)."""
+    libdir = os.path.dirname(out)
+    os.makedirs(libdir, exist_ok=True)
     objs = []
     for src, extra in UNITS:
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        obj = os.path.join(libdir, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *ARCH, *COMMON, *[f"-D{d}" for d in defines], *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
@@ -43,14 +46,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if ptxas_info or verbose:
             sys.stderr.write(r.stderr)
         objs.append(obj)
-    cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", out, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc link failed")
     for o in objs:
         os.remove(o)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

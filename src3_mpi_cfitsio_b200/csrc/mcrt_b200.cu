@@ -26,6 +26,8 @@ cudaError_t launch_diffusion_finalize(const DevModel& m, const int32_t* ndiff, c
 int transport_fp64_blocks_per_sm();
 cudaError_t launch_transport_sched_fp64(const LaunchParams& p, int grid, cudaStream_t s);
 int transport_sched_fp64_blocks_per_sm();
+cudaError_t launch_peel_fp64(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s);
+int peel_fp64_blocks_per_sm();
 int transport_mixed_blocks_per_sm();
 }  // namespace mcrt
 
@@ -63,7 +65,10 @@ struct mcrt_ctx {
   // tallies
   void *d_tally = nullptr;
   size_t tally_bytes = 0;
-  unsigned long long *d_next = nullptr;
+  unsigned long long *d_next = nullptr;    // [0] packets, [1] peel jobs, [2] peel items
+  PeelJob *d_jobs = nullptr;
+  int64_t job_cap = 0;
+  int64_t chunk_packets = 1 << 20;
   int32_t *d_err = nullptr;
   mcrt_packet_log *d_log = nullptr;
   int64_t nlog = 0;
@@ -335,7 +340,7 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   t.dsg = ip; ip += ctx->ncell;
   t.killed = ip; ip += ctx->ncell;
   t.ndiff = ip;
-  if ((rc = dalloc(ctx, &ctx->d_next, 1))) { *out = ctx; return rc; }
+  if ((rc = dalloc(ctx, &ctx->d_next, 4))) { *out = ctx; return rc; }
   if ((rc = dalloc(ctx, &ctx->d_err, 4))) { *out = ctx; return rc; }
   CK(cudaMemset(ctx->d_tally, 0, ctx->tally_bytes));
   *out = ctx;
@@ -626,23 +631,46 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   P.log = ctx->d_log;
   P.nlog = ctx->nlog;
   P.err = ctx->d_err;
-  CK(cudaMemsetAsync(ctx->d_next, 0, sizeof(unsigned long long), ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_err, 0, 4 * sizeof(int32_t), ctx->stream));
   const int64_t npk = hi - lo + 1;
   P.event_batch = ctx->event_batch;
   const bool warp = ctx->schedule == MCRT_SCHED_WARP;
+  // peel-offs go through the job queue and the peel-off kernel
+  const bool queue = P.ipeel && warp && ctx->precision == MCRT_PREC_FP64 && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
+  if (queue && !ctx->d_jobs) {
+    ctx->job_cap = 8 * ctx->chunk_packets;
+    int rc = dalloc(ctx, &ctx->d_jobs, (size_t)ctx->job_cap);
+    if (rc) return rc;
+  }
+  P.jobs = queue ? ctx->d_jobs : nullptr;
+  P.njobs = ctx->d_next + 1;
+  P.job_cap = ctx->job_cap;
   int per_sm = ctx->precision == MCRT_PREC_FP64 ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
                                                 : transport_mixed_blocks_per_sm();
-  int64_t want = (npk + kTransportBlock - 1) / kTransportBlock;
-  int grid = (int)std::min<int64_t>((int64_t)ctx->nsm * std::max(per_sm, 1), std::max<int64_t>(want, 1));
+  const int full_grid = ctx->nsm * std::max(per_sm, 1);
+  const int peel_grid = ctx->nsm * peel_fp64_blocks_per_sm();
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  cudaError_t e = ctx->precision == MCRT_PREC_FP64
-                      ? (warp ? launch_transport_sched_fp64(P, grid, ctx->stream) : launch_transport_fp64(P, grid, ctx->stream))
-                      : launch_transport_mixed(P, grid, ctx->stream);
-  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
+  const int64_t chunk = queue ? ctx->chunk_packets : npk;
+  for (int64_t c_lo = lo; c_lo <= hi; c_lo += chunk) {
+    const int64_t c_hi = std::min(hi, c_lo + chunk - 1);
+    P.lo = c_lo;
+    P.hi = c_hi;
+    CK(cudaMemsetAsync(ctx->d_next, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    const int64_t want = (c_hi - c_lo + 1 + kTransportBlock - 1) / kTransportBlock;
+    const int grid = (int)std::min<int64_t>(full_grid, std::max<int64_t>(want, 1));
+    cudaError_t e = ctx->precision == MCRT_PREC_FP64
+                        ? (warp ? launch_transport_sched_fp64(P, grid, ctx->stream) : launch_transport_fp64(P, grid, ctx->stream))
+                        : launch_transport_mixed(P, grid, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
+    if (queue) {
+      e = launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
+      if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
+    }
+  }
+  P.lo = lo;
+  P.hi = hi;
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
-  e = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);
-  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion finalize: %s", cudaGetErrorString(e));
+  cudaError_t ef = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);
+  if (ef != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion finalize: %s", cudaGetErrorString(ef));
   CK(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));

@@ -78,6 +78,21 @@ struct DevModel {
   const int64_t *jump1, *jump2;
 };
 
+// One peel-off request: the packet's state at an emission, scattering or
+// absorption, walked to every inclination by the peel-off kernel
+// (peeloff_3d_2_test.f90:7-347 called from newdisktherm_5_fuv.f90:378-413
+// and propagate_5_fuv.f90:84-89, 163-169).
+constexpr int kJobSlots = 4;   // species slots carried in a job
+struct __align__(16) PeelJob {
+  double x, y, z, rs, rt;         // position
+  double si, sq, su, sv;          // Stokes (si is the un-weighted I of a direct peel-off)
+  double d0, d1, d2, d3, d4;      // packet direction cost,sint,cosp,sinp,phi; direct: cosb,sinb,coslp,sinlp
+  double kapd[kJobSlots];         // opacity per species slot at the packet's frequency
+  double g, pl;                   // phase-function parameters of the scattering species
+  int32_t r, t, p;                // cell
+  uint32_t bits;                  // onw | iflag<<1 | direct<<2 | (i_orig)<<3 | (inub-1)<<8
+};
+
 struct LaunchParams {
   DevModel m;
   DevTallies t;
@@ -90,6 +105,9 @@ struct LaunchParams {
   double nphot_diff;            // nphot of emit_common's surface heating (ns of this shard)
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter
+  PeelJob *jobs;                // peel-off job queue (nullptr: peel inline)
+  unsigned long long *njobs;    // jobs queued
+  int64_t job_cap;
   mcrt_packet_log *log;
   int64_t nlog;
   int32_t *err;                 // device error flags

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "mcrt_sched.cuh"
+#include "mcrt_peel.cuh"
 
 namespace mcrt {
 
@@ -14,6 +15,17 @@ cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t 
 cudaError_t launch_transport_sched_fp64(const LaunchParams& p, int grid, cudaStream_t s) {
   transport_sched<<<grid, kBlock, 0, s>>>(p);
   return cudaGetLastError();
+}
+
+cudaError_t launch_peel_fp64(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s) {
+  peel_sched<<<grid, kBlock, 0, s>>>(p, next_item);
+  return cudaGetLastError();
+}
+
+int peel_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, peel_sched, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
 }
 
 int transport_sched_fp64_blocks_per_sm() {

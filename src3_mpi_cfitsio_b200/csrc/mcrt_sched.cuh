@@ -55,13 +55,13 @@ struct Lane {
   double xpold, ypold, zpold;
   int peel_ctx, peelid, peel_idust2;
   double peel_si, coslp, sinlp;
-  unsigned long long c_pkt, c_int, c_sca, c_geo, c_kil, c_exit, c_star;
+  unsigned long long c_pkt, c_int, c_sca, c_geo, c_kil, c_exit, c_star, c_jobs;
   int64_t ray_steps;
 
   __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase) : pk(m, t, sbase) {
     ev = EV_FETCH;
     status = 0;
-    c_pkt = c_int = c_sca = c_geo = c_kil = c_exit = c_star = 0;
+    c_pkt = c_int = c_sca = c_geo = c_kil = c_exit = c_star = c_jobs = 0;
   }
 
   __device__ __forceinline__ void ray_from_packet(bool peel) {
@@ -157,6 +157,30 @@ struct Lane {
       if (R.r == m.nrg) { ev = EV_PEEL_BIN; return; }
       if (R.r == 0) { ev = EV_PEEL_NEXT; return; }
     }
+  }
+
+  // Queue a peel-off job for the peel kernel; false if the queue is full
+  // (the lane then walks the peel-offs itself).
+  __device__ bool push_job(const LaunchParams& P, int ctx, int idust2) {
+    const DevModel& m = pk.m;
+    if (!P.jobs || m.nslot > kJobSlots) return false;
+    const unsigned long long j = atomicAdd(P.njobs, 1ull);
+    if ((int64_t)j >= P.job_cap) return false;
+    PeelJob J;
+    J.x = pk.xp; J.y = pk.yp; J.z = pk.zp; J.rs = pk.rsq; J.rt = pk.rtot;
+    J.si = pk.sip; J.sq = pk.sqp; J.su = pk.sup; J.sv = pk.svp;
+    if (ctx == PC_DIRECT) { J.d0 = pk.cosb; J.d1 = pk.sinb; J.d2 = coslp; J.d3 = sinlp; J.d4 = 0.0; }
+    else { J.d0 = pk.cost; J.d1 = pk.sint; J.d2 = pk.cosp; J.d3 = pk.sinp; J.d4 = pk.phi; }
+    for (int s = 0; s < kJobSlots; ++s) J.kapd[s] = s < m.nslot ? pk.sp.kapd(s) : 0.0;
+    const int ss = (pk.iflag == 1) ? pk.idust2slot(idust2) : 0;
+    J.g = pk.sp.g(ss);
+    J.pl = pk.sp.pl(ss);
+    J.r = pk.ir; J.t = pk.it; J.p = pk.ip;
+    J.bits = (pk.on_wall ? 1u : 0u) | ((pk.iflag == 1 ? 1u : 0u) << 1) | ((ctx == PC_DIRECT ? 1u : 0u) << 2) |
+             ((uint32_t)pk.i_orig << 3) | ((uint32_t)(pk.freq_bin(pk.nub) - 1) << 8);
+    P.jobs[j] = J;
+    ++c_jobs;
+    return true;
   }
 
   // ---------------------------------------------------------- peel-off
@@ -283,7 +307,7 @@ struct Lane {
           pk.on_wall = true;
           pk.it = locate(m.thetarr, m.ntg, acos(pk.cosb));
           pk.ip = locate(m.phiarr, m.npg, pk.lp);
-          if (P.ipeel == 1 && !m.partial_peeloff) {
+          if (P.ipeel == 1 && !m.partial_peeloff && !push_job(P, PC_DIRECT, 0)) {
             peel_ctx = PC_DIRECT;
             peelid = 0;
             peel_idust2 = 0;
@@ -358,7 +382,7 @@ struct Lane {
             ++iint;
             ++pk.nscat;
             slot_s = slot;
-            if (P.ipeel == 1) {
+            if (P.ipeel == 1 && !push_job(P, PC_SCATTER, idust2)) {
               peel_ctx = PC_SCATTER; peelid = 0; peel_idust2 = idust2;
               ev = EV_PEEL_NEXT;
             } else {
@@ -390,7 +414,7 @@ struct Lane {
             pk.iflag = 0;
             pk.opacset(pk.nub, KAPD_PROPAGATE);
             pk.ifuv = Packet::is_fuv(pk.nub) ? m.ifuv_ori : 0.0;
-            if (P.ipeel == 1 && !m.partial_peeloff) {
+            if (P.ipeel == 1 && !m.partial_peeloff && !push_job(P, PC_ABSORB, idust2)) {
               peel_ctx = PC_ABSORB; peelid = 0; peel_idust2 = idust2;
               ev = EV_PEEL_NEXT;
             } else {
@@ -488,7 +512,10 @@ struct Lane {
 
 // Warp-scheduled persistent kernel.  All 32 lanes of a warp stay in the loop
 // until every lane is out of packets, so the warp votes are well defined.
-__global__ void __launch_bounds__(kBlock) transport_sched(LaunchParams P) {
+#ifndef MCRT_SCHED_MIN_BLOCKS
+#define MCRT_SCHED_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(kBlock, MCRT_SCHED_MIN_BLOCKS) transport_sched(LaunchParams P) {
   __shared__ double spec[5 * kMaxSlot * kBlock];
   Lane L(P.m, P.t, spec);
   const unsigned FULL = 0xffffffffu;
@@ -505,9 +532,9 @@ __global__ void __launch_bounds__(kBlock) transport_sched(LaunchParams P) {
       L.step(P);
     }
   }
-  unsigned long long v[12] = {L.c_pkt, L.pk.c_cross, L.c_int, L.c_sca, L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin,
-                              L.c_geo, L.pk.c_reset, L.c_kil, L.c_exit, L.c_star};
-  for (int i = 0; i < 12; ++i) {
+  unsigned long long v[14] = {L.c_pkt, L.pk.c_cross, L.c_int, L.c_sca, L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin,
+                              L.c_geo, L.pk.c_reset, L.c_kil, L.c_exit, L.c_star, 0ull, L.c_jobs};
+  for (int i = 0; i < 14; ++i) {
     unsigned long long x = warp_sum(v[i]);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(P.t.cnt + i, x);
   }

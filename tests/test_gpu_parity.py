@@ -191,3 +191,25 @@ def test_schedules_agree_bitwise(warm_small, batch):
     a, b = logs
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_peel_queue_matches_inline_peel_offs(warm_small):
+    """Queued peel-offs (peel-off kernel) give the tallies of peel-offs walked
+    inline by the packet's own thread, up to FP64 summation order."""
+    n = 4000
+    tals = []
+    for sched in ("packet", "warp"):
+        eng = _engine(warm_small)
+        eng.set_schedule(sched, 16)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        tals.append(eng.download())
+        eng.close()
+    a, b = tals
+    ca, cb = a.counters(), b.counters()
+    assert cb["peel_jobs"] > 0 and ca["peel_jobs"] == 0
+    for k in ("peels", "peel_cross", "peel_binned", "packets", "crossings", "interactions"):
+        assert ca[k] == cb[k], k
+    assert cb["peel_resets"] == 0
+    for k in ("ti", "tq", "tu", "numt", "image_m_i", "image_m_q", "si", "nums"):
+        assert np.allclose(a[k], b[k], rtol=1e-5, atol=1e-6 * max(1e-30, float(np.abs(a[k]).max()))), k
