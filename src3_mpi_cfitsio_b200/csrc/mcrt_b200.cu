@@ -28,6 +28,8 @@ cudaError_t launch_transport_sched_fp64(const LaunchParams& p, int grid, cudaStr
 int transport_sched_fp64_blocks_per_sm();
 cudaError_t launch_peel_fp64(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s);
 int peel_fp64_blocks_per_sm();
+cudaError_t launch_peel_mixed(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s);
+int peel_mixed_blocks_per_sm();
 int transport_mixed_blocks_per_sm();
 }  // namespace mcrt
 
@@ -633,9 +635,10 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   P.err = ctx->d_err;
   const int64_t npk = hi - lo + 1;
   P.event_batch = ctx->event_batch;
-  const bool warp = ctx->schedule == MCRT_SCHED_WARP;
+  const bool mixed = ctx->precision == MCRT_PREC_MIXED;
+  const bool warp = ctx->schedule == MCRT_SCHED_WARP || mixed;   // the mixed build is warp-scheduled only
   // peel-offs go through the job queue and the peel-off kernel
-  const bool queue = P.ipeel && warp && ctx->precision == MCRT_PREC_FP64 && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
+  const bool queue = P.ipeel && warp && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
   if (queue && !ctx->d_jobs) {
     ctx->job_cap = 8 * ctx->chunk_packets;
     int rc = dalloc(ctx, &ctx->d_jobs, (size_t)ctx->job_cap);
@@ -647,7 +650,7 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   int per_sm = ctx->precision == MCRT_PREC_FP64 ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
                                                 : transport_mixed_blocks_per_sm();
   const int full_grid = ctx->nsm * std::max(per_sm, 1);
-  const int peel_grid = ctx->nsm * peel_fp64_blocks_per_sm();
+  const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   const int64_t chunk = queue ? ctx->chunk_packets : npk;
   for (int64_t c_lo = lo; c_lo <= hi; c_lo += chunk) {
@@ -662,7 +665,8 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
                         : launch_transport_mixed(P, grid, ctx->stream);
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
     if (queue) {
-      e = launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
+      e = mixed ? launch_peel_mixed(P, ctx->d_next + 2, peel_grid, ctx->stream)
+                : launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
       if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
     }
   }

@@ -1,12 +1,49 @@
-// mcrt_mixed.cu -- mixed-precision transport build (FP32 walk and scattering,
-// FP64 radial roots, optical-depth sums and tallies).
+// mcrt_mixed.cu -- mixed-precision transport build.
+//
+// The transport and peel-off kernels of mcrt_sched.cuh / mcrt_peel.cuh
+// compiled with MCRT_MIXED: scattering (rejection sampling, frame rotations,
+// the peel-off phase matrix) runs in FP32.  The walk's geometry stays FP64,
+// because testgrid resolves 1e-4 of a cell and the rim and equatorial cells
+// are 6.5e-4 wide in cos(theta), beyond FP32 positions; the mixed walk drops
+// the divisions instead (grid tests as products, one reciprocal per face
+// quadratic, FMA contraction on).  Positions, face roots, the cumulative
+// optical depth and its comparison with the sampled tau, opacities and all
+// tallies are FP64.  The device code is
+// compiled into its own namespace so that it can coexist with the FP64
+// build's kernels; the launch parameters have the same layout.
 #include <cuda_runtime.h>
 
-#include "mcrt_device.cuh"
+#define MCRT_MIXED 1
+#define mcrt mcrt_mixed
+#include "mcrt_sched.cuh"
+#include "mcrt_peel.cuh"
+#undef mcrt
 
 namespace mcrt {
+struct LaunchParams;
 
-cudaError_t launch_transport_mixed(const LaunchParams&, int, cudaStream_t) { return cudaErrorNotSupported; }
-int transport_mixed_blocks_per_sm() { return 1; }
+cudaError_t launch_transport_mixed(const LaunchParams& p, int grid, cudaStream_t s) {
+  const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);
+  mcrt_mixed::transport_sched<<<grid, mcrt_mixed::kBlock, 0, s>>>(q);
+  return cudaGetLastError();
+}
+
+int transport_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::transport_sched, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+cudaError_t launch_peel_mixed(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s) {
+  const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);
+  mcrt_mixed::peel_sched<<<grid, mcrt_mixed::kBlock, 0, s>>>(q, next_item);
+  return cudaGetLastError();
+}
+
+int peel_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::peel_sched, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
 
 }  // namespace mcrt

@@ -94,7 +94,9 @@ struct PeelLane {
     R.z = R.z + dt * R.vz;
     R.onw = true;
     R.rs = R.x * R.x + R.y * R.y + R.z * R.z;
-    R.rt = sqrt(R.rs);
+#ifndef MCRT_MIXED
+    R.rt = sqrt(R.rs);            // the mixed testgrid forms rt itself
+#endif
     ++pk.c_pcross;
     if (R.r == m.nrg) { state = 1; return; }
     if (R.r == 0) { state = 2; return; }

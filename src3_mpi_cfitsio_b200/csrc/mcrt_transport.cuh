@@ -374,6 +374,84 @@ struct Packet {
   // testgrid.f90:1-128.  For npg == 2 the phi checks can never fire
   // (phi in [0,2pi) against phiarr = [0,2pi]), so atan2 is only evaluated
   // when a re-location needs it.
+#ifdef MCRT_MIXED
+  // Mixed build: the same FP64 tests as testgrid.f90 written without
+  // divisions (a fraction compared with a bound becomes a product with the
+  // cell width).  FP32 positions cannot be used here: the tests resolve 1e-4
+  // of a cell, and the rim and equatorial cells are 6.5e-4 wide in cos(theta).
+  __device__ void testgrid(double& x, double& y, double& z, double& rs, double& rt, int& r, int& t, int& p, bool& onw) {
+    const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
+    const double tol = 1.0e-4;
+    const double* r2 = m.r2arr;
+    const double* ca = m.costarr;
+    const double* pa = m.phiarr;
+    // num/den < v and num/den > v without the division
+    auto lt = [](double num, double den, double v) { return den > 0.0 ? num < v * den : num > v * den; };
+    auto gt = [](double num, double den, double v) { return den > 0.0 ? num > v * den : num < v * den; };
+    rt = sqrt(rs);
+    const double irt = 1.0 / rt;
+    double cb = chk(z * irt);
+    const bool need_phi = npg > 2;
+    double ph = 0.0;
+    if (need_phi) {
+      ph = atan2(y, x);
+      if (ph < 0.0) ph = ph + R2P;
+    }
+    bool reset = false;
+    const double r20 = __ldg(r2), r21 = __ldg(r2 + 1), r2a = __ldg(r2 + nrg - 2), r2b = __ldg(r2 + nrg - 1);
+    if (lt(rs - r20, r21 - r20, -tol) || gt(rs - r2a, r2b - r2a, 1.0 + tol)) {
+      const double third = (double)(1.0f / 3.0f);
+      const double r1 = m.rarr[0], rn = m.rarr[nrg - 1];
+      rt = pow(ran() * (pow(rn, 3.0) - pow(r1, 3.0)) + pow(r1, 3.0), third);
+      reset = true;
+    }
+    const double c0 = __ldg(ca), c1 = __ldg(ca + 1), ca2 = __ldg(ca + ntg - 2), cb2 = __ldg(ca + ntg - 1);
+    if (lt(cb - c0, c1 - c0, -tol) || gt(cb - ca2, cb2 - ca2, 1.0 + tol)) {
+      cb = ran() * (cb2 - c0) + c0;
+      reset = true;
+    }
+    if (need_phi && (lt(ph - pa[0], pa[1] - pa[0], -tol) || gt(ph - pa[npg - 2], pa[npg - 1] - pa[npg - 2], 1.0 + tol))) {
+      ph = ran() * (pa[npg - 1] - pa[0]) + pa[0];
+      reset = true;
+    }
+    if (reset) {
+      if (!need_phi) {
+        ph = atan2(y, x);
+        if (ph < 0.0) ph = ph + R2P;
+      }
+      double sq = sqrt(1.0 - cb * cb);
+      x = rt * sq * cos(ph);
+      y = rt * sq * sin(ph);
+      z = rt * cb;
+      rs = rt * rt;
+      onw = false;
+      ++c_reset;
+    }
+    if (r < 1 || r > nrg) r = locate(r2, nrg, rs);
+    if (t < 1 || t > ntg) t = locate(ca, ntg, cb);
+    if (p < 1 || p > npg) {
+      if (!need_phi) { ph = atan2(y, x); if (ph < 0.0) ph = ph + R2P; }
+      p = locate(pa, npg, ph);
+    }
+    const double ra = __ldg(r2 + r - 1), rb = __ldg(r2 + r);
+    const double ta = __ldg(ca + t - 1), tb = __ldg(ca + t);
+    bool phierr = false;
+    if (need_phi) {
+      if (lt(ph - pa[p - 1], pa[p] - pa[p - 1], -tol) || gt(ph - pa[p - 1], pa[p] - pa[p - 1], 1.0 + tol)) {
+        double d1 = ph - pa[p - 1];
+        if (d1 > PI) d1 -= R2P;
+        if (d1 < -PI) d1 += R2P;
+        double d2 = ph - pa[p];
+        if (d2 > PI) d2 -= R2P;
+        if (d2 < -PI) d2 += R2P;
+        phierr = fabs(d1) > tol && fabs(d2) > tol;
+      }
+    }
+    if (lt(rs - ra, rb - ra, -tol) || gt(rs - ra, rb - ra, 1.0 + tol)) r = locate(r2, nrg, rs);
+    if (lt(cb - ta, tb - ta, -tol) || gt(cb - ta, tb - ta, 1.0 + tol)) t = locate(ca, ntg, cb);
+    if (phierr) p = locate(pa, npg, ph);
+  }
+#else
   __device__ void testgrid(double& x, double& y, double& z, double& rs, double& rt, int& r, int& t, int& p, bool& onw) {
     const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
     const double tol = 1.0e-4;
@@ -442,6 +520,7 @@ struct Packet {
     if (tfrac < -tol || tfrac > 1.0 + tol) t = locate(ca, ntg, cb);
     if (phierr) p = locate(pa, npg, ph);
   }
+#endif
 
   // radface / thetaface / phiface (radface.f90, thetaface.f90, phiface.f90)
   __device__ __forceinline__ void faces(Walls& w, double vx, double vy, double vz, double x, double y, double z,
@@ -462,6 +541,59 @@ struct Packet {
       w.insert((-bb + descr) * 0.5, 2);
       w.insert((-bb - descr) * 0.5, 2);
     }
+#ifdef MCRT_MIXED
+    // Mixed build: thetaface/phiface in FP64 (see testgrid) with one
+    // reciprocal per quadratic instead of two divisions.
+    if (m.ntg > 2) {
+      const double t1 = __ldg(m.tan2arr + t - 1), t2 = __ldg(m.tan2arr + t);
+      const double tmp1 = x * vx + y * vy, tmp2 = vx * vx + vy * vy, tmp3 = x * x + y * y;
+      double ta, tb;
+      int i1, i2;
+      if (t2 < t1) { ta = t2; tb = t1; i1 = 4; i2 = 3; }
+      else { ta = t1; tb = t2; i1 = 3; i2 = 4; }
+      if (ta < 0.0) {
+        if (vz != 0.0) w.insert(-z / vz, i1);
+      } else {
+        const double b2 = 2.0 * (tmp1 - ta * vz * z);
+        const double aa = tmp2 - ta * vz * vz;
+        const double c2 = tmp3 - z * z * ta;
+        if (fabs(aa) > 1.0e-10) {
+          double d = b2 * b2 - 4.0 * aa * c2;
+          if (d > 0.0 && ta != 0.0) {
+            d = sqrt(d);
+            const double ia = 0.5 / aa;
+            w.insert((-b2 + d) * ia, i1);
+            w.insert((-b2 - d) * ia, i1);
+          }
+        } else if (fabs(b2) > 1.0e-10) {
+          w.insert(-c2 / b2, i1);
+        }
+      }
+      const double b2 = 2.0 * (tmp1 - tb * vz * z);
+      const double aa = tmp2 - tb * vz * vz;
+      const double c2 = tmp3 - z * z * tb;
+      if (fabs(aa) > 1.0e-10) {
+        double d = b2 * b2 - 4.0 * aa * c2;
+        if (d > 0.0 && tb != 0.0) {
+          d = sqrt(d);
+          const double ia = 0.5 / aa;
+          w.insert((-b2 + d) * ia, i2);
+          w.insert((-b2 - d) * ia, i2);
+        }
+      } else if (fabs(b2) > 1.0e-10) {
+        w.insert(-c2 / b2, i2);
+      }
+    }
+    if (m.npg > 2 && m.ntg > 2) {
+      const double A1 = __ldg(m.aarr + p - 1), B1 = __ldg(m.barr + p - 1);
+      const double A2 = __ldg(m.aarr + p), B2 = __ldg(m.barr + p);
+      const double d1 = (A1 * vx + B1 * vy);
+      if (d1 != 0.0) w.insert(-(A1 * x + B1 * y) / d1, 5);
+      const double d2 = (A2 * vx + B2 * vy);
+      if (d2 != 0.0) w.insert(-(A2 * x + B2 * y) / d2, 6);
+    }
+  }
+#else
     if (m.ntg > 2) {
       const double t1 = __ldg(m.tan2arr + t - 1), t2 = __ldg(m.tan2arr + t);
       const double tmp1 = x * vx + y * vy, tmp2 = vx * vx + vy * vy, tmp3 = x * x + y * y;
@@ -509,6 +641,7 @@ struct Packet {
       if (d2 != 0.0) w.insert(-(A2 * x + B2 * y + 0.0 * z + 0.0) / d2, 6);
     }
   }
+#endif
 
   __device__ __forceinline__ int64_t cidx(int r, int t, int p) const {
     return (int64_t)(r - 1) + (int64_t)m.nrg * ((t - 1) + (int64_t)m.ntg * (p - 1));
@@ -619,6 +752,147 @@ struct Packet {
   // (stokes.f90:183-216 and :284-317; stokespeel.f90:193-210, :293-309).
   struct Mat { double a11, a12, a13, a21, a22, a23, a31, a32, a33, a43, a44; };
 
+#ifdef MCRT_MIXED
+  // FP32 scattering: the same rejection sampling and rotations in float
+  __device__ __forceinline__ void dustmat_f(float bmu, float cosb2, int s, float& p1, float& p2, float& p3) const {
+    const float gg = (float)sp.g(s);
+    const float g2 = gg * gg;
+    const float temp = (g2 + 1.0f) - (2.0f * gg) * bmu;
+    p1 = 1.5f * (1.0f - g2) / (2.0f + g2) * (1.0f + cosb2) / (temp * sqrtf(temp));
+    p2 = -(float)sp.pl(s) * p1 * (1.0f - cosb2) / (1.0f + cosb2);
+    p3 = p1 * 2.0f * bmu / (1.0f + cosb2);
+  }
+
+  __device__ void stokes(int s) {
+    const float PIf = 3.14159265358979f, R2Pf = 6.28318530717959f;
+    const float costp = (float)cost, sintp = (float)sint, phip = (float)phi;
+    const float fsi = (float)sip, fsq = (float)sqp, fsu = (float)sup, fsv = (float)svp;
+    const float gg = (float)sp.g(s);
+    const float g2 = gg * gg;
+    float peak;
+    {
+      const float temp = (gg > 0.0f) ? (g2 + 1.0f) - (2.0f * gg) : (g2 + 1.0f) + (2.0f * gg);
+      peak = 1.5f * (1.0f - g2) / (2.0f + g2) * 2.0f / temp / sqrtf(temp) * 1.01f;
+    }
+    float bmu, cosb2, sinbt, p1, p2, p3, a, ci, si_, c2i, s2i;
+    bool upper;
+    for (;;) {
+      bmu = 1.0f - 2.0f * (float)ran();
+      cosb2 = bmu * bmu;
+      if (m.idust == 0) {
+        p1 = 0.75f * (1.0f + cosb2); p2 = 0.75f * (cosb2 - 1.0f); p3 = 0.75f * (2.0f * bmu);
+        peak = 1.501f;
+      } else {
+        dustmat_f(bmu, cosb2, s, p1, p2, p3);
+      }
+      sinbt = sqrtf(fmaxf(0.0f, 1.0f - cosb2));
+      const float ri1 = R2Pf * (float)ran();
+      upper = ri1 > PIf;
+      const float ang = upper ? R2Pf - ri1 : ri1;
+      sincosf(ang, &si_, &ci);
+      s2i = 2.0f * si_ * ci;
+      c2i = 2.0f * ci * ci - 1.0f;
+      const float a12 = p2 * c2i;
+      const float a13 = upper ? p2 * s2i : -p2 * s2i;
+      const float rprob = (p1 * fsi + a12 * fsq + a13 * fsu) / fsi;
+      if (rprob > peak) peak = rprob;
+      if (peak * (float)ran() > rprob) continue;
+      a = rprob;
+      break;
+    }
+    if (bmu == 1.0f) return;
+    float sini2, cosi2 = 0.0f, ncost, nsint;
+    if (bmu == -1.0f) {
+      si_ = 1.0f; sini2 = 1.0f; ci = 0.0f; cosi2 = 0.0f;
+      ncost = -costp; nsint = sintp;
+    } else {
+      ncost = costp * bmu + sintp * sinbt * ci;
+      if (fabsf(ncost) < 1.0f) {
+        nsint = sqrtf(1.0f - ncost * ncost);
+        sini2 = si_ * sintp / nsint;
+        const float bott = nsint * sinbt;
+        cosi2 = costp / bott - ncost * bmu / bott;
+      } else {
+        nsint = 0.0f; sini2 = 0.0f;
+        if (ncost >= 1.0f) cosi2 = -1.0f;
+        if (ncost <= -1.0f) cosi2 = 1.0f;
+      }
+    }
+    float cosdph = -cosi2 * ci + sini2 * si_ * bmu;
+    cosdph = fminf(1.0f, fmaxf(-1.0f, cosdph));
+    float nphi = upper ? phip + acosf(cosdph) : phip - acosf(cosdph);
+    if (nphi > R2Pf) nphi = nphi - R2Pf;
+    if (nphi < 0.0f) nphi = nphi + R2Pf;
+    const float sin2i2 = 2.0f * sini2 * cosi2, cos2i2 = 2.0f * cosi2 * cosi2 - 1.0f;
+    const float sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const float sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    const float a11 = p1, a12 = p2 * c2i, a21 = p2 * cos2i2, a22 = p1 * cos2 - p3 * sin2;
+    const float a33 = -p1 * sin2 + p3 * cos2, a44 = p3;
+    float a13, a23, a31, a32;
+    if (upper) {
+      a13 = p2 * s2i; a23 = p1 * cos2sin1 + p3 * sin2cos1; a31 = -p2 * sin2i2; a32 = -p1 * sin2cos1 - p3 * cos2sin1;
+    } else {
+      a13 = -p2 * s2i; a23 = -p1 * cos2sin1 - p3 * sin2cos1; a31 = p2 * sin2i2; a32 = p1 * sin2cos1 + p3 * cos2sin1;
+    }
+    const float ia = 1.0f / a;
+    sip = (double)((a11 * fsi + a12 * fsq + a13 * fsu) * ia);
+    sqp = (double)((a21 * fsi + a22 * fsq + a23 * fsu) * ia);
+    sup = (double)((a31 * fsi + a32 * fsq + a33 * fsu) * ia);
+    svp = (double)((a44 * fsv) * ia);
+    // the walk's face roots assume |u| = 1 to FP64 precision: rebuild the
+    // direction from cos(theta) and phi in FP64
+    cost = (double)ncost;
+    sint = (nsint == 0.0f) ? 0.0 : sqrt(fmax(0.0, 1.0 - cost * cost));
+    phi = (double)nphi;
+    sincos(phi, &sinp, &cosp);
+    (void)nsint;
+  }
+
+  __device__ void stokespeel(double& qi, double& qq, double& qu, double& qv, double cst, double snt, double ri1d,
+                             double bmud, double costpd, double sintpd, int s) const {
+    const float PIf = 3.14159265358979f, R2Pf = 6.28318530717959f;
+    const float bmu = (float)bmud, cstf = (float)cst, sntf = (float)snt, costp = (float)costpd, sintp = (float)sintpd;
+    float p1, p2, p3;
+    const float cosb2 = bmu * bmu;
+    if (m.idust == 0) { p1 = 0.75f * (1.0f + cosb2); p2 = 0.75f * (cosb2 - 1.0f); p3 = 0.75f * (2.0f * bmu); }
+    else dustmat_f(bmu, cosb2, s, p1, p2, p3);
+    const float sinbt = sqrtf(fmaxf(0.0f, 1.0f - cosb2));
+    const float ri1 = (float)ri1d;
+    const bool upper = ri1 > PIf;
+    const float ang = upper ? R2Pf - ri1 : ri1;
+    float ci, si_;
+    sincosf(ang, &si_, &ci);
+    const float s2i = 2.0f * si_ * ci, c2i = 2.0f * ci * ci - 1.0f;
+    if (bmu == 1.0f) return;
+    float sini2, cosi2 = 0.0f;
+    if (bmu == -1.0f) { si_ = 1.0f; sini2 = 1.0f; ci = 0.0f; cosi2 = 0.0f; }
+    else if (fabsf(cstf) < 1.0f) {
+      sini2 = si_ * sintp / sntf;
+      const float bott = sntf * sinbt;
+      cosi2 = costp / bott - cstf * bmu / bott;
+    } else {
+      sini2 = 0.0f;
+      if (cstf >= 1.0f) cosi2 = -1.0f;
+      if (cstf <= -1.0f) cosi2 = 1.0f;
+    }
+    const float sin2i2 = 2.0f * sini2 * cosi2, cos2i2 = 2.0f * cosi2 * cosi2 - 1.0f;
+    const float sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const float sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    const float a11 = p1, a12 = p2 * c2i, a21 = p2 * cos2i2, a22 = p1 * cos2 - p3 * sin2;
+    const float a33 = -p1 * sin2 + p3 * cos2, a44 = p3;
+    float a13, a23, a31, a32;
+    if (upper) {
+      a13 = p2 * s2i; a23 = p1 * cos2sin1 + p3 * sin2cos1; a31 = -p2 * sin2i2; a32 = -p1 * sin2cos1 - p3 * cos2sin1;
+    } else {
+      a13 = -p2 * s2i; a23 = -p1 * cos2sin1 - p3 * sin2cos1; a31 = p2 * sin2i2; a32 = p1 * sin2cos1 + p3 * cos2sin1;
+    }
+    const float fi = (float)qi, fq = (float)qq, fu = (float)qu, fv = (float)qv;
+    qi = (double)(a11 * fi + a12 * fq + a13 * fu);
+    qq = (double)(a21 * fi + a22 * fq + a23 * fu);
+    qu = (double)(a31 * fi + a32 * fq + a33 * fu);
+    qv = (double)(a44 * fv);
+  }
+#else
   __device__ void stokes(int s) {                  // stokes.f90:1-340 (p4 = 0)
     const double costp = cost, sintp = sint, phip = phi;
     const double gg = sp.g(s);
@@ -751,6 +1025,7 @@ struct Packet {
     const double nv = (a42 * qq + a43 * qu + a44 * qv);
     qi = ni; qq = nq; qu = nu_; qv = nv;
   }
+#endif
 
   __device__ __forceinline__ int freq_bin(double nu) const {
     const double v = (double)m.nfreq * log(nu / m.numin) / m.lnurat;

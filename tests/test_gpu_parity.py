@@ -213,3 +213,28 @@ def test_peel_queue_matches_inline_peel_offs(warm_small):
     assert cb["peel_resets"] == 0
     for k in ("ti", "tq", "tu", "numt", "image_m_i", "image_m_q", "si", "nums"):
         assert np.allclose(a[k], b[k], rtol=1e-5, atol=1e-6 * max(1e-30, float(np.abs(a[k]).max()))), k
+
+
+def test_mixed_precision_agrees_with_fp64(oracle_mod):
+    """The mixed build (FP32 scattering, division-free FP64 walk) follows the
+    same random streams, so its ensemble tallies agree with the FP64 build
+    far inside the Monte Carlo error; the walk must not lose packets."""
+    m = model.with_diffusion(model.warm(model.small_2d()))
+    n = 40000
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng = _engine(m, precision=prec)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        out[prec] = eng.download()
+        eng.close()
+    a, b = out["fp64"], out["mixed"]
+    ca, cb = a.counters(), b.counters()
+    assert cb["geom_fail"] == 0 and cb["packets"] == n
+    assert abs(cb["crossings"] - ca["crossings"]) <= 0.01 * ca["crossings"]
+    assert abs(cb["interactions"] - ca["interactions"]) <= 0.02 * ca["interactions"] + 50
+    for k in ("nums", "si", "numt", "ti", "image_m_i"):
+        x, y = a[k].astype(np.float64), b[k].astype(np.float64)
+        assert abs(y.sum() - x.sum()) <= 0.01 * abs(x.sum()) + 1e-12, k
+        assert np.abs(y - x).sum() <= 0.05 * np.abs(x).sum() + 1e-12, k
+    assert np.abs(b["dtauabs"] - a["dtauabs"]).sum() <= 0.03 * np.abs(a["dtauabs"]).sum()
