@@ -113,10 +113,23 @@ def algorithmic_bytes(c: dict) -> float:
             16.0 * (c["exited"] + c["peel_binned"]))
 
 
+def _errors(a, b):
+    """Relative L1 distance of tally b from tally a (per-bin SED, images)."""
+    import numpy as np
+    out = {}
+    for k in ("si", "ti", "image_m_i", "image_m_q"):
+        if k in a.arrays and k in b.arrays:
+            x = a[k].astype(np.float64)
+            y = b[k].astype(np.float64)
+            den = np.abs(x).sum()
+            if den > 0:
+                out[k] = float(np.abs(y - x).sum() / den)
+    return out
+
+
 def run_ours(args, rank, world):
     import numpy as np
 
-    from src3_mpi_cfitsio_b200 import abi
     from src3_mpi_cfitsio_b200.engine import Engine
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -130,27 +143,26 @@ def run_ours(args, rank, world):
         import torch
         import torch.distributed as tdist
 
-    def reduce_cells(tal):
+    def allreduce(arr, op="sum"):
         if not dist:
-            return tal
-        for k in ("dtauabs",):
-            t = torch.from_numpy(tal[k]).cuda(dev)
-            tdist.all_reduce(t)
-            tal.arrays[k][:] = t.cpu().numpy()
-        return tal
+            return arr
+        t = torch.from_numpy(np.ascontiguousarray(arr)).cuda(dev)
+        tdist.all_reduce(t, op=tdist.ReduceOp.SUM if op == "sum" else tdist.ReduceOp.MAX)
+        return t.cpu().numpy()
 
-    def step(it):
-        eng.reset_tallies()
-        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
-        eng.update_temperature(np_total, it)
+    def step(it, e, precision=None):
+        e.reset_tallies()
+        e.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+        kms = e.kernel_ms()
+        e.update_temperature(np_total, it)
+        return kms
 
-    # warm-up iterations (also converge the temperature a little)
+    # warm-up Lucy iterations (they also bring the temperature toward convergence)
     for w in range(args.warmup):
-        step(w + 1)
+        step(w + 1, eng)
     eng.synchronize()
     if dist:
         tdist.barrier()
-    counters = {}
     kernel_ms = []
     with Clocks(dev) as clk:
         eng.flush_l2()
@@ -166,75 +178,111 @@ def run_ours(args, rank, world):
         eng.mark(1)
         eng.synchronize()
         ms = eng.elapsed_ms(0, 1)
-    tal = eng.download(images=False)
-    counters = tal.counters()
+    tal_last = eng.download(images=bool(args.ipeel))
+    counters = tal_last.counters()
     flush_ms = 0.0
     if args.steps > 1:
         eng.mark(2)
         eng.flush_l2()
         eng.mark(3)
         flush_ms = eng.elapsed_ms(2, 3) * (args.steps - 1)
-    ms_steps = ms - flush_ms
-    if dist:
-        t = torch.tensor([ms_steps], dtype=torch.float64, device=f"cuda:{dev}")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        ms_steps = float(t.item())
+    ms_steps = float(allreduce(np.array([ms - flush_ms]), "max")[0])
     value = np_total * args.steps / (ms_steps / 1e3)
 
     # ---- end-to-end through the public API with host buffers
-    e2e_steps = max(1, min(args.steps, 3))
+    h2d = sum(m.grid[n].nbytes for n in ("densarr", "findopac", "diffus", "diffdir", "tdust", "vcell"))
     eng.synchronize()
-    h2d = 0
-    for name in ("densarr", "findopac", "diffus", "tdust", "vcell"):
-        h2d += m.grid[name].nbytes
     t0 = time.perf_counter()
     eng.mark(4)
-    for s in range(e2e_steps):
-        it = args.warmup + args.steps + s + 1
-        eng.upload_grid()
-        eng.reset_tallies()
-        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
-        tl = eng.download(images=bool(args.ipeel))
-        reduce_cells(tl)
-        td, _, _ = eng.update_temperature(np_total, it)
+    it = args.warmup + args.steps + 1
+    eng.upload_grid()
+    eng.reset_tallies()
+    eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+    tl = eng.download(images=bool(args.ipeel))
+    tl.arrays["dtauabs"][:] = allreduce(tl["dtauabs"])
+    td, _, _ = eng.update_temperature(np_total, it)
     eng.mark(5)
     eng.synchronize()
-    e2e_ms = eng.elapsed_ms(4, 5)
-    wall_e2e = time.perf_counter() - t0
-    d2h = sum(a.nbytes for k, a in tl.arrays.items()) + td.nbytes
-    e2e_ms = max(e2e_ms, wall_e2e * 1e3)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{dev}")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = np_total * e2e_steps / (e2e_ms / 1e3)
+    e2e_ms = max(eng.elapsed_ms(4, 5), (time.perf_counter() - t0) * 1e3)
+    d2h = sum(a.nbytes for a in tl.arrays.values()) + td.nbytes
+    e2e_ms = float(allreduce(np.array([e2e_ms]), "max")[0])
+    e2e = np_total / (e2e_ms / 1e3)
 
-    # ---- roofline of the dominant kernel (transport)
-    per_launch = {k: v / args.steps for k, v in counters.items()}   # tallies of the last step only
-    per_launch = counters
+    # ---- roofline of the dominant kernel (transport, last timed step)
     kms = kernel_ms[-1]
-    abytes = algorithmic_bytes(per_launch)
+    abytes = algorithmic_bytes(counters)
     achieved = abytes / (kms / 1e3) / 1e9
     peaks = _peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
+    kname = "transport_sched (mixed)" if args.precision == "mixed" else "transport_sched (fp64)"
+
+    # ---- mixed vs FP64 at equal packet count (same random streams), and the
+    # peeled imaging iteration, each measured once
+    extra = {}
+    if rank == 0 and not args.no_compare:
+        from src3_mpi_cfitsio_b200 import model as mdl
+        other = "fp64" if args.precision == "mixed" else "mixed"
+        itc = it + 1
+        base = mdl.tdust_from_tdave(m, td)
+        res = {}
+        for prec in (args.precision, other):
+            eng.set_precision(prec)
+            m.grid["tdust"] = base.copy()
+            eng.upload_grid()
+            eng.tdave = td.copy()
+            eng.reset_tallies()
+            eng.run(P, iteration=itc, ipeel=0)
+            k0 = eng.kernel_ms()
+            t0_ = eng.download(images=False)
+            tdp, _, _ = eng.update_temperature(P, itc)
+            m.grid["tdust"] = base.copy()
+            eng.upload_grid()
+            eng.reset_tallies()
+            eng.run(args.peel_packets, iteration=itc, ipeel=1)
+            k1 = eng.kernel_ms()
+            t1_ = eng.download(images=True)
+            res[prec] = (k0, k1, t0_, t1_, tdp)
+        eng.set_precision(args.precision)
+        a64 = res["fp64"]
+        amx = res["mixed"]
+        tmask = (a64[4] > 1.0 / 11605.0) & (amx[4] > 1.0 / 11605.0)
+        terr = np.abs(amx[4][tmask] / a64[4][tmask] - 1.0)
+        extra = {
+            "fp64_value": P / (a64[0] / 1e3), "mixed_value": P / (amx[0] / 1e3),
+            "mixed_over_fp64": a64[0] / amx[0],
+            "peeled_iteration": {"packets": args.peel_packets,
+                                 "fp64_packets_per_s": args.peel_packets / (a64[1] / 1e3),
+                                 "mixed_packets_per_s": args.peel_packets / (amx[1] / 1e3),
+                                 "mixed_over_fp64": a64[1] / amx[1]},
+            "mixed_vs_fp64_error": {"sed_l1": _errors(a64[2], amx[2]).get("si"),
+                                    "peeled_sed_l1": _errors(a64[3], amx[3]).get("ti"),
+                                    "image_i_l1": _errors(a64[3], amx[3]).get("image_m_i"),
+                                    "image_q_l1": _errors(a64[3], amx[3]).get("image_m_q"),
+                                    "temperature_median_rel": float(np.median(terr)) if terr.size else None,
+                                    "temperature_p99_rel": float(np.quantile(terr, 0.99)) if terr.size else None,
+                                    "note": "same packets and random streams; differences are Monte Carlo "
+                                            "divergence of histories after FP32 scattering"},
+        }
     out = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=ms_steps / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64" if args.precision == "fp64" else "f32+f64",
         data="synthetic (seeded model generator; no reference parameter files)",
-        config={"workload": "2-D disk+envelope+cavity, nr=100 ntheta=99 nphi=1, Lucy iteration",
+        config={"workload": "2-D disk+envelope+cavity (nr=100, ntheta=99, nphi=1), one Lucy iteration of "
+                            f"{np_total:.0e} packets, diffusion on, peel-off {'on' if args.ipeel else 'off'}",
                 "packets_per_gpu": P, "packets_total": np_total, "peel_off": bool(args.ipeel),
-                "precision": args.precision, "l2": "flushed between steps (256 MiB write)",
+                "precision": args.precision, "schedule": "warp",
+                "l2": "flushed between steps (256 MiB write); working set L2-resident by design",
                 "parallelism": f"packet shards x{world}"},
         e2e={"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                  "frac": achieved / peak, "traffic": None,
+                  "frac": achieved / peak, "traffic": args.traffic_per_packet * np_total if args.traffic_per_packet else None,
                   "peak_source": "measured" if not peaks.get("_fallback") else "fallback",
-                  "kernel": "transport_fp64" if args.precision == "fp64" else "transport_mixed",
-                  "kernel_ms": kms, "algorithmic_bytes": abytes},
-        gpu_launches=4 * args.steps,
+                  "kernel": kname, "kernel_ms": kms, "algorithmic_bytes": abytes},
+        gpu_launches=5 * args.steps,
         clocks=clk.summary(),
         counters=counters,
+        **extra,
     )
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args, m)
@@ -292,11 +340,15 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--packets", type=int, default=1_000_000)
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--packets", type=int, default=100_000_000)
+    ap.add_argument("--peel-packets", type=int, default=10_000_000)
     ap.add_argument("--ipeel", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--traffic-per-packet", type=float, default=None,
+                    help="DRAM bytes per packet of the transport kernel from an ncu capture (profiles/)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

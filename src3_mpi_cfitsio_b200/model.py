@@ -643,3 +643,14 @@ def setdiffus(m: Model, tdave: np.ndarray, iteration: int) -> Model:
 def with_diffusion(m: Model, iteration: int = 2) -> Model:
     """setdiffus on the model's current temperature."""
     return setdiffus(m, m.grid["tdust"].copy(), iteration)
+
+
+def tdust_from_tdave(m: Model, tdave: np.ndarray) -> np.ndarray:
+    """The dust temperature an iteration starts from (gridset_5_model13new.f90:
+    1855-1866): tdave, except 0.1 K in diffusion cells and empty cells."""
+    w = m.w
+    td = np.asarray(tdave, dtype=np.float64).reshape((w.nrg, w.ntg, w.npg), order="F")
+    dif = m.grid["diffus"].reshape((w.nrg, w.ntg, w.npg), order="F") > 0
+    T = np.where(dif, 0.1 / 11605.0, td)
+    T = np.where(m.dens4().sum(axis=-1) > 0, T, 0.1 / 11605.0)
+    return np.asfortranarray(T).ravel(order="F")
