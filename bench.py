@@ -135,6 +135,7 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     m = build_model(args)
     eng = Engine(m, device=dev, precision=args.precision)
+    eng.set_schedule(args.schedule)
     P = args.packets
     np_total = P * world
     lo, hi = rank * P + 1, (rank + 1) * P
@@ -271,7 +272,7 @@ def run_ours(args, rank, world):
         config={"workload": "2-D disk+envelope+cavity (nr=100, ntheta=99, nphi=1), one Lucy iteration of "
                             f"{np_total:.0e} packets, diffusion on, peel-off {'on' if args.ipeel else 'off'}",
                 "packets_per_gpu": P, "packets_total": np_total, "peel_off": bool(args.ipeel),
-                "precision": args.precision, "schedule": "warp",
+                "precision": args.precision, "schedule": args.schedule,
                 "l2": "flushed between steps (256 MiB write); working set L2-resident by design",
                 "parallelism": f"packet shards x{world}"},
         e2e={"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -279,7 +280,10 @@ def run_ours(args, rank, world):
                   "frac": achieved / peak, "traffic": args.traffic_per_packet * np_total if args.traffic_per_packet else None,
                   "peak_source": "measured" if not peaks.get("_fallback") else "fallback",
                   "kernel": kname, "kernel_ms": kms, "algorithmic_bytes": abytes},
-        gpu_launches=5 * args.steps,
+        # kernels of the last timed step (transport launches counted by the
+        # engine, plus tfinal_cells / tfinal_mirror / tfinal_stats /
+        # tdust_from_tdave), times the timed steps
+        gpu_launches=int((counters["launches"] + 4) * args.steps),
         clocks=clk.summary(),
         counters=counters,
         **extra,
@@ -341,6 +345,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--schedule", default="wave", choices=["wave", "warp", "packet"])
     ap.add_argument("--packets", type=int, default=100_000_000)
     ap.add_argument("--peel-packets", type=int, default=10_000_000)
     ap.add_argument("--ipeel", type=int, default=0)

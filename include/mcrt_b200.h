@@ -52,10 +52,12 @@ extern "C" {
 /* ---- scheduling of the transport kernels ---- */
 #define MCRT_SCHED_PACKET  0   /* one thread runs one packet start to finish         */
 #define MCRT_SCHED_WARP    1   /* lanes step rays in lockstep, events run in batches */
+#define MCRT_SCHED_WAVE    2   /* wavefront: walk kernel and event kernel alternate  */
+                               /* over a pool of in-flight packets kept in HBM       */
 
 /* ---- arithmetic of the transport kernels ---- */
 #define MCRT_PREC_FP64   0   /* everything in FP64 (event-for-event with the oracle) */
-#define MCRT_PREC_MIXED  1   /* FP32 walk/scatter, FP64 radial roots, tau sums, tallies */
+#define MCRT_PREC_MIXED  1   /* FP32 scattering; FP64 division-free walk, tau sums, tallies */
 
 /*
  * Run configuration: the scalars of tts_mod/grid_mod/dust_mod/spot_mod that
@@ -176,6 +178,8 @@ typedef struct mcrt_tallies {
 #define MCRT_C_STARHITS     11  /* packets absorbed + re-emitted by the star */
 #define MCRT_C_PEEL_RESETS  12  /* testgrid re-locations inside queued peel-off walks */
 #define MCRT_C_PEEL_JOBS    13  /* peel-off jobs queued for the peel-off kernel */
+#define MCRT_C_WAVES        14  /* walk/event launch pairs of the wavefront schedule */
+#define MCRT_C_LAUNCHES     15  /* kernels launched by mcrt_run_iteration calls */
 #define MCRT_NCOUNTERS      16
 
 /* Per-packet summary used by the parity tests (event-for-event checks). */
@@ -206,11 +210,27 @@ int mcrt_upload_tables(mcrt_ctx *ctx, const mcrt_tables *tab);
 /* Select FP64 or mixed-precision transport (MCRT_PREC_*). */
 int mcrt_set_precision(mcrt_ctx *ctx, int32_t mode);
 
-/* Select the kernel schedule (MCRT_SCHED_*; default MCRT_SCHED_WARP) and,
- * for the warp schedule, how many lanes of a warp must wait for an event
- * before the warp stops stepping rays to run them (1..32, default 16).
- * Results do not depend on either choice. */
+/* Select the kernel schedule (MCRT_SCHED_*; default MCRT_SCHED_WAVE) and
+ * its batch size (1..32): for the warp schedule, how many lanes of a warp
+ * must wait for an event before the warp stops stepping rays to run them
+ * (default 16); for the wavefront schedule, how many lanes of a walk warp
+ * must be idle before it takes new walks from the queue (default 8).  Every
+ * packet's history, and so every tally up to the order of floating-point
+ * additions, is independent of either choice.  No reference counterpart
+ * (the reference runs one packet per MPI rank thread). */
 int mcrt_set_schedule(mcrt_ctx *ctx, int32_t schedule, int32_t event_batch);
+
+/* Wavefront schedule sizes.  `slots`: in-flight packet slots (default
+ * 2,097,152; 784 bytes of device memory each).  `peel_jobs`: capacity of the
+ * peel-off job queue in jobs (176 bytes each; 0 = default, the larger of
+ * 8,388,608 and 3 x slots; else at least 2 x slots); the loop runs the
+ * peel-off kernel whenever fewer than `slots` free jobs remain.
+ * `tail_packets`: once every packet of the range has started and at most
+ * this many are in flight, one launch of the warp-scheduled loop finishes
+ * them (negative = default, 8 per lane of that launch; 0 = never, waves to
+ * the end).  Takes effect at the next mcrt_run_iteration.  No reference
+ * counterpart. */
+int mcrt_set_wave_pool(mcrt_ctx *ctx, int64_t slots, int64_t peel_jobs, int64_t tail_packets);
 
 /* Zero the tallies of one iteration (initarr_2_new.f90:79-119). */
 int mcrt_reset_tallies(mcrt_ctx *ctx);

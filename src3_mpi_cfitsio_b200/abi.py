@@ -22,7 +22,7 @@ PREC_MIXED = 1
 SCALARS = ["flux", "sflux", "nscat", "tot", "scount", "dscount", "aflux", "abflux"]
 COUNTERS = ["packets", "crossings", "interactions", "scatters", "peels", "peel_cross",
             "peel_binned", "geom_fail", "resets", "killed", "exited", "starhits",
-            "peel_resets", "peel_jobs", "c14", "c15"]
+            "peel_resets", "peel_jobs", "waves", "launches"]
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

@@ -31,6 +31,19 @@ int peel_fp64_blocks_per_sm();
 cudaError_t launch_peel_mixed(const LaunchParams& p, unsigned long long* next_item, int grid, cudaStream_t s);
 int peel_mixed_blocks_per_sm();
 int transport_mixed_blocks_per_sm();
+cudaError_t launch_wave_init(const WaveArgs& w, cudaStream_t s);
+cudaError_t launch_wave_event_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+cudaError_t launch_wave_walk_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+int wave_event_fp64_blocks_per_sm();
+int wave_walk_fp64_blocks_per_sm();
+cudaError_t launch_wave_event_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+cudaError_t launch_wave_walk_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+int wave_event_mixed_blocks_per_sm();
+int wave_walk_mixed_blocks_per_sm();
+cudaError_t launch_wave_tail_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+cudaError_t launch_wave_tail_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
+int wave_tail_fp64_blocks_per_sm();
+int wave_tail_mixed_blocks_per_sm();
 }  // namespace mcrt
 
 using namespace mcrt;
@@ -40,8 +53,19 @@ struct mcrt_ctx {
   int device = 0;
   int nsm = 148;
   int precision = MCRT_PREC_FP64;
-  int schedule = MCRT_SCHED_WARP;
+  int schedule = MCRT_SCHED_WAVE;
   int event_batch = 16;
+  int wave_batch = 8;
+  // wavefront pool
+  int64_t wave_pool = 1 << 21;
+  int64_t wave_jobs = 0;              // peel-off job queue capacity asked for (0: default)
+  int64_t wave_tail = -1;             // tail launch at <= this many live packets (<0: 8 per tail lane, 0: never)
+  int64_t wave_cap = 0;
+  WaveRec *d_recs = nullptr;
+  int32_t *d_walkq = nullptr, *d_evq = nullptr;
+  WaveCtl *d_wctl = nullptr;
+  unsigned long long *h_wctl = nullptr;   // pinned: n_front, n_back, peel jobs
+  int64_t last_waves = 0;
   bool have_grid = false, have_tables = false;
   std::string err;
   cudaStream_t stream = nullptr;
@@ -285,6 +309,11 @@ __global__ void tfinal_stats(int nrg, int ntg, const double* told, const double*
 constexpr int64_t kNoAllocMaxCells = 524288;
 static __device__ __align__(256) double g_tfinal_scratch[3 * kNoAllocMaxCells + 16];
 
+__global__ void add_counters(unsigned long long* cnt, unsigned long long waves, unsigned long long launches) {
+  cnt[MCRT_C_WAVES] += waves;
+  cnt[MCRT_C_LAUNCHES] += launches;
+}
+
 __global__ void to_float(const double* src, float* dst, int64_t n) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
     dst[k] = (float)src[k];
@@ -354,6 +383,7 @@ void mcrt_destroy(mcrt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->h_wctl) cudaFreeHost(ctx->h_wctl);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (auto& e : ctx->marks) if (e) cudaEventDestroy(e);
@@ -370,10 +400,23 @@ int mcrt_set_precision(mcrt_ctx* ctx, int32_t mode) {
 
 int mcrt_set_schedule(mcrt_ctx* ctx, int32_t schedule, int32_t event_batch) {
   if (!ctx) return MCRT_ERR_ARG;
-  if (schedule != MCRT_SCHED_PACKET && schedule != MCRT_SCHED_WARP) return fail(ctx, MCRT_ERR_ARG, "unknown schedule %d", schedule);
+  if (schedule != MCRT_SCHED_PACKET && schedule != MCRT_SCHED_WARP && schedule != MCRT_SCHED_WAVE)
+    return fail(ctx, MCRT_ERR_ARG, "unknown schedule %d", schedule);
   if (event_batch < 1 || event_batch > 32) return fail(ctx, MCRT_ERR_ARG, "event_batch must be 1..32");
   ctx->schedule = schedule;
-  ctx->event_batch = event_batch;
+  if (schedule == MCRT_SCHED_WAVE) ctx->wave_batch = event_batch;
+  else ctx->event_batch = event_batch;
+  return MCRT_OK;
+}
+
+int mcrt_set_wave_pool(mcrt_ctx* ctx, int64_t slots, int64_t peel_jobs, int64_t tail_packets) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (slots < 32 || slots > ((int64_t)1 << 30)) return fail(ctx, MCRT_ERR_ARG, "wave pool must hold 32..2^30 slots");
+  if (peel_jobs != 0 && (peel_jobs < 2 * slots || peel_jobs > ((int64_t)1 << 32)))
+    return fail(ctx, MCRT_ERR_ARG, "peel-off job queue must hold 2 x slots .. 2^32 jobs (or 0 for the default)");
+  ctx->wave_pool = slots;
+  ctx->wave_jobs = peel_jobs;
+  ctx->wave_tail = tail_packets;
   return MCRT_OK;
 }
 
@@ -636,24 +679,133 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   const int64_t npk = hi - lo + 1;
   P.event_batch = ctx->event_batch;
   const bool mixed = ctx->precision == MCRT_PREC_MIXED;
-  const bool warp = ctx->schedule == MCRT_SCHED_WARP || mixed;   // the mixed build is warp-scheduled only
+  const bool wave = ctx->schedule == MCRT_SCHED_WAVE;
+  const bool warp = !wave && (ctx->schedule == MCRT_SCHED_WARP || mixed);   // the mixed build has no per-thread kernel
   // peel-offs go through the job queue and the peel-off kernel
-  const bool queue = P.ipeel && warp && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
-  if (queue && !ctx->d_jobs) {
-    ctx->job_cap = 8 * ctx->chunk_packets;
-    int rc = dalloc(ctx, &ctx->d_jobs, (size_t)ctx->job_cap);
+  const bool queue = P.ipeel && (warp || wave) && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
+  const int64_t wave_slots = wave ? std::min<int64_t>(ctx->wave_pool, npk) : 0;
+  if (queue) {
+    // the wavefront loop drains the queue once fewer than one wave of jobs
+    // (at most one per slot) is left
+    const bool exact = wave && ctx->wave_jobs > 0;    // capacity set by mcrt_set_wave_pool
+    const int64_t want = exact ? std::max<int64_t>(ctx->wave_jobs, 2 * wave_slots)
+                               : std::max<int64_t>(8 * ctx->chunk_packets, 3 * wave_slots);
+    if (ctx->job_cap < want || (exact && ctx->job_cap != want)) {
+      if (ctx->d_jobs) dfree(ctx, ctx->d_jobs);
+      ctx->d_jobs = nullptr;
+      ctx->job_cap = 0;
+      int rc = dalloc(ctx, &ctx->d_jobs, (size_t)want);
+      if (rc) return rc;
+      ctx->job_cap = want;
+    }
+  }
+  if (wave && ctx->wave_cap < wave_slots) {
+    if (ctx->d_recs) dfree(ctx, ctx->d_recs);
+    if (ctx->d_walkq) dfree(ctx, ctx->d_walkq);
+    if (ctx->d_evq) dfree(ctx, ctx->d_evq);
+    ctx->d_recs = nullptr; ctx->d_walkq = ctx->d_evq = nullptr;
+    ctx->wave_cap = 0;
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->d_recs, (size_t)wave_slots)) || (rc = dalloc(ctx, &ctx->d_walkq, (size_t)wave_slots)) ||
+        (rc = dalloc(ctx, &ctx->d_evq, (size_t)wave_slots)))
+      return rc;
+    ctx->wave_cap = wave_slots;
+  }
+  if (wave && !ctx->d_wctl) {
+    int rc = dalloc(ctx, &ctx->d_wctl, 1);
     if (rc) return rc;
+    CK(cudaHostAlloc((void**)&ctx->h_wctl, 4 * sizeof(unsigned long long), cudaHostAllocDefault));
   }
   P.jobs = queue ? ctx->d_jobs : nullptr;
   P.njobs = ctx->d_next + 1;
   P.job_cap = ctx->job_cap;
-  int per_sm = ctx->precision == MCRT_PREC_FP64 ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
-                                                : transport_mixed_blocks_per_sm();
-  const int full_grid = ctx->nsm * std::max(per_sm, 1);
   const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
+  int64_t launches = 0;                     // kernels this call launches (MCRT_C_LAUNCHES)
+  auto launch_peel = [&]() -> int {
+    ++launches;
+    cudaError_t e = mixed ? launch_peel_mixed(P, ctx->d_next + 2, peel_grid, ctx->stream)
+                          : launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
+    return MCRT_OK;
+  };
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (wave) {
+    // Wavefront loop: event launch (emission / interactions / exits up to
+    // the next walk), walk launch (every queued walk to its next event).
+    // The host reads the queue sizes after every walk launch and drains the
+    // peel-off job queue before it can overflow.  Once every packet of the
+    // range has started and few are left in flight, one tail launch
+    // finishes them without per-wave synchronisation.
+    WaveArgs W{};
+    W.recs = ctx->d_recs;
+    W.walkq = ctx->d_walkq;
+    W.evq = ctx->d_evq;
+    W.ctl = ctx->d_wctl;
+    W.slots = wave_slots;
+    W.walk_batch = ctx->wave_batch;
+    const int egrid = ctx->nsm * (mixed ? wave_event_mixed_blocks_per_sm() : wave_event_fp64_blocks_per_sm());
+    const int wgrid = ctx->nsm * (mixed ? wave_walk_mixed_blocks_per_sm() : wave_walk_fp64_blocks_per_sm());
+    const int tgrid = ctx->nsm * (mixed ? wave_tail_mixed_blocks_per_sm() : wave_tail_fp64_blocks_per_sm());
+    const unsigned long long tail_live = ctx->wave_tail < 0 ? (unsigned long long)tgrid * kTransportBlock * 8ull
+                                                            : (unsigned long long)ctx->wave_tail;
+    CK(cudaMemsetAsync(ctx->d_next, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    cudaError_t e = launch_wave_init(W, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave init: %s", cudaGetErrorString(e));
+    ++launches;
+    // every wave advances each live packet by at least one event, and a
+    // packet ends after at most 1e8 events (the event watchdog)
+    const int64_t max_waves = 400000000;
+    int64_t waves = 0;
+    unsigned long long* h = ctx->h_wctl;      // n_front, n_back, packets started, peel jobs
+    for (;;) {
+      CK(cudaMemsetAsync(&ctx->d_wctl->n_walk, 0, 2 * sizeof(unsigned long long), ctx->stream));
+      e = mixed ? launch_wave_event_mixed(P, W, egrid, ctx->stream) : launch_wave_event_fp64(P, W, egrid, ctx->stream);
+      if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave event launch: %s", cudaGetErrorString(e));
+      CK(cudaMemsetAsync(&ctx->d_wctl->n_front, 0, 3 * sizeof(unsigned long long), ctx->stream));
+      e = mixed ? launch_wave_walk_mixed(P, W, wgrid, ctx->stream) : launch_wave_walk_fp64(P, W, wgrid, ctx->stream);
+      if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave walk launch: %s", cudaGetErrorString(e));
+      ++waves;
+      launches += 2;
+      CK(cudaMemcpyAsync(h, &ctx->d_wctl->n_front, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(h + 2, ctx->d_next, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      const unsigned long long live = h[0] + h[1];
+#ifdef MCRT_WAVE_TRACE
+      fprintf(stderr, "wave %lld live %llu interactions %llu started %llu jobs %llu\n", (long long)waves, live, h[0],
+              h[2], h[3]);
+#endif
+      if (live == 0) break;
+      if (waves > max_waves) return fail(ctx, MCRT_ERR_CUDA, "wavefront loop did not finish in %lld waves", (long long)waves);
+      const bool tail = tail_live > 0 && (int64_t)h[2] >= npk && live <= tail_live;
+      if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && 2 * (int64_t)h[3] > ctx->job_cap))) {
+        CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
+        int rc = launch_peel();
+        if (rc) return rc;
+        CK(cudaMemsetAsync(ctx->d_next + 1, 0, sizeof(unsigned long long), ctx->stream));
+      }
+      if (tail) {
+        LaunchParams T = P;
+        T.fetch_off = 1;
+        CK(cudaMemsetAsync(&ctx->d_wctl->n_walk, 0, 2 * sizeof(unsigned long long), ctx->stream));
+        e = mixed ? launch_wave_tail_mixed(T, W, tgrid, ctx->stream) : launch_wave_tail_fp64(T, W, tgrid, ctx->stream);
+        if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave tail launch: %s", cudaGetErrorString(e));
+        ++launches;
+        break;
+      }
+    }
+    if (queue) {
+      CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
+      int rc = launch_peel();
+      if (rc) return rc;
+    }
+    ctx->last_waves = waves;
+  }
+  int per_sm = wave ? 1 : ctx->precision == MCRT_PREC_FP64
+                              ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
+                              : transport_mixed_blocks_per_sm();
+  const int full_grid = ctx->nsm * std::max(per_sm, 1);
   const int64_t chunk = queue ? ctx->chunk_packets : npk;
-  for (int64_t c_lo = lo; c_lo <= hi; c_lo += chunk) {
+  for (int64_t c_lo = lo; !wave && c_lo <= hi; c_lo += chunk) {
     const int64_t c_hi = std::min(hi, c_lo + chunk - 1);
     P.lo = c_lo;
     P.hi = c_hi;
@@ -664,10 +816,10 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
                         ? (warp ? launch_transport_sched_fp64(P, grid, ctx->stream) : launch_transport_fp64(P, grid, ctx->stream))
                         : launch_transport_mixed(P, grid, ctx->stream);
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
+    ++launches;
     if (queue) {
-      e = mixed ? launch_peel_mixed(P, ctx->d_next + 2, peel_grid, ctx->stream)
-                : launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
-      if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
+      int rc = launch_peel();
+      if (rc) return rc;
     }
   }
   P.lo = lo;
@@ -675,6 +827,10 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   cudaError_t ef = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);
   if (ef != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion finalize: %s", cudaGetErrorString(ef));
+  launches += 2;                              // diffusion_finalize and add_counters
+  add_counters<<<1, 1, 0, ctx->stream>>>(ctx->dt.cnt, (unsigned long long)(wave ? ctx->last_waves : 0),
+                                         (unsigned long long)launches);
+  CK(cudaGetLastError());
   CK(cudaEventSynchronize(ctx->ev1));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));

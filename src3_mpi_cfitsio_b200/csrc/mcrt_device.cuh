@@ -93,6 +93,49 @@ struct __align__(16) PeelJob {
   uint32_t bits;                  // onw | iflag<<1 | direct<<2 | (i_orig)<<3 | (inub-1)<<8
 };
 
+// Wavefront schedule: one in-flight packet per pool slot, kept in HBM
+// between the walk kernel and the event kernel.  The walk part (first 200
+// bytes) is what the walk kernel reads and writes; the event kernel moves the
+// whole record.  `spec` holds the species columns kapd, alb, g, pl, kap
+// (kMaxSlot each) of the packet's current frequency.
+struct __align__(16) WaveRec {
+  // walk part
+  double x, y, z, rs, rt, vx, vy, vz, tsum;   // ray
+  double tau, ifuv;
+  int64_t ray_steps;
+  int32_t r, t, p, rbits;                     // rbits: ray onw | ray peel << 1
+  int32_t s1, s2, ndraws, ev;
+  int32_t status, ncross, exitflag, on_wall;
+  int32_t ir, it, ip, pad0;
+  double xp, yp, zp, rsq, rtot;
+  // event part
+  double ux, uy, uz, cost, sint, cosp, sinp, phi, sip, sqp, sup, svp, nub, cosb, sinb, lp;
+  double xpold, ypold, zpold, peel_si, coslp, sinlp;
+  int64_t nev, iphot, kfetch;
+  int32_t iflag, i_orig, nscat, nabsev, nstar, ndiffev, iscat, iint;
+  int32_t first, slot_s, prev_r, prev_t, prev_p, peel_ctx, peelid, peel_idust2;
+  double spec[5 * kMaxSlot];
+};
+static_assert(sizeof(WaveRec) % 16 == 0, "WaveRec must keep 16-byte alignment");
+
+// Queue counters of the wavefront loop.  The event queue is filled from both
+// ends by the walk kernel: interactions from the front, every other event
+// from the back, so the event kernel's warps see one kind of event at a time.
+struct WaveCtl {
+  unsigned long long n_front, n_back, walk_fetch, pad0;   // zeroed before each walk launch
+  unsigned long long n_walk, ev_fetch, pad1, pad2;        // zeroed before each event launch
+};
+
+struct WaveArgs {
+  WaveRec* recs;        // [slots]
+  int32_t* walkq;       // [slots] slots to walk (event kernel -> walk kernel)
+  int32_t* evq;         // [slots] slots with a pending event (walk kernel -> event kernel)
+  WaveCtl* ctl;
+  int64_t slots;
+  int32_t walk_batch;   // idle lanes of a warp before the walk kernel fetches new walks
+  int32_t pad_;
+};
+
 struct LaunchParams {
   DevModel m;
   DevTallies t;
@@ -101,7 +144,7 @@ struct LaunchParams {
   int64_t ns, npacc, npaccstar; // packet split (newdisktherm_5_fuv.f90:158-191)
   int32_t ipeel, ips;
   int32_t event_batch;          // warp scheduler: lanes that must wait before events run
-  int32_t pad_;
+  int32_t fetch_off;            // 1: a finished packet starts no new packet (wavefront tail launch)
   double nphot_diff;            // nphot of emit_common's surface heating (ns of this shard)
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter

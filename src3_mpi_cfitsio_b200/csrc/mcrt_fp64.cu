@@ -2,10 +2,52 @@
 // every FP64 add/multiply is a separate IEEE operation, as in the oracle.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"
+#include "mcrt_wave.cuh"
 
 namespace mcrt {
+
+cudaError_t launch_wave_init(const WaveArgs& w, cudaStream_t s) {
+  const int grid = (int)std::min<int64_t>((w.slots + 255) / 256, 4096);
+  wave_init<<<grid > 0 ? grid : 1, 256, 0, s>>>(w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_event_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  wave_event<<<grid, kBlock, 0, s>>>(p, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_walk_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  wave_walk<<<grid, kBlock, 0, s>>>(p, w);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_tail_fp64(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  wave_tail<<<grid, kBlock, 0, s>>>(p, w);
+  return cudaGetLastError();
+}
+
+int wave_tail_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_tail, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+int wave_event_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_event, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+int wave_walk_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_walk, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
 
 cudaError_t launch_transport_fp64(const LaunchParams& p, int grid, cudaStream_t s) {
   transport_fp64<<<grid, kBlock, 0, s>>>(p);

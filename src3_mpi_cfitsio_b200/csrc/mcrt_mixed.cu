@@ -17,10 +17,51 @@
 #define mcrt mcrt_mixed
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"
+#include "mcrt_wave.cuh"
 #undef mcrt
 
 namespace mcrt {
 struct LaunchParams;
+struct WaveArgs;
+
+cudaError_t launch_wave_event_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);
+  const auto& v = reinterpret_cast<const mcrt_mixed::WaveArgs&>(w);
+  mcrt_mixed::wave_event<<<grid, mcrt_mixed::kBlock, 0, s>>>(q, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_walk_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);
+  const auto& v = reinterpret_cast<const mcrt_mixed::WaveArgs&>(w);
+  mcrt_mixed::wave_walk<<<grid, mcrt_mixed::kBlock, 0, s>>>(q, v);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wave_tail_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
+  const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);
+  const auto& v = reinterpret_cast<const mcrt_mixed::WaveArgs&>(w);
+  mcrt_mixed::wave_tail<<<grid, mcrt_mixed::kBlock, 0, s>>>(q, v);
+  return cudaGetLastError();
+}
+
+int wave_tail_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::wave_tail, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+int wave_event_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::wave_event, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
+
+int wave_walk_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::wave_walk, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
 
 cudaError_t launch_transport_mixed(const LaunchParams& p, int grid, cudaStream_t s) {
   const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);

@@ -35,6 +35,7 @@ enum Ev : int {
   EV_NEXT_TAU,       // sample tau, resume the packet walk
   EV_EXIT,           // packet left the grid: SED binning
   EV_FINISH,         // packet finished (status set)
+  EV_STAR,           // packet walk reached the stellar surface (wavefront walk only)
   EV_DONE            // no packets left for this lane
 };
 enum PeelCtx : int { PC_DIRECT = 0, PC_SCATTER = 1, PC_ABSORB = 2 };
@@ -80,9 +81,33 @@ struct Lane {
     ev = EV_NONE;
   }
 
+  // Stellar-surface hit inside the packet walk: re-emission from the surface
+  // with the sampled tau kept (tauint_3d_2_fuv.f90:184-206).  The packet
+  // position has been copied from the ray.
+  __device__ void star_reemit() {
+    const DevModel& m = pk.m;
+    atomicAdd(pk.T.scal + MCRT_S_AFLUX, 1.0);
+    ++pk.nstar;
+    pk.rtot = sqrt(pk.rsq);
+    pk.initpabs();
+    pk.opacset(pk.nub, KAPD_TAUINT);
+    pk.ifuv = Packet::is_fuv(pk.nub) ? m.ifuv_ori : 0.0;
+    pk.i_orig = 1;
+    pk.iflag = 0;
+    pk.ir = 1;
+    const double tsave = 0.0;
+    ray_from_packet(false);
+    ray.vx = pk.ux; ray.vy = pk.uy; ray.vz = pk.uz;
+    ray.tsum = tsave;
+  }
+
   // ---------------------------------------------------------- ray step
   // One cell crossing of the current ray: tauint_3d_2_fuv.f90:36-206 for the
-  // packet walk, peeloff_3d_2_test.f90:133-214 for a peel-off walk.
+  // packet walk, peeloff_3d_2_test.f90:133-214 for a peel-off walk.  With
+  // kStarEvent the stellar-surface hit ends the step with EV_STAR instead of
+  // re-emitting in place, so that the walk needs only the opacity and
+  // albedo columns of the species state (kapd, alb).
+  template <bool kStarEvent = false>
   __device__ __forceinline__ void step(const LaunchParams& P) {
     const DevModel& m = pk.m;
     Ray& R = ray;
@@ -140,19 +165,8 @@ struct Lane {
       if (R.r == m.nrg) { pk.exitflag = 1; packet_from_ray(); ev = EV_EXIT; return; }
       if (R.r == 0) {                 // star hit: re-emission, tau kept (tauint_3d_2_fuv.f90:184-206)
         packet_from_ray();
-        atomicAdd(pk.T.scal + MCRT_S_AFLUX, 1.0);
-        ++pk.nstar;
-        pk.rtot = sqrt(pk.rsq);
-        pk.initpabs();
-        pk.opacset(pk.nub, KAPD_TAUINT);
-        pk.ifuv = Packet::is_fuv(pk.nub) ? m.ifuv_ori : 0.0;
-        pk.i_orig = 1;
-        pk.iflag = 0;
-        pk.ir = 1;
-        const double tsave = 0.0;
-        ray_from_packet(false);
-        ray.vx = pk.ux; ray.vy = pk.uy; ray.vz = pk.uz;
-        ray.tsum = tsave;
+        if (kStarEvent) { ev = EV_STAR; return; }
+        star_reemit();
       }
     } else {
       ++pk.c_pcross;
@@ -274,6 +288,7 @@ struct Lane {
         case EV_DONE:
           return;
         case EV_FETCH: {
+          if (P.fetch_off) { ev = EV_DONE; return; }
           const unsigned long long k = atomicAdd(P.next, 1ull);
           if ((int64_t)k >= P.hi - P.lo + 1) { ev = EV_DONE; return; }
           kfetch = (int64_t)k;
@@ -441,6 +456,10 @@ struct Lane {
           pk.uz = pk.cost;
           prev_r = pk.ir; prev_t = pk.it; prev_p = pk.ip;
           start_walk();
+          return;
+        case EV_STAR:                  // tauint_3d_2_fuv.f90:184-206, walk resumes
+          star_reemit();
+          ev = EV_NONE;
           return;
         case EV_EXIT:                  // propagate_5_fuv.f90:231-320
           exit_bin();

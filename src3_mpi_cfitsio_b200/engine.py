@@ -45,6 +45,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_upload_tables.argtypes = [C.c_void_p, P(abi.Tables)]
     lib.mcrt_set_precision.argtypes = [C.c_void_p, C.c_int32]
     lib.mcrt_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+    lib.mcrt_set_wave_pool.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
     lib.mcrt_reset_tallies.argtypes = [C.c_void_p]
     lib.mcrt_run_iteration.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32, C.c_int32]
@@ -65,7 +66,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
     for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision", "mcrt_set_schedule",
-                 "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
+                 "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_mark", "mcrt_elapsed_ms",
                  "mcrt_flush_l2", "mcrt_synchronize"):
@@ -114,10 +115,23 @@ class Engine:
         self._check(self.lib.mcrt_set_precision(self.ctx, mode))
         self.precision = precision
 
-    def set_schedule(self, schedule: str = "warp", event_batch: int = 16):
-        mode = {"packet": 0, "warp": 1}[schedule]
+    def set_schedule(self, schedule: str = "wave", event_batch: int | None = None):
+        """Kernel schedule: "packet" (one thread per packet), "warp" (lockstep
+        lanes, batched events) or "wave" (walk / event kernels over a pool of
+        in-flight packets).  `event_batch`: warp schedule -- lanes waiting
+        before events run (default 16); wave -- idle lanes before a walk
+        warp takes new walks (default 8)."""
+        mode = {"packet": 0, "warp": 1, "wave": 2}[schedule]
+        if event_batch is None:
+            event_batch = 8 if schedule == "wave" else 16
         self._check(self.lib.mcrt_set_schedule(self.ctx, mode, event_batch))
         self.schedule = schedule
+
+    def set_wave_pool(self, slots: int = 1 << 21, peel_jobs: int = 0, tail_packets: int = -1):
+        """Wavefront schedule sizes: in-flight packet slots, peel-off job
+        queue capacity (0: default) and the live-packet count at which one
+        tail launch finishes the iteration (<0: default, 0: never)."""
+        self._check(self.lib.mcrt_set_wave_pool(self.ctx, int(slots), int(peel_jobs), int(tail_packets)))
 
     def upload_grid(self):
         self.bundle = abi.Bundle(self.model)

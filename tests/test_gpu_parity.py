@@ -144,7 +144,8 @@ def diffusion_small():
     return model.with_diffusion(model.warm(model.small_2d()))
 
 
-def test_diffusion_statistical_and_pre_diffusion_exact(diffusion_small, oracle_mod):
+@pytest.mark.parametrize("schedule", ["warp", "wave"])
+def test_diffusion_statistical_and_pre_diffusion_exact(diffusion_small, oracle_mod, schedule):
     """Diffusion (emit_common_2.f90:201-372): packets that never reach a
     diffusion cell stay event-for-event equal; the ones that do depend on
     the order in which diffusion absorptions heat the surface cell, so the
@@ -152,6 +153,9 @@ def test_diffusion_statistical_and_pre_diffusion_exact(diffusion_small, oracle_m
     m = diffusion_small
     n = 20000
     eng = _engine(m)
+    eng.set_schedule(schedule)
+    if schedule == "wave":
+        eng.set_wave_pool(2048)
     eng.enable_packet_log(n)
     eng.reset_tallies()
     eng.run(n, ipeel=0)
@@ -191,6 +195,78 @@ def test_schedules_agree_bitwise(warm_small, batch):
     a, b = logs
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("precision,pool,batch,tail", [("fp64", 1 << 21, 8, -1), ("fp64", 96, 1, 0),
+                                                       ("fp64", 512, 32, 200), ("mixed", 1 << 21, 8, -1),
+                                                       ("mixed", 256, 8, 0)])
+def test_wave_schedule_matches_warp_bitwise(warm_small, precision, pool, batch, tail):
+    """The wavefront schedule (walk and event kernels over a pool of
+    in-flight packets in HBM, then one tail launch for the last packets)
+    runs every packet's steps in the same order on the same random stream as
+    the warp schedule: packet logs agree bit for bit, counters exactly,
+    tallies up to FP64 summation order.  Small pools take many waves and
+    drain the peel-off job queue more than once; tail 0 waves to the end."""
+    n = 3000
+    logs, tals = [], []
+    for sched in ("warp", "wave"):
+        eng = _engine(warm_small, precision=precision)
+        eng.set_schedule(sched, batch if sched == "wave" else 16)
+        if sched == "wave":
+            eng.set_wave_pool(pool, 2 * pool if pool < 1000 else 0, tail)
+        eng.enable_packet_log(n)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        logs.append(abi.packet_log_to_numpy(eng.packet_log(n)))
+        tals.append(eng.download())
+        eng.close()
+    a, b = logs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    ca, cb = tals[0].counters(), tals[1].counters()
+    assert cb["waves"] > 0 and ca["waves"] == 0
+    for k in ("packets", "crossings", "interactions", "scatters", "peels", "peel_cross", "peel_binned",
+              "geom_fail", "resets", "killed", "exited", "starhits"):
+        assert ca[k] == cb[k], k
+    # the waves never overflow the job queue; the tail launch walks the
+    # peel-offs of a full queue inline, as the warp kernel does
+    if tail == 0:
+        assert ca["peel_jobs"] == cb["peel_jobs"]
+    else:
+        assert cb["peel_jobs"] <= ca["peel_jobs"]
+    if tail == 0:
+        assert cb["waves"] > n // pool
+    for k in ("ti", "tq", "tu", "numt", "image_m_i", "image_m_q", "si", "sq", "nums", "dtauabs"):
+        x, y = tals[0][k], tals[1][k]
+        assert np.allclose(x, y, rtol=1e-5, atol=1e-6 * max(1e-30, float(np.abs(x).max()))), k
+    for k in ("nabs", "dbig", "dsg", "killed"):
+        assert np.array_equal(tals[0][k], tals[1][k]), k
+
+
+def test_wave_schedule_without_peel_offs_and_shards(warm_small):
+    """Wavefront runs of packet sub-ranges add up to the full range run with
+    the warp schedule (the sharding used across ranks)."""
+    n = 4000
+    eng = _engine(warm_small)
+    eng.set_schedule("warp")
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    a = eng.download()
+    eng.close()
+    eng = _engine(warm_small)
+    eng.set_schedule("wave")
+    eng.set_wave_pool(256, 0, 100)
+    eng.reset_tallies()
+    for lo, hi in ((1, 1234), (1235, 3001), (3002, 4000)):
+        eng.run(n, lo, hi, ipeel=0)
+    b = eng.download()
+    eng.close()
+    ca, cb = a.counters(), b.counters()
+    for k in ("packets", "crossings", "interactions", "exited", "starhits"):
+        assert ca[k] == cb[k], k
+    for k in ("si", "nums", "dtauabs"):
+        assert np.allclose(a[k], b[k], rtol=1e-5, atol=1e-6 * max(1e-30, float(np.abs(a[k]).max()))), k
+    assert np.array_equal(a["nabs"], b["nabs"])
 
 
 def test_peel_queue_matches_inline_peel_offs(warm_small):
