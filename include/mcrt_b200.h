@@ -222,9 +222,11 @@ int mcrt_set_schedule(mcrt_ctx *ctx, int32_t schedule, int32_t event_batch);
 
 /* Wavefront schedule sizes.  `slots`: in-flight packet slots (default
  * 2,097,152; 784 bytes of device memory each).  `peel_jobs`: capacity of the
- * peel-off job queue in jobs (176 bytes each; 0 = default, the larger of
- * 8,388,608 and 3 x slots; else at least 2 x slots); the loop runs the
- * peel-off kernel whenever fewer than `slots` free jobs remain.
+ * peel-off job queue in jobs (176 bytes each; 0 = default, 16 x slots
+ * within [8,388,608, 67,108,864]; else at least 2 x slots); the loop runs
+ * the peel-off kernel whenever fewer than `slots` free jobs remain and
+ * before the tail launch, whose peel-offs beyond the capacity are walked
+ * inline.
  * `tail_packets`: once every packet of the range has started and at most
  * this many are in flight, one launch of the warp-scheduled loop finishes
  * them (negative = default, 8 per lane of that launch; 0 = never, waves to

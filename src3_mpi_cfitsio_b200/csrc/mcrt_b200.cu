@@ -687,9 +687,15 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   if (queue) {
     // the wavefront loop drains the queue once fewer than one wave of jobs
     // (at most one per slot) is left
+    // The tail launch of the wavefront loop cannot drain the queue while it
+    // runs: the remaining interactions of its packets (the heavy-tailed
+    // histories of optically thick regions, several per live packet) must
+    // fit, else their peel-offs are walked inline.
     const bool exact = wave && ctx->wave_jobs > 0;    // capacity set by mcrt_set_wave_pool
     const int64_t want = exact ? std::max<int64_t>(ctx->wave_jobs, 2 * wave_slots)
-                               : std::max<int64_t>(8 * ctx->chunk_packets, 3 * wave_slots);
+                         : wave ? std::min<int64_t>(std::max<int64_t>(16 * wave_slots, 8 * ctx->chunk_packets),
+                                                    (int64_t)1 << 26)
+                                : 8 * ctx->chunk_packets;
     if (ctx->job_cap < want || (exact && ctx->job_cap != want)) {
       if (ctx->d_jobs) dfree(ctx, ctx->d_jobs);
       ctx->d_jobs = nullptr;
@@ -777,7 +783,7 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
       if (live == 0) break;
       if (waves > max_waves) return fail(ctx, MCRT_ERR_CUDA, "wavefront loop did not finish in %lld waves", (long long)waves);
       const bool tail = tail_live > 0 && (int64_t)h[2] >= npk && live <= tail_live;
-      if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && 2 * (int64_t)h[3] > ctx->job_cap))) {
+      if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && h[3] > 0))) {
         CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
         int rc = launch_peel();
         if (rc) return rc;
