@@ -26,7 +26,12 @@
 namespace mcrt {
 
 // ------------------------------------------------------------ record I/O
-__device__ __forceinline__ void wave_load_walk(Lane& L, const WaveRec& R, int nslot) {
+// The walk kernel reads the ray part only: every way a packet walk ends
+// (interaction point, exit, stellar surface, geometry failure) first copies
+// the ray into the packet position (packet_from_ray), and a peel-off walk
+// never changes it, so the packet position is written back after packet
+// walks and never read by the walk kernel.
+__device__ __forceinline__ void wave_load_ray(Lane& L, const WaveRec& R, int nslot) {
   Ray& y = L.ray;
   y.x = R.x; y.y = R.y; y.z = R.z; y.rs = R.rs; y.rt = R.rt;
   y.vx = R.vx; y.vy = R.vy; y.vz = R.vz; y.tsum = R.tsum;
@@ -38,16 +43,21 @@ __device__ __forceinline__ void wave_load_walk(Lane& L, const WaveRec& R, int ns
   L.ray_steps = R.ray_steps;
   k.rng.s1 = R.s1; k.rng.s2 = R.s2; k.rng.ndraws = R.ndraws;
   L.ev = R.ev; L.status = R.status;
-  k.ncross = R.ncross; k.exitflag = R.exitflag; k.on_wall = R.on_wall != 0;
-  k.ir = R.ir; k.it = R.it; k.ip = R.ip;
-  k.xp = R.xp; k.yp = R.yp; k.zp = R.zp; k.rsq = R.rsq; k.rtot = R.rtot;
+  k.ncross = R.ncross; k.exitflag = R.exitflag;
   for (int s = 0; s < nslot; ++s) {
     k.sp.kapd(s) = R.spec[s];
     k.sp.alb(s) = R.spec[kMaxSlot + s];
   }
 }
 
-__device__ __forceinline__ void wave_save_walk(const Lane& L, WaveRec& R) {
+__device__ __forceinline__ void wave_load_pos(Lane& L, const WaveRec& R) {
+  Packet& k = L.pk;
+  k.on_wall = R.on_wall != 0;
+  k.ir = R.ir; k.it = R.it; k.ip = R.ip;
+  k.xp = R.xp; k.yp = R.yp; k.zp = R.zp; k.rsq = R.rsq; k.rtot = R.rtot;
+}
+
+__device__ __forceinline__ void wave_save_ray(const Lane& L, WaveRec& R) {
   const Ray& y = L.ray;
   R.x = y.x; R.y = y.y; R.z = y.z; R.rs = y.rs; R.rt = y.rt;
   R.vx = y.vx; R.vy = y.vy; R.vz = y.vz; R.tsum = y.tsum;
@@ -58,9 +68,24 @@ __device__ __forceinline__ void wave_save_walk(const Lane& L, WaveRec& R) {
   R.ray_steps = L.ray_steps;
   R.s1 = k.rng.s1; R.s2 = k.rng.s2; R.ndraws = k.rng.ndraws;
   R.ev = L.ev; R.status = L.status;
-  R.ncross = k.ncross; R.exitflag = k.exitflag; R.on_wall = k.on_wall ? 1 : 0;
+  R.ncross = k.ncross; R.exitflag = k.exitflag;
+}
+
+__device__ __forceinline__ void wave_save_pos(const Lane& L, WaveRec& R) {
+  const Packet& k = L.pk;
+  R.on_wall = k.on_wall ? 1 : 0;
   R.ir = k.ir; R.it = k.it; R.ip = k.ip;
   R.xp = k.xp; R.yp = k.yp; R.zp = k.zp; R.rsq = k.rsq; R.rtot = k.rtot;
+}
+
+__device__ __forceinline__ void wave_load_walk(Lane& L, const WaveRec& R, int nslot) {
+  wave_load_ray(L, R, nslot);
+  wave_load_pos(L, R);
+}
+
+__device__ __forceinline__ void wave_save_walk(const Lane& L, WaveRec& R) {
+  wave_save_ray(L, R);
+  wave_save_pos(L, R);
 }
 
 __device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int nslot) {
@@ -151,7 +176,10 @@ __global__ void wave_init(WaveArgs W) {
 // Events of every queued packet up to its next walk (or to the end of the
 // packet range for this slot).  One queued packet per thread at a time; the
 // queue order keeps interactions and the other events in separate warps.
-__global__ void __launch_bounds__(kBlock) wave_event(LaunchParams P, WaveArgs W) {
+#ifndef MCRT_EVENT_MIN_BLOCKS
+#define MCRT_EVENT_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kBlock, MCRT_EVENT_MIN_BLOCKS) wave_event(LaunchParams P, WaveArgs W) {
   __shared__ double spec[5 * kMaxSlot * kBlock];
   Lane L(P.m, P.t, spec);
   const int nslot = P.m.nslot;
@@ -217,7 +245,7 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
         const unsigned long long k = base + (unsigned long long)__popc(idle & ((1u << lane) - 1u));
         if (k < nw) {
           slot = W.walkq[k];
-          wave_load_walk(L, W.recs[slot], nslot);
+          wave_load_ray(L, W.recs[slot], nslot);
           have = true;
         }
       }
@@ -230,7 +258,11 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
     if (have) {
       L.step<true>(P);
       done = L.ev != EV_NONE;
-      if (done) wave_save_walk(L, W.recs[slot]);
+      if (done) {
+        WaveRec& R = W.recs[slot];
+        wave_save_ray(L, R);
+        if (!L.ray.peel) wave_save_pos(L, R);
+      }
     }
     const bool front = done && L.ev == EV_AFTER_WALK;
     const bool back = done && !front;
