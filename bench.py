@@ -173,6 +173,8 @@ def run_ours(args, rank, world):
             eng.reset_tallies()
             eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
             kernel_ms.append(eng.kernel_ms())
+            if args.schedule == "wave":
+                wave_stats_last = eng.wave_stats()
             eng.update_temperature(np_total, it)
             if s + 1 < args.steps:
                 eng.flush_l2()
@@ -209,13 +211,31 @@ def run_ours(args, rank, world):
     e2e_ms = float(allreduce(np.array([e2e_ms]), "max")[0])
     e2e = np_total / (e2e_ms / 1e3)
 
-    # ---- roofline of the dominant kernel (transport, last timed step)
-    kms = kernel_ms[-1]
-    abytes = algorithmic_bytes(counters)
-    achieved = abytes / (kms / 1e3) / 1e9
+    # ---- roofline of the dominant kernel (last timed step)
     peaks = _peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
-    kname = "transport_sched (mixed)" if args.precision == "mixed" else "transport_sched (fp64)"
+    kernels = None
+    traffic = None
+    if args.schedule == "wave":
+        # wavefront: the walk kernel carries the cell crossings; achieved =
+        # 16 B per crossing it stepped / its summed launch time (the same
+        # ratio as per launch); traffic = DRAM bytes per walk (ncu capture)
+        # x walks per walk launch
+        ws = wave_stats_last
+        kernels = {k: ws[f"{k}_ms"] for k in ("walk", "event", "tail", "peel")}
+        kernels["launches"] = {k: ws[f"{k}_launches"] for k in ("walk", "event", "tail", "peel")}
+        kernels["walks"] = ws["walks"]
+        kernels["walk_crossings"] = ws["walk_crossings"]
+        kname = f"wave_walk ({args.precision})"
+        kms = ws["walk_ms"] / max(ws["walk_launches"], 1)
+        abytes = 16.0 * ws["walk_crossings"] / max(ws["walk_launches"], 1)
+        if args.traffic_per_walk:
+            traffic = args.traffic_per_walk * ws["walks"] / max(ws["walk_launches"], 1)
+    else:
+        kms = kernel_ms[-1]
+        abytes = algorithmic_bytes(counters)
+        kname = f"transport_sched ({args.precision})"
+    achieved = abytes / (kms / 1e3) / 1e9
 
     # ---- mixed vs FP64 at equal packet count (same random streams), and the
     # peeled imaging iteration, each measured once
@@ -277,9 +297,12 @@ def run_ours(args, rank, world):
                 "parallelism": f"packet shards x{world}"},
         e2e={"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                  "frac": achieved / peak, "traffic": args.traffic_per_packet * np_total if args.traffic_per_packet else None,
+                  "frac": achieved / peak, "traffic": traffic,
                   "peak_source": "measured" if not peaks.get("_fallback") else "fallback",
-                  "kernel": kname, "kernel_ms": kms, "algorithmic_bytes": abytes},
+                  "kernel": kname, "kernel_ms_per_launch": kms, "algorithmic_bytes_per_launch": abytes,
+                  "note": "cell walk: L2-resident grid, issue/latency-bound; 16 B per crossing is the "
+                          "algorithmic HBM-equivalent traffic"},
+        kernels_ms_last_step=kernels,
         # kernels of the last timed step (transport launches counted by the
         # engine, plus tfinal_cells / tfinal_mirror / tfinal_stats /
         # tdust_from_tdave), times the timed steps
@@ -352,8 +375,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
-    ap.add_argument("--traffic-per-packet", type=float, default=None,
-                    help="DRAM bytes per packet of the transport kernel from an ncu capture (profiles/)")
+    # 706 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
+    # launch over 2,097,152 walks (profiles/wave_walk_wave_event_mixed_2d_8e6.md)
+    ap.add_argument("--traffic-per-walk", type=float, default=705.9,
+                    help="DRAM bytes per walk of the wave_walk kernel from an ncu capture (profiles/)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

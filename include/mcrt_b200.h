@@ -287,6 +287,14 @@ int mcrt_download_packet_log(mcrt_ctx *ctx, mcrt_packet_log *out, int64_t n);
 /* Device time of the last mcrt_run_iteration's transport kernels [ms]. */
 int mcrt_last_kernel_ms(mcrt_ctx *ctx, double *ms);
 
+/* Per-kernel breakdown of the last wavefront-schedule run (zeros after a
+ * run with another schedule): kernel_ms[4] = summed device time [ms] of the
+ * walk, event, tail and peel-off launches (CUDA events on the engine's
+ * stream); counts[6] = launches of each of those four, walks stepped by the
+ * walk launches, cell crossings stepped by the walk launches.  No reference
+ * counterpart (profiling aid). */
+int mcrt_wave_stats(mcrt_ctx *ctx, double *kernel_ms, int64_t *counts);
+
 /* Measurement support: record CUDA event `slot` (0..15) on the context's
  * stream, and the device time between two recorded events [ms]. */
 int mcrt_mark(mcrt_ctx *ctx, int32_t slot);

@@ -64,8 +64,13 @@ struct mcrt_ctx {
   WaveRec *d_recs = nullptr;
   int32_t *d_walkq = nullptr, *d_evq = nullptr;
   WaveCtl *d_wctl = nullptr;
-  unsigned long long *h_wctl = nullptr;   // pinned: n_front, n_back, peel jobs
+  unsigned long long *h_wctl = nullptr;   // pinned: n_front, n_back, packets started, peel jobs, walks, crossings
   int64_t last_waves = 0;
+  // device time per kernel class of the last wavefront run: walk, event, tail, peel-off
+  cudaEvent_t kt_ev[4][2] = {};
+  bool kt_pending[4] = {};
+  double kt_ms[4] = {};
+  int64_t kt_walks = 0, kt_walk_cross = 0, kt_launch[4] = {};
   bool have_grid = false, have_tables = false;
   std::string err;
   cudaStream_t stream = nullptr;
@@ -384,6 +389,8 @@ void mcrt_destroy(mcrt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->h_wctl) cudaFreeHost(ctx->h_wctl);
+  for (auto& p : ctx->kt_ev)
+    for (auto& e : p) if (e) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (auto& e : ctx->marks) if (e) cudaEventDestroy(e);
@@ -720,19 +727,51 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   if (wave && !ctx->d_wctl) {
     int rc = dalloc(ctx, &ctx->d_wctl, 1);
     if (rc) return rc;
-    CK(cudaHostAlloc((void**)&ctx->h_wctl, 4 * sizeof(unsigned long long), cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&ctx->h_wctl, 6 * sizeof(unsigned long long), cudaHostAllocDefault));
+    for (auto& p : ctx->kt_ev)
+      for (auto& e : p) CK(cudaEventCreate(&e));
   }
   P.jobs = queue ? ctx->d_jobs : nullptr;
   P.njobs = ctx->d_next + 1;
   P.job_cap = ctx->job_cap;
   const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
   int64_t launches = 0;                     // kernels this call launches (MCRT_C_LAUNCHES)
+  // device time per kernel class (wavefront schedule): events around each
+  // launch, read back at the next host synchronisation
+  enum { KT_WALK = 0, KT_EVENT = 1, KT_TAIL = 2, KT_PEEL = 3 };
+  if (wave) {
+    for (int k = 0; k < 4; ++k) { ctx->kt_ms[k] = 0.0; ctx->kt_pending[k] = false; ctx->kt_launch[k] = 0; }
+    ctx->kt_walks = ctx->kt_walk_cross = 0;
+  }
+  auto kt_begin = [&](int k) -> int {
+    if (wave) CK(cudaEventRecord(ctx->kt_ev[k][0], ctx->stream));
+    return MCRT_OK;
+  };
+  auto kt_end = [&](int k) -> int {
+    if (!wave) return MCRT_OK;
+    CK(cudaEventRecord(ctx->kt_ev[k][1], ctx->stream));
+    ctx->kt_pending[k] = true;
+    ++ctx->kt_launch[k];
+    return MCRT_OK;
+  };
+  auto kt_collect = [&]() -> int {        // after a host synchronisation
+    for (int k = 0; k < 4; ++k) {
+      if (!ctx->kt_pending[k]) continue;
+      float f = 0.f;
+      CK(cudaEventElapsedTime(&f, ctx->kt_ev[k][0], ctx->kt_ev[k][1]));
+      ctx->kt_ms[k] += f;
+      ctx->kt_pending[k] = false;
+    }
+    return MCRT_OK;
+  };
   auto launch_peel = [&]() -> int {
     ++launches;
+    int rc = kt_begin(KT_PEEL);
+    if (rc) return rc;
     cudaError_t e = mixed ? launch_peel_mixed(P, ctx->d_next + 2, peel_grid, ctx->stream)
                           : launch_peel_fp64(P, ctx->d_next + 2, peel_grid, ctx->stream);
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
-    return MCRT_OK;
+    return kt_end(KT_PEEL);
   };
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (wave) {
@@ -762,19 +801,28 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     // packet ends after at most 1e8 events (the event watchdog)
     const int64_t max_waves = 400000000;
     int64_t waves = 0;
-    unsigned long long* h = ctx->h_wctl;      // n_front, n_back, packets started, peel jobs
+    // h: n_front, n_back, packets started, peel jobs, walks of this wave, walk crossings so far
+    unsigned long long* h = ctx->h_wctl;
+    int rc;
     for (;;) {
       CK(cudaMemsetAsync(&ctx->d_wctl->n_walk, 0, 2 * sizeof(unsigned long long), ctx->stream));
+      if ((rc = kt_begin(KT_EVENT))) return rc;
       e = mixed ? launch_wave_event_mixed(P, W, egrid, ctx->stream) : launch_wave_event_fp64(P, W, egrid, ctx->stream);
       if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave event launch: %s", cudaGetErrorString(e));
+      if ((rc = kt_end(KT_EVENT))) return rc;
       CK(cudaMemsetAsync(&ctx->d_wctl->n_front, 0, 3 * sizeof(unsigned long long), ctx->stream));
+      if ((rc = kt_begin(KT_WALK))) return rc;
       e = mixed ? launch_wave_walk_mixed(P, W, wgrid, ctx->stream) : launch_wave_walk_fp64(P, W, wgrid, ctx->stream);
       if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave walk launch: %s", cudaGetErrorString(e));
+      if ((rc = kt_end(KT_WALK))) return rc;
       ++waves;
       launches += 2;
       CK(cudaMemcpyAsync(h, &ctx->d_wctl->n_front, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaMemcpyAsync(h + 2, ctx->d_next, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaMemcpyAsync(h + 4, &ctx->d_wctl->n_walk, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
+      if ((rc = kt_collect())) return rc;
+      ctx->kt_walks += (int64_t)h[4];
       const unsigned long long live = h[0] + h[1];
 #ifdef MCRT_WAVE_TRACE
       fprintf(stderr, "wave %lld live %llu interactions %llu started %llu jobs %llu\n", (long long)waves, live, h[0],
@@ -785,25 +833,27 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
       const bool tail = tail_live > 0 && (int64_t)h[2] >= npk && live <= tail_live;
       if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && h[3] > 0))) {
         CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
-        int rc = launch_peel();
-        if (rc) return rc;
+        if ((rc = launch_peel())) return rc;
         CK(cudaMemsetAsync(ctx->d_next + 1, 0, sizeof(unsigned long long), ctx->stream));
       }
       if (tail) {
         LaunchParams T = P;
         T.fetch_off = 1;
         CK(cudaMemsetAsync(&ctx->d_wctl->n_walk, 0, 2 * sizeof(unsigned long long), ctx->stream));
+        if ((rc = kt_begin(KT_TAIL))) return rc;
         e = mixed ? launch_wave_tail_mixed(T, W, tgrid, ctx->stream) : launch_wave_tail_fp64(T, W, tgrid, ctx->stream);
         if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave tail launch: %s", cudaGetErrorString(e));
+        if ((rc = kt_end(KT_TAIL))) return rc;
         ++launches;
         break;
       }
     }
     if (queue) {
       CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
-      int rc = launch_peel();
-      if (rc) return rc;
+      if ((rc = launch_peel())) return rc;
     }
+    CK(cudaMemcpyAsync(h + 5, &ctx->d_wctl->walk_cross, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       ctx->stream));
     ctx->last_waves = waves;
   }
   int per_sm = wave ? 1 : ctx->precision == MCRT_PREC_FP64
@@ -841,6 +891,11 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->last_ms = ms;
+  if (wave) {
+    int rc = kt_collect();
+    if (rc) return rc;
+    ctx->kt_walk_cross = (int64_t)ctx->h_wctl[5];
+  }
   CK(cudaGetLastError());
   return MCRT_OK;
 }
@@ -875,6 +930,17 @@ int mcrt_synchronize(mcrt_ctx* ctx) {
   if (!ctx) return MCRT_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_wave_stats(mcrt_ctx* ctx, double* kernel_ms, int64_t* counts) {
+  if (!ctx || !kernel_ms || !counts) return MCRT_ERR_ARG;
+  for (int k = 0; k < 4; ++k) {
+    kernel_ms[k] = ctx->kt_ms[k];
+    counts[k] = ctx->kt_launch[k];
+  }
+  counts[4] = ctx->kt_walks;
+  counts[5] = ctx->kt_walk_cross;
   return MCRT_OK;
 }
 

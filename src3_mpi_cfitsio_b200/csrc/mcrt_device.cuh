@@ -122,7 +122,8 @@ static_assert(sizeof(WaveRec) % 16 == 0, "WaveRec must keep 16-byte alignment");
 // ends by the walk kernel: interactions from the front, every other event
 // from the back, so the event kernel's warps see one kind of event at a time.
 struct WaveCtl {
-  unsigned long long n_front, n_back, walk_fetch, pad0;   // zeroed before each walk launch
+  unsigned long long n_front, n_back, walk_fetch;         // zeroed before each walk launch
+  unsigned long long walk_cross;                          // crossings stepped by walk launches (whole loop)
   unsigned long long n_walk, ev_fetch, pad1, pad2;        // zeroed before each event launch
 };
 

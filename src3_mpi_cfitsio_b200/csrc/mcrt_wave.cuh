@@ -168,6 +168,7 @@ __global__ void wave_init(WaveArgs W) {
     c.n_front = 0;
     c.n_back = (unsigned long long)n;
     c.walk_fetch = 0;
+    c.walk_cross = 0;
     c.n_walk = 0;
     c.ev_fetch = 0;
   }
@@ -273,6 +274,10 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
     if (front) W.evq[pf] = slot;
     if (back) W.evq[W.slots - 1 - (int64_t)pb] = slot;
     if (done) have = false;
+  }
+  {
+    const unsigned long long x = warp_sum(L.pk.c_cross);
+    if (lane == 0 && x) atomicAdd(&W.ctl->walk_cross, x);
   }
   flush_counters(P, L);
 }

@@ -56,6 +56,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_enable_packet_log.argtypes = [C.c_void_p, C.c_int64]
     lib.mcrt_download_packet_log.argtypes = [C.c_void_p, P(abi.PacketLog), C.c_int64]
     lib.mcrt_last_kernel_ms.argtypes = [C.c_void_p, P(C.c_double)]
+    lib.mcrt_wave_stats.argtypes = [C.c_void_p, P(C.c_double), P(C.c_int64)]
     lib.mcrt_mark.argtypes = [C.c_void_p, C.c_int32]
     lib.mcrt_elapsed_ms.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]
     lib.mcrt_flush_l2.argtypes = [C.c_void_p]
@@ -68,7 +69,7 @@ def load_library(path: str = LIB_PATH):
     for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision", "mcrt_set_schedule",
                  "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
-                 "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_mark", "mcrt_elapsed_ms",
+                 "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
                  "mcrt_flush_l2", "mcrt_synchronize"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -153,6 +154,18 @@ class Engine:
         v = C.c_double()
         self._check(self.lib.mcrt_last_kernel_ms(self.ctx, C.byref(v)))
         return v.value
+
+    def wave_stats(self) -> dict:
+        """Per-kernel device time and counts of the last wavefront run."""
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 6)()
+        self._check(self.lib.mcrt_wave_stats(self.ctx, ms, n))
+        names = ("walk", "event", "tail", "peel")
+        out = {f"{k}_ms": ms[i] for i, k in enumerate(names)}
+        out.update({f"{k}_launches": n[i] for i, k in enumerate(names)})
+        out["walks"] = n[4]
+        out["walk_crossings"] = n[5]
+        return out
 
     def mark(self, slot: int):
         self._check(self.lib.mcrt_mark(self.ctx, slot))
