@@ -151,10 +151,20 @@ def run_ours(args, rank, world):
         tdist.all_reduce(t, op=tdist.ReduceOp.SUM if op == "sum" else tdist.ReduceOp.MAX)
         return t.cpu().numpy()
 
+    def reduce_ranks(e):
+        """The rank reduction of the tallies: NCCL all-reduce of the device
+        tally buffer in place, then the diffusion refresh from the summed
+        counts (newdisktherm_5_fuv.f90:520-604)."""
+        if dist:
+            from src3_mpi_cfitsio_b200 import dist as mdist
+            mdist.allreduce_device_tallies(e, device=dev)
+            e.refresh_diffusion()
+
     def step(it, e, precision=None):
         e.reset_tallies()
         e.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
         kms = e.kernel_ms()
+        reduce_ranks(e)
         e.update_temperature(np_total, it)
         return kms
 
@@ -175,6 +185,7 @@ def run_ours(args, rank, world):
             kernel_ms.append(eng.kernel_ms())
             if args.schedule == "wave":
                 wave_stats_last = eng.wave_stats()
+            reduce_ranks(eng)
             eng.update_temperature(np_total, it)
             if s + 1 < args.steps:
                 eng.flush_l2()
@@ -201,8 +212,8 @@ def run_ours(args, rank, world):
     eng.upload_grid()
     eng.reset_tallies()
     eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+    reduce_ranks(eng)
     tl = eng.download(images=bool(args.ipeel))
-    tl.arrays["dtauabs"][:] = allreduce(tl["dtauabs"])
     td, _, _ = eng.update_temperature(np_total, it)
     eng.mark(5)
     eng.synchronize()

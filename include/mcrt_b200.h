@@ -253,9 +253,33 @@ int mcrt_run_iteration(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo,
  * newdisktherm_5_fuv.f90:520-604 for a single GPU). */
 int mcrt_download_tallies(mcrt_ctx *ctx, mcrt_tallies *out);
 
-/* Add a tally set from another process into this context's device tallies
- * (the summing half of MPI_ALLREDUCE for multi-process runs). */
+/* Add a tally set (host arrays, the layout mcrt_download_tallies writes)
+ * into this context's device tallies: the summing half of the rank
+ * reduction newdisktherm_5_fuv.f90:520-604 when the ranks reduce on the host
+ * (download, sum across processes, mcrt_reset_tallies, accumulate the sum).
+ * NULL members are skipped.  The diffusion absorption counts are not part of
+ * mcrt_tallies; reduce through mcrt_device_tallies_view to include them. */
 int mcrt_accumulate_tallies(mcrt_ctx *ctx, const mcrt_tallies *in);
+
+/* The device tally buffer as three contiguous segments, for an in-place
+ * all-reduce across GPUs (NCCL sum) -- the MPI_ALLREDUCE block of
+ * newdisktherm_5_fuv.f90:520-604 without a host round trip.  Sum every
+ * segment over the ranks, then call mcrt_refresh_diffusion and
+ * mcrt_update_temperature.  Pointers are device addresses owned by the
+ * context and valid until mcrt_destroy. */
+typedef struct mcrt_device_tallies {
+  double   *f64;  int64_t n_f64;  /* dtauabs, fuvmean, SEDs, peeled SEDs, images, scalars */
+  uint64_t *u64;  int64_t n_u64;  /* counters                                            */
+  int32_t  *i32;  int64_t n_i32;  /* nabs, dbig, dsg, killed, diffusion absorption counts */
+} mcrt_device_tallies;
+int mcrt_device_tallies_view(mcrt_ctx *ctx, mcrt_device_tallies *out);
+
+/* Recompute the diffusion cells' end-of-iteration temperature of the last
+ * mcrt_run_iteration from the (reduced) diffusion absorption counts and the
+ * whole iteration's stellar packet count -- the single-process result of
+ * emit_common_2.f90:260-339; each rank's packets were emitted with its own
+ * counts, as each MPI rank heats a private copy in the reference. */
+int mcrt_refresh_diffusion(mcrt_ctx *ctx);
 
 /* Lucy temperature update on the device: tfinal(nphot,iter,converge)
  * (tfinal_5_test1.f90:1-447) with dusttemp (dusttemp_5.f90:8-152).

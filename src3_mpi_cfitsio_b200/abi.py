@@ -86,6 +86,12 @@ class PacketLog(C.Structure):
         "nub", "cost", "phi", "sip", "sqp", "sup", "svp", "xp", "yp", "zp")]
 
 
+class DeviceTallies(C.Structure):
+    """mcrt_device_tallies: device addresses of the three tally segments."""
+    _fields_ = [("f64", C.c_void_p), ("n_f64", C.c_int64), ("u64", C.c_void_p), ("n_u64", C.c_int64),
+                ("i32", C.c_void_p), ("n_i32", C.c_int64)]
+
+
 def _ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
@@ -155,6 +161,18 @@ class TallyArrays:
 
     def __getitem__(self, k):
         return self.arrays[k]
+
+    def add_(self, other: "TallyArrays"):
+        """Sum another tally set into this one in place (the struct keeps
+        pointing at the same arrays): integers and FP64 exactly, the REAL
+        arrays in FP64 with one rounding."""
+        for k, a in self.arrays.items():
+            b = other.arrays[k]
+            if a.dtype == np.float32:
+                a[:] = (a.astype(np.float64) + b).astype(np.float32)
+            else:
+                a += b
+        return self
 
     def scalars(self) -> dict:
         return dict(zip(SCALARS, self.arrays["scalars"].tolist()))

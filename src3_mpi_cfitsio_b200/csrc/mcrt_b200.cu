@@ -86,6 +86,9 @@ struct mcrt_ctx {
   double *d_tdust = nullptr, *d_vcell = nullptr;
   double *d_tdust0 = nullptr;         // tdust at the start of the iteration (read by the transport)
   double last_nphot_diff = 1.0;
+  DevModel last_m{};                  // model view of the last run (mcrt_refresh_diffusion)
+  bool have_last_run = false;
+  double last_ns = 0.0;               // stellar packets of the whole iteration of the last run
   double *d_dens_thermal = nullptr;   // [ncell] density of the thermal component (tfinal)
   int32_t *d_idust3 = nullptr;        // [ncell] its opacity species (0 = none)
   int32_t *d_diffus = nullptr;
@@ -313,6 +316,18 @@ __global__ void tfinal_stats(int nrg, int ntg, const double* told, const double*
 // the library holds it (3*524288+16 doubles, 12 MiB) on each device it uses.
 constexpr int64_t kNoAllocMaxCells = 524288;
 static __device__ __align__(256) double g_tfinal_scratch[3 * kNoAllocMaxCells + 16];
+
+// dst[i] += src[i]; kind 0: f64 -> f64, 1: i64 -> u64, 2: f32 -> f64, 3: i32 -> i32
+__global__ void add_tally(int kind, const void* src, void* dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    switch (kind) {
+      case 0: ((double*)dst)[i] += ((const double*)src)[i]; break;
+      case 1: ((unsigned long long*)dst)[i] += (unsigned long long)((const long long*)src)[i]; break;
+      case 2: ((double*)dst)[i] += (double)((const float*)src)[i]; break;
+      default: ((int32_t*)dst)[i] += ((const int32_t*)src)[i]; break;
+    }
+  }
+}
 
 __global__ void add_counters(unsigned long long* cnt, unsigned long long waves, unsigned long long launches) {
   cnt[MCRT_C_WAVES] += waves;
@@ -677,6 +692,7 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   P.ipeel = ipeel ? 1 : 0;
   P.nphot_diff = (double)ns * (double)(hi - lo + 1) / (double)np;
   ctx->last_nphot_diff = P.nphot_diff;
+  ctx->last_ns = (double)ns;
   P.ips = (c.rddust > 100.0) ? 1 : 0;
   P.g1 = (int32_t)g1; P.g2 = (int32_t)g2;
   P.next = ctx->d_next;
@@ -891,6 +907,8 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->last_ms = ms;
+  ctx->last_m = P.m;
+  ctx->have_last_run = true;
   if (wave) {
     int rc = kt_collect();
     if (rc) return rc;
@@ -990,8 +1008,68 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
 }
 
 int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
-  (void)in;
-  return fail(ctx, MCRT_ERR_UNSUPPORTED, "mcrt_accumulate_tallies: use the device-side all-reduce path");
+  if (!ctx || !in) return MCRT_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  const DevTallies& t = ctx->dt;
+  const int64_t nc = ctx->ncell;
+  const int64_t nmax = std::max<int64_t>(std::max<int64_t>(nc, MCRT_NCOUNTERS),
+                                         std::max(ctx->nsed, std::max(ctx->npsed, ctx->nimg)));
+  void* d_in = nullptr;
+  int rc = dalloc(ctx, (char**)&d_in, (size_t)nmax * 8);
+  if (rc) return rc;
+  const int grid = (int)std::min<int64_t>((nmax + 255) / 256, 4096);
+  // one host array: copy it to the staging buffer and add it to its device tally
+  auto add = [&](const void* h, int kind, void* dst, int64_t n) -> int {
+    if (!h || n == 0) return MCRT_OK;
+    const size_t esz = (kind == 2) ? 4 : (kind == 3 ? 4 : 8);
+    cudaError_t e = cudaMemcpyAsync(d_in, h, (size_t)n * esz, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "accumulate copy: %s", cudaGetErrorString(e));
+    add_tally<<<grid, 256, 0, ctx->stream>>>(kind, d_in, dst, n);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "accumulate launch: %s", cudaGetErrorString(e));
+    e = cudaStreamSynchronize(ctx->stream);     // the staging buffer is reused by the next array
+    if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "accumulate: %s", cudaGetErrorString(e));
+    return MCRT_OK;
+  };
+  // kinds: 0 f64 -> f64, 1 i64 -> u64, 2 f32 -> f64, 3 i32 -> i32
+  const float* sed[10] = {in->si, in->sq, in->su, in->sv, in->si2, in->sq2, in->su2, in->sv2, in->nums, in->aveinc};
+  const float* ps[9] = {in->ti, in->tq, in->tu, in->tv, in->ti2, in->tq2, in->tu2, in->tv2, in->numt};
+  const float* im[4] = {in->image_m_i, in->image_m_q, in->image_m_u, in->image_m_v};
+  if ((rc = add(in->nabs, 3, t.nabs, nc)) || (rc = add(in->dbig, 3, t.dbig, nc)) || (rc = add(in->dsg, 3, t.dsg, nc)) ||
+      (rc = add(in->killed, 3, t.killed, nc)) || (rc = add(in->dtauabs, 0, t.dtauabs, nc)) ||
+      (rc = add(in->fuvmean, 0, t.fuvmean, nc)) || (rc = add(in->scalars, 0, t.scal, MCRT_NSCALARS)) ||
+      (rc = add(in->counters, 1, t.cnt, MCRT_NCOUNTERS))) {
+    dfree(ctx, d_in);
+    return rc;
+  }
+  for (int k = 0; k < 10 && !rc; ++k) rc = add(sed[k], 2, t.sed + k * ctx->nsed, ctx->nsed);
+  for (int k = 0; k < 9 && !rc; ++k) rc = add(ps[k], 2, t.psed + k * ctx->npsed, ctx->npsed);
+  for (int k = 0; k < 4 && !rc; ++k) rc = add(im[k], 2, t.img + k * ctx->nimg, ctx->nimg);
+  dfree(ctx, d_in);
+  return rc;
+}
+
+int mcrt_device_tallies_view(mcrt_ctx* ctx, mcrt_device_tallies* out) {
+  if (!ctx || !out) return MCRT_ERR_ARG;
+  const int64_t nc = ctx->ncell;
+  out->f64 = ctx->dt.dtauabs;                 // first member of the allocation
+  out->n_f64 = 2 * nc + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + MCRT_NSCALARS;
+  out->u64 = (uint64_t*)ctx->dt.cnt;
+  out->n_u64 = MCRT_NCOUNTERS;
+  out->i32 = ctx->dt.nabs;
+  out->n_i32 = 5 * nc;                        // nabs, dbig, dsg, killed, ndiff
+  return MCRT_OK;
+}
+
+int mcrt_refresh_diffusion(mcrt_ctx* ctx) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (!ctx->have_last_run) return fail(ctx, MCRT_ERR_STATE, "mcrt_refresh_diffusion before any mcrt_run_iteration");
+  CK(cudaSetDevice(ctx->device));
+  cudaError_t e = launch_diffusion_finalize(ctx->last_m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust,
+                                            std::max(ctx->last_ns, 1.0), ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion refresh: %s", cudaGetErrorString(e));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return MCRT_OK;
 }
 
 int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* tdave, int32_t* converge, double* sig) {

@@ -57,6 +57,8 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_download_packet_log.argtypes = [C.c_void_p, P(abi.PacketLog), C.c_int64]
     lib.mcrt_last_kernel_ms.argtypes = [C.c_void_p, P(C.c_double)]
     lib.mcrt_wave_stats.argtypes = [C.c_void_p, P(C.c_double), P(C.c_int64)]
+    lib.mcrt_device_tallies_view.argtypes = [C.c_void_p, P(abi.DeviceTallies)]
+    lib.mcrt_refresh_diffusion.argtypes = [C.c_void_p]
     lib.mcrt_mark.argtypes = [C.c_void_p, C.c_int32]
     lib.mcrt_elapsed_ms.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]
     lib.mcrt_flush_l2.argtypes = [C.c_void_p]
@@ -70,6 +72,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
+                 "mcrt_device_tallies_view", "mcrt_refresh_diffusion",
                  "mcrt_flush_l2", "mcrt_synchronize"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -185,6 +188,20 @@ class Engine:
         tal = abi.TallyArrays(self.cfg, images=images)
         self._check(self.lib.mcrt_download_tallies(self.ctx, C.byref(tal.struct)))
         return tal
+
+    def accumulate(self, tal: abi.TallyArrays):
+        """Add host tallies (e.g. the sum over ranks) into the device tallies."""
+        self._check(self.lib.mcrt_accumulate_tallies(self.ctx, C.byref(tal.struct)))
+
+    def device_tallies(self) -> abi.DeviceTallies:
+        """Device addresses and lengths of the tally segments (in-place all-reduce)."""
+        v = abi.DeviceTallies()
+        self._check(self.lib.mcrt_device_tallies_view(self.ctx, C.byref(v)))
+        return v
+
+    def refresh_diffusion(self):
+        """Diffusion-cell temperatures of the last run from the (reduced) counts."""
+        self._check(self.lib.mcrt_refresh_diffusion(self.ctx))
 
     def enable_packet_log(self, n: int):
         self._check(self.lib.mcrt_enable_packet_log(self.ctx, n))
