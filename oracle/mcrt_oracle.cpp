@@ -1150,14 +1150,111 @@ struct Packet {
     return 0;
   }
 
+  // initpacc_4.f90:19-99 with emit_common: a disk-accretion packet.  The
+  // radius comes once from the luminosity CDF Ldint (locate, cell centre
+  // ravearr); the azimuth (rantheta, random.f90:23-42) and the height
+  // hdisk*gasdev (random.f90:119-138, polar Box-Muller keeping its second
+  // deviate) are redrawn until the point lies in a cell with thermal dust
+  // (initpacc_4.f90:22, goto 11).  Two choices of this restatement, shared
+  // with the engine: gasdev's saved deviate belongs to the packet (the
+  // reference carries it from one packet to the next of a rank's single
+  // stream; packets here use independent streams), and a point outside the
+  // grid is redrawn (the reference would index past its arrays).  The
+  // reference's dsg/dbig/nabs rules (:83-97) reduce to dbig and nabs for the
+  // selected thermal component.  Returns idust2, or 0 on failure.
+  int accretion_emission(int* ii) {
+    const mcrt_grid* g = m->g;
+    const int nrg = m->nrg;
+    const double xi = ran();
+    int r0 = locate(g->Ldint, nrg - 1, xi);
+    r0 = std::min(std::max(r0, 1), nrg - 1);
+    const double rp = g->ravearr[r0 - 1], hd = g->hdisk[r0 - 1];
+    bool have_g = false, found = false;
+    double gsave = 0.0;
+    int ir = 0, it = 0, ip = 0;
+    for (int tries = 0; tries < 1000000 && !found; ++tries) {
+      double x = 0.0, y = 0.0, r2 = 2.0;
+      while (r2 > 1.0) {
+        x = ran(); x = x + x - 1.0;
+        y = ran(); y = y + y - 1.0;
+        r2 = x * x + y * y;
+      }
+      const double rr = std::sqrt(r2);
+      const double st = y / rr, ct = x / rr;
+      xp = rp * ct;
+      yp = rp * st;
+      double gd;
+      if (!have_g) {
+        double v1, v2, q;
+        do {
+          v1 = 2.0 * ran() - 1.0;
+          v2 = 2.0 * ran() - 1.0;
+          q = v1 * v1 + v2 * v2;
+        } while (!(q < 1.0 && q > 0.0));
+        const double fac = std::sqrt(-2.0 * std::log(q) / q);
+        gsave = v1 * fac;
+        gd = v2 * fac;
+        have_g = true;
+      } else {
+        gd = gsave;
+        have_g = false;
+      }
+      zp = hd * gd;
+      sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+      rsq = xp * xp + yp * yp + zp * zp;
+      rtot = std::sqrt(rsq);
+      ir = locate(m->r2arr.data(), nrg, rsq);
+      cosb = zp / rtot;
+      it = locate(m->costarr.data(), m->ntg, cosb);
+      lp = std::atan2(yp, xp);
+      if (lp < 0.0) lp = lp + R2P;
+      ip = locate(m->phiarr.data(), m->npg, lp);
+      if (ir < 1 || ir > nrg - 1 || it < 1 || it > m->ntg - 1 || ip < 1 || ip > m->npg - 1) continue;
+      double th = 0.0;
+      for (int id = 1; id <= MCRT_NDG2; ++id) if (!m->is_sg[id - 1]) th += m->dens(ir, it, ip, id);
+      found = th > 0.0;
+    }
+    if (!found) return 0;
+    int idust2 = select_thermal(ir, it, ip);
+    if (idust2 == 0) return 0;
+    const int64_t cc = m->cidx(ir, it, ip);
+    T->dbig[cc]++;
+    T->nabs[cc]++;
+    ii[0] = ir; ii[1] = it; ii[2] = ip;
+    if (!m->g->diffus[cc]) {               // emit_common, thermal branch: reemit.f90 + lucydustfreq
+      const double tave = m->g->tdust[cc];
+      sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+      cost = 1.0 - 2.0 * ran();
+      sint = std::sqrt(1.0 - cost * cost);
+      phi = R2P * ran();
+      cosp = std::cos(phi);
+      sinp = std::sin(phi);
+      nub = lucydustfreq(tave, m->fopac(ir, it, ip, idust2));
+      uy = sint * sinp;
+      ux = sint * cosp;
+      uz = cost;
+    } else {
+      ++ndiffev;
+      if (!emit_diffusion(ir, it, ip, idust2)) return 0;
+      ii[1] = it;
+    }
+    return idust2;
+  }
+
   // ----------------------------------------------------------- packet
   // newdisktherm_5_fuv.f90:220-491 for one packet, then propagate
   int run(int64_t iphot, int64_t np, int64_t ns, int64_t npacc, int64_t npaccstar, int ips) {
     const mcrt_config& c = m->c;
     on_wall = false;
     int ii[3] = {0, 0, 0};
-    if (iphot < npacc) {
-      return -1;   // disk-accretion packets need the diffusion/accretion tables: rejected up front
+    if (iphot < npacc) {                    // disk accretion, newdisktherm_5_fuv.f90:238-287
+      const int idust2 = accretion_emission(ii);
+      if (idust2 == 0) return 3;
+      opacset(nub);
+      kapd_disk();
+      iflag = 0;
+      i_orig = 2;
+      if (ipeel == 1) peel_all(sip, ii[0], ii[1], ii[2], idust2);
     } else if (iphot <= npacc + ns) {
       if (iphot < npacc + npaccstar) {
         if (ips == 0) initpspot(1); else initp_ps(1);
@@ -1377,7 +1474,8 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   int64_t npaccstar = (int64_t)(cfg->accfrac2 * (double)np);
   int64_t nsum = ns + npacc + npout;
   if (nsum != np) ns = ns + np - nsum;
-  if (npacc > 1 || npout > 0) return MCRT_ERR_UNSUPPORTED;
+  if (npout > 0) return MCRT_ERR_UNSUPPORTED;
+  if (npacc > 1 && (!grid->ravearr || !grid->Ldint || !grid->hdisk)) return MCRT_ERR_ARG;
   // emit_common receives nphot = ns of the (rank's) run; a shard uses its share
   m.nphot_diff = (double)ns * (double)(iphot_hi - iphot_lo + 1) / (double)np;
   int ips = (cfg->rddust > 100.0) ? 1 : 0;

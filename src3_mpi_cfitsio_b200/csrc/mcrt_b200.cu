@@ -72,6 +72,7 @@ struct mcrt_ctx {
   double kt_ms[4] = {};
   int64_t kt_walks = 0, kt_walk_cross = 0, kt_launch[4] = {};
   bool have_grid = false, have_tables = false;
+  bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
   std::string err;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -510,6 +511,20 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   addp(g->phiarr, npg, g->phiarr[npg - 1]);
   addp(g->aarr, npg, g->aarr[npg - 1]);
   addp(g->barr, npg, g->barr[npg - 1]);
+  // disk-accretion emission tables (initpacc_4.f90:28-36), [nrg-1] each;
+  // optional: absent, accretion packets are refused at run time
+  const bool acc = g->ravearr && g->Ldint && g->hdisk;
+  if (acc) {
+    for (int i = 1; i < nrg - 1; ++i)
+      if (!(g->Ldint[i] >= g->Ldint[i - 1])) return fail(ctx, MCRT_ERR_ARG, "Ldint must be non-decreasing");
+    for (int i = 0; i < nrg - 1; ++i)
+      if (!(g->hdisk[i] >= 0.0) || !(g->ravearr[i] > 0.0)) return fail(ctx, MCRT_ERR_ARG, "ravearr/hdisk must be positive");
+  }
+  const std::vector<double> zeros(nrg > 1 ? nrg - 1 : 1, 0.0);
+  addp(acc ? g->ravearr : zeros.data(), nrg - 1, 0.0);
+  addp(acc ? g->Ldint : zeros.data(), nrg - 1, 1.0);
+  addp(acc ? g->hdisk : zeros.data(), nrg - 1, 0.0);
+  ctx->have_acc = acc;
   ctx->h_rarr.assign(g->rarr, g->rarr + nrg);
   if (!ctx->have_grid) {
     int rc;
@@ -541,7 +556,10 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   m.sintarr = w; w += ntg + 1;
   m.phiarr = w; w += npg + 1;
   m.aarr = w; w += npg + 1;
-  m.barr = w;
+  m.barr = w; w += npg + 1;
+  m.ravearr = w; w += nrg;
+  m.Ldint = w; w += nrg;
+  m.hdisk = w;
   m.cells = ctx->d_cells;
   m.tdust = ctx->d_tdust0;
   m.vcell = ctx->d_vcell;
@@ -666,7 +684,8 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   int64_t npaccstar = (int64_t)(c.accfrac2 * (double)np);
   const int64_t nsum = ns + npacc + npout;
   if (nsum != np) ns = ns + np - nsum;
-  if (npacc > 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "disk-accretion packets (initpacc) are outside the built scope");
+  if (npacc > 1 && !ctx->have_acc)
+    return fail(ctx, MCRT_ERR_ARG, "accretion packets (accfrac > 0) need ravearr, Ldint and hdisk in mcrt_upload_grid");
   if (npout > 0) return fail(ctx, MCRT_ERR_UNSUPPORTED, "external-illumination packets (initpout) are outside the built scope");
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;

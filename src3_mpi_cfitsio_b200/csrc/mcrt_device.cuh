@@ -61,6 +61,8 @@ struct DevModel {
   double cspot1, sspot1, scspot1, ssspot1, cspot2, sspot2, scspot2, ssspot2, csprad;
   // walls
   const double *rarr, *r2arr, *thetarr, *costarr, *tan2arr, *phiarr, *aarr, *barr, *sintarr;
+  // disk-accretion emission (initpacc): cell-centre radii, luminosity CDF, scale heights [nrg-1]
+  const double *ravearr, *Ldint, *hdisk;
   // cells
   const CellRec *cells;
   const double *tdust, *vcell;              // tdust: start-of-iteration values

@@ -38,7 +38,7 @@ enum Ev : int {
   EV_STAR,           // packet walk reached the stellar surface (wavefront walk only)
   EV_DONE            // no packets left for this lane
 };
-enum PeelCtx : int { PC_DIRECT = 0, PC_SCATTER = 1, PC_ABSORB = 2 };
+enum PeelCtx : int { PC_DIRECT = 0, PC_SCATTER = 1, PC_ABSORB = 2, PC_ACCRETION = 3 };
 
 struct Ray {
   double x, y, z, rs, rt, vx, vy, vz, tsum;
@@ -297,7 +297,21 @@ struct Lane {
           pk.on_wall = false;
           pk.nscat = pk.nabsev = pk.ncross = pk.nstar = pk.ndiffev = 0;
           status = 0;
-          if (iphot < P.npacc || iphot > P.npacc + P.ns) { status = 3; ev = EV_FINISH; break; }
+          if (iphot > P.npacc + P.ns) { status = 3; ev = EV_FINISH; break; }   // external illumination: refused at launch
+          if (iphot < P.npacc) {            // disk accretion, newdisktherm_5_fuv.f90:238-287
+            const int idust2 = pk.accretion_emission(P);
+            if (idust2 < 0) { status = 3; ev = EV_FINISH; break; }
+            pk.opacset(pk.nub, KAPD_DISK);
+            pk.iflag = 0;
+            pk.i_orig = 2;
+            if (P.ipeel == 1 && !push_job(P, PC_ACCRETION, idust2)) {
+              peel_ctx = PC_ACCRETION; peelid = 0; peel_idust2 = idust2;
+              ev = EV_PEEL_NEXT;
+            } else {
+              ev = EV_PROP_START;
+            }
+            break;
+          }
           // newdisktherm_5_fuv.f90:295-366
           if (iphot < P.npacc + P.npaccstar) {
             if (P.ips == 0) pk.initpspot(1); else pk.initp_ps(1);
@@ -355,7 +369,8 @@ struct Lane {
             started = peel_setup(peelid);
           }
           if (started) return;
-          ev = (peel_ctx == PC_DIRECT) ? EV_PROP_START : (peel_ctx == PC_SCATTER ? EV_SCATTER_DONE : EV_ABSORB_DONE);
+          ev = (peel_ctx == PC_DIRECT || peel_ctx == PC_ACCRETION) ? EV_PROP_START
+               : (peel_ctx == PC_SCATTER ? EV_SCATTER_DONE : EV_ABSORB_DONE);
           break;
         }
         case EV_PEEL_BIN:
@@ -411,23 +426,8 @@ struct Lane {
             if (idust2 == 1 || idust2 == 2 || idust2 == 5 || idust2 == 6 || idust2 == 9) pk.i_orig = 2;
             else if (idust2 == 3 || idust2 == 7) pk.i_orig = 3;
             else pk.i_orig = 4;
-            if (!cell_diffus(c.flags)) {
-              atomicAdd(pk.T.nabs + ci, 1);
-              const double tave = __ldg(m.tdust + ci);
-              pk.sip = 1.0; pk.sqp = 0.0; pk.sup = 0.0; pk.svp = 0.0;
-              pk.cost = 1.0 - 2.0 * pk.ran();
-              pk.sint = sqrt(1.0 - pk.cost * pk.cost);
-              pk.phi = R2P * pk.ran();
-              pk.cosp = cos(pk.phi);
-              pk.sinp = sin(pk.phi);
-              pk.nub = pk.lucydustfreq(tave, m.slot_species[slot]);
-              pk.uy = pk.sint * pk.sinp;
-              pk.ux = pk.sint * pk.cosp;
-              pk.uz = pk.cost;
-            } else {
-              ++pk.ndiffev;
-              if (!pk.emit_diffusion(P)) { status = 3; ev = EV_FINISH; break; }
-            }
+            if (!cell_diffus(c.flags)) atomicAdd(pk.T.nabs + ci, 1);
+            if (!pk.emit_common(P, ci, c, slot)) { status = 3; ev = EV_FINISH; break; }
             pk.iflag = 0;
             pk.opacset(pk.nub, KAPD_PROPAGATE);
             pk.ifuv = Packet::is_fuv(pk.nub) ? m.ifuv_ori : 0.0;

@@ -29,6 +29,7 @@ constexpr int kBlock = kTransportBlock;
 // watchdog: a packet is killed after this many interactions in total (the
 // reference only kills after 10000 in one cell, propagate_5_fuv.f90:208-213)
 constexpr int64_t kMaxEvents = 100000000;
+constexpr int kMaxAccTries = 1000000;   // accretion emission redraws before the packet is dropped
 
 // --------------------------------------------------------------- RNG ----
 struct Rng {
@@ -1265,10 +1266,124 @@ struct Packet {
   }
 
   // ------------------------------------------------------------ packet
+  // emit_common (emit_common_2.f90:1-384) for the absorbing / emitting cell
+  // ci and its thermal component in species slot `slot`: Lucy reemission
+  // at the cell's temperature (reemit.f90 + lucydustfreq), or, in a
+  // diffusion cell, emission from the diffusion surface.  false = geometry
+  // failure.
+  __device__ bool emit_common(const LaunchParams& P, int64_t ci, const CellRec& c, int slot) {
+    if (!cell_diffus(c.flags)) {
+      const double tave = __ldg(m.tdust + ci);
+      sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90
+      cost = 1.0 - 2.0 * ran();
+      sint = sqrt(1.0 - cost * cost);
+      phi = R2P * ran();
+      cosp = cos(phi);
+      sinp = sin(phi);
+      nub = lucydustfreq(tave, m.slot_species[slot]);
+      uy = sint * sinp;
+      ux = sint * cosp;
+      uz = cost;
+      return true;
+    }
+    ++ndiffev;
+    return emit_diffusion(P);
+  }
+
+  // initpacc_4.f90:19-81: a disk-accretion emission point.  The radius is
+  // drawn once from the luminosity CDF Ldint (cell centre ravearr); the
+  // azimuth (rantheta, random.f90:23-42) and the height hdisk * gasdev
+  // (random.f90:119-138, Box-Muller polar form with its saved second
+  // deviate) are redrawn until the point lies in a cell with thermal dust.
+  // The saved deviate lives in the packet: packets draw from independent
+  // streams here, where the reference passes it from one packet to the
+  // next of its rank's single stream.  Points outside the grid are redrawn
+  // (the reference would index past its arrays).  Returns the thermal
+  // component index in the cell record, or -1 after kMaxAccTries draws.
+  __device__ int initpacc(int64_t& ci) {
+    const double xi = ran();
+    int r0 = locate(m.Ldint, m.nrg - 1, xi);
+    r0 = min(max(r0, 1), m.nrg - 1);
+    const double rp = __ldg(m.ravearr + r0 - 1);
+    const double hd = __ldg(m.hdisk + r0 - 1);
+    bool have_g = false;
+    double gsave = 0.0;
+    for (int tries = 0; tries < kMaxAccTries; ++tries) {
+      double x = 0.0, y = 0.0, r2 = 2.0;
+      while (r2 > 1.0) {
+        x = ran(); x = x + x - 1.0;
+        y = ran(); y = y + y - 1.0;
+        r2 = x * x + y * y;
+      }
+      const double rr = sqrt(r2);
+      const double st = y / rr, ct = x / rr;
+      xp = rp * ct;
+      yp = rp * st;
+      double g;
+      if (!have_g) {
+        double v1, v2, q;
+        do {
+          v1 = 2.0 * ran() - 1.0;
+          v2 = 2.0 * ran() - 1.0;
+          q = v1 * v1 + v2 * v2;
+        } while (!(q < 1.0 && q > 0.0));
+        const double fac = sqrt(-2.0 * log(q) / q);
+        gsave = v1 * fac;
+        g = v2 * fac;
+        have_g = true;
+      } else {
+        g = gsave;
+        have_g = false;
+      }
+      zp = hd * g;
+      sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+      rsq = xp * xp + yp * yp + zp * zp;
+      rtot = sqrt(rsq);
+      ir = locate(m.r2arr, m.nrg, rsq);
+      cosb = zp / rtot;
+      it = locate(m.costarr, m.ntg, cosb);
+      lp = atan2(yp, xp);
+      if (lp < 0.0) lp = lp + R2P;
+      ip = locate(m.phiarr, m.npg, lp);
+      if (ir < 1 || ir > m.nrg - 1 || it < 1 || it > m.ntg - 1 || ip < 1 || ip > m.npg - 1) continue;
+      ci = cidx(ir, it, ip);
+      const CellRec c = m.cells[ci];
+      if (!cell_thermal(c.flags)) continue;
+      return select_thermal(c);
+    }
+    return -1;
+  }
+
+  // initpacc_4.f90:83-99 after the position: tallies of the emitting cell
+  // and emit_common.  The selected component is a thermal one with non-zero
+  // density, so dbig and nabs count every accretion packet.  Returns idust2
+  // (1-based component id), or -1 on failure.
+  __device__ int accretion_emission(const LaunchParams& P) {
+    int64_t ci = 0;
+    const int k = initpacc(ci);
+    if (k < 0) return -1;
+    const CellRec c = m.cells[ci];
+    atomicAdd(T.dbig + ci, 1);
+    atomicAdd(T.nabs + ci, 1);
+    if (!emit_common(P, ci, c, cell_slot(c.meta, k))) return -1;
+    return cell_id(c.meta, k);
+  }
+
   __device__ int run(int64_t iphot, const LaunchParams& P) {
     on_wall = false;
     nscat = nabsev = ncross = nstar = ndiffev = 0;
-    if (iphot < P.npacc || iphot > P.npacc + P.ns) return 3;   // rejected at launch
+    if (iphot > P.npacc + P.ns) return 3;   // external illumination: rejected at launch
+    if (iphot < P.npacc) {                  // disk accretion, newdisktherm_5_fuv.f90:238-287
+      const int idust2 = accretion_emission(P);
+      if (idust2 < 0) return 3;
+      opacset(nub, KAPD_DISK);
+      iflag = 0;
+      i_orig = 2;
+      if (P.ipeel == 1)
+        for (int peelid = 1; peelid <= m.npeel; ++peelid) peeloff(sip, ir, it, ip, idust2, peelid);
+      ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;
+      return propagate(P);
+    }
     if (iphot < P.npacc + P.npaccstar) {
       if (P.ips == 0) initpspot(1); else initp_ps(1);
       if (ran() < 0.5) nub = 1.2398 / 0.06 + ran() * (1.2398 / 0.015 - 1.2398 / 0.06);
@@ -1342,23 +1457,8 @@ struct Packet {
           if (idust2 == 1 || idust2 == 2 || idust2 == 5 || idust2 == 6 || idust2 == 9) i_orig = 2;
           else if (idust2 == 3 || idust2 == 7) i_orig = 3;
           else i_orig = 4;
-          if (!cell_diffus(c.flags)) {
-            atomicAdd(T.nabs + ci, 1);
-            const double tave = __ldg(m.tdust + ci);
-            sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90
-            cost = 1.0 - 2.0 * ran();
-            sint = sqrt(1.0 - cost * cost);
-            phi = R2P * ran();
-            cosp = cos(phi);
-            sinp = sin(phi);
-            nub = lucydustfreq(tave, m.slot_species[slot]);
-            uy = sint * sinp;
-            ux = sint * cosp;
-            uz = cost;
-          } else {
-            ++ndiffev;
-            if (!emit_diffusion(P)) return 3;
-          }
+          if (!cell_diffus(c.flags)) atomicAdd(T.nabs + ci, 1);
+          if (!emit_common(P, ci, c, slot)) return 3;
           iflag = 0;
           opacset(nub, KAPD_PROPAGATE);
           ifuv = is_fuv(nub) ? m.ifuv_ori : 0.0;

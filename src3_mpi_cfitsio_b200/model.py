@@ -440,6 +440,22 @@ class Model:
         loghnu[0] = 0.0
         return atmosnu, hnuint, lognu, loghnu
 
+    @staticmethod
+    def _accretion_cdf(rarr, rin, rout):
+        """Ldint(nrg-1): cumulative disk-accretion luminosity, the table
+        initpacc draws the emitting radius from (diskprofile_model11.f90:
+        170-227 builds it from its disk structure).  Here the viscous-disk
+        profile dL ~ r^-2 (1 - r^-1/2) dr (r in stellar radii) between the
+        dust radius and the disk edge.  initpacc takes cell j when
+        Ldint(j) <= xi < Ldint(j+1) (locate), so Ldint(j) holds the
+        luminosity of the cells before j, normalised to the total."""
+        a = np.clip(rarr[:-1], rin, rout)
+        b = np.clip(rarr[1:], rin, rout)
+        lum = (1.0 / a - 1.0 / b) - (2.0 / 3.0) * (a ** -1.5 - b ** -1.5)
+        lum = np.maximum(lum, 0.0)
+        cum = np.concatenate([[0.0], np.cumsum(lum[:-1])])
+        return cum / cum[-1] if cum[-1] > 0 else cum
+
     # ---------------------------------------------------------------- build
     def _build(self):
         w = self.w
@@ -494,7 +510,7 @@ class Model:
             tan2arr=tan2arr, phiarr=phiarr, aarr=aarr, barr=barr,
             densarr=F(dens), findopac=F(findopac), diffus=F(diffus), diffdir=F(diffdir),
             tdust=F(tdust), vcell=F(vcell), ravearr=rave,
-            Ldint=np.linspace(1.0 / (nrg - 1), 1.0, nrg - 1),
+            Ldint=self._accretion_cdf(rarr, rddust, w.rmaxd_au * autors),
             hdisk=(w.h100_au * autors / (100.0 * autors) ** w.b_exp) * rave ** w.b_exp,
         )
         self.tables = dict(

@@ -68,3 +68,21 @@ def test_polarisation_bound(oracle_mod, small_model):
     p2 = L["sqp"] ** 2 + L["sup"] ** 2 + L["svp"] ** 2
     assert np.all(p2 <= L["sip"] ** 2 * (1 + 1e-9))
     assert (L["nscat"] > 0).sum() > 10
+
+
+def test_accretion_packets_leave_the_disk(oracle_mod):
+    """Disk-accretion packets (initpacc_4.f90) with the diffusion treatment:
+    each is emitted once by a thermal component (one dbig and one nabs
+    count per packet on top of the absorptions), reemitted thermally, and
+    leaves the grid."""
+    m = model.with_diffusion(model.warm(model.small_2d()))
+    m.config["accfrac"] = 0.25
+    n, npacc = 2000, 500
+    tal, log = oracle_mod.run(abi.Bundle(m), n, ipeel=0, threads=2, nlog=n)
+    L = abi.packet_log_to_numpy(log)
+    acc = L["iphot"] < npacc
+    assert acc.sum() == npacc - 1
+    assert (L["status"] == 0).all()
+    assert set(np.unique(L["i_orig"][acc])) <= {2, 3, 4}
+    absorptions = int(L["nabs"].sum())
+    assert tal["dbig"].sum() == absorptions + npacc - 1
