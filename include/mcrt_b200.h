@@ -136,6 +136,15 @@ typedef struct mcrt_tables {
   const double  *u;                           /* [nmu] SED cos(theta) bins   */
   const double  *coste_arr, *sinte_arr, *cospe_arr, *sinpe_arr; /* [npeel]   */
   const double  *limb_prob;                   /* [100] Eddington CDF (samptabl.f90:1-23), limb=1 only */
+  /* Tabulated scattering matrices (stokes6.f90, stokespeel6.f90, tab_mod.f90),
+   * optional; NULL selects the analytic dustmat phase matrix.
+   * mueller(6,narr,nlammax,nopac): S11 S12 S22 S33 S34 S44 (Bohren & Huffman
+   * sign of S34) on narr cosine bins, bin i centred on -1+(i-0.5)*2/narr as
+   * reatab.f90 resamples them, for every species and wavelength node of
+   * nudust; S11 normalised like reatab (sum of S11*dct/2 over the bins = 1).
+   * A scattering interpolates two wavelength nodes with opacset's weights. */
+  const double  *mueller;
+  int32_t        narr, pad_mueller;
 } mcrt_tables;
 
 /*

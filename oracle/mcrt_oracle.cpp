@@ -711,6 +711,187 @@ struct Packet {
     }
   }
 
+  // --------------------------------------------- tabulated scattering
+  // stokes6.f90 / stokespeel6.f90 with the tables of tab_mod.f90 per species
+  // and wavelength node (the reference keeps one table, reatab.f90, and its
+  // stokes6 indexes s11arr(narr,4) with one subscript, so it does not
+  // compile; this restatement and the engine share one definition):
+  //   row      = species x wavelength node a of opacset's bracket, weight f
+  //              of node a-1 (the interpolation of kappa, albedo, g);
+  //   itab     = int((1+bmu)/dct)+1 within 1..narr (stokes6.f90:62);
+  //   rejection bound = max over the row of S11+|S12| (max of the two rows
+  //              when interpolating), which bounds the sampling probability
+  //              for any polarisation; stokes6's running `peak` is not kept.
+  void mueller_row(double nu, int id, int& row, double& f) const {
+    const mcrt_tables* t = m->t;
+    const int nl = m->c.nlammax;
+    const double* nud = t->nudust + (int64_t)nl * id;
+    const int n = t->nlambda[id];
+    int a;
+    if (nu >= nud[0]) { a = 0; f = 0.0; }
+    else if (nu <= nud[n - 1]) { a = n - 1; f = 0.0; }
+    else {
+      int i0 = 1, i1 = n;
+      while (i1 - i0 > 1) {
+        int i = (i1 + i0) / 2;
+        if (nu <= nud[i - 1]) i0 = i; else i1 = i;
+      }
+      a = i1 - 1;
+      const int b = i0 - 1;
+      f = (nu - nud[a]) / (nud[b] - nud[a]);
+    }
+    row = a + nl * id;
+  }
+  double mueller_el(int row, double f, int itab, int k) const {
+    const double* tab = m->t->mueller;
+    const int narr = m->t->narr;
+    const double va = tab[6 * ((int64_t)(itab - 1) + (int64_t)narr * row) + k];
+    if (f == 0.0) return va;
+    const double vb = tab[6 * ((int64_t)(itab - 1) + (int64_t)narr * (row - 1)) + k];
+    return (1.0 - f) * va + f * vb;
+  }
+  int mueller_bin(double bmu) const {
+    const int narr = m->t->narr;
+    return std::min(std::max((int)((1.0 + bmu) / (2.0 / (double)narr)) + 1, 1), narr);
+  }
+  double mueller_peak(int row, double f) const {
+    auto rowpeak = [&](int r) {
+      double pk = 0.0;
+      const double* tab = m->t->mueller;
+      for (int i = 0; i < m->t->narr; ++i) {
+        const double* e = tab + 6 * ((int64_t)i + (int64_t)m->t->narr * r);
+        pk = std::max(pk, e[0] + std::fabs(e[1]));
+      }
+      return pk;
+    };
+    return f == 0.0 ? rowpeak(row) : std::max(rowpeak(row), rowpeak(row - 1));
+  }
+  // stokes6.f90:174-201 (i1 > pi) and :286-306 (i1 < pi)
+  void mueller6(int row, double f, int itab, bool upper, double s11, double s12, double c2i, double s2i,
+                double sini2, double cosi2, double* A) const {
+    const double sin2i2 = 2.0 * sini2 * cosi2, cos2i2 = 2.0 * cosi2 * cosi2 - 1.0;
+    const double sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const double sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    const double s22 = mueller_el(row, f, itab, 2), s33 = mueller_el(row, f, itab, 3);
+    const double s34 = mueller_el(row, f, itab, 4), s44 = mueller_el(row, f, itab, 5);
+    // A: a11 a12 a13 a21 a22 a23 a24 a31 a32 a33 a34 a42 a43 a44
+    A[0] = s11; A[1] = s12 * c2i; A[3] = s12 * cos2i2;
+    A[4] = s22 * cos2 - s33 * sin2;
+    A[9] = -s22 * sin2 + s33 * cos2;
+    A[10] = s34 * cos2i2;
+    A[12] = -s34 * c2i;
+    A[13] = s44;
+    if (upper) {
+      A[2] = s12 * s2i; A[5] = s22 * cos2sin1 + s33 * sin2cos1; A[6] = s34 * sin2i2;
+      A[7] = -s12 * sin2i2; A[8] = -s22 * sin2cos1 - s33 * cos2sin1; A[11] = s34 * s2i;
+    } else {
+      A[2] = -s12 * s2i; A[5] = -s22 * cos2sin1 - s33 * sin2cos1; A[6] = -s34 * sin2i2;
+      A[7] = s12 * sin2i2; A[8] = s22 * sin2cos1 + s33 * cos2sin1; A[11] = -s34 * s2i;
+    }
+  }
+  void stokes6(int id) {          // stokes6.f90:1-336, id 0-based species
+    int row;
+    double f;
+    mueller_row(nub, id, row, f);
+    const double peak = mueller_peak(row, f);
+    const double costp = cost, sintp = sint, phip = phi;
+    double bmu, s11, s12, sinbt, a, ci, si_, c2i, s2i;
+    int itab;
+    bool upper;
+    for (;;) {
+      bmu = 1.0 - 2.0 * ran();
+      itab = mueller_bin(bmu);
+      s11 = mueller_el(row, f, itab, 0);
+      s12 = mueller_el(row, f, itab, 1);
+      const double cosb2 = bmu * bmu;
+      sinbt = std::sqrt(1.0 - cosb2);
+      const double ri1 = R2P * ran();
+      upper = ri1 > PI;
+      const double ang = upper ? R2P - ri1 : ri1;
+      ci = std::cos(ang);
+      si_ = std::sin(ang);
+      s2i = 2.0 * si_ * ci;
+      c2i = 2.0 * ci * ci - 1.0;
+      const double a12 = s12 * c2i;
+      const double a13 = upper ? s12 * s2i : -s12 * s2i;
+      const double rprob = (s11 * sip + a12 * sqp + a13 * sup) / sip;
+      if (peak * ran() > rprob) continue;
+      a = rprob;
+      break;
+    }
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) {
+      si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0;
+      cost = -costp; sint = sintp;
+    } else {
+      cost = costp * bmu + sintp * sinbt * ci;
+      if (std::fabs(cost) < 1.0) {
+        sint = std::fabs(std::sqrt(1.0 - cost * cost));
+        sini2 = si_ * sintp / sint;
+        const double bott = sint * sinbt;
+        cosi2 = costp / bott - cost * bmu / bott;
+      } else {
+        sint = 0.0; sini2 = 0.0;
+        if (cost >= 1.0) { cosi2 = -1.0; cost = 1.0; }
+        if (cost <= -1.0) { cosi2 = 1.0; cost = -1.0; }
+      }
+    }
+    double cosdph = -cosi2 * ci + sini2 * si_ * bmu;
+    if (std::fabs(cosdph) > 1.0) cosdph = (cosdph > 1.0) ? 1.0 : -1.0;
+    phi = upper ? phip + std::acos(cosdph) : phip - std::acos(cosdph);
+    if (phi > R2P) phi = phi - R2P;
+    if (phi < 0.0) phi = phi + R2P;
+    double A[14];
+    mueller6(row, f, itab, upper, s11, s12, c2i, s2i, sini2, cosi2, A);
+    const double nsi = (A[0] * sip + A[1] * sqp + A[2] * sup) / a;
+    const double nsq = (A[3] * sip + A[4] * sqp + A[5] * sup + A[6] * svp) / a;
+    const double nsu = (A[7] * sip + A[8] * sqp + A[9] * sup + A[10] * svp) / a;
+    const double nsv = (A[11] * sqp + A[12] * sup + A[13] * svp) / a;
+    sip = nsi; sqp = nsq; sup = nsu; svp = nsv;
+    cosp = std::cos(phi);
+    sinp = std::sin(phi);
+  }
+  void stokespeel6(double& s_i, double& s_q, double& s_u, double& s_v, double cst, double snt, double ri1,
+                   double bmu, double costp, double sintp, int id) const {   // stokespeel6.f90:1-321
+    int row;
+    double f;
+    mueller_row(nub, id, row, f);
+    const int itab = mueller_bin(bmu);
+    const double s11 = mueller_el(row, f, itab, 0), s12 = mueller_el(row, f, itab, 1);
+    const double cosb2 = bmu * bmu;
+    const double sinbt = std::sqrt(1.0 - cosb2);
+    const bool upper = ri1 > PI;
+    const double ang = upper ? R2P - ri1 : ri1;
+    double ci = std::cos(ang), si_ = std::sin(ang);
+    const double s2i = 2.0 * si_ * ci, c2i = 2.0 * ci * ci - 1.0;
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) { si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0; }
+    else if (std::fabs(cst) < 1.0) {
+      sini2 = si_ * sintp / snt;
+      const double bott = snt * sinbt;
+      cosi2 = costp / bott - cst * bmu / bott;
+    } else {
+      sini2 = 0.0;
+      if (cst >= 1.0) cosi2 = -1.0;
+      if (cst <= -1.0) cosi2 = 1.0;
+    }
+    double A[14];
+    mueller6(row, f, itab, upper, s11, s12, c2i, s2i, sini2, cosi2, A);
+    const double ni = (A[0] * s_i + A[1] * s_q + A[2] * s_u);
+    const double nq = (A[3] * s_i + A[4] * s_q + A[5] * s_u + A[6] * s_v);
+    const double nu_ = (A[7] * s_i + A[8] * s_q + A[9] * s_u + A[10] * s_v);
+    const double nv = (A[11] * s_q + A[12] * s_u + A[13] * s_v);
+    s_i = ni; s_q = nq; s_u = nu_; s_v = nv;
+  }
+  void scatter(int id) { if (m->t->mueller && m->t->narr > 0) stokes6(id); else stokes(id); }
+  void peel_matrix(double& s_i, double& s_q, double& s_u, double& s_v, double cst, double snt, double ri1,
+                   double bmu, double costp, double sintp, int id) const {
+    if (m->t->mueller && m->t->narr > 0) stokespeel6(s_i, s_q, s_u, s_v, cst, snt, ri1, bmu, costp, sintp, id);
+    else stokespeel(s_i, s_q, s_u, s_v, cst, snt, ri1, bmu, costp, sintp, id);
+  }
+
   // ---------------------------------------------------------- scattering
   void dustmat(double bmu, double cosb2, int id, double& p1, double& p2, double& p3, double& p4) const {
     // dustmat.f90:343-412
@@ -1002,7 +1183,7 @@ struct Packet {
     if (iflag == 1) {
       double bmu, sinbm, ri1;
       findangle3(cost, sint, phi, cosp, sinp, coste, sinte, 0.0, cospe, sinpe, bmu, sinbm, ri1);
-      stokespeel(q_i, q_q, q_u, q_v, coste, sinte, ri1, bmu, cost, sint, m->fopac(ir, it, ip, idust2) - 1);
+      peel_matrix(q_i, q_q, q_u, q_v, coste, sinte, ri1, bmu, cost, sint, m->fopac(ir, it, ip, idust2) - 1);
     }
     double yimage = z1 * sinte - y1 * coste * sinpe - x1 * coste * cospe;
     double ximage = y1 * cospe - x1 * sinpe;
@@ -1330,7 +1511,7 @@ struct Packet {
           ++nscat;
           T->cnt[MCRT_C_SCATTERS]++;
           if (ipeel == 1) peel_all(sip, ii[0], ii[1], ii[2], idust2);
-          stokes(fo);
+          scatter(fo);
         } else {                            // absorbed + re-emitted
           ++nabsev;
           int64_t cc = m->cidx(ir, it, ip);

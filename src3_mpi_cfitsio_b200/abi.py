@@ -59,7 +59,7 @@ TABLE_FIELDS = [("nlambda", _ip), ("nudust", _dp), ("kappad", _dp), ("adust", _d
                 ("kappar", _dp), ("atmosnu", _dp), ("hnuint", _dp), ("lognu", _dp),
                 ("loghnu", _dp), ("aperture2", _dp), ("u", _dp), ("coste_arr", _dp),
                 ("sinte_arr", _dp), ("cospe_arr", _dp), ("sinpe_arr", _dp),
-                ("limb_prob", _dp)]
+                ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32)]
 
 
 class Tables(C.Structure):
@@ -117,6 +117,9 @@ class Bundle:
         for name, ptype in cls._fields_:
             a = arrays.get(name)
             if a is None:
+                continue
+            if ptype is C.c_int32:          # scalar member
+                setattr(s, name, int(a))
                 continue
             if ptype is _ip:
                 a = np.ascontiguousarray(a, dtype=np.int32)

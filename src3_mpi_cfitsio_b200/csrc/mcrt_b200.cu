@@ -600,6 +600,26 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   add(c.npeel ? t->coste_arr : pz.data(), np); add(c.npeel ? t->sinte_arr : pz.data(), np);            // 18-19
   add(c.npeel ? t->cospe_arr : pz.data(), np); add(c.npeel ? t->sinpe_arr : pz.data(), np);            // 20-21
   add(t->Tint, c.nT); add(t->kappap, (int64_t)c.nT * c.nopac);                                          // 22-23
+  // tabulated scattering matrices: the table and, per (species, wavelength)
+  // row, the rejection bound max(S11 + |S12|) over the cosine bins, which
+  // bounds the sampling probability (S11 I + S12 (cos2i Q +- sin2i U)) / I
+  // for any polarisation; it replaces stokes6's running `peak`
+  const bool mueller = t->mueller != nullptr && t->narr > 0;
+  if (mueller) {
+    if (t->narr < 2 || t->narr > 1000000) return fail(ctx, MCRT_ERR_ARG, "narr must be 2..1e6");
+    const int64_t nrow = nl, nb = t->narr;
+    std::vector<double> peak(nrow, 0.0);
+    for (int64_t r = 0; r < nrow; ++r)
+      for (int64_t i = 0; i < nb; ++i) {
+        const double* e = t->mueller + 6 * (i + nb * r);
+        for (int k = 0; k < 6; ++k)
+          if (!std::isfinite(e[k])) return fail(ctx, MCRT_ERR_ARG, "mueller table holds a non-finite value");
+        if (!(e[0] >= 0.0)) return fail(ctx, MCRT_ERR_ARG, "mueller S11 must be non-negative");
+        peak[r] = std::max(peak[r], e[0] + std::fabs(e[1]));
+      }
+    add(t->mueller, 6 * nb * nrow);                                                                    // 24
+    add(peak.data(), nrow);                                                                            // 25
+  }
   // jump tables a^(2^30 * 2^k)
   std::vector<int64_t> jump(128);
   int64_t j1 = 1033780774, j2 = 1494757890;   // a1w, a2w (ecuyer_cote_mod.f90:14-15)
@@ -626,6 +646,10 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.limb_prob = b + off[13]; m.inczeta = b + off[14];
   m.aperture2 = b + off[15]; m.u = b + off[16]; m.sini = b + off[17];
   m.coste = b + off[18]; m.sinte = b + off[19]; m.cospe = b + off[20]; m.sinpe = b + off[21];
+  m.mueller = mueller ? b + off[24] : nullptr;
+  m.mpeak = mueller ? b + off[25] : nullptr;
+  m.narr = mueller ? t->narr : 0;
+  m.dct = mueller ? 2.0 / (double)t->narr : 0.0;
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;

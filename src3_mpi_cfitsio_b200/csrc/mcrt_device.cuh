@@ -71,6 +71,11 @@ struct DevModel {
   const int32_t *nlambda;
   const double *nudust, *kappad, *adust, *gdust, *pldust, *kappav;
   const double *kapint, *lTint, *nuint;
+  // tabulated scattering (stokes6): [nopac][nlammax][narr][6] and the
+  // per-row rejection bound; mueller == nullptr selects dustmat
+  const double *mueller, *mpeak;
+  int narr;
+  double dct;
   // star
   const double *atmosnu, *hnuint, *lognu, *loghnu, *limb_prob;
   const double *inczeta;                     // [MCRT_IZMAX]
@@ -90,7 +95,8 @@ struct __align__(16) PeelJob {
   double si, sq, su, sv;          // Stokes (si is the un-weighted I of a direct peel-off)
   double d0, d1, d2, d3, d4;      // packet direction cost,sint,cosp,sinp,phi; direct: cosb,sinb,coslp,sinlp
   double kapd[kJobSlots];         // opacity per species slot at the packet's frequency
-  double g, pl;                   // phase-function parameters of the scattering species
+  double g, pl;                   // phase-function parameters of the scattering species; with a
+                                  // tabulated matrix: g = wavelength weight f, pl = table row
   int32_t r, t, p;                // cell
   uint32_t bits;                  // onw | iflag<<1 | direct<<2 | (i_orig)<<3 | (inub-1)<<8
 };

@@ -125,9 +125,13 @@ struct PeelLane {
         if (0.0 > phi) ri1 = (0.0 - phi > PI) ? x : R2P - x;
         else ri1 = (phi - 0.0 > PI) ? R2P - x : x;
       }
-      pk.sp.g(0) = J.g;
-      pk.sp.pl(0) = J.pl;
-      pk.stokespeel(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, 0);
+      if (m.mueller) {       // the job carries the table row and wavelength weight
+        pk.stokespeel6(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, (int)J.pl, J.g);
+      } else {
+        pk.sp.g(0) = J.g;
+        pk.sp.pl(0) = J.pl;
+        pk.stokespeel(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, 0);
+      }
     }
     const double x1 = ray.x, y1 = ray.y, z1 = ray.z;
     const double yimage = z1 * sinte - y1 * coste * sinpe - x1 * coste * cospe;

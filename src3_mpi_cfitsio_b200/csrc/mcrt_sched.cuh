@@ -189,8 +189,16 @@ struct Lane {
     else { J.d0 = pk.cost; J.d1 = pk.sint; J.d2 = pk.cosp; J.d3 = pk.sinp; J.d4 = pk.phi; }
     for (int s = 0; s < kJobSlots; ++s) J.kapd[s] = s < m.nslot ? pk.sp.kapd(s) : 0.0;
     const int ss = (pk.iflag == 1) ? pk.idust2slot(idust2) : 0;
-    J.g = pk.sp.g(ss);
-    J.pl = pk.sp.pl(ss);
+    if (m.mueller) {         // tabulated matrix: the row and wavelength weight instead of g, pl
+      int row = 0;
+      double f = 0.0;
+      if (pk.iflag == 1) pk.mueller_row(pk.nub, ss, row, f);
+      J.g = f;
+      J.pl = (double)row;
+    } else {
+      J.g = pk.sp.g(ss);
+      J.pl = pk.sp.pl(ss);
+    }
     J.r = pk.ir; J.t = pk.it; J.p = pk.ip;
     J.bits = (pk.on_wall ? 1u : 0u) | ((pk.iflag == 1 ? 1u : 0u) << 1) | ((ctx == PC_DIRECT ? 1u : 0u) << 2) |
              ((uint32_t)pk.i_orig << 3) | ((uint32_t)(pk.freq_bin(pk.nub) - 1) << 8);
@@ -245,7 +253,7 @@ struct Lane {
         if (0.0 > pk.phi) ri1 = (0.0 - pk.phi > PI) ? x : R2P - x;
         else ri1 = (pk.phi - 0.0 > PI) ? R2P - x : x;
       }
-      pk.stokespeel(qi, qq, qu, qv, coste, sinte, ri1, costnew, pk.cost, pk.sint, pk.idust2slot(peel_idust2));
+      pk.peel_matrix(qi, qq, qu, qv, coste, sinte, ri1, costnew, pk.cost, pk.sint, pk.idust2slot(peel_idust2));
     }
     const double x1 = ray.x, y1 = ray.y, z1 = ray.z;
     const double yimage = z1 * sinte - y1 * coste * sinpe - x1 * coste * cospe;
@@ -441,7 +449,7 @@ struct Lane {
           break;
         }
         case EV_SCATTER_DONE:
-          pk.stokes(slot_s);
+          pk.scatter(slot_s);
           ev = EV_NEXT_TAU;
           break;
         case EV_ABSORB_DONE:

@@ -739,6 +739,200 @@ struct Packet {
     return false;
   }
 
+  // ------------------------------------------- tabulated scattering
+  // Table row of the species in slot s at the wavelength node a of
+  // frequency nu, and the weight f of node a-1: opacset's bracket and
+  // weights (dust_5.f90:9-109), so the matrix is interpolated in wavelength
+  // exactly as kappa, albedo and g are.
+  __device__ void mueller_row(double nu, int s, int& row, double& f) const {
+    const int id = m.slot_species[s] - 1;
+    const int nl = m.nlammax;
+    const double* nud = m.nudust + (int64_t)nl * id;
+    const int n = m.nlambda[id];
+    int a;
+    if (nu >= __ldg(nud)) { a = 0; f = 0.0; }
+    else if (nu <= __ldg(nud + n - 1)) { a = n - 1; f = 0.0; }
+    else {
+      int i0 = 1, i1 = n;
+      while (i1 - i0 > 1) {
+        const int i = (i1 + i0) >> 1;
+        if (nu <= __ldg(nud + i - 1)) i0 = i; else i1 = i;
+      }
+      a = i1 - 1;
+      const int b = i0 - 1;
+      f = (nu - __ldg(nud + a)) / (__ldg(nud + b) - __ldg(nud + a));
+    }
+    row = a + nl * id;
+  }
+  // matrix element k (S11 S12 S22 S33 S34 S44) in cosine bin itab
+  __device__ __forceinline__ double mueller_el(int row, double f, int itab, int k) const {
+    const double va = __ldg(m.mueller + 6 * ((int64_t)(itab - 1) + (int64_t)m.narr * row) + k);
+    if (f == 0.0) return va;
+    const double vb = __ldg(m.mueller + 6 * ((int64_t)(itab - 1) + (int64_t)m.narr * (row - 1)) + k);
+    return (1.0 - f) * va + f * vb;
+  }
+  // itab = int((1+bmu)/dct)+1 (stokes6.f90:62), kept inside the table
+  __device__ __forceinline__ int mueller_bin(double bmu) const {
+    return min(max((int)((1.0 + bmu) / m.dct) + 1, 1), m.narr);
+  }
+  // Rejection bound of the interpolated row: the per-row max(S11 + |S12|)
+  // bounds (S11 I + S12 (cos2i Q +- sin2i U)) / I for any polarisation, and
+  // a linear interpolation of two rows by the larger of their bounds.
+  __device__ __forceinline__ double mueller_peak(int row, double f) const {
+    return f == 0.0 ? __ldg(m.mpeak + row) : fmax(__ldg(m.mpeak + row), __ldg(m.mpeak + row - 1));
+  }
+
+  // The six-element matrix product of stokes6.f90:174-201 (i1 > pi) and
+  // :286-306 (i1 < pi), Bohren & Huffman sign of S34.
+  struct Mueller6 { double a11, a12, a13, a21, a22, a23, a24, a31, a32, a33, a34, a42, a43, a44; };
+  __device__ __forceinline__ Mueller6 mueller6(int row, double f, int itab, bool upper, double s11, double s12,
+                                               double c2i, double s2i, double sini2, double cosi2) const {
+    const double sin2i2 = 2.0 * sini2 * cosi2, cos2i2 = 2.0 * cosi2 * cosi2 - 1.0;
+    const double sin2 = sin2i2 * s2i, cos2 = cos2i2 * c2i;
+    const double sin2cos1 = sin2i2 * c2i, cos2sin1 = cos2i2 * s2i;
+    const double s22 = mueller_el(row, f, itab, 2), s33 = mueller_el(row, f, itab, 3);
+    const double s34 = mueller_el(row, f, itab, 4), s44 = mueller_el(row, f, itab, 5);
+    Mueller6 A;
+    A.a11 = s11;
+    A.a12 = s12 * c2i;
+    A.a21 = s12 * cos2i2;
+    A.a22 = s22 * cos2 - s33 * sin2;
+    A.a33 = -s22 * sin2 + s33 * cos2;
+    A.a34 = s34 * cos2i2;
+    A.a43 = -s34 * c2i;
+    A.a44 = s44;
+    if (upper) {
+      A.a13 = s12 * s2i;
+      A.a23 = s22 * cos2sin1 + s33 * sin2cos1;
+      A.a24 = s34 * sin2i2;
+      A.a31 = -s12 * sin2i2;
+      A.a32 = -s22 * sin2cos1 - s33 * cos2sin1;
+      A.a42 = s34 * s2i;
+    } else {
+      A.a13 = -s12 * s2i;
+      A.a23 = -s22 * cos2sin1 - s33 * sin2cos1;
+      A.a24 = -s34 * sin2i2;
+      A.a31 = s12 * sin2i2;
+      A.a32 = s22 * sin2cos1 + s33 * cos2sin1;
+      A.a42 = -s34 * s2i;
+    }
+    return A;
+  }
+
+  // stokes6.f90:1-336: scattering with the tabulated matrix of the species
+  // in slot s, by rejection under the row's bound.
+  __device__ void stokes6(int s) {
+    int row;
+    double f;
+    mueller_row(nub, s, row, f);
+    const double peak = mueller_peak(row, f);
+    const double costp = cost, sintp = sint, phip = phi;
+    double bmu, s11, s12, sinbt, a, ci, si_, c2i, s2i;
+    int itab;
+    bool upper;
+    for (;;) {
+      bmu = 1.0 - 2.0 * ran();
+      itab = mueller_bin(bmu);
+      s11 = mueller_el(row, f, itab, 0);
+      s12 = mueller_el(row, f, itab, 1);
+      const double cosb2 = bmu * bmu;
+      sinbt = sqrt(1.0 - cosb2);
+      const double ri1 = R2P * ran();
+      upper = ri1 > PI;
+      const double ang = upper ? R2P - ri1 : ri1;
+      ci = cos(ang);
+      si_ = sin(ang);
+      s2i = 2.0 * si_ * ci;
+      c2i = 2.0 * ci * ci - 1.0;
+      const double a12 = s12 * c2i;
+      const double a13 = upper ? s12 * s2i : -s12 * s2i;
+      const double rprob = (s11 * sip + a12 * sqp + a13 * sup) / sip;
+      if (peak * ran() > rprob) continue;
+      a = rprob;
+      break;
+    }
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) {
+      si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0;
+      cost = -costp; sint = sintp;
+    } else {
+      cost = costp * bmu + sintp * sinbt * ci;
+      if (fabs(cost) < 1.0) {
+        sint = fabs(sqrt(1.0 - cost * cost));
+        sini2 = si_ * sintp / sint;
+        const double bott = sint * sinbt;
+        cosi2 = costp / bott - cost * bmu / bott;
+      } else {
+        sint = 0.0; sini2 = 0.0;
+        if (cost >= 1.0) { cosi2 = -1.0; cost = 1.0; }
+        if (cost <= -1.0) { cosi2 = 1.0; cost = -1.0; }
+      }
+    }
+    double cosdph = -cosi2 * ci + sini2 * si_ * bmu;
+    if (fabs(cosdph) > 1.0) cosdph = (cosdph > 1.0) ? 1.0 : -1.0;
+    phi = upper ? phip + acos(cosdph) : phip - acos(cosdph);
+    if (phi > R2P) phi = phi - R2P;
+    if (phi < 0.0) phi = phi + R2P;
+    const Mueller6 A = mueller6(row, f, itab, upper, s11, s12, c2i, s2i, sini2, cosi2);
+    const double nsi = (A.a11 * sip + A.a12 * sqp + A.a13 * sup) / a;
+    const double nsq = (A.a21 * sip + A.a22 * sqp + A.a23 * sup + A.a24 * svp) / a;
+    const double nsu = (A.a31 * sip + A.a32 * sqp + A.a33 * sup + A.a34 * svp) / a;
+    const double nsv = (A.a42 * sqp + A.a43 * sup + A.a44 * svp) / a;
+    sip = nsi; sqp = nsq; sup = nsu; svp = nsv;
+    cosp = cos(phi);
+    sinp = sin(phi);
+  }
+
+  // stokespeel6.f90:1-321: the peel-off weight matrix of the tabulated row
+  // (row, f) for scattering angle bmu (no normalisation).
+  __device__ void stokespeel6(double& qi, double& qq, double& qu, double& qv, double cst, double snt, double ri1,
+                              double bmu, double costp, double sintp, int row, double f) const {
+    const int itab = mueller_bin(bmu);
+    const double s11 = mueller_el(row, f, itab, 0), s12 = mueller_el(row, f, itab, 1);
+    const double cosb2 = bmu * bmu;
+    const double sinbt = sqrt(1.0 - cosb2);
+    const bool upper = ri1 > PI;
+    const double ang = upper ? R2P - ri1 : ri1;
+    double ci = cos(ang), si_ = sin(ang);
+    const double s2i = 2.0 * si_ * ci, c2i = 2.0 * ci * ci - 1.0;
+    if (bmu == 1.0) return;
+    double sini2, cosi2 = 0.0;
+    if (bmu == -1.0) { si_ = 1.0; sini2 = 1.0; ci = 0.0; cosi2 = 0.0; }
+    else if (fabs(cst) < 1.0) {
+      sini2 = si_ * sintp / snt;
+      const double bott = snt * sinbt;
+      cosi2 = costp / bott - cst * bmu / bott;
+    } else {
+      sini2 = 0.0;
+      if (cst >= 1.0) cosi2 = -1.0;
+      if (cst <= -1.0) cosi2 = 1.0;
+    }
+    const Mueller6 A = mueller6(row, f, itab, upper, s11, s12, c2i, s2i, sini2, cosi2);
+    const double ni = (A.a11 * qi + A.a12 * qq + A.a13 * qu);
+    const double nq = (A.a21 * qi + A.a22 * qq + A.a23 * qu + A.a24 * qv);
+    const double nu_ = (A.a31 * qi + A.a32 * qq + A.a33 * qu + A.a34 * qv);
+    const double nv = (A.a42 * qq + A.a43 * qu + A.a44 * qv);
+    qi = ni; qq = nq; qu = nu_; qv = nv;
+  }
+
+  // scattering of the species in slot s: tabulated matrix (stokes6) when the
+  // model has one, else the analytic phase matrix (stokes)
+  __device__ __forceinline__ void scatter(int s) {
+    if (m.mueller) stokes6(s); else stokes(s);
+  }
+  __device__ __forceinline__ void peel_matrix(double& qi, double& qq, double& qu, double& qv, double cst, double snt,
+                                              double ri1, double bmu, double costp, double sintp, int s) const {
+    if (m.mueller) {
+      int row;
+      double f;
+      mueller_row(nub, s, row, f);
+      stokespeel6(qi, qq, qu, qv, cst, snt, ri1, bmu, costp, sintp, row, f);
+    } else {
+      stokespeel(qi, qq, qu, qv, cst, snt, ri1, bmu, costp, sintp, s);
+    }
+  }
+
   // ------------------------------------------------------- scattering
   __device__ __forceinline__ void dustmat(double bmu, double cosb2, int s, double& p1, double& p2, double& p3) const {
     const double gg = sp.g(s);
@@ -1104,7 +1298,7 @@ struct Packet {
       for (int k = 0; k < n; ++k)
         if (cell_id(cf.meta, k) == idust2) { sslot = cell_slot(cf.meta, k); found = true; }
       if (!found) sslot = idust2slot(idust2);
-      stokespeel(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, sslot);
+      peel_matrix(qi, qq, qu, qv, coste, sinte, ri1, costnew, cost, sint, sslot);
     }
     const double yimage = z1 * sinte - y1 * coste * sinpe - x1 * coste * cospe;
     const double ximage = y1 * cospe - x1 * sinpe;
@@ -1449,7 +1643,7 @@ struct Packet {
           ++nscat;
           if (P.ipeel == 1)
             for (int peelid = 1; peelid <= m.npeel; ++peelid) peeloff(sip, ir, it, ip, idust2, peelid);
-          stokes(slot);
+          scatter(slot);
         } else {                                    // absorbed + re-emitted
           ++nabsev;
           const int64_t ci = cidx(ir, it, ip);

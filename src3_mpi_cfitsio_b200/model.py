@@ -670,3 +670,40 @@ def tdust_from_tdave(m: Model, tdave: np.ndarray) -> np.ndarray:
     T = np.where(dif, 0.1 / 11605.0, td)
     T = np.where(m.dens4().sum(axis=-1) > 0, T, 0.1 / 11605.0)
     return np.asfortranarray(T).ravel(order="F")
+
+
+def with_mueller(m: Model, narr: int = 720, nang: int = 181, s34_frac: float = 0.0) -> Model:
+    """Tabulated scattering matrices (stokes6 / tab_mod) for every species
+    and wavelength node, generated from the dustmat law (dustmat.f90) with
+    each node's g and pmax on `nang` scattering angles (0..180 deg, the
+    reference's nar=181 of reatab.f90) and resampled to `narr` uniform
+    cosine bins as reatab.f90 does (linearly here), S11 normalised so that
+    the sum of S11*dct/2 over the bins is 1.  S11=S22=p1, S12=p2, S33=S44=p3;
+    `s34_frac` in [0,1] adds S34 = s34_frac p1 sqrt(1-pmax^2)(1-mu^2)/(1+mu^2),
+    which keeps S11^2 >= S12^2+S33^2+S34^2 and makes scattering generate
+    circular polarisation.  Returns the model with tables["mueller"] and
+    tables["narr"] set (layout mueller(6,narr,nlammax,nopac))."""
+    c = m.config
+    nl, nop = c["nlammax"], c["nopac"]
+    gd = m.tables["gdust"].reshape((nl, nop), order="F")
+    pd = m.tables["pldust"].reshape((nl, nop), order="F")
+    th = np.linspace(0.0, PI, nang)
+    mu_in = np.cos(th)[::-1]                        # ascending
+    dct = 2.0 / narr
+    mu = -1.0 + (np.arange(1, narr + 1) - 0.5) * dct
+    out = np.zeros((nop, nl, narr, 6))
+    for sp in range(nop):
+        for j in range(nl):
+            g, pl = gd[j, sp], pd[j, sp]
+            cb2 = mu_in * mu_in
+            temp = (g * g + 1.0) - 2.0 * g * mu_in
+            p1 = 1.5 * (1.0 - g * g) / (2.0 + g * g) * (1.0 + cb2) / (temp * np.sqrt(temp))
+            p2 = -pl * p1 * (1.0 - cb2) / (1.0 + cb2)
+            p3 = p1 * 2.0 * mu_in / (1.0 + cb2)
+            p4 = s34_frac * p1 * math.sqrt(max(0.0, 1.0 - pl * pl)) * (1.0 - cb2) / (1.0 + cb2)
+            cols = [np.interp(mu, mu_in, v) for v in (p1, p2, p1, p3, p4, p3)]
+            tot = np.sum(0.5 * cols[0] * dct)
+            out[sp, j] = np.stack(cols, axis=-1) / tot
+    m.tables["mueller"] = np.ascontiguousarray(out).ravel()
+    m.tables["narr"] = int(narr)
+    return m

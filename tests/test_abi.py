@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "mcrt_b200.h")
 
@@ -33,6 +35,40 @@ def test_struct_sizes_match_header():
     from src3_mpi_cfitsio_b200 import abi
     assert ctypes.sizeof(abi.Config) == 24 * 4 + 23 * 8
     assert ctypes.sizeof(abi.Grid) == 18 * 8
-    assert ctypes.sizeof(abi.Tables) == 24 * 8
+    assert ctypes.sizeof(abi.Tables) == 25 * 8 + 2 * 4
     assert ctypes.sizeof(abi.Tallies) == (4 + 2 + 10 + 9 + 4 + 2) * 8
     assert ctypes.sizeof(abi.PacketLog) == 8 + 12 * 4 + 10 * 8
+
+
+def test_struct_layouts_match_the_c_compiler():
+    """The ctypes mirrors have the sizes and member offsets the C compiler
+    gives the header's structs."""
+    import os
+    import shutil
+    import subprocess
+    import tempfile
+    from src3_mpi_cfitsio_b200 import abi
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    structs = {"mcrt_config": abi.Config, "mcrt_grid": abi.Grid, "mcrt_tables": abi.Tables,
+               "mcrt_tallies": abi.Tallies, "mcrt_packet_log": abi.PacketLog,
+               "mcrt_device_tallies": abi.DeviceTallies}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mcrt_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        src = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(src, "w").write("\n".join(lines))
+        subprocess.run([cc, "-I", inc, src, "-o", exe], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

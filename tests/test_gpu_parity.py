@@ -377,3 +377,55 @@ def test_accretion_wave_matches_warp_bitwise(warm_small, precision):
     for k in a:
         assert np.array_equal(a[k][nod], b[k][nod]), k
     assert (b["status"] == 0).all()
+
+
+@pytest.fixture(scope="module")
+def mueller_small():
+    return model.with_mueller(model.warm(model.small_2d()), s34_frac=0.6)
+
+
+@pytest.mark.parametrize("ipeel", [0, 1])
+def test_tabulated_scattering_event_for_event(mueller_small, oracle_mod, ipeel):
+    """stokes6 / stokespeel6 with tabulated matrices (S34 on), engine vs
+    oracle packet for packet; peel-offs through the job queue carry the
+    table row and wavelength weight."""
+    m = mueller_small
+    n = 3000
+    eng = _engine(m)
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=ipeel)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    tg = eng.download()
+    to, lo = oracle_mod.run(abi.Bundle(m), n, ipeel=ipeel, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    same, exact = _same_packets(g, o)
+    assert exact.mean() >= 0.995
+    both = same & (g["nscat"] > 0)
+    assert both.sum() > 100
+    assert np.allclose(g["svp"][both], o["svp"][both], rtol=1e-9, atol=1e-12)
+    assert np.abs(g["svp"][both]).max() > 1e-3
+    if ipeel:
+        for k in ("ti", "tq", "tv", "numt", "image_m_i", "image_m_v"):
+            a, b = tg[k].astype(np.float64).sum(), to[k].astype(np.float64).sum()
+            assert abs(a - b) <= 1e-2 * max(abs(b), 1e-6 * tg["ti"].astype(np.float64).sum()), k
+    eng.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tabulated_scattering_wave_matches_warp_bitwise(mueller_small, precision):
+    n = 3000
+    logs = []
+    for sched in ("warp", "wave"):
+        eng = _engine(mueller_small, precision=precision)
+        eng.set_schedule(sched)
+        if sched == "wave":
+            eng.set_wave_pool(512, 0, 100)
+        eng.enable_packet_log(n)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        logs.append(abi.packet_log_to_numpy(eng.packet_log(n)))
+        eng.close()
+    a, b = logs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k

@@ -86,3 +86,36 @@ def test_accretion_packets_leave_the_disk(oracle_mod):
     assert set(np.unique(L["i_orig"][acc])) <= {2, 3, 4}
     absorptions = int(L["nabs"].sum())
     assert tal["dbig"].sum() == absorptions + npacc - 1
+
+
+def test_tabulated_matrix_reproduces_the_analytic_law(oracle_mod):
+    """stokes6 with tables generated from the dustmat law (model.with_mueller)
+    scatters like the analytic stokes: the same flux, scatterings and linear
+    polarisation within the Monte Carlo error, and no circular polarisation
+    without S34."""
+    n = 20000
+    out = {}
+    for name, m in (("analytic", model.warm(model.small_2d())),
+                    ("table", model.with_mueller(model.warm(model.small_2d())))):
+        tal, log = oracle_mod.run(abi.Bundle(m), n, ipeel=1, threads=4, nlog=n)
+        out[name] = (tal, abi.packet_log_to_numpy(log))
+    (ta, la), (tt, lt) = out["analytic"], out["table"]
+    assert abs(lt["nscat"].sum() - la["nscat"].sum()) <= 0.03 * la["nscat"].sum()
+    for k in ("ti", "nums"):
+        x, y = ta[k].astype(np.float64).sum(), tt[k].astype(np.float64).sum()
+        assert abs(y - x) <= 0.01 * abs(x), k
+    assert abs(tt["tq"].astype(np.float64).sum() - ta["tq"].astype(np.float64).sum()) <= \
+        0.2 * abs(ta["tq"].astype(np.float64).sum()) + 0.002 * ta["ti"].astype(np.float64).sum()
+    assert tt["tv"].sum() == 0.0 and (lt["svp"] == 0.0).all()
+
+
+def test_tabulated_s34_makes_circular_polarisation_within_the_bound(oracle_mod):
+    m = model.with_mueller(model.warm(model.small_2d()), s34_frac=0.8)
+    n = 10000
+    tal, log = oracle_mod.run(abi.Bundle(m), n, ipeel=1, threads=4, nlog=n)
+    L = abi.packet_log_to_numpy(log)
+    scattered = L["nscat"] > 0
+    assert np.abs(L["svp"][scattered]).max() > 1e-3
+    pol = np.sqrt(L["sqp"] ** 2 + L["sup"] ** 2 + L["svp"] ** 2)
+    assert (pol <= L["sip"] * (1.0 + 1e-9) + 1e-12).all()
+    assert np.abs(tal["tv"].astype(np.float64)).sum() > 0.0
