@@ -274,6 +274,17 @@ def run_ours(args, rank, world):
             k1 = eng.kernel_ms()
             t1_ = eng.download(images=True)
             res[prec] = (k0, k1, t0_, t1_, tdp)
+        # the plain FP64 GPU path: one thread per packet start to finish
+        # (transport_fp64), on a bounded sample of the same iteration
+        eng.set_precision("fp64")
+        eng.set_schedule("packet")
+        m.grid["tdust"] = base.copy()
+        eng.upload_grid()
+        eng.reset_tallies()
+        n_plain = min(P, args.plain_packets)
+        eng.run(P, 1, n_plain, iteration=itc, ipeel=0)
+        plain_pps = n_plain / (eng.kernel_ms() / 1e3)
+        eng.set_schedule(args.schedule)
         eng.set_precision(args.precision)
         a64 = res["fp64"]
         amx = res["mixed"]
@@ -282,6 +293,9 @@ def run_ours(args, rank, world):
         extra = {
             "fp64_value": P / (a64[0] / 1e3), "mixed_value": P / (amx[0] / 1e3),
             "mixed_over_fp64": a64[0] / amx[0],
+            "fp64_plain": {"packets": n_plain, "packets_per_s": plain_pps,
+                           "kernel": "transport_fp64 (one thread per packet, FP64)",
+                           "mixed_over_fp64_plain": (P / (amx[0] / 1e3)) / plain_pps},
             "peeled_iteration": {"packets": args.peel_packets,
                                  "fp64_packets_per_s": args.peel_packets / (a64[1] / 1e3),
                                  "mixed_packets_per_s": args.peel_packets / (amx[1] / 1e3),
@@ -384,6 +398,8 @@ def main():
     ap.add_argument("--peel-packets", type=int, default=10_000_000)
     ap.add_argument("--ipeel", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--plain-packets", type=int, default=5_000_000,
+                    help="packets of the plain FP64 per-thread comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     # 706 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk

@@ -429,3 +429,51 @@ def test_tabulated_scattering_wave_matches_warp_bitwise(mueller_small, precision
     a, b = logs
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.fixture(scope="module")
+def clumpy_small():
+    """The 3-D clumpy workload in miniature: fractal clumps, 3-D walls
+    (phi planes), tabulated Mueller matrices with S34."""
+    return model.with_mueller(model.warm(model.clumpy_3d(nrg=41, ntg=41, npg=17, nfreq=20, npeel=4,
+                                                         nxhst=31, rim_walls=8)), s34_frac=0.3)
+
+
+def test_clumpy_3d_event_for_event(clumpy_small, oracle_mod):
+    m = clumpy_small
+    n = 3000
+    eng = _engine(m)
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=1)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    tg = eng.download()
+    to, lo = oracle_mod.run(abi.Bundle(m), n, ipeel=1, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    same, exact = _same_packets(g, o)
+    assert exact.mean() >= 0.99
+    cg, co = tg.counters(), to.counters()
+    assert cg["geom_fail"] == co["geom_fail"] == 0
+    assert abs(cg["crossings"] - co["crossings"]) <= 0.01 * co["crossings"]
+    for k in ("ti", "numt", "image_m_i"):
+        a, b = tg[k].astype(np.float64).sum(), to[k].astype(np.float64).sum()
+        assert abs(a - b) <= 2e-2 * abs(b), k
+    eng.close()
+
+
+def test_clumpy_3d_mixed_wave_loses_no_packets(clumpy_small):
+    """Mixed build on the 3-D walls: no geometry failures, ensemble within
+    the Monte Carlo error of the FP64 build."""
+    n = 20000
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng = _engine(clumpy_small, precision=prec)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        out[prec] = eng.download()
+        eng.close()
+    a, b = out["fp64"], out["mixed"]
+    assert b.counters()["geom_fail"] == 0 and b.counters()["packets"] == n
+    for k in ("nums", "numt"):
+        x, y = a[k].astype(np.float64).sum(), b[k].astype(np.float64).sum()
+        assert abs(y - x) <= 0.02 * x + 50, k
