@@ -283,6 +283,26 @@ typedef struct mcrt_device_tallies {
 } mcrt_device_tallies;
 int mcrt_device_tallies_view(mcrt_ctx *ctx, mcrt_device_tallies *out);
 
+/* Path-replay adjoint of the peeled outputs for packets lo..hi of an
+ * np-packet iteration (with peel-offs).  Objective
+ *   L = sum_k lam_psed[k] * ti[k] + sum_p lam_img[p] * image_m_i[p]
+ * (peeled SED and monochromatic image, Stokes I; lam_img may be NULL).
+ * Writes *objective = L of this run and grad[ncell*10] = dL/dlog(rho) per
+ * cell and density component id (Fortran order (nrg,ntg,npg,10)), the
+ * derivative of this run's estimate with its random numbers held fixed:
+ * peel-off rays contribute -C*tau, and the packet's own path segments their
+ * score (interaction density minus tau) times the peel-off contribution
+ * that follows them.  Two passes: the forward run (peel-off kernel records
+ * each job's weighted contribution) and a replay of the contributing
+ * packets on the same streams.  Diffusion surfaces keep their
+ * start-of-iteration temperature during both passes.  The device tallies
+ * after the call hold both passes (reset before the next iteration).
+ * Gradients of parameters of a density law follow by the chain rule over
+ * grad.  No reference counterpart (the reference has no derivatives). */
+int mcrt_adjoint(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo, int64_t iphot_hi, int32_t iter,
+                 int32_t seed1, int32_t seed2, int32_t generator,
+                 const double *lam_psed, const double *lam_img, double *grad, double *objective);
+
 /* Recompute the diffusion cells' end-of-iteration temperature of the last
  * mcrt_run_iteration from the (reduced) diffusion absorption counts and the
  * whole iteration's stellar packet count -- the single-process result of

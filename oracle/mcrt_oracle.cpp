@@ -240,12 +240,34 @@ void atomic_add(double& x, double v) {
 }
 
 // ------------------------------------------------------------- packet ----
+// Path-replay adjoint of the peeled outputs (engine's mcrt_adjoint, restated
+// sequentially).  Objective L = sum lam_psed * ti + sum lam_img * image_m_i
+// (Stokes I).  With the random numbers held fixed, dL/dlog(rho[c,id]) is
+//   sum over peel-offs   -C * tau[c,id] along the peel ray
+// + sum over segments k  A_k * (delta(c,id = interaction cell, species) - tau[c,id] along k)
+// where C is a peel-off's weighted contribution and A_k the summed C of the
+// packet's peel-offs after segment k (at interactions k, k+1, ...).  Pass 1
+// runs the packet with peel-offs, pass 2 replays it (same stream, no
+// peel-offs) and scores the segments.
+struct Adjoint {
+  const double* lam_psed = nullptr;   // [npsed] weights of ti
+  const double* lam_img = nullptr;    // [nimg] weights of image_m_i
+  std::vector<double>* grad = nullptr;   // [ncell*10] this thread's sums
+  double obj = 0.0;
+  bool record = false, replay = false;
+  double A = 0.0;
+  std::vector<std::pair<int, double>> ev;   // (event index, C) of the packet, in event order
+  size_t pos = 0;
+  std::vector<std::pair<int64_t, double>> cross;   // crossings of the current peel ray: (cell, length)
+};
+
 struct Packet {
   const Model* m;
   Tally* T;
   Images* I;
   Rng rng;
   int ipeel;
+  Adjoint* adj = nullptr;
   // taunum_mod / stokes_mod / tts_mod state
   double xp, yp, zp, rsq, rtot, ux, uy, uz, tau;
   double cost, sint, cosp, sinp, phi, sip, sqp, sup, svp;
@@ -636,6 +658,12 @@ struct Packet {
 
   void tally_abs(int ir, int it, int ip, double len) {   // tauint_3d_2_fuv.f90:83-98, 122-144
     int64_t c = m->cidx(ir, it, ip);
+    if (adj && adj->replay && adj->A != 0.0) {
+      for (int id = 1; id <= MCRT_NDG2; ++id) {
+        const double d = m->dens(ir, it, ip, id);
+        if (d > 0.0) (*adj->grad)[c + m->ncell * (id - 1)] -= adj->A * (kapd[m->fopac(ir, it, ip, id) - 1] * d * len);
+      }
+    }
     for (int id = 1; id <= MCRT_NDG2; ++id) {
       double d = m->dens(ir, it, ip, id);
       if (!m->is_sg[id - 1] && d > 0.0) {
@@ -1134,6 +1162,11 @@ struct Packet {
     const double cospe = t->cospe_arr[peelid - 1], sinpe = t->sinpe_arr[peelid - 1];
     const double coste = t->coste_arr[peelid - 1], sinte = t->sinte_arr[peelid - 1];
     const double ux1 = sinte * cospe, uy1 = sinte * sinpe, uz1 = coste;
+    // adjoint pass 1: the peel walk draws (testgrid re-locations) from a
+    // copy of the stream, as the engine's peel-off kernel uses its own
+    const Rng saved = rng;
+    struct Restore { Packet* p; const Rng& r; bool on; ~Restore() { if (on) p->rng = r; } } restore{this, saved, adj != nullptr};
+    if (adj) adj->cross.clear();
     if (onw) {
       bool inner = std::fabs(rs1 - m->r2arr[ir - 1]) < std::fabs(rs1 - m->r2arr[ir]);
       bool outwards = ux1 * x1 + uy1 * y1 + uz1 * z1 > 0.0;
@@ -1155,6 +1188,7 @@ struct Packet {
       if (dt == HUGE_D || iface < 1 || iface > 6) { T->cnt[MCRT_C_GEOM_FAIL]++; return; }
       double opac = cell_opac(ir, it, ip);
       tsum = tsum + opac * dt;
+      if (adj) adj->cross.emplace_back(m->cidx(ir, it, ip), dt);
       if (tsum > 25.0) return;
       switch (iface) {
         case 1: ir = ir - 1; break;
@@ -1191,10 +1225,14 @@ struct Packet {
     double vx = (ximage + c.rmaxi) / fractxh, vy = (yimage + c.rmaxi) / fractxh;
     double rho2 = ximage * ximage + yimage * yimage;
     int inub = freq_bin(nub);
+    int64_t img_k = -1;
+    int64_t e_list[64];
+    int ne = 0;
     if (c.output_imcube && vx > -1.0e9 && vx < 1.0e9 && vy > -1.0e9 && vy < 1.0e9) {
       int ix = (int)vx + 1, iy = (int)vy + 1;
       if (ix <= c.nxhst && iy <= c.nxhst && ix > 0 && iy > 0) {
         int64_t k = (int64_t)(peelid - 1) + (int64_t)c.npeel * ((ix - 1) + (int64_t)c.nxhst * ((iy - 1) + (int64_t)c.nxhst * (inub - 1)));
+        img_k = k;
         atomic_add(I->im[0][k], q_i);
         atomic_add(I->im[1][k], q_q);
         atomic_add(I->im[2][k], q_u);
@@ -1207,12 +1245,14 @@ struct Packet {
       if (rho2 < t->aperture2[ia - 1]) {
         for (int k = 0; k < 3; ++k) {
           int64_t e = (inub - 1) + (int64_t)c.nfreq * ((peelid - 1) + (int64_t)c.npeel * ((ia - 1) + (int64_t)c.nap * (indx[k] - 1)));
+          if (ne < 64) e_list[ne++] = e;
           T->psed[0][e] += q_i; T->psed[1][e] += q_q; T->psed[2][e] += q_u; T->psed[3][e] += q_v;
           T->psed[4][e] += q_i * q_i; T->psed[5][e] += q_q * q_q; T->psed[6][e] += q_u * q_u; T->psed[7][e] += q_v * q_v;
           T->psed[8][e] += 1.0;
         }
       }
     }
+    if (adj && adj->record) adjoint_peel(q_i, img_k, e_list, ne);
   }
 
   void peel_all(double s_i, int ir, int it, int ip, int idust2) {
@@ -1296,7 +1336,9 @@ struct Packet {
     int nth = 0;
     for (int id = 1; id <= MCRT_NDG2; ++id) if (!m->is_sg[id - 1] && m->dens(ir, it, ip, id) > 0.0) ++nth;
     if (nth == 0) return false;
-    const int32_t k = m->ndiff[cs].fetch_add(nth) + nth;
+    // adjoint evaluations freeze the surface at its start-of-iteration
+    // temperature (a replay must see the forward pass's heating)
+    const int32_t k = adj ? 0 : m->ndiff[cs].fetch_add(nth) + nth;
     double T4d = g->tdust[cs] * g->tdust[cs];
     T4d = T4d * T4d;
     const double T4 = T4d + (double)k * (4.0 * PI * T4s / (m->nphot_diff * dA));
@@ -1422,6 +1464,41 @@ struct Packet {
     return idust2;
   }
 
+  // ------------------------------------------------------------ adjoint
+  // Replay: before the walk that follows interaction k (k = nscat + nabsev;
+  // 0 after the emission), drop the peel-offs of event k from A.
+  void adjoint_advance() {
+    if (!adj || !adj->replay) return;
+    const int k = nscat + nabsev;
+    while (adj->pos < adj->ev.size() && adj->ev[adj->pos].first <= k) adj->A -= adj->ev[adj->pos++].second;
+  }
+  // Replay: the interaction density kapd*rho of the selected component at
+  // the end of the segment.
+  void adjoint_interaction(int ir, int it, int ip, int idust2) {
+    if (!adj || !adj->replay || adj->A == 0.0) return;
+    (*adj->grad)[m->cidx(ir, it, ip) + m->ncell * (idust2 - 1)] += adj->A;
+  }
+  // Pass 1: weighted contribution of one binned peel-off and its -C*tau
+  // terms along the recorded ray.
+  void adjoint_peel(double q_i, int64_t img_k, const int64_t* e_list, int ne) {
+    const double* lp = adj->lam_psed;
+    double C = 0.0;
+    for (int j = 0; j < ne; ++j) C += lp[e_list[j]] * q_i;
+    if (img_k >= 0 && adj->lam_img) C += adj->lam_img[img_k] * q_i;
+    adj->obj += C;
+    const int k = nscat + nabsev;
+    if (!adj->ev.empty() && adj->ev.back().first == k) adj->ev.back().second += C;
+    else adj->ev.emplace_back(k, C);
+    if (C == 0.0) return;
+    for (const auto& cr : adj->cross) {
+      const int64_t c = cr.first;
+      for (int id = 1; id <= MCRT_NDG2; ++id) {
+        const double d = m->g->densarr[c + m->ncell * (id - 1)];
+        if (d > 0.0) (*adj->grad)[c + m->ncell * (id - 1)] -= C * (kapd[m->g->findopac[c + m->ncell * (id - 1)] - 1] * d * cr.second);
+      }
+    }
+  }
+
   // ----------------------------------------------------------- packet
   // newdisktherm_5_fuv.f90:220-491 for one packet, then propagate
   int run(int64_t iphot, int64_t np, int64_t ns, int64_t npacc, int64_t npaccstar, int ips) {
@@ -1494,12 +1571,14 @@ struct Packet {
     exitflag = 0;
     int iscat = 0, iint = 0, idust2 = 0;
     int64_t nev = 0;
+    adjoint_advance();
     tau = -std::log(ran());
     if (!tauint(ii[0], ii[1], ii[2])) return 3;
     int ir = ii[0], it = ii[1], ip = ii[2];
     if (exitflag != 1) {
       idust2 = select_dust(ir, it, ip);
       if (idust2 == 0) return 3;
+      adjoint_interaction(ir, it, ip, idust2);
       T->scal[MCRT_S_TOT] += 1.0;
       for (;;) {
         int fo = m->fopac(ir, it, ip, idust2) - 1;
@@ -1546,6 +1625,7 @@ struct Packet {
           if (ipeel == 1 && !c.partial_peeloff) peel_all(sip, ii[0], ii[1], ii[2], idust2);
           ++iint;
         }
+        adjoint_advance();
         tau = -std::log(ran());
         xpold = xp; ypold = yp; zpold = zp;
         ux = sint * cosp;
@@ -1565,6 +1645,7 @@ struct Packet {
         }
         idust2 = select_dust(ir, it, ip);
         if (idust2 == 0) return 3;
+        adjoint_interaction(ir, it, ip, idust2);
       }
     }
     // exit: bin into the SED arrays (propagate_5_fuv.f90:231-320)
@@ -1916,3 +1997,102 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
 }
 
 }  // extern "C"
+
+
+// Path-replay adjoint (see struct Adjoint): packets lo..hi of an np-packet
+// iteration with peel-offs, objective and dL/dlog(rho) per (cell, component
+// id) summed into grad[ncell*10] (Fortran order (nrg,ntg,npg,10)), objective
+// into *obj.  Test infrastructure: the FP64 reference of mcrt_adjoint.
+extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables* tab, int64_t np,
+                              int64_t iphot_lo, int64_t iphot_hi, int32_t iter, int32_t seed1, int32_t seed2,
+                              int32_t generator, int32_t nthreads, const double* lam_psed, const double* lam_img,
+                              double* grad, double* obj) {
+  if (iter < 1 || !lam_psed || !grad || !obj) return MCRT_ERR_ARG;
+  const int64_t block0 = (int64_t)(iter - 1) * np;
+  Model m;
+  m.c = *cfg;
+  m.g = grid;
+  m.t = tab;
+  m.nrg = cfg->nrg; m.ntg = cfg->ntg; m.npg = cfg->npg;
+  m.ncell = (int64_t)m.nrg * m.ntg * m.npg;
+  zetainit(m.inczeta);
+  const bool sg[MCRT_NDG2] = {false, false, false, false, true, true, true, true, false, false};
+  for (int i = 0; i < MCRT_NDG2; ++i) m.is_sg[i] = sg[i];
+  m.rmincgs = cfg->rstar * RSOL;
+  m.pad_walls();
+  if (cfg->ilucy != 1) return MCRT_ERR_UNSUPPORTED;
+  std::vector<std::atomic<int32_t>> ndiff(m.ncell);
+  for (auto& a : ndiff) a.store(0);
+  m.ndiff = ndiff.data();
+  int64_t npout = (int64_t)(cfg->isrf_frac * (double)np);
+  double rn = cfg->isrf_frac * (double)np;
+  if (rn - (double)npout > 0.5) npout++;
+  int64_t ns = (int64_t)((double)np * (1.0 - cfg->accfrac - cfg->isrf_frac));
+  rn = (double)(float)np * (1.0 - cfg->accfrac - cfg->isrf_frac);
+  if (rn - (double)ns > 0.5) ns++;
+  int64_t npacc = (int64_t)((double)np * cfg->accfrac);
+  int64_t npaccstar = (int64_t)(cfg->accfrac2 * (double)np);
+  if (ns + npacc + npout != np) ns = ns + np - (ns + npacc + npout);
+  if (npout > 0) return MCRT_ERR_UNSUPPORTED;
+  m.nphot_diff = (double)ns * (double)(iphot_hi - iphot_lo + 1) / (double)np;
+  const int ips = (cfg->rddust > 100.0) ? 1 : 0;
+  const int64_t nsed = (int64_t)cfg->nfreq * cfg->nmu * cfg->nph * cfg->nap * MCRT_NO;
+  const int64_t npsed = (int64_t)cfg->nfreq * cfg->npeel * cfg->nap * MCRT_NO;
+  const int64_t nimg = (int64_t)cfg->npeel * cfg->nxhst * cfg->nxhst * cfg->nfreq;
+  Images img;
+  for (auto& v : img.im) v.assign(cfg->output_imcube ? nimg : 0, 0.0);
+  const int nt = std::max(1, (int)nthreads);
+  std::vector<Tally> tl(nt);
+  for (auto& t : tl) t.init(m.ncell, nsed, npsed);
+  std::vector<std::vector<double>> gl(nt, std::vector<double>(m.ncell * MCRT_NDG2, 0.0));
+  std::vector<double> objs(nt, 0.0);
+  std::atomic<int64_t> next(iphot_lo);
+  auto worker = [&](int tid) {
+    Packet p;
+    Adjoint A;
+    A.lam_psed = lam_psed;
+    A.lam_img = cfg->output_imcube ? lam_img : nullptr;
+    A.grad = &gl[tid];
+    p.m = &m; p.T = &tl[tid]; p.I = &img; p.adj = &A;
+    for (auto* v : {&p.kappa, &p.albedo, &p.g, &p.pl, &p.g2, &p.onemg2, &p.g2p1, &p.twog, &p.kapd}) v->assign(cfg->nopac, 0.0);
+    for (;;) {
+      const int64_t lo = next.fetch_add(64);
+      if (lo > iphot_hi) break;
+      const int64_t hi = std::min(lo + 63, iphot_hi);
+      for (int64_t iphot = lo; iphot <= hi; ++iphot) {
+        // pass 1: the packet with its peel-offs
+        A.ev.clear();
+        A.record = true; A.replay = false;
+        p.ipeel = 1;
+        p.rng = stream(seed1, seed2, generator, block0 + iphot - 1);
+        p.nscat = p.nabsev = p.ncross = p.nstar = p.ndiffev = 0;
+        p.run(iphot, np, ns, npacc, npaccstar, ips);
+        double R = 0.0;
+        for (const auto& e : A.ev) R += e.second;
+        if (R == 0.0) continue;
+        // pass 2: replay on the same stream, scoring the segments
+        A.record = false; A.replay = true;
+        A.A = R; A.pos = 0;
+        p.ipeel = 0;
+        p.rng = stream(seed1, seed2, generator, block0 + iphot - 1);
+        p.nscat = p.nabsev = p.ncross = p.nstar = p.ndiffev = 0;
+        p.run(iphot, np, ns, npacc, npaccstar, ips);
+        A.replay = false;
+      }
+    }
+    objs[tid] = A.obj;
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < nt; ++i) th.emplace_back(worker, i);
+  worker(0);
+  for (auto& t : th) t.join();
+  for (int64_t k = 0; k < m.ncell * MCRT_NDG2; ++k) {
+    double s = 0.0;
+    for (int i = 0; i < nt; ++i) s += gl[i][k];
+    grad[k] = s;
+  }
+  double o = 0.0;
+  for (int i = 0; i < nt; ++i) o += objs[i];
+  *obj = o;
+  return MCRT_OK;
+}

@@ -37,6 +37,11 @@ def load():
                                    C.POINTER(abi.Tallies), C.POINTER(abi.PacketLog), C.c_int64,
                                    C.POINTER(C.c_double)]
         lib.oracle_run.restype = C.c_int
+        D = C.POINTER(C.c_double)
+        lib.oracle_adjoint.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
+                                       C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_int32, D, D, D, D]
+        lib.oracle_adjoint.restype = C.c_int
         lib.oracle_rng.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.oracle_inczeta.argtypes = [C.POINTER(C.c_double)]
@@ -98,3 +103,28 @@ def tfinal(bundle: abi.Bundle, dtauabs: np.ndarray, nphot: int, iteration: int, 
     if rc != 0:
         raise RuntimeError(f"oracle_tfinal failed with code {rc}")
     return td, sig
+
+
+def adjoint(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img: np.ndarray | None = None,
+            lo: int = 1, hi: int | None = None, *, iteration: int = 1, seeds=(12345678, 87654321),
+            generator: int = 1, threads: int | None = None):
+    """Path-replay adjoint of L = sum lam_psed*ti + sum lam_img*image_m_i:
+    returns (grad [ncell*10] = dL/dlog(rho) per cell and component id,
+    Fortran order, and L).  Diffusion surfaces keep their start-of-iteration
+    temperature (no within-iteration heating)."""
+    lib = load()
+    hi = np_total if hi is None else hi
+    threads = threads or os.cpu_count() or 1
+    c = bundle.config
+    ncell = c.nrg * c.ntg * c.npg
+    lp = np.ascontiguousarray(lam_psed, dtype=np.float64)
+    li = None if lam_img is None else np.ascontiguousarray(lam_img, dtype=np.float64)
+    grad = np.zeros(ncell * 10, np.float64)
+    obj = C.c_double(0.0)
+    D = C.POINTER(C.c_double)
+    rc = lib.oracle_adjoint(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables), np_total, lo, hi,
+                            iteration, seeds[0], seeds[1], generator, threads, lp.ctypes.data_as(D),
+                            li.ctypes.data_as(D) if li is not None else None, grad.ctypes.data_as(D), C.byref(obj))
+    if rc != 0:
+        raise RuntimeError(f"oracle_adjoint failed with code {rc}")
+    return grad, obj.value

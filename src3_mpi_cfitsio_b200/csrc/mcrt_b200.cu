@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "mcrt_device.cuh"
 
 namespace mcrt {
@@ -71,6 +73,14 @@ struct mcrt_ctx {
   bool kt_pending[4] = {};
   double kt_ms[4] = {};
   int64_t kt_walks = 0, kt_walk_cross = 0, kt_launch[4] = {};
+  // path-replay adjoint buffers (mcrt_adjoint)
+  AdjointArgs adj{};
+  int64_t adj_rec_used = 0;
+  int64_t adj_npk_cap = 0;
+  unsigned long long *d_adj_nlist = nullptr;
+  void *d_adj_tmp = nullptr;
+  size_t adj_tmp_bytes = 0;
+  int64_t adj_sort_cap = 0;           // capacity of the sorted copies (skey, sc) and the sort scratch
   bool have_grid = false, have_tables = false;
   bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
   std::string err;
@@ -317,6 +327,24 @@ __global__ void tfinal_stats(int nrg, int ntg, const double* told, const double*
 // the library holds it (3*524288+16 doubles, 12 MiB) on each device it uses.
 constexpr int64_t kNoAllocMaxCells = 524288;
 static __device__ __align__(256) double g_tfinal_scratch[3 * kNoAllocMaxCells + 16];
+
+// Sorted adjoint records: the range [start, end) of each packet's records
+// and the list of packets that have any (keys ~0 mark jobs without a
+// contribution and sort last).
+__global__ void adjoint_ranges(const unsigned long long* key, int64_t n, int64_t* start, int64_t* end, int32_t* list,
+                               unsigned long long* nlist) {
+  const unsigned long long none = ~0ull;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = key[i];
+    if (k == none) continue;
+    const unsigned long long p = k >> kAdjEvBits;
+    if (i == 0 || (key[i - 1] >> kAdjEvBits) != p) {
+      start[p] = i;
+      list[atomicAdd(nlist, 1ull)] = (int32_t)p;
+    }
+    if (i == n - 1 || key[i + 1] == none || (key[i + 1] >> kAdjEvBits) != p) end[p] = i + 1;
+  }
+}
 
 // dst[i] += src[i]; kind 0: f64 -> f64, 1: i64 -> u64, 2: f32 -> f64, 3: i32 -> i32
 __global__ void add_tally(int kind, const void* src, void* dst, int64_t n) {
@@ -687,8 +715,37 @@ int mcrt_download_packet_log(mcrt_ctx* ctx, mcrt_packet_log* out, int64_t n) {
   return MCRT_OK;
 }
 
-int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
-                       int32_t seed1, int32_t seed2, int32_t generator) {
+// Grow the adjoint's job records to hold at least `need`, keeping the ones
+// written so far (the host calls it between launches).
+static int adjoint_grow(mcrt_ctx* ctx, int64_t need) {
+  AdjointArgs& A = ctx->adj;
+  const int64_t cap = std::max<int64_t>(need, 2 * A.rec_cap);
+  unsigned long long* rk = nullptr;
+  double* rcv = nullptr;
+  int rc;
+  if ((rc = dalloc(ctx, &rk, cap)) || (rc = dalloc(ctx, &rcv, cap))) return rc;
+  const int64_t used = ctx->adj_rec_used;
+  CK(cudaMemsetAsync(rk, 0xff, (size_t)cap * 8, ctx->stream));
+  CK(cudaMemsetAsync(rcv, 0, (size_t)cap * 8, ctx->stream));
+  if (used > 0) {
+    CK(cudaMemcpyAsync(rk, A.rec_key, (size_t)used * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(rcv, A.rec_c, (size_t)used * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, A.rec_key);
+  dfree(ctx, A.rec_c);
+  A.rec_key = rk;
+  A.rec_c = rcv;
+  A.rec_cap = cap;
+  return MCRT_OK;
+}
+
+// adj_mode 0: an ordinary iteration; 1: the adjoint's forward pass (wave
+// schedule, no tail launch so that every peel-off goes through the peel-off
+// kernel, records in ctx->adj); 2: the adjoint's replay (warp schedule over
+// ctx->adj's packet list, no peel-offs).
+static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
+                              int32_t seed1, int32_t seed2, int32_t generator, int adj_mode) {
   if (!ctx) return MCRT_ERR_ARG;
   if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
   if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range %lld..%lld of %lld", (long long)lo, (long long)hi, (long long)np);
@@ -745,8 +802,12 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   const int64_t npk = hi - lo + 1;
   P.event_batch = ctx->event_batch;
   const bool mixed = ctx->precision == MCRT_PREC_MIXED;
-  const bool wave = ctx->schedule == MCRT_SCHED_WAVE;
-  const bool warp = !wave && (ctx->schedule == MCRT_SCHED_WARP || mixed);   // the mixed build has no per-thread kernel
+  const bool wave = adj_mode == 1 || (adj_mode == 0 && ctx->schedule == MCRT_SCHED_WAVE);
+  const bool warp = !wave && (adj_mode == 2 || ctx->schedule == MCRT_SCHED_WARP || mixed);   // the mixed build has no per-thread kernel
+  if (adj_mode) {
+    P.adj = ctx->adj;
+    P.adj.mode = adj_mode;
+  }
   // peel-offs go through the job queue and the peel-off kernel
   const bool queue = P.ipeel && (warp || wave) && ctx->dm.nslot <= kJobSlots && c.npeel > 0;
   const int64_t wave_slots = wave ? std::min<int64_t>(ctx->wave_pool, npk) : 0;
@@ -823,8 +884,21 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     }
     return MCRT_OK;
   };
-  auto launch_peel = [&]() -> int {
+  // njobs_now: jobs in the queue at this launch (adjoint record bookkeeping)
+  auto launch_peel = [&](int64_t njobs_now) -> int {
     ++launches;
+    if (adj_mode == 1) {
+      const int64_t n = std::min<int64_t>(njobs_now, ctx->job_cap);
+      if (ctx->adj_rec_used + n > ctx->adj.rec_cap) {   // grow the records (no kernel writes them now)
+        int rc = adjoint_grow(ctx, ctx->adj_rec_used + n);
+        if (rc) return rc;
+        P.adj.rec_key = ctx->adj.rec_key;
+        P.adj.rec_c = ctx->adj.rec_c;
+        P.adj.rec_cap = ctx->adj.rec_cap;
+      }
+      P.adj.rec_base = ctx->adj_rec_used;
+      ctx->adj_rec_used += n;
+    }
     int rc = kt_begin(KT_PEEL);
     if (rc) return rc;
     cudaError_t e = mixed ? launch_peel_mixed(P, ctx->d_next + 2, peel_grid, ctx->stream)
@@ -850,8 +924,9 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     const int egrid = ctx->nsm * (mixed ? wave_event_mixed_blocks_per_sm() : wave_event_fp64_blocks_per_sm());
     const int wgrid = ctx->nsm * (mixed ? wave_walk_mixed_blocks_per_sm() : wave_walk_fp64_blocks_per_sm());
     const int tgrid = ctx->nsm * (mixed ? wave_tail_mixed_blocks_per_sm() : wave_tail_fp64_blocks_per_sm());
-    const unsigned long long tail_live = ctx->wave_tail < 0 ? (unsigned long long)tgrid * kTransportBlock * 8ull
-                                                            : (unsigned long long)ctx->wave_tail;
+    const unsigned long long tail_live = adj_mode ? 0ull
+                                         : ctx->wave_tail < 0 ? (unsigned long long)tgrid * kTransportBlock * 8ull
+                                                              : (unsigned long long)ctx->wave_tail;
     CK(cudaMemsetAsync(ctx->d_next, 0, 4 * sizeof(unsigned long long), ctx->stream));
     cudaError_t e = launch_wave_init(W, ctx->stream);
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave init: %s", cudaGetErrorString(e));
@@ -892,7 +967,7 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
       const bool tail = tail_live > 0 && (int64_t)h[2] >= npk && live <= tail_live;
       if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && h[3] > 0))) {
         CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
-        if ((rc = launch_peel())) return rc;
+        if ((rc = launch_peel((int64_t)h[3]))) return rc;
         CK(cudaMemsetAsync(ctx->d_next + 1, 0, sizeof(unsigned long long), ctx->stream));
       }
       if (tail) {
@@ -908,8 +983,10 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
       }
     }
     if (queue) {
+      CK(cudaMemcpyAsync(h + 3, ctx->d_next + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
       CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
-      if ((rc = launch_peel())) return rc;
+      if ((rc = launch_peel((int64_t)h[3]))) return rc;
     }
     CK(cudaMemcpyAsync(h + 5, &ctx->d_wctl->walk_cross, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        ctx->stream));
@@ -933,7 +1010,7 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "transport launch: %s", cudaGetErrorString(e));
     ++launches;
     if (queue) {
-      int rc = launch_peel();
+      int rc = launch_peel(0);
       if (rc) return rc;
     }
   }
@@ -958,6 +1035,122 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     ctx->kt_walk_cross = (int64_t)ctx->h_wctl[5];
   }
   CK(cudaGetLastError());
+  return MCRT_OK;
+}
+
+int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
+                       int32_t seed1, int32_t seed2, int32_t generator) {
+  return run_iteration_impl(ctx, np, lo, hi, iter, ipeel, seed1, seed2, generator, 0);
+}
+
+int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t seed1, int32_t seed2,
+                 int32_t generator, const double* lam_psed, const double* lam_img, double* grad, double* objective) {
+  if (!ctx || !lam_psed || !grad || !objective) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range");
+  const mcrt_config& c = ctx->cfg;
+  if (c.npeel < 1) return fail(ctx, MCRT_ERR_ARG, "the adjoint differentiates peeled outputs: npeel must be >= 1");
+  if (ctx->dm.nslot > kJobSlots) return fail(ctx, MCRT_ERR_UNSUPPORTED, "adjoint needs at most %d opacity species", kJobSlots);
+  const int64_t npk = hi - lo + 1;
+  if (npk >= ((int64_t)1 << 31)) return fail(ctx, MCRT_ERR_ARG, "adjoint packet range must be < 2^31");
+  CK(cudaSetDevice(ctx->device));
+  const int64_t ncell = ctx->ncell;
+  AdjointArgs& A = ctx->adj;
+  int rc;
+  // buffers (kept between calls; re-sized for larger ranges)
+  if (!A.grad) {
+    double *lp, *gr, *ob, *li = nullptr;
+    if ((rc = dalloc(ctx, &lp, (size_t)std::max<int64_t>(ctx->npsed, 1))) || (rc = dalloc(ctx, &gr, (size_t)ncell * 10)) ||
+        (rc = dalloc(ctx, &ob, 1)) || (ctx->nimg > 0 && (rc = dalloc(ctx, &li, (size_t)ctx->nimg))) ||
+        (rc = dalloc(ctx, &ctx->d_adj_nlist, 1)))
+      return rc;
+    A.lam_psed = lp; A.grad = gr; A.obj = ob; A.lam_img = li;
+  }
+  if (ctx->adj_npk_cap < npk) {
+    for (void* q : {(void*)A.rec_key, (void*)A.rec_c, (void*)A.start, (void*)A.end, (void*)A.list})
+      if (q) dfree(ctx, q);
+    A.rec_key = nullptr; A.rec_c = nullptr; A.start = nullptr; A.end = nullptr;
+    A.list = nullptr; ctx->adj_npk_cap = 0;
+    const int64_t cap = std::max<int64_t>(16 * npk, 1 << 16);
+    unsigned long long* rk;
+    double* rcv;
+    int64_t *st, *en;
+    int32_t* ls;
+    if ((rc = dalloc(ctx, &rk, cap)) || (rc = dalloc(ctx, &rcv, cap)) || (rc = dalloc(ctx, &st, npk)) ||
+        (rc = dalloc(ctx, &en, npk)) || (rc = dalloc(ctx, &ls, npk)))
+      return rc;
+    A.rec_key = rk; A.rec_c = rcv; A.start = st; A.end = en; A.list = ls;
+    A.rec_cap = cap;
+    ctx->adj_npk_cap = npk;
+    ctx->adj_sort_cap = 0;
+  }
+  CK(cudaMemcpyAsync((void*)A.lam_psed, lam_psed, (size_t)ctx->npsed * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->nimg > 0) {
+    if (lam_img) CK(cudaMemcpyAsync((void*)A.lam_img, lam_img, (size_t)ctx->nimg * 8, cudaMemcpyHostToDevice, ctx->stream));
+    else CK(cudaMemsetAsync((void*)A.lam_img, 0, (size_t)ctx->nimg * 8, ctx->stream));
+  }
+  CK(cudaMemsetAsync(A.grad, 0, (size_t)ncell * 10 * 8, ctx->stream));
+  CK(cudaMemsetAsync(A.obj, 0, 8, ctx->stream));
+  CK(cudaMemsetAsync(A.rec_key, 0xff, (size_t)A.rec_cap * 8, ctx->stream));
+  CK(cudaMemsetAsync(A.rec_c, 0, (size_t)A.rec_cap * 8, ctx->stream));
+  CK(cudaMemsetAsync((void*)A.start, 0, (size_t)npk * 8, ctx->stream));
+  CK(cudaMemsetAsync((void*)A.end, 0, (size_t)npk * 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_adj_nlist, 0, 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream));
+  ctx->adj_rec_used = 0;
+  double total_ms = 0.0;
+  // forward pass: the iteration with its peel-offs, records and -C*tau terms
+  if ((rc = run_iteration_impl(ctx, np, lo, hi, iter, 1, seed1, seed2, generator, 1))) return rc;
+  total_ms += ctx->last_ms;
+  int32_t herr = 0;
+  CK(cudaMemcpy(&herr, ctx->d_err, 4, cudaMemcpyDeviceToHost));
+  if (herr) return fail(ctx, MCRT_ERR_ARG, "adjoint: peel-off record capacity exceeded");
+  // records by (packet, event); the range of each packet; the packet list
+  const int64_t nrec = ctx->adj_rec_used;
+  cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
+  CK(cudaEventRecord(e0, ctx->stream));
+  if (nrec > ctx->adj_sort_cap) {      // sorted copies and scratch for nrec records
+    for (void* q : {(void*)A.skey, (void*)A.sc, ctx->d_adj_tmp})
+      if (q) dfree(ctx, q);
+    A.skey = nullptr; A.sc = nullptr; ctx->d_adj_tmp = nullptr;
+    const int64_t cap = std::max<int64_t>(nrec, 2 * ctx->adj_sort_cap);
+    if (cap > INT32_MAX) return fail(ctx, MCRT_ERR_ARG, "adjoint: more than 2^31 peel-off records");
+    unsigned long long* sk;
+    double* scv;
+    if ((rc = dalloc(ctx, &sk, cap)) || (rc = dalloc(ctx, &scv, cap))) return rc;
+    size_t tmp = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, A.rec_key, sk, A.rec_c, scv, (int)cap));
+    if ((rc = dalloc(ctx, (char**)&ctx->d_adj_tmp, std::max<size_t>(tmp, 1)))) return rc;
+    ctx->adj_tmp_bytes = tmp;
+    A.skey = sk;
+    A.sc = scv;
+    ctx->adj_sort_cap = cap;
+  }
+  if (nrec > 0) {
+    size_t tmp = ctx->adj_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairs(ctx->d_adj_tmp, tmp, A.rec_key, (unsigned long long*)A.skey, A.rec_c,
+                                       (double*)A.sc, (int)nrec, 0, 64, ctx->stream));
+    adjoint_ranges<<<(int)std::min<int64_t>((nrec + 255) / 256, 8192), 256, 0, ctx->stream>>>(
+        A.skey, nrec, (int64_t*)A.start, (int64_t*)A.end, (int32_t*)A.list, ctx->d_adj_nlist);
+    CK(cudaGetLastError());
+  }
+  unsigned long long nlist = 0;
+  CK(cudaMemcpyAsync(&nlist, ctx->d_adj_nlist, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaEventRecord(e1, ctx->stream));
+  CK(cudaEventSynchronize(e1));
+  float sort_ms = 0.f;
+  CK(cudaEventElapsedTime(&sort_ms, e0, e1));
+  total_ms += sort_ms;
+  // replay pass: the packets with peel-off records, scoring their segments
+  A.nlist = (int64_t)nlist;
+  if (nlist > 0) {
+    if ((rc = run_iteration_impl(ctx, np, lo, hi, iter, 0, seed1, seed2, generator, 2))) return rc;
+    total_ms += ctx->last_ms;
+  }
+  ctx->last_ms = total_ms;
+  CK(cudaMemcpyAsync(grad, A.grad, (size_t)ncell * 10 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(objective, A.obj, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return MCRT_OK;
 }
 

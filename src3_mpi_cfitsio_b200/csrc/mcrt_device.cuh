@@ -99,6 +99,7 @@ struct __align__(16) PeelJob {
                                   // tabulated matrix: g = wavelength weight f, pl = table row
   int32_t r, t, p;                // cell
   uint32_t bits;                  // onw | iflag<<1 | direct<<2 | (i_orig)<<3 | (inub-1)<<8
+  int32_t pkt, ev;                // packet index in its launch range, event index (0 = emission, k = interaction k)
 };
 
 // Wavefront schedule: one in-flight packet per pool slot, kept in HBM
@@ -145,6 +146,33 @@ struct WaveArgs {
   int32_t pad_;
 };
 
+// Path-replay adjoint (mcrt_adjoint).  mode 0: off.  mode 1, forward pass:
+// the peel-off kernel records every job's weighted contribution C (one
+// record per job: key = packet << 24 | event) and re-walks each contributing
+// ray to scatter -C * tau per (cell, component).  mode 2, replay pass: the
+// warp-scheduled loop replays the packets that have records on the same
+// streams and scores their segments with A, the sum of their later
+// peel-offs' C.
+struct AdjointArgs {
+  int32_t mode;
+  int32_t pad_;
+  const double* lam_psed;          // [npsed] weights of ti
+  const double* lam_img;           // [nimg] weights of image_m_i, or nullptr
+  double* grad;                    // [10][ncell] dL/dlog(rho) per component id
+  double* obj;                     // objective
+  unsigned long long* rec_key;     // [rec_cap] forward: written per job (~0: none)
+  double* rec_c;                   // [rec_cap]
+  int64_t rec_base;                // record of job 0 of this peel-off launch
+  int64_t rec_cap;
+  const int32_t* list;             // replay: packets with records
+  int64_t nlist;
+  const int64_t* start;            // replay: sorted record range [start, end) per packet
+  const int64_t* end;
+  const unsigned long long* skey;  // replay: sorted records
+  const double* sc;
+};
+constexpr int kAdjEvBits = 24;    // event index bits of a record key
+
 struct LaunchParams {
   DevModel m;
   DevTallies t;
@@ -163,6 +191,7 @@ struct LaunchParams {
   mcrt_packet_log *log;
   int64_t nlog;
   int32_t *err;                 // device error flags
+  AdjointArgs adj;
 };
 
 }  // namespace mcrt

@@ -19,12 +19,14 @@ namespace mcrt {
 struct PeelLane {
   Packet pk;        // walk helpers (testgrid, faces, cell_opac, stokespeel, binning index)
   Ray ray;
-  int state;        // 0 walk, 1 bin, 2 need item, 3 done
+  int state;        // 0 walk, 1 bin, 2 need item, 3 done, 5 adjoint re-walk
   int dir;
   unsigned long long item;
   double si;        // I weight of this direction
   int64_t steps;
   PeelJob J;
+  double adjC;      // adjoint forward pass: weighted contribution of the binned ray
+  Rng rng0;         // stream state at the walk's start (the re-walk repeats it)
 
   __device__ PeelLane(const DevModel& m, const DevTallies& t, double* sbase) : pk(m, t, sbase) {
     state = 2;
@@ -54,7 +56,17 @@ struct PeelLane {
       si = J.si;
     }
     ++pk.c_peel;
+    rng0 = pk.rng;
     for (int s = 0; s < kJobSlots && s < m.nslot; ++s) pk.sp.kapd(s) = J.kapd[s];
+    return set_ray();
+  }
+
+  // The ray of (J, dir) at its start (peeloff_3d_2_test.f90:91-122); false
+  // if it ends at once.
+  __device__ bool set_ray() {
+    const DevModel& m = pk.m;
+    const double cospe = __ldg(m.cospe + dir - 1), sinpe = __ldg(m.sinpe + dir - 1);
+    const double coste = __ldg(m.coste + dir - 1), sinte = __ldg(m.sinte + dir - 1);
     ray.x = J.x; ray.y = J.y; ray.z = J.z; ray.rs = J.rs; ray.rt = J.rt;
     ray.r = J.r; ray.t = J.t; ray.p = J.p; ray.onw = (J.bits & 1u) != 0; ray.peel = true; ray.tsum = 0.0;
     ray.vx = sinte * cospe;
@@ -73,8 +85,10 @@ struct PeelLane {
     return true;
   }
 
-  // one crossing (peeloff_3d_2_test.f90:133-214); sets state 1 (bin) or 2 (done, no bin)
-  __device__ __forceinline__ void step() {
+  // one crossing (peeloff_3d_2_test.f90:133-214); sets state 1 (bin) or 2
+  // (done, no bin).  In the adjoint re-walk (state 5) the same crossings
+  // scatter -C * tau per (cell, component) and the walk ends in state 2.
+  __device__ __forceinline__ void step(const LaunchParams& P) {
     const DevModel& m = pk.m;
     Ray& R = ray;
     pk.testgrid(R.x, R.y, R.z, R.rs, R.rt, R.r, R.t, R.p, R.onw);
@@ -85,9 +99,16 @@ struct PeelLane {
     int iface;
     w.next(R.onw, dt, iface);
     if (dt == HUGE_D || iface < 1 || iface > 6 || ++steps > 10000000) { state = 2; return; }
-    const CellRec c = m.cells[pk.cidx(R.r, R.t, R.p)];
+    const int64_t ci = pk.cidx(R.r, R.t, R.p);
+    const CellRec c = m.cells[ci];
     R.tsum = R.tsum + pk.cell_opac(c) * dt;
     if (R.tsum > 25.0) { state = 2; return; }
+    if (state == 5) {
+      const int n = cell_n(c.meta);
+      for (int k = 0; k < n; ++k)
+        atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1),
+                  -(adjC * (pk.sp.kapd(cell_slot(c.meta, k)) * c.rho[k] * dt)));
+    }
     pk.step_index(iface, R.r, R.t, R.p);
     R.x = R.x + dt * R.vx;
     R.y = R.y + dt * R.vy;
@@ -97,13 +118,13 @@ struct PeelLane {
 #ifndef MCRT_MIXED
     R.rt = sqrt(R.rs);            // the mixed testgrid forms rt itself
 #endif
-    ++pk.c_pcross;
-    if (R.r == m.nrg) { state = 1; return; }
+    if (state != 5) ++pk.c_pcross;
+    if (R.r == m.nrg) { state = (state == 5) ? 2 : 1; return; }
     if (R.r == 0) { state = 2; return; }
   }
 
   // peeloff_3d_2_test.f90:217-345
-  __device__ void bin() {
+  __device__ void bin(const LaunchParams& P) {
     const DevModel& m = pk.m;
     const int id = dir;
     ++pk.c_pbin;
@@ -141,10 +162,13 @@ struct PeelLane {
     const int inub = (int)(J.bits >> 8) + 1;
     const int i_orig = (int)((J.bits >> 3) & 31u);
     const DevTallies& T = pk.T;
+    const bool adj = P.adj.mode == 1;
+    adjC = 0.0;
     if (m.output_imcube && vx > -1.0e9 && vx < 1.0e9 && vy > -1.0e9 && vy < 1.0e9) {
       const int ix = (int)vx + 1, iy = (int)vy + 1;
       if (ix <= m.nxhst && iy <= m.nxhst && ix > 0 && iy > 0) {
         const int64_t k = (int64_t)(id - 1) + (int64_t)m.npeel * ((ix - 1) + (int64_t)m.nxhst * ((iy - 1) + (int64_t)m.nxhst * (inub - 1)));
+        if (adj && P.adj.lam_img) adjC += P.adj.lam_img[k] * qi;
         atomicAdd(T.img + k, qi);
         atomicAdd(T.img + m.nimg + k, qq);
         atomicAdd(T.img + 2 * m.nimg + k, qu);
@@ -157,6 +181,7 @@ struct PeelLane {
       if (rho2 < __ldg(m.aperture2 + ia - 1)) {
         for (int k = 0; k < 3; ++k) {
           const int64_t e = (inub - 1) + (int64_t)m.nfreq * ((id - 1) + (int64_t)m.npeel * ((ia - 1) + (int64_t)m.nap * (indx[k] - 1)));
+          if (adj) adjC += P.adj.lam_psed[e] * qi;
           double* Q = T.psed + e;
           atomicAdd(Q, qi); atomicAdd(Q + m.npsed, qq); atomicAdd(Q + 2 * m.npsed, qu); atomicAdd(Q + 3 * m.npsed, qv);
           atomicAdd(Q + 4 * m.npsed, qi * qi); atomicAdd(Q + 5 * m.npsed, qq * qq);
@@ -179,14 +204,32 @@ __global__ void __launch_bounds__(kBlock) peel_sched(LaunchParams P, unsigned lo
   if ((int64_t)njobs > P.job_cap) njobs = (unsigned long long)P.job_cap;
   const unsigned long long nitems = njobs * (unsigned long long)P.m.npeel;
   for (;;) {
-    const bool stepping = L.state == 0;
+    const bool stepping = L.state == 0 || L.state == 5;
     const bool pending = L.state == 1 || L.state == 2;
     const unsigned s = __ballot_sync(FULL, stepping);
     const unsigned e = __ballot_sync(FULL, pending);
     if (s == 0u && e == 0u) break;
     if (s == 0u || __popc(e) >= batch) {
       if (pending) {
-        if (L.state == 1) { L.bin(); L.state = 2; }
+        if (L.state == 1) {
+          L.bin(P);
+          L.state = 2;
+          if (P.adj.mode == 1 && L.adjC != 0.0) {
+            // adjoint forward pass: record the job's contribution, then walk
+            // the ray again (same stream state) to scatter -C * tau
+            const unsigned long long jid = L.item / (unsigned long long)P.m.npeel;
+            const int64_t r = P.adj.rec_base + (int64_t)jid;
+            if (r < P.adj.rec_cap) {
+              P.adj.rec_key[r] = ((unsigned long long)L.J.pkt << kAdjEvBits) | (unsigned long long)L.J.ev;
+              atomicAdd(P.adj.rec_c + r, L.adjC);
+            } else {
+              atomicAdd(P.err, 1);
+            }
+            atomicAdd(P.adj.obj, L.adjC);
+            L.pk.rng = L.rng0;
+            if (L.set_ray()) L.state = 5;
+          }
+        }
         while (L.state == 2) {
           const unsigned long long k = atomicAdd(next_item, 1ull);
           if (k >= nitems) { L.state = 3; break; }
@@ -195,7 +238,7 @@ __global__ void __launch_bounds__(kBlock) peel_sched(LaunchParams P, unsigned lo
         }
       }
     } else if (stepping) {
-      L.step();
+      L.step(P);
     }
   }
   unsigned long long v[4] = {L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin, L.pk.c_reset};

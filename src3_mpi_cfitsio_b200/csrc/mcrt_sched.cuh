@@ -58,6 +58,8 @@ struct Lane {
   double peel_si, coslp, sinlp;
   unsigned long long c_pkt, c_int, c_sca, c_geo, c_kil, c_exit, c_star, c_jobs;
   int64_t ray_steps;
+  double adjA;                      // replay: summed C of the packet's peel-offs still ahead
+  int64_t adj_pos, adj_end;         // replay: the packet's next record
 
   __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase) : pk(m, t, sbase) {
     ev = EV_FETCH;
@@ -134,6 +136,7 @@ struct Lane {
       if (R.tsum + dtau > pk.tau) {
         const double ds = (pk.tau - R.tsum) / opac;
         pk.tally_abs(ci, c, ds);
+        if (P.adj.mode == 2) adjoint_score(P, ci, c, ds);
         R.x = R.x + ds * R.vx;
         R.y = R.y + ds * R.vy;
         R.z = R.z + ds * R.vz;
@@ -145,6 +148,7 @@ struct Lane {
         return;
       }
       pk.tally_abs(ci, c, dt);
+      if (P.adj.mode == 2) adjoint_score(P, ci, c, dt);
     } else {
       R.tsum = R.tsum + opac * dt;
       if (R.tsum > 25.0) { ev = EV_PEEL_NEXT; return; }
@@ -175,6 +179,25 @@ struct Lane {
     }
   }
 
+  // ------------------------------------------------------------ adjoint
+  // Replay: -A * tau of a walk piece of length len in cell ci, per component.
+  __device__ __forceinline__ void adjoint_score(const LaunchParams& P, int64_t ci, const CellRec& c, double len) {
+    if (adjA == 0.0) return;
+    const int n = cell_n(c.meta);
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(adjA * (pk.sp.kapd(cell_slot(c.meta, k)) * c.rho[k] * len)));
+    }
+  }
+  // Replay: before the walk that follows event k (0 = emission, else the
+  // k-th interaction), drop that event's peel-offs from A.
+  __device__ __forceinline__ void adjoint_advance(const LaunchParams& P) {
+    if (P.adj.mode != 2) return;
+    const unsigned long long k = (unsigned long long)(pk.nscat + pk.nabsev);
+    const unsigned long long mask = (1ull << kAdjEvBits) - 1ull;
+    while (adj_pos < adj_end && (P.adj.skey[adj_pos] & mask) <= k) adjA -= P.adj.sc[adj_pos++];
+  }
+
   // Queue a peel-off job for the peel kernel; false if the queue is full
   // (the lane then walks the peel-offs itself).
   __device__ bool push_job(const LaunchParams& P, int ctx, int idust2) {
@@ -200,6 +223,8 @@ struct Lane {
       J.pl = pk.sp.pl(ss);
     }
     J.r = pk.ir; J.t = pk.it; J.p = pk.ip;
+    J.pkt = (int32_t)kfetch;
+    J.ev = min(pk.nscat + pk.nabsev, (1 << kAdjEvBits) - 1);
     J.bits = (pk.on_wall ? 1u : 0u) | ((pk.iflag == 1 ? 1u : 0u) << 1) | ((ctx == PC_DIRECT ? 1u : 0u) << 2) |
              ((uint32_t)pk.i_orig << 3) | ((uint32_t)(pk.freq_bin(pk.nub) - 1) << 8);
     P.jobs[j] = J;
@@ -298,9 +323,18 @@ struct Lane {
         case EV_FETCH: {
           if (P.fetch_off) { ev = EV_DONE; return; }
           const unsigned long long k = atomicAdd(P.next, 1ull);
-          if ((int64_t)k >= P.hi - P.lo + 1) { ev = EV_DONE; return; }
-          kfetch = (int64_t)k;
-          iphot = P.lo + (int64_t)k;
+          if (P.adj.mode == 2) {          // replay: the packets that have peel-off records
+            if ((int64_t)k >= P.adj.nlist) { ev = EV_DONE; return; }
+            kfetch = P.adj.list[k];
+            adj_pos = P.adj.start[kfetch];
+            adj_end = P.adj.end[kfetch];
+            adjA = 0.0;
+            for (int64_t r = adj_pos; r < adj_end; ++r) adjA += P.adj.sc[r];
+          } else {
+            if ((int64_t)k >= P.hi - P.lo + 1) { ev = EV_DONE; return; }
+            kfetch = (int64_t)k;
+          }
+          iphot = P.lo + kfetch;
           pk.rng = rng_block(m, P.g1, P.g2, P.block0 + iphot - 1);
           pk.on_wall = false;
           pk.nscat = pk.nabsev = pk.ncross = pk.nstar = pk.ndiffev = 0;
@@ -394,6 +428,7 @@ struct Lane {
           iint = 0;
           nev = 0;
           first = 1;
+          adjoint_advance(P);
           pk.tau = -log(pk.ran());
           start_walk();
           return;
@@ -413,6 +448,8 @@ struct Lane {
           const CellRec c = m.cells[ci];
           const int k = pk.select_dust(c);
           if (k < 0) { status = 3; ev = EV_FINISH; break; }
+          if (P.adj.mode == 2 && adjA != 0.0)   // replay: the interaction density at the segment's end
+            atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1), adjA);
           if (first) { atomicAdd(pk.T.scal + MCRT_S_TOT, 1.0); first = 0; }
           const int slot = cell_slot(c.meta, k);
           const int idust2 = cell_id(c.meta, k);
@@ -457,6 +494,7 @@ struct Lane {
           ev = EV_NEXT_TAU;
           break;
         case EV_NEXT_TAU:              // propagate_5_fuv.f90:177-193
+          adjoint_advance(P);
           pk.tau = -log(pk.ran());
           xpold = pk.xp; ypold = pk.yp; zpold = pk.zp;
           pk.ux = pk.sint * pk.cosp;

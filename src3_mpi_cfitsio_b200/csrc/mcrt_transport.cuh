@@ -1414,7 +1414,9 @@ struct Packet {
     int nth = 0;
     for (int k = 0; k < cell_n(c.meta); ++k) { const int id = cell_id(c.meta, k); if (!(id >= 5 && id <= 8)) ++nth; }
     if (nth == 0) return false;
-    const int32_t k = atomicAdd(T.ndiff + cs, nth) + nth;
+    // adjoint evaluations freeze the surface at its start-of-iteration
+    // temperature (a replay must see the forward pass's heating)
+    const int32_t k = P.adj.mode ? 0 : atomicAdd(T.ndiff + cs, nth) + nth;
     const double t0 = __ldg(m.tdust + cs);
     double T4d = t0 * t0;
     T4d = T4d * T4d;

@@ -59,6 +59,9 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_wave_stats.argtypes = [C.c_void_p, P(C.c_double), P(C.c_int64)]
     lib.mcrt_device_tallies_view.argtypes = [C.c_void_p, P(abi.DeviceTallies)]
     lib.mcrt_refresh_diffusion.argtypes = [C.c_void_p]
+    D = P(C.c_double)
+    lib.mcrt_adjoint.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                 C.c_int32, D, D, D, D]
     lib.mcrt_mark.argtypes = [C.c_void_p, C.c_int32]
     lib.mcrt_elapsed_ms.argtypes = [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]
     lib.mcrt_flush_l2.argtypes = [C.c_void_p]
@@ -72,7 +75,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
-                 "mcrt_device_tallies_view", "mcrt_refresh_diffusion",
+                 "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -198,6 +201,22 @@ class Engine:
         v = abi.DeviceTallies()
         self._check(self.lib.mcrt_device_tallies_view(self.ctx, C.byref(v)))
         return v
+
+    def adjoint(self, np_total: int, lam_psed, lam_img=None, lo: int = 1, hi: int | None = None, *,
+                iteration: int = 1, seeds=(12345678, 87654321), generator: int = 1):
+        """Path-replay adjoint of L = sum lam_psed*ti + sum lam_img*image_m_i:
+        returns (dL/dlog(rho) as [ncell*10] Fortran (nrg,ntg,npg,10), L)."""
+        hi = np_total if hi is None else hi
+        c = self.cfg
+        lp = np.ascontiguousarray(lam_psed, dtype=np.float64)
+        li = None if lam_img is None else np.ascontiguousarray(lam_img, dtype=np.float64)
+        grad = np.zeros(c.nrg * c.ntg * c.npg * 10, np.float64)
+        obj = C.c_double(0.0)
+        D = C.POINTER(C.c_double)
+        self._check(self.lib.mcrt_adjoint(self.ctx, np_total, lo, hi, iteration, seeds[0], seeds[1], generator,
+                                          lp.ctypes.data_as(D), li.ctypes.data_as(D) if li is not None else None,
+                                          grad.ctypes.data_as(D), C.byref(obj)))
+        return grad, obj.value
 
     def refresh_diffusion(self):
         """Diffusion-cell temperatures of the last run from the (reduced) counts."""

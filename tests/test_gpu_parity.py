@@ -477,3 +477,58 @@ def test_clumpy_3d_mixed_wave_loses_no_packets(clumpy_small):
     for k in ("nums", "numt"):
         x, y = a[k].astype(np.float64).sum(), b[k].astype(np.float64).sum()
         assert abs(y - x) <= 0.02 * x + 50, k
+
+
+def _adjoint_weights(m):
+    c = m.config
+    lam = np.zeros((c["nfreq"], c["npeel"], c["nap"], 8))
+    lam[:, :, :, 0] = np.linspace(0.5, 1.5, c["nfreq"])[:, None, None]
+    img = np.linspace(0.2, 1.0, c["npeel"] * c["nxhst"] ** 2 * c["nfreq"])
+    return lam.ravel(order="F"), img
+
+
+@pytest.mark.parametrize("diffusion", [False, True])
+def test_adjoint_matches_oracle(warm_small, oracle_mod, diffusion):
+    """mcrt_adjoint (forward pass through the wave and peel-off kernels,
+    records sorted on the device, replay through the warp schedule) against
+    the oracle's sequential path replay on the same packets: the same
+    objective and dL/dlog(rho) per (cell, component) up to the order of the
+    FP64 sums and the rare packet that parts company."""
+    m = model.with_diffusion(warm_small) if diffusion else warm_small
+    lam, img = _adjoint_weights(m)
+    n = 4000
+    eng = _engine(m)
+    eng.reset_tallies()
+    g_gpu, L_gpu = eng.adjoint(n, lam, img)
+    eng.close()
+    g_or, L_or = oracle_mod.adjoint(abi.Bundle(m), n, lam, img)
+    assert L_gpu > 0
+    assert abs(L_gpu - L_or) <= 1e-3 * abs(L_or)
+    assert np.abs(g_gpu - g_or).sum() <= 2e-2 * np.abs(g_or).sum()
+    ncell = m.config["nrg"] * m.config["ntg"] * m.config["npg"]
+    for comp in range(10):
+        a = g_gpu.reshape((ncell, 10), order="F")[:, comp].sum()
+        b = g_or.reshape((ncell, 10), order="F")[:, comp].sum()
+        assert abs(a - b) <= 2e-2 * np.abs(g_or.reshape((ncell, 10), order="F")[:, comp]).sum() + 1e-12, comp
+
+
+def test_adjoint_mixed_precision_and_repeatability(warm_small):
+    m = model.with_diffusion(warm_small)
+    lam, img = _adjoint_weights(m)
+    n = 20000
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng = _engine(m, precision=prec)
+        g1, L1 = eng.adjoint(n, lam, img)
+        g2, L2 = eng.adjoint(n, lam, img)
+        eng.close()
+        # the same paths; only the order of the FP64 atomic sums differs
+        assert abs(L1 - L2) <= 1e-12 * abs(L1) and np.allclose(g1, g2, rtol=1e-9, atol=1e-12 * np.abs(g1).max())
+        out[prec] = (g1, L1)
+    (ga, La), (gb, Lb) = out["fp64"], out["mixed"]
+    assert abs(Lb - La) <= 0.01 * La
+    ncell = m.config["nrg"] * m.config["ntg"] * m.config["npg"]
+    for comp in (2, 3):
+        a = ga.reshape((ncell, 10), order="F")[:, comp].sum()
+        b = gb.reshape((ncell, 10), order="F")[:, comp].sum()
+        assert abs(b - a) <= 0.1 * abs(a), comp
