@@ -309,6 +309,23 @@ def run_ours(args, rank, world):
                                     "note": "same packets and random streams; differences are Monte Carlo "
                                             "divergence of histories after FP32 scattering"},
         }
+    # ---- gradient time: the path-replay adjoint of the peeled SED and the
+    # 3.6/24/70 um images on the same model (mcrt_adjoint), mixed build
+    if rank == 0 and args.grad_packets > 0:
+        from src3_mpi_cfitsio_b200 import adjoint as madj
+        lam, img = madj.sed_image_weights(m)
+        eng.adjoint(min(args.grad_packets, 100000), lam, img, iteration=it + 2)   # warm
+        eng.synchronize()
+        t0g = time.perf_counter()
+        g, Lg = eng.adjoint(args.grad_packets, lam, img, iteration=it + 2)
+        grad_wall = time.perf_counter() - t0g
+        pgrad = madj.parameter_gradient(m, g)
+        extra["gradient"] = {"packets": args.grad_packets, "seconds": grad_wall,
+                             "device_seconds": eng.kernel_ms() / 1e3, "objective": Lg,
+                             "outputs": "peeled SED (all bins) + 3.6/24/70 um images, Stokes I",
+                             "wrt": "log rho per cell and component (10 x nr x ntheta); disk parameters",
+                             "disk_parameters": pgrad, "precision": args.precision}
+        eng.reset_tallies()
     out = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=ms_steps / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
@@ -398,6 +415,8 @@ def main():
     ap.add_argument("--peel-packets", type=int, default=10_000_000)
     ap.add_argument("--ipeel", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--grad-packets", type=int, default=10_000_000,
+                    help="packets of the adjoint-gradient timing (0: skip)")
     ap.add_argument("--plain-packets", type=int, default=5_000_000,
                     help="packets of the plain FP64 per-thread comparison run")
     ap.add_argument("--no-cpu-baseline", action="store_true")

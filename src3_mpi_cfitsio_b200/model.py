@@ -254,19 +254,7 @@ class Model:
         rmincgs = w.rstar * RSOL
 
         # disk (setup.f90:96-99 R100 scale height, setup_wave.f90:60-88)
-        rmaxd = w.rmaxd_au * autors
-        z1 = w.h100_au * autors / (100.0 * autors) ** w.b_exp
-        p = w.b_exp - w.a_exp
-        const = R2P ** 1.5 * rmincgs ** 2 * (rmincgs * z1)
-        rmind = rddust
-        rho0 = w.massd * MSOL / const / (
-            1.0 / (p + 2.0) * (rmaxd ** (p + 2.0) - rmind ** (p + 2.0))
-            - 1.0 / (p + 1.5) * (rmaxd ** (p + 1.5) - rmind ** (p + 1.5)))
-        h = z1 * wcyl ** w.b_exp
-        with np.errstate(invalid="ignore", divide="ignore"):
-            rho_d = rho0 * (1.0 - np.sqrt(1.0 / wcyl)) * wcyl ** (-w.a_exp) * np.exp(-0.5 * (zp / h) ** 2)
-        rho_d = np.where((rad > rddust) & (wcyl <= rmaxd) & (wcyl > 1.0), rho_d, 0.0)
-        rho_d = np.where(rho_d > 1e-300, rho_d, 0.0)
+        rho_d = self._disk_rho(w, autors, rddust, rarr, thetarr)
 
         # Ulrich envelope (envset.f90:157-160, densenv.f90:37-43)
         rc = w.rc_au * autors
@@ -314,6 +302,31 @@ class Model:
         vcell[:nr, :nt, :npc] = (-(dr3[:, None] * dcost[None, :]) * (R2P / npc) / 3.0
                                  * rmincgs ** 3)[:, :, None]
         return rave, dens, vcell
+
+    @staticmethod
+    def _disk_rho(w: Workload, autors, rddust, rarr, thetarr):
+        """Whitney flared disk on the cell centres (nrg-1, ntg-1):
+        rho0 (1-sqrt(R*/w)) w^-a exp(-z^2/2h^2), h = z1 w^b, rho0 from Mdisk."""
+        rave = 0.5 * (rarr[:-1] + rarr[1:])
+        thave = 0.5 * (thetarr[:-1] + thetarr[1:])
+        rad = rave[:, None]
+        th = thave[None, :]
+        wcyl = rad * np.sin(th)
+        zp = rad * np.abs(np.cos(th))
+        rmincgs = w.rstar * RSOL
+        rmaxd = w.rmaxd_au * autors
+        z1 = w.h100_au * autors / (100.0 * autors) ** w.b_exp
+        p = w.b_exp - w.a_exp
+        const = R2P ** 1.5 * rmincgs ** 2 * (rmincgs * z1)
+        rmind = rddust
+        rho0 = w.massd * MSOL / const / (
+            1.0 / (p + 2.0) * (rmaxd ** (p + 2.0) - rmind ** (p + 2.0))
+            - 1.0 / (p + 1.5) * (rmaxd ** (p + 1.5) - rmind ** (p + 1.5)))
+        h = z1 * wcyl ** w.b_exp
+        with np.errstate(invalid="ignore", divide="ignore"):
+            rho_d = rho0 * (1.0 - np.sqrt(1.0 / wcyl)) * wcyl ** (-w.a_exp) * np.exp(-0.5 * (zp / h) ** 2)
+        rho_d = np.where((rad > rddust) & (wcyl <= rmaxd) & (wcyl > 1.0), rho_d, 0.0)
+        return np.where(rho_d > 1e-300, rho_d, 0.0)
 
     def _clump_field(self, nr, nt, npc):
         """Seeded hierarchical clump multiplier with mean 1 (fractal_sph.f90 style)."""
@@ -707,3 +720,58 @@ def with_mueller(m: Model, narr: int = 720, nang: int = 181, s34_frac: float = 0
     m.tables["mueller"] = np.ascontiguousarray(out).ravel()
     m.tables["narr"] = int(narr)
     return m
+
+
+# ----------------------------------------------------------- disk parameters
+DISK_PARAMS = ("massd", "b_exp", "h100_au")
+
+
+def disk_log_derivatives(m: Model, rel_step: float = 1e-4) -> dict:
+    """d log(rho_disk) / d(param) on the model's grid, per disk cell
+    (nrg-1, ntg-1): for Mdisk and h(100 AU) with respect to the log of the
+    parameter, for the flaring index b with respect to b itself.  Central
+    differences of the disk law at fixed walls (the law is smooth; the step
+    is far below the Monte Carlo noise of any gradient)."""
+    import copy
+    w = m.w
+    autors = 214.94 / w.rstar
+    rddust = w.rddust_au * autors
+    rarr = m.grid["rarr"]
+    thetarr = m.grid["thetarr"]
+    base = Model._disk_rho(w, autors, rddust, rarr, thetarr)
+    out = {}
+    for name in DISK_PARAMS:
+        v = getattr(w, name)
+        h = rel_step * (abs(v) if name != "b_exp" else 1.0)
+        wp, wm = copy.copy(w), copy.copy(w)
+        setattr(wp, name, v + h)
+        setattr(wm, name, v - h)
+        rp = Model._disk_rho(wp, autors, rddust, rarr, thetarr)
+        rm = Model._disk_rho(wm, autors, rddust, rarr, thetarr)
+        ok = (base > 0) & (rp > 0) & (rm > 0)
+        d = np.zeros_like(base)
+        d[ok] = (np.log(rp[ok]) - np.log(rm[ok])) / (2.0 * h)
+        if name != "b_exp":
+            d = d * v                     # d/d log(param)
+        out[name] = d
+    return out
+
+
+def with_disk_params(m: Model, **params) -> Model:
+    """The model with its disk component recomputed for new disk parameters
+    on the same grid, with the same cells owning the disk and the same
+    diffusion flags (the fixed structure an adjoint gradient is taken at)."""
+    import copy
+    mm = copy.deepcopy(m)
+    w = copy.copy(m.w)
+    for k, v in params.items():
+        setattr(w, k, v)
+    autors = 214.94 / w.rstar
+    rho = Model._disk_rho(w, autors, w.rddust_au * autors, m.grid["rarr"], m.grid["thetarr"])
+    dens = mm.grid["densarr"].reshape((w.nrg, w.ntg, w.npg, NDG2), order="F").copy()
+    nr, nt, npc = w.nrg - 1, w.ntg - 1, max(w.npg - 1, 1)
+    owned = dens[:nr, :nt, :npc, 1] > 0
+    dens[:nr, :nt, :npc, 1] = np.where(owned, rho[:, :, None], 0.0)
+    mm.grid["densarr"] = np.asfortranarray(dens).ravel(order="F")
+    mm.w = w
+    return mm

@@ -163,3 +163,26 @@ def test_oracle_adjoint_matches_central_differences(oracle_mod):
         assert abs(adj - fd) <= 0.1 * abs(fd), (comp + 1, adj, fd)
         checked += 1
     assert checked == 2 and L > 0
+
+
+def test_disk_law_log_derivatives():
+    """Chain-rule factors of the disk parameters: rho_disk is proportional
+    to Mdisk; d log rho/d log h100 = z^2/h^2 - 1 (the scale height and the
+    normalisation); with_disk_params changes the disk cells only."""
+    m = model.small_2d()
+    w = m.w
+    d = model.disk_log_derivatives(m)
+    on = d["massd"] != 0
+    assert on.sum() > 10 and np.allclose(d["massd"][on], 1.0, atol=1e-6)
+    autors = 214.94 / w.rstar
+    r = m.grid["rarr"]; t = m.grid["thetarr"]
+    rad = (0.5 * (r[:-1] + r[1:]))[:, None]
+    th = (0.5 * (t[:-1] + t[1:]))[None, :]
+    wcyl, z = rad * np.sin(th), rad * np.abs(np.cos(th))
+    h = w.h100_au * autors / (100.0 * autors) ** w.b_exp * wcyl ** w.b_exp
+    expect = (z / h) ** 2 - 1.0
+    assert np.allclose(d["h100_au"][on], expect[on], rtol=1e-5, atol=1e-6)
+    mm = model.with_disk_params(m, massd=2.0 * w.massd)
+    a = m.grid["densarr"].reshape(-1, 10, order="F")
+    b = mm.grid["densarr"].reshape(-1, 10, order="F")
+    assert np.allclose(b[:, 1], 2.0 * a[:, 1], rtol=1e-12) and np.array_equal(b[:, 2:], a[:, 2:])
