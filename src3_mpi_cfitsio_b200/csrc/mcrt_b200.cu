@@ -46,6 +46,14 @@ cudaError_t launch_wave_tail_fp64(const LaunchParams& p, const WaveArgs& w, int 
 cudaError_t launch_wave_tail_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s);
 int wave_tail_fp64_blocks_per_sm();
 int wave_tail_mixed_blocks_per_sm();
+cudaError_t launch_batch_fp64(const LaunchParams* params, const BatchItem* items, int64_t nitems,
+                              unsigned long long* item_next, unsigned long long* chunk_next, int32_t event_batch,
+                              int grid, cudaStream_t s);
+cudaError_t launch_batch_mixed(const LaunchParams* params, const BatchItem* items, int64_t nitems,
+                               unsigned long long* item_next, unsigned long long* chunk_next, int32_t event_batch,
+                               int grid, cudaStream_t s);
+int batch_fp64_blocks_per_sm();
+int batch_mixed_blocks_per_sm();
 }  // namespace mcrt
 
 using namespace mcrt;
@@ -88,6 +96,7 @@ struct mcrt_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   int64_t ncell = 0, nsed = 0, npsed = 0, nimg = 0;
+  int64_t uploads = 0;                // grid and table uploads so far (batch graphs hold their pointers)
   DevModel dm{};
   DevTallies dt{};
   std::vector<void*> allocs;         // device buffers owned by the context
@@ -473,6 +482,7 @@ int mcrt_set_wave_pool(mcrt_ctx* ctx, int64_t slots, int64_t peel_jobs, int64_t 
 
 int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   if (!ctx || !g) return MCRT_ERR_ARG;
+  ++ctx->uploads;
   CK(cudaSetDevice(ctx->device));
   const mcrt_config& c = ctx->cfg;
   const int nrg = c.nrg, ntg = c.ntg, npg = c.npg;
@@ -599,6 +609,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
 
 int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   if (!ctx || !t) return MCRT_ERR_ARG;
+  ++ctx->uploads;
   CK(cudaSetDevice(ctx->device));
   const mcrt_config& c = ctx->cfg;
   if (!t->nlambda || !t->nudust || !t->kappad || !t->adust || !t->gdust || !t->pldust || !t->kappav || !t->kapint ||
@@ -744,8 +755,11 @@ static int adjoint_grow(mcrt_ctx* ctx, int64_t need) {
 // schedule, no tail launch so that every peel-off goes through the peel-off
 // kernel, records in ctx->adj); 2: the adjoint's replay (warp schedule over
 // ctx->adj's packet list, no peel-offs).
-static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
-                              int32_t seed1, int32_t seed2, int32_t generator, int adj_mode) {
+// Validated launch parameters of packets lo..hi of an np-packet iteration:
+// the packet split (newdisktherm_5_fuv.f90:158-191), generator seeds
+// (set_all_seeds), the model and tally views of the context.
+static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel, int32_t seed1,
+                       int32_t seed2, int32_t generator, LaunchParams& P) {
   if (!ctx) return MCRT_ERR_ARG;
   if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
   if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range %lld..%lld of %lld", (long long)lo, (long long)hi, (long long)np);
@@ -771,7 +785,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;
   for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }
-  LaunchParams P{};
+  P = LaunchParams{};
   P.m = ctx->dm;
   DevModel& m = P.m;
   m.nrg = c.nrg; m.ntg = c.ntg; m.npg = c.npg; m.nopac = c.nopac; m.nlammax = c.nlammax; m.nT = c.nT; m.nnu = c.nnu;
@@ -799,8 +813,19 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
   P.log = ctx->d_log;
   P.nlog = ctx->nlog;
   P.err = ctx->d_err;
-  const int64_t npk = hi - lo + 1;
   P.event_batch = ctx->event_batch;
+  return MCRT_OK;
+}
+
+static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
+                              int32_t seed1, int32_t seed2, int32_t generator, int adj_mode) {
+  LaunchParams P{};
+  {
+    const int rc0 = make_params(ctx, np, lo, hi, iter, ipeel, seed1, seed2, generator, P);
+    if (rc0) return rc0;
+  }
+  const mcrt_config& c = ctx->cfg;
+  const int64_t npk = hi - lo + 1;
   const bool mixed = ctx->precision == MCRT_PREC_MIXED;
   const bool wave = adj_mode == 1 || (adj_mode == 0 && ctx->schedule == MCRT_SCHED_WAVE);
   const bool warp = !wave && (adj_mode == 2 || ctx->schedule == MCRT_SCHED_WARP || mixed);   // the mixed build has no per-thread kernel
@@ -1422,3 +1447,259 @@ int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, 
 }
 
 }  // extern "C"
+
+
+// ---------------------------------------------------------------- batch --
+// Many models in one launch (mcrt_batch.cuh), one CUDA graph per packet-count
+// vector: parameter upload, tally reset, the batch kernel, the diffusion
+// finalisation of every model.
+struct mcrt_batch {
+  std::vector<mcrt_ctx*> ctx;
+  int device = 0;
+  int precision = MCRT_PREC_FP64;
+  int nsm = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  LaunchParams* h_params = nullptr;       // pinned: read by the graph's upload node
+  LaunchParams* d_params = nullptr;
+  BatchItem* d_items = nullptr;
+  int64_t nitems = 0, items_cap = 0;
+  unsigned long long* d_counters = nullptr;   // [1 + items_cap]: item counter, per-item packet counters
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<int64_t> graph_np;
+  std::vector<int64_t> graph_uploads;         // each context's upload count at capture
+  int graph_key[3] = {0, 0, 0};
+  // tuning: blocks per SM (0: occupancy maximum), event batch, items per warp
+  int blocks_per_sm = 0, event_batch = 16, items_per_warp = 4;
+  double last_ms = 0.0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(mcrt_batch* b, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  return code;
+}
+
+#define BK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return bfail(b, MCRT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+int batch_max_blocks(const mcrt_batch* b) {
+  return b->precision == MCRT_PREC_MIXED ? batch_mixed_blocks_per_sm() : batch_fp64_blocks_per_sm();
+}
+
+void batch_drop_graph(mcrt_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_np.clear();
+  b->graph_uploads.clear();
+}
+
+// items: each model's range cut into chunks, about items_per_warp items per
+// warp of the launch over the batch's total packet count
+int batch_build_graph(mcrt_batch* b, const int64_t* np) {
+  const int n = (int)b->ctx.size();
+  const int bps = b->blocks_per_sm > 0 ? std::min(b->blocks_per_sm, batch_max_blocks(b)) : batch_max_blocks(b);
+  const int grid = b->nsm * std::max(bps, 1);
+  int64_t total = 0;
+  for (int i = 0; i < n; ++i) total += np[i];
+  const int64_t nwarps = (int64_t)grid * (kTransportBlock / 32);
+  const int64_t chunk = std::max<int64_t>(256, (total + nwarps * b->items_per_warp - 1) / (nwarps * b->items_per_warp));
+  std::vector<BatchItem> items;
+  for (int i = 0; i < n; ++i)
+    for (int64_t lo = 1; lo <= np[i]; lo += chunk) {
+      BatchItem it{};
+      it.model = i;
+      it.lo = lo;
+      it.hi = std::min(np[i], lo + chunk - 1);
+      items.push_back(it);
+    }
+  batch_drop_graph(b);
+  if ((int64_t)items.size() > b->items_cap) {
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_counters) cudaFree(b->d_counters);
+    b->d_items = nullptr;
+    b->d_counters = nullptr;
+    b->items_cap = 0;
+    BK(cudaMalloc(&b->d_items, items.size() * sizeof(BatchItem)));
+    BK(cudaMalloc(&b->d_counters, (items.size() + 1) * sizeof(unsigned long long)));
+    b->items_cap = (int64_t)items.size();
+  }
+  b->nitems = (int64_t)items.size();
+  BK(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice));
+  BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemcpyAsync(b->d_params, b->h_params, (size_t)n * sizeof(LaunchParams), cudaMemcpyHostToDevice,
+                                  b->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, (size_t)(b->nitems + 1) * sizeof(unsigned long long), b->stream);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaMemsetAsync(b->ctx[i]->d_tally, 0, b->ctx[i]->tally_bytes, b->stream);
+  if (e == cudaSuccess)
+    e = b->precision == MCRT_PREC_MIXED
+            ? launch_batch_mixed(b->d_params, b->d_items, b->nitems, b->d_counters, b->d_counters + 1, b->event_batch,
+                                 grid, b->stream)
+            : launch_batch_fp64(b->d_params, b->d_items, b->nitems, b->d_counters, b->d_counters + 1, b->event_batch,
+                                grid, b->stream);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    mcrt_ctx* c = b->ctx[i];
+    e = launch_diffusion_finalize(b->h_params[i].m, c->dt.ndiff, c->d_tdust0, c->d_tdust, b->h_params[i].nphot_diff,
+                                  b->stream);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return bfail(b, MCRT_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : ee));
+  }
+  b->graph = g;
+  BK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->graph_np.assign(np, np + n);
+  for (int i = 0; i < n; ++i) b->graph_uploads.push_back(b->ctx[i]->uploads);
+  b->graph_key[0] = b->blocks_per_sm;
+  b->graph_key[1] = b->event_batch;
+  b->graph_key[2] = b->items_per_warp;
+  return MCRT_OK;
+}
+
+}  // namespace
+
+int mcrt_batch_create(mcrt_ctx* const* ctxs, int32_t n, mcrt_batch** out) {
+  if (!ctxs || n < 1 || !out) return MCRT_ERR_ARG;
+  *out = nullptr;
+  auto* b = new mcrt_batch();
+  for (int i = 0; i < n; ++i) {
+    mcrt_ctx* c = ctxs[i];
+    if (!c) { delete b; return MCRT_ERR_ARG; }
+    if (!c->have_grid || !c->have_tables) { delete b; return MCRT_ERR_STATE; }
+    if (i > 0 && (c->device != ctxs[0]->device || c->precision != ctxs[0]->precision)) { delete b; return MCRT_ERR_ARG; }
+    b->ctx.push_back(c);
+  }
+  b->device = ctxs[0]->device;
+  b->precision = ctxs[0]->precision;
+  b->nsm = ctxs[0]->nsm;
+  *out = b;
+  BK(cudaSetDevice(b->device));
+  BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BK(cudaEventCreate(&b->e0));
+  BK(cudaEventCreate(&b->e1));
+  BK(cudaHostAlloc((void**)&b->h_params, (size_t)n * sizeof(LaunchParams), cudaHostAllocDefault));
+  BK(cudaMalloc(&b->d_params, (size_t)n * sizeof(LaunchParams)));
+  return MCRT_OK;
+}
+
+int mcrt_batch_run_iteration(mcrt_batch* b, const int64_t* np, int32_t iter, int32_t seed1, int32_t seed2,
+                             int32_t generator) {
+  if (!b || !np) return MCRT_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  const int n = (int)b->ctx.size();
+  for (int i = 0; i < n; ++i) {
+    mcrt_ctx* c = b->ctx[i];
+    if (c->precision != b->precision) return bfail(b, MCRT_ERR_ARG, "model %d changed precision", i);
+    BK(cudaStreamSynchronize(c->stream));      // its uploads are complete
+    LaunchParams P{};
+    const int rc = make_params(c, np[i], 1, np[i], iter, 0, seed1, seed2, generator, P);
+    if (rc) return bfail(b, rc, "model %d: %s", i, c->err.c_str());
+    P.jobs = nullptr;
+    P.event_batch = b->event_batch;
+    b->h_params[i] = P;
+    c->last_m = P.m;
+    c->have_last_run = true;
+  }
+  const bool same = (int)b->graph_np.size() == n && std::equal(b->graph_np.begin(), b->graph_np.end(), np) &&
+                    b->graph_key[0] == b->blocks_per_sm && b->graph_key[1] == b->event_batch &&
+                    b->graph_key[2] == b->items_per_warp;
+  bool fresh = same;                           // no context re-uploaded since the capture
+  for (int i = 0; fresh && i < n; ++i) fresh = b->graph_uploads[i] == b->ctx[i]->uploads;
+  if (!b->exec || !fresh) {
+    const int rc = batch_build_graph(b, np);
+    if (rc) return rc;
+  }
+  BK(cudaEventRecord(b->e0, b->stream));
+  BK(cudaGraphLaunch(b->exec, b->stream));
+  BK(cudaEventRecord(b->e1, b->stream));
+  BK(cudaEventSynchronize(b->e1));
+  float ms = 0.f;
+  BK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+  b->last_ms = ms;
+  for (int i = 0; i < n; ++i) b->ctx[i]->last_ms = ms;
+  return MCRT_OK;
+}
+
+// Coordinate search from (occupancy maximum, 16, 2): items per warp, then
+// the event batch, then one block per SM fewer; each candidate is timed on
+// one iteration of sample_packets per model (the graph launch's events).
+int mcrt_batch_tune(mcrt_batch* b, int64_t sample_packets, int32_t* chosen) {
+  if (!b || sample_packets < 1) return MCRT_ERR_ARG;
+  const int n = (int)b->ctx.size();
+  std::vector<int64_t> np(n, sample_packets);
+  const int maxb = batch_max_blocks(b);
+  int cur[3] = {maxb, 16, 2};
+  double best = 1e300;
+  auto time_it = [&](const int* c, double* ms) -> int {
+    b->blocks_per_sm = c[0];
+    b->event_batch = c[1];
+    b->items_per_warp = c[2];
+    const int rc = mcrt_batch_run_iteration(b, np.data(), 1, 12345678, 87654321, 1);
+    *ms = b->last_ms;
+    return rc;
+  };
+  int rc = time_it(cur, &best);
+  if (rc) return rc;
+  const std::vector<int> cand[3] = {{maxb - 1}, {8, 12, 24}, {1, 4, 8}};
+  for (int dim : {2, 1, 0})
+    for (int v : cand[dim]) {
+      if (v < 1) continue;
+      int c[3] = {cur[0], cur[1], cur[2]};
+      c[dim] = v;
+      double ms = 0.0;
+      if ((rc = time_it(c, &ms))) return rc;
+      if (ms < best) { best = ms; cur[dim] = v; }
+    }
+  b->blocks_per_sm = cur[0];
+  b->event_batch = cur[1];
+  b->items_per_warp = cur[2];
+  batch_drop_graph(b);
+  if (chosen) { chosen[0] = cur[0]; chosen[1] = cur[1]; chosen[2] = cur[2]; }
+  return MCRT_OK;
+}
+
+int mcrt_batch_set_tuning(mcrt_batch* b, int32_t blocks_per_sm, int32_t event_batch, int32_t items_per_warp) {
+  if (!b || blocks_per_sm < 0 || event_batch < 1 || event_batch > 32 || items_per_warp < 1) return MCRT_ERR_ARG;
+  b->blocks_per_sm = blocks_per_sm;
+  b->event_batch = event_batch;
+  b->items_per_warp = items_per_warp;
+  return MCRT_OK;
+}
+
+int mcrt_batch_last_ms(mcrt_batch* b, double* ms) {
+  if (!b || !ms) return MCRT_ERR_ARG;
+  *ms = b->last_ms;
+  return MCRT_OK;
+}
+
+const char* mcrt_batch_last_error(mcrt_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void mcrt_batch_destroy(mcrt_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_counters) cudaFree(b->d_counters);
+  if (b->d_params) cudaFree(b->d_params);
+  if (b->h_params) cudaFreeHost(b->h_params);
+  if (b->e0) cudaEventDestroy(b->e0);
+  if (b->e1) cudaEventDestroy(b->e1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}

@@ -173,6 +173,14 @@ struct AdjointArgs {
 };
 constexpr int kAdjEvBits = 24;    // event index bits of a record key
 
+// One work item of the batch kernel (mcrt_batch.cuh): a chunk of one model's
+// packet range.
+struct BatchItem {
+  int32_t model;
+  int32_t pad_;
+  int64_t lo, hi;             // 1-based packet range of the chunk
+};
+
 struct LaunchParams {
   DevModel m;
   DevTallies t;
@@ -190,6 +198,7 @@ struct LaunchParams {
   int64_t job_cap;
   mcrt_packet_log *log;
   int64_t nlog;
+  int64_t log_off;              // log entry of the launch's k-th packet: k + log_off
   int32_t *err;                 // device error flags
   AdjointArgs adj;
 };

@@ -7,8 +7,24 @@
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"
 #include "mcrt_wave.cuh"
+#include "mcrt_batch.cuh"
 
 namespace mcrt {
+
+static_assert(sizeof(LaunchParams) % 4 == 0, "LaunchParams is copied as 32-bit words");
+
+cudaError_t launch_batch_fp64(const LaunchParams* params, const BatchItem* items, int64_t nitems,
+                              unsigned long long* item_next, unsigned long long* chunk_next, int32_t event_batch,
+                              int grid, cudaStream_t s) {
+  transport_batch<<<grid, kBlock, 0, s>>>(params, items, nitems, item_next, chunk_next, event_batch);
+  return cudaGetLastError();
+}
+
+int batch_fp64_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_batch, kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
 
 cudaError_t launch_wave_init(const WaveArgs& w, cudaStream_t s) {
   const int grid = (int)std::min<int64_t>((w.slots + 255) / 256, 4096);

@@ -18,11 +18,28 @@
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"
 #include "mcrt_wave.cuh"
+#include "mcrt_batch.cuh"
 #undef mcrt
 
 namespace mcrt {
 struct LaunchParams;
 struct WaveArgs;
+struct BatchItem;
+
+cudaError_t launch_batch_mixed(const LaunchParams* params, const BatchItem* items, int64_t nitems,
+                               unsigned long long* item_next, unsigned long long* chunk_next, int32_t event_batch,
+                               int grid, cudaStream_t s) {
+  mcrt_mixed::transport_batch<<<grid, mcrt_mixed::kBlock, 0, s>>>(
+      reinterpret_cast<const mcrt_mixed::LaunchParams*>(params), reinterpret_cast<const mcrt_mixed::BatchItem*>(items),
+      nitems, item_next, chunk_next, event_batch);
+  return cudaGetLastError();
+}
+
+int batch_mixed_blocks_per_sm() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mcrt_mixed::transport_batch, mcrt_mixed::kBlock, 0) != cudaSuccess) return 1;
+  return n > 0 ? n : 1;
+}
 
 cudaError_t launch_wave_event_mixed(const LaunchParams& p, const WaveArgs& w, int grid, cudaStream_t s) {
   const auto& q = reinterpret_cast<const mcrt_mixed::LaunchParams&>(p);

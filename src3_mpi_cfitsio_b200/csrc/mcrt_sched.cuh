@@ -520,8 +520,8 @@ struct Lane {
           if (status == 3) ++c_geo;
           if (status == 1) ++c_kil;
           if (status == 0) ++c_exit;
-          if (P.log && kfetch < P.nlog) {
-            mcrt_packet_log& L = P.log[kfetch];
+          if (P.log && kfetch + P.log_off < P.nlog) {
+            mcrt_packet_log& L = P.log[kfetch + P.log_off];
             L.iphot = iphot; L.nscat = pk.nscat; L.nabs = pk.nabsev; L.ncross = pk.ncross; L.nstar = pk.nstar;
             L.status = status; L.ir = 0; L.it = 0; L.ip = 0; L.ndraws = pk.rng.ndraws;
             L.iflag = pk.iflag; L.i_orig = pk.i_orig; L.pad = pk.ndiffev;
@@ -582,9 +582,10 @@ struct Lane {
 #ifndef MCRT_SCHED_MIN_BLOCKS
 #define MCRT_SCHED_MIN_BLOCKS 2
 #endif
-__global__ void __launch_bounds__(kBlock, MCRT_SCHED_MIN_BLOCKS) transport_sched(LaunchParams P) {
-  __shared__ double spec[5 * kMaxSlot * kBlock];
-  Lane L(P.m, P.t, spec);
+// The warp-scheduled loop of one Lane over the packets of P (all 32 lanes
+// of the warp stay in the loop until every lane is out of packets, so the
+// warp votes are well defined), then its counters into P's tallies.
+__device__ __forceinline__ void warp_loop(Lane& L, const LaunchParams& P) {
   const unsigned FULL = 0xffffffffu;
   const int batch = P.event_batch > 0 ? P.event_batch : 12;
   for (;;) {
@@ -605,6 +606,13 @@ __global__ void __launch_bounds__(kBlock, MCRT_SCHED_MIN_BLOCKS) transport_sched
     unsigned long long x = warp_sum(v[i]);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(P.t.cnt + i, x);
   }
+}
+
+// Warp-scheduled persistent kernel.
+__global__ void __launch_bounds__(kBlock, MCRT_SCHED_MIN_BLOCKS) transport_sched(LaunchParams P) {
+  __shared__ double spec[5 * kMaxSlot * kBlock];
+  Lane L(P.m, P.t, spec);
+  warp_loop(L, P);
 }
 
 }  // namespace mcrt

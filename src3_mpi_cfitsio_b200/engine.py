@@ -71,12 +71,22 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.argtypes = [C.c_void_p]
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
+    lib.mcrt_batch_create.argtypes = [P(C.c_void_p), C.c_int32, P(C.c_void_p)]
+    lib.mcrt_batch_run_iteration.argtypes = [C.c_void_p, P(C.c_int64), C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    lib.mcrt_batch_tune.argtypes = [C.c_void_p, C.c_int64, P(C.c_int32)]
+    lib.mcrt_batch_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
+    lib.mcrt_batch_last_ms.argtypes = [C.c_void_p, P(C.c_double)]
+    lib.mcrt_batch_last_error.argtypes = [C.c_void_p]
+    lib.mcrt_batch_last_error.restype = C.c_char_p
+    lib.mcrt_batch_destroy.argtypes = [C.c_void_p]
+    lib.mcrt_batch_destroy.restype = None
     for name in ("mcrt_create", "mcrt_upload_grid", "mcrt_upload_tables", "mcrt_set_precision", "mcrt_set_schedule",
                  "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
-                 "mcrt_flush_l2", "mcrt_synchronize"):
+                 "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
+                 "mcrt_batch_tune", "mcrt_batch_set_tuning", "mcrt_batch_last_ms"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

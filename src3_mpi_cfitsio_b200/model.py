@@ -775,3 +775,27 @@ def with_disk_params(m: Model, **params) -> Model:
     mm.grid["densarr"] = np.asfortranarray(dens).ravel(order="F")
     mm.w = w
     return mm
+
+
+def batch_models(n: int = 64, seed: int = 20240605) -> list:
+    """A seeded parameter sweep of uneven models for the batched launch:
+    nr 50-200, ntheta 49-199 (odd: the equator is a wall), nphi 1-32 cells;
+    Mdisk log-uniform in 1e-4..0.1 Msun, envelope infall rate log-uniform in
+    1e-7..1e-5 Msun/yr, cavity opening angle uniform in 5..40 deg; the dust
+    law sampled on 60-140 wavelengths (uneven wavelength sets).  No image
+    cube (temperature iterations do not peel)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nr = int(rng.integers(50, 201))
+        nt = int(rng.integers(24, 100)) * 2 + 1
+        nph = int(rng.integers(1, 33))
+        w = Workload(nrg=nr + 1, ntg=nt, npg=nph + 1,
+                     massd=float(10.0 ** rng.uniform(-4.0, -1.0)),
+                     rate=float(10.0 ** rng.uniform(-7.0, -5.0)),
+                     thet1_deg=float(rng.uniform(5.0, 40.0)),
+                     nlambda=int(rng.integers(60, 141)))
+        m = Model(w)
+        m.config["output_imcube"] = 0
+        out.append(m)
+    return out
