@@ -366,34 +366,44 @@ void mcrt_destroy(mcrt_ctx *ctx);
 /* ---- batched models (no reference counterpart) ----------------------------
  * The reference runs one model per MPI job (newdisktherm_5_fuv.f90, the
  * `disk` loop at :220-491 inside the Lucy iterations).  A batch runs one Lucy
- * iteration of many models in ONE persistent launch: the packet ranges of all
- * models are cut into chunks, and the blocks of a single kernel take
- * (model, chunk) items from a queue.  Each model keeps its own context
+ * iteration of many models in ONE graph launch.  Each model keeps its own context
  * (grid, tables, tallies, temperature); the packets of model i use block
  * (iter-1)*np[i] + iphot-1 of the generator's stream, so every model's
  * histories are those of mcrt_run_iteration(ctx[i], np[i], 1, np[i], iter, 0,
  * ...) and its tallies equal that call's up to FP64 summation order.  One
  * iteration is one CUDA graph launch: parameter upload, tally reset, the
- * batch kernel, each model's diffusion-heating finalisation (the graph is
- * re-captured when np[], the tuning or a context's grid or tables change).  No peel-offs (ipeel=0: the
+ * packet loop, each model's diffusion-heating finalisation (the graph is
+ * re-captured when np[], the seeds, the tuning or a context's grid, tables
+ * or packet log change).  Two schedules: MCRT_BATCH_PERSISTENT runs every
+ * model's packets in one persistent launch (blocks take (model, chunk)
+ * items); MCRT_BATCH_WAVE runs each model's wavefront loop (the default
+ * single-model schedule) on the device as a CUDA-graph WHILE node, the
+ * models as parallel branches of the one graph.  No peel-offs (ipeel=0: the
  * temperature iterations; run the final peel-off iteration per context).
  * All contexts must be on one device with one precision and have their grid
  * and tables uploaded; they must outlive the batch. */
 typedef struct mcrt_batch mcrt_batch;
+#define MCRT_BATCH_PERSISTENT 0  /* one persistent launch over (model, packet chunk) work items */
+#define MCRT_BATCH_WAVE       1  /* every model's wavefront loop on the device (graph WHILE node), models in parallel branches */
 int mcrt_batch_create(mcrt_ctx *const *ctxs, int32_t n, mcrt_batch **out);
 /* Resets each model's tallies, then one iteration of every model (np[i]
  * packets, n entries).  Blocks until done; the device time is read with
  * mcrt_batch_last_ms.  Follow with mcrt_update_temperature per context. */
 int mcrt_batch_run_iteration(mcrt_batch *b, const int64_t *np, int32_t iter, int32_t seed1, int32_t seed2,
                              int32_t generator);
-/* Autotuner: a coordinate search over the work items per warp (chunk size
- * of the item queue), the warp schedule's event batch and the blocks per SM,
- * each candidate timed on one iteration of `sample_packets` per model; keeps
- * the fastest, chosen[3] (may be NULL) = (blocks per SM, event batch, items
- * per warp).  The tuning runs overwrite the models' tallies. */
+/* Autotuner: times one iteration of `sample_packets` per model for both
+ * schedules at their defaults, keeps the faster and searches its knobs --
+ * persistent: work items per warp (chunk size of the item queue), the warp
+ * schedule's event batch, blocks per SM; wavefront: in-flight packet slots
+ * per model (the packet queue size).  chosen[5] (may be NULL) = (schedule,
+ * blocks per SM, event batch, items per warp, wave slots).  The tuning runs
+ * overwrite the models' tallies. */
 int mcrt_batch_tune(mcrt_batch *b, int64_t sample_packets, int32_t *chosen);
-/* Set the tuning by hand: blocks_per_sm 0 = occupancy maximum, event_batch
- * 1..32, items_per_warp >= 1. */
+/* Schedule of the batch (MCRT_BATCH_PERSISTENT or MCRT_BATCH_WAVE) and, for
+ * the wavefront, the in-flight packet slots per model (64..2^30). */
+int mcrt_batch_set_schedule(mcrt_batch *b, int32_t mode, int64_t wave_slots);
+/* Persistent schedule by hand: blocks_per_sm 0 = occupancy maximum,
+ * event_batch 1..32, items_per_warp >= 1. */
 int mcrt_batch_set_tuning(mcrt_batch *b, int32_t blocks_per_sm, int32_t event_batch, int32_t items_per_warp);
 int mcrt_batch_last_ms(mcrt_batch *b, double *ms);
 const char *mcrt_batch_last_error(mcrt_batch *b);

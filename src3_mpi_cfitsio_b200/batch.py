@@ -3,11 +3,13 @@
 The reference runs one model per MPI job: ``newtts.f90`` calls ``disk`` once
 per Lucy iteration for its single grid.  A parameter sweep of that code is
 many such jobs.  Here the temperature iterations of a whole sweep share the
-GPU: ``Batch.run_iteration`` runs one iteration of every model in one
-persistent launch (work items = (model, packet chunk)), captured in a CUDA
-graph together with the tally resets and the diffusion-heating
-finalisation; ``Batch.tune`` is the autotuner over blocks per SM, the warp
-schedule's event batch and the work items per warp.  Each model keeps its
+GPU: ``Batch.run_iteration`` runs one iteration of every model as one CUDA
+graph launch (tally resets, packet loops, diffusion-heating finalisation)
+with one of two schedules: "persistent" (one launch whose warps take
+(model, packet chunk) items) or "wave" (each model's wavefront loop driven
+on the device by a graph WHILE node, the models in parallel branches).
+``Batch.tune`` is the autotuner: the schedule, then its knobs (items per
+warp, event batch, blocks per SM; or in-flight packet slots per model).  Each model keeps its
 own ``Engine`` (context), so the temperature update and the final peel-off
 iteration stay per model.
 
@@ -21,6 +23,8 @@ import ctypes as C
 import numpy as np
 
 from .engine import Engine, MCRTError, load_library
+
+SCHEDULES = {"persistent": 0, "wave": 1}
 
 
 class Batch:
@@ -56,16 +60,23 @@ class Batch:
         except Exception:
             pass
 
-    def set_tuning(self, blocks_per_sm: int = 0, event_batch: int = 16, items_per_warp: int = 4):
-        self._check(self.lib.mcrt_batch_set_tuning(self.h, blocks_per_sm, event_batch, items_per_warp))
-        self.tuning = (blocks_per_sm, event_batch, items_per_warp)
+    def set_schedule(self, schedule: str = "persistent", wave_slots: int = 1 << 18):
+        """"persistent": one launch over (model, chunk) items; "wave": every
+        model's wavefront loop on the device, models in parallel graph
+        branches, `wave_slots` in-flight packets per model."""
+        self._check(self.lib.mcrt_batch_set_schedule(self.h, SCHEDULES[schedule], int(wave_slots)))
 
-    def tune(self, sample_packets: int) -> tuple:
+    def set_tuning(self, blocks_per_sm: int = 0, event_batch: int = 16, items_per_warp: int = 4):
+        """Knobs of the persistent schedule."""
+        self._check(self.lib.mcrt_batch_set_tuning(self.h, blocks_per_sm, event_batch, items_per_warp))
+
+    def tune(self, sample_packets: int) -> dict:
         """Autotune on `sample_packets` per model (overwrites the tallies);
-        returns (blocks_per_sm, event_batch, items_per_warp)."""
-        ch = (C.c_int32 * 3)()
+        returns the chosen schedule and knobs."""
+        ch = (C.c_int32 * 5)()
         self._check(self.lib.mcrt_batch_tune(self.h, int(sample_packets), ch))
-        self.tuning = tuple(int(x) for x in ch)
+        self.tuning = dict(schedule={v: k for k, v in SCHEDULES.items()}[int(ch[0])], blocks_per_sm=int(ch[1]),
+                           event_batch=int(ch[2]), items_per_warp=int(ch[3]), wave_slots=int(ch[4]))
         return self.tuning
 
     def run_iteration(self, np_per_model, iteration: int = 1, seeds=(12345678, 87654321), generator: int = 1):

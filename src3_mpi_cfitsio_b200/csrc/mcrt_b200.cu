@@ -96,7 +96,7 @@ struct mcrt_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   int64_t ncell = 0, nsed = 0, npsed = 0, nimg = 0;
-  int64_t uploads = 0;                // grid and table uploads so far (batch graphs hold their pointers)
+  int64_t uploads = 0;                // grid, table and log-buffer changes so far (batch graphs hold their pointers)
   DevModel dm{};
   DevTallies dt{};
   std::vector<void*> allocs;         // device buffers owned by the context
@@ -370,6 +370,39 @@ __global__ void add_tally(int kind, const void* src, void* dst, int64_t n) {
 __global__ void add_counters(unsigned long long* cnt, unsigned long long waves, unsigned long long launches) {
   cnt[MCRT_C_WAVES] += waves;
   cnt[MCRT_C_LAUNCHES] += launches;
+}
+
+// Device-driven wavefront loop (a CUDA-graph WHILE node whose body is event
+// launch, wave_loop_mid, walk launch, wave_loop_cond): the decisions the
+// host loop of run_iteration_impl takes after each walk launch.
+__global__ void wave_loop_mid(WaveCtl* c) {
+  c->n_front = 0;
+  c->n_back = 0;
+  c->walk_fetch = 0;
+}
+
+// pad1 counts waves, pad2 flags a loop stopped by the wave limit.  Ends the
+// loop when no packet is live, or hands the rest to the tail launch once
+// every packet has started and at most tail_live are live.
+__global__ void wave_loop_cond(WaveCtl* c, const unsigned long long* next, int64_t npk, unsigned long long tail_live,
+                               unsigned long long max_waves, cudaGraphConditionalHandle h) {
+  const unsigned long long live = c->n_front + c->n_back;
+  const unsigned long long waves = c->pad1 + 1;
+  c->pad1 = waves;
+  c->n_walk = 0;                      // for the next event launch or the tail
+  c->ev_fetch = 0;
+  bool go = live > 0;
+  if (go && tail_live > 0 && (int64_t)next[0] >= npk && live <= tail_live) go = false;
+  if (go && waves >= max_waves) {
+    go = false;
+    c->pad2 = 1;
+  }
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+__global__ void wave_loop_finish(unsigned long long* cnt, const WaveCtl* c) {
+  cnt[MCRT_C_WAVES] += c->pad1;
+  cnt[MCRT_C_LAUNCHES] += 4 * c->pad1 + 4;    // + wave_init, tail, diffusion_finalize, this
 }
 
 __global__ void to_float(const double* src, float* dst, int64_t n) {
@@ -708,6 +741,7 @@ int mcrt_reset_tallies(mcrt_ctx* ctx) {
 
 int mcrt_enable_packet_log(mcrt_ctx* ctx, int64_t max_packets) {
   if (!ctx || max_packets < 0) return MCRT_ERR_ARG;
+  ++ctx->uploads;                     // the log buffer is replaced
   CK(cudaSetDevice(ctx->device));
   if (ctx->d_log) { dfree(ctx, ctx->d_log); ctx->d_log = nullptr; }
   ctx->nlog = max_packets;
@@ -1469,9 +1503,29 @@ struct mcrt_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<int64_t> graph_np;
   std::vector<int64_t> graph_uploads;         // each context's upload count at capture
-  int graph_key[3] = {0, 0, 0};
-  // tuning: blocks per SM (0: occupancy maximum), event batch, items per warp
+  int graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // schedule: MCRT_BATCH_PERSISTENT (one launch over (model, chunk) items) or
+  // MCRT_BATCH_WAVE (each model's wavefront loop as a WHILE node, the models
+  // as parallel branches of one graph)
+  int mode = MCRT_BATCH_PERSISTENT;
+  // persistent tuning: blocks per SM (0: occupancy maximum), event batch, items per warp
   int blocks_per_sm = 0, event_batch = 16, items_per_warp = 4;
+  // wavefront tuning: in-flight packet slots per model
+  int64_t wave_slots = (int64_t)1 << 18;
+  struct Wave {
+    WaveRec* recs = nullptr;
+    int32_t* walkq = nullptr;
+    int32_t* evq = nullptr;
+    WaveCtl* ctl = nullptr;
+    unsigned long long* next = nullptr;     // [4] packet counter (and unused job counters)
+    int64_t cap = 0;
+  };
+  std::vector<Wave> wave;
+  std::vector<cudaStream_t> branch;           // capture streams of the parallel branches
+  cudaStream_t body_stream = nullptr;
+  cudaEvent_t e_fork = nullptr, e_join = nullptr;
+  int64_t* h_block0 = nullptr;                // pinned [n]: (iter-1)*np[i], uploaded by the graph
+  int64_t* d_block0 = nullptr;
   double last_ms = 0.0;
   std::string err;
 };
@@ -1505,6 +1559,124 @@ void batch_drop_graph(mcrt_batch* b) {
   b->graph = nullptr;
   b->graph_np.clear();
   b->graph_uploads.clear();
+}
+
+int batch_wave_buffers(mcrt_batch* b, int i, int64_t slots) {
+  mcrt_batch::Wave& w = b->wave[i];
+  if (w.cap >= slots && w.ctl) return MCRT_OK;
+  for (void* q : {(void*)w.recs, (void*)w.walkq, (void*)w.evq, (void*)w.ctl, (void*)w.next})
+    if (q) cudaFree(q);
+  w = mcrt_batch::Wave{};
+  BK(cudaMalloc(&w.recs, (size_t)slots * sizeof(WaveRec)));
+  BK(cudaMalloc(&w.walkq, (size_t)slots * sizeof(int32_t)));
+  BK(cudaMalloc(&w.evq, (size_t)slots * sizeof(int32_t)));
+  BK(cudaMalloc(&w.ctl, sizeof(WaveCtl)));
+  BK(cudaMalloc(&w.next, 4 * sizeof(unsigned long long)));
+  w.cap = slots;
+  return MCRT_OK;
+}
+
+// One branch per model, captured on its own stream: tally and loop reset,
+// wave_init, the WHILE node (event, mid, walk, cond), the tail launch (no
+// work when the loop ended with no live packet), diffusion finalisation and
+// the wave counters.  Kernel arguments are fixed at capture; the iteration
+// enters through block0_dev.
+cudaError_t batch_capture_wave_branch(mcrt_batch* b, int i, int64_t npk, cudaStream_t s) {
+  mcrt_ctx* c = b->ctx[i];
+  mcrt_batch::Wave& w = b->wave[i];
+  const bool mixed = b->precision == MCRT_PREC_MIXED;
+  const LaunchParams& P = b->h_params[i];
+  WaveArgs W{};
+  W.recs = w.recs;
+  W.walkq = w.walkq;
+  W.evq = w.evq;
+  W.ctl = w.ctl;
+  W.slots = std::min<int64_t>(b->wave_slots, npk);
+  W.walk_batch = c->wave_batch > 0 ? c->wave_batch : 8;
+  const int egrid = b->nsm * (mixed ? wave_event_mixed_blocks_per_sm() : wave_event_fp64_blocks_per_sm());
+  const int wgrid = b->nsm * (mixed ? wave_walk_mixed_blocks_per_sm() : wave_walk_fp64_blocks_per_sm());
+  const int tgrid = b->nsm * (mixed ? wave_tail_mixed_blocks_per_sm() : wave_tail_fp64_blocks_per_sm());
+  const unsigned long long tail_live = (unsigned long long)tgrid * kTransportBlock * 8ull;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(c->d_tally, 0, c->tally_bytes, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.next, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.ctl, 0, sizeof(WaveCtl), s)) != cudaSuccess) return e;
+  if ((e = launch_wave_init(W, s)) != cudaSuccess) return e;
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn;
+  if ((e = cudaGraphAddNode(&cn, g, deps, nd, &cp)) != cudaSuccess) return e;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t bs = b->body_stream;
+  if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return e;
+  cudaError_t eb = mixed ? launch_wave_event_mixed(P, W, egrid, bs) : launch_wave_event_fp64(P, W, egrid, bs);
+  if (eb == cudaSuccess) {
+    wave_loop_mid<<<1, 1, 0, bs>>>(w.ctl);
+    eb = cudaGetLastError();
+  }
+  if (eb == cudaSuccess) eb = mixed ? launch_wave_walk_mixed(P, W, wgrid, bs) : launch_wave_walk_fp64(P, W, wgrid, bs);
+  if (eb == cudaSuccess) {
+    // the tail launch takes over once every packet has started, so the loop
+    // needs a few thousand waves at most; the limit only bounds a fault
+    wave_loop_cond<<<1, 1, 0, bs>>>(w.ctl, w.next, npk, tail_live, 1000000ull, h);
+    eb = cudaGetLastError();
+  }
+  cudaGraph_t bout = nullptr;
+  e = cudaStreamEndCapture(bs, &bout);
+  if (eb != cudaSuccess) return eb;
+  if (e != cudaSuccess) return e;
+  if ((e = cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess) return e;
+  LaunchParams T = P;
+  T.fetch_off = 1;
+  if ((e = mixed ? launch_wave_tail_mixed(T, W, tgrid, s) : launch_wave_tail_fp64(T, W, tgrid, s)) != cudaSuccess) return e;
+  if ((e = launch_diffusion_finalize(P.m, c->dt.ndiff, c->d_tdust0, c->d_tdust, P.nphot_diff, s)) != cudaSuccess) return e;
+  wave_loop_finish<<<1, 1, 0, s>>>(c->dt.cnt, w.ctl);
+  return cudaGetLastError();
+}
+
+int batch_build_wave(mcrt_batch* b, const int64_t* np) {
+  const int n = (int)b->ctx.size();
+  batch_drop_graph(b);
+  if ((int)b->wave.size() < n) b->wave.resize(n);
+  for (int i = 0; i < n; ++i) {
+    const int rc = batch_wave_buffers(b, i, std::min<int64_t>(b->wave_slots, np[i]));
+    if (rc) return rc;
+  }
+  while ((int)b->branch.size() < n) {
+    cudaStream_t s;
+    BK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    b->branch.push_back(s);
+  }
+  BK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemcpyAsync(b->d_block0, b->h_block0, (size_t)n * sizeof(int64_t), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(b->e_fork, b->stream);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) {
+    cudaStream_t s = b->branch[i];
+    e = cudaStreamWaitEvent(s, b->e_fork, 0);
+    if (e == cudaSuccess) e = batch_capture_wave_branch(b, i, np[i], s);
+    if (e == cudaSuccess) e = cudaEventRecord(b->e_join, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->e_join, 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return bfail(b, MCRT_ERR_CUDA, "batch wave graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : ee));
+  }
+  b->graph = g;
+  BK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return MCRT_OK;
 }
 
 // items: each model's range cut into chunks, about items_per_warp items per
@@ -1563,11 +1735,6 @@ int batch_build_graph(mcrt_batch* b, const int64_t* np) {
   }
   b->graph = g;
   BK(cudaGraphInstantiate(&b->exec, b->graph, 0));
-  b->graph_np.assign(np, np + n);
-  for (int i = 0; i < n; ++i) b->graph_uploads.push_back(b->ctx[i]->uploads);
-  b->graph_key[0] = b->blocks_per_sm;
-  b->graph_key[1] = b->event_batch;
-  b->graph_key[2] = b->items_per_warp;
   return MCRT_OK;
 }
 
@@ -1594,6 +1761,11 @@ int mcrt_batch_create(mcrt_ctx* const* ctxs, int32_t n, mcrt_batch** out) {
   BK(cudaEventCreate(&b->e1));
   BK(cudaHostAlloc((void**)&b->h_params, (size_t)n * sizeof(LaunchParams), cudaHostAllocDefault));
   BK(cudaMalloc(&b->d_params, (size_t)n * sizeof(LaunchParams)));
+  BK(cudaHostAlloc((void**)&b->h_block0, (size_t)n * sizeof(int64_t), cudaHostAllocDefault));
+  BK(cudaMalloc(&b->d_block0, (size_t)n * sizeof(int64_t)));
+  BK(cudaStreamCreateWithFlags(&b->body_stream, cudaStreamNonBlocking));
+  BK(cudaEventCreateWithFlags(&b->e_fork, cudaEventDisableTiming));
+  BK(cudaEventCreateWithFlags(&b->e_join, cudaEventDisableTiming));
   return MCRT_OK;
 }
 
@@ -1602,6 +1774,22 @@ int mcrt_batch_run_iteration(mcrt_batch* b, const int64_t* np, int32_t iter, int
   if (!b || !np) return MCRT_ERR_ARG;
   BK(cudaSetDevice(b->device));
   const int n = (int)b->ctx.size();
+  const bool wave = b->mode == MCRT_BATCH_WAVE;
+  for (int i = 0; i < n; ++i)
+    if (np[i] < 1) return bfail(b, MCRT_ERR_ARG, "model %d: np must be >= 1", i);
+  // the graph holds every launch argument but the iteration's block offsets
+  const int key[8] = {b->mode, b->blocks_per_sm, b->event_batch, b->items_per_warp, (int)b->wave_slots,
+                      seed1, seed2, generator};
+  bool fresh = b->exec && (int)b->graph_np.size() == n && std::equal(b->graph_np.begin(), b->graph_np.end(), np) &&
+               std::equal(key, key + 8, b->graph_key);
+  for (int i = 0; fresh && i < n; ++i) fresh = b->graph_uploads[i] == b->ctx[i]->uploads;
+  if (wave && !fresh) {
+    if ((int)b->wave.size() < n) b->wave.resize(n);
+    for (int i = 0; i < n; ++i) {
+      const int rc = batch_wave_buffers(b, i, std::min<int64_t>(b->wave_slots, np[i]));
+      if (rc) return rc;
+    }
+  }
   for (int i = 0; i < n; ++i) {
     mcrt_ctx* c = b->ctx[i];
     if (c->precision != b->precision) return bfail(b, MCRT_ERR_ARG, "model %d changed precision", i);
@@ -1611,18 +1799,21 @@ int mcrt_batch_run_iteration(mcrt_batch* b, const int64_t* np, int32_t iter, int
     if (rc) return bfail(b, rc, "model %d: %s", i, c->err.c_str());
     P.jobs = nullptr;
     P.event_batch = b->event_batch;
+    if (wave) {
+      P.next = b->wave[i].next;
+      P.block0_dev = b->d_block0 + i;
+    }
     b->h_params[i] = P;
+    b->h_block0[i] = P.block0;
     c->last_m = P.m;
     c->have_last_run = true;
   }
-  const bool same = (int)b->graph_np.size() == n && std::equal(b->graph_np.begin(), b->graph_np.end(), np) &&
-                    b->graph_key[0] == b->blocks_per_sm && b->graph_key[1] == b->event_batch &&
-                    b->graph_key[2] == b->items_per_warp;
-  bool fresh = same;                           // no context re-uploaded since the capture
-  for (int i = 0; fresh && i < n; ++i) fresh = b->graph_uploads[i] == b->ctx[i]->uploads;
-  if (!b->exec || !fresh) {
-    const int rc = batch_build_graph(b, np);
+  if (!fresh) {
+    const int rc = wave ? batch_build_wave(b, np) : batch_build_graph(b, np);
     if (rc) return rc;
+    b->graph_np.assign(np, np + n);
+    for (int i = 0; i < n; ++i) b->graph_uploads.push_back(b->ctx[i]->uploads);
+    std::copy(key, key + 8, b->graph_key);
   }
   BK(cudaEventRecord(b->e0, b->stream));
   BK(cudaGraphLaunch(b->exec, b->stream));
@@ -1632,44 +1823,94 @@ int mcrt_batch_run_iteration(mcrt_batch* b, const int64_t* np, int32_t iter, int
   BK(cudaEventElapsedTime(&ms, b->e0, b->e1));
   b->last_ms = ms;
   for (int i = 0; i < n; ++i) b->ctx[i]->last_ms = ms;
+  if (wave) {   // a loop stopped by the wave limit is an error
+    for (int i = 0; i < n; ++i) {
+      unsigned long long flag = 0;
+      BK(cudaMemcpy(&flag, &b->wave[i].ctl->pad2, sizeof flag, cudaMemcpyDeviceToHost));
+      if (flag) return bfail(b, MCRT_ERR_CUDA, "model %d: wavefront loop did not finish", i);
+    }
+  }
   return MCRT_OK;
 }
 
-// Coordinate search from (occupancy maximum, 16, 2): items per warp, then
-// the event batch, then one block per SM fewer; each candidate is timed on
-// one iteration of sample_packets per model (the graph launch's events).
+// Autotuner.  Times one iteration of sample_packets per model for: both
+// schedules at their defaults; then, for the faster one, a coordinate search
+// -- persistent: items per warp, event batch, one block per SM fewer;
+// wavefront: in-flight slots per model (the packet queue size) within a
+// quarter of the free device memory.
 int mcrt_batch_tune(mcrt_batch* b, int64_t sample_packets, int32_t* chosen) {
   if (!b || sample_packets < 1) return MCRT_ERR_ARG;
   const int n = (int)b->ctx.size();
   std::vector<int64_t> np(n, sample_packets);
   const int maxb = batch_max_blocks(b);
-  int cur[3] = {maxb, 16, 2};
-  double best = 1e300;
-  auto time_it = [&](const int* c, double* ms) -> int {
-    b->blocks_per_sm = c[0];
-    b->event_batch = c[1];
-    b->items_per_warp = c[2];
+  struct Cand { int mode, bps, eb, ipw; int64_t slots; };
+  auto apply = [&](const Cand& c) {
+    b->mode = c.mode; b->blocks_per_sm = c.bps; b->event_batch = c.eb; b->items_per_warp = c.ipw; b->wave_slots = c.slots;
+  };
+  auto time_it = [&](const Cand& c, double* ms) -> int {
+    apply(c);
     const int rc = mcrt_batch_run_iteration(b, np.data(), 1, 12345678, 87654321, 1);
     *ms = b->last_ms;
     return rc;
   };
-  int rc = time_it(cur, &best);
+  size_t freeb = 0, totalb = 0;
+  BK(cudaMemGetInfo(&freeb, &totalb));
+  const int64_t per_slot = (int64_t)sizeof(WaveRec) + 8;
+  auto slots_fit = [&](int64_t slots) {
+    int64_t need = 0;
+    for (int i = 0; i < n; ++i) need += std::min<int64_t>(slots, np[i]) * per_slot;
+    return need <= (int64_t)(freeb / 4);
+  };
+  Cand best{MCRT_BATCH_PERSISTENT, maxb, 16, 2, (int64_t)1 << 18};
+  double tbest = 1e300;
+  int rc = time_it(best, &tbest);
   if (rc) return rc;
-  const std::vector<int> cand[3] = {{maxb - 1}, {8, 12, 24}, {1, 4, 8}};
-  for (int dim : {2, 1, 0})
-    for (int v : cand[dim]) {
-      if (v < 1) continue;
-      int c[3] = {cur[0], cur[1], cur[2]};
-      c[dim] = v;
-      double ms = 0.0;
-      if ((rc = time_it(c, &ms))) return rc;
-      if (ms < best) { best = ms; cur[dim] = v; }
+  {
+    Cand w = best;
+    w.mode = MCRT_BATCH_WAVE;
+    w.slots = (int64_t)1 << 16;
+    double t = 0.0;
+    if ((rc = time_it(w, &t))) return rc;
+    if (t < tbest) { tbest = t; best = w; }
+  }
+  if (best.mode == MCRT_BATCH_PERSISTENT) {
+    for (int dim = 0; dim < 3; ++dim) {
+      const std::vector<int> vals = dim == 0 ? std::vector<int>{1, 4, 8} : dim == 1 ? std::vector<int>{8, 12, 24}
+                                                                                     : std::vector<int>{maxb - 1};
+      for (int v : vals) {
+        if (v < 1) continue;
+        Cand c = best;
+        (dim == 0 ? c.ipw : dim == 1 ? c.eb : c.bps) = v;
+        double t = 0.0;
+        if ((rc = time_it(c, &t))) return rc;
+        if (t < tbest) { tbest = t; best = c; }
+      }
     }
-  b->blocks_per_sm = cur[0];
-  b->event_batch = cur[1];
-  b->items_per_warp = cur[2];
+  } else {
+    for (int64_t slots : {(int64_t)1 << 14, (int64_t)1 << 18, (int64_t)1 << 20}) {
+      if (!slots_fit(slots)) continue;
+      Cand c = best;
+      c.slots = slots;
+      double t = 0.0;
+      if ((rc = time_it(c, &t))) return rc;
+      if (t < tbest) { tbest = t; best = c; }
+    }
+  }
+  apply(best);
   batch_drop_graph(b);
-  if (chosen) { chosen[0] = cur[0]; chosen[1] = cur[1]; chosen[2] = cur[2]; }
+  if (chosen) {
+    chosen[0] = best.mode; chosen[1] = best.bps; chosen[2] = best.eb; chosen[3] = best.ipw;
+    chosen[4] = (int32_t)best.slots;
+  }
+  return MCRT_OK;
+}
+
+int mcrt_batch_set_schedule(mcrt_batch* b, int32_t mode, int64_t wave_slots) {
+  if (!b || (mode != MCRT_BATCH_PERSISTENT && mode != MCRT_BATCH_WAVE) || wave_slots < 64 ||
+      wave_slots > ((int64_t)1 << 30))
+    return MCRT_ERR_ARG;
+  b->mode = mode;
+  b->wave_slots = wave_slots;
   return MCRT_OK;
 }
 
@@ -1694,6 +1935,15 @@ void mcrt_batch_destroy(mcrt_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   batch_drop_graph(b);
+  for (auto& w : b->wave)
+    for (void* q : {(void*)w.recs, (void*)w.walkq, (void*)w.evq, (void*)w.ctl, (void*)w.next})
+      if (q) cudaFree(q);
+  for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
+  if (b->body_stream) cudaStreamDestroy(b->body_stream);
+  if (b->e_fork) cudaEventDestroy(b->e_fork);
+  if (b->e_join) cudaEventDestroy(b->e_join);
+  if (b->d_block0) cudaFree(b->d_block0);
+  if (b->h_block0) cudaFreeHost(b->h_block0);
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_counters) cudaFree(b->d_counters);
   if (b->d_params) cudaFree(b->d_params);

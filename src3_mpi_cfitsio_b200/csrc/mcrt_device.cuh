@@ -186,6 +186,7 @@ struct LaunchParams {
   DevTallies t;
   int64_t np, lo, hi;           // iteration size and this launch's packet range
   int64_t block0;               // first random block of the iteration: (iter-1)*np
+  const int64_t *block0_dev;    // non-null: block0 read from device memory (graphs replayed over iterations)
   int64_t ns, npacc, npaccstar; // packet split (newdisktherm_5_fuv.f90:158-191)
   int32_t ipeel, ips;
   int32_t event_batch;          // warp scheduler: lanes that must wait before events run

@@ -335,7 +335,7 @@ struct Lane {
             kfetch = (int64_t)k;
           }
           iphot = P.lo + kfetch;
-          pk.rng = rng_block(m, P.g1, P.g2, P.block0 + iphot - 1);
+          pk.rng = rng_block(m, P.g1, P.g2, (P.block0_dev ? *P.block0_dev : P.block0) + iphot - 1);
           pk.on_wall = false;
           pk.nscat = pk.nabsev = pk.ncross = pk.nstar = pk.ndiffev = 0;
           status = 0;

@@ -74,6 +74,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_batch_create.argtypes = [P(C.c_void_p), C.c_int32, P(C.c_void_p)]
     lib.mcrt_batch_run_iteration.argtypes = [C.c_void_p, P(C.c_int64), C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     lib.mcrt_batch_tune.argtypes = [C.c_void_p, C.c_int64, P(C.c_int32)]
+    lib.mcrt_batch_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
     lib.mcrt_batch_set_tuning.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]
     lib.mcrt_batch_last_ms.argtypes = [C.c_void_p, P(C.c_double)]
     lib.mcrt_batch_last_error.argtypes = [C.c_void_p]
@@ -86,7 +87,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
-                 "mcrt_batch_tune", "mcrt_batch_set_tuning", "mcrt_batch_last_ms"):
+                 "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -66,8 +66,9 @@ def _compare(ref, got):
         assert np.allclose(tda, tdb, rtol=1e-9, atol=0)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_matches_single_runs(uneven, precision):
+@pytest.mark.parametrize("schedule,precision", [("persistent", "fp64"), ("persistent", "mixed"), ("wave", "fp64"),
+                                                ("wave", "mixed")])
+def test_batch_matches_single_runs(uneven, schedule, precision):
     from src3_mpi_cfitsio_b200.batch import Batch
     nps = [3000, 1700, 2200]
     nlog = 1700
@@ -77,6 +78,7 @@ def test_batch_matches_single_runs(uneven, precision):
         e.enable_packet_log(nlog)
     b = Batch(engines)
     b.set_tuning(0, 16, 3)                   # several chunks per model
+    b.set_schedule(schedule, 512)            # several waves per model
     b.run_iteration(nps, iteration=2)
     assert b.kernel_ms() > 0
     got = []
@@ -91,7 +93,8 @@ def test_batch_matches_single_runs(uneven, precision):
         e.close()
 
 
-def test_batch_with_diffusion_cells(uneven):
+@pytest.mark.parametrize("schedule", ["persistent", "wave"])
+def test_batch_with_diffusion_cells(uneven, schedule):
     """A model with diffusion cells in the batch: packets that never reach a
     diffusion cell stay bit-equal to its own run, the diffusion count agrees
     within Monte Carlo error (the surface cells heat in arrival order), and
@@ -106,6 +109,7 @@ def test_batch_with_diffusion_cells(uneven):
     engines[1].enable_packet_log(nlog)
     b = Batch(engines)
     b.set_tuning(0, 16, 2)
+    b.set_schedule(schedule, 4096)
     b.run_iteration(nps, iteration=2)
     got = []
     for e, n, nl in zip(engines, nps, (20000, nlog)):
@@ -130,24 +134,45 @@ def _head(log, n):
     return {k: v[:n] for k, v in log.items()}
 
 
-def test_batch_graph_replay_and_recapture(uneven):
+@pytest.mark.parametrize("schedule", ["persistent", "wave"])
+def test_batch_graph_replay_and_recapture(uneven, schedule):
     """The same packet counts replay the captured graph (tallies are reset
-    inside it); new counts re-capture it; the tuner leaves a valid choice."""
+    inside it, the iteration's random blocks are read from device memory);
+    new counts re-capture it."""
     from src3_mpi_cfitsio_b200.batch import Batch
     engines = [_engine(m, "mixed") for m in uneven]
     b = Batch(engines)
-    chosen = b.tune(600)
-    assert chosen[0] >= 1 and 1 <= chosen[1] <= 32 and chosen[2] >= 1
+    b.set_schedule(schedule, 1000)
     res = []
-    for nps in ([2000, 1000, 1500], [2000, 1000, 1500], [900, 2100, 1200], [2000, 1000, 1500]):
-        b.run_iteration(nps, iteration=1)
+    runs = (([2000, 1000, 1500], 1), ([2000, 1000, 1500], 1), ([900, 2100, 1200], 1), ([2000, 1000, 1500], 2))
+    for nps, it in runs:
+        b.run_iteration(nps, iteration=it)
         res.append([e.download(images=False) for e in engines])
     for k in ("nabs", "dbig"):
         for i in range(3):
             assert np.array_equal(res[0][i][k], res[1][i][k]), k
-            assert np.array_equal(res[0][i][k], res[3][i][k]), k
     for i, n in enumerate([900, 2100, 1200]):
         assert res[2][i].counters()["packets"] == n
+    # the replayed graph at iteration 2 = a single run at iteration 2
+    ref = _single(uneven[1:2], [1000], "mixed", 2, 1)
+    assert np.array_equal(res[3][1]["nabs"], ref[0][1]["nabs"])
+    assert not np.array_equal(res[3][1]["nabs"], res[0][1]["nabs"])
+    b.close()
+    for e in engines:
+        e.close()
+
+
+def test_batch_tuner_choice(uneven):
+    from src3_mpi_cfitsio_b200.batch import Batch
+    engines = [_engine(m, "mixed") for m in uneven]
+    b = Batch(engines)
+    t = b.tune(600)
+    assert t["schedule"] in ("persistent", "wave")
+    assert t["blocks_per_sm"] >= 1 and 1 <= t["event_batch"] <= 32 and t["items_per_warp"] >= 1
+    assert t["wave_slots"] >= 64
+    b.run_iteration([700, 800, 900])
+    for e, n in zip(engines, (700, 800, 900)):
+        assert e.download(images=False).counters()["packets"] == n
     b.close()
     for e in engines:
         e.close()
