@@ -127,6 +127,75 @@ def _errors(a, b):
     return out
 
 
+def bench_clumpy(args, dev):
+    """3-D clumpy model (nr=200, ntheta=199, nphi=64, fractal clumps, tabulated
+    S11-S44 scattering matrices), mixed precision, peeled iteration with
+    201x201 Stokes images at 20 wavelengths and 20 inclinations: device
+    packets/s on a sample of the 1e9-packet run."""
+    from src3_mpi_cfitsio_b200 import model
+    from src3_mpi_cfitsio_b200.engine import Engine
+    m = model.with_diffusion(model.warm(model.with_mueller(model.clumpy_3d())))
+    eng = Engine(m, device=dev, precision="mixed")
+    eng.set_schedule("wave")
+    n = args.clumpy_packets
+    eng.reset_tallies()
+    eng.run(max(n // 10, 1000), iteration=1, ipeel=1)          # warm
+    eng.reset_tallies()
+    eng.flush_l2()
+    eng.run(n, iteration=2, ipeel=1)
+    ms = eng.kernel_ms()
+    c = eng.download(images=False).counters()
+    eng.close()
+    return {"workload": "3-D clumpy (nr=200, ntheta=199, nphi=64; fractal dim 2.6, 50% mass in clumps), tabulated "
+                        "Mueller matrices, 201x201 images x 4 Stokes x 20 wavelengths x 20 inclinations, peel-off on",
+            "packets": n, "precision": "mixed", "packets_per_s": n / (ms / 1e3),
+            "seconds_for_1e9": 1e9 / (n / (ms / 1e3)),
+            "crossings_per_packet": c["crossings"] / n, "peel_crossings_per_packet": c["peel_cross"] / n}
+
+
+def bench_batch(args, dev):
+    """Batched sweep: `--batch-models` seeded uneven models (nr 50-200,
+    ntheta 49-199, nphi 1-32; Mdisk, Mdot, cavity angle and wavelength set
+    drawn from the seed), `--batch-packets` packets each, mixed precision,
+    one Lucy iteration per CUDA-graph launch, schedule and queue sizes from
+    the autotuner.  Compared with the same models run one after another
+    (Engine.run, wavefront schedule) on a sample of 8 models."""
+    from src3_mpi_cfitsio_b200 import model
+    from src3_mpi_cfitsio_b200.batch import Batch
+    from src3_mpi_cfitsio_b200.engine import Engine
+    nmod, n = args.batch_models, args.batch_packets
+    models = [model.with_diffusion(model.warm(m)) for m in model.batch_models(nmod)]
+    engines = [Engine(m, device=dev, precision="mixed") for m in models]
+    b = Batch(engines)
+    tuned = b.tune(args.batch_tune_packets)
+    b.run_iteration([n] * nmod, iteration=1)                 # capture + warm
+    t0 = time.perf_counter()
+    b.run_iteration([n] * nmod, iteration=2)
+    wall = time.perf_counter() - t0
+    ms = b.kernel_ms()
+    pk = sum(e.download(images=False).counters()["packets"] for e in engines)
+    b.close()
+    seq_ms = 0.0
+    sample = engines[:min(8, nmod)]
+    for e in sample:
+        e.set_schedule("wave")
+        e.reset_tallies()
+        e.run(n, iteration=2, ipeel=0)
+        seq_ms += e.kernel_ms()
+    for e in engines:
+        e.close()
+    seq_pps = len(sample) * n / (seq_ms / 1e3)
+    cells = [mm.ncells for mm in models]
+    return {"workload": f"{nmod} uneven models (cells {min(cells)}-{max(cells)}), {n:.0e} packets each, one Lucy "
+                        "iteration per graph launch, diffusion on",
+            "models": nmod, "packets_per_model": n, "packets_total": pk, "precision": "mixed",
+            "packets_per_s": nmod * n / (ms / 1e3), "seconds": ms / 1e3, "wall_seconds": wall,
+            "tuning": tuned,
+            "sequential_wave_packets_per_s": seq_pps,
+            "batch_over_sequential": (nmod * n / (ms / 1e3)) / seq_pps,
+            "sequential_sample": f"first {len(sample)} models, Engine.run each (host-driven wavefront loop)"}
+
+
 def run_ours(args, rank, world):
     import numpy as np
 
@@ -203,21 +272,31 @@ def run_ours(args, rank, world):
     ms_steps = float(allreduce(np.array([ms - flush_ms]), "max")[0])
     value = np_total * args.steps / (ms_steps / 1e3)
 
-    # ---- end-to-end through the public API with host buffers
+    # ---- end-to-end through the public API with host buffers: per step the
+    # driver's grid arrays go up (with the dust temperature of the previous
+    # tfinal, as the Fortran driver holds it), the iteration runs, and the
+    # tallies and the new temperature come back
+    from src3_mpi_cfitsio_b200 import model as mdl
     h2d = sum(m.grid[n].nbytes for n in ("densarr", "findopac", "diffus", "diffdir", "tdust", "vcell"))
     eng.synchronize()
-    t0 = time.perf_counter()
-    eng.mark(4)
-    it = args.warmup + args.steps + 1
-    eng.upload_grid()
-    eng.reset_tallies()
-    eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
-    reduce_ranks(eng)
-    tl = eng.download(images=bool(args.ipeel))
-    td, _, _ = eng.update_temperature(np_total, it)
-    eng.mark(5)
-    eng.synchronize()
-    e2e_ms = max(eng.elapsed_ms(4, 5), (time.perf_counter() - t0) * 1e3)
+    e2e_steps = []
+    for s in range(args.steps):
+        it = args.warmup + args.steps + 1 + s
+        m.grid["tdust"] = mdl.tdust_from_tdave(m, eng.tdave)
+        eng.flush_l2()
+        eng.synchronize()
+        t0 = time.perf_counter()
+        eng.mark(4)
+        eng.upload_grid()
+        eng.reset_tallies()
+        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+        reduce_ranks(eng)
+        tl = eng.download(images=bool(args.ipeel))
+        td, _, _ = eng.update_temperature(np_total, it)
+        eng.mark(5)
+        eng.synchronize()
+        e2e_steps.append(max(eng.elapsed_ms(4, 5), (time.perf_counter() - t0) * 1e3))
+    e2e_ms = sum(e2e_steps) / len(e2e_steps)
     d2h = sum(a.nbytes for a in tl.arrays.values()) + td.nbytes
     e2e_ms = float(allreduce(np.array([e2e_ms]), "max")[0])
     e2e = np_total / (e2e_ms / 1e3)
@@ -326,6 +405,10 @@ def run_ours(args, rank, world):
                              "wrt": "log rho per cell and component (10 x nr x ntheta); disk parameters",
                              "disk_parameters": pgrad, "precision": args.precision}
         eng.reset_tallies()
+    if rank == 0 and args.clumpy_packets > 0:
+        extra["clumpy_3d"] = bench_clumpy(args, dev)
+    if rank == 0 and args.batch_models > 0:
+        extra["batch"] = bench_batch(args, dev)
     out = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=ms_steps / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
@@ -419,6 +502,12 @@ def main():
                     help="packets of the adjoint-gradient timing (0: skip)")
     ap.add_argument("--plain-packets", type=int, default=5_000_000,
                     help="packets of the plain FP64 per-thread comparison run")
+    ap.add_argument("--clumpy-packets", type=int, default=10_000_000,
+                    help="packets of the 3-D clumpy peeled-iteration sample (0: skip)")
+    ap.add_argument("--batch-models", type=int, default=64, help="models of the batched sweep (0: skip)")
+    ap.add_argument("--batch-packets", type=int, default=10_000_000, help="packets per model of the batched sweep")
+    ap.add_argument("--batch-tune-packets", type=int, default=200_000,
+                    help="packets per model of each autotuner trial")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     # 706 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
