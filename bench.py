@@ -506,7 +506,7 @@ def main():
                     help="packets of the 3-D clumpy peeled-iteration sample (0: skip)")
     ap.add_argument("--batch-models", type=int, default=64, help="models of the batched sweep (0: skip)")
     ap.add_argument("--batch-packets", type=int, default=10_000_000, help="packets per model of the batched sweep")
-    ap.add_argument("--batch-tune-packets", type=int, default=200_000,
+    ap.add_argument("--batch-tune-packets", type=int, default=1_000_000,
                     help="packets per model of each autotuner trial")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")

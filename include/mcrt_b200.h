@@ -392,7 +392,10 @@ int mcrt_batch_create(mcrt_ctx *const *ctxs, int32_t n, mcrt_batch **out);
 int mcrt_batch_run_iteration(mcrt_batch *b, const int64_t *np, int32_t iter, int32_t seed1, int32_t seed2,
                              int32_t generator);
 /* Autotuner: times one iteration of `sample_packets` per model for both
- * schedules at their defaults, keeps the faster and searches its knobs --
+ * schedules at their defaults, keeps the faster (the persistent one only if
+ * it wins by 10 %: its advantage on small samples shrinks as packet counts
+ * grow; sample at a tenth of the production count or more) and searches its
+ * knobs --
  * persistent: work items per warp (chunk size of the item queue), the warp
  * schedule's event batch, blocks per SM; wavefront: in-flight packet slots
  * per model (the packet queue size).  chosen[5] (may be NULL) = (schedule,

@@ -1834,7 +1834,8 @@ int mcrt_batch_run_iteration(mcrt_batch* b, const int64_t* np, int32_t iter, int
 }
 
 // Autotuner.  Times one iteration of sample_packets per model for: both
-// schedules at their defaults; then, for the faster one, a coordinate search
+// schedules at their defaults (the persistent one kept only if 10 % faster);
+// then, for the chosen one, a coordinate search
 // -- persistent: items per warp, event batch, one block per SM fewer;
 // wavefront: in-flight slots per model (the packet queue size) within a
 // quarter of the free device memory.
@@ -1861,17 +1862,20 @@ int mcrt_batch_tune(mcrt_batch* b, int64_t sample_packets, int32_t* chosen) {
     for (int i = 0; i < n; ++i) need += std::min<int64_t>(slots, np[i]) * per_slot;
     return need <= (int64_t)(freeb / 4);
   };
-  Cand best{MCRT_BATCH_PERSISTENT, maxb, 16, 2, (int64_t)1 << 18};
+  Cand best{MCRT_BATCH_WAVE, maxb, 16, 2, (int64_t)1 << 16};
   double tbest = 1e300;
   int rc = time_it(best, &tbest);
   if (rc) return rc;
   {
-    Cand w = best;
-    w.mode = MCRT_BATCH_WAVE;
-    w.slots = (int64_t)1 << 16;
+    // The persistent form runs the warp schedule, about half the wavefront's
+    // per-packet rate once waves fill; on a sample it wins only by skipping
+    // the waves' fixed cost, which shrinks as the packet counts grow, so it
+    // must win by 10 % to be kept.
+    Cand p = best;
+    p.mode = MCRT_BATCH_PERSISTENT;
     double t = 0.0;
-    if ((rc = time_it(w, &t))) return rc;
-    if (t < tbest) { tbest = t; best = w; }
+    if ((rc = time_it(p, &t))) return rc;
+    if (t < 0.9 * tbest) { tbest = t; best = p; }
   }
   if (best.mode == MCRT_BATCH_PERSISTENT) {
     for (int dim = 0; dim < 3; ++dim) {
