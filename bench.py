@@ -153,6 +153,33 @@ def bench_clumpy(args, dev):
             "crossings_per_packet": c["crossings"] / n, "peel_crossings_per_packet": c["peel_cross"] / n}
 
 
+def bench_setemiss(args, dev):
+    """The emission tables of dustinit/setemiss (dust_5.f90:486-699) built on
+    the GPU: the model's 8 dust species, and 187 species (the reference's
+    opacity count: its dust plus gas tables) made by perturbing them."""
+    import numpy as np
+
+    from src3_mpi_cfitsio_b200 import model
+    from src3_mpi_cfitsio_b200.engine import setemiss
+    t = model.reference_2d().tables
+    nl = np.asarray(t["nlambda"])
+    nlm = t["nudust"].size // nl.size
+    out = {}
+    for nsp in (nl.size, 187):
+        reps = -(-nsp // nl.size)
+        scale = np.repeat(1.0 + 0.01 * np.arange(reps * nl.size), nlm)[:nsp * nlm]
+        kd = np.tile(t["kappad"], reps)[:nsp * nlm] * scale
+        r = setemiss(np.tile(t["nudust"], reps)[:nsp * nlm], kd, np.tile(t["adust"], reps)[:nsp * nlm],
+                     np.tile(nl, reps)[:nsp], device=dev)
+        t0 = time.perf_counter()
+        r = setemiss(np.tile(t["nudust"], reps)[:nsp * nlm], kd, np.tile(t["adust"], reps)[:nsp * nlm],
+                     np.tile(nl, reps)[:nsp], device=dev)
+        out[f"species_{nsp}"] = {"device_ms": r["device_ms"], "wall_ms": 1e3 * (time.perf_counter() - t0),
+                                 "qsimp_misses": r["qsimp_misses"]}
+    out["grid"] = "nT=500 temperatures x nnu=513 frequency intervals, two qsimp integrals each"
+    return out
+
+
 def bench_batch(args, dev):
     """Batched sweep: `--batch-models` seeded uneven models (nr 50-200,
     ntheta 49-199, nphi 1-32; Mdisk, Mdot, cavity angle and wavelength set
@@ -407,6 +434,8 @@ def run_ours(args, rank, world):
         eng.reset_tallies()
     if rank == 0 and args.clumpy_packets > 0:
         extra["clumpy_3d"] = bench_clumpy(args, dev)
+    if rank == 0:
+        extra["setemiss"] = bench_setemiss(args, dev)
     if rank == 0 and args.batch_models > 0:
         extra["batch"] = bench_batch(args, dev)
     out = dict(
@@ -455,8 +484,14 @@ def cpu_baseline(args, m=None, sample=None):
     t0 = time.perf_counter()
     tal, _ = oracle.run(b, n, ipeel=args.ipeel, threads=cores, iteration=2)
     dt = time.perf_counter() - t0
+    # the emission tables (setemiss) of the model's 8 dust species on the
+    # same host threads, beside the GPU build in the "setemiss" key
+    t0 = time.perf_counter()
+    oracle.setemiss(m.tables["nudust"], m.tables["kappad"], m.tables["adust"], m.tables["nlambda"], threads=cores)
+    st = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} packets of one Lucy iteration of the same model, {cores} host threads"}
+            "sample": f"{n} packets of one Lucy iteration of the same model, {cores} host threads",
+            "setemiss_8_species_ms": 1e3 * st}
 
 
 def run_reference(args, rank, world):

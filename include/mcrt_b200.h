@@ -360,8 +360,26 @@ int mcrt_flush_l2(mcrt_ctx *ctx);
 /* Block until all work queued on the context's stream has finished. */
 int mcrt_synchronize(mcrt_ctx *ctx);
 
-const char *mcrt_last_error(mcrt_ctx *ctx);
+const char *mcrt_last_error(mcrt_ctx *ctx);   /* NULL: the last failed context-free call of this thread */
 void mcrt_destroy(mcrt_ctx *ctx);
+
+/* Emission tables on the GPU: replaces the temperature and frequency grids
+ * of dustinit (dust_5.f90:486-494) and setemiss (dust_5.f90:507-699; the
+ * reference splits the species over its MPI ranks and reduces).  No context
+ * needed; runs on `device`.  In: the dust tables in the mcrt_tables layout
+ * (nudust/kappad/adust Fortran (nlammax, nopac), nu strictly decreasing in
+ * each column; nlambda[nopac]); ndg = the number of dust species (ids above
+ * it are gas opacities, whose Planck mean is smoothed as the reference
+ * does); nT >= 21, nnu <= 3072 (the reference: 500, 513).  Out (host
+ * arrays): lTint[nT], Tint[nT], nuint[nnu], kapint (nT, nnu, nopac),
+ * kappap and kappar (nT, nopac), ready for mcrt_upload_tables;
+ * *qsimp_misses (may be NULL) = interval integrals that hit the 20-level
+ * limit (the reference counts and ignores them); *device_ms (may be NULL) =
+ * kernel time.  Allocates and frees its own device memory. */
+int mcrt_setemiss(int32_t device, int32_t nopac, int32_t ndg, int32_t nlammax, const int32_t *nlambda,
+                  const double *nudust, const double *kappad, const double *adust, int32_t nT, int32_t nnu,
+                  double *lTint, double *Tint, double *nuint, double *kapint, double *kappap, double *kappar,
+                  int64_t *qsimp_misses, double *device_ms);
 
 /* ---- batched models (no reference counterpart) ----------------------------
  * The reference runs one model per MPI job (newdisktherm_5_fuv.f90, the

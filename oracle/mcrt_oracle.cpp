@@ -2096,3 +2096,183 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
   *obj = o;
   return MCRT_OK;
 }
+
+// ===================================================================
+// setemiss: the emission tables of the Lucy reemission (oracle restatement)
+// -------------------------------------------------------------------
+// dust_5.f90:486-494 (the temperature and frequency grids), dust_5.f90:507-
+// 699 (setemiss: per species and temperature, the cumulative integral of
+// kappa_abs * B_nu and the Rosseland integral of dB_nu/dT / chi over 513
+// frequency intervals, each interval integrated by qsimp; the normalised
+// cumulative table, the Planck mean and the Rosseland mean; the 21-point
+// smoothing of the Planck mean of gas opacities, ids > ndg), dust_5.f90:784-
+// 831 (the integrands kappaB, chidB), mathsubs.f90:4-47 (Bnu, dBnu),
+// mathsubs.f90:79-113 (expm1 by the Abramowitz & Stegun 4.2.45 expansion
+// below ln 2), nr_2.f:209-254 (qsimp/trapzd: trapezoid refinement with the
+// Simpson combination, relative tolerance 1e-5, at most 20 levels; the
+// Numerical Recipes algorithm, restated from its definition) and
+// dust_5.f90:9-55 (opacset's interpolation of kappa and albedo in nu).
+// ===================================================================
+namespace setemiss_oracle {
+
+double expm1_as(double x) {
+  static const double c[7] = {0.9999999995, 0.4999999206, 0.1666653019, 0.0416573475,
+                              0.0083013598, 0.0013298820, 0.0001413161};
+  if (std::fabs(x) > 0.6931472) return std::exp(x) - 1.0;
+  double s = 0.0;
+  for (int i = 6; i >= 0; --i) s = x * (c[i] + s);
+  return s;
+}
+
+const double kNorm = 0.1539897;   // 15/pi^4 as the reference writes it
+
+double planck(double nu, double T) {
+  const double x = nu / T;
+  if (x == 0.0) return 0.0;
+  return kNorm * x * x * x / expm1_as(x);
+}
+
+double dplanck(double nu, double T) {
+  const double x = nu / T;
+  if (x == 0.0) return 0.0;
+  return -(kNorm * x * x * x * x) / (4.0 * expm1_as(x) * expm1_as(-x));
+}
+
+// kappa and albedo of one species at nu (linear in nu between the bracketing
+// nodes of the descending nudust column, clamped at the ends)
+void interp(const double* nud, const double* kd, const double* ad, int n, double nu, double& kap, double& alb) {
+  if (nu >= nud[0]) { kap = kd[0]; alb = ad[0]; return; }
+  if (nu <= nud[n - 1]) { kap = kd[n - 1]; alb = ad[n - 1]; return; }
+  int i0 = 1, i1 = n;
+  while (i1 - i0 > 1) {
+    const int i = (i1 + i0) / 2;
+    if (nu <= nud[i - 1]) i0 = i; else i1 = i;
+  }
+  const double f = (nu - nud[i1 - 1]) / (nud[i0 - 1] - nud[i1 - 1]);
+  const double fm1 = 1.0 - f;
+  kap = fm1 * kd[i1 - 1] + f * kd[i0 - 1];
+  alb = fm1 * ad[i1 - 1] + f * ad[i0 - 1];
+}
+
+// trapezoid refinement on [0, 1] with the Simpson combination; `miss` is set
+// when 20 levels do not reach the tolerance
+template <class F>
+double qsimp(const F& fn, bool& miss) {
+  double st = 0.0, ost = -1.0e30, os = -1.0e30, s = 0.0;
+  for (int j = 1; j <= 20; ++j) {
+    if (j == 1) {
+      st = 0.5 * (1.0 - 0.0) * (fn(0.0) + fn(1.0));
+    } else {
+      const long it = 1L << (j - 2);
+      const double tnm = (double)it;
+      const double del = (1.0 - 0.0) / tnm;
+      double x = 0.0 + 0.5 * del, sum = 0.0;
+      for (long k = 0; k < it; ++k) { sum = sum + fn(x); x = x + del; }
+      st = 0.5 * (st + (1.0 - 0.0) * sum / tnm);
+    }
+    s = (4.0 * st - ost) / 3.0;
+    if (std::fabs(s - os) < 1.0e-5 * std::fabs(os)) return s;
+    os = s;
+    ost = st;
+  }
+  miss = true;
+  return s;
+}
+
+void one(int i, int id, int nT, int nnu, int nlammax, const int32_t* nlambda, const double* nudust,
+         const double* kappad, const double* adust, const double* Tint, const double* nuint, double* kapint,
+         double* kappap, double* kappar, int64_t* misses) {
+  const double* nud = nudust + (int64_t)nlammax * id;
+  const double* kd = kappad + (int64_t)nlammax * id;
+  const double* ad = adust + (int64_t)nlammax * id;
+  const int n = nlambda[id];
+  const double T = Tint[i];
+  double nu1 = 0.0, k1 = 0.0, a1 = 0.0;
+  interp(nud, kd, ad, n, nu1, k1, a1);
+  double chi1 = k1, kap1 = (1.0 - a1) * k1;
+  double cum = 0.0, ross = 0.0;
+  int64_t miss = 0;
+  for (int j = 1; j <= nnu; ++j) {
+    const double nu0 = nu1;
+    nu1 = nuint[j - 1] * T;
+    const double dnu = nu1 - nu0;
+    const double dx = dnu / T;
+    const double chi0 = chi1, kap0 = kap1;
+    interp(nud, kd, ad, n, nu1, k1, a1);
+    chi1 = k1;
+    kap1 = (1.0 - a1) * k1;
+    double ik = 0.0, ic = 0.0;
+    if (nu0 / T < 50.0) {
+      bool m1 = false, m2 = false;
+      ik = qsimp([&](double f) { return ((1.0 - f) * kap0 + f * kap1) * planck(nu0 + f * dnu, T); }, m1);
+      ic = qsimp([&](double f) { return dplanck(nu0 + f * dnu, T) / ((1.0 - f) * chi0 + f * chi1); }, m2);
+      miss += (m1 ? 1 : 0) + (m2 ? 1 : 0);
+    }
+    if (j == 1) { cum = dx * ik; ross = dx * ic; }
+    else { cum = dx * ik + cum; ross = dx * ic + ross; }
+    kapint[i + (int64_t)nT * ((j - 1) + (int64_t)nnu * id)] = cum;
+  }
+  kappar[i + (int64_t)nT * id] = 1.0 / ross;
+  const double top = kapint[i + (int64_t)nT * ((nnu - 1) + (int64_t)nnu * id)];
+  kappap[i + (int64_t)nT * id] = top;
+  for (int j = 1; j <= nnu - 1; ++j) {
+    double& v = kapint[i + (int64_t)nT * ((j - 1) + (int64_t)nnu * id)];
+    v = v / top;
+  }
+  kapint[i + (int64_t)nT * ((nnu - 1) + (int64_t)nnu * id)] = 1.0;
+  misses[0] += miss;
+}
+
+// two passes of the 21-point box average of the Planck mean (ids > ndg)
+void smooth(int nT, double* kp) {
+  const int ns = 10;
+  std::vector<double> out(nT);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int i = 1; i <= nT; ++i) {
+      int lo, hi;
+      if (i > ns && i <= nT - ns) { lo = i - ns; hi = i + ns; }
+      else if (i <= ns) { lo = 1; hi = 2 * i + 1; }
+      else { lo = 2 * i - nT; hi = nT; }
+      double s = 0.0;
+      for (int k = lo; k <= hi; ++k) s = s + kp[k - 1];
+      out[i - 1] = s / (double)(hi - lo + 1);
+    }
+    for (int i = 0; i < nT; ++i) kp[i] = out[i];
+  }
+}
+
+}  // namespace setemiss_oracle
+
+extern "C" int oracle_setemiss(int32_t nopac, int32_t ndg, int32_t nlammax, const int32_t* nlambda,
+                               const double* nudust, const double* kappad, const double* adust, int32_t nT,
+                               int32_t nnu, double* lTint, double* Tint, double* nuint, double* kapint,
+                               double* kappap, double* kappar, int64_t* qsimp_misses, int32_t threads) {
+  using namespace setemiss_oracle;
+  if (nopac < 1 || nT < 21 || nnu < 2 || nlammax < 2 || ndg < 0 || ndg > nopac) return 1;   // 21: the smoothing window
+  const double Tmin = 0.1, Tmax = 200000.0, numax = 32.0, numin = numax / 1024.0;
+  for (int i = 1; i <= nT; ++i) {
+    lTint[i - 1] = std::log(Tmin / 11605.0) + (double)(i - 1) * std::log(Tmax / Tmin) / (double)(nT - 1);
+    Tint[i - 1] = std::exp(lTint[i - 1]);
+  }
+  for (int i = 1; i <= nnu; ++i) nuint[i - 1] = numin + (double)(i - 1) * (numax - numin) / (double)(nnu - 1);
+  const int64_t work = (int64_t)nT * nopac;
+  const int nth = std::max(1, threads);
+  std::atomic<int64_t> next{0};
+  std::vector<int64_t> miss(nth, 0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nth; ++t)
+    th.emplace_back([&, t]() {
+      for (;;) {
+        const int64_t w = next.fetch_add(1);
+        if (w >= work) break;
+        one((int)(w % nT), (int)(w / nT), nT, nnu, nlammax, nlambda, nudust, kappad, adust, Tint, nuint, kapint,
+            kappap, kappar, &miss[t]);
+      }
+    });
+  for (auto& x : th) x.join();
+  for (int id = ndg; id < nopac; ++id) smooth(nT, kappap + (int64_t)nT * id);
+  int64_t m = 0;
+  for (auto v : miss) m += v;
+  if (qsimp_misses) *qsimp_misses = m;
+  return 0;
+}

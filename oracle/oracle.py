@@ -49,6 +49,10 @@ def load():
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32, C.c_int32,
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.oracle_tfinal.restype = C.c_int
+        D = C.POINTER(C.c_double)
+        lib.oracle_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), D, D, D, C.c_int32,
+                                        C.c_int32, D, D, D, D, D, D, C.POINTER(C.c_int64), C.c_int32]
+        lib.oracle_setemiss.restype = C.c_int
         _lib = lib
     return _lib
 
@@ -128,3 +132,35 @@ def adjoint(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img: np
     if rc != 0:
         raise RuntimeError(f"oracle_adjoint failed with code {rc}")
     return grad, obj.value
+
+
+def setemiss(nudust, kappad, adust, nlambda, nT: int = 500, nnu: int = 513, ndg: int | None = None,
+             threads: int | None = None) -> dict:
+    """Emission tables of the reference's setemiss (dust_5.f90:486-699) from
+    dust tables in the engine layout (nudust/kappad/adust: Fortran
+    (nlammax, nopac), descending nu per column; nlambda: [nopac]).  Species
+    with index > ndg are gas opacities (Planck mean smoothed); default: all
+    dust.  Returns lTint, Tint, nuint, kapint (Fortran (nT, nnu, nopac),
+    normalised cumulative), kappap, kappar (Fortran (nT, nopac)) and the
+    number of qsimp integrals that hit the 20-level limit."""
+    lib = load()
+    nl = np.ascontiguousarray(nlambda, dtype=np.int32)
+    nopac = nl.size
+    nud = np.ascontiguousarray(nudust, dtype=np.float64)
+    nlammax = nud.size // nopac
+    kd = np.ascontiguousarray(kappad, dtype=np.float64)
+    ad = np.ascontiguousarray(adust, dtype=np.float64)
+    out = dict(lTint=np.zeros(nT), Tint=np.zeros(nT), nuint=np.zeros(nnu), kapint=np.zeros(nT * nnu * nopac),
+               kappap=np.zeros(nT * nopac), kappar=np.zeros(nT * nopac))
+    miss = C.c_int64(0)
+    D = C.POINTER(C.c_double)
+    rc = lib.oracle_setemiss(nopac, nopac if ndg is None else ndg, nlammax, nl.ctypes.data_as(C.POINTER(C.c_int32)),
+                             nud.ctypes.data_as(D), kd.ctypes.data_as(D), ad.ctypes.data_as(D), nT, nnu,
+                             *(out[k].ctypes.data_as(D) for k in ("lTint", "Tint", "nuint", "kapint", "kappap",
+                                                                 "kappar")),
+                             C.byref(miss), threads or os.cpu_count() or 1)
+    if rc != 0:
+        raise RuntimeError(f"oracle_setemiss failed ({rc})")
+    out["qsimp_misses"] = int(miss.value)
+    return out
+

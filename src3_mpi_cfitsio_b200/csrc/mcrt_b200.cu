@@ -54,6 +54,7 @@ cudaError_t launch_batch_mixed(const LaunchParams* params, const BatchItem* item
                                int grid, cudaStream_t s);
 int batch_fp64_blocks_per_sm();
 int batch_mixed_blocks_per_sm();
+cudaError_t launch_setemiss(const SetemissArgs& a, double* tmp, cudaStream_t s);
 }  // namespace mcrt
 
 using namespace mcrt;
@@ -417,7 +418,13 @@ extern "C" {
 
 const char* mcrt_version(void) { return "mcrt-b200 1.0 (sm_100a)"; }
 
-const char* mcrt_last_error(mcrt_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+// message of the last failed context-free call (mcrt_setemiss) of this thread
+static thread_local std::string g_free_err;
+
+const char* mcrt_last_error(mcrt_ctx* ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_free_err.empty() ? "null context" : g_free_err.c_str();
+}
 
 int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   mcrt_ctx* ctx = nullptr;
@@ -1957,3 +1964,120 @@ void mcrt_batch_destroy(mcrt_batch* b) {
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
+
+// ------------------------------------------------------------- setemiss --
+// The emission tables of dustinit (dust_5.f90:486-494 grids, setemiss
+// dust_5.f90:507-699) on the GPU; mcrt_setemiss.cuh holds the kernels.
+namespace {
+int sfail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_free_err = buf;
+  return code;
+}
+}  // namespace
+
+int mcrt_setemiss(int32_t device, int32_t nopac, int32_t ndg, int32_t nlammax, const int32_t* nlambda,
+                  const double* nudust, const double* kappad, const double* adust, int32_t nT, int32_t nnu,
+                  double* lTint, double* Tint, double* nuint, double* kapint, double* kappap, double* kappar,
+                  int64_t* qsimp_misses, double* device_ms) {
+  g_free_err.clear();
+  if (!nlambda || !nudust || !kappad || !adust || !lTint || !Tint || !nuint || !kapint || !kappap || !kappar)
+    return sfail(MCRT_ERR_ARG, "mcrt_setemiss: null array");
+  if (nopac < 1 || nopac > 65535 || nlammax < 2 || ndg < 0 || ndg > nopac)
+    return sfail(MCRT_ERR_ARG, "mcrt_setemiss: nopac %d, nlammax %d, ndg %d out of range", nopac, nlammax, ndg);
+  if (nT < 21 || nnu < 2 || nnu > 3072)
+    return sfail(MCRT_ERR_ARG, "mcrt_setemiss: nT must be >= 21 (smoothing window) and nnu in 2..3072");
+  for (int id = 0; id < nopac; ++id) {
+    const int n = nlambda[id];
+    if (n < 2 || n > nlammax) return sfail(MCRT_ERR_ARG, "mcrt_setemiss: nlambda(%d)=%d out of range", id + 1, n);
+    const double* nud = nudust + (int64_t)nlammax * id;
+    for (int k = 1; k < n; ++k)
+      if (!(nud[k] < nud[k - 1]))
+        return sfail(MCRT_ERR_ARG, "mcrt_setemiss: nudust(:,%d) must decrease strictly", id + 1);
+  }
+  // temperature grid 0.1 K .. 2e5 K (log-spaced, in eV) and frequency grid
+  // numax/1024 .. numax = 32 in units of kT (dust_5.f90:353-362, 486-494)
+  const double Tmin = 0.1, Tmax = 200000.0, numax = 32.0, numin = numax / 1024.0;
+  for (int i = 1; i <= nT; ++i) {
+    lTint[i - 1] = std::log(Tmin / 11605.0) + (double)(i - 1) * std::log(Tmax / Tmin) / (double)(nT - 1);
+    Tint[i - 1] = std::exp(lTint[i - 1]);
+  }
+  for (int i = 1; i <= nnu; ++i) nuint[i - 1] = numin + (double)(i - 1) * (numax - numin) / (double)(nnu - 1);
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return sfail(MCRT_ERR_CUDA, "mcrt_setemiss: cudaSetDevice: %s", cudaGetErrorString(e));
+  const size_t nl = (size_t)nlammax * nopac, nk = (size_t)nT * nnu * nopac, np_ = (size_t)nT * nopac;
+  const size_t ngas = (size_t)(nopac - ndg);
+  // one allocation, every piece 256-byte aligned: sizes first, then offsets
+  const size_t sizes[11] = {nl * 8, nl * 8, nl * 8, (size_t)nopac * 4, (size_t)nT * 8, (size_t)nnu * 8,
+                            nk * 8, np_ * 8, np_ * 8, 8, ngas * nT * 8 + 8};
+  size_t bytes = 0;
+  for (size_t z : sizes) bytes += (z + 255) / 256 * 256;
+  char* buf = nullptr;
+  e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return sfail(MCRT_ERR_CUDA, "mcrt_setemiss: cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  size_t off = 0;
+  int piece = 0;
+  bool layout_ok = true;
+  auto take = [&](size_t n) {        // the pieces in the order of `sizes`
+    layout_ok = layout_ok && piece < 11 && n == sizes[piece];
+    char* p = buf + off;
+    off += (sizes[piece < 11 ? piece : 10] + 255) / 256 * 256;
+    ++piece;
+    return p;
+  };
+  double* d_nud = (double*)take(nl * 8);
+  double* d_kd = (double*)take(nl * 8);
+  double* d_ad = (double*)take(nl * 8);
+  int32_t* d_nl = (int32_t*)take((size_t)nopac * 4);
+  double* d_T = (double*)take((size_t)nT * 8);
+  double* d_nu = (double*)take((size_t)nnu * 8);
+  double* d_ki = (double*)take(nk * 8);
+  double* d_kp = (double*)take(np_ * 8);
+  double* d_kr = (double*)take(np_ * 8);
+  unsigned long long* d_miss = (unsigned long long*)take(8);
+  double* d_tmp = (double*)take(ngas * nT * 8 + 8);
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = MCRT_OK;
+  auto chk = [&](cudaError_t x, const char* what) {
+    if (x != cudaSuccess && rc == MCRT_OK) rc = sfail(MCRT_ERR_CUDA, "mcrt_setemiss: %s: %s", what, cudaGetErrorString(x));
+    return rc == MCRT_OK;
+  };
+  if (!layout_ok || off > bytes) rc = sfail(MCRT_ERR_CUDA, "mcrt_setemiss: internal buffer layout");
+  if (rc == MCRT_OK && chk(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream") &&
+      chk(cudaEventCreate(&e0), "event") && chk(cudaEventCreate(&e1), "event") &&
+      chk(cudaMemcpyAsync(d_nud, nudust, nl * 8, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemcpyAsync(d_kd, kappad, nl * 8, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemcpyAsync(d_ad, adust, nl * 8, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemcpyAsync(d_nl, nlambda, (size_t)nopac * 4, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemcpyAsync(d_T, Tint, (size_t)nT * 8, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemcpyAsync(d_nu, nuint, (size_t)nnu * 8, cudaMemcpyHostToDevice, s), "upload") &&
+      chk(cudaMemsetAsync(d_miss, 0, 8, s), "memset") && chk(cudaEventRecord(e0, s), "event")) {
+    SetemissArgs a{};
+    a.nopac = nopac; a.ndg = ndg; a.nlammax = nlammax; a.nT = nT; a.nnu = nnu;
+    a.nlambda = d_nl; a.nudust = d_nud; a.kappad = d_kd; a.adust = d_ad; a.Tint = d_T; a.nuint = d_nu;
+    a.kapint = d_ki; a.kappap = d_kp; a.kappar = d_kr; a.misses = d_miss;
+    unsigned long long miss = 0;
+    float ms = 0.f;
+    if (chk(launch_setemiss(a, d_tmp, s), "launch") && chk(cudaEventRecord(e1, s), "event") &&
+        chk(cudaMemcpyAsync(kapint, d_ki, nk * 8, cudaMemcpyDeviceToHost, s), "download") &&
+        chk(cudaMemcpyAsync(kappap, d_kp, np_ * 8, cudaMemcpyDeviceToHost, s), "download") &&
+        chk(cudaMemcpyAsync(kappar, d_kr, np_ * 8, cudaMemcpyDeviceToHost, s), "download") &&
+        chk(cudaMemcpyAsync(&miss, d_miss, 8, cudaMemcpyDeviceToHost, s), "download") &&
+        chk(cudaStreamSynchronize(s), "synchronize") && chk(cudaEventElapsedTime(&ms, e0, e1), "timing")) {
+      if (qsimp_misses) *qsimp_misses = (int64_t)miss;
+      if (device_ms) *device_ms = ms;
+    }
+  }
+  if (s) cudaStreamSynchronize(s);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaFree(buf);
+  return rc;
+}
+

@@ -173,6 +173,21 @@ struct AdjointArgs {
 };
 constexpr int kAdjEvBits = 24;    // event index bits of a record key
 
+// Arguments of the emission-table kernels (mcrt_setemiss.cuh).
+struct SetemissArgs {
+  int32_t nopac, ndg, nlammax, nT, nnu, pad_;
+  const int32_t* nlambda;       // [nopac]
+  const double* nudust;         // (nlammax, nopac), descending nu per species
+  const double* kappad;
+  const double* adust;
+  const double* Tint;           // [nT] temperature grid [eV]
+  const double* nuint;          // [nnu] frequency grid in units of kT
+  double* kapint;               // (nT, nnu, nopac) out: normalised cumulative
+  double* kappap;               // (nT, nopac) out: Planck mean
+  double* kappar;               // (nT, nopac) out: Rosseland mean
+  unsigned long long* misses;   // qsimp integrals that hit the level limit
+};
+
 // One work item of the batch kernel (mcrt_batch.cuh): a chunk of one model's
 // packet range.
 struct BatchItem {

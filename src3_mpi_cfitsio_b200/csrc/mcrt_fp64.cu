@@ -8,6 +8,7 @@
 #include "mcrt_peel.cuh"
 #include "mcrt_wave.cuh"
 #include "mcrt_batch.cuh"
+#include "mcrt_setemiss.cuh"
 
 namespace mcrt {
 
@@ -24,6 +25,16 @@ int batch_fp64_blocks_per_sm() {
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, transport_batch, kBlock, 0) != cudaSuccess) return 1;
   return n > 0 ? n : 1;
+}
+
+cudaError_t launch_setemiss(const SetemissArgs& a, double* tmp, cudaStream_t s) {
+  const dim3 grid((unsigned)a.nT, (unsigned)a.nopac);
+  setemiss_tables<<<grid, kSetemissBlock, (size_t)2 * a.nnu * sizeof(double), s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || a.ndg >= a.nopac) return e;
+  const int ngas = a.nopac - a.ndg;
+  setemiss_smooth<<<(ngas + 63) / 64, 64, 0, s>>>(a.kappap, tmp, a.nT, a.ndg, a.nopac);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_wave_init(const WaveArgs& w, cudaStream_t s) {

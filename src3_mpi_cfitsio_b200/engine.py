@@ -71,6 +71,10 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.argtypes = [C.c_void_p]
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
+    lib.mcrt_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_double),
+                                  P(C.c_double), P(C.c_double), C.c_int32, C.c_int32, P(C.c_double), P(C.c_double),
+                                  P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int64),
+                                  P(C.c_double)]
     lib.mcrt_batch_create.argtypes = [P(C.c_void_p), C.c_int32, P(C.c_void_p)]
     lib.mcrt_batch_run_iteration.argtypes = [C.c_void_p, P(C.c_int64), C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     lib.mcrt_batch_tune.argtypes = [C.c_void_p, C.c_int64, P(C.c_int32)]
@@ -87,10 +91,58 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
-                 "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms"):
+                 "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
+                 "mcrt_setemiss"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
+
+
+def setemiss(nudust, kappad, adust, nlambda, ndg: int | None = None, nT: int = 500, nnu: int = 513,
+             device: int = 0) -> dict:
+    """The reference's emission tables (dustinit grids and setemiss,
+    dust_5.f90:486-699) built on the GPU (C ABI ``mcrt_setemiss``).
+
+    nudust/kappad/adust: Fortran (nlammax, nopac) as in ``mcrt_tables``
+    (nu strictly decreasing per species); nlambda: [nopac]; species above
+    `ndg` (default: none) are gas opacities.  Returns lTint, Tint, nuint,
+    kapint (nT*nnu*nopac, Fortran), kappap, kappar (nT*nopac), the count of
+    qsimp integrals that hit the level limit and the kernel time [ms]."""
+    lib = load_library()
+    nl = np.ascontiguousarray(nlambda, dtype=np.int32)
+    nopac = nl.size
+    nud = np.ascontiguousarray(nudust, dtype=np.float64)
+    kd = np.ascontiguousarray(kappad, dtype=np.float64)
+    ad = np.ascontiguousarray(adust, dtype=np.float64)
+    nlammax = nud.size // nopac
+    out = dict(lTint=np.zeros(nT), Tint=np.zeros(nT), nuint=np.zeros(nnu), kapint=np.zeros(nT * nnu * nopac),
+               kappap=np.zeros(nT * nopac), kappar=np.zeros(nT * nopac))
+    miss = C.c_int64(0)
+    ms = C.c_double(0.0)
+    D = C.POINTER(C.c_double)
+    rc = lib.mcrt_setemiss(device, nopac, nopac if ndg is None else ndg, nlammax,
+                           nl.ctypes.data_as(C.POINTER(C.c_int32)), nud.ctypes.data_as(D), kd.ctypes.data_as(D),
+                           ad.ctypes.data_as(D), nT, nnu,
+                           *(out[k].ctypes.data_as(D) for k in ("lTint", "Tint", "nuint", "kapint", "kappap",
+                                                               "kappar")),
+                           C.byref(miss), C.byref(ms))
+    if rc != 0:
+        raise MCRTError(f"mcrt_setemiss failed (code {rc}): {lib.mcrt_last_error(None).decode()}")
+    out["qsimp_misses"] = int(miss.value)
+    out["device_ms"] = ms.value
+    return out
+
+
+def with_setemiss_tables(model, ndg: int | None = None, device: int = 0):
+    """Replace the model's emission tables by the reference's setemiss
+    tables built on the GPU (the model generator uses its own quadrature)."""
+    t = model.tables
+    r = setemiss(t["nudust"], t["kappad"], t["adust"], t["nlambda"], ndg=ndg, device=device)
+    for k in ("lTint", "Tint", "nuint", "kapint", "kappap", "kappar"):
+        t[k] = r[k]
+    model.config["nT"] = r["lTint"].size
+    model.config["nnu"] = r["nuint"].size
+    return model
 
 
 class Engine:

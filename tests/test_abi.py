@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -72,3 +73,14 @@ def test_struct_layouts_match_the_c_compiler():
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_setemiss_rejects_bad_tables_without_a_gpu():
+    """mcrt_setemiss checks its inputs before any CUDA call: a wavelength
+    column whose nu does not decrease is refused with a message."""
+    from src3_mpi_cfitsio_b200.engine import MCRTError, setemiss
+    nud = np.array([1.0, 2.0, 0.5])
+    with pytest.raises(MCRTError, match="decrease"):
+        setemiss(nud, np.ones(3), np.zeros(3), [3])
+    with pytest.raises(MCRTError, match="nT"):
+        setemiss(np.array([2.0, 1.0]), np.ones(2), np.zeros(2), [2], nT=10)

@@ -186,3 +186,75 @@ def test_disk_law_log_derivatives():
     a = m.grid["densarr"].reshape(-1, 10, order="F")
     b = mm.grid["densarr"].reshape(-1, 10, order="F")
     assert np.allclose(b[:, 1], 2.0 * a[:, 1], rtol=1e-12) and np.array_equal(b[:, 2:], a[:, 2:])
+
+
+def _gray_dust(nl=100, kap=2.0, alb=0.25):
+    nud = np.logspace(2, -4, nl)
+    return nud, np.full(nl, kap), np.full(nl, alb)
+
+
+def test_setemiss_oracle_gray_dust_is_the_planck_integral():
+    """setemiss restatement (dust_5.f90:507-699) for a gray absorber: the
+    Planck mean is (1-albedo) kappa times the normalised Planck integral up to
+    x = 32, the Rosseland mean is kappa, and the cumulative table is the
+    normalised Planck integral, all to the qsimp tolerance (1e-5) and the
+    reference's 7-digit 15/pi^4 and A&S expm1."""
+    from scipy import integrate
+    from oracle import oracle as O
+    nud, kd, ad = _gray_dust()
+    r = O.setemiss(nud, kd, ad, [nud.size], threads=4)
+    assert r["qsimp_misses"] == 0
+    norm = 0.1539897
+    F = lambda x: norm * x ** 3 / np.expm1(x)
+    dF = lambda x: norm * x ** 4 * np.exp(x) / (4.0 * np.expm1(x) ** 2)
+    tot = integrate.quad(F, 0, 32, epsabs=0, epsrel=1e-13, limit=200)[0]
+    dtot = integrate.quad(dF, 0, 32, epsabs=0, epsrel=1e-13, limit=200)[0]
+    assert np.allclose(r["kappap"], 0.75 * 2.0 * tot, rtol=1e-6, atol=0)
+    assert np.allclose(r["kappar"], 2.0 / dtot, rtol=1e-6, atol=0)
+    ki = r["kapint"].reshape((500, 513), order="F")
+    xs = r["nuint"][[10, 64, 200, 400]]
+    cum = np.array([integrate.quad(F, 0, x, epsabs=0, epsrel=1e-13)[0] for x in xs]) / tot
+    assert np.allclose(ki[250, [10, 64, 200, 400]], cum, rtol=2e-5, atol=0)
+    assert np.all(np.diff(ki, axis=1) >= 0) and np.all(ki[:, -1] == 1.0)
+
+
+def test_setemiss_oracle_agrees_with_an_independent_quadrature():
+    """The reference's algorithm (qsimp per interval, opacity and albedo
+    interpolated separately) against the model generator's 12-point
+    Gauss-Legendre tables of the same dust law."""
+    from oracle import oracle as O
+    m = model.small_2d()
+    t = m.tables
+    r = O.setemiss(t["nudust"], t["kappad"], t["adust"], t["nlambda"], threads=4)
+    assert np.array_equal(r["lTint"], t["lTint"]) and np.array_equal(r["nuint"], t["nuint"])
+    assert np.abs(r["kappap"] / t["kappap"] - 1).max() < 1e-3
+    assert np.abs(r["kappar"] / t["kappar"] - 1).max() < 1e-4
+    assert np.abs(r["kapint"] - t["kapint"]).max() < 1e-3
+
+
+def test_setemiss_oracle_smooths_gas_planck_means():
+    """Species above ndg (gas opacities) get two passes of the 21-point box
+    average of the Planck mean with the window shrinking at the ends
+    (dust_5.f90:623-663); dust species and the other tables are unchanged."""
+    from oracle import oracle as O
+    nl = 60
+    nud = np.logspace(2, -4, nl)
+    lam = 1.2398 / nud
+    cols = [np.stack([nud, 3.0 * lam ** -1.5, 0.5 / (1 + lam)]),
+            np.stack([nud, 1.0 + np.sin(np.log(lam)) ** 2, np.full(nl, 0.1)])]
+    nudust = np.concatenate([c[0] for c in cols])
+    kd = np.concatenate([c[1] for c in cols])
+    ad = np.concatenate([c[2] for c in cols])
+    a = O.setemiss(nudust, kd, ad, [nl, nl], threads=2)
+    b = O.setemiss(nudust, kd, ad, [nl, nl], ndg=1, threads=2)
+    nT = 500
+    assert np.array_equal(a["kapint"], b["kapint"]) and np.array_equal(a["kappar"], b["kappar"])
+    assert np.array_equal(a["kappap"][:nT], b["kappap"][:nT])
+    kp = a["kappap"][nT:].copy()
+    for _ in range(2):
+        out = np.empty(nT)
+        for i in range(1, nT + 1):
+            lo, hi = (i - 10, i + 10) if 10 < i <= nT - 10 else ((1, 2 * i + 1) if i <= 10 else (2 * i - nT, nT))
+            out[i - 1] = kp[lo - 1:hi].sum() / (hi - lo + 1)
+        kp = out
+    assert np.allclose(b["kappap"][nT:], kp, rtol=1e-13, atol=0)
