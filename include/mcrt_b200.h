@@ -302,6 +302,15 @@ int mcrt_device_tallies_view(mcrt_ctx *ctx, mcrt_device_tallies *out);
 int mcrt_adjoint(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo, int64_t iphot_hi, int32_t iter,
                  int32_t seed1, int32_t seed2, int32_t generator,
                  const double *lam_psed, const double *lam_img, double *grad, double *objective);
+/* Packets per adjoint chunk (default 2^25).  No reference counterpart.  The
+ * adjoint runs its range in chunks: forward pass, record sort and replay
+ * per chunk, with the gradient and objective summed.  Packets are
+ * independent in the adjoint because diffusion heating is frozen, so the
+ * sums equal a single pass.  A chunk whose peel-off records would reach 2^31
+ * (the device sort's 32-bit count) is redone in halves; optically thick
+ * models without diffusion cells can need that.  Every chunk's forward pass
+ * ends with its own tail of long-lived packets, so large chunks are faster. */
+int mcrt_set_adjoint_chunk(mcrt_ctx *ctx, int64_t packets);
 
 /* Recompute the diffusion cells' end-of-iteration temperature of the last
  * mcrt_run_iteration from the (reduced) diffusion absorption counts and the

@@ -89,6 +89,8 @@ struct mcrt_ctx {
   unsigned long long *d_adj_nlist = nullptr;
   void *d_adj_tmp = nullptr;
   size_t adj_tmp_bytes = 0;
+  int64_t adj_chunk = (int64_t)1 << 25;   // packets per adjoint chunk (halved when its records reach 2^31)
+  double* d_adj_sum = nullptr;        // [ncell*10 + 1] gradient and objective summed over chunks
   int64_t adj_sort_cap = 0;           // capacity of the sorted copies (skey, sc) and the sort scratch
   bool have_grid = false, have_tables = false;
   bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
@@ -1109,29 +1111,12 @@ int mcrt_run_iteration(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   return run_iteration_impl(ctx, np, lo, hi, iter, ipeel, seed1, seed2, generator, 0);
 }
 
-int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t seed1, int32_t seed2,
-                 int32_t generator, const double* lam_psed, const double* lam_img, double* grad, double* objective) {
-  if (!ctx || !lam_psed || !grad || !objective) return MCRT_ERR_ARG;
-  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
-  if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range");
-  const mcrt_config& c = ctx->cfg;
-  if (c.npeel < 1) return fail(ctx, MCRT_ERR_ARG, "the adjoint differentiates peeled outputs: npeel must be >= 1");
-  if (ctx->dm.nslot > kJobSlots) return fail(ctx, MCRT_ERR_UNSUPPORTED, "adjoint needs at most %d opacity species", kJobSlots);
-  const int64_t npk = hi - lo + 1;
-  if (npk >= ((int64_t)1 << 31)) return fail(ctx, MCRT_ERR_ARG, "adjoint packet range must be < 2^31");
-  CK(cudaSetDevice(ctx->device));
-  const int64_t ncell = ctx->ncell;
+namespace {
+
+// per-packet record arrays for a chunk of npk packets (kept between calls)
+int adjoint_buffers(mcrt_ctx* ctx, int64_t npk) {
   AdjointArgs& A = ctx->adj;
   int rc;
-  // buffers (kept between calls; re-sized for larger ranges)
-  if (!A.grad) {
-    double *lp, *gr, *ob, *li = nullptr;
-    if ((rc = dalloc(ctx, &lp, (size_t)std::max<int64_t>(ctx->npsed, 1))) || (rc = dalloc(ctx, &gr, (size_t)ncell * 10)) ||
-        (rc = dalloc(ctx, &ob, 1)) || (ctx->nimg > 0 && (rc = dalloc(ctx, &li, (size_t)ctx->nimg))) ||
-        (rc = dalloc(ctx, &ctx->d_adj_nlist, 1)))
-      return rc;
-    A.lam_psed = lp; A.grad = gr; A.obj = ob; A.lam_img = li;
-  }
   if (ctx->adj_npk_cap < npk) {
     for (void* q : {(void*)A.rec_key, (void*)A.rec_c, (void*)A.start, (void*)A.end, (void*)A.list})
       if (q) dfree(ctx, q);
@@ -1150,11 +1135,21 @@ int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter
     ctx->adj_npk_cap = npk;
     ctx->adj_sort_cap = 0;
   }
-  CK(cudaMemcpyAsync((void*)A.lam_psed, lam_psed, (size_t)ctx->npsed * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if (ctx->nimg > 0) {
-    if (lam_img) CK(cudaMemcpyAsync((void*)A.lam_img, lam_img, (size_t)ctx->nimg * 8, cudaMemcpyHostToDevice, ctx->stream));
-    else CK(cudaMemsetAsync((void*)A.lam_img, 0, (size_t)ctx->nimg * 8, ctx->stream));
-  }
+  return MCRT_OK;
+}
+
+// One chunk lo..hi of the packet range: forward pass, record sort, replay.
+// The chunk's gradient and objective are left in A.grad / A.obj (zeroed
+// here).  *too_many: the chunk holds 2^31 records or more (the device sort
+// takes a 32-bit count); nothing is sorted or replayed then.
+int adjoint_chunk(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t seed1, int32_t seed2,
+                  int32_t generator, double* total_ms_out, bool* too_many) {
+  AdjointArgs& A = ctx->adj;
+  const int64_t ncell = ctx->ncell;
+  const int64_t npk = hi - lo + 1;
+  int rc;
+  *too_many = false;
+  if ((rc = adjoint_buffers(ctx, npk))) return rc;
   CK(cudaMemsetAsync(A.grad, 0, (size_t)ncell * 10 * 8, ctx->stream));
   CK(cudaMemsetAsync(A.obj, 0, 8, ctx->stream));
   CK(cudaMemsetAsync(A.rec_key, 0xff, (size_t)A.rec_cap * 8, ctx->stream));
@@ -1175,22 +1170,26 @@ int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter
   const int64_t nrec = ctx->adj_rec_used;
   cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
   CK(cudaEventRecord(e0, ctx->stream));
+  if (nrec > INT32_MAX) {               // before any buffer changes: the caller halves the chunk
+    *too_many = true;
+    return MCRT_OK;
+  }
   if (nrec > ctx->adj_sort_cap) {      // sorted copies and scratch for nrec records
     for (void* q : {(void*)A.skey, (void*)A.sc, ctx->d_adj_tmp})
       if (q) dfree(ctx, q);
+    const int64_t cap32 = std::min<int64_t>(std::max<int64_t>(nrec, 2 * ctx->adj_sort_cap), INT32_MAX);
     A.skey = nullptr; A.sc = nullptr; ctx->d_adj_tmp = nullptr;
-    const int64_t cap = std::max<int64_t>(nrec, 2 * ctx->adj_sort_cap);
-    if (cap > INT32_MAX) return fail(ctx, MCRT_ERR_ARG, "adjoint: more than 2^31 peel-off records");
+    ctx->adj_sort_cap = 0;
     unsigned long long* sk;
     double* scv;
-    if ((rc = dalloc(ctx, &sk, cap)) || (rc = dalloc(ctx, &scv, cap))) return rc;
+    if ((rc = dalloc(ctx, &sk, cap32)) || (rc = dalloc(ctx, &scv, cap32))) return rc;
     size_t tmp = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, A.rec_key, sk, A.rec_c, scv, (int)cap));
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tmp, A.rec_key, sk, A.rec_c, scv, (int)cap32));
     if ((rc = dalloc(ctx, (char**)&ctx->d_adj_tmp, std::max<size_t>(tmp, 1)))) return rc;
     ctx->adj_tmp_bytes = tmp;
     A.skey = sk;
     A.sc = scv;
-    ctx->adj_sort_cap = cap;
+    ctx->adj_sort_cap = cap32;
   }
   if (nrec > 0) {
     size_t tmp = ctx->adj_tmp_bytes;
@@ -1213,9 +1212,74 @@ int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter
     if ((rc = run_iteration_impl(ctx, np, lo, hi, iter, 0, seed1, seed2, generator, 2))) return rc;
     total_ms += ctx->last_ms;
   }
+  *total_ms_out += total_ms;
+  return MCRT_OK;
+}
+
+__global__ void add_doubles(const double* src, double* dst, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] += src[i];
+}
+
+}  // namespace
+
+int mcrt_set_adjoint_chunk(mcrt_ctx* ctx, int64_t packets) {
+  if (!ctx || packets < 1 || packets >= ((int64_t)1 << 31)) return MCRT_ERR_ARG;
+  ctx->adj_chunk = packets;
+  return MCRT_OK;
+}
+
+int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t seed1, int32_t seed2,
+                 int32_t generator, const double* lam_psed, const double* lam_img, double* grad, double* objective) {
+  if (!ctx || !lam_psed || !grad || !objective) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (np < 1 || lo < 1 || hi > np || lo > hi) return fail(ctx, MCRT_ERR_ARG, "bad packet range");
+  const mcrt_config& c = ctx->cfg;
+  if (c.npeel < 1) return fail(ctx, MCRT_ERR_ARG, "the adjoint differentiates peeled outputs: npeel must be >= 1");
+  if (ctx->dm.nslot > kJobSlots) return fail(ctx, MCRT_ERR_UNSUPPORTED, "adjoint needs at most %d opacity species", kJobSlots);
+  const int64_t npk = hi - lo + 1;
+  CK(cudaSetDevice(ctx->device));
+  const int64_t ncell = ctx->ncell;
+  AdjointArgs& A = ctx->adj;
+  int rc;
+  // buffers (kept between calls; re-sized for larger ranges)
+  if (!A.grad) {
+    double *lp, *gr, *ob, *li = nullptr;
+    if ((rc = dalloc(ctx, &lp, (size_t)std::max<int64_t>(ctx->npsed, 1))) || (rc = dalloc(ctx, &gr, (size_t)ncell * 10)) ||
+        (rc = dalloc(ctx, &ob, 1)) || (ctx->nimg > 0 && (rc = dalloc(ctx, &li, (size_t)ctx->nimg))) ||
+        (rc = dalloc(ctx, &ctx->d_adj_nlist, 1)))
+      return rc;
+    A.lam_psed = lp; A.grad = gr; A.obj = ob; A.lam_img = li;
+  }
+  CK(cudaMemcpyAsync((void*)A.lam_psed, lam_psed, (size_t)ctx->npsed * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->nimg > 0) {
+    if (lam_img) CK(cudaMemcpyAsync((void*)A.lam_img, lam_img, (size_t)ctx->nimg * 8, cudaMemcpyHostToDevice, ctx->stream));
+    else CK(cudaMemsetAsync((void*)A.lam_img, 0, (size_t)ctx->nimg * 8, ctx->stream));
+  }
+  if (!ctx->d_adj_sum && (rc = dalloc(ctx, &ctx->d_adj_sum, (size_t)ncell * 10 + 1))) return rc;
+  CK(cudaMemsetAsync(ctx->d_adj_sum, 0, ((size_t)ncell * 10 + 1) * 8, ctx->stream));
+  // Packets are independent here (diffusion heating is frozen), so the
+  // gradient and the objective of lo..hi are the sums over chunks; a chunk
+  // whose records would reach 2^31 is redone in halves.
+  double total_ms = 0.0;
+  int64_t chunk = std::min<int64_t>(npk, ctx->adj_chunk);
+  for (int64_t c_lo = lo; c_lo <= hi;) {
+    const int64_t c_hi = std::min(hi, c_lo + chunk - 1);
+    bool too_many = false;
+    if ((rc = adjoint_chunk(ctx, np, c_lo, c_hi, iter, seed1, seed2, generator, &total_ms, &too_many))) return rc;
+    if (too_many) {
+      if (c_hi == c_lo) return fail(ctx, MCRT_ERR_ARG, "adjoint: one packet with 2^31 peel-off records");
+      chunk = std::max<int64_t>(1, (c_hi - c_lo + 1) / 2);
+      continue;
+    }
+    add_doubles<<<256, 256, 0, ctx->stream>>>(A.grad, ctx->d_adj_sum, ncell * 10);
+    add_doubles<<<1, 32, 0, ctx->stream>>>(A.obj, ctx->d_adj_sum + ncell * 10, 1);
+    CK(cudaGetLastError());
+    c_lo = c_hi + 1;
+  }
   ctx->last_ms = total_ms;
-  CK(cudaMemcpyAsync(grad, A.grad, (size_t)ncell * 10 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(objective, A.obj, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(grad, ctx->d_adj_sum, (size_t)ncell * 10 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(objective, ctx->d_adj_sum + ncell * 10, 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return MCRT_OK;
 }

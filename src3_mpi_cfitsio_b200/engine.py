@@ -71,6 +71,7 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.argtypes = [C.c_void_p]
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
+    lib.mcrt_set_adjoint_chunk.argtypes = [C.c_void_p, C.c_int64]
     lib.mcrt_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_double),
                                   P(C.c_double), P(C.c_double), C.c_int32, C.c_int32, P(C.c_double), P(C.c_double),
                                   P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int64),
@@ -92,7 +93,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
                  "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
-                 "mcrt_setemiss"):
+                 "mcrt_setemiss", "mcrt_set_adjoint_chunk"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -280,6 +281,11 @@ class Engine:
                                           lp.ctypes.data_as(D), li.ctypes.data_as(D) if li is not None else None,
                                           grad.ctypes.data_as(D), C.byref(obj)))
         return grad, obj.value
+
+    def set_adjoint_chunk(self, packets: int):
+        """Packets per adjoint chunk (forward, sort and replay per chunk;
+        gradients and objective summed)."""
+        self._check(self.lib.mcrt_set_adjoint_chunk(self.ctx, int(packets)))
 
     def refresh_diffusion(self):
         """Diffusion-cell temperatures of the last run from the (reduced) counts."""

@@ -532,3 +532,25 @@ def test_adjoint_mixed_precision_and_repeatability(warm_small):
         a = ga.reshape((ncell, 10), order="F")[:, comp].sum()
         b = gb.reshape((ncell, 10), order="F")[:, comp].sum()
         assert abs(b - a) <= 0.1 * abs(a), comp
+
+
+def test_adjoint_chunks_sum_to_one_pass(warm_small):
+    """mcrt_adjoint in packet chunks (forward, sort and replay per chunk)
+    gives the single pass's gradient and objective: the packets are
+    independent with diffusion heating frozen."""
+    m = model.with_diffusion(warm_small)
+    lam, img = _adjoint_weights(m)
+    n = 6000
+    eng = _engine(m)
+    g1, L1 = eng.adjoint(n, lam, img)
+    eng.set_adjoint_chunk(1500)
+    g2, L2 = eng.adjoint(n, lam, img)
+    eng.set_adjoint_chunk(777)                 # ragged last chunk
+    g3, L3 = eng.adjoint(n, lam, img, lo=1001, hi=n)
+    eng.set_adjoint_chunk(1 << 23)
+    g4, L4 = eng.adjoint(n, lam, img, lo=1001, hi=n)
+    eng.close()
+    assert abs(L2 - L1) <= 1e-12 * abs(L1) and abs(L4 - L3) <= 1e-12 * abs(L4)
+    tol = 1e-9 * np.abs(g1).max()
+    assert np.allclose(g1, g2, rtol=1e-9, atol=tol) and np.allclose(g3, g4, rtol=1e-9, atol=tol)
+    assert L3 < L1
