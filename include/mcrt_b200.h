@@ -372,6 +372,44 @@ int mcrt_synchronize(mcrt_ctx *ctx);
 const char *mcrt_last_error(mcrt_ctx *ctx);   /* NULL: the last failed context-free call of this thread */
 void mcrt_destroy(mcrt_ctx *ctx);
 
+/* Parameters of the density law of mcrt_model_density (lengths in stellar
+ * radii unless noted). */
+typedef struct mcrt_density_params {
+  double rstar;        /* stellar radius [Rsun] */
+  double autors;       /* AU in stellar radii (214.94 / rstar, setup.f90:45) */
+  double rddust;       /* dust destruction radius = inner disk and envelope edge */
+  double rmax;         /* outer grid radius */
+  double rmaxd;        /* outer disk radius */
+  double massd;        /* disk mass [Msun] */
+  double a_exp, b_exp; /* disk density and flaring exponents */
+  double h100_au;      /* disk scale height at 100 AU [AU] */
+  double rate;         /* envelope infall rate [Msun/yr] */
+  double rc;           /* centrifugal radius */
+  double massc;        /* central mass [Msun] */
+  double rhoamb;       /* ambient density floor [g/cm^3] */
+  double thet1_deg;    /* cavity opening angle at rmax [deg] */
+  double ex1;          /* cavity shape exponent */
+  double rhoconst1;    /* cavity density [g/cm^3] */
+} mcrt_density_params;
+
+/* Density grid on the GPU: the disk + Ulrich envelope + polynomial cavity
+ * model of gridset for one parameter set.  Replaces the density part of
+ * gridset_5_model13new.f90: the disk (setup_wave.f90:60-88, scale height
+ * setup.f90:96-99), the Ulrich envelope (envset.f90:157-160, densenv.f90:37-43;
+ * the mu0 cubic of zerod.f90), the polynomial cavity (envset.f90:182-189,
+ * densenv.f90:76-90), the disk's ownership of the cells where it is denser
+ * than the envelope and cavity gas (gridset_5_model13new.f90:1217-1224) and
+ * the cell volumes (:1147-1150).  In: walls rarr[nrg], thetarr[ntg]
+ * (stellar radii, radians); `clump` (may be NULL) multiplies the envelope
+ * per cell, Fortran (nrg-1, ntg-1, npg-1).  Out: densarr Fortran
+ * (nrg, ntg, npg, 10) with components 2 (disk), 3 (envelope), 4 (cavity);
+ * vcell (nrg, ntg, npg) [cm^3]; dlog_disk (may be NULL) Fortran
+ * (nrg-1, ntg-1, 3) = d log rho_disk / d (log Mdisk, b, log h100) per cell,
+ * analytic, zero outside the disk.  No context needed; runs on `device`. */
+int mcrt_model_density(int32_t device, const mcrt_density_params *p, int32_t nrg, int32_t ntg, int32_t npg,
+                       const double *rarr, const double *thetarr, const double *clump, double *densarr,
+                       double *vcell, double *dlog_disk);
+
 /* Emission tables on the GPU: replaces the temperature and frequency grids
  * of dustinit (dust_5.f90:486-494) and setemiss (dust_5.f90:507-699; the
  * reference splits the species over its MPI ranks and reduces).  No context

@@ -86,6 +86,13 @@ class PacketLog(C.Structure):
         "nub", "cost", "phi", "sip", "sqp", "sup", "svp", "xp", "yp", "zp")]
 
 
+class DensityParams(C.Structure):
+    """mcrt_density_params (parameters of mcrt_model_density)."""
+    _fields_ = [(n, C.c_double) for n in (
+        "rstar", "autors", "rddust", "rmax", "rmaxd", "massd", "a_exp", "b_exp", "h100_au", "rate", "rc",
+        "massc", "rhoamb", "thet1_deg", "ex1", "rhoconst1")]
+
+
 class DeviceTallies(C.Structure):
     """mcrt_device_tallies: device addresses of the three tally segments."""
     _fields_ = [("f64", C.c_void_p), ("n_f64", C.c_int64), ("u64", C.c_void_p), ("n_u64", C.c_int64),

@@ -2145,3 +2145,172 @@ int mcrt_setemiss(int32_t device, int32_t nopac, int32_t ndg, int32_t nlammax, c
   return rc;
 }
 
+
+// -------------------------------------------------------- density model --
+// One thread per (r, theta) cell: the disk law, the Ulrich envelope, the
+// polynomial cavity, the disk's ownership of a cell and the cell volume for
+// every phi plane, plus the disk law's analytic log-derivatives.
+namespace {
+
+constexpr double kPi = 3.1415926535897932384626433;
+constexpr double kRsun = 6.9598e10, kMsun = 1.989e33, kGN = 6.67428e-8;
+
+struct DensityArgs {
+  mcrt_density_params p;
+  int32_t nrg, ntg, npg, has_clump;
+  const double *rarr, *thetarr, *clump;
+  double *dens, *vcell, *dlog;
+  double rho0, z1, rhoe0, c1e, dlog_b_const;   // cell-independent parts, from the host
+};
+
+// the positive root of mu0^3 + (rx-1) mu0 - rx mu = 0 (zerod.f90), in [1e-12, 1]
+__device__ double ulrich_mu0(double mu, double rx) {
+  const double a2 = rx - 1.0, a3 = -rx * mu;
+  const double q = (-3.0 * a2) / 9.0, r = (27.0 * a3) / 54.0;
+  const double q3 = q * q * q;
+  double out;
+  if (q3 - r * r >= 0.0) {
+    const double qh = sqrt(q);
+    const double th = acos(fmin(fmax(r / sqrt(q3), -1.0), 1.0));
+    out = HUGE_VAL;
+    const double roots[3] = {-2.0 * qh * cos(th / 3.0), -2.0 * qh * cos((th + 2.0 * kPi) / 3.0),
+                             -2.0 * qh * cos((th + 4.0 * kPi) / 3.0)};
+    for (double x : roots)
+      if (x > 0.0 && x < out) out = x;
+  } else {
+    const double fac = sqrt(r * r - q3) + fabs(r);
+    const double f3 = pow(fac, 1.0 / 3.0);
+    const double sg = r > 0.0 ? 1.0 : (r < 0.0 ? -1.0 : 0.0);
+    out = -sg * (f3 + q / f3);
+  }
+  return fmin(fmax(out, 1e-12), 1.0);
+}
+
+__global__ void model_density(DensityArgs a) {
+  const int nr = a.nrg - 1, nt = a.ntg - 1, npc = a.npg - 1;
+  const int64_t n = (int64_t)nr * nt;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(c % nr), it = (int)(c / nr);
+    const mcrt_density_params& p = a.p;
+    const double rave = 0.5 * (a.rarr[ir] + a.rarr[ir + 1]);
+    const double thave = 0.5 * (a.thetarr[it] + a.thetarr[it + 1]);
+    const double wcyl = rave * sin(thave), zp = rave * fabs(cos(thave));
+    // disk (setup_wave.f90:60-88): rho0 (1 - sqrt(R*/w)) w^-a exp(-z^2/2h^2), h = z1 w^b
+    const double h = a.z1 * pow(wcyl, p.b_exp);
+    double rho_d = a.rho0 * (1.0 - sqrt(1.0 / wcyl)) * pow(wcyl, -p.a_exp) * exp(-0.5 * ((zp / h) * (zp / h)));
+    if (!(rave > p.rddust && wcyl <= p.rmaxd && wcyl > 1.0) || !(rho_d > 1e-300)) rho_d = 0.0;
+    // Ulrich envelope (densenv.f90:37-43), floor rhoamb outside the dust radius
+    const double mu = zp / rave, rx = rave / p.rc;
+    const double mu0 = ulrich_mu0(mu, rx);
+    const double factor = 1.0 / ((mu / mu0) + 2.0 * mu0 * mu0 / rx);
+    double rho_e = a.rhoe0 * pow(rx, -1.5) * factor / sqrt(1.0 + mu / mu0);
+    rho_e = rave > p.rddust ? fmax(rho_e, p.rhoamb) : 0.0;
+    // polynomial cavity (densenv.f90:76-90)
+    const double zup = a.c1e * pow(wcyl, p.ex1);
+    const bool inhole = zp > zup;
+    const double rho_c = (inhole && rave > p.rddust && rave < p.rmax) ? p.rhoconst1 : 0.0;
+    if (inhole || rave >= p.rmax) rho_e = 0.0;
+    const double dr3 = a.rarr[ir + 1] * a.rarr[ir + 1] * a.rarr[ir + 1] - a.rarr[ir] * a.rarr[ir] * a.rarr[ir];
+    const double dcost = cos(a.thetarr[it + 1]) - cos(a.thetarr[it]);
+    const double rmincgs = p.rstar * kRsun;
+    const double vol = -(dr3 * dcost) * (2.0 * kPi / npc) / 3.0 * (rmincgs * rmincgs * rmincgs);
+    for (int ip = 0; ip < npc; ++ip) {
+      const int64_t cell = ir + (int64_t)a.nrg * (it + (int64_t)a.ntg * ip);
+      const int64_t ncell = (int64_t)a.nrg * a.ntg * a.npg;
+      const double re = a.has_clump ? rho_e * a.clump[ir + (int64_t)nr * (it + (int64_t)nt * ip)] : rho_e;
+      // the disk owns the cell where it is denser (gridset_5_model13new.f90:1217-1224)
+      const bool disk = rho_d > re + rho_c;
+      a.dens[cell + ncell * 1] = disk ? rho_d : 0.0;
+      a.dens[cell + ncell * 2] = disk ? 0.0 : re;
+      a.dens[cell + ncell * 3] = disk ? 0.0 : rho_c;
+      a.vcell[cell] = vol;
+    }
+    if (a.dlog) {
+      double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+      if (rho_d > 0.0) {
+        const double zh2 = (zp / h) * (zp / h);
+        d0 = 1.0;                                             // log Mdisk
+        d1 = a.dlog_b_const + zh2 * (log(wcyl) - log(100.0 * p.autors));   // b
+        d2 = zh2 - 1.0;                                       // log h100
+      }
+      a.dlog[c] = d0;
+      a.dlog[c + n] = d1;
+      a.dlog[c + 2 * n] = d2;
+    }
+  }
+}
+
+}  // namespace
+
+int mcrt_model_density(int32_t device, const mcrt_density_params* p, int32_t nrg, int32_t ntg, int32_t npg,
+                       const double* rarr, const double* thetarr, const double* clump, double* densarr,
+                       double* vcell, double* dlog_disk) {
+  g_free_err.clear();
+  if (!p || !rarr || !thetarr || !densarr || !vcell) return sfail(MCRT_ERR_ARG, "mcrt_model_density: null array");
+  if (nrg < 3 || ntg < 2 || npg < 2) return sfail(MCRT_ERR_ARG, "mcrt_model_density: grid too small");
+  if (!(p->rstar > 0) || !(p->autors > 0) || !(p->rddust > 1.0) || !(p->rmaxd > p->rddust) || !(p->rmax > p->rddust) ||
+      !(p->massd >= 0) || !(p->h100_au > 0) || !(p->rc > 0) || !(p->massc > 0) || !(p->rate >= 0) ||
+      !(p->thet1_deg > 0 && p->thet1_deg < 90))
+    return sfail(MCRT_ERR_ARG, "mcrt_model_density: parameters out of range");
+  for (int i = 1; i < nrg; ++i)
+    if (!(rarr[i] > rarr[i - 1])) return sfail(MCRT_ERR_ARG, "mcrt_model_density: rarr must increase");
+  for (int i = 1; i < ntg; ++i)
+    if (!(thetarr[i] > thetarr[i - 1])) return sfail(MCRT_ERR_ARG, "mcrt_model_density: thetarr must increase");
+  DensityArgs a{};
+  a.p = *p;
+  a.nrg = nrg; a.ntg = ntg; a.npg = npg; a.has_clump = clump ? 1 : 0;
+  // cell-independent parts: disk normalisation to Mdisk over [rddust, rmaxd]
+  // (setup_wave.f90:60-88), the envelope constant (envset.f90:157-160) and
+  // the cavity shape (envset.f90:182-189)
+  const double b = p->b_exp, pp = p->b_exp - p->a_exp;
+  const double rmincgs = p->rstar * kRsun;
+  a.z1 = p->h100_au * p->autors / std::pow(100.0 * p->autors, b);
+  const double cst = std::pow(2.0 * kPi, 1.5) * rmincgs * rmincgs * (rmincgs * a.z1);
+  const double R = p->rmaxd, r = p->rddust;
+  const double A = std::pow(R, pp + 2.0) - std::pow(r, pp + 2.0), B = std::pow(R, pp + 1.5) - std::pow(r, pp + 1.5);
+  const double I = 1.0 / (pp + 2.0) * A - 1.0 / (pp + 1.5) * B;
+  a.rho0 = p->massd * kMsun / cst / I;
+  const double dA = std::pow(R, pp + 2.0) * std::log(R) - std::pow(r, pp + 2.0) * std::log(r);
+  const double dB = std::pow(R, pp + 1.5) * std::log(R) - std::pow(r, pp + 1.5) * std::log(r);
+  const double dI = dA / (pp + 2.0) - A / ((pp + 2.0) * (pp + 2.0)) - dB / (pp + 1.5) + B / ((pp + 1.5) * (pp + 1.5));
+  a.dlog_b_const = std::log(100.0 * p->autors) - dI / I;
+  const double rdcgs = p->rc * rmincgs;
+  const double cenv = 1.0 / 3.15576e7 * std::sqrt(kMsun) / (4.0 * kPi) / std::sqrt(kGN);
+  a.rhoe0 = cenv * p->rate / std::sqrt(p->massc) / std::pow(rdcgs, 1.5);
+  const double r1max = p->rmax * std::tan(p->thet1_deg * kPi / 180.0);
+  a.c1e = p->rmax / std::pow(r1max, p->ex1);
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return sfail(MCRT_ERR_CUDA, "mcrt_model_density: cudaSetDevice: %s", cudaGetErrorString(e));
+  const int64_t nr = nrg - 1, nt = ntg - 1, npc = npg - 1;
+  const size_t ncell = (size_t)nrg * ntg * npg;
+  const size_t sz[6] = {(size_t)nrg * 8, (size_t)ntg * 8, clump ? (size_t)(nr * nt * npc) * 8 : 8, ncell * 10 * 8,
+                        ncell * 8, dlog_disk ? (size_t)(nr * nt * 3) * 8 : 8};
+  size_t bytes = 0;
+  for (size_t z : sz) bytes += (z + 255) / 256 * 256;
+  char* buf = nullptr;
+  e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return sfail(MCRT_ERR_CUDA, "mcrt_model_density: cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  char* ptr[6];
+  size_t off = 0;
+  for (int k = 0; k < 6; ++k) { ptr[k] = buf + off; off += (sz[k] + 255) / 256 * 256; }
+  a.rarr = (double*)ptr[0]; a.thetarr = (double*)ptr[1]; a.clump = clump ? (double*)ptr[2] : nullptr;
+  a.dens = (double*)ptr[3]; a.vcell = (double*)ptr[4]; a.dlog = dlog_disk ? (double*)ptr[5] : nullptr;
+  int rc = MCRT_OK;
+  auto chk = [&](cudaError_t x, const char* what) {
+    if (x != cudaSuccess && rc == MCRT_OK) rc = sfail(MCRT_ERR_CUDA, "mcrt_model_density: %s: %s", what, cudaGetErrorString(x));
+    return rc == MCRT_OK;
+  };
+  if (chk(cudaMemcpy(ptr[0], rarr, sz[0], cudaMemcpyHostToDevice), "upload") &&
+      chk(cudaMemcpy(ptr[1], thetarr, sz[1], cudaMemcpyHostToDevice), "upload") &&
+      (!clump || chk(cudaMemcpy(ptr[2], clump, sz[2], cudaMemcpyHostToDevice), "upload")) &&
+      chk(cudaMemset(ptr[3], 0, sz[3]), "memset") && chk(cudaMemset(ptr[4], 0, sz[4]), "memset")) {
+    const int grid = (int)std::min<int64_t>((nr * nt + 255) / 256, 4096);
+    model_density<<<grid, 256>>>(a);
+    if (chk(cudaGetLastError(), "launch") && chk(cudaDeviceSynchronize(), "kernel") &&
+        chk(cudaMemcpy(densarr, ptr[3], sz[3], cudaMemcpyDeviceToHost), "download") &&
+        chk(cudaMemcpy(vcell, ptr[4], sz[4], cudaMemcpyDeviceToHost), "download"))
+      if (dlog_disk) chk(cudaMemcpy(dlog_disk, ptr[5], sz[5], cudaMemcpyDeviceToHost), "download");
+  }
+  cudaFree(buf);
+  return rc;
+}

@@ -71,6 +71,9 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_destroy.argtypes = [C.c_void_p]
     lib.mcrt_destroy.restype = None
     lib.mcrt_version.restype = C.c_char_p
+    lib.mcrt_model_density.argtypes = [C.c_int32, P(abi.DensityParams), C.c_int32, C.c_int32, C.c_int32,
+                                       P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double),
+                                       P(C.c_double)]
     lib.mcrt_set_adjoint_chunk.argtypes = [C.c_void_p, C.c_int64]
     lib.mcrt_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_double),
                                   P(C.c_double), P(C.c_double), C.c_int32, C.c_int32, P(C.c_double), P(C.c_double),
@@ -93,7 +96,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
                  "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
-                 "mcrt_setemiss", "mcrt_set_adjoint_chunk"):
+                 "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_model_density"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -132,6 +135,42 @@ def setemiss(nudust, kappad, adust, nlambda, ndg: int | None = None, nT: int = 5
     out["qsimp_misses"] = int(miss.value)
     out["device_ms"] = ms.value
     return out
+
+
+def density_params(w) -> "abi.DensityParams":
+    """mcrt_density_params of a model.Workload (lengths to stellar radii)."""
+    autors = 214.94 / w.rstar
+    return abi.DensityParams(rstar=w.rstar, autors=autors, rddust=w.rddust_au * autors, rmax=w.rmax_au * autors,
+                             rmaxd=w.rmaxd_au * autors, massd=w.massd, a_exp=w.a_exp, b_exp=w.b_exp,
+                             h100_au=w.h100_au, rate=w.rate, rc=w.rc_au * autors, massc=w.massc, rhoamb=w.rhoamb,
+                             thet1_deg=w.thet1_deg, ex1=w.ex1, rhoconst1=w.rhoconst1)
+
+
+def model_density(model, device: int = 0, derivatives: bool = True):
+    """The model's density grid built on the GPU (C ABI mcrt_model_density)
+    from its Workload parameters and walls: (densarr [ncell*10] Fortran,
+    vcell [ncell], dlog_disk or None).  dlog_disk is Fortran
+    (nrg-1, ntg-1, 3): d log rho_disk / d (log Mdisk, b, log h100), analytic."""
+    lib = load_library()
+    w = model.w
+    nrg, ntg, npg = w.nrg, w.ntg, w.npg
+    prm = density_params(w)
+    D = C.POINTER(C.c_double)
+    rarr = np.ascontiguousarray(model.grid["rarr"], dtype=np.float64)
+    thetarr = np.ascontiguousarray(model.grid["thetarr"], dtype=np.float64)
+    clump = None
+    if w.clump_seed is not None:
+        clump = np.asfortranarray(model._clump_field(nrg - 1, ntg - 1, max(npg - 1, 1))).ravel(order="F")
+    dens = np.zeros(nrg * ntg * npg * 10)
+    vcell = np.zeros(nrg * ntg * npg)
+    dlog = np.zeros((nrg - 1) * (ntg - 1) * 3) if derivatives else None
+    rc = lib.mcrt_model_density(device, C.byref(prm), nrg, ntg, npg, rarr.ctypes.data_as(D),
+                                thetarr.ctypes.data_as(D), clump.ctypes.data_as(D) if clump is not None else None,
+                                dens.ctypes.data_as(D), vcell.ctypes.data_as(D),
+                                dlog.ctypes.data_as(D) if dlog is not None else None)
+    if rc != 0:
+        raise MCRTError(f"mcrt_model_density failed (code {rc}): {lib.mcrt_last_error(None).decode()}")
+    return dens, vcell, dlog
 
 
 def with_setemiss_tables(model, ndg: int | None = None, device: int = 0):

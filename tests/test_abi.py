@@ -55,7 +55,7 @@ def test_struct_layouts_match_the_c_compiler():
     inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
     structs = {"mcrt_config": abi.Config, "mcrt_grid": abi.Grid, "mcrt_tables": abi.Tables,
                "mcrt_tallies": abi.Tallies, "mcrt_packet_log": abi.PacketLog,
-               "mcrt_device_tallies": abi.DeviceTallies}
+               "mcrt_device_tallies": abi.DeviceTallies, "mcrt_density_params": abi.DensityParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mcrt_b200.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
