@@ -425,7 +425,8 @@ def run_ours(args, rank, world):
         t0g = time.perf_counter()
         g, Lg = eng.adjoint(args.grad_packets, lam, img, iteration=it + 2)
         grad_wall = time.perf_counter() - t0g
-        pgrad = madj.parameter_gradient(m, g)
+        from src3_mpi_cfitsio_b200.engine import model_density
+        pgrad = madj.parameter_gradient(m, g, dlog=model_density(m, device=dev)[2])   # analytic disk-law derivatives
         extra["gradient"] = {"packets": args.grad_packets, "seconds": grad_wall,
                              "device_seconds": eng.kernel_ms() / 1e3, "objective": Lg,
                              "outputs": "peeled SED (all bins) + 3.6/24/70 um images, Stokes I",

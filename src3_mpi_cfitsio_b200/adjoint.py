@@ -47,15 +47,22 @@ def sed_image_weights(m, image_um=(3.6, 24.0, 70.0), sed_weight: float = 1.0, im
     return lam.ravel(order="F"), img.ravel(order="F")
 
 
-def parameter_gradient(m, grad: np.ndarray) -> dict:
+def parameter_gradient(m, grad: np.ndarray, dlog: np.ndarray | None = None) -> dict:
     """Chain rule from dL/dlog(rho) (engine layout [ncell*10], Fortran
     (nrg,ntg,npg,10)) to the disk parameters of ``model.DISK_PARAMS``:
-    dL/dlog(Mdisk), dL/db, dL/dlog(h100)."""
+    dL/dlog(Mdisk), dL/db, dL/dlog(h100).  `dlog`: the disk law's
+    log-derivatives, Fortran (nrg-1, ntg-1, 3), e.g. the analytic ones of
+    ``engine.model_density``; default: central differences of the host law."""
     w = m.w
     G = grad.reshape((w.nrg, w.ntg, w.npg, 10), order="F")[:-1, :-1, :max(w.npg - 1, 1), DISK_ID - 1]
     dens = m.grid["densarr"].reshape((w.nrg, w.ntg, w.npg, 10), order="F")[:-1, :-1, :max(w.npg - 1, 1), DISK_ID - 1]
+    if dlog is None:
+        ders = mdl.disk_log_derivatives(m)
+    else:
+        D = np.asarray(dlog).reshape((w.nrg - 1, w.ntg - 1, 3), order="F")
+        ders = {name: D[:, :, k] for k, name in enumerate(mdl.DISK_PARAMS)}
     out = {}
-    for name, d in mdl.disk_log_derivatives(m).items():
+    for name, d in ders.items():
         out[name] = float(np.sum(np.where(dens > 0, G * d[:, :, None], 0.0)))
     return out
 
