@@ -180,47 +180,63 @@ def bench_setemiss(args, dev):
     return out
 
 
-def bench_batch(args, dev):
+def bench_batch(args, dev, rank=0, world=1, allreduce=None):
     """Batched sweep: `--batch-models` seeded uneven models (nr 50-200,
     ntheta 49-199, nphi 1-32; Mdisk, Mdot, cavity angle and wavelength set
     drawn from the seed), `--batch-packets` packets each, mixed precision,
     one Lucy iteration per CUDA-graph launch, schedule and queue sizes from
-    the autotuner.  Compared with the same models run one after another
-    (Engine.run, wavefront schedule) on a sample of 8 models."""
-    from src3_mpi_cfitsio_b200 import model
+    the autotuner.  Under torchrun the models are sharded whole over the
+    ranks (dist.shard_models, no exchange) and the time is the maximum over
+    ranks.  Compared with the same models run one after another (Engine.run,
+    wavefront schedule) on a sample of 8 of rank 0's models."""
+    import numpy as np
+
+    from src3_mpi_cfitsio_b200 import dist, model
     from src3_mpi_cfitsio_b200.batch import Batch
     from src3_mpi_cfitsio_b200.engine import Engine
     nmod, n = args.batch_models, args.batch_packets
-    models = [model.with_diffusion(model.warm(m)) for m in model.batch_models(nmod)]
+    works = model.batch_workloads(nmod)
+    mine = dist.shard_models([w.nrg + w.ntg + w.npg for w in works], world)[rank]   # ~crossings per packet
+    models = [model.with_diffusion(model.warm(model.batch_model(works[i]))) for i in mine]
     engines = [Engine(m, device=dev, precision="mixed") for m in models]
-    b = Batch(engines)
-    tuned = b.tune(args.batch_tune_packets)
-    b.run_iteration([n] * nmod, iteration=1)                 # capture + warm
-    t0 = time.perf_counter()
-    b.run_iteration([n] * nmod, iteration=2)
-    wall = time.perf_counter() - t0
-    ms = b.kernel_ms()
-    pk = sum(e.download(images=False).counters()["packets"] for e in engines)
-    b.close()
-    seq_ms = 0.0
-    sample = engines[:min(8, nmod)]
-    for e in sample:
-        e.set_schedule("wave")
-        e.reset_tallies()
-        e.run(n, iteration=2, ipeel=0)
-        seq_ms += e.kernel_ms()
+    ms = 0.0
+    tuned = None
+    pk = 0
+    if engines:
+        b = Batch(engines)
+        tuned = b.tune(args.batch_tune_packets)
+        b.run_iteration([n] * len(engines), iteration=1)          # capture + warm
+        b.run_iteration([n] * len(engines), iteration=2)
+        ms = b.kernel_ms()
+        pk = sum(e.download(images=False).counters()["packets"] for e in engines)
+        b.close()
+    ms_max = float(allreduce(np.array([ms]), "max")[0]) if allreduce else ms
+    pk_all = int(allreduce(np.array([float(pk)]), "sum")[0]) if allreduce else pk
+    seq_pps = None
+    if rank == 0 and engines:
+        seq_ms = 0.0
+        sample = engines[:min(8, len(engines))]
+        for e in sample:
+            e.set_schedule("wave")
+            e.reset_tallies()
+            e.run(n, iteration=2, ipeel=0)
+            seq_ms += e.kernel_ms()
+        seq_pps = len(sample) * n / (seq_ms / 1e3)
     for e in engines:
         e.close()
-    seq_pps = len(sample) * n / (seq_ms / 1e3)
-    cells = [mm.ncells for mm in models]
+    if rank != 0:
+        return None
+    cells = [(w.nrg - 1) * (w.ntg - 1) * (w.npg - 1) for w in works]
+    own = len(mine) * n / (ms / 1e3) if ms > 0 else None
     return {"workload": f"{nmod} uneven models (cells {min(cells)}-{max(cells)}), {n:.0e} packets each, one Lucy "
                         "iteration per graph launch, diffusion on",
-            "models": nmod, "packets_per_model": n, "packets_total": pk, "precision": "mixed",
-            "packets_per_s": nmod * n / (ms / 1e3), "seconds": ms / 1e3, "wall_seconds": wall,
-            "tuning": tuned,
-            "sequential_wave_packets_per_s": seq_pps,
-            "batch_over_sequential": (nmod * n / (ms / 1e3)) / seq_pps,
-            "sequential_sample": f"first {len(sample)} models, Engine.run each (host-driven wavefront loop)"}
+            "models": nmod, "packets_per_model": n, "packets_total": pk_all, "precision": "mixed",
+            "ranks": world, "models_on_rank0": len(mine),
+            "packets_per_s": nmod * n / (ms_max / 1e3), "seconds": ms_max / 1e3,
+            "tuning_rank0": tuned,
+            "sequential_wave_packets_per_s_rank0": seq_pps,
+            "batch_over_sequential_rank0": (own / seq_pps) if (own and seq_pps) else None,
+            "sequential_sample": "first 8 of rank 0's models, Engine.run each (host-driven wavefront loop)"}
 
 
 def run_ours(args, rank, world):
@@ -437,8 +453,10 @@ def run_ours(args, rank, world):
         extra["clumpy_3d"] = bench_clumpy(args, dev)
     if rank == 0:
         extra["setemiss"] = bench_setemiss(args, dev)
-    if rank == 0 and args.batch_models > 0:
-        extra["batch"] = bench_batch(args, dev)
+    if args.batch_models > 0:                  # every rank: the models are sharded over the ranks
+        res = bench_batch(args, dev, rank, world, allreduce if dist else None)
+        if rank == 0:
+            extra["batch"] = res
     out = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=ms_steps / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,

@@ -8,6 +8,9 @@ iteration's packet range into contiguous shards of the same substream
 sequence, so the summed tallies equal a one-GPU run of the whole range
 whatever the number of ranks.
 
+A batched sweep (``batch.Batch``) shards whole models instead
+(``shard_models``): its models are independent, so no tally crosses ranks.
+
 Two reductions:
 
 * ``allreduce_device_tallies`` sums the device tally buffer in place over
@@ -33,6 +36,26 @@ def shard_range(np_total: int, rank: int, world: int) -> tuple[int, int]:
     lo = rank * base + min(rank, extra) + 1
     hi = lo + base - 1 + (1 if rank < extra else 0)
     return lo, hi
+
+
+def shard_models(weights, world: int) -> list:
+    """Models of a batched sweep per rank (no exchange between ranks: every
+    model is whole on one GPU).  Greedy longest-first assignment by `weights`
+    (e.g. packets x cells per model) to the least-loaded rank, ties to the
+    lower rank: deterministic, and the heaviest rank carries at most the
+    lightest one's load plus one model.  Returns one ascending index list
+    per rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    w = [float(x) for x in weights]
+    order = sorted(range(len(w)), key=lambda i: (-w[i], i))
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += w[i]
+    return [sorted(x) for x in out]
 
 
 class _DeviceArray:

@@ -784,18 +784,28 @@ def batch_models(n: int = 64, seed: int = 20240605) -> list:
     1e-7..1e-5 Msun/yr, cavity opening angle uniform in 5..40 deg; the dust
     law sampled on 60-140 wavelengths (uneven wavelength sets).  No image
     cube (temperature iterations do not peel)."""
+    return [batch_model(w) for w in batch_workloads(n, seed)]
+
+
+def batch_workloads(n: int = 64, seed: int = 20240605) -> list:
+    """The parameters of ``batch_models`` without building the models (a
+    sharded sweep builds only its own)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n):
         nr = int(rng.integers(50, 201))
         nt = int(rng.integers(24, 100)) * 2 + 1
         nph = int(rng.integers(1, 33))
-        w = Workload(nrg=nr + 1, ntg=nt, npg=nph + 1,
-                     massd=float(10.0 ** rng.uniform(-4.0, -1.0)),
-                     rate=float(10.0 ** rng.uniform(-7.0, -5.0)),
-                     thet1_deg=float(rng.uniform(5.0, 40.0)),
-                     nlambda=int(rng.integers(60, 141)))
-        m = Model(w)
-        m.config["output_imcube"] = 0
-        out.append(m)
+        out.append(Workload(nrg=nr + 1, ntg=nt, npg=nph + 1,
+                            massd=float(10.0 ** rng.uniform(-4.0, -1.0)),
+                            rate=float(10.0 ** rng.uniform(-7.0, -5.0)),
+                            thet1_deg=float(rng.uniform(5.0, 40.0)),
+                            nlambda=int(rng.integers(60, 141))))
     return out
+
+
+def batch_model(w: Workload) -> Model:
+    """One sweep model: no image cube."""
+    m = Model(w)
+    m.config["output_imcube"] = 0
+    return m

@@ -73,3 +73,50 @@ def test_two_gloo_ranks_reduce_to_the_single_run(oracle_mod):
         if a.dtype == np.float32:
             assert np.allclose(red[k], a, rtol=2e-6, atol=1e-6 * max(1e-30, float(np.abs(a).max()))), k
     assert one["ti"].sum() > 0 and one["nums"].sum() > 0
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_shard_models_balances_whole_models(world):
+    rng = np.random.default_rng(world)
+    w = rng.uniform(1.0, 100.0, 64)
+    parts = dist.shard_models(w, world)
+    assert sorted(i for p in parts for i in p) == list(range(64))
+    loads = [float(w[np.array(p, dtype=int)].sum()) for p in parts]
+    assert max(loads) - min(loads) <= w.max() + 1e-9
+    assert parts == dist.shard_models(w, world)          # deterministic
+
+
+def _sweep_rank(rank, world, port, out_dir):
+    import torch.distributed as tdist
+    from oracle import oracle
+    tdist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        models = _sweep_models()
+        mine = dist.shard_models([m.ncells for m in models], world)[rank]
+        for i in mine:
+            tal, _ = oracle.run(abi.Bundle(models[i]), 300, ipeel=0, threads=1)
+            np.savez(os.path.join(out_dir, f"model{i}.npz"), nabs=tal["nabs"], counters=tal["counters"],
+                     dtauabs=tal["dtauabs"])
+        tdist.barrier()
+    finally:
+        tdist.destroy_process_group()
+
+
+def _sweep_models():
+    return [model.warm(model.small_2d(nrg=n, ntg=t, npg=p, massd=md))
+            for n, t, p, md in ((21, 15, 2, 1e-3), (27, 17, 4, 3e-3), (31, 21, 2, 1e-2), (25, 13, 3, 5e-4))]
+
+
+def test_two_gloo_ranks_run_a_sharded_sweep(oracle_mod):
+    """A sweep sharded by whole models over two ranks gives every model the
+    result of its own single-process run (no exchange between ranks)."""
+    import torch.multiprocessing as mp
+    world = 2
+    with tempfile.TemporaryDirectory() as d:
+        mp.start_processes(_sweep_rank, args=(world, _free_port(), d), nprocs=world, join=True,
+                           start_method="spawn")
+        got = [dict(np.load(os.path.join(d, f"model{i}.npz"))) for i in range(4)]
+    for i, m in enumerate(_sweep_models()):
+        one, _ = oracle_mod.run(abi.Bundle(m), 300, ipeel=0, threads=1)
+        assert np.array_equal(got[i]["nabs"], one["nabs"]) and np.array_equal(got[i]["counters"], one["counters"])
+        assert np.allclose(got[i]["dtauabs"], one["dtauabs"], rtol=1e-12, atol=0)
