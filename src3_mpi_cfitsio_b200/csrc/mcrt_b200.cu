@@ -134,6 +134,7 @@ struct mcrt_ctx {
   void *d_flush = nullptr;
   int64_t off_Tint = 0, off_kappap = 0;   // offsets of Tint/kappap in d_tabs (tfinal)
   std::vector<double> h_rarr;
+  std::vector<int32_t> species_grid;  // per species: first species with a bit-identical wavelength column
 };
 
 namespace {
@@ -734,6 +735,17 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;
+  // species that share a wavelength column (same length, same values bit for
+  // bit) share opacset's bracket search
+  ctx->species_grid.assign(c.nopac, 0);
+  for (int id = 0; id < c.nopac; ++id) {
+    ctx->species_grid[id] = id;
+    for (int k = 0; k < id; ++k) {
+      if (ctx->species_grid[k] != k || t->nlambda[k] != t->nlambda[id]) continue;
+      if (std::memcmp(t->nudust + (int64_t)c.nlammax * k, t->nudust + (int64_t)c.nlammax * id,
+                      (size_t)t->nlambda[id] * 8) == 0) { ctx->species_grid[id] = k; break; }
+    }
+  }
   ctx->have_tables = true;
   ctx->off_Tint = off[22];
   ctx->off_kappap = off[23];
@@ -841,6 +853,12 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   m.ifuv_ori = c.ifuv_ori;
   m.cspot1 = c.cspot1; m.sspot1 = c.sspot1; m.scspot1 = c.scspot1; m.ssspot1 = c.ssspot1;
   m.cspot2 = c.cspot2; m.sspot2 = c.sspot2; m.scspot2 = c.scspot2; m.ssspot2 = c.ssspot2; m.csprad = c.csprad;
+  for (int s = 0; s < kMaxSlot; ++s) {      // slot -> first slot on the same wavelength grid
+    m.slot_grid[s] = s;
+    if (s >= m.nslot) continue;
+    for (int k = 0; k < s; ++k)
+      if (ctx->species_grid[m.slot_species[k] - 1] == ctx->species_grid[m.slot_species[s] - 1]) { m.slot_grid[s] = k; break; }
+  }
   P.t = ctx->dt;
   P.np = np; P.lo = lo; P.hi = hi;
   if (iter < 1) return fail(ctx, MCRT_ERR_ARG, "iter must be >= 1");

@@ -68,6 +68,7 @@ struct DevModel {
   const double *tdust, *vcell;              // tdust: start-of-iteration values
   // species: slot -> species (1-based) and the species tables
   int slot_species[kMaxSlot];
+  int slot_grid[kMaxSlot];          // first slot whose species has the same wavelength grid (opacset shares its bracket)
   const int32_t *nlambda;
   const double *nudust, *kappad, *adust, *gdust, *pldust, *kappav;
   const double *kapint, *lTint, *nuint;

@@ -144,24 +144,31 @@ struct Packet {
 
   // opacset (dust_5.f90:9-109) for the referenced species, then kapd with
   // the association order of the calling site.
+  // opacset (dust_5.f90:9-55) for the species of every slot.  Slots whose
+  // species share a wavelength column (slot_grid) reuse the bracket and the
+  // interpolation weight of the first such slot: the same search over the
+  // same values gives the same result.
   __device__ void opacset(double nu, int order) {
+    int a = 0, b = 0, have = -1;
+    double f = 0.0;
     for (int s = 0; s < m.nslot; ++s) {
       const int id = m.slot_species[s] - 1;
       const int nl = m.nlammax;
-      const double* nud = m.nudust + (int64_t)nl * id;
-      const int n = m.nlambda[id];
-      int a, b;
-      double f;
-      if (nu >= __ldg(nud)) { a = 0; b = 0; f = 0.0; }
-      else if (nu <= __ldg(nud + n - 1)) { a = n - 1; b = n - 1; f = 0.0; }
-      else {
-        int i0 = 1, i1 = n;
-        while (i1 - i0 > 1) {
-          int i = (i1 + i0) >> 1;
-          if (nu <= __ldg(nud + i - 1)) i0 = i; else i1 = i;
+      if (m.slot_grid[s] != have) {
+        const double* nud = m.nudust + (int64_t)nl * id;
+        const int n = m.nlambda[id];
+        if (nu >= __ldg(nud)) { a = 0; b = 0; f = 0.0; }
+        else if (nu <= __ldg(nud + n - 1)) { a = n - 1; b = n - 1; f = 0.0; }
+        else {
+          int i0 = 1, i1 = n;
+          while (i1 - i0 > 1) {
+            int i = (i1 + i0) >> 1;
+            if (nu <= __ldg(nud + i - 1)) i0 = i; else i1 = i;
+          }
+          a = i1 - 1; b = i0 - 1;
+          f = (nu - __ldg(nud + a)) / (__ldg(nud + b) - __ldg(nud + a));
         }
-        a = i1 - 1; b = i0 - 1;
-        f = (nu - __ldg(nud + a)) / (__ldg(nud + b) - __ldg(nud + a));
+        have = m.slot_grid[s];
       }
       const double* kd = m.kappad + (int64_t)nl * id;
       const double* ad = m.adust + (int64_t)nl * id;
