@@ -145,6 +145,12 @@ typedef struct mcrt_tables {
    * A scattering interpolates two wavelength nodes with opacset's weights. */
   const double  *mueller;
   int32_t        narr, pad_mueller;
+  /* External illumination (ISRF packets, isrf_frac > 0), optional: the
+   * sampling table that isrf_cdf.f90 leaves in isrf_mod, isrf(nisrf,3) =
+   * cdf_i, logcdf_i, logfreq_i (frequencies in eV, the first row as that
+   * routine sets it: cdf 0, log cdf -99, log freq 0).  NULL when unused. */
+  const double  *isrf;
+  int32_t        nisrf, pad_isrf;
 } mcrt_tables;
 
 /*

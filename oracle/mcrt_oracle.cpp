@@ -449,6 +449,38 @@ struct Packet {
     sinp = std::sin(phi);
     cosp = std::cos(phi);
   }
+  // initpout.f90:1-68 with rep_isrf.f90: a point on the outer sphere
+  // (uniform cosb and longitude), an inward direction with cos = -xi in the
+  // local frame, rotated by initp_transform; the frequency from the ISRF cdf
+  // table, interpolated linearly in log10(cdf) and log10(nu).
+  void initpout() {
+    sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+    double xran = ran();
+    cosb = 1.0 - 2.0 * xran;
+    sinb = std::sqrt(1.0 - cosb * cosb);
+    xran = ran();
+    cost = -xran;
+    sint = std::sqrt(1.0 - cost * cost);
+    xran = ran();
+    phi = R2P * xran;
+    cosp = std::cos(phi);
+    sinp = std::sin(phi);
+    xran = ran();
+    lp = R2P * xran;
+    initp_transform();
+    xran = ran();
+    const int n = m->t->nisrf;
+    const double* cdf = m->t->isrf;
+    const double* lcdf = cdf + n;
+    const double* lfrq = cdf + 2 * n;
+    int ifreq = locate(cdf, n, xran);
+    if (ifreq == n) ifreq = n - 1;
+    if (ifreq == 0) ifreq = 1;
+    const double logfreq = lfrq[ifreq - 1] + (std::log10(xran) - lcdf[ifreq - 1]) / (lcdf[ifreq] - lcdf[ifreq - 1]) *
+                                                 (lfrq[ifreq] - lfrq[ifreq - 1]);
+    nub = std::pow(10.0, logfreq);
+  }
+
   void initpspot(int ispotph) {    // initpspot.f90:3-175
     const mcrt_config& c = m->c;
     sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
@@ -1555,8 +1587,28 @@ struct Packet {
           }
         }
       }
-    } else {
-      return -1;   // external illumination: rejected up front
+    } else {                                 // external illumination, newdisktherm_5_fuv.f90:416-460
+      initpout();
+      on_wall = true;
+      i_orig = 5;
+      opacset(nub);
+      kapd_disk();
+      const double coslp = std::cos(lp), sinlp = std::sin(lp);
+      const double rmax = m->rarr[m->nrg - 1];
+      zp = cosb * rmax * 0.999999;
+      const double rp = sinb * rmax * 0.999999;
+      xp = rp * coslp;
+      yp = rp * sinlp;
+      rsq = zp * zp + rp * rp;
+      rtot = std::sqrt(rsq);
+      ux = sint * cosp;
+      uy = sint * sinp;
+      uz = cost;
+      iflag = 0;
+      ii[0] = m->nrg - 1;
+      ii[1] = locate(m->thetarr.data(), m->ntg, std::acos(cosb));
+      ii[2] = locate(m->phiarr.data(), m->npg, lp);
+      // no peel-off of the direct light: it is the sky background
     }
     ifuv = is_fuv(nub) ? c.ifuv_ori : 0.0;
     return propagate(ii);
@@ -1736,7 +1788,7 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   int64_t npaccstar = (int64_t)(cfg->accfrac2 * (double)np);
   int64_t nsum = ns + npacc + npout;
   if (nsum != np) ns = ns + np - nsum;
-  if (npout > 0) return MCRT_ERR_UNSUPPORTED;
+  if (npout > 0 && (!tab->isrf || tab->nisrf < 2)) return MCRT_ERR_ARG;   // external packets need the ISRF table
   if (npacc > 1 && (!grid->ravearr || !grid->Ldint || !grid->hdisk)) return MCRT_ERR_ARG;
   // emit_common receives nphot = ns of the (rank's) run; a shard uses its share
   m.nphot_diff = (double)ns * (double)(iphot_hi - iphot_lo + 1) / (double)np;
@@ -2033,7 +2085,7 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
   int64_t npacc = (int64_t)((double)np * cfg->accfrac);
   int64_t npaccstar = (int64_t)(cfg->accfrac2 * (double)np);
   if (ns + npacc + npout != np) ns = ns + np - (ns + npacc + npout);
-  if (npout > 0) return MCRT_ERR_UNSUPPORTED;
+  if (npout > 0 && (!tab->isrf || tab->nisrf < 2)) return MCRT_ERR_ARG;   // external packets need the ISRF table
   m.nphot_diff = (double)ns * (double)(iphot_hi - iphot_lo + 1) / (double)np;
   const int ips = (cfg->rddust > 100.0) ? 1 : 0;
   const int64_t nsed = (int64_t)cfg->nfreq * cfg->nmu * cfg->nph * cfg->nap * MCRT_NO;

@@ -59,7 +59,8 @@ TABLE_FIELDS = [("nlambda", _ip), ("nudust", _dp), ("kappad", _dp), ("adust", _d
                 ("kappar", _dp), ("atmosnu", _dp), ("hnuint", _dp), ("lognu", _dp),
                 ("loghnu", _dp), ("aperture2", _dp), ("u", _dp), ("coste_arr", _dp),
                 ("sinte_arr", _dp), ("cospe_arr", _dp), ("sinpe_arr", _dp),
-                ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32)]
+                ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32),
+                ("isrf", _dp), ("nisrf", C.c_int32), ("pad_isrf", C.c_int32)]
 
 
 class Tables(C.Structure):

@@ -94,6 +94,7 @@ struct mcrt_ctx {
   int64_t adj_sort_cap = 0;           // capacity of the sorted copies (skey, sc) and the sort scratch
   bool have_grid = false, have_tables = false;
   bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
+  bool have_isrf = false;             // ISRF sampling table uploaded (external-illumination packets)
   std::string err;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -702,6 +703,16 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
     add(t->mueller, 6 * nb * nrow);                                                                    // 24
     add(peak.data(), nrow);                                                                            // 25
   }
+  // ISRF sampling table of external-illumination packets (isrf_cdf.f90):
+  // cdf_i, logcdf_i, logfreq_i, as the driver's isrf_mod holds them
+  const bool isrf = t->isrf != nullptr && t->nisrf > 0;
+  const int isrf_at = isrf ? (int)off.size() : -1;
+  if (isrf) {
+    if (t->nisrf < 2 || t->nisrf > 1000000) return fail(ctx, MCRT_ERR_ARG, "nisrf must be 2..1e6");
+    for (int i = 1; i < t->nisrf; ++i)
+      if (!(t->isrf[i] >= t->isrf[i - 1])) return fail(ctx, MCRT_ERR_ARG, "isrf cdf must be non-decreasing");
+    add(t->isrf, 3 * (int64_t)t->nisrf);
+  }
   // jump tables a^(2^30 * 2^k)
   std::vector<int64_t> jump(128);
   int64_t j1 = 1033780774, j2 = 1494757890;   // a1w, a2w (ecuyer_cote_mod.f90:14-15)
@@ -732,6 +743,11 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.mpeak = mueller ? b + off[25] : nullptr;
   m.narr = mueller ? t->narr : 0;
   m.dct = mueller ? 2.0 / (double)t->narr : 0.0;
+  m.nisrf = isrf ? t->nisrf : 0;
+  m.isrf_cdf = isrf ? b + off[isrf_at] : nullptr;
+  m.isrf_logcdf = isrf ? m.isrf_cdf + t->nisrf : nullptr;
+  m.isrf_logfreq = isrf ? m.isrf_cdf + 2 * (int64_t)t->nisrf : nullptr;
+  ctx->have_isrf = isrf;
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;
@@ -836,7 +852,8 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   if (nsum != np) ns = ns + np - nsum;
   if (npacc > 1 && !ctx->have_acc)
     return fail(ctx, MCRT_ERR_ARG, "accretion packets (accfrac > 0) need ravearr, Ldint and hdisk in mcrt_upload_grid");
-  if (npout > 0) return fail(ctx, MCRT_ERR_UNSUPPORTED, "external-illumination packets (initpout) are outside the built scope");
+  if (npout > 0 && !ctx->have_isrf)
+    return fail(ctx, MCRT_ERR_ARG, "external-illumination packets (isrf_frac > 0) need the isrf table in mcrt_upload_tables");
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;
   for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }

@@ -77,6 +77,9 @@ struct DevModel {
   const double *mueller, *mpeak;
   int narr;
   double dct;
+  // external illumination: the ISRF sampling table (isrf_mod after isrf_cdf.f90)
+  const double *isrf_cdf, *isrf_logcdf, *isrf_logfreq;
+  int nisrf;
   // star
   const double *atmosnu, *hnuint, *lognu, *loghnu, *limb_prob;
   const double *inczeta;                     // [MCRT_IZMAX]

@@ -339,7 +339,30 @@ struct Lane {
           pk.on_wall = false;
           pk.nscat = pk.nabsev = pk.ncross = pk.nstar = pk.ndiffev = 0;
           status = 0;
-          if (iphot > P.npacc + P.ns) { status = 3; ev = EV_FINISH; break; }   // external illumination: refused at launch
+          if (iphot > P.npacc + P.ns) {     // external illumination, newdisktherm_5_fuv.f90:416-460
+            pk.initpout();
+            pk.on_wall = true;
+            pk.i_orig = 5;
+            pk.opacset(pk.nub, KAPD_DISK);
+            coslp = cos(pk.lp);
+            sinlp = sin(pk.lp);
+            const double rmax = m.rarr[m.nrg - 1];
+            pk.zp = pk.cosb * rmax * 0.999999;
+            const double rp = pk.sinb * rmax * 0.999999;
+            pk.xp = rp * coslp;
+            pk.yp = rp * sinlp;
+            pk.rsq = pk.zp * pk.zp + rp * rp;
+            pk.rtot = sqrt(pk.rsq);
+            pk.ux = pk.sint * pk.cosp;
+            pk.uy = pk.sint * pk.sinp;
+            pk.uz = pk.cost;
+            pk.iflag = 0;
+            pk.ir = m.nrg - 1;
+            pk.it = locate(m.thetarr, m.ntg, acos(pk.cosb));
+            pk.ip = locate(m.phiarr, m.npg, pk.lp);
+            ev = EV_PROP_START;        // no peel-off of the direct light (the sky background)
+            break;
+          }
           if (iphot < P.npacc) {            // disk accretion, newdisktherm_5_fuv.f90:238-287
             const int idust2 = pk.accretion_emission(P);
             if (idust2 < 0) { status = 3; ev = EV_FINISH; break; }

@@ -365,6 +365,38 @@ struct Packet {
     if (ispotph == 0) nub = (m.iplanckst == 0) ? atmosfreq() : bbfreq(m.tstar);
     else nub = bbfreq(m.tshock);
   }
+  // External illumination (initpout.f90:1-68): an unpolarised packet on the
+  // sphere of the grid's outer radius (cosb uniform, longitude lp uniform),
+  // heading inward with cos(theta) = -xi in the local frame (isotropic in a
+  // volume), rotated to the grid frame by initp_transform; the frequency
+  // from the ISRF table (rep_isrf.f90: locate in the cdf, then linear in
+  // log10 cdf and log10 nu between the bracketing rows).
+  __device__ void initpout() {
+    sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+    double xran = ran();
+    cosb = 1.0 - 2.0 * xran;
+    sinb = sqrt(1.0 - cosb * cosb);
+    xran = ran();
+    cost = -xran;
+    sint = sqrt(1.0 - cost * cost);
+    xran = ran();
+    phi = R2P * xran;
+    cosp = cos(phi);
+    sinp = sin(phi);
+    xran = ran();
+    lp = R2P * xran;
+    initp_transform();
+    xran = ran();
+    const int n = m.nisrf;
+    int i = locate(m.isrf_cdf, n, xran);
+    if (i == n) i = n - 1;
+    if (i == 0) i = 1;
+    const double* lc = m.isrf_logcdf;
+    const double* lf = m.isrf_logfreq;
+    const double lg = lf[i - 1] + (log10(xran) - lc[i - 1]) / (lc[i] - lc[i - 1]) * (lf[i] - lf[i - 1]);
+    nub = pow(10.0, lg);
+  }
+
   __device__ void initpabs() {                     // initpabs.f90:1-44
     sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
     cosb = zp / rtot;

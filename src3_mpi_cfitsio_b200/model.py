@@ -809,3 +809,53 @@ def batch_model(w: Workload) -> Model:
     m = Model(w)
     m.config["output_imcube"] = 0
     return m
+
+
+def isrf_table(nisrf: int = 200, lmin_um: float = 0.0912, lmax_um: float = 1000.0, av: float = 0.0,
+               kext=None) -> np.ndarray:
+    """The external-illumination sampling table the engine takes
+    (mcrt_tables.isrf, Fortran (nisrf, 3): cdf, log10 cdf, log10 nu [eV]),
+    built by the steps of isrf_cdf.f90:67-212: nisrf wavelengths log-spaced
+    over (lmin, lmax], frequencies ascending, the spectrum per unit
+    frequency times exp(-kappa/kappa_V/1.086 * Av), the trapezoid cumulative,
+    normalised, and the first row as that routine leaves it (cdf 0, log cdf
+    -99, log nu 0).  The spectrum is a synthetic stand-in for the reference's
+    tabulated one (not present here): the three diluted blackbodies of the
+    stellar interstellar radiation field of Mathis, Mezger & Panagia (1983),
+    W = 1e-14, 1e-13, 4e-13 at T = 7500, 4000, 3000 K.  `kext(lam_um)`: the
+    extinction curve relative to V for Av > 0."""
+    c = 2.99792458e14                                 # um/s
+    h_k = 4.799243e-11                                # h/k [K s]
+    freq = np.empty(nisrf)
+    for i in range(1, nisrf + 1):
+        lam = lmin_um * (lmax_um / lmin_um) ** (i / nisrf)
+        freq[nisrf - i] = c / lam
+    def bnu(nu, T):
+        x = h_k * nu / T
+        return nu ** 3 / np.expm1(x)
+    pdf = sum(W * bnu(freq, T) for W, T in ((1e-14, 7500.0), (1e-13, 4000.0), (4e-13, 3000.0)))
+    if av > 0.0:
+        pdf = pdf * np.exp(-np.asarray(kext(c / freq)) / 1.086 * av)
+    cdf = np.zeros(nisrf)
+    for i in range(1, nisrf):
+        cdf[i] = cdf[i - 1] + 0.5 * (pdf[i] + pdf[i - 1]) * (freq[i] - freq[i - 1])
+    logcdf = np.zeros(nisrf)
+    logfreq = np.zeros(nisrf)
+    cdf[1:] = cdf[1:] / cdf[-1]
+    cdf[0] = 0.0
+    logcdf[0] = -99.0
+    logfreq[0] = 0.0
+    logcdf[1:] = np.log10(cdf[1:])
+    logfreq[1:] = np.log10(freq[1:] * 1.2398 / c)
+    return np.concatenate([cdf, logcdf, logfreq])
+
+
+def with_isrf(m: Model, frac: float = 0.2, **kw) -> Model:
+    """External-illumination packets (isrf_frac): a fraction `frac` of every
+    iteration's packets enters from the outer sphere with the ISRF spectrum
+    of ``isrf_table``."""
+    t = isrf_table(**kw)
+    m.tables["isrf"] = t
+    m.tables["nisrf"] = t.size // 3
+    m.config["isrf_frac"] = frac
+    return m

@@ -36,7 +36,7 @@ def test_struct_sizes_match_header():
     from src3_mpi_cfitsio_b200 import abi
     assert ctypes.sizeof(abi.Config) == 24 * 4 + 23 * 8
     assert ctypes.sizeof(abi.Grid) == 18 * 8
-    assert ctypes.sizeof(abi.Tables) == 25 * 8 + 2 * 4
+    assert ctypes.sizeof(abi.Tables) == 26 * 8 + 4 * 4
     assert ctypes.sizeof(abi.Tallies) == (4 + 2 + 10 + 9 + 4 + 2) * 8
     assert ctypes.sizeof(abi.PacketLog) == 8 + 12 * 4 + 10 * 8
 

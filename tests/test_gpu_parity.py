@@ -554,3 +554,51 @@ def test_adjoint_chunks_sum_to_one_pass(warm_small):
     tol = 1e-9 * np.abs(g1).max()
     assert np.allclose(g1, g2, rtol=1e-9, atol=tol) and np.allclose(g3, g4, rtol=1e-9, atol=tol)
     assert L3 < L1
+
+
+@pytest.fixture(scope="module")
+def isrf_small():
+    return model.with_isrf(model.with_diffusion(model.warm(model.small_2d())), 0.3)
+
+
+@pytest.mark.parametrize("ipeel", [0, 1])
+def test_isrf_packets_event_for_event(isrf_small, oracle_mod, ipeel):
+    """External-illumination packets (30 % of the iteration) follow the
+    oracle packet by packet; diffusion is on, so only packets that reach a
+    diffusion cell may part company."""
+    m = isrf_small
+    n = 4000
+    eng = _engine(m)
+    eng.set_schedule("warp")
+    eng.enable_packet_log(n)
+    eng.reset_tallies()
+    eng.run(n, ipeel=ipeel)
+    g = abi.packet_log_to_numpy(eng.packet_log(n))
+    eng.close()
+    _, lo = oracle_mod.run(abi.Bundle(m), n, ipeel=ipeel, nlog=n)
+    o = abi.packet_log_to_numpy(lo)
+    nodiff = (g["pad"] == 0) & (o["pad"] == 0)
+    same, exact = _same_packets(g, o)
+    ext = np.arange(1, n + 1) > n - int(round(0.3 * n))
+    assert (o["i_orig"][ext] == 5).mean() > 0.3               # external packets ran
+    assert exact[nodiff & ext].mean() >= 0.995 and exact[nodiff].mean() >= 0.995
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_isrf_wave_matches_warp_bitwise(isrf_small, precision):
+    m = model.with_isrf(model.warm(model.small_2d()), 0.3)
+    n = 3000
+    logs = []
+    for sched in ("warp", "wave"):
+        eng = _engine(m, precision=precision)
+        eng.set_schedule(sched)
+        if sched == "wave":
+            eng.set_wave_pool(512)
+        eng.enable_packet_log(n)
+        eng.reset_tallies()
+        eng.run(n, ipeel=1)
+        logs.append(abi.packet_log_to_numpy(eng.packet_log(n)))
+        eng.close()
+    for k in logs[0]:
+        assert np.array_equal(logs[0][k], logs[1][k]), k
+

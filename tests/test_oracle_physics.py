@@ -258,3 +258,31 @@ def test_setemiss_oracle_smooths_gas_planck_means():
             out[i - 1] = kp[lo - 1:hi].sum() / (hi - lo + 1)
         kp = out
     assert np.allclose(b["kappap"][nT:], kp, rtol=1e-13, atol=0)
+
+
+def test_isrf_packets_sample_the_table_and_are_not_binned_unscattered(oracle_mod):
+    """External illumination (initpout.f90 + rep_isrf.f90): in an empty grid
+    every packet crosses unscattered, so its exit frequency is its emitted
+    one and nothing is binned (unscattered external light is the sky
+    background, not part of the SED).  The frequencies follow the table:
+    mapped back through its log-log interpolation they are uniform on
+    (cdf_2, 1)."""
+    m = model.with_isrf(model.warm(model.small_2d()), 1.0)
+    m.grid["densarr"] = np.zeros_like(m.grid["densarr"])
+    n = 20000
+    tal, lo = oracle_mod.run(abi.Bundle(m), n, ipeel=1, nlog=n, threads=4)
+    g = abi.packet_log_to_numpy(lo)
+    c = tal.counters()
+    assert c["packets"] == n and c["exited"] == n and c["interactions"] == 0
+    assert np.all(g["i_orig"] == 5) and np.all(g["nscat"] == 0)
+    assert tal["si"].sum() == 0 and tal["ti"].sum() == 0 and tal["image_m_i"].sum() == 0
+    t = m.tables["isrf"]
+    k = t.size // 3
+    cdf, lcdf, lfr = t[:k], t[k:2 * k], t[2 * k:]
+    lnu = np.log10(g["nub"])
+    sel = lnu >= lfr[1]
+    i = np.clip(np.searchsorted(lfr[1:], lnu[sel], side="right"), 1, k - 2)    # rows i..i+1 (0-based, >= 1)
+    x = 10.0 ** (lcdf[i] + (lnu[sel] - lfr[i]) / (lfr[i + 1] - lfr[i]) * (lcdf[i + 1] - lcdf[i]))
+    u = np.sort((x - cdf[1]) / (1.0 - cdf[1]))
+    ks = np.max(np.abs(u - (np.arange(1, u.size + 1) - 0.5) / u.size))
+    assert sel.mean() > 0.99 and ks < 1.63 / np.sqrt(u.size) + 1e-3
