@@ -229,7 +229,7 @@ int mcrt_set_precision(mcrt_ctx *ctx, int32_t mode);
  * its batch size (1..32): for the warp schedule, how many lanes of a warp
  * must wait for an event before the warp stops stepping rays to run them
  * (default 16); for the wavefront schedule, how many lanes of a walk warp
- * must be idle before it takes new walks from the queue (default 8).  Every
+ * must be idle before it takes new walks from the queue (default 4).  Every
  * packet's history, and so every tally up to the order of floating-point
  * additions, is independent of either choice.  No reference counterpart
  * (the reference runs one packet per MPI rank thread). */

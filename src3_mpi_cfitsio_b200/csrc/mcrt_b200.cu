@@ -66,7 +66,7 @@ struct mcrt_ctx {
   int precision = MCRT_PREC_FP64;
   int schedule = MCRT_SCHED_WAVE;
   int event_batch = 16;
-  int wave_batch = 8;
+  int wave_batch = 4;
   // wavefront pool
   int64_t wave_pool = 1 << 21;
   int64_t wave_jobs = 0;              // peel-off job queue capacity asked for (0: default)

@@ -230,10 +230,10 @@ class Engine:
         lanes, batched events) or "wave" (walk / event kernels over a pool of
         in-flight packets).  `event_batch`: warp schedule -- lanes waiting
         before events run (default 16); wave -- idle lanes before a walk
-        warp takes new walks (default 8)."""
+        warp takes new walks (default 4)."""
         mode = {"packet": 0, "warp": 1, "wave": 2}[schedule]
         if event_batch is None:
-            event_batch = 8 if schedule == "wave" else 16
+            event_batch = 4 if schedule == "wave" else 16
         self._check(self.lib.mcrt_set_schedule(self.ctx, mode, event_batch))
         self.schedule = schedule
 
