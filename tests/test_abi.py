@@ -84,3 +84,30 @@ def test_setemiss_rejects_bad_tables_without_a_gpu():
         setemiss(nud, np.ones(3), np.zeros(3), [3])
     with pytest.raises(MCRTError, match="nT"):
         setemiss(np.array([2.0, 1.0]), np.ones(2), np.zeros(2), [2], nT=10)
+
+
+def test_model_density_and_batch_refuse_bad_input_without_a_gpu():
+    """mcrt_model_density checks its walls and parameters, and
+    mcrt_batch_create its context list, before any CUDA call."""
+    import ctypes as C
+    from src3_mpi_cfitsio_b200 import abi, model
+    from src3_mpi_cfitsio_b200.engine import density_params, load_library
+    lib = load_library()
+    m = model.small_2d()
+    p = density_params(m.w)
+    r = np.ascontiguousarray(m.grid["rarr"][::-1])           # decreasing walls
+    t = np.ascontiguousarray(m.grid["thetarr"])
+    out = np.zeros(m.w.nrg * m.w.ntg * m.w.npg * 10)
+    vc = np.zeros(m.w.nrg * m.w.ntg * m.w.npg)
+    D = C.POINTER(C.c_double)
+    rc = lib.mcrt_model_density(0, C.byref(p), m.w.nrg, m.w.ntg, m.w.npg, r.ctypes.data_as(D), t.ctypes.data_as(D),
+                                None, out.ctypes.data_as(D), vc.ctypes.data_as(D), None)
+    assert rc == 1 and b"rarr" in lib.mcrt_last_error(None)
+    p.thet1_deg = 95.0
+    rc = lib.mcrt_model_density(0, C.byref(p), m.w.nrg, m.w.ntg, m.w.npg, t.ctypes.data_as(D), t.ctypes.data_as(D),
+                                None, out.ctypes.data_as(D), vc.ctypes.data_as(D), None)
+    assert rc == 1 and b"parameters" in lib.mcrt_last_error(None)
+    h = C.c_void_p()
+    assert lib.mcrt_batch_create(None, 2, C.byref(h)) == 1 and not h.value
+    arr = (C.c_void_p * 2)(None, None)
+    assert lib.mcrt_batch_create(arr, 2, C.byref(h)) == 1 and not h.value
