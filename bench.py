@@ -18,6 +18,23 @@ e2e   : the same through the public C ABI with host buffers: grid upload
 ``--impl reference`` times the CPU restatement of the reference's packet
 loop (the oracle; the Fortran itself cannot be built here) on all host
 cores for a bounded sample of the same workload.
+
+Further keys of the line, each measured once after the timed steps:
+
+* ``roofline`` (the walk kernel against HBM) and ``roofline_compute``
+  (against the FP64 rate);
+* the FP64 build and the plain per-thread FP64 path (``fp64_value``,
+  ``fp64_plain``);
+* the peeled imaging iteration and the mixed-vs-FP64 errors;
+* ``gradient``: the path-replay adjoint of the peeled SED and images;
+* ``clumpy_3d``: the 3-D clumpy model with tabulated Mueller matrices,
+  peeled, on a sample of its 1e9-packet run;
+* ``setemiss``: the emission tables built on the GPU;
+* ``batch``: the 64-model sweep, sharded over the ranks under torchrun;
+* ``cpu_baseline``.
+
+Flags switch the sections off (``--grad-packets 0``, ``--clumpy-packets 0``,
+``--batch-models 0``, ``--no-compare``, ``--no-cpu-baseline``).
 """
 from __future__ import annotations
 
