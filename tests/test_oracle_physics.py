@@ -286,3 +286,35 @@ def test_isrf_packets_sample_the_table_and_are_not_binned_unscattered(oracle_mod
     u = np.sort((x - cdf[1]) / (1.0 - cdf[1]))
     ks = np.max(np.abs(u - (np.arange(1, u.size + 1) - 0.5) / u.size))
     assert sel.mean() > 0.99 and ks < 1.63 / np.sqrt(u.size) + 1e-3
+
+
+def test_sweep_workloads_follow_the_configured_ranges():
+    """The batched sweep's models: nr 50-200, ntheta 49-199 (odd wall count),
+    nphi 1-32 cells, Mdisk in 1e-4..0.1 Msun, Mdot in 1e-7..1e-5 Msun/yr,
+    cavity 5-40 deg, 60-140 wavelengths; seeded, so repeatable."""
+    ws = model.batch_workloads(64)
+    assert len(ws) == 64
+    for w in ws:
+        assert 50 <= w.nrg - 1 <= 200 and 49 <= w.ntg <= 199 and w.ntg % 2 == 1 and 1 <= w.npg - 1 <= 32
+        assert 1e-4 <= w.massd <= 0.1 and 1e-7 <= w.rate <= 1e-5 and 5.0 <= w.thet1_deg <= 40.0
+        assert 60 <= w.nlambda <= 140
+    again = model.batch_workloads(64)
+    assert all(a == b for a, b in zip(ws, again))
+    assert len({(w.nrg, w.ntg, w.npg) for w in ws}) > 50            # uneven grids
+
+
+def test_isrf_table_has_the_reference_layout():
+    """isrf_table: a normalised non-decreasing cdf over ascending
+    frequencies, log10 columns consistent with it, and the first row as
+    isrf_cdf.f90 leaves it (cdf 0, log cdf -99, log nu 0)."""
+    t = model.isrf_table()
+    k = t.size // 3
+    cdf, lcdf, lfr = t[:k], t[k:2 * k], t[2 * k:]
+    assert k == 200 and cdf[0] == 0.0 and lcdf[0] == -99.0 and lfr[0] == 0.0
+    assert np.all(np.diff(cdf) >= 0) and cdf[-1] == 1.0
+    assert np.allclose(lcdf[1:], np.log10(cdf[1:])) and np.all(np.diff(lfr[1:]) > 0)
+    # wavelengths lmin (lmax/lmin)^(i/200), i = 1..200 (the loop of
+    # isrf_cdf.f90 starts at i = 1), so the top frequency sits one step
+    # below 1.2398/lmin eV
+    top = 1.2398 / (0.0912 * (1000.0 / 0.0912) ** (1.0 / 200))
+    assert abs(10 ** lfr[-1] / top - 1.0) < 1e-9 and 10 ** lfr[1] > 1.2398 / 1000.0
