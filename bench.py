@@ -114,11 +114,13 @@ class Clocks:
 
 
 def build_model(args):
-    """The 2-D workload with the reference's default diffusion treatment of
-    the optically thick disk interior (DIFFUSION=YES, tts_mod_5.f90:33)."""
+    """The 2-D workload at its converged Lucy temperature (the state a Lucy
+    sequence settles in; committed with the package), with the reference's
+    default diffusion treatment of the optically thick disk interior
+    (DIFFUSION=YES, tts_mod_5.f90:33).  Every arm -- the GPU steps, the
+    CPU baseline and the reference arm -- starts from this same state."""
     from src3_mpi_cfitsio_b200 import model
-    m = model.warm(model.reference_2d())
-    return model.with_diffusion(m)
+    return model.reference_2d_converged()
 
 
 def algorithmic_bytes(c: dict) -> float:
@@ -514,58 +516,88 @@ def run_ours(args, rank, world):
         **extra,
     )
     if rank == 0 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(args, m)
+        out["cpu_baseline"] = cpu_baseline(args)      # a pristine model: the state the GPU steps started from
     eng.close()
     return out
 
 
+def _cpu_step(b, n, it, cores, ipeel):
+    """One CPU Lucy step on the oracle: the packet loop over n packets, then
+    tfinal on its tallies (timed, not applied: every step sees the same
+    temperature).  Returns seconds."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+    tal, _ = oracle.run(b, n, ipeel=ipeel, threads=cores, iteration=it, images=bool(ipeel))
+    oracle.tfinal(b, tal["dtauabs"], n, it, b.tdave0)
+    return time.perf_counter() - t0
+
+
+def _cpu_setup():
+    """The oracle built for this host (-march=native, FMA contraction still
+    off) and the host description."""
+    from oracle import oracle
+    oracle.use_native()
+    oracle.load()
+    return {"cpu_model": oracle.cpu_model(), "build": "g++ -O3 -march=native -ffp-contract=off (oracle/Makefile native)"}
+
+
 def cpu_baseline(args, m=None, sample=None):
-    """The oracle (CPU restatement of the reference loop) on all host cores."""
+    """The oracle (CPU restatement of the reference loop) on all host cores,
+    on the state the GPU arm starts from, and on one core."""
+    import numpy as np
     from oracle import oracle
     from src3_mpi_cfitsio_b200 import abi
+    host = _cpu_setup()
     if m is None:
         m = build_model(args)
     b = abi.Bundle(m)
+    b.tdave0 = np.asarray(m.grid["tdust"], dtype=np.float64).copy()
     cores = os.cpu_count() or 1
     n = sample or args.cpu_sample
-    oracle.run(b, min(n, 2000), ipeel=args.ipeel, threads=cores)      # warm caches
-    t0 = time.perf_counter()
-    tal, _ = oracle.run(b, n, ipeel=args.ipeel, threads=cores, iteration=2)
-    dt = time.perf_counter() - t0
+    _cpu_step(b, min(n, 20000), 1, cores, args.ipeel)                  # warm caches
+    dt = _cpu_step(b, n, 2, cores, args.ipeel)
+    n1 = max(n // 20, 1000)
+    dt1 = _cpu_step(b, n1, 2, 1, args.ipeel)
     # the emission tables (setemiss) of the model's 8 dust species on the
     # same host threads, beside the GPU build in the "setemiss" key
     t0 = time.perf_counter()
     oracle.setemiss(m.tables["nudust"], m.tables["kappad"], m.tables["adust"], m.tables["nlambda"], threads=cores)
     st = time.perf_counter() - t0
     return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} packets of one Lucy iteration of the same model, {cores} host threads",
+            "sample": f"{n} packets of one Lucy iteration (packet loop + tfinal) of the same model at the same "
+                      f"converged temperature, {cores} host threads",
+            "packets_per_s_one_core": n1 / dt1, **host,
             "setemiss_8_species_ms": 1e3 * st}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU restatement of the reference's packet loop
+    (the Fortran + MPI code cannot be built here) on all host cores, each
+    step a bounded sample of the same Lucy iteration at the same converged
+    temperature as the GPU arm."""
     if rank != 0:
         return None
-    from oracle import oracle
+    import numpy as np
     from src3_mpi_cfitsio_b200 import abi
+    host = _cpu_setup()
     m = build_model(args)
     b = abi.Bundle(m)
+    b.tdave0 = np.asarray(m.grid["tdust"], dtype=np.float64).copy()
     cores = os.cpu_count() or 1
     n = args.cpu_sample
     for w in range(args.warmup):
-        oracle.run(b, min(n, 5000), ipeel=args.ipeel, threads=cores, iteration=w + 1)
-    times = []
-    for s in range(args.steps):
-        t0 = time.perf_counter()
-        oracle.run(b, n, ipeel=args.ipeel, threads=cores, iteration=args.warmup + s + 1)
-        times.append(time.perf_counter() - t0)
+        _cpu_step(b, max(n // 10, 1000), w + 1, cores, args.ipeel)
+    times = [_cpu_step(b, n, args.warmup + s + 1, cores, args.ipeel) for s in range(args.steps)]
     v = n * args.steps / sum(times)
     return dict(metric=METRIC, value=v, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=1e3 * sum(times) / args.steps, higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
-                config={"workload": "2-D disk+envelope+cavity, nr=100 ntheta=99 nphi=1, Lucy iteration",
-                        "packets_per_step": n, "peel_off": bool(args.ipeel)},
+                config={"workload": "2-D disk+envelope+cavity (nr=100, ntheta=99, nphi=1), one Lucy iteration "
+                                    "(packet loop + tfinal) at the converged temperature, diffusion on",
+                        "packets_per_step": n, "peel_off": bool(args.ipeel), "precision": "fp64"},
                 cpu_baseline={"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                              "sample": f"{n} packets per step, {cores} host threads"},
+                              "sample": f"{n} packets per step (packet loop + tfinal), {cores} host threads",
+                              **host},
                 e2e={"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
 
 
@@ -580,7 +612,8 @@ def main():
     ap.add_argument("--packets", type=int, default=100_000_000)
     ap.add_argument("--peel-packets", type=int, default=10_000_000)
     ap.add_argument("--ipeel", type=int, default=0)
-    ap.add_argument("--cpu-sample", type=int, default=20000)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000,
+                    help="packets per CPU step (reference arm) and of the cpu_baseline sample")
     ap.add_argument("--grad-packets", type=int, default=10_000_000,
                     help="packets of the adjoint-gradient timing (0: skip)")
     ap.add_argument("--plain-packets", type=int, default=5_000_000,
@@ -594,9 +627,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     # 706 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
-    # launch over 2,097,152 walks (profiles/wave_walk_wave_event_mixed_2d_8e6.md)
+    # launch over 2,097,152 walks, from an ncu capture of the 8e6-packet case
     ap.add_argument("--traffic-per-walk", type=float, default=705.9,
-                    help="DRAM bytes per walk of the wave_walk kernel from an ncu capture (profiles/)")
+                    help="DRAM bytes per walk of the wave_walk kernel from an ncu capture")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

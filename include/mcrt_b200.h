@@ -341,9 +341,11 @@ int mcrt_update_temperature(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
  * mcrt_update_temperature (sig to summation order), but the scratch lives in
  * a fixed 12 MiB device array inside the library, so models are limited to
  * nrg*ntg*npg <= 524288 cells (larger ones return MCRT_ERR_ARG).  The first
- * call on each device looks the array up and should come before any stream
- * capture.  All calls in the process share the array: calls that overlap on
- * a GPU (two contexts on one device, or two host threads) race. */
+ * call on each context looks the array's device address up (with the
+ * context's device current; a context created after a device reset looks
+ * it up again) and should come before any stream capture.  All calls in the
+ * process share the array: calls that overlap on a GPU (two contexts on one
+ * device, or two host threads) race. */
 int mcrt_update_temperature_noalloc(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
                                     double *tdave, int32_t *converge, double *sig);
 

@@ -18,6 +18,7 @@ from src3_mpi_cfitsio_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libmcrt_oracle.so")
 _lib = None
+_native = False
 
 
 def build() -> str:
@@ -25,12 +26,50 @@ def build() -> str:
     return LIB
 
 
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def native_lib() -> str:
+    """The oracle built with -march=native for THIS host (timing only; the
+    arithmetic is the same: FMA contraction stays off).  The file name
+    carries a hash of the host's CPU model and flags, so a copy built on
+    another machine is never loaded here."""
+    import hashlib
+    flags = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "")
+    except OSError:
+        pass
+    tag = hashlib.sha1((cpu_model() + flags).encode()).hexdigest()[:12]
+    out = os.path.join(HERE, "_build", f"libmcrt_oracle_native_{tag}.so")
+    if not os.path.exists(out):
+        subprocess.run(["make", "-s", "-C", HERE, "native", f"NATIVE_OUT={out}"], check=True)
+    return out
+
+
+def use_native() -> None:
+    """Switch this module to the host-native build (bench.py's CPU legs)."""
+    global _lib, _native
+    if not _native:
+        _lib = None
+        _native = True
+
+
 def load():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
+        if not _native and not os.path.exists(LIB):
             build()
-        lib = C.CDLL(LIB)
+        lib = C.CDLL(native_lib() if _native else LIB)
         lib.oracle_run.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
                                    C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                    C.c_int32, C.c_int32, C.c_int32, C.c_int32,

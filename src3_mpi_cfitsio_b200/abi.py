@@ -1,7 +1,7 @@
 """ctypes mirror of include/mcrt_b200.h.
 
 The structs here are byte-for-byte the C structs of the engine's C ABI (the
-boundary a Fortran ``iso_c_binding`` interface binds, see INTEGRATION.md).
+boundary a Fortran ``iso_c_binding`` interface binds).
 ``Bundle`` keeps the numpy arrays alive for as long as a struct points at
 them.
 """

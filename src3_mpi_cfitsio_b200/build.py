@@ -31,21 +31,26 @@ def build(verbose: bool = False, ptxas_info: bool = False, out: str = LIB, defin
     (compile-time tuning knobs of the kernels)."""
     libdir = os.path.dirname(out)
     os.makedirs(libdir, exist_ok=True)
-    objs = []
-    for src, extra in UNITS:
+    objs, procs = [], []
+    for src, extra in UNITS:          # the translation units compile in parallel
         obj = os.path.join(libdir, src.replace(".cu", ".o"))
         cmd = [nvcc(), *ARCH, *COMMON, *[f"-D{d}" for d in defines], *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError(f"nvcc failed on {src}")
-        if ptxas_info or verbose:
-            sys.stderr.write(r.stderr)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(obj)
+    failed = []
+    for src, p in procs:
+        out_s, err_s = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out_s + err_s)
+            failed.append(src)
+        elif ptxas_info or verbose:
+            sys.stderr.write(err_s)
+    if failed:
+        raise RuntimeError(f"nvcc failed on {', '.join(failed)}")
     cmd = [nvcc(), *ARCH, "-shared", "-o", out, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

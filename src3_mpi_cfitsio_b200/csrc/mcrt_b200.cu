@@ -107,6 +107,8 @@ struct mcrt_ctx {
   // model buffers
   double *d_walls = nullptr;
   CellRec *d_cells = nullptr;
+  CellRecF *d_cellsf = nullptr;       // FP32 cells of the mixed walk
+  unsigned char *d_walk32 = nullptr;  // FP32 walk tables: tcone | pplane | wall64
   double *d_tdust = nullptr, *d_vcell = nullptr;
   double *d_tdust0 = nullptr;         // tdust at the start of the iteration (read by the transport)
   double last_nphot_diff = 1.0;
@@ -136,6 +138,7 @@ struct mcrt_ctx {
   int64_t off_Tint = 0, off_kappap = 0;   // offsets of Tint/kappap in d_tabs (tfinal)
   std::vector<double> h_rarr;
   std::vector<int32_t> species_grid;  // per species: first species with a bit-identical wavelength column
+  double* noalloc_scratch = nullptr;   // device address of g_tfinal_scratch (mcrt_update_temperature_noalloc)
 };
 
 namespace {
@@ -602,6 +605,37 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     for (int i = 0; i < nrg - 1; ++i)
       if (!(g->hdisk[i] >= 0.0) || !(g->ravearr[i] > 0.0)) return fail(ctx, MCRT_ERR_ARG, "ravearr/hdisk must be positive");
   }
+  // FP32 walk tables (mixed build): cells with FP32 densities; per theta
+  // wall (mu, mu^2) with the plane (tan2arr = -1) and the poles (tan2arr =
+  // 0, skipped by thetaface.f90) flagged; per phi wall the plane (A, B);
+  // per radial wall the FP64-root flag of walls next to thin cells.
+  std::vector<CellRecF> cellsf(ncell);
+  for (int64_t k = 0; k < ncell; ++k) {
+    for (int i = 0; i < kMaxComp; ++i) cellsf[k].rho[i] = (float)cells[k].rho[i];
+    cellsf[k].meta = cells[k].meta;
+  }
+  std::vector<float2> tcone(ntg + 1), pplane(npg + 1);
+  for (int j = 0; j <= ntg; ++j) {
+    const double mu = j < ntg ? g->costarr[j] : g->costarr[ntg - 1] - 1.0;
+    const double t2 = j < ntg ? g->tan2arr[j] : 0.0;
+    tcone[j].x = (float)mu;
+    tcone[j].y = t2 < 0.0 ? -1.0f : (t2 == 0.0 ? 2.0f : (float)(mu * mu));
+  }
+  for (int j = 0; j <= npg; ++j) {
+    pplane[j].x = (float)(j < npg ? g->aarr[j] : g->aarr[npg - 1]);
+    pplane[j].y = (float)(j < npg ? g->barr[j] : g->barr[npg - 1]);
+  }
+  const size_t w32_cone = 0, w32_plane = (size_t)(ntg + 1) * sizeof(float2);
+  const size_t w32_flag = w32_plane + (size_t)(npg + 1) * sizeof(float2);
+  std::vector<unsigned char> walk32(w32_flag + (size_t)(nrg + 1), 0);
+  std::memcpy(walk32.data() + w32_cone, tcone.data(), tcone.size() * sizeof(float2));
+  std::memcpy(walk32.data() + w32_plane, pplane.data(), pplane.size() * sizeof(float2));
+  for (int w = 0; w < nrg; ++w) {
+    bool thin = false;
+    if (w > 0 && g->rarr[w] - g->rarr[w - 1] < kThinWall * g->rarr[w]) thin = true;
+    if (w + 1 < nrg && g->rarr[w + 1] - g->rarr[w] < kThinWall * g->rarr[w + 1]) thin = true;
+    walk32[w32_flag + w] = thin ? 1 : 0;
+  }
   const std::vector<double> zeros(nrg > 1 ? nrg - 1 : 1, 0.0);
   addp(acc ? g->ravearr : zeros.data(), nrg - 1, 0.0);
   addp(acc ? g->Ldint : zeros.data(), nrg - 1, 1.0);
@@ -612,6 +646,8 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     int rc;
     if ((rc = dalloc(ctx, &ctx->d_walls, walls.size()))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_cells, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_cellsf, ncell))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_walk32, walk32.size()))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_tdust, ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_tdust0, ncell))) return rc;
     if ((rc = dalloc(ctx, &ctx->d_vcell, ncell))) return rc;
@@ -621,6 +657,8 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   }
   CK(cudaMemcpyAsync(ctx->d_walls, walls.data(), walls.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_cells, cells.data(), ncell * sizeof(CellRec), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_cellsf, cellsf.data(), ncell * sizeof(CellRecF), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_walk32, walk32.data(), walk32.size(), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_tdust, g->tdust, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_tdust0, g->tdust, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_vcell, g->vcell, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
@@ -643,6 +681,10 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   m.Ldint = w; w += nrg;
   m.hdisk = w;
   m.cells = ctx->d_cells;
+  m.cellsf = ctx->d_cellsf;
+  m.tcone = reinterpret_cast<const float2*>(ctx->d_walk32 + w32_cone);
+  m.pplane = reinterpret_cast<const float2*>(ctx->d_walk32 + w32_plane);
+  m.wall64 = ctx->d_walk32 + w32_flag;
   m.tdust = ctx->d_tdust0;
   m.vcell = ctx->d_vcell;
   m.nslot = (int)slot_species.size();
@@ -1534,7 +1576,6 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
 // be made while a stream is being captured.
 int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* tdave, int32_t* converge,
                                     double* sig) {
-  static double* scratch_of_device[64] = {};
   if (!ctx || !tdave || !converge) return MCRT_ERR_ARG;
   if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
   if (nphot < 1) return fail(ctx, MCRT_ERR_ARG, "nphot must be positive");
@@ -1543,13 +1584,12 @@ int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, 
   if (nc > kNoAllocMaxCells)
     return fail(ctx, MCRT_ERR_ARG, "mcrt_update_temperature_noalloc: %lld cells exceed its fixed scratch of %lld cells",
                 (long long)nc, (long long)kNoAllocMaxCells);
-  if (ctx->device < 0 || ctx->device >= 64) return fail(ctx, MCRT_ERR_ARG, "device index out of range");
   CK(cudaSetDevice(ctx->device));
-  double* base = scratch_of_device[ctx->device];
-  if (!base) {
-    CK(cudaGetSymbolAddress((void**)&base, g_tfinal_scratch));
-    scratch_of_device[ctx->device] = base;
-  }
+  // the scratch array's device address, looked up once per context with the
+  // context's device current (a new context, e.g. after a device reset,
+  // looks it up again)
+  if (!ctx->noalloc_scratch) CK(cudaGetSymbolAddress((void**)&ctx->noalloc_scratch, g_tfinal_scratch));
+  double* base = ctx->noalloc_scratch;
   double* d_told = base;
   double* d_tnew = base + kNoAllocMaxCells;
   double* d_res = base + 2 * kNoAllocMaxCells;

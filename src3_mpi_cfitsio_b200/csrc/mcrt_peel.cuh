@@ -69,6 +69,9 @@ struct PeelLane {
     const double coste = __ldg(m.coste + dir - 1), sinte = __ldg(m.sinte + dir - 1);
     ray.x = J.x; ray.y = J.y; ray.z = J.z; ray.rs = J.rs; ray.rt = J.rt;
     ray.r = J.r; ray.t = J.t; ray.p = J.p; ray.onw = (J.bits & 1u) != 0; ray.peel = true; ray.tsum = 0.0;
+#ifdef MCRT_MIXED
+    ray.qready = false;
+#endif
     ray.vx = sinte * cospe;
     ray.vy = sinte * sinpe;
     ray.vz = coste;
@@ -88,6 +91,55 @@ struct PeelLane {
   // one crossing (peeloff_3d_2_test.f90:133-214); sets state 1 (bin) or 2
   // (done, no bin).  In the adjoint re-walk (state 5) the same crossings
   // scatter -C * tau per (cell, component) and the walk ends in state 2.
+#ifdef MCRT_MIXED
+  // Mixed build: the FP32 walk (QRay).  The bin reads the start point: the
+  // image coordinates are projections along the peel-off direction.
+  __device__ __forceinline__ void step(const LaunchParams& P) {
+    const DevModel& m = pk.m;
+    Ray& R = ray;
+    QRay& g = R.g;
+    if (!R.qready) {
+      for (int s = 0; s < kJobSlots && s < m.nslot; ++s) pk.kf(s) = (float)J.kapd[s];
+      pk.qbegin(g, R.x, R.y, R.z, R.vx, R.vy, R.vz, R.r, R.t, R.p);
+      R.qready = true;
+    }
+    double qn = g.qr;
+    int d = 0;
+    if (g.qt < qn) { qn = g.qt; d = 1; }
+    if (g.qp < qn) { qn = g.qp; d = 2; }
+    if (!(qn < HUGE_D) || ++steps > 10000000) { state = 2; return; }
+    const float dt = (float)(qn - g.q);
+    const int64_t ci = pk.cidx(R.r, R.t, R.p);
+    const CellRecF c = m.cellsf[ci];
+    float opac = 0.0f;
+    const int n = cell_n(c.meta);
+    for (int k = 0; k < n; ++k) opac = fmaf(pk.kf(cell_slot(c.meta, k)), c.rho[k], opac);
+    R.tsum = R.tsum + (double)(opac * dt);
+    if (R.tsum > 25.0) { state = 2; return; }
+    if (state == 5) {
+      for (int k = 0; k < n; ++k)
+        atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1),
+                  -(adjC * (double)(pk.kf(cell_slot(c.meta, k)) * c.rho[k] * dt)));
+    }
+    g.q = qn;
+    R.onw = true;
+    if (d == 0) {
+      R.r += g.sr;
+    } else if (d == 1) {
+      R.t += g.st;
+    } else {
+      R.p += g.sp;
+      if (R.p == 0) R.p = m.npg - 1;
+      if (R.p == m.npg) R.p = 1;
+    }
+    if (state != 5) ++pk.c_pcross;
+    if (R.r == m.nrg) { state = (state == 5) ? 2 : 1; return; }
+    if (R.r == 0) { state = 2; return; }
+    if (d == 0) pk.qnext_r(g, R.r);
+    else if (d == 1) pk.qnext_t(g, R.t);
+    else pk.qnext_p(g, R.p);
+  }
+#else
   __device__ __forceinline__ void step(const LaunchParams& P) {
     const DevModel& m = pk.m;
     Ray& R = ray;
@@ -122,6 +174,7 @@ struct PeelLane {
     if (R.r == m.nrg) { state = (state == 5) ? 2 : 1; return; }
     if (R.r == 0) { state = 2; return; }
   }
+#endif
 
   // peeloff_3d_2_test.f90:217-345
   __device__ void bin(const LaunchParams& P) {

@@ -41,9 +41,13 @@ enum Ev : int {
 enum PeelCtx : int { PC_DIRECT = 0, PC_SCATTER = 1, PC_ABSORB = 2, PC_ACCRETION = 3 };
 
 struct Ray {
-  double x, y, z, rs, rt, vx, vy, vz, tsum;
+  double x, y, z, rs, rt, vx, vy, vz, tsum;   // mixed build: x..rt = the walk's start point
   int r, t, p;
   bool onw, peel;
+#ifdef MCRT_MIXED
+  bool qready;                                 // g set up for this walk
+  QRay g;
+#endif
 };
 
 struct Lane {
@@ -61,7 +65,7 @@ struct Lane {
   double adjA;                      // replay: summed C of the packet's peel-offs still ahead
   int64_t adj_pos, adj_end;         // replay: the packet's next record
 
-  __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase) : pk(m, t, sbase) {
+  __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase, float* fbase = nullptr) : pk(m, t, sbase, fbase) {
     ev = EV_FETCH;
     status = 0;
     c_pkt = c_int = c_sca = c_geo = c_kil = c_exit = c_star = c_jobs = 0;
@@ -72,11 +76,27 @@ struct Lane {
     ray.r = pk.ir; ray.t = pk.it; ray.p = pk.ip; ray.onw = pk.on_wall; ray.peel = peel;
     ray.tsum = 0.0;
     ray_steps = 0;
+#ifdef MCRT_MIXED
+    ray.qready = false;
+#endif
   }
+#ifdef MCRT_MIXED
+  // The packet at the walk's current point: start + (q - q0) u in FP64.
+  __device__ __forceinline__ void packet_from_ray() {
+    const double d = ray.g.q - ray.g.q0;
+    pk.xp = ray.x + d * ray.vx;
+    pk.yp = ray.y + d * ray.vy;
+    pk.zp = ray.z + d * ray.vz;
+    pk.rsq = pk.xp * pk.xp + pk.yp * pk.yp + pk.zp * pk.zp;
+    pk.rtot = sqrt(pk.rsq);
+    pk.ir = ray.r; pk.it = ray.t; pk.ip = ray.p; pk.on_wall = ray.onw;
+  }
+#else
   __device__ __forceinline__ void packet_from_ray() {
     pk.xp = ray.x; pk.yp = ray.y; pk.zp = ray.z; pk.rsq = ray.rs; pk.rtot = ray.rt;
     pk.ir = ray.r; pk.it = ray.t; pk.ip = ray.p; pk.on_wall = ray.onw;
   }
+#endif
   __device__ __forceinline__ void start_walk() {
     ray_from_packet(false);
     ray.vx = pk.ux; ray.vy = pk.uy; ray.vz = pk.uz;
@@ -109,6 +129,95 @@ struct Lane {
   // kStarEvent the stellar-surface hit ends the step with EV_STAR instead of
   // re-emitting in place, so that the walk needs only the opacity and
   // albedo columns of the species state (kapd, alb).
+#ifdef MCRT_MIXED
+  // Mixed build: one crossing of the FP32 walk (QRay, mcrt_transport.cuh)
+  // with the same outcomes as the FP64 step below.  A ray's peel-off bin
+  // reads the start point: the image coordinates are projections along the
+  // peel-off direction, the same for every point of the ray.
+  template <bool kStarEvent = false>
+  __device__ __forceinline__ void step(const LaunchParams& P) {
+    const DevModel& m = pk.m;
+    Ray& R = ray;
+    QRay& g = R.g;
+    if (!R.qready) {
+      pk.walk_columns();
+      pk.qbegin(g, R.x, R.y, R.z, R.vx, R.vy, R.vz, R.r, R.t, R.p);
+      R.qready = true;
+    }
+    double qn = g.qr;
+    int d = 0;
+    if (g.qt < qn) { qn = g.qt; d = 1; }
+    if (g.qp < qn) { qn = g.qp; d = 2; }
+    if (!(qn < HUGE_D) || ++ray_steps > 50000000) {
+      if (!R.peel) { packet_from_ray(); status = 3; ev = EV_FINISH; }
+      else ev = EV_PEEL_NEXT;
+      return;
+    }
+    const double dt = qn - g.q;
+    const int64_t ci = pk.cidx(R.r, R.t, R.p);
+    const CellRecF c = m.cellsf[ci];
+    float opac, absc;
+    pk.cell_coefs(c, opac, absc);
+    if (!R.peel) {
+      const double dtau = (double)(opac * (float)dt);
+      if (R.tsum + dtau > pk.tau) {
+        const double ds = (pk.tau - R.tsum) / (double)opac;
+        pk.tally_absf(ci, absc, ds);
+        if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)ds);
+        g.q = g.q + ds;
+        R.onw = false;
+        packet_from_ray();
+        ev = EV_AFTER_WALK;
+        return;
+      }
+      pk.tally_absf(ci, absc, dt);
+      if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)dt);
+      R.tsum = R.tsum + dtau;
+    } else {
+      R.tsum = R.tsum + (double)(opac * (float)dt);
+      if (R.tsum > 25.0) { ev = EV_PEEL_NEXT; return; }
+    }
+    g.q = qn;
+    R.onw = true;
+    if (d == 0) {
+      R.r += g.sr;
+    } else if (d == 1) {
+      R.t += g.st;
+    } else {
+      R.p += g.sp;
+      if (R.p == 0) R.p = m.npg - 1;
+      if (R.p == m.npg) R.p = 1;
+    }
+    if (!R.peel) {
+      ++pk.ncross;
+      ++pk.c_cross;
+      if (R.r == m.nrg) { pk.exitflag = 1; packet_from_ray(); ev = EV_EXIT; return; }
+      if (R.r == 0) {                 // star hit: re-emission, tau kept (tauint_3d_2_fuv.f90:184-206)
+        packet_from_ray();
+        if (kStarEvent) { ev = EV_STAR; return; }
+        star_reemit();
+        return;
+      }
+    } else {
+      ++pk.c_pcross;
+      if (R.r == m.nrg) { ev = EV_PEEL_BIN; return; }
+      if (R.r == 0) { ev = EV_PEEL_NEXT; return; }
+    }
+    if (d == 0) pk.qnext_r(g, R.r);
+    else if (d == 1) pk.qnext_t(g, R.t);
+    else pk.qnext_p(g, R.p);
+  }
+
+  // Replay: -A * tau of a walk piece in cell ci, per component (FP32 cell).
+  __device__ __forceinline__ void adjoint_scoref(const LaunchParams& P, int64_t ci, const CellRecF& c, float len) {
+    if (adjA == 0.0) return;
+    const int n = cell_n(c.meta);
+    for (int k = 0; k < n; ++k) {
+      const int id = cell_id(c.meta, k);
+      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(adjA * (double)(pk.kf(cell_slot(c.meta, k)) * c.rho[k] * len)));
+    }
+  }
+#else
   template <bool kStarEvent = false>
   __device__ __forceinline__ void step(const LaunchParams& P) {
     const DevModel& m = pk.m;
@@ -178,6 +287,7 @@ struct Lane {
       if (R.r == 0) { ev = EV_PEEL_NEXT; return; }
     }
   }
+#endif
 
   // ------------------------------------------------------------ adjoint
   // Replay: -A * tau of a walk piece of length len in cell ci, per component.

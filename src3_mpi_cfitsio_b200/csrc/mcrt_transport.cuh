@@ -106,7 +106,36 @@ struct Walls {
   }
 };
 
-// Shared per-thread species state: S[q][slot][tid]
+#ifdef MCRT_MIXED
+// --------------------------------------------------- FP32 cell walk ----
+// The mixed build walks a ray in the closest-approach form: a point of the
+// ray is c + q u, with c the point nearest the origin (c . u = 0) and q the
+// signed distance from it.  Every face of the spherical-polar grid is then a
+// root in q that depends on the ray and the wall only, never on the current
+// position, so the on-wall cancellation of radface/thetaface/phiface
+// (|x|^2 - R^2 -> 0 on the wall just crossed) does not arise:
+//   sphere R:  q = +-sqrt(R^2 - p^2), p^2 = |c|^2 (inward half first);
+//   cone mu:   (c_z + u_z q)^2 = mu^2 (p^2 + q^2) on the nappe sign(z) = sign(mu);
+//   plane A x + B y = 0:  q = -(A c_x + B c_y) / (A u_x + B u_y).
+// Each dimension's next crossing is kept and only the dimension just
+// crossed is solved again, so a crossing costs one sphere root or two cone
+// roots.  The walk state, the cone and plane roots and the opacity sums are
+// FP32; q, p^2 and the sphere roots are FP64 where a wall borders a thin
+// cell (kThinWall), and the cumulative optical depth, its comparison with
+// the sampled tau and the tallies are FP64.
+struct QRay {
+  double q, p2, q0;            // current q, squared impact parameter, q of the walk's start point
+  double qr, qt, qp;           // next crossing per dimension (r, theta, phi); HUGE_D: none
+  float cx, cy, cz, ux, uy, uz, p2f, pabs;
+  int sr, st, sp;              // index step of the pending crossing per dimension
+  bool lzpos;                  // the azimuth grows along the ray (L_z > 0)
+};
+#endif
+
+// Shared per-thread species state: S[q][slot][tid], q = kapd, albedo, g,
+// pl.  Kernels reserve a fifth column of kMaxSlot doubles per thread: the
+// mixed build keeps the FP32 walk columns there (Packet::sfb).
+constexpr int kSpecCols = 5;
 struct SpecState {
   double* base;
   int tid;
@@ -114,7 +143,6 @@ struct SpecState {
   __device__ __forceinline__ double& alb(int s) const { return base[(1 * kMaxSlot + s) * kBlock + tid]; }
   __device__ __forceinline__ double& g(int s) const { return base[(2 * kMaxSlot + s) * kBlock + tid]; }
   __device__ __forceinline__ double& pl(int s) const { return base[(3 * kMaxSlot + s) * kBlock + tid]; }
-  __device__ __forceinline__ double& kap(int s) const { return base[(4 * kMaxSlot + s) * kBlock + tid]; }
 };
 
 enum KapdOrder { KAPD_DISK = 0, KAPD_PROPAGATE = 1, KAPD_TAUINT = 2 };
@@ -133,11 +161,19 @@ struct Packet {
   int nscat, nabsev, ncross, nstar, ndiffev;
   unsigned long long c_cross, c_peel, c_pcross, c_pbin, c_reset;
 
-  __device__ Packet(const DevModel& mm, const DevTallies& tt, double* sbase)
+  // sbase: kSpecCols columns of kMaxSlot doubles per thread (the species
+  // state and, in the mixed build, the FP32 walk columns in the last one);
+  // fbase, if given, holds the FP32 walk columns instead.
+  __device__ Packet(const DevModel& mm, const DevTallies& tt, double* sbase, float* fbase = nullptr)
       : m(mm), T(tt) {
     sp.base = sbase;
     sp.tid = threadIdx.x;
     c_cross = c_peel = c_pcross = c_pbin = c_reset = 0;
+#ifdef MCRT_MIXED
+    sfb = fbase ? fbase : reinterpret_cast<float*>(sbase + 4 * kMaxSlot * kBlock);
+#else
+    (void)fbase;
+#endif
   }
 
   __device__ __forceinline__ double ran() { return rng.ran(); }
@@ -193,7 +229,6 @@ struct Packet {
       sp.alb(s) = alb;
       sp.g(s) = gg;
       sp.pl(s) = pll;
-      sp.kap(s) = kap;
     }
   }
 
@@ -722,6 +757,179 @@ struct Packet {
     if (p == 0) p = m.npg - 1;
     if (p == m.npg) p = 1;
   }
+
+#ifdef MCRT_MIXED
+  // ------------------------------------------------ FP32 walk (QRay)
+  // FP32 opacity columns of the walk: kapd and kapd*(1-albedo) per slot.
+  float* sfb = nullptr;                                  // [2][kMaxSlot][kBlock] in shared memory
+  __device__ __forceinline__ float& kf(int s) const { return sfb[s * kBlock + threadIdx.x]; }
+  __device__ __forceinline__ float& kaf(int s) const { return sfb[(kMaxSlot + s) * kBlock + threadIdx.x]; }
+  __device__ __forceinline__ void walk_columns() {
+    for (int s = 0; s < m.nslot; ++s) {
+      kf(s) = (float)sp.kapd(s);
+      kaf(s) = (float)(sp.kapd(s) * (1.0 - sp.alb(s)));
+    }
+  }
+  // Opacity and thermal absorption coefficient of a cell at the walk's
+  // frequency (tauint_3d_2_fuv.f90:59-65, :83-90; small grains, ids 5-8,
+  // take no part in the absorption tally).
+  __device__ __forceinline__ void cell_coefs(const CellRecF& c, float& opac, float& absc) const {
+    const int n = cell_n(c.meta);
+    opac = 0.0f;
+    absc = 0.0f;
+    for (int k = 0; k < n; ++k) {
+      const int s = cell_slot(c.meta, k);
+      opac = fmaf(kf(s), c.rho[k], opac);
+      const int id = cell_id(c.meta, k);
+      if (id < 5 || id > 8) absc = fmaf(kaf(s), c.rho[k], absc);
+    }
+  }
+  __device__ __forceinline__ void tally_absf(int64_t ci, float absc, double len) {
+    if (absc > 0.0f) atomicAdd(T.dtauabs + ci, len * (double)absc);
+    if (m.iffuv) atomicAdd(T.fuvmean + ci, len * (m.rstar * RSOL) * ifuv / __ldg(m.vcell + ci));
+  }
+
+  // Next sphere crossing of cell r: the inner wall while the ray still
+  // approaches the origin (q < 0) and passes inside it, else the outer wall.
+  __device__ __forceinline__ void qnext_r(QRay& g, int r) const {
+    const double a2 = __ldg(m.r2arr + r - 1);
+    const bool inner = g.q < 0.0 && g.p2 < a2;
+    const int w = inner ? r - 1 : r;
+    const double d = fmax((inner ? a2 : __ldg(m.r2arr + r)) - g.p2, 0.0);
+    const double s = __ldg(m.wall64 + w) ? sqrt(d) : (double)sqrtf((float)d);
+    g.qr = inner ? -s : s;
+    g.sr = inner ? -1 : 1;
+  }
+
+  // Roots of cone wall w on its own nappe.  A root within `win` of the
+  // current point counts only if the ray moves towards that wall there
+  // (toward: mu changes toward the wall's mu), which settles the crossings
+  // that FP32 rounding cannot order, such as the wall a walk starts next to
+  // or has just crossed.
+  __device__ __forceinline__ void qcone(const QRay& g, int w, int step, bool toward, float qf, float win, double& best,
+                                        int& st) const {
+    const float2 c = __ldg(m.tcone + w);
+    if (c.y > 1.5f) return;                               // pole (tan2arr = 0): never crossed
+    float q1, q2;
+    if (c.y < 0.0f) {                                     // the theta = 90 deg plane z = 0
+      if (g.uz == 0.0f) return;
+      q1 = -g.cz / g.uz;
+      q2 = -HUGE_VALF;
+    } else {
+      const float A = fmaf(g.uz, g.uz, -c.y);
+      const float B = g.cz * g.uz;
+      const float D = fmaf(g.p2f, A, g.cz * g.cz);           // discriminant / mu^2
+      if (!(D > 0.0f)) return;
+      const float s = fabsf(c.x) * sqrtf(D);
+      const float den = B >= 0.0f ? -B - s : s - B;         // no cancellation
+      const float C = fmaf(-c.y, g.p2f, g.cz * g.cz);
+      q1 = __fdividef(den, A);
+      q2 = __fdividef(C, den);
+      // a root on the other nappe (z of opposite sign to mu) is not this wall
+      if (fmaf(g.uz, q1, g.cz) * c.x <= 0.0f) q1 = -HUGE_VALF;
+      if (fmaf(g.uz, q2, g.cz) * c.x <= 0.0f) q2 = -HUGE_VALF;
+    }
+    const float qq[2] = {q1, q2};
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float qi = qq[i];
+      const bool ok = qi > qf + win || (qi >= qf - win && toward);
+      if (ok && (double)qi < best) { best = fmax((double)qi, g.q); st = step; }
+    }
+  }
+
+  // Next cone crossing of cell t (walls t-1 above, t below in theta).
+  __device__ __forceinline__ void qnext_t(QRay& g, int t) const {
+    g.qt = HUGE_D;
+    g.st = 0;
+    if (m.ntg <= 2) return;
+    const float qf = (float)g.q;
+    const float win = 1.0e-5f * (fabsf(qf) + g.pabs);
+    // d mu / dq has the sign of u_z p^2 - c_z q
+    const float dmu = fmaf(g.uz, g.p2f, -g.cz * qf);
+    double best = HUGE_D;
+    int st = 0;
+    qcone(g, t - 1, -1, dmu > 0.0f, qf, win, best, st);
+    qcone(g, t, 1, dmu < 0.0f, qf, win, best, st);
+    g.qt = best;
+    g.st = st;
+  }
+
+  // Next phi-plane crossing of cell p: the azimuth moves monotonically with
+  // the sign of L_z = c_x u_y - c_y u_x, so only the wall ahead is solved.
+  __device__ __forceinline__ void qnext_p(QRay& g, int p) const {
+    g.qp = HUGE_D;
+    g.sp = 0;
+    if (m.npg <= 2 || m.ntg <= 2) return;
+    const int w = g.lzpos ? p : p - 1;
+    const float2 ab = __ldg(m.pplane + w);
+    const float den = fmaf(ab.x, g.ux, ab.y * g.uy);
+    if (den == 0.0f) return;
+    const float qi = -__fdividef(fmaf(ab.x, g.cx, ab.y * g.cy), den);
+    const float qf = (float)g.q;
+    const float win = 1.0e-5f * (fabsf(qf) + g.pabs);
+    if (qi >= qf - win) {
+      g.qp = fmax((double)qi, g.q);
+      g.sp = g.lzpos ? 1 : -1;
+    }
+  }
+
+  // Set up the walk of the ray from (x,y,z) along (vx,vy,vz) in cell
+  // (r,t,p).  testgrid's role (testgrid.f90:1-128) is played here, once per
+  // walk: an index that disagrees with the start point beyond 1e-4 of the
+  // cell is re-located; a start point outside the grid is clamped to its
+  // first or last cell (counted as a reset).
+  __device__ void qbegin(QRay& g, double x, double y, double z, double vx, double vy, double vz, int& r, int& t,
+                         int& p) {
+    const double q0 = x * vx + y * vy + z * vz;
+    const double cx = x - q0 * vx, cy = y - q0 * vy, cz = z - q0 * vz;
+    g.q = q0;
+    g.q0 = q0;
+    g.p2 = cx * cx + cy * cy + cz * cz;
+    g.p2f = (float)g.p2;
+    g.pabs = sqrtf(g.p2f);
+    g.cx = (float)cx; g.cy = (float)cy; g.cz = (float)cz;
+    g.ux = (float)vx; g.uy = (float)vy; g.uz = (float)vz;
+    g.lzpos = x * vy - y * vx > 0.0;
+    const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
+    const double tol = 1.0e-4;
+    const double rs = x * x + y * y + z * z;
+    bool moved = false;
+    {
+      const bool bad = r < 1 || r > nrg - 1;
+      const double a = bad ? 0.0 : __ldg(m.r2arr + r - 1), b = bad ? 0.0 : __ldg(m.r2arr + r);
+      if (bad || rs - a < -tol * (b - a) || rs - b > tol * (b - a)) {
+        const int r0 = locate(m.r2arr, nrg, rs);
+        r = min(max(r0, 1), nrg - 1);
+        moved = moved || r0 < 1 || r0 > nrg - 1;
+      }
+    }
+    if (ntg > 2) {
+      const double cb = chk(z / sqrt(rs));
+      const bool bad = t < 1 || t > ntg - 1;
+      const double a = bad ? 0.0 : __ldg(m.costarr + t - 1), b = bad ? 0.0 : __ldg(m.costarr + t);
+      if (bad || cb - a > tol * (a - b) || b - cb > tol * (a - b)) {
+        const int t0 = locate(m.costarr, ntg, cb);
+        t = min(max(t0, 1), ntg - 1);
+        moved = moved || t0 < 1 || t0 > ntg - 1;
+      }
+    }
+    if (npg > 2) {
+      double ph = atan2(y, x);
+      if (ph < 0.0) ph = ph + R2P;
+      const bool bad = p < 1 || p > npg - 1;
+      const double a = bad ? 0.0 : __ldg(m.phiarr + p - 1), b = bad ? 0.0 : __ldg(m.phiarr + p);
+      if (bad || ph - a < -tol * (b - a) || ph - b > tol * (b - a)) {
+        const int p0 = locate(m.phiarr, npg, ph);
+        p = min(max(p0, 1), npg - 1);
+      }
+    }
+    if (moved) ++c_reset;
+    qnext_r(g, r);
+    qnext_t(g, t);
+    qnext_p(g, p);
+  }
+#endif
 
   // tauint_3d_2_fuv.f90:5-210.  false = geometry failure.
   __device__ bool tauint() {

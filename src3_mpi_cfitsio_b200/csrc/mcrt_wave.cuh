@@ -105,7 +105,6 @@ __device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int n
   for (int s = 0; s < nslot; ++s) {
     k.sp.g(s) = R.spec[2 * kMaxSlot + s];
     k.sp.pl(s) = R.spec[3 * kMaxSlot + s];
-    k.sp.kap(s) = R.spec[4 * kMaxSlot + s];
   }
 }
 
@@ -128,7 +127,6 @@ __device__ __forceinline__ void wave_save_event(const Lane& L, WaveRec& R, int n
     R.spec[kMaxSlot + s] = k.sp.alb(s);
     R.spec[2 * kMaxSlot + s] = k.sp.g(s);
     R.spec[3 * kMaxSlot + s] = k.sp.pl(s);
-    R.spec[4 * kMaxSlot + s] = k.sp.kap(s);
   }
 }
 
@@ -225,7 +223,12 @@ __global__ void __launch_bounds__(kBlock, MCRT_EVENT_MIN_BLOCKS) wave_event(Laun
 // `walk_batch` idle lanes.
 __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(LaunchParams P, WaveArgs W) {
   __shared__ double spec[2 * kMaxSlot * kBlock];   // kapd and alb columns only (step<true> reads no others)
+#ifdef MCRT_MIXED
+  __shared__ float specf[2 * kMaxSlot * kBlock];   // the FP32 walk columns
+  Lane L(P.m, P.t, spec, specf);
+#else
   Lane L(P.m, P.t, spec);
+#endif
   const int nslot = P.m.nslot;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;

@@ -31,6 +31,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 
 import numpy as np
 
@@ -672,6 +673,22 @@ def setdiffus(m: Model, tdave: np.ndarray, iteration: int) -> Model:
 def with_diffusion(m: Model, iteration: int = 2) -> Model:
     """setdiffus on the model's current temperature."""
     return setdiffus(m, m.grid["tdust"].copy(), iteration)
+
+
+LUCY_STATE_2D = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "reference_2d_tdave.npy")
+
+
+def reference_2d_converged(**over) -> Model:
+    """The 2-D benchmark model at its converged Lucy temperature: tdave from
+    data/reference_2d_tdave.npy (made by data/make_lucy_state.py with the
+    FP64 engine) and the diffusion region it implies (setdiffus); the
+    power-law stand-in temperature (warm) if the file is absent."""
+    m = reference_2d(**over)
+    if not over and os.path.exists(LUCY_STATE_2D):
+        td = np.load(LUCY_STATE_2D)
+        if td.size == m.w.nrg * m.w.ntg * m.w.npg:
+            return setdiffus(m, td, 2)
+    return with_diffusion(warm(m))
 
 
 def tdust_from_tdave(m: Model, tdave: np.ndarray) -> np.ndarray:

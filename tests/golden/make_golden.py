@@ -80,4 +80,6 @@ def main(src_dir: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src3_mpi_cfitsio")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference's src3_mpi_cfitsio directory>")
+    main(sys.argv[1])

@@ -16,39 +16,48 @@ from src3_mpi_cfitsio_b200 import model
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(eng, nphot, it, tdave):
+def _noalloc(eng, nphot, it, tdave, converge=0):
     lib = eng.lib
     lib.mcrt_update_temperature_noalloc.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double),
                                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]
     lib.mcrt_update_temperature_noalloc.restype = C.c_int
     td = np.ascontiguousarray(tdave, dtype=np.float64).copy()
-    conv = C.c_int32(0)
+    conv = C.c_int32(converge)
     sig = np.zeros(3)
     rc = lib.mcrt_update_temperature_noalloc(eng.ctx, nphot, it, td.ctypes.data_as(C.POINTER(C.c_double)),
                                              C.byref(conv), sig.ctypes.data_as(C.POINTER(C.c_double)))
     assert rc == 0, lib.mcrt_last_error(eng.ctx)
-    return td, sig
+    return td, bool(conv.value), sig
 
 
 def test_noalloc_matches_allocating_entry_point_twice():
-    """Two Lucy iterations; after each packet run both entry points update
-    the temperature from the same device tallies and must agree."""
+    """Three Lucy iterations on a model with diffusion cells: two engines run
+    the same packets (same streams, so the same histories; tallies differ
+    only by the order of the FP64 atomic additions), one updates the
+    temperature with each entry point, and the temperatures, the
+    convergence statistics and the convergence flag must agree call after
+    call (the no-alloc scratch keeps the previous call's contents)."""
     from src3_mpi_cfitsio_b200.engine import Engine
-    m = model.warm(model.small_2d())
+    m = model.with_diffusion(model.warm(model.small_2d()))
+    assert (m.grid["diffus"] > 0).any()
     n = 20000
-    eng = Engine(m)
-    tdave = m.grid["tdust"].copy()
-    for it in (1, 2):
-        eng.reset_tallies()
-        eng.run(n, iteration=it, ipeel=0)
-        td_b, sig_b = _noalloc(eng, n, it, tdave)
-        eng.tdave = tdave
-        td_a, _, sig_a = eng.update_temperature(n, it)
-        assert np.isfinite(td_b).all() and (td_b > 0).all()
-        assert np.allclose(td_b, td_a, rtol=1e-12, atol=0), np.abs(td_b - td_a).max()
-        assert np.allclose(sig_b, sig_a, rtol=1e-9, equal_nan=True)
-        tdave = td_a
-    eng.close()
+    ea, eb = Engine(m), Engine(m)
+    for e in (ea, eb):
+        e.set_schedule("warp")
+    ta = tb = m.grid["tdust"].copy()
+    for it in (1, 2, 3):
+        for e in (ea, eb):
+            e.reset_tallies()
+            e.run(n, iteration=it, ipeel=0)
+        ea.tdave = ta
+        ta, conv_a, sig_a = ea.update_temperature(n, it)
+        tb, conv_b, sig_b = _noalloc(eb, n, it, tb)
+        assert np.isfinite(tb).all() and (tb > 0).all()
+        assert np.allclose(tb, ta, rtol=1e-10, atol=0), np.abs(tb - ta).max()
+        assert np.allclose(sig_b, sig_a, rtol=1e-8, equal_nan=True)
+        assert conv_a == conv_b
+    ea.close()
+    eb.close()
 
 
 def test_noalloc_rejects_models_beyond_its_scratch():
