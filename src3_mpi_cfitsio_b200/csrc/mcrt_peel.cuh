@@ -127,6 +127,7 @@ struct PeelLane {
       R.r += g.sr;
     } else if (d == 1) {
       R.t += g.st;
+      if (R.t < 1 || R.t > m.ntg - 1) { state = 2; return; }   // no cell beyond a non-pole theta wall
     } else {
       R.p += g.sp;
       if (R.p == 0) R.p = m.npg - 1;

@@ -66,6 +66,9 @@ struct Lane {
   int64_t adj_pos, adj_end;         // replay: the packet's next record
 
   __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase, float* fbase = nullptr) : pk(m, t, sbase, fbase) {
+#ifdef MCRT_MIXED
+    ray.qready = false;
+#endif
     ev = EV_FETCH;
     status = 0;
     c_pkt = c_int = c_sca = c_geo = c_kil = c_exit = c_star = c_jobs = 0;
@@ -183,6 +186,11 @@ struct Lane {
       R.r += g.sr;
     } else if (d == 1) {
       R.t += g.st;
+      if (R.t < 1 || R.t > m.ntg - 1) {       // a theta wall that is not a pole was left: no cell beyond
+        if (!R.peel) { packet_from_ray(); status = 3; ev = EV_FINISH; }
+        else ev = EV_PEEL_NEXT;
+        return;
+      }
     } else {
       R.p += g.sp;
       if (R.p == 0) R.p = m.npg - 1;

@@ -38,6 +38,9 @@ __device__ __forceinline__ void wave_load_ray(Lane& L, const WaveRec& R, int nsl
   y.r = R.r; y.t = R.t; y.p = R.p;
   y.onw = (R.rbits & 1) != 0;
   y.peel = (R.rbits & 2) != 0;
+#ifdef MCRT_MIXED
+  y.qready = false;                 // every loaded walk sets up its own closest-approach form
+#endif
   Packet& k = L.pk;
   k.tau = R.tau; k.ifuv = R.ifuv;
   L.ray_steps = R.ray_steps;

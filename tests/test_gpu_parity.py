@@ -292,28 +292,35 @@ def test_peel_queue_matches_inline_peel_offs(warm_small):
 
 
 def test_mixed_precision_agrees_with_fp64(oracle_mod):
-    """The mixed build (FP32 scattering, division-free FP64 walk) follows the
-    same random streams, so its ensemble tallies agree with the FP64 build
-    far inside the Monte Carlo error; the walk must not lose packets."""
+    """The mixed build (FP32 closest-approach walk and FP32 scattering) runs
+    the same random streams as the FP64 build, but its walk places faces to
+    FP32 precision, so histories part company and the comparison is
+    statistical: per-packet crossing and interaction counts agree within
+    4 standard errors, no packet is lost, and every ensemble tally agrees
+    far inside the Monte Carlo error."""
     m = model.with_diffusion(model.warm(model.small_2d()))
     n = 40000
-    out = {}
+    out, logs = {}, {}
     for prec in ("fp64", "mixed"):
         eng = _engine(m, precision=prec)
+        eng.enable_packet_log(n)
         eng.reset_tallies()
         eng.run(n, ipeel=1)
         out[prec] = eng.download()
+        logs[prec] = abi.packet_log_to_numpy(eng.packet_log(n))
         eng.close()
     a, b = out["fp64"], out["mixed"]
-    ca, cb = a.counters(), b.counters()
+    cb = b.counters()
     assert cb["geom_fail"] == 0 and cb["packets"] == n
-    assert abs(cb["crossings"] - ca["crossings"]) <= 0.01 * ca["crossings"]
-    assert abs(cb["interactions"] - ca["interactions"]) <= 0.02 * ca["interactions"] + 50
+    for k in ("ncross", "nscat", "nabs"):
+        x, y = logs["fp64"][k].astype(np.float64), logs["mixed"][k].astype(np.float64)
+        se = np.sqrt((x.var() + y.var()) / n)
+        assert abs(x.mean() - y.mean()) <= 4.0 * se + 1e-9, (k, x.mean(), y.mean(), se)
     for k in ("nums", "si", "numt", "ti", "image_m_i"):
         x, y = a[k].astype(np.float64), b[k].astype(np.float64)
-        assert abs(y.sum() - x.sum()) <= 0.01 * abs(x.sum()) + 1e-12, k
-        assert np.abs(y - x).sum() <= 0.05 * np.abs(x).sum() + 1e-12, k
-    assert np.abs(b["dtauabs"] - a["dtauabs"]).sum() <= 0.03 * np.abs(a["dtauabs"]).sum()
+        assert abs(y.sum() - x.sum()) <= 0.02 * abs(x.sum()) + 1e-12, k
+        assert np.abs(y - x).sum() <= 0.08 * np.abs(x).sum() + 1e-12, k
+    assert np.abs(b["dtauabs"] - a["dtauabs"]).sum() <= 0.05 * np.abs(a["dtauabs"]).sum()
 
 
 def _with_accretion(m, frac=0.3):
