@@ -136,13 +136,16 @@ struct Lane {
   // Mixed build: one crossing of the FP32 walk (QRay, mcrt_transport.cuh)
   // with the same outcomes as the FP64 step below.  A ray's peel-off bin
   // reads the start point: the image coordinates are projections along the
-  // peel-off direction, the same for every point of the ray.
+  // peel-off direction, the same for every point of the ray.  With
+  // kStarEvent (the walk kernel) the walk is set up by the record load and
+  // the packet position is formed by the record save (wave_save_qwalk), so
+  // the start point is not held through the walk.
   template <bool kStarEvent = false>
   __device__ __forceinline__ void step(const LaunchParams& P) {
     const DevModel& m = pk.m;
     Ray& R = ray;
     QRay& g = R.g;
-    if (!R.qready) {
+    if (!kStarEvent && !R.qready) {
       pk.walk_columns();
       pk.qbegin(g, R.x, R.y, R.z, R.vx, R.vy, R.vz, R.r, R.t, R.p);
       R.qready = true;
@@ -152,7 +155,7 @@ struct Lane {
     if (g.qt < qn) { qn = g.qt; d = 1; }
     if (g.qp < qn) { qn = g.qp; d = 2; }
     if (!(qn < HUGE_D) || ++ray_steps > 50000000) {
-      if (!R.peel) { packet_from_ray(); status = 3; ev = EV_FINISH; }
+      if (!R.peel) { if (!kStarEvent) packet_from_ray(); status = 3; ev = EV_FINISH; }
       else ev = EV_PEEL_NEXT;
       return;
     }
@@ -169,7 +172,7 @@ struct Lane {
         if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)ds);
         g.q = g.q + ds;
         R.onw = false;
-        packet_from_ray();
+        if (!kStarEvent) packet_from_ray();
         ev = EV_AFTER_WALK;
         return;
       }
@@ -187,7 +190,7 @@ struct Lane {
     } else if (d == 1) {
       R.t += g.st;
       if (R.t < 1 || R.t > m.ntg - 1) {       // a theta wall that is not a pole was left: no cell beyond
-        if (!R.peel) { packet_from_ray(); status = 3; ev = EV_FINISH; }
+        if (!R.peel) { if (!kStarEvent) packet_from_ray(); status = 3; ev = EV_FINISH; }
         else ev = EV_PEEL_NEXT;
         return;
       }
@@ -199,9 +202,9 @@ struct Lane {
     if (!R.peel) {
       ++pk.ncross;
       ++pk.c_cross;
-      if (R.r == m.nrg) { pk.exitflag = 1; packet_from_ray(); ev = EV_EXIT; return; }
+      if (R.r == m.nrg) { pk.exitflag = 1; if (!kStarEvent) packet_from_ray(); ev = EV_EXIT; return; }
       if (R.r == 0) {                 // star hit: re-emission, tau kept (tauint_3d_2_fuv.f90:184-206)
-        packet_from_ray();
+        if (!kStarEvent) packet_from_ray();
         if (kStarEvent) { ev = EV_STAR; return; }
         star_reemit();
         return;

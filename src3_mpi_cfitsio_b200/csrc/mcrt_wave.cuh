@@ -133,6 +133,53 @@ __device__ __forceinline__ void wave_save_event(const Lane& L, WaveRec& R, int n
   }
 }
 
+#ifdef MCRT_MIXED
+// The mixed walk kernel's record I/O: the walk is set up in its
+// closest-approach form straight from the record (start point, direction,
+// FP32 opacity columns), and the save writes only what a walk changes; the
+// packet position at the walk's end is start + (q - q0) u with the start
+// point and direction read again from the record, which the walk kernel
+// never writes.  The random stream is not used by the mixed walk.
+__device__ __forceinline__ void wave_load_qwalk(Lane& L, const WaveRec& R, int nslot) {
+  Ray& y = L.ray;
+  Packet& k = L.pk;
+  y.r = R.r; y.t = R.t; y.p = R.p;
+  y.onw = (R.rbits & 1) != 0;
+  y.peel = (R.rbits & 2) != 0;
+  y.tsum = R.tsum;
+  y.qready = true;
+  k.tau = R.tau; k.ifuv = R.ifuv;
+  L.ray_steps = R.ray_steps;
+  L.ev = R.ev; L.status = R.status;
+  k.ncross = R.ncross; k.exitflag = R.exitflag;
+  for (int s = 0; s < nslot; ++s) {
+    const double kd = R.spec[s];
+    k.kf(s) = (float)kd;
+    k.kaf(s) = (float)(kd * (1.0 - R.spec[kMaxSlot + s]));
+  }
+  k.qbegin(y.g, R.x, R.y, R.z, R.vx, R.vy, R.vz, y.r, y.t, y.p);
+}
+
+__device__ __forceinline__ void wave_save_qwalk(const Lane& L, WaveRec& R) {
+  const Ray& y = L.ray;
+  const Packet& k = L.pk;
+  R.tsum = y.tsum;
+  R.r = y.r; R.t = y.t; R.p = y.p;
+  R.rbits = (y.onw ? 1 : 0) | (y.peel ? 2 : 0);
+  R.ray_steps = L.ray_steps;
+  R.ev = L.ev; R.status = L.status;
+  R.ncross = k.ncross; R.exitflag = k.exitflag;
+  if (!y.peel) {
+    const double d = y.g.q - y.g.q0;
+    const double x = R.x + d * R.vx, yy = R.y + d * R.vy, z = R.z + d * R.vz;
+    const double rs = x * x + yy * yy + z * z;
+    R.xp = x; R.yp = yy; R.zp = z; R.rsq = rs; R.rtot = sqrt(rs);
+    R.on_wall = y.onw ? 1 : 0;
+    R.ir = y.r; R.it = y.t; R.ip = y.p;
+  }
+}
+#endif
+
 __device__ __forceinline__ void flush_counters(const LaunchParams& P, const Lane& L) {
   unsigned long long v[14] = {L.c_pkt, L.pk.c_cross, L.c_int, L.c_sca, L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin,
                               L.c_geo, L.pk.c_reset, L.c_kil, L.c_exit, L.c_star, 0ull, L.c_jobs};
@@ -225,11 +272,11 @@ __global__ void __launch_bounds__(kBlock, MCRT_EVENT_MIN_BLOCKS) wave_event(Laun
 // event.  Lanes take new walks from the queue in warp batches of at least
 // `walk_batch` idle lanes.
 __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(LaunchParams P, WaveArgs W) {
-  __shared__ double spec[2 * kMaxSlot * kBlock];   // kapd and alb columns only (step<true> reads no others)
 #ifdef MCRT_MIXED
-  __shared__ float specf[2 * kMaxSlot * kBlock];   // the FP32 walk columns
-  Lane L(P.m, P.t, spec, specf);
+  __shared__ float specf[2 * kMaxSlot * kBlock];   // the FP32 walk columns (the only species state it reads)
+  Lane L(P.m, P.t, nullptr, specf);
 #else
+  __shared__ double spec[2 * kMaxSlot * kBlock];   // kapd and alb columns only (step<true> reads no others)
   Lane L(P.m, P.t, spec);
 #endif
   const int nslot = P.m.nslot;
@@ -252,7 +299,11 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
         const unsigned long long k = base + (unsigned long long)__popc(idle & ((1u << lane) - 1u));
         if (k < nw) {
           slot = W.walkq[k];
+#ifdef MCRT_MIXED
+          wave_load_qwalk(L, W.recs[slot], nslot);
+#else
           wave_load_ray(L, W.recs[slot], nslot);
+#endif
           have = true;
         }
       }
@@ -267,8 +318,12 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
       done = L.ev != EV_NONE;
       if (done) {
         WaveRec& R = W.recs[slot];
+#ifdef MCRT_MIXED
+        wave_save_qwalk(L, R);
+#else
         wave_save_ray(L, R);
         if (!L.ray.peel) wave_save_pos(L, R);
+#endif
       }
     }
     const bool front = done && L.ev == EV_AFTER_WALK;
