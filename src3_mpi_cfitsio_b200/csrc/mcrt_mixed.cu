@@ -1,19 +1,27 @@
 // mcrt_mixed.cu -- mixed-precision transport build.
 //
 // The transport and peel-off kernels of mcrt_sched.cuh / mcrt_peel.cuh
-// compiled with MCRT_MIXED: scattering (rejection sampling, frame rotations,
-// the peel-off phase matrix) runs in FP32.  The walk's geometry stays FP64,
-// because testgrid resolves 1e-4 of a cell and the rim and equatorial cells
-// are 6.5e-4 wide in cos(theta), beyond FP32 positions; the mixed walk drops
-// the divisions instead (grid tests as products, one reciprocal per face
-// quadratic, FMA contraction on).  Positions, face roots, the cumulative
-// optical depth and its comparison with the sampled tau, opacities and all
-// tallies are FP64.  The device code is
-// compiled into its own namespace so that it can coexist with the FP64
-// build's kernels; the launch parameters have the same layout.
+// compiled with MCRT_MIXED:
+//  * the packet walk and the peel-off walk run in FP32 in the
+//    closest-approach form (QRay, mcrt_transport.cuh): cone and plane roots,
+//    cell opacities and the walk state in FP32; sphere roots in FP64 where
+//    a wall borders a cell thinner than 1 % of its radius (the disk rim);
+//    the along-ray coordinate, the cumulative optical depth, its comparison
+//    with the sampled tau, and every tally in FP64;
+//  * scattering (rejection sampling, frame rotations, the peel-off phase
+//    matrix) in FP32.
+// Packet positions between walks, directions, frequencies and the event
+// code stay FP64.  The device code is compiled into its own namespace so
+// that it can coexist with the FP64 build's kernels; the launch parameters
+// have the same layout.
 #include <cuda_runtime.h>
 
 #define MCRT_MIXED 1
+// The FP32 walk kernel runs 8 blocks (32 warps) per SM at <= 64 registers:
+// 1.33x the walk rate of 4 blocks on the 1e8-packet 2-D iteration.
+#ifndef MCRT_WALK_MIN_BLOCKS
+#define MCRT_WALK_MIN_BLOCKS 8
+#endif
 #define mcrt mcrt_mixed
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"

@@ -168,9 +168,7 @@ struct PeelLane {
     R.z = R.z + dt * R.vz;
     R.onw = true;
     R.rs = R.x * R.x + R.y * R.y + R.z * R.z;
-#ifndef MCRT_MIXED
-    R.rt = sqrt(R.rs);            // the mixed testgrid forms rt itself
-#endif
+    R.rt = sqrt(R.rs);
     if (state != 5) ++pk.c_pcross;
     if (R.r == m.nrg) { state = (state == 5) ? 2 : 1; return; }
     if (R.r == 0) { state = 2; return; }

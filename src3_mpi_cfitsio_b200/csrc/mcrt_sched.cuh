@@ -279,9 +279,7 @@ struct Lane {
     R.z = R.z + dt * R.vz;
     R.onw = true;
     R.rs = R.x * R.x + R.y * R.y + R.z * R.z;
-#ifndef MCRT_MIXED
-    R.rt = sqrt(R.rs);            // the mixed testgrid forms rt itself
-#endif
+    R.rt = sqrt(R.rs);
     if (!R.peel) {
       R.tsum = R.tsum + dtau;
       ++pk.ncross;

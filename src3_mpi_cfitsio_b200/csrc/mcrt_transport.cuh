@@ -446,87 +446,9 @@ struct Packet {
   }
 
   // -------------------------------------------------------------- grid
-  // testgrid.f90:1-128.  For npg == 2 the phi checks can never fire
-  // (phi in [0,2pi) against phiarr = [0,2pi]), so atan2 is only evaluated
-  // when a re-location needs it.
-#ifdef MCRT_MIXED
-  // Mixed build: the same FP64 tests as testgrid.f90 written without
-  // divisions (a fraction compared with a bound becomes a product with the
-  // cell width).  FP32 positions cannot be used here: the tests resolve 1e-4
-  // of a cell, and the rim and equatorial cells are 6.5e-4 wide in cos(theta).
-  __device__ void testgrid(double& x, double& y, double& z, double& rs, double& rt, int& r, int& t, int& p, bool& onw) {
-    const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
-    const double tol = 1.0e-4;
-    const double* r2 = m.r2arr;
-    const double* ca = m.costarr;
-    const double* pa = m.phiarr;
-    // num/den < v and num/den > v without the division
-    auto lt = [](double num, double den, double v) { return den > 0.0 ? num < v * den : num > v * den; };
-    auto gt = [](double num, double den, double v) { return den > 0.0 ? num > v * den : num < v * den; };
-    rt = sqrt(rs);
-    const double irt = 1.0 / rt;
-    double cb = chk(z * irt);
-    const bool need_phi = npg > 2;
-    double ph = 0.0;
-    if (need_phi) {
-      ph = atan2(y, x);
-      if (ph < 0.0) ph = ph + R2P;
-    }
-    bool reset = false;
-    const double r20 = __ldg(r2), r21 = __ldg(r2 + 1), r2a = __ldg(r2 + nrg - 2), r2b = __ldg(r2 + nrg - 1);
-    if (lt(rs - r20, r21 - r20, -tol) || gt(rs - r2a, r2b - r2a, 1.0 + tol)) {
-      const double third = (double)(1.0f / 3.0f);
-      const double r1 = m.rarr[0], rn = m.rarr[nrg - 1];
-      rt = pow(ran() * (pow(rn, 3.0) - pow(r1, 3.0)) + pow(r1, 3.0), third);
-      reset = true;
-    }
-    const double c0 = __ldg(ca), c1 = __ldg(ca + 1), ca2 = __ldg(ca + ntg - 2), cb2 = __ldg(ca + ntg - 1);
-    if (lt(cb - c0, c1 - c0, -tol) || gt(cb - ca2, cb2 - ca2, 1.0 + tol)) {
-      cb = ran() * (cb2 - c0) + c0;
-      reset = true;
-    }
-    if (need_phi && (lt(ph - pa[0], pa[1] - pa[0], -tol) || gt(ph - pa[npg - 2], pa[npg - 1] - pa[npg - 2], 1.0 + tol))) {
-      ph = ran() * (pa[npg - 1] - pa[0]) + pa[0];
-      reset = true;
-    }
-    if (reset) {
-      if (!need_phi) {
-        ph = atan2(y, x);
-        if (ph < 0.0) ph = ph + R2P;
-      }
-      double sq = sqrt(1.0 - cb * cb);
-      x = rt * sq * cos(ph);
-      y = rt * sq * sin(ph);
-      z = rt * cb;
-      rs = rt * rt;
-      onw = false;
-      ++c_reset;
-    }
-    if (r < 1 || r > nrg) r = locate(r2, nrg, rs);
-    if (t < 1 || t > ntg) t = locate(ca, ntg, cb);
-    if (p < 1 || p > npg) {
-      if (!need_phi) { ph = atan2(y, x); if (ph < 0.0) ph = ph + R2P; }
-      p = locate(pa, npg, ph);
-    }
-    const double ra = __ldg(r2 + r - 1), rb = __ldg(r2 + r);
-    const double ta = __ldg(ca + t - 1), tb = __ldg(ca + t);
-    bool phierr = false;
-    if (need_phi) {
-      if (lt(ph - pa[p - 1], pa[p] - pa[p - 1], -tol) || gt(ph - pa[p - 1], pa[p] - pa[p - 1], 1.0 + tol)) {
-        double d1 = ph - pa[p - 1];
-        if (d1 > PI) d1 -= R2P;
-        if (d1 < -PI) d1 += R2P;
-        double d2 = ph - pa[p];
-        if (d2 > PI) d2 -= R2P;
-        if (d2 < -PI) d2 += R2P;
-        phierr = fabs(d1) > tol && fabs(d2) > tol;
-      }
-    }
-    if (lt(rs - ra, rb - ra, -tol) || gt(rs - ra, rb - ra, 1.0 + tol)) r = locate(r2, nrg, rs);
-    if (lt(cb - ta, tb - ta, -tol) || gt(cb - ta, tb - ta, 1.0 + tol)) t = locate(ca, ntg, cb);
-    if (phierr) p = locate(pa, npg, ph);
-  }
-#else
+  // testgrid.f90:1-128 (the FP64 walk).  For npg == 2 the phi checks can
+  // never fire (phi in [0,2pi) against phiarr = [0,2pi]), so atan2 is only
+  // evaluated when a re-location needs it.
   __device__ void testgrid(double& x, double& y, double& z, double& rs, double& rt, int& r, int& t, int& p, bool& onw) {
     const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
     const double tol = 1.0e-4;
@@ -595,7 +517,6 @@ struct Packet {
     if (tfrac < -tol || tfrac > 1.0 + tol) t = locate(ca, ntg, cb);
     if (phierr) p = locate(pa, npg, ph);
   }
-#endif
 
   // radface / thetaface / phiface (radface.f90, thetaface.f90, phiface.f90)
   __device__ __forceinline__ void faces(Walls& w, double vx, double vy, double vz, double x, double y, double z,
@@ -616,59 +537,6 @@ struct Packet {
       w.insert((-bb + descr) * 0.5, 2);
       w.insert((-bb - descr) * 0.5, 2);
     }
-#ifdef MCRT_MIXED
-    // Mixed build: thetaface/phiface in FP64 (see testgrid) with one
-    // reciprocal per quadratic instead of two divisions.
-    if (m.ntg > 2) {
-      const double t1 = __ldg(m.tan2arr + t - 1), t2 = __ldg(m.tan2arr + t);
-      const double tmp1 = x * vx + y * vy, tmp2 = vx * vx + vy * vy, tmp3 = x * x + y * y;
-      double ta, tb;
-      int i1, i2;
-      if (t2 < t1) { ta = t2; tb = t1; i1 = 4; i2 = 3; }
-      else { ta = t1; tb = t2; i1 = 3; i2 = 4; }
-      if (ta < 0.0) {
-        if (vz != 0.0) w.insert(-z / vz, i1);
-      } else {
-        const double b2 = 2.0 * (tmp1 - ta * vz * z);
-        const double aa = tmp2 - ta * vz * vz;
-        const double c2 = tmp3 - z * z * ta;
-        if (fabs(aa) > 1.0e-10) {
-          double d = b2 * b2 - 4.0 * aa * c2;
-          if (d > 0.0 && ta != 0.0) {
-            d = sqrt(d);
-            const double ia = 0.5 / aa;
-            w.insert((-b2 + d) * ia, i1);
-            w.insert((-b2 - d) * ia, i1);
-          }
-        } else if (fabs(b2) > 1.0e-10) {
-          w.insert(-c2 / b2, i1);
-        }
-      }
-      const double b2 = 2.0 * (tmp1 - tb * vz * z);
-      const double aa = tmp2 - tb * vz * vz;
-      const double c2 = tmp3 - z * z * tb;
-      if (fabs(aa) > 1.0e-10) {
-        double d = b2 * b2 - 4.0 * aa * c2;
-        if (d > 0.0 && tb != 0.0) {
-          d = sqrt(d);
-          const double ia = 0.5 / aa;
-          w.insert((-b2 + d) * ia, i2);
-          w.insert((-b2 - d) * ia, i2);
-        }
-      } else if (fabs(b2) > 1.0e-10) {
-        w.insert(-c2 / b2, i2);
-      }
-    }
-    if (m.npg > 2 && m.ntg > 2) {
-      const double A1 = __ldg(m.aarr + p - 1), B1 = __ldg(m.barr + p - 1);
-      const double A2 = __ldg(m.aarr + p), B2 = __ldg(m.barr + p);
-      const double d1 = (A1 * vx + B1 * vy);
-      if (d1 != 0.0) w.insert(-(A1 * x + B1 * y) / d1, 5);
-      const double d2 = (A2 * vx + B2 * vy);
-      if (d2 != 0.0) w.insert(-(A2 * x + B2 * y) / d2, 6);
-    }
-  }
-#else
     if (m.ntg > 2) {
       const double t1 = __ldg(m.tan2arr + t - 1), t2 = __ldg(m.tan2arr + t);
       const double tmp1 = x * vx + y * vy, tmp2 = vx * vx + vy * vy, tmp3 = x * x + y * y;
@@ -716,7 +584,6 @@ struct Packet {
       if (d2 != 0.0) w.insert(-(A2 * x + B2 * y + 0.0 * z + 0.0) / d2, 6);
     }
   }
-#endif
 
   __device__ __forceinline__ int64_t cidx(int r, int t, int p) const {
     return (int64_t)(r - 1) + (int64_t)m.nrg * ((t - 1) + (int64_t)m.ntg * (p - 1));
