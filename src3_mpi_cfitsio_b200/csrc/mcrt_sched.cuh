@@ -86,12 +86,7 @@ struct Lane {
 #ifdef MCRT_MIXED
   // The packet at the walk's current point: start + (q - q0) u in FP64.
   __device__ __forceinline__ void packet_from_ray() {
-    const double d = ray.g.q - ray.g.q0;
-    pk.xp = ray.x + d * ray.vx;
-    pk.yp = ray.y + d * ray.vy;
-    pk.zp = ray.z + d * ray.vz;
-    pk.rsq = pk.xp * pk.xp + pk.yp * pk.yp + pk.zp * pk.zp;
-    pk.rtot = sqrt(pk.rsq);
+    Packet::qpos(ray.x, ray.y, ray.z, ray.vx, ray.vy, ray.vz, ray.g.q, ray.g.q0, pk.xp, pk.yp, pk.zp, pk.rsq, pk.rtot);
     pk.ir = ray.r; pk.it = ray.t; pk.ip = ray.p; pk.on_wall = ray.onw;
   }
 #else

@@ -741,13 +741,27 @@ struct Packet {
     }
   }
 
+  // The point of the walk at q: start + (q - q0) u, and its r^2 and r.
+  // Not inlined: every schedule forms the packet position with this one
+  // compiled sequence, so the schedules stay bitwise equal.
+  __device__ __noinline__ static void qpos(double x0, double y0, double z0, double vx, double vy, double vz,
+                                           double q, double q0, double& x, double& y, double& z, double& rs,
+                                           double& rt) {
+    const double d = q - q0;
+    x = x0 + d * vx;
+    y = y0 + d * vy;
+    z = z0 + d * vz;
+    rs = x * x + y * y + z * z;
+    rt = sqrt(rs);
+  }
+
   // Set up the walk of the ray from (x,y,z) along (vx,vy,vz) in cell
   // (r,t,p).  testgrid's role (testgrid.f90:1-128) is played here, once per
   // walk: an index that disagrees with the start point beyond 1e-4 of the
   // cell is re-located; a start point outside the grid is clamped to its
   // first or last cell (counted as a reset).
-  __device__ void qbegin(QRay& g, double x, double y, double z, double vx, double vy, double vz, int& r, int& t,
-                         int& p) {
+  __device__ __noinline__ void qbegin(QRay& g, double x, double y, double z, double vx, double vy, double vz, int& r,
+                                      int& t, int& p) {
     const double q0 = x * vx + y * vy + z * vz;
     const double cx = x - q0 * vx, cy = y - q0 * vy, cz = z - q0 * vz;
     g.q = q0;

@@ -170,10 +170,9 @@ __device__ __forceinline__ void wave_save_qwalk(const Lane& L, WaveRec& R) {
   R.ev = L.ev; R.status = L.status;
   R.ncross = k.ncross; R.exitflag = k.exitflag;
   if (!y.peel) {
-    const double d = y.g.q - y.g.q0;
-    const double x = R.x + d * R.vx, yy = R.y + d * R.vy, z = R.z + d * R.vz;
-    const double rs = x * x + yy * yy + z * z;
-    R.xp = x; R.yp = yy; R.zp = z; R.rsq = rs; R.rtot = sqrt(rs);
+    double x, yy, z, rs, rt;
+    Packet::qpos(R.x, R.y, R.z, R.vx, R.vy, R.vz, y.g.q, y.g.q0, x, yy, z, rs, rt);
+    R.xp = x; R.yp = yy; R.zp = z; R.rsq = rs; R.rtot = rt;
     R.on_wall = y.onw ? 1 : 0;
     R.ir = y.r; R.it = y.t; R.ip = y.p;
   }

@@ -31,30 +31,37 @@ def _noalloc(eng, nphot, it, tdave, converge=0):
 
 
 def test_noalloc_matches_allocating_entry_point_twice():
-    """Three Lucy iterations on a model with diffusion cells: two engines run
-    the same packets (same streams, so the same histories; tallies differ
-    only by the order of the FP64 atomic additions), one updates the
-    temperature with each entry point, and the temperatures, the
-    convergence statistics and the convergence flag must agree call after
-    call (the no-alloc scratch keeps the previous call's contents)."""
+    """Three Lucy iterations on a model with diffusion cells.  Two engines
+    each run one half of the packets and both take the sum of the two
+    halves' tallies, so they hold the same device state bit for bit (the
+    sharded reduction of a multi-GPU run); one then updates the temperature
+    with the allocating entry point, the other with the no-alloc one, and
+    the temperatures, the convergence statistics and the convergence flag
+    must agree call after call (the no-alloc scratch keeps the previous
+    call's contents)."""
+    from src3_mpi_cfitsio_b200 import dist
     from src3_mpi_cfitsio_b200.engine import Engine
     m = model.with_diffusion(model.warm(model.small_2d()))
     assert (m.grid["diffus"] > 0).any()
     n = 20000
     ea, eb = Engine(m), Engine(m)
-    for e in (ea, eb):
-        e.set_schedule("warp")
     ta = tb = m.grid["tdust"].copy()
     for it in (1, 2, 3):
+        for r, e in enumerate((ea, eb)):
+            lo, hi = dist.shard_range(n, r, 2)
+            e.reset_tallies()
+            e.run(n, lo, hi, iteration=it, ipeel=0)
+        total = ea.download(images=False).add_(eb.download(images=False))
         for e in (ea, eb):
             e.reset_tallies()
-            e.run(n, iteration=it, ipeel=0)
+            e.accumulate(total)
+            e.refresh_diffusion()
         ea.tdave = ta
         ta, conv_a, sig_a = ea.update_temperature(n, it)
         tb, conv_b, sig_b = _noalloc(eb, n, it, tb)
         assert np.isfinite(tb).all() and (tb > 0).all()
-        assert np.allclose(tb, ta, rtol=1e-10, atol=0), np.abs(tb - ta).max()
-        assert np.allclose(sig_b, sig_a, rtol=1e-8, equal_nan=True)
+        assert np.allclose(tb, ta, rtol=1e-12, atol=0), np.abs(tb - ta).max()
+        assert np.allclose(sig_b, sig_a, rtol=1e-9, equal_nan=True)
         assert conv_a == conv_b
     ea.close()
     eb.close()
