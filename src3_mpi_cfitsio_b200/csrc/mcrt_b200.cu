@@ -108,7 +108,7 @@ struct mcrt_ctx {
   double *d_walls = nullptr;
   CellRec *d_cells = nullptr;
   CellRecF *d_cellsf = nullptr;       // FP32 cells of the mixed walk
-  unsigned char *d_walk32 = nullptr;  // FP32 walk tables: tcone | pplane | wall64
+  unsigned char *d_walk32 = nullptr;  // FP32 walk tables: tcone | pplane
   double *d_tdust = nullptr, *d_vcell = nullptr;
   double *d_tdust0 = nullptr;         // tdust at the start of the iteration (read by the transport)
   double last_nphot_diff = 1.0;
@@ -607,8 +607,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   }
   // FP32 walk tables (mixed build): cells with FP32 densities; per theta
   // wall (mu, mu^2) with the plane (tan2arr = -1) and the poles (tan2arr =
-  // 0, skipped by thetaface.f90) flagged; per phi wall the plane (A, B);
-  // per radial wall the FP64-root flag of walls next to thin cells.
+  // 0, skipped by thetaface.f90) flagged; per phi wall the plane (A, B).
   std::vector<CellRecF> cellsf(ncell);
   for (int64_t k = 0; k < ncell; ++k) {
     for (int i = 0; i < kMaxComp; ++i) cellsf[k].rho[i] = (float)cells[k].rho[i];
@@ -626,16 +625,9 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     pplane[j].y = (float)(j < npg ? g->barr[j] : g->barr[npg - 1]);
   }
   const size_t w32_cone = 0, w32_plane = (size_t)(ntg + 1) * sizeof(float2);
-  const size_t w32_flag = w32_plane + (size_t)(npg + 1) * sizeof(float2);
-  std::vector<unsigned char> walk32(w32_flag + (size_t)(nrg + 1), 0);
+  std::vector<unsigned char> walk32(w32_plane + (size_t)(npg + 1) * sizeof(float2), 0);
   std::memcpy(walk32.data() + w32_cone, tcone.data(), tcone.size() * sizeof(float2));
   std::memcpy(walk32.data() + w32_plane, pplane.data(), pplane.size() * sizeof(float2));
-  for (int w = 0; w < nrg; ++w) {
-    bool thin = false;
-    if (w > 0 && g->rarr[w] - g->rarr[w - 1] < kThinWall * g->rarr[w]) thin = true;
-    if (w + 1 < nrg && g->rarr[w + 1] - g->rarr[w] < kThinWall * g->rarr[w + 1]) thin = true;
-    walk32[w32_flag + w] = thin ? 1 : 0;
-  }
   const std::vector<double> zeros(nrg > 1 ? nrg - 1 : 1, 0.0);
   addp(acc ? g->ravearr : zeros.data(), nrg - 1, 0.0);
   addp(acc ? g->Ldint : zeros.data(), nrg - 1, 1.0);
@@ -684,7 +676,6 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   m.cellsf = ctx->d_cellsf;
   m.tcone = reinterpret_cast<const float2*>(ctx->d_walk32 + w32_cone);
   m.pplane = reinterpret_cast<const float2*>(ctx->d_walk32 + w32_plane);
-  m.wall64 = ctx->d_walk32 + w32_flag;
   m.tdust = ctx->d_tdust0;
   m.vcell = ctx->d_vcell;
   m.nslot = (int)slot_species.size();

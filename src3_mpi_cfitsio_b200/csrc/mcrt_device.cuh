@@ -39,12 +39,6 @@ struct __align__(16) CellRecF {
 };
 static_assert(sizeof(CellRecF) == 16, "CellRecF must stay 16 bytes");
 
-// Radial walls whose neighbouring cells are thinner than this fraction of
-// their outer radius get FP64 face roots in the FP32 walk: an FP32 root
-// carries ~1e-7 of the radius, which must stay well below the cell width
-// (the disk rim's refined cells are ~1.6e-6 of the radius wide).
-constexpr double kThinWall = 1.0e-2;
-
 __host__ __device__ inline int cell_n(uint32_t meta) { return (int)(meta & 3u); }
 __host__ __device__ inline int cell_slot(uint32_t meta, int k) { return (int)((meta >> (2 + 7 * k)) & 7u); }
 __host__ __device__ inline int cell_id(uint32_t meta, int k) { return (int)((meta >> (5 + 7 * k)) & 15u) + 1; }
@@ -79,10 +73,8 @@ struct DevModel {
   const double *ravearr, *Ldint, *hdisk;
   // FP32 walk (mixed build): per theta wall (mu, mu^2) with mu = cos(theta)
   // in FP32 (mu^2 = -1: the theta = 90 deg plane, 2: a pole no ray crosses);
-  // per phi wall (A, B) of the plane A x + B y = 0; per radial wall 1 where
-  // the face roots need FP64 (kThinWall)
+  // per phi wall (A, B) of the plane A x + B y = 0
   const float2 *tcone, *pplane;
-  const unsigned char *wall64;
   const CellRecF *cellsf;
   // cells
   const CellRec *cells;

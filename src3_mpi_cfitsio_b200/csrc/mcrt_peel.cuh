@@ -113,8 +113,8 @@ struct PeelLane {
     const CellRecF c = m.cellsf[ci];
     float opac = 0.0f;
     const int n = cell_n(c.meta);
-    for (int k = 0; k < n; ++k) opac = fmaf(pk.kf(cell_slot(c.meta, k)), c.rho[k], opac);
-    R.tsum = R.tsum + (double)(opac * dt);
+    for (int k = 0; k < n; ++k) opac = __fmaf_rn(pk.kf(cell_slot(c.meta, k)), c.rho[k], opac);
+    R.tsum = __dadd_rn(R.tsum, (double)__fmul_rn(opac, dt));
     if (R.tsum > 25.0) { state = 2; return; }
     if (state == 5) {
       for (int k = 0; k < n; ++k)
@@ -137,7 +137,7 @@ struct PeelLane {
     if (R.r == m.nrg) { state = (state == 5) ? 2 : 1; return; }
     if (R.r == 0) { state = 2; return; }
     if (d == 0) pk.qnext_r(g, R.r);
-    else if (d == 1) pk.qnext_t(g, R.t);
+    else if (d == 1) pk.qnext_t(g, R.t, g.st);
     else pk.qnext_p(g, R.p);
   }
 #else

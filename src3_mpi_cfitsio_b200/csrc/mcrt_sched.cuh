@@ -154,18 +154,18 @@ struct Lane {
       else ev = EV_PEEL_NEXT;
       return;
     }
-    const double dt = qn - g.q;
+    const double dt = __dsub_rn(qn, g.q);
     const int64_t ci = pk.cidx(R.r, R.t, R.p);
     const CellRecF c = m.cellsf[ci];
     float opac, absc;
     pk.cell_coefs(c, opac, absc);
     if (!R.peel) {
-      const double dtau = (double)(opac * (float)dt);
-      if (R.tsum + dtau > pk.tau) {
-        const double ds = (pk.tau - R.tsum) / (double)opac;
+      const double dtau = (double)__fmul_rn(opac, (float)dt);
+      if (__dadd_rn(R.tsum, dtau) > pk.tau) {
+        const double ds = __ddiv_rn(__dsub_rn(pk.tau, R.tsum), (double)opac);
         pk.tally_absf(ci, absc, ds);
         if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)ds);
-        g.q = g.q + ds;
+        g.q = __dadd_rn(g.q, ds);
         R.onw = false;
         if (!kStarEvent) packet_from_ray();
         ev = EV_AFTER_WALK;
@@ -173,9 +173,9 @@ struct Lane {
       }
       pk.tally_absf(ci, absc, dt);
       if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)dt);
-      R.tsum = R.tsum + dtau;
+      R.tsum = __dadd_rn(R.tsum, dtau);
     } else {
-      R.tsum = R.tsum + (double)(opac * (float)dt);
+      R.tsum = __dadd_rn(R.tsum, (double)__fmul_rn(opac, (float)dt));
       if (R.tsum > 25.0) { ev = EV_PEEL_NEXT; return; }
     }
     g.q = qn;
@@ -210,7 +210,7 @@ struct Lane {
       if (R.r == 0) { ev = EV_PEEL_NEXT; return; }
     }
     if (d == 0) pk.qnext_r(g, R.r);
-    else if (d == 1) pk.qnext_t(g, R.t);
+    else if (d == 1) pk.qnext_t(g, R.t, g.st);
     else pk.qnext_p(g, R.p);
   }
 

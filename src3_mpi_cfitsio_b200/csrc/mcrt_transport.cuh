@@ -118,15 +118,20 @@ struct Walls {
 //   cone mu:   (c_z + u_z q)^2 = mu^2 (p^2 + q^2) on the nappe sign(z) = sign(mu);
 //   plane A x + B y = 0:  q = -(A c_x + B c_y) / (A u_x + B u_y).
 // Each dimension's next crossing is kept and only the dimension just
-// crossed is solved again, so a crossing costs one sphere root or two cone
-// roots.  The walk state, the cone and plane roots and the opacity sums are
-// FP32; q, p^2 and the sphere roots are FP64 where a wall borders a thin
-// cell (kThinWall), and the cumulative optical depth, its comparison with
-// the sampled tau and the tallies are FP64.
+// crossed is solved again, and the roots of the theta cell's two cones are
+// kept too (a theta crossing shares one wall with the new cell), so a
+// crossing costs one sphere root or one cone root.  The walk state, the
+// cone and plane roots and the opacity sums are FP32.  q and p^2 are FP64,
+// and so is every sphere root: an FP32 square root refined by one Newton
+// step on the FP64 residual (R^2 - p^2 - s^2), accurate to ~1e-14 of the
+// radius, which resolves the disk rim's refined cells (~1.6e-6 of their
+// radius wide).  The cumulative optical depth, its comparison with the
+// sampled tau and the tallies are FP64.
 struct QRay {
   double q, p2, q0;            // current q, squared impact parameter, q of the walk's start point
   double qr, qt, qp;           // next crossing per dimension (r, theta, phi); HUGE_D: none
   float cx, cy, cz, ux, uy, uz, p2f, pabs;
+  float ta1, ta2, tb1, tb2;    // roots of the theta cell's upper (t-1) and lower (t) cone; -inf: none
   int sr, st, sp;              // index step of the pending crossing per dimension
   bool lzpos;                  // the azimuth grows along the ray (L_z > 0)
 };
@@ -634,7 +639,7 @@ struct Packet {
   __device__ __forceinline__ void walk_columns() {
     for (int s = 0; s < m.nslot; ++s) {
       kf(s) = (float)sp.kapd(s);
-      kaf(s) = (float)(sp.kapd(s) * (1.0 - sp.alb(s)));
+      kaf(s) = (float)__dmul_rn(sp.kapd(s), __dsub_rn(1.0, sp.alb(s)));
     }
   }
   // Opacity and thermal absorption coefficient of a cell at the walk's
@@ -646,80 +651,94 @@ struct Packet {
     absc = 0.0f;
     for (int k = 0; k < n; ++k) {
       const int s = cell_slot(c.meta, k);
-      opac = fmaf(kf(s), c.rho[k], opac);
+      opac = __fmaf_rn(kf(s), c.rho[k], opac);
       const int id = cell_id(c.meta, k);
-      if (id < 5 || id > 8) absc = fmaf(kaf(s), c.rho[k], absc);
+      if (id < 5 || id > 8) absc = __fmaf_rn(kaf(s), c.rho[k], absc);
     }
   }
   __device__ __forceinline__ void tally_absf(int64_t ci, float absc, double len) {
-    if (absc > 0.0f) atomicAdd(T.dtauabs + ci, len * (double)absc);
+    if (absc > 0.0f) atomicAdd(T.dtauabs + ci, __dmul_rn(len, (double)absc));
     if (m.iffuv) atomicAdd(T.fuvmean + ci, len * (m.rstar * RSOL) * ifuv / __ldg(m.vcell + ci));
   }
 
   // Next sphere crossing of cell r: the inner wall while the ray still
   // approaches the origin (q < 0) and passes inside it, else the outer wall.
+  // sqrt(R^2 - p^2): an FP32 reciprocal-square-root seed and one Newton step
+  // on the FP64 residual, the same instructions for every wall.
   __device__ __forceinline__ void qnext_r(QRay& g, int r) const {
     const double a2 = __ldg(m.r2arr + r - 1);
     const bool inner = g.q < 0.0 && g.p2 < a2;
-    const int w = inner ? r - 1 : r;
-    const double d = fmax((inner ? a2 : __ldg(m.r2arr + r)) - g.p2, 0.0);
-    const double s = __ldg(m.wall64 + w) ? sqrt(d) : (double)sqrtf((float)d);
+    const double d = fmax(__dsub_rn(inner ? a2 : __ldg(m.r2arr + r), g.p2), 0.0);
+    const float df = (float)d;
+    double s = 0.0;
+    if (df > 0.0f) {
+      const float s0 = __fmul_rn(df, rsqrtf(df));
+      s = (double)s0;
+      s = __dadd_rn(s, (double)__fmul_rn((float)__fma_rn(-s, s, d), __fdividef(0.5f, s0)));
+    }
     g.qr = inner ? -s : s;
     g.sr = inner ? -1 : 1;
   }
 
-  // Roots of cone wall w on its own nappe.  A root within `win` of the
-  // current point counts only if the ray moves towards that wall there
-  // (toward: mu changes toward the wall's mu), which settles the crossings
-  // that FP32 rounding cannot order, such as the wall a walk starts next to
-  // or has just crossed.
-  __device__ __forceinline__ void qcone(const QRay& g, int w, int step, bool toward, float qf, float win, double& best,
-                                        int& st) const {
+  // Roots of cone wall w on its own nappe (-inf: none).
+  __device__ __forceinline__ void cone_roots(const QRay& g, int w, float& q1, float& q2) const {
     const float2 c = __ldg(m.tcone + w);
+    q1 = -HUGE_VALF;
+    q2 = -HUGE_VALF;
     if (c.y > 1.5f) return;                               // pole (tan2arr = 0): never crossed
-    float q1, q2;
     if (c.y < 0.0f) {                                     // the theta = 90 deg plane z = 0
-      if (g.uz == 0.0f) return;
-      q1 = -g.cz / g.uz;
-      q2 = -HUGE_VALF;
-    } else {
-      const float A = fmaf(g.uz, g.uz, -c.y);
-      const float B = g.cz * g.uz;
-      const float D = fmaf(g.p2f, A, g.cz * g.cz);           // discriminant / mu^2
-      if (!(D > 0.0f)) return;
-      const float s = fabsf(c.x) * sqrtf(D);
-      const float den = B >= 0.0f ? -B - s : s - B;         // no cancellation
-      const float C = fmaf(-c.y, g.p2f, g.cz * g.cz);
-      q1 = __fdividef(den, A);
-      q2 = __fdividef(C, den);
-      // a root on the other nappe (z of opposite sign to mu) is not this wall
-      if (fmaf(g.uz, q1, g.cz) * c.x <= 0.0f) q1 = -HUGE_VALF;
-      if (fmaf(g.uz, q2, g.cz) * c.x <= 0.0f) q2 = -HUGE_VALF;
+      if (g.uz != 0.0f) q1 = -__fdividef(g.cz, g.uz);
+      return;
     }
-    const float qq[2] = {q1, q2};
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float qi = qq[i];
-      const bool ok = qi > qf + win || (qi >= qf - win && toward);
-      if (ok && (double)qi < best) { best = fmax((double)qi, g.q); st = step; }
-    }
+    const float A = __fmaf_rn(g.uz, g.uz, -c.y);
+    const float B = __fmul_rn(g.cz, g.uz);
+    const float cz2 = __fmul_rn(g.cz, g.cz);
+    const float D = __fmaf_rn(g.p2f, A, cz2);             // discriminant / mu^2
+    if (!(D > 0.0f)) return;
+    const float sq = __fmul_rn(fabsf(c.x), __fmul_rn(D, rsqrtf(D)));
+    const float den = B >= 0.0f ? __fsub_rn(-B, sq) : __fsub_rn(sq, B);   // no cancellation
+    const float C = __fmaf_rn(-c.y, g.p2f, cz2);
+    const float r1 = __fdividef(den, A), r2 = __fdividef(C, den);
+    // a root on the other nappe (z of opposite sign to mu) is not this wall
+    if (__fmul_rn(__fmaf_rn(g.uz, r1, g.cz), c.x) > 0.0f) q1 = r1;
+    if (__fmul_rn(__fmaf_rn(g.uz, r2, g.cz), c.x) > 0.0f) q2 = r2;
   }
 
-  // Next cone crossing of cell t (walls t-1 above, t below in theta).
-  __device__ __forceinline__ void qnext_t(QRay& g, int t) const {
-    g.qt = HUGE_D;
-    g.st = 0;
-    if (m.ntg <= 2) return;
+  // Next cone crossing from the cached roots.  A root within `win` of the
+  // current point counts only if the ray moves towards that wall there
+  // (mu grows toward the upper wall), which settles the crossings that FP32
+  // rounding cannot order, such as the wall a walk starts next to or has
+  // just crossed.
+  __device__ __forceinline__ void qpick_t(QRay& g) const {
     const float qf = (float)g.q;
-    const float win = 1.0e-5f * (fabsf(qf) + g.pabs);
-    // d mu / dq has the sign of u_z p^2 - c_z q
-    const float dmu = fmaf(g.uz, g.p2f, -g.cz * qf);
-    double best = HUGE_D;
+    const float win = __fmul_rn(1.0e-5f, __fadd_rn(fabsf(qf), g.pabs));
+    const float dmu = __fmaf_rn(g.uz, g.p2f, -__fmul_rn(g.cz, qf));   // d mu / dq has this sign
+    const bool up = dmu > 0.0f, down = dmu < 0.0f;
+    float best = HUGE_VALF;
     int st = 0;
-    qcone(g, t - 1, -1, dmu > 0.0f, qf, win, best, st);
-    qcone(g, t, 1, dmu < 0.0f, qf, win, best, st);
-    g.qt = best;
+    auto take = [&](float qi, bool toward, int step) {
+      const bool ok = qi > qf + win || (qi >= qf - win && toward);
+      if (ok && qi < best) { best = qi; st = step; }
+    };
+    take(g.ta1, up, -1);
+    take(g.ta2, up, -1);
+    take(g.tb1, down, 1);
+    take(g.tb2, down, 1);
+    g.qt = st != 0 ? fmax((double)best, g.q) : HUGE_D;
     g.st = st;
+  }
+
+  // After a theta crossing into cell t by `step`: the wall just crossed is
+  // one of the new cell's walls (its roots are kept), the other is solved.
+  __device__ __forceinline__ void qnext_t(QRay& g, int t, int step) const {
+    if (step > 0) {
+      g.ta1 = g.tb1; g.ta2 = g.tb2;
+      cone_roots(g, t, g.tb1, g.tb2);
+    } else {
+      g.tb1 = g.ta1; g.tb2 = g.ta2;
+      cone_roots(g, t - 1, g.ta1, g.ta2);
+    }
+    qpick_t(g);
   }
 
   // Next phi-plane crossing of cell p: the azimuth moves monotonically with
@@ -730,11 +749,11 @@ struct Packet {
     if (m.npg <= 2 || m.ntg <= 2) return;
     const int w = g.lzpos ? p : p - 1;
     const float2 ab = __ldg(m.pplane + w);
-    const float den = fmaf(ab.x, g.ux, ab.y * g.uy);
+    const float den = __fmaf_rn(ab.x, g.ux, __fmul_rn(ab.y, g.uy));
     if (den == 0.0f) return;
-    const float qi = -__fdividef(fmaf(ab.x, g.cx, ab.y * g.cy), den);
+    const float qi = -__fdividef(__fmaf_rn(ab.x, g.cx, __fmul_rn(ab.y, g.cy)), den);
     const float qf = (float)g.q;
-    const float win = 1.0e-5f * (fabsf(qf) + g.pabs);
+    const float win = __fmul_rn(1.0e-5f, __fadd_rn(fabsf(qf), g.pabs));
     if (qi >= qf - win) {
       g.qp = fmax((double)qi, g.q);
       g.sp = g.lzpos ? 1 : -1;
@@ -742,17 +761,18 @@ struct Packet {
   }
 
   // The point of the walk at q: start + (q - q0) u, and its r^2 and r.
-  // Not inlined: every schedule forms the packet position with this one
-  // compiled sequence, so the schedules stay bitwise equal.
-  __device__ __noinline__ static void qpos(double x0, double y0, double z0, double vx, double vy, double vz,
-                                           double q, double q0, double& x, double& y, double& z, double& rs,
-                                           double& rt) {
-    const double d = q - q0;
-    x = x0 + d * vx;
-    y = y0 + d * vy;
-    z = z0 + d * vz;
-    rs = x * x + y * y + z * z;
-    rt = sqrt(rs);
+  // Written with explicit rounding intrinsics, which the compiler neither
+  // contracts nor reassociates, so every schedule that inlines it forms the
+  // same bits (the FP32 walk helpers below are written the same way).
+  __device__ __forceinline__ static void qpos(double x0, double y0, double z0, double vx, double vy, double vz,
+                                              double q, double q0, double& x, double& y, double& z, double& rs,
+                                              double& rt) {
+    const double d = __dsub_rn(q, q0);
+    x = __fma_rn(d, vx, x0);
+    y = __fma_rn(d, vy, y0);
+    z = __fma_rn(d, vz, z0);
+    rs = __fma_rn(z, z, __fma_rn(y, y, __dmul_rn(x, x)));
+    rt = __dsqrt_rn(rs);
   }
 
   // Set up the walk of the ray from (x,y,z) along (vx,vy,vz) in cell
@@ -760,18 +780,18 @@ struct Packet {
   // walk: an index that disagrees with the start point beyond 1e-4 of the
   // cell is re-located; a start point outside the grid is clamped to its
   // first or last cell (counted as a reset).
-  __device__ __noinline__ void qbegin(QRay& g, double x, double y, double z, double vx, double vy, double vz, int& r,
-                                      int& t, int& p) {
-    const double q0 = x * vx + y * vy + z * vz;
-    const double cx = x - q0 * vx, cy = y - q0 * vy, cz = z - q0 * vz;
+  __device__ __forceinline__ void qbegin(QRay& g, double x, double y, double z, double vx, double vy, double vz, int& r,
+                                         int& t, int& p) {
+    const double q0 = __fma_rn(z, vz, __fma_rn(y, vy, __dmul_rn(x, vx)));
+    const double cx = __fma_rn(-q0, vx, x), cy = __fma_rn(-q0, vy, y), cz = __fma_rn(-q0, vz, z);
     g.q = q0;
     g.q0 = q0;
-    g.p2 = cx * cx + cy * cy + cz * cz;
+    g.p2 = __fma_rn(cz, cz, __fma_rn(cy, cy, __dmul_rn(cx, cx)));
     g.p2f = (float)g.p2;
-    g.pabs = sqrtf(g.p2f);
+    g.pabs = __fsqrt_rn(g.p2f);
     g.cx = (float)cx; g.cy = (float)cy; g.cz = (float)cz;
     g.ux = (float)vx; g.uy = (float)vy; g.uz = (float)vz;
-    g.lzpos = x * vy - y * vx > 0.0;
+    g.lzpos = __fma_rn(x, vy, -__dmul_rn(y, vx)) > 0.0;
     const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
     const double tol = 1.0e-4;
     const double rs = x * x + y * y + z * z;
@@ -807,7 +827,14 @@ struct Packet {
     }
     if (moved) ++c_reset;
     qnext_r(g, r);
-    qnext_t(g, t);
+    if (ntg > 2) {
+      cone_roots(g, t - 1, g.ta1, g.ta2);
+      cone_roots(g, t, g.tb1, g.tb2);
+      qpick_t(g);
+    } else {
+      g.qt = HUGE_D;
+      g.st = 0;
+    }
     qnext_p(g, p);
   }
 #endif

@@ -155,7 +155,7 @@ __device__ __forceinline__ void wave_load_qwalk(Lane& L, const WaveRec& R, int n
   for (int s = 0; s < nslot; ++s) {
     const double kd = R.spec[s];
     k.kf(s) = (float)kd;
-    k.kaf(s) = (float)(kd * (1.0 - R.spec[kMaxSlot + s]));
+    k.kaf(s) = (float)__dmul_rn(kd, __dsub_rn(1.0, R.spec[kMaxSlot + s]));
   }
   k.qbegin(y.g, R.x, R.y, R.z, R.vx, R.vy, R.vz, y.r, y.t, y.p);
 }
