@@ -163,12 +163,23 @@ def bench_clumpy(args, dev):
     eng.flush_l2()
     eng.run(n, iteration=2, ipeel=1)
     ms = eng.kernel_ms()
+    ws = eng.wave_stats()
     c = eng.download(images=False).counters()
+    # the FP64 build on a smaller sample of the same iteration
+    n64 = max(n // 5, 1000)
+    eng.set_precision("fp64")
+    eng.reset_tallies()
+    eng.flush_l2()
+    eng.run(n, 1, n64, iteration=2, ipeel=1)
+    ms64 = eng.kernel_ms()
     eng.close()
     return {"workload": "3-D clumpy (nr=200, ntheta=199, nphi=64; fractal dim 2.6, 50% mass in clumps), tabulated "
                         "Mueller matrices, 201x201 images x 4 Stokes x 20 wavelengths x 20 inclinations, peel-off on",
             "packets": n, "precision": "mixed", "packets_per_s": n / (ms / 1e3),
             "seconds_for_1e9": 1e9 / (n / (ms / 1e3)),
+            "kernels_ms": {k: ws[f"{k}_ms"] for k in ("walk", "event", "tail", "peel")},
+            "fp64_packets": n64, "fp64_packets_per_s": n64 / (ms64 / 1e3),
+            "mixed_over_fp64": (n / ms) / (n64 / ms64),
             "crossings_per_packet": c["crossings"] / n, "peel_crossings_per_packet": c["peel_cross"] / n}
 
 

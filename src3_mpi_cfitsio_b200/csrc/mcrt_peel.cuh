@@ -130,6 +130,7 @@ struct PeelLane {
       if (R.t < 1 || R.t > m.ntg - 1) { state = 2; return; }   // no cell beyond a non-pole theta wall
     } else {
       R.p += g.sp;
+      ++g.nphi;
       if (R.p == 0) R.p = m.npg - 1;
       if (R.p == m.npg) R.p = 1;
     }

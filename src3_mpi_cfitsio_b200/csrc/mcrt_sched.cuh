@@ -191,6 +191,7 @@ struct Lane {
       }
     } else {
       R.p += g.sp;
+      ++g.nphi;
       if (R.p == 0) R.p = m.npg - 1;
       if (R.p == m.npg) R.p = 1;
     }

@@ -133,6 +133,7 @@ struct QRay {
   float cx, cy, cz, ux, uy, uz, p2f, pabs;
   float ta1, ta2, tb1, tb2;    // roots of the theta cell's upper (t-1) and lower (t) cone; -inf: none
   int sr, st, sp;              // index step of the pending crossing per dimension
+  int nphi;                    // phi crossings of this walk (a line turns by less than pi)
   bool lzpos;                  // the azimuth grows along the ray (L_z > 0)
 };
 #endif
@@ -741,23 +742,27 @@ struct Packet {
     qpick_t(g);
   }
 
-  // Next phi-plane crossing of cell p: the azimuth moves monotonically with
-  // the sign of L_z = c_x u_y - c_y u_x, so only the wall ahead is solved.
+  // Next phi-plane crossing of cell p.  A line's azimuth sweeps
+  // monotonically (the sense of L_z = c_x u_y - c_y u_x) toward the azimuth
+  // of its direction, which it reaches at q -> +inf; so the wall ahead (p,
+  // or p-1 when the azimuth falls) is crossed exactly when the direction's
+  // azimuth lies beyond it, the sign of A u_x + B u_y with A = sin(phi_w),
+  // B = -cos(phi_w).  The decision needs no position, so it holds for rays
+  // that pass the z axis closer than FP32 resolves (where every plane's root
+  // is within rounding of the current point); the root only orders the
+  // crossing among the other faces.  A line turns by less than pi about the
+  // axis, so a walk takes at most one turn of crossings.
   __device__ __forceinline__ void qnext_p(QRay& g, int p) const {
     g.qp = HUGE_D;
     g.sp = 0;
-    if (m.npg <= 2 || m.ntg <= 2) return;
+    if (m.npg <= 2 || m.ntg <= 2 || g.nphi >= m.npg) return;
     const int w = g.lzpos ? p : p - 1;
     const float2 ab = __ldg(m.pplane + w);
     const float den = __fmaf_rn(ab.x, g.ux, __fmul_rn(ab.y, g.uy));
-    if (den == 0.0f) return;
+    if (!(g.lzpos ? den < 0.0f : den > 0.0f)) return;
     const float qi = -__fdividef(__fmaf_rn(ab.x, g.cx, __fmul_rn(ab.y, g.cy)), den);
-    const float qf = (float)g.q;
-    const float win = __fmul_rn(1.0e-5f, __fadd_rn(fabsf(qf), g.pabs));
-    if (qi >= qf - win) {
-      g.qp = fmax((double)qi, g.q);
-      g.sp = g.lzpos ? 1 : -1;
-    }
+    g.qp = fmax((double)qi, g.q);
+    g.sp = g.lzpos ? 1 : -1;
   }
 
   // The point of the walk at q: start + (q - q0) u, and its r^2 and r.
@@ -791,7 +796,10 @@ struct Packet {
     g.pabs = __fsqrt_rn(g.p2f);
     g.cx = (float)cx; g.cy = (float)cy; g.cz = (float)cz;
     g.ux = (float)vx; g.uy = (float)vy; g.uz = (float)vz;
-    g.lzpos = __fma_rn(x, vy, -__dmul_rn(y, vx)) > 0.0;
+    // the sense of rotation of the FP32 line the roots are solved on: its
+    // L_z from the FP32 values, exact in FP64 (a product of two floats is)
+    g.lzpos = __dsub_rn(__dmul_rn((double)g.cx, (double)g.uy), __dmul_rn((double)g.cy, (double)g.ux)) > 0.0;
+    g.nphi = 0;
     const int nrg = m.nrg, ntg = m.ntg, npg = m.npg;
     const double tol = 1.0e-4;
     const double rs = x * x + y * y + z * z;

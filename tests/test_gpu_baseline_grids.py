@@ -154,19 +154,20 @@ def test_mixed_vs_fp64_chi2_with_independent_seeds(bench2d):
 
 
 def test_mixed_vs_fp64_temperatures_within_half_a_percent(bench2d):
-    """Cell temperatures after tfinal from 4e7-packet iterations with
-    independent streams: in cells with >= 2e4 absorptions (Monte Carlo
-    error of T ~0.15 % per run) the mixed build's temperatures are within
+    """Cell temperatures after tfinal from 1e8-packet iterations with
+    independent streams: in cells with >= 5e4 absorptions (Monte Carlo
+    error of T ~0.1 % per run) the mixed build's temperatures are within
     0.5 % of the FP64 build's in 95 % of the cells, unbiased to 0.05 %, and
     spread no wider than FP64 against itself."""
     m = bench2d
-    a, ta, _ = _run(m, "fp64", 40_000_000, SEEDS[0], 0)
-    b, tb, _ = _run(m, "fp64", 40_000_000, SEEDS[1], 0)
-    c, tc, _ = _run(m, "mixed", 40_000_000, SEEDS[2], 0)
-    good = (a["nabs"] >= 20000) & (c["nabs"] >= 20000) & (ta > 2.0 / 11605.0)
+    a, ta, _ = _run(m, "fp64", 100_000_000, SEEDS[0], 0)
+    b, tb, _ = _run(m, "fp64", 100_000_000, SEEDS[1], 0)
+    c, tc, _ = _run(m, "mixed", 100_000_000, SEEDS[2], 0)
+    good = (a["nabs"] >= 50000) & (c["nabs"] >= 50000) & (ta > 2.0 / 11605.0)
     assert good.sum() > 500, good.sum()
-    rel_mix = tc[good] / ta[good] - 1.0
-    rel_ctl = tb[good] / ta[good] - 1.0
-    assert np.quantile(np.abs(rel_mix), 0.95) <= 0.005, np.quantile(np.abs(rel_mix), 0.95)
-    assert abs(np.median(rel_mix)) <= 5e-4, np.median(rel_mix)
-    assert np.quantile(np.abs(rel_mix), 0.9) <= 1.3 * np.quantile(np.abs(rel_ctl), 0.9) + 2e-4
+    rel_mix = np.abs(tc[good] / ta[good] - 1.0)
+    rel_ctl = np.abs(tb[good] / ta[good] - 1.0)
+    q95m, q95c = np.quantile(rel_mix, 0.95), np.quantile(rel_ctl, 0.95)
+    assert q95m <= 0.005, (q95m, q95c, good.sum())
+    assert abs(np.median(tc[good] / ta[good] - 1.0)) <= 5e-4
+    assert q95m <= 1.3 * q95c + 2e-4, (q95m, q95c)
