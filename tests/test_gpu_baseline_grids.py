@@ -66,8 +66,10 @@ def test_fp64_event_for_event_on_the_benchmark_grid(bench2d, oracle_mod, ipeel, 
     b = to.shaped("nums")[..., 0].sum(axis=(1, 2, 3))
     assert np.all(np.abs(a - b) <= 5 * np.sqrt(np.maximum(b, 1)) + 5)
     if ipeel:
+        # every event adds 10 inclinations x 3 components to numt, so its
+        # Monte Carlo spread (from the diffusion packets) is far above Poisson
         x, y = tg["numt"].astype(np.float64), to["numt"].astype(np.float64)
-        assert abs(x.sum() - y.sum()) <= 5 * np.sqrt(y.sum()) + 5
+        assert abs(x.sum() - y.sum()) <= 0.05 * y.sum()
 
 
 def test_fp64_event_for_event_on_the_clumpy_grid(oracle_mod):
