@@ -755,14 +755,27 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
     j1 = mulmod_h(j1, j1, 2147483563);
     j2 = mulmod_h(j2, j2, 2147483399);
   }
+  // digit tables A^(j * 2^(14 c)), A = a^(2^30): [gen][c][j]
+  jump.resize(128 + 6 * (size_t)kJumpDigit);
+  for (int gen = 0; gen < 2; ++gen) {
+    const int64_t mod = gen == 0 ? 2147483563 : 2147483399;
+    int64_t base = jump[64 * gen];                       // A
+    int64_t* T = jump.data() + 128 + (size_t)gen * 3 * kJumpDigit;
+    for (int cdig = 0; cdig < 3; ++cdig) {
+      int64_t* Tc = T + (size_t)cdig * kJumpDigit;
+      Tc[0] = 1;
+      for (int j = 1; j < kJumpDigit; ++j) Tc[j] = mulmod_h(Tc[j - 1], base, mod);
+      base = mulmod_h(Tc[kJumpDigit - 1], base, mod);   // A^(2^(14 (c+1)))
+    }
+  }
   int rc;
   if (ctx->have_tables) { dfree(ctx, ctx->d_tabs); dfree(ctx, ctx->d_nlambda); dfree(ctx, ctx->d_jump); }
   if ((rc = dalloc(ctx, &ctx->d_tabs, tab.size()))) return rc;
   if ((rc = dalloc(ctx, &ctx->d_nlambda, c.nopac))) return rc;
-  if ((rc = dalloc(ctx, &ctx->d_jump, 128))) return rc;
+  if ((rc = dalloc(ctx, &ctx->d_jump, jump.size()))) return rc;
   CK(cudaMemcpyAsync(ctx->d_tabs, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_nlambda, t->nlambda, c.nopac * 4, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_jump, jump.data(), 128 * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_jump, jump.data(), jump.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   DevModel& m = ctx->dm;
   const double* b = ctx->d_tabs;
@@ -784,6 +797,8 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;
+  m.jdig1 = ctx->d_jump + 128;
+  m.jdig2 = ctx->d_jump + 128 + 3 * kJumpDigit;
   // species that share a wavelength column (same length, same values bit for
   // bit) share opacset's bracket search
   ctx->species_grid.assign(c.nopac, 0);

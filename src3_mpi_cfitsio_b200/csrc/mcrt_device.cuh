@@ -23,6 +23,8 @@ namespace mcrt {
 constexpr int kMaxComp = 3;   // non-zero density components per cell
 constexpr int kMaxSlot = 8;   // distinct opacity species referenced by the grid
 constexpr int kTransportBlock = 128;  // threads per transport block
+constexpr int kJumpBits = 14;         // block-index digit of the jump tables
+constexpr int kJumpDigit = 1 << kJumpBits;
 
 struct __align__(16) CellRec {
   double rho[kMaxComp];       // densarr of the non-zero components, id order
@@ -98,8 +100,12 @@ struct DevModel {
   const double *inczeta;                     // [MCRT_IZMAX]
   // observer
   const double *aperture2, *u, *sini, *coste, *sinte, *cospe, *sinpe;
-  // random-number jump tables: a^(2^30 * 2^k) mod m, k = 0..63
+  // random-number jump tables: a^(2^30 * 2^k) mod m, k = 0..63; and per
+  // generator three digit tables A^(j * 2^(14 c)), A = a^(2^30), c = 0..2,
+  // j < 2^14 ([3][kJumpDigit]), so a block index below 2^42 jumps in three
+  // multiplications
   const int64_t *jump1, *jump2;
+  const int64_t *jdig1, *jdig2;
 };
 
 // One peel-off request: the packet's state at an emission, scattering or

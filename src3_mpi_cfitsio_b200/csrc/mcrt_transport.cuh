@@ -54,14 +54,38 @@ __device__ __forceinline__ int64_t mulmod(int64_t a, int64_t b, int64_t m) {
   return (int64_t)(((unsigned long long)a * (unsigned long long)b) % (unsigned long long)m);
 }
 
-// Block `b` of the generator seeded (g1,g2): a^(b*2^30) * g mod m via the
-// precomputed squares a^(2^30*2^k) (reinitialize_current_generator(1) b times).
+// a*b mod m for 0 <= a, b < m < 2^31, exactly: the FP64 quotient estimate is
+// within one of floor(a*b/m) (its relative error is ~3*2^-53 of a value
+// below 2^31), and the remainder is corrected in exact 64-bit integers.
+__device__ __forceinline__ int64_t mulmod31(int64_t a, int64_t b, int64_t mod, double inv) {
+  const int64_t q = (int64_t)(__dmul_rn(__dmul_rn((double)a, (double)b), inv));
+  int64_t r = a * b - q * mod;
+  if (r < 0) r += mod;
+  else if (r >= mod) r -= mod;
+  return r;
+}
+
+// Block `b` of the generator seeded (g1,g2): a^(b*2^30) * g mod m
+// (reinitialize_current_generator(1) b times).  Below 2^42 blocks: the
+// three 14-bit digits of b index the tables A^(j*2^(14c)); otherwise the
+// binary powers a^(2^30*2^k).  Exact modular arithmetic either way.
 __device__ __forceinline__ Rng rng_block(const DevModel& m, int32_t g1, int32_t g2, int64_t b) {
+  constexpr int64_t M1 = 2147483563, M2 = 2147483399;
   int64_t r1 = g1, r2 = g2;
-  for (int k = 0; b != 0; ++k, b >>= 1) {
-    if (b & 1) {
-      r1 = mulmod(r1, m.jump1[k], 2147483563);
-      r2 = mulmod(r2, m.jump2[k], 2147483399);
+  if (m.jdig1 && b >= 0 && b < ((int64_t)1 << (3 * kJumpBits))) {
+    const double i1 = 1.0 / (double)M1, i2 = 1.0 / (double)M2;
+    const int d0 = (int)(b & (kJumpDigit - 1)), d1 = (int)((b >> kJumpBits) & (kJumpDigit - 1));
+    const int d2 = (int)(b >> (2 * kJumpBits));
+    const int64_t a0 = __ldg(m.jdig1 + d0), a1 = __ldg(m.jdig1 + kJumpDigit + d1), a2 = __ldg(m.jdig1 + 2 * kJumpDigit + d2);
+    const int64_t c0 = __ldg(m.jdig2 + d0), c1 = __ldg(m.jdig2 + kJumpDigit + d1), c2 = __ldg(m.jdig2 + 2 * kJumpDigit + d2);
+    r1 = mulmod31(mulmod31(mulmod31(r1, a0, M1, i1), a1, M1, i1), a2, M1, i1);
+    r2 = mulmod31(mulmod31(mulmod31(r2, c0, M2, i2), c1, M2, i2), c2, M2, i2);
+  } else {
+    for (int k = 0; b != 0; ++k, b >>= 1) {
+      if (b & 1) {
+        r1 = mulmod(r1, m.jump1[k], M1);
+        r2 = mulmod(r2, m.jump2[k], M2);
+      }
     }
   }
   Rng r;
