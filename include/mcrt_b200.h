@@ -40,8 +40,8 @@ extern "C" {
 #define MCRT_ERR_ARG          1   /* bad argument / inconsistent sizes          */
 #define MCRT_ERR_CUDA         2   /* CUDA runtime error (message has details)    */
 #define MCRT_ERR_UNSUPPORTED  3   /* model feature outside the built scope       */
-#define MCRT_ERR_GEOM         4   /* packets lost to a geometry failure          */
-#define MCRT_ERR_TIMEOUT      5   /* device watchdog ended a launch              */
+#define MCRT_ERR_GEOM         4   /* packets lost to geometry failures (mcrt_set_limits) */
+#define MCRT_ERR_TIMEOUT      5   /* wave-loop watchdog ended a run (mcrt_set_limits)    */
 #define MCRT_ERR_STATE        6   /* call order violated (e.g. run before upload)*/
 
 /* ---- fixed reference dimensions ---- */
@@ -217,6 +217,34 @@ int mcrt_create(const mcrt_config *cfg, int device, mcrt_ctx **out);
 /* Upload the grid/model arrays that gridset fills every iteration
  * (newdisktherm_5_fuv.f90:89 -> gridset_5_model13new.f90). */
 int mcrt_upload_grid(mcrt_ctx *ctx, const mcrt_grid *grid);
+
+/* Check a grid before it is uploaded, on the host only (no device, no
+ * context): the walls finite and increasing, every density finite and
+ * non-negative, every temperature finite and non-negative, every cell with
+ * dust of finite positive volume.  The reference reads these from its
+ * parameter files and would run on with a NaN (gridset_5_model13new.f90);
+ * here a bad value is refused with MCRT_ERR_ARG and the first offending
+ * entry named in `msg` (msg_len bytes, may be NULL).  mcrt_upload_grid
+ * runs the same check before any CUDA call. */
+int mcrt_check_grid(const mcrt_config *cfg, const mcrt_grid *grid, char *msg, int32_t msg_len);
+
+/* Watchdogs of the packet loop (no reference counterpart: the reference
+ * stops the program on a geometry failure, testgrid.f90 / tauint, and has
+ * no time limit).
+ *   walk_crossings: crossings of one walk after which the walk is given up
+ *                   and its packet dropped as a geometry failure (<= 0:
+ *                   the default 5e7);
+ *   waves:          walk/event launch pairs of one wavefront loop after
+ *                   which mcrt_run_iteration stops and returns
+ *                   MCRT_ERR_TIMEOUT, abandoning the packets in flight
+ *                   (<= 0: the default 4e8); the context stays usable;
+ *   geom_fraction:  mcrt_run_iteration returns MCRT_ERR_GEOM when more
+ *                   than this fraction of its packets was lost to
+ *                   geometry failures (default 1e-6; < 0: never).  The
+ *                   tallies hold every other packet and the counter
+ *                   MCRT_C_GEOM_FAIL the losses.
+ * Takes effect at the next run. */
+int mcrt_set_limits(mcrt_ctx *ctx, int64_t walk_crossings, int64_t waves, double geom_fraction);
 
 /* Upload dust, atmosphere and observer tables (dustinit dust_5.f90:345-504,
  * atmosinit starbarb_2.f90:3-122, setup.f90:115-195). */

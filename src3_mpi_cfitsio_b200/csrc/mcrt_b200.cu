@@ -139,6 +139,11 @@ struct mcrt_ctx {
   std::vector<double> h_rarr;
   std::vector<int32_t> species_grid;  // per species: first species with a bit-identical wavelength column
   double* noalloc_scratch = nullptr;   // device address of g_tfinal_scratch (mcrt_update_temperature_noalloc)
+  // watchdogs (mcrt_set_limits)
+  int64_t walk_limit = 50000000;       // crossings of one walk before it is given up as a geometry failure
+  int64_t wave_limit = 400000000;      // waves of one wavefront loop before the call returns MCRT_ERR_TIMEOUT
+  double geom_fraction = 1.0e-6;       // lost packets (geometry failures) per packet that make a run return MCRT_ERR_GEOM
+  unsigned long long* h_geom = nullptr;   // pinned: the geometry-failure counter before and after a run
 };
 
 namespace {
@@ -489,6 +494,7 @@ void mcrt_destroy(mcrt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->h_wctl) cudaFreeHost(ctx->h_wctl);
+  if (ctx->h_geom) cudaFreeHost(ctx->h_geom);
   for (auto& p : ctx->kt_ev)
     for (auto& e : p) if (e) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -529,14 +535,16 @@ int mcrt_set_wave_pool(mcrt_ctx* ctx, int64_t slots, int64_t peel_jobs, int64_t 
 
 int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   if (!ctx || !g) return MCRT_ERR_ARG;
+  {
+    char msg[256];
+    const int rc = mcrt_check_grid(&ctx->cfg, g, msg, (int32_t)sizeof msg);
+    if (rc) return fail(ctx, rc, "mcrt_upload_grid: %s", msg);
+  }
   ++ctx->uploads;
   CK(cudaSetDevice(ctx->device));
   const mcrt_config& c = ctx->cfg;
   const int nrg = c.nrg, ntg = c.ntg, npg = c.npg;
   const int64_t ncell = ctx->ncell;
-  if (!g->rarr || !g->r2arr || !g->thetarr || !g->costarr || !g->tan2arr || !g->phiarr || !g->aarr || !g->barr ||
-      !g->densarr || !g->findopac || !g->diffus || !g->tdust || !g->vcell || !g->sintarr)
-    return fail(ctx, MCRT_ERR_ARG, "mcrt_upload_grid: missing array");
   // transport layout: one CellRec per cell with the non-zero components
   std::vector<CellRec> cells(ncell);
   std::vector<int> slot_species;
@@ -681,6 +689,61 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   m.nslot = (int)slot_species.size();
   for (int s = 0; s < kMaxSlot; ++s) m.slot_species[s] = s < m.nslot ? slot_species[s] : 1;
   ctx->have_grid = true;
+  return MCRT_OK;
+}
+
+int mcrt_check_grid(const mcrt_config* c, const mcrt_grid* g, char* msg, int32_t msg_len) {
+  auto bad = [&](int code, const char* fmt, auto... a) {
+    if (msg && msg_len > 0) snprintf(msg, (size_t)msg_len, fmt, a...);
+    return code;
+  };
+  if (msg && msg_len > 0) msg[0] = 0;
+  if (!c || !g) return bad(MCRT_ERR_ARG, "missing config or grid");
+  const int nrg = c->nrg, ntg = c->ntg, npg = c->npg;
+  if (nrg < 3 || ntg < 2 || npg < 2) return bad(MCRT_ERR_ARG, "grid of %d x %d x %d walls is too small", nrg, ntg, npg);
+  if (!g->rarr || !g->r2arr || !g->thetarr || !g->costarr || !g->tan2arr || !g->phiarr || !g->aarr || !g->barr ||
+      !g->densarr || !g->findopac || !g->diffus || !g->tdust || !g->vcell || !g->sintarr)
+    return bad(MCRT_ERR_ARG, "missing array");
+  for (int i = 0; i < nrg; ++i) {
+    if (!(std::isfinite(g->rarr[i]) && g->rarr[i] > 0.0) || !(std::isfinite(g->r2arr[i])))
+      return bad(MCRT_ERR_ARG, "rarr(%d) = %g is not a finite positive radius", i + 1, g->rarr[i]);
+    if (i > 0 && !(g->rarr[i] > g->rarr[i - 1])) return bad(MCRT_ERR_ARG, "rarr is not increasing at %d", i + 1);
+  }
+  for (int i = 0; i < ntg; ++i) {
+    if (!(std::isfinite(g->thetarr[i]) && std::isfinite(g->costarr[i]) && std::isfinite(g->tan2arr[i])))
+      return bad(MCRT_ERR_ARG, "theta wall %d is not finite", i + 1);
+    if (i > 0 && !(g->thetarr[i] > g->thetarr[i - 1])) return bad(MCRT_ERR_ARG, "thetarr is not increasing at %d", i + 1);
+  }
+  for (int i = 0; i < npg; ++i) {
+    if (!(std::isfinite(g->phiarr[i]) && std::isfinite(g->aarr[i]) && std::isfinite(g->barr[i])))
+      return bad(MCRT_ERR_ARG, "phi wall %d is not finite", i + 1);
+    if (i > 0 && !(g->phiarr[i] > g->phiarr[i - 1])) return bad(MCRT_ERR_ARG, "phiarr is not increasing at %d", i + 1);
+  }
+  const int64_t ncell = (int64_t)nrg * ntg * npg;
+  for (int64_t k = 0; k < ncell; ++k) {
+    bool dust = false;
+    for (int id = 0; id < MCRT_NDG2; ++id) {
+      const double rho = g->densarr[k + ncell * id];
+      if (!(std::isfinite(rho) && rho >= 0.0))
+        return bad(MCRT_ERR_ARG, "densarr(cell %lld, component %d) = %g is not a finite non-negative density",
+                   (long long)k + 1, id + 1, rho);
+      dust = dust || rho > 0.0;
+    }
+    if (!(std::isfinite(g->tdust[k]) && g->tdust[k] >= 0.0))
+      return bad(MCRT_ERR_ARG, "tdust(cell %lld) = %g is not a finite non-negative temperature", (long long)k + 1,
+                 g->tdust[k]);
+    if (!std::isfinite(g->vcell[k]) || (dust && !(g->vcell[k] > 0.0)))
+      return bad(MCRT_ERR_ARG, "vcell(cell %lld) = %g: a cell with dust needs a finite positive volume", (long long)k + 1,
+                 g->vcell[k]);
+  }
+  return MCRT_OK;
+}
+
+int mcrt_set_limits(mcrt_ctx* ctx, int64_t walk_crossings, int64_t waves, double geom_fraction) {
+  if (!ctx) return MCRT_ERR_ARG;
+  ctx->walk_limit = walk_crossings > 0 ? walk_crossings : 50000000;
+  ctx->wave_limit = waves > 0 ? waves : 400000000;
+  ctx->geom_fraction = geom_fraction;
   return MCRT_OK;
 }
 
@@ -940,6 +1003,7 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   P.nlog = ctx->nlog;
   P.err = ctx->d_err;
   P.event_batch = ctx->event_batch;
+  P.walk_limit = ctx->walk_limit;
   return MCRT_OK;
 }
 
@@ -1057,6 +1121,9 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "peel-off launch: %s", cudaGetErrorString(e));
     return kt_end(KT_PEEL);
   };
+  if (!ctx->h_geom) CK(cudaHostAlloc((void**)&ctx->h_geom, 2 * sizeof(unsigned long long), cudaHostAllocDefault));
+  CK(cudaMemcpyAsync(ctx->h_geom, ctx->dt.cnt + MCRT_C_GEOM_FAIL, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (wave) {
     // Wavefront loop: event launch (emission / interactions / exits up to
@@ -1084,7 +1151,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     ++launches;
     // every wave advances each live packet by at least one event, and a
     // packet ends after at most 1e8 events (the event watchdog)
-    const int64_t max_waves = 400000000;
+    const int64_t max_waves = ctx->wave_limit;
     int64_t waves = 0;
     // h: n_front, n_back, packets started, peel jobs, walks of this wave, walk crossings so far
     unsigned long long* h = ctx->h_wctl;
@@ -1114,7 +1181,9 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
               h[2], h[3]);
 #endif
       if (live == 0) break;
-      if (waves > max_waves) return fail(ctx, MCRT_ERR_CUDA, "wavefront loop did not finish in %lld waves", (long long)waves);
+      if (waves >= max_waves)                // the packets in flight are abandoned; the context stays usable
+        return fail(ctx, MCRT_ERR_TIMEOUT, "wavefront loop stopped after %lld waves with %llu packets in flight",
+                    (long long)waves, live);
       const bool tail = tail_live > 0 && (int64_t)h[2] >= npk && live <= tail_live;
       if (queue && ((int64_t)h[3] + wave_slots > ctx->job_cap || (tail && h[3] > 0))) {
         CK(cudaMemsetAsync(ctx->d_next + 2, 0, sizeof(unsigned long long), ctx->stream));
@@ -1174,7 +1243,10 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
   add_counters<<<1, 1, 0, ctx->stream>>>(ctx->dt.cnt, (unsigned long long)(wave ? ctx->last_waves : 0),
                                          (unsigned long long)launches);
   CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ctx->h_geom + 1, ctx->dt.cnt + MCRT_C_GEOM_FAIL, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     ctx->stream));
   CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaStreamSynchronize(ctx->stream));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->last_ms = ms;
@@ -1186,6 +1258,13 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     ctx->kt_walk_cross = (int64_t)ctx->h_wctl[5];
   }
   CK(cudaGetLastError());
+  // packets lost to geometry failures (the reference stops the run on one):
+  // the tallies hold every other packet; above the set fraction the call
+  // reports it
+  const unsigned long long lost = ctx->h_geom[1] - ctx->h_geom[0];
+  if (ctx->geom_fraction >= 0.0 && (double)lost > ctx->geom_fraction * (double)npk)
+    return fail(ctx, MCRT_ERR_GEOM, "%llu of %lld packets lost to geometry failures (limit %g per packet)", lost,
+                (long long)npk, ctx->geom_fraction);
   return MCRT_OK;
 }
 

@@ -239,6 +239,7 @@ struct LaunchParams {
   int64_t nlog;
   int64_t log_off;              // log entry of the launch's k-th packet: k + log_off
   int32_t *err;                 // device error flags
+  int64_t walk_limit;           // crossings after which a walk is given up (geometry failure)
   AdjointArgs adj;
 };
 

@@ -107,7 +107,7 @@ struct PeelLane {
     int d = 0;
     if (g.qt < qn) { qn = g.qt; d = 1; }
     if (g.qp < qn) { qn = g.qp; d = 2; }
-    if (!(qn < HUGE_D) || ++steps > 10000000) { state = 2; return; }
+    if (!(qn < HUGE_D) || ++steps > P.walk_limit) { state = 2; return; }
     const float dt = (float)(qn - g.q);
     const int64_t ci = pk.cidx(R.r, R.t, R.p);
     const CellRecF c = m.cellsf[ci];
@@ -152,7 +152,7 @@ struct PeelLane {
     double dt;
     int iface;
     w.next(R.onw, dt, iface);
-    if (dt == HUGE_D || iface < 1 || iface > 6 || ++steps > 10000000) { state = 2; return; }
+    if (dt == HUGE_D || iface < 1 || iface > 6 || ++steps > P.walk_limit) { state = 2; return; }
     const int64_t ci = pk.cidx(R.r, R.t, R.p);
     const CellRec c = m.cells[ci];
     R.tsum = R.tsum + pk.cell_opac(c) * dt;

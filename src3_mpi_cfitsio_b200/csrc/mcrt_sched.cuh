@@ -149,7 +149,7 @@ struct Lane {
     int d = 0;
     if (g.qt < qn) { qn = g.qt; d = 1; }
     if (g.qp < qn) { qn = g.qp; d = 2; }
-    if (!(qn < HUGE_D) || ++ray_steps > 50000000) {
+    if (!(qn < HUGE_D) || ++ray_steps > P.walk_limit) {
       if (!R.peel) { if (!kStarEvent) packet_from_ray(); status = 3; ev = EV_FINISH; }
       else ev = EV_PEEL_NEXT;
       return;
@@ -236,7 +236,7 @@ struct Lane {
     double dt;
     int iface;
     w.next(R.onw, dt, iface);
-    const bool bad = dt == HUGE_D || iface < 1 || iface > 6 || ++ray_steps > 50000000;
+    const bool bad = dt == HUGE_D || iface < 1 || iface > 6 || ++ray_steps > P.walk_limit;
     if (!R.peel) {
       if (bad || dt < 0.0) { packet_from_ray(); status = 3; ev = EV_FINISH; return; }
     } else if (bad) {

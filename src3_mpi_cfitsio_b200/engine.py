@@ -28,7 +28,11 @@ _lib = None
 
 
 class MCRTError(RuntimeError):
-    pass
+    """A failed C-ABI call; `code` is its MCRT_ERR_* return code."""
+
+    def __init__(self, msg: str, code: int | None = None):
+        super().__init__(msg)
+        self.code = code
 
 
 def load_library(path: str = LIB_PATH):
@@ -47,6 +51,10 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_set_schedule.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
     lib.mcrt_set_wave_pool.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64]
     lib.mcrt_reset_tallies.argtypes = [C.c_void_p]
+    lib.mcrt_check_grid.argtypes = [P(abi.Config), P(abi.Grid), C.c_char_p, C.c_int32]
+    lib.mcrt_check_grid.restype = C.c_int
+    lib.mcrt_set_limits.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_double]
+    lib.mcrt_set_limits.restype = C.c_int
     lib.mcrt_run_iteration.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32, C.c_int32]
     lib.mcrt_download_tallies.argtypes = [C.c_void_p, P(abi.Tallies)]
@@ -137,6 +145,16 @@ def setemiss(nudust, kappad, adust, nlambda, ndg: int | None = None, nT: int = 5
     return out
 
 
+def check_grid(model) -> tuple:
+    """mcrt_check_grid on a model's arrays (host only, no device): the
+    return code and the message naming the first bad entry."""
+    lib = load_library()
+    b = abi.Bundle(model)
+    msg = C.create_string_buffer(256)
+    rc = lib.mcrt_check_grid(C.byref(b.config), C.byref(b.grid), msg, 256)
+    return rc, msg.value.decode()
+
+
 def density_params(w) -> "abi.DensityParams":
     """mcrt_density_params of a model.Workload (lengths to stellar radii)."""
     autors = 214.94 / w.rstar
@@ -207,7 +225,7 @@ class Engine:
         if rc != 0:
             c = ctx if ctx is not None else self.ctx
             msg = self.lib.mcrt_last_error(c).decode() if c else ""
-            raise MCRTError(f"mcrt call failed (code {rc}): {msg}")
+            raise MCRTError(f"mcrt call failed (code {rc}): {msg}", rc)
 
     def close(self):
         if getattr(self, "ctx", None):
@@ -236,6 +254,13 @@ class Engine:
             event_batch = 4 if schedule == "wave" else 16
         self._check(self.lib.mcrt_set_schedule(self.ctx, mode, event_batch))
         self.schedule = schedule
+
+    def set_limits(self, walk_crossings: int = 0, waves: int = 0, geom_fraction: float = 1e-6):
+        """Watchdogs (mcrt_set_limits): crossings per walk before a packet is
+        dropped as a geometry failure, waves per wavefront loop before a run
+        returns MCRT_ERR_TIMEOUT, and the fraction of lost packets above
+        which a run returns MCRT_ERR_GEOM (0 / 0: the defaults)."""
+        self._check(self.lib.mcrt_set_limits(self.ctx, walk_crossings, waves, geom_fraction))
 
     def set_wave_pool(self, slots: int = 1 << 21, peel_jobs: int = 0, tail_packets: int = -1):
         """Wavefront schedule sizes: in-flight packet slots, peel-off job

@@ -111,3 +111,38 @@ def test_model_density_and_batch_refuse_bad_input_without_a_gpu():
     assert lib.mcrt_batch_create(None, 2, C.byref(h)) == 1 and not h.value
     arr = (C.c_void_p * 2)(None, None)
     assert lib.mcrt_batch_create(arr, 2, C.byref(h)) == 1 and not h.value
+
+
+def _bad(m, key, index, value):
+    import copy
+    b = copy.deepcopy(m)
+    a = np.array(b.grid[key], dtype=np.float64, copy=True)
+    a[index] = value
+    b.grid[key] = a
+    return b
+
+
+def test_grid_check_accepts_the_models():
+    """mcrt_check_grid runs on the host alone (no device is touched)."""
+    from src3_mpi_cfitsio_b200 import engine, model
+    for m in (model.small_2d(), model.reference_2d_converged()):
+        rc, msg = engine.check_grid(m)
+        assert rc == 0 and msg == ""
+
+
+@pytest.mark.parametrize("key,index,value,word", [("densarr", 5000, float("nan"), "densarr"),
+                                                  ("densarr", 7, -1e-20, "densarr"),
+                                                  ("tdust", 100, float("inf"), "tdust"),
+                                                  ("vcell", None, 0.0, "vcell"),
+                                                  ("rarr", 3, 0.5, "rarr"),
+                                                  ("costarr", 4, float("nan"), "theta")])
+def test_grid_check_refuses_bad_values(key, index, value, word):
+    """A non-finite or negative density or temperature, a dust cell without
+    volume and non-increasing walls are refused with MCRT_ERR_ARG (1) and the
+    entry named, before any CUDA call; the driver's data is not touched."""
+    from src3_mpi_cfitsio_b200 import engine, model
+    m = model.small_2d()
+    if index is None:      # the first cell that holds dust
+        index = int(np.flatnonzero(m.dens4().reshape(-1, m.dens4().shape[-1], order="F").sum(axis=1) > 0)[0])
+    rc, msg = engine.check_grid(_bad(m, key, index, value))
+    assert rc == 1 and word in msg, msg

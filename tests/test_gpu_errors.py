@@ -1,0 +1,88 @@
+"""Error paths of the C ABI, made on the host or by a watchdog setting,
+never by a device fault: a bad grid is refused at upload, packets given up
+by the walk's crossing limit make the run report MCRT_ERR_GEOM, the wave
+loop's limit makes it report MCRT_ERR_TIMEOUT, and after each the context
+runs the next iteration normally."""
+import copy
+
+import numpy as np
+import pytest
+
+from src3_mpi_cfitsio_b200 import model
+
+pytestmark = pytest.mark.gpu
+
+ERR_ARG, ERR_GEOM, ERR_TIMEOUT = 1, 4, 5
+
+
+def _engine(m, precision="fp64"):
+    from src3_mpi_cfitsio_b200.engine import Engine
+    return Engine(m, precision=precision)
+
+
+def _normal_run(eng, n=4000):
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    c = eng.download(images=False).counters()
+    assert c["packets"] == n and c["geom_fail"] == 0
+
+
+def test_upload_refuses_a_nan_density_and_the_context_stays_usable():
+    from src3_mpi_cfitsio_b200.engine import MCRTError
+    m = model.warm(model.small_2d())
+    eng = _engine(m)
+    bad = copy.deepcopy(m)
+    d = bad.grid["densarr"].copy()
+    d[int(np.flatnonzero(d > 0)[10])] = np.nan
+    bad.grid["densarr"] = d
+    eng.model = bad
+    with pytest.raises(MCRTError) as e:
+        eng.upload_grid()
+    assert e.value.code == ERR_ARG and "densarr" in str(e.value)
+    eng.model = m
+    eng.upload_grid()
+    _normal_run(eng)
+    eng.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_walk_limit_reports_lost_packets(precision):
+    """A walk limit of 3 crossings gives up most walks: their packets are
+    dropped and counted, the run returns MCRT_ERR_GEOM with the count, the
+    other packets are tallied, and with the default limits the next run is
+    clean."""
+    from src3_mpi_cfitsio_b200.engine import MCRTError
+    m = model.warm(model.small_2d())
+    eng = _engine(m, precision)
+    n = 4000
+    eng.set_limits(walk_crossings=3)
+    eng.reset_tallies()
+    with pytest.raises(MCRTError) as e:
+        eng.run(n, ipeel=1)
+    assert e.value.code == ERR_GEOM and "geometry" in str(e.value)
+    c = eng.download(images=False).counters()
+    assert c["packets"] == n and 0 < c["geom_fail"] < n
+    assert c["exited"] + c["geom_fail"] + c["killed"] == n
+    eng.set_limits()
+    _normal_run(eng)
+    eng.close()
+
+
+def test_wave_limit_times_out_and_the_next_run_is_whole():
+    """Two waves cannot finish 20000 packets in a 1024-slot pool: the run
+    stops with MCRT_ERR_TIMEOUT, abandoning the packets in flight; the next
+    run of the same context starts a fresh pool and finishes every packet."""
+    from src3_mpi_cfitsio_b200.engine import MCRTError
+    m = model.warm(model.small_2d())
+    eng = _engine(m, "mixed")
+    eng.set_schedule("wave")
+    eng.set_wave_pool(1024, 0, 0)
+    eng.set_limits(waves=2)
+    eng.reset_tallies()
+    with pytest.raises(MCRTError) as e:
+        eng.run(20000, ipeel=0)
+    assert e.value.code == ERR_TIMEOUT and "waves" in str(e.value)
+    assert eng.download(images=False).counters()["packets"] < 20000
+    eng.set_limits()
+    _normal_run(eng, 20000)
+    eng.close()
