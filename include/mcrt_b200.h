@@ -218,6 +218,20 @@ int mcrt_create(const mcrt_config *cfg, int device, mcrt_ctx **out);
  * (newdisktherm_5_fuv.f90:89 -> gridset_5_model13new.f90). */
 int mcrt_upload_grid(mcrt_ctx *ctx, const mcrt_grid *grid);
 
+/* diskflux (flux_test.f90:1-143): the tallies as mcrt_download_tallies
+ * gives them, with the reference's output normalisation applied on the
+ * device in its FP32 order of operations: the SED si..sv divided by
+ * np/nmu/nph/(ltot/lsol), and where nums > 1 the relative errors
+ * si2 = sqrt((si2 - si^2/nums)/(nums-1)*nums)/si + 1/nums (sq2..sv2 the
+ * same without the 1/nums term, relative to si), aveinc/nums (errors 0
+ * elsewhere); with ipeel = 1 the peeled SED ti..tv and the image cubes
+ * divided by np/(ltot/lsol), and where numt > 1 the relative errors
+ * ti2 = sqrt((ti2*numt/ti^2 - 1)/(numt-1)) (0 elsewhere).  As in the
+ * reference a peeled Stokes sum of 0 gives a NaN error.  np is the
+ * iteration's packet count, ltot_lsol the driver's ltot/lsol.  The
+ * filter-band images (image_b_*) are not built. */
+int mcrt_diskflux(mcrt_ctx *ctx, int64_t np, double ltot_lsol, int32_t ipeel, mcrt_tallies *out);
+
 /* Check a grid before it is uploaded, on the host only (no device, no
  * context): the walls finite and increasing, every density finite and
  * non-negative, every temperature finite and non-negative, every cell with

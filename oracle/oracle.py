@@ -203,3 +203,42 @@ def setemiss(nudust, kappad, adust, nlambda, nT: int = 500, nnu: int = 513, ndg:
     out["qsimp_misses"] = int(miss.value)
     return out
 
+
+
+def diskflux(tal, np_total: int, ltot_lsol: float, nmu: int, nph: int, ipeel: int, imcube: bool) -> dict:
+    """diskflux (flux_test.f90:14-82) on the REAL tally arrays of `tal`
+    (float32, as the download gives them), in the reference's FP32 order of
+    operations: numpy float32 arithmetic is IEEE single precision without
+    fused operations, like the Fortran REAL expressions.  Returns the
+    normalised arrays by name."""
+    f32 = np.float32
+    out = {}
+    rnorm = f32(float(np_total) / float(nmu) / float(nph) / ltot_lsol)
+    inorm = f32(float(np_total) / ltot_lsol)
+    si, nums = tal["si"].astype(f32), tal["nums"].astype(f32)
+    big = nums > f32(1.0)
+    with np.errstate(all="ignore"):
+        for k in ("si", "sq", "su", "sv"):
+            x, x2 = tal[k].astype(f32), tal[k + "2"].astype(f32)
+            e = np.sqrt((x2 - x ** 2 / nums) / (nums - f32(1.0)) * nums) / si
+            if k == "si":
+                e = e + f32(1.0) / nums
+            out[k + "2"] = np.where(big, e, f32(0.0)).astype(f32)
+            out[k] = (x / rnorm).astype(f32)
+        ave = tal["aveinc"].astype(f32)
+        out["aveinc"] = np.where(big, ave / nums, ave).astype(f32)
+        out["nums"] = nums
+        if ipeel == 1:
+            numt = tal["numt"].astype(f32)
+            bigt = numt > f32(1.0)
+            for k in ("ti", "tq", "tu", "tv"):
+                x, x2 = tal[k].astype(f32), tal[k + "2"].astype(f32)
+                e = np.sqrt((x2 * numt / x ** 2 - f32(1.0)) / (numt - f32(1.0)))
+                out[k + "2"] = np.where(bigt, e, f32(0.0)).astype(f32)
+                out[k] = (x / inorm).astype(f32)
+            out["numt"] = numt
+            if imcube:
+                for k in ("image_m_i", "image_m_q", "image_m_u", "image_m_v"):
+                    if k in tal.arrays:
+                        out[k] = (tal[k].astype(f32) / inorm).astype(f32)
+    return out

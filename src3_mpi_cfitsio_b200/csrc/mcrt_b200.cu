@@ -418,6 +418,60 @@ __global__ void wave_loop_finish(unsigned long long* cnt, const WaveCtl* c) {
   cnt[MCRT_C_LAUNCHES] += 4 * c->pad1 + 4;    // + wave_init, tail, diffusion_finalize, this
 }
 
+// diskflux (flux_test.f90:14-82) on the REAL arrays the download produces
+// (the FP64 device sums rounded to FP32), in the reference's FP32 order of
+// operations; the intrinsics keep the compiler from fusing any of them.
+// SED: dst[10][n] = si sq su sv, their relative errors, nums, aveinc.
+__global__ void diskflux_sed(const double* sed, int64_t n, float rnorm, float* dst) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    float v[10];
+    for (int a = 0; a < 10; ++a) v[a] = (float)sed[a * n + k];
+    const float si = v[0], nums = v[8];
+    float e[4] = {0.f, 0.f, 0.f, 0.f};
+    float aveinc = v[9];
+    if (nums > 1.0f) {
+      const float nm1 = __fsub_rn(nums, 1.0f);
+      for (int a = 0; a < 4; ++a) {         // sqrt((x2 - x**2/nums)/(nums-1.)*nums)/si
+        const float x = v[a], x2 = v[4 + a];
+        const float var = __fmul_rn(__fdiv_rn(__fsub_rn(x2, __fdiv_rn(__fmul_rn(x, x), nums)), nm1), nums);
+        e[a] = __fdiv_rn(__fsqrt_rn(var), si);
+      }
+      e[0] = __fadd_rn(e[0], __fdiv_rn(1.0f, nums));
+      aveinc = __fdiv_rn(aveinc, nums);
+    }
+    for (int a = 0; a < 4; ++a) {
+      dst[a * n + k] = __fdiv_rn(v[a], rnorm);
+      dst[(4 + a) * n + k] = e[a];
+    }
+    dst[8 * n + k] = nums;
+    dst[9 * n + k] = aveinc;
+  }
+}
+
+// Peeled SED: dst[9][n] = ti tq tu tv, their relative errors, numt.
+__global__ void diskflux_psed(const double* ps, int64_t n, float inorm, float* dst) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    float v[9];
+    for (int a = 0; a < 9; ++a) v[a] = (float)ps[a * n + k];
+    const float numt = v[8];
+    for (int a = 0; a < 4; ++a) {
+      float e = 0.f;
+      if (numt > 1.0f) {                    // sqrt((x2*numt/x**2-1.)/(numt-1.))
+        const float x = v[a], x2 = v[4 + a];
+        e = __fsqrt_rn(__fdiv_rn(__fsub_rn(__fdiv_rn(__fmul_rn(x2, numt), __fmul_rn(x, x)), 1.0f), __fsub_rn(numt, 1.0f)));
+      }
+      dst[a * n + k] = __fdiv_rn(v[a], inorm);
+      dst[(4 + a) * n + k] = e;
+    }
+    dst[8 * n + k] = numt;
+  }
+}
+
+__global__ void diskflux_img(const double* img, int64_t n, float inorm, float* dst) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    dst[k] = __fdiv_rn((float)img[k], inorm);
+}
+
 __global__ void to_float(const double* src, float* dst, int64_t n) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
     dst[k] = (float)src[k];
@@ -1533,6 +1587,62 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
   CK(cudaStreamSynchronize(ctx->stream));
   dfree(ctx, d_f);
   return MCRT_OK;
+}
+
+int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mcrt_tallies* out) {
+  if (!ctx || !out) return MCRT_ERR_ARG;
+  if (np < 1 || !(ltot_lsol > 0.0) || !std::isfinite(ltot_lsol))
+    return fail(ctx, MCRT_ERR_ARG, "mcrt_diskflux: np must be positive and ltot/lsol finite and positive");
+  // the counts, FP64 cell tallies, scalars and counters as downloaded
+  mcrt_tallies rest = *out;
+  for (float** f : {&rest.si, &rest.sq, &rest.su, &rest.sv, &rest.si2, &rest.sq2, &rest.su2, &rest.sv2, &rest.nums,
+                    &rest.aveinc, &rest.ti, &rest.tq, &rest.tu, &rest.tv, &rest.ti2, &rest.tq2, &rest.tu2, &rest.tv2,
+                    &rest.numt, &rest.image_m_i, &rest.image_m_q, &rest.image_m_u, &rest.image_m_v})
+    *f = nullptr;
+  int rc = mcrt_download_tallies(ctx, &rest);
+  if (rc) return rc;
+  const mcrt_config& c = ctx->cfg;
+  const double rnp = (double)np;
+  const float rnorm = (float)(rnp / (double)c.nmu / (double)c.nph / ltot_lsol);   // flux_test.f90:20-21
+  const float inorm = (float)(rnp / ltot_lsol);
+  const bool peel = ipeel == 1;
+  const int64_t nsed = ctx->nsed, npsed = ctx->npsed, nimg = (peel && c.output_imcube) ? ctx->nimg : 0;
+  float* d_f = nullptr;
+  if ((rc = dalloc(ctx, &d_f, std::max<int64_t>({10 * nsed, 9 * npsed, 4 * nimg, 1})))) return rc;
+  auto grid = [](int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); };
+  auto get = [&](float* dst, const float* src, int64_t n) -> int {
+    if (!dst) return MCRT_OK;
+    cudaError_t e = cudaMemcpyAsync(dst, src, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    return e == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux copy: %s", cudaGetErrorString(e));
+  };
+  const DevTallies& t = ctx->dt;
+  float* sed[10] = {out->si, out->sq, out->su, out->sv, out->si2, out->sq2, out->su2, out->sv2, out->nums, out->aveinc};
+  float* ps[9] = {out->ti, out->tq, out->tu, out->tv, out->ti2, out->tq2, out->tu2, out->tv2, out->numt};
+  float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
+  diskflux_sed<<<grid(nsed), 256, 0, ctx->stream>>>(t.sed, nsed, rnorm, d_f);
+  for (int a = 0; a < 10 && !rc; ++a) rc = get(sed[a], d_f + a * nsed, nsed);
+  if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
+  if (!rc && peel) {
+    diskflux_psed<<<grid(npsed), 256, 0, ctx->stream>>>(t.psed, npsed, inorm, d_f);
+    for (int a = 0; a < 9 && !rc; ++a) rc = get(ps[a], d_f + a * npsed, npsed);
+    if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
+    for (int a = 0; a < 4 && !rc && nimg > 0; ++a) {
+      diskflux_img<<<grid(nimg), 256, 0, ctx->stream>>>(t.img + a * nimg, nimg, inorm, d_f);
+      rc = get(im[a], d_f, nimg);
+      if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
+    }
+  } else if (!rc) {                          // ipeel /= 1: the peeled arrays as downloaded (flux_test.f90:44)
+    mcrt_tallies pe{};
+    pe.ti = out->ti; pe.tq = out->tq; pe.tu = out->tu; pe.tv = out->tv;
+    pe.ti2 = out->ti2; pe.tq2 = out->tq2; pe.tu2 = out->tu2; pe.tv2 = out->tv2; pe.numt = out->numt;
+    pe.image_m_i = out->image_m_i; pe.image_m_q = out->image_m_q;
+    pe.image_m_u = out->image_m_u; pe.image_m_v = out->image_m_v;
+    rc = mcrt_download_tallies(ctx, &pe);
+  }
+  cudaError_t le = cudaGetLastError();
+  if (!rc && le != cudaSuccess) rc = fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux: %s", cudaGetErrorString(le));
+  dfree(ctx, d_f);
+  return rc;
 }
 
 int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {

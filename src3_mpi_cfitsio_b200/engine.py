@@ -55,6 +55,8 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_check_grid.restype = C.c_int
     lib.mcrt_set_limits.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_double]
     lib.mcrt_set_limits.restype = C.c_int
+    lib.mcrt_diskflux.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int32, P(abi.Tallies)]
+    lib.mcrt_diskflux.restype = C.c_int
     lib.mcrt_run_iteration.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32, C.c_int32]
     lib.mcrt_download_tallies.argtypes = [C.c_void_p, P(abi.Tallies)]
@@ -318,6 +320,14 @@ class Engine:
     def download(self, images: bool = True) -> abi.TallyArrays:
         tal = abi.TallyArrays(self.cfg, images=images)
         self._check(self.lib.mcrt_download_tallies(self.ctx, C.byref(tal.struct)))
+        return tal
+
+    def diskflux(self, np_total: int, ltot_lsol: float, ipeel: int = 1, images: bool = True) -> abi.TallyArrays:
+        """``subroutine diskflux`` (flux_test.f90): the tallies with the
+        reference's output normalisation and error arrays, computed on the
+        device (mcrt_diskflux)."""
+        tal = abi.TallyArrays(self.cfg, images=images)
+        self._check(self.lib.mcrt_diskflux(self.ctx, np_total, ltot_lsol, ipeel, C.byref(tal.struct)))
         return tal
 
     def accumulate(self, tal: abi.TallyArrays):

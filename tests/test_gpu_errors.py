@@ -47,10 +47,10 @@ def test_upload_refuses_a_nan_density_and_the_context_stays_usable():
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_walk_limit_reports_lost_packets(precision):
-    """A walk limit of 3 crossings gives up most walks: their packets are
-    dropped and counted, the run returns MCRT_ERR_GEOM with the count, the
-    other packets are tallied, and with the default limits the next run is
-    clean."""
+    """A walk limit of 3 crossings gives up the walks (a packet leaving the
+    star crosses more walls than that): their packets are dropped and
+    counted, the run returns MCRT_ERR_GEOM with the count, every packet is
+    accounted for, and with the default limits the next run is clean."""
     from src3_mpi_cfitsio_b200.engine import MCRTError
     m = model.warm(model.small_2d())
     eng = _engine(m, precision)
@@ -61,7 +61,8 @@ def test_walk_limit_reports_lost_packets(precision):
         eng.run(n, ipeel=1)
     assert e.value.code == ERR_GEOM and "geometry" in str(e.value)
     c = eng.download(images=False).counters()
-    assert c["packets"] == n and 0 < c["geom_fail"] < n
+    assert c["packets"] == n and c["geom_fail"] > 0
+    assert f"{c['geom_fail']} of {n} packets" in str(e.value)
     assert c["exited"] + c["geom_fail"] + c["killed"] == n
     eng.set_limits()
     _normal_run(eng)
