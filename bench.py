@@ -120,7 +120,7 @@ def build_model(args):
     (DIFFUSION=YES, tts_mod_5.f90:33).  Every arm -- the GPU steps, the
     CPU baseline and the reference arm -- starts from this same state."""
     from src3_mpi_cfitsio_b200 import model
-    return model.reference_2d_converged()
+    return model.with_velocities(model.reference_2d_converged())
 
 
 def algorithmic_bytes(c: dict) -> float:
@@ -181,6 +181,41 @@ def bench_clumpy(args, dev):
             "fp64_packets": n64, "fp64_packets_per_s": n64 / (ms64 / 1e3),
             "mixed_over_fp64": (n / ms) / (n64 / ms64),
             "crossings_per_packet": c["crossings"] / n, "peel_crossings_per_packet": c["peel_cross"] / n}
+
+
+def bench_velocity(args, dev):
+    """What the velocity terms of tfinal (dusttemp_5.f90:42-53, the infall
+    field of the envelope) do to the temperatures: one iteration's tallies,
+    tfinal with the field and without it on the same dtauabs, iteration 5
+    (20 passes, the last 10 averaged)."""
+    import copy
+    import numpy as np
+    from src3_mpi_cfitsio_b200.engine import Engine
+    m = build_model(args)
+    rest = copy.deepcopy(m)
+    for k in ("vrarr", "vthetarr", "divvarr"):
+        del rest.grid[k]
+    n = 10_000_000
+    ev = Engine(m, device=dev, precision="mixed")
+    ev.reset_tallies()
+    ev.run(n, iteration=5, ipeel=0)
+    tal = ev.download(images=False)
+    t0 = time.perf_counter()
+    tv, _, _ = ev.update_temperature(n, 5)
+    tv_s = time.perf_counter() - t0
+    er = Engine(rest, device=dev, precision="mixed")
+    er.reset_tallies()
+    er.accumulate(tal)
+    t0 = time.perf_counter()
+    tr, _, _ = er.update_temperature(n, 5)
+    tr_s = time.perf_counter() - t0
+    ev.close()
+    er.close()
+    env = (m.dens4()[..., 2] > 0).ravel(order="F") & (tr > 2.0 / 11605.0)
+    rel = np.abs(tv[env] / tr[env] - 1.0)
+    return {"packets": n, "iteration": 5, "envelope_cells": int(env.sum()),
+            "rel_change_median": float(np.median(rel)), "rel_change_max": float(rel.max()),
+            "tfinal_seconds_with_velocity": tv_s, "tfinal_seconds_at_rest": tr_s}
 
 
 def bench_setemiss(args, dev):
@@ -490,6 +525,7 @@ def run_ours(args, rank, world):
         extra["clumpy_3d"] = bench_clumpy(args, dev)
     if rank == 0:
         extra["setemiss"] = bench_setemiss(args, dev)
+        extra["velocity_terms"] = bench_velocity(args, dev)
     if args.batch_models > 0:                  # every rank: the models are sharded over the ranks
         res = bench_batch(args, dev, rank, world, allreduce if dist else None)
         if rank == 0:

@@ -117,6 +117,14 @@ typedef struct mcrt_grid {
   const double  *ravearr;     /* [nrg-1] (accretion emission)               */
   const double  *Ldint;       /* [nrg-1] accretion luminosity CDF           */
   const double  *hdisk;       /* [nrg-1] disk scale height                  */
+  /* Gas velocity field (gridset_5_model13new.f90:1383-1480), optional: all
+   * three NULL is a gas at rest.  With it, tfinal adds the adiabatic
+   * (Tint*divv) and advective (vr*dT/dr + vtheta*dT/dtheta) terms of
+   * dusttemp (dusttemp_5.f90:42-53) and forms the temperature gradients
+   * from 31x31-cell smoothings over its passes (tfinal_5_test1.f90:61-200). */
+  const double  *vrarr;       /* [nrg,ntg,npg] cm/s                         */
+  const double  *vthetarr;    /* [nrg,ntg,npg] cm/s                         */
+  const double  *divvarr;     /* [nrg,ntg,npg] cm/s per stellar radius      */
 } mcrt_grid;
 
 /*
@@ -387,7 +395,9 @@ int mcrt_update_temperature(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
  * context's device current; a context created after a device reset looks
  * it up again) and should come before any stream capture.  All calls in the
  * process share the array: calls that overlap on a GPU (two contexts on one
- * device, or two host threads) race. */
+ * device, or two host threads) race.  Models with a gas velocity field
+ * (mcrt_grid.vrarr...) need pass buffers it does not have and are refused
+ * with MCRT_ERR_UNSUPPORTED. */
 int mcrt_update_temperature_noalloc(mcrt_ctx *ctx, int32_t nphot, int32_t iter,
                                     double *tdave, int32_t *converge, double *sig);
 

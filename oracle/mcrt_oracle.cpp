@@ -1929,20 +1929,29 @@ static double kapP(const mcrt_config* c, const mcrt_tables* t, double T, int idu
   return (1.0 - f) * kp[k - 1] + f * kp[k];
 }
 
-// dusttemp (dusttemp_5.f90:8-152) with zero velocities (divv=vr=vthet=0)
+// dusttemp (dusttemp_5.f90:8-152).  kappaT(i) = emission + adiabatic +
+// advective term (:42-53); with vel == false (a gas at rest) only the
+// emission term, as the other two are exact zeros then.
 static double dusttemp(const mcrt_config* c, const mcrt_tables* t, double na, int nphot, int idust3, double mcell,
-                       double gradtr, double gradtt, double divv, double vr, double vthet) {
+                       double gradtr, double gradtt, double divv, double vr, double vthet, bool vel = false) {
   const int nT = c->nT;
   const double Tmax = 199999.0;
   const double rstar = c->rstar, tstar = c->tstarave;
   std::vector<double> kappaT(nT);
   const double* kp = t->kappap + (int64_t)nT * (idust3 - 1);
   const double kv = t->kappav[idust3 - 1];
-  // Tint**4 etc. are integer powers in Fortran: x2=x*x, x4=x2*x2.  With a
-  // zero velocity field the adiabatic and advective terms are exact zeros.
+  // Tint**4 etc. are integer powers in Fortran: x2=x*x, x4=x2*x2
   auto p4 = [](double x) { double x2 = x * x; return x2 * x2; };
-  (void)divv; (void)vr; (void)vthet; (void)gradtr; (void)gradtt;
-  for (int i = 0; i < nT; ++i) kappaT[i] = p4(t->Tint[i]) * kp[i];
+  const double p3 = 11605.0 * 11605.0 * 11605.0;
+  const double c1 = KB / 4.0 / SIGT / 2.3 / MHY, c2 = KB * 3.0 / 8.0 / SIGT / 2.3 / MHY;
+  const double gr = vr * gradtr + vthet * gradtt;
+  for (int i = 0; i < nT; ++i) {
+    const double emi = p4(t->Tint[i]) * kp[i];
+    if (!vel) { kappaT[i] = emi; continue; }
+    const double adi = c1 / kv / p3 * t->Tint[i] * divv / rstar / RSOL;
+    const double adv = c2 / kv / p3 * gr / rstar / RSOL;
+    kappaT[i] = emi + adi + adv;
+  }
   double Td = 0.1 / 11605.0;
   if (mcell > 0.0) {
     double abs_ = p4(tstar) * (na * PI * rstar * rstar) / ((double)nphot * kv);
@@ -1979,8 +1988,9 @@ static double dusttemp(const mcrt_config* c, const mcrt_tables* t, double na, in
   return Td;
 }
 
-// tfinal (tfinal_5_test1.f90:1-447) for axisymmetric models, zero velocity
-// field (divvarr = vrarr = vthetarr = 0, so the gradient terms vanish).
+// tfinal (tfinal_5_test1.f90:1-447) for axisymmetric models; with a gas
+// velocity field every pass smooths the temperature, forms and smooths its
+// gradients and adds dusttemp's adiabatic and advective terms.
 int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t, const double* dtauabs,
                   const double* tdust_now, int32_t nphot, int32_t iter, double* tdave, int32_t* converge,
                   double* sig_out) {
@@ -1993,9 +2003,76 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
   const double Tmax = 199999.0, T01 = 0.1 / 11605.0;
   std::vector<double> old(tdave, tdave + ncell), iter_acc(ncell, 0.0);
   int maxii = (iter > 3) ? 20 : 1;
+  // gas velocity field: the temperature gradients of every pass
+  // (tfinal_5_test1.f90:61-200) feed dusttemp's advective term
+  const bool vel = g->vrarr && g->vthetarr && g->divvarr;
+  const int64_t n2 = (int64_t)nrg * ntg;
+  std::vector<double> tsm(vel ? n2 : 0), gtr(vel ? n2 : 0), gtt(vel ? n2 : 0), gtr2(vel ? n2 : 0), gtt2(vel ? n2 : 0);
+  auto c2d = [&](int ir, int it) { return (int64_t)(ir - 1) + (int64_t)nrg * (it - 1); };
+  auto box = [](int i, int w, int n, int& lo, int& hi) {
+    if (i > w && i < n - w) { lo = i - w; hi = i + w; }
+    else if (i <= w) { lo = 1; hi = i + w; }
+    else { lo = i - w; hi = n - 1; }
+  };
+  auto rave = [&](int ir) { return g->ravearr ? g->ravearr[ir - 1] : 0.5 * (g->rarr[ir - 1] + g->rarr[ir]); };
   for (int ii = 1; ii <= maxii; ++ii) {
-    // the gradient smoothing passes feed only the velocity terms, which are zero here
     const int ip = 1;
+    if (vel) {
+      std::fill(tsm.begin(), tsm.end(), 0.0);
+      for (int ir = 1; ir <= nrg - 1; ++ir)
+        for (int it = 1; it <= ntg - 1; ++it) {
+          int r1, r2, t1, t2;
+          box(ir, 15, nrg, r1, r2);
+          box(it, 15, ntg, t1, t2);
+          double tot = 0.0;
+          int nsm = 0;
+          for (int iir = r1; iir <= r2; ++iir)
+            for (int iit = t1; iit <= t2; ++iit)
+              if (tdave[ci(iir, iit, 1)] > T01) { ++nsm; tot += tdave[ci(iir, iit, 1)]; }
+          if (nsm > 0) tot = tot / (double)nsm;
+          tsm[c2d(ir, it)] = (tdave[ci(ir, it, 1)] == T01) ? T01 : tot;
+        }
+      auto T = [&](int i, int j) { return tsm[c2d(i, j)]; };
+      auto disk = [&](int ir, int it) { return dens(ir, it, 1, 1) + dens(ir, it, 1, 2) + dens(ir, it, 1, 9) > 0.0; };
+      for (int ir = 1; ir <= nrg - 1; ++ir) {
+        const double rad = rave(ir), dr = g->rarr[ir] - g->rarr[ir - 1];
+        for (int it = 1; it <= ntg - 1; ++it) {
+          const double dt = g->thetarr[it] - g->thetarr[it - 1];
+          double gr = 0.0, gt = 0.0;
+          if (ii > 1) {
+            gr = (T(ir + 1, it) - T(ir, it)) / dr;
+            if (it <= 15) gr = (T(ir + 1, 16) - T(ir, 16)) / dr;
+            if (ir >= nrg - 16) gr = gtr[c2d(nrg - 17, it)];
+            if (disk(ir, it)) gr = 0.0;
+            gt = (T(ir, it + 1) - T(ir, it)) / dt / rad;
+            if (it <= 15) gt = (T(ir, 17) - T(ir, 16)) / rad / (g->thetarr[16] - g->thetarr[15]);
+            if (ir >= nrg - 16) gt = gtt[c2d(nrg - 17, it)];
+            if (disk(ir, it)) gt = 0.0;
+          }
+          gtr[c2d(ir, it)] = gr;
+          gtt[c2d(ir, it)] = gt;
+        }
+      }
+      for (int ir = 1; ir <= nrg - 1; ++ir)
+        for (int it = 1; it <= ntg - 1; ++it) {
+          int r1, r2;
+          box(ir, 15, nrg, r1, r2);
+          double gr = 0.0, gt = 0.0;
+          if (dens(ir, it, 1, 4) + dens(ir, it, 1, 10) > 0.0) {
+            int nsm = 0;
+            for (int iir = r1; iir <= r2; ++iir)
+              if (gtr[c2d(iir, it)] < 0.0) { ++nsm; gr += gtr[c2d(iir, it)]; }
+            if (nsm > 0) gr = gr / (double)nsm;
+          } else {
+            for (int iir = r1; iir <= r2; ++iir) gr += gtr[c2d(iir, it)];
+            gr = gr / (double)(r2 - r1 + 1) / 1.0;
+          }
+          for (int iir = r1; iir <= r2; ++iir) gt += gtt[c2d(iir, it)];
+          gt = gt / (double)(r2 - r1 + 1) / 1.0;
+          gtr2[c2d(ir, it)] = gr;
+          gtt2[c2d(ir, it)] = gt;
+        }
+    }
     for (int ir = 1; ir <= nrg - 1; ++ir) {
       for (int it = 1; it <= (ntg - 1) / 2; ++it) {
         double td = T01;
@@ -2006,10 +2083,13 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
             if (!g->diffus[ci(ir, it, ip)]) {
               double m1 = std::pow(dens(ir, it, ip, id) * g->vcell[ci(ir, it, ip)], 0.25);
               double m2 = std::pow(dens(ir, itm, ip, id) * g->vcell[ci(ir, it, ip)], 0.25);
-              double t1 = dusttemp(c, t, dtauabs[ci(ir, it, ip)], nphot, idust3, m1, 0, 0, 0, 0, 0);
+              const double gr = vel ? gtr2[c2d(ir, it)] : 0.0, gt = vel ? gtt2[c2d(ir, it)] : 0.0;
+              const int64_t a = ci(ir, it, ip), b = ci(ir, itm, ip);
+              double t1 = dusttemp(c, t, dtauabs[a], nphot, idust3, m1, gr, gt, vel ? g->divvarr[a] : 0.0,
+                                   vel ? g->vrarr[a] : 0.0, vel ? g->vthetarr[a] : 0.0, vel);
               int idust3b = g->findopac[ci(ir, itm, ip) + ncell * (id - 1)];
-              double t2 = dusttemp(c, t, dtauabs[ci(ir, itm, ip)], nphot, idust3b, m2, 0, 0, 0, 0, 0);
-              (void)KB; (void)MHY; (void)SIGT;
+              double t2 = dusttemp(c, t, dtauabs[b], nphot, idust3b, m2, gr, gt, vel ? g->divvarr[b] : 0.0,
+                                   vel ? g->vrarr[b] : 0.0, vel ? g->vthetarr[b] : 0.0, vel);
               td = (t1 + t2) / 2.0;
             } else {
               td = (tdust_now[ci(ir, it, ip)] + tdust_now[ci(ir, itm, ip)]) / 2.0;

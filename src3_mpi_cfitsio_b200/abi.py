@@ -46,7 +46,7 @@ GRID_FIELDS = [("rarr", _dp), ("r2arr", _dp), ("thetarr", _dp), ("costarr", _dp)
                ("sintarr", _dp), ("tan2arr", _dp), ("phiarr", _dp), ("aarr", _dp),
                ("barr", _dp), ("densarr", _dp), ("findopac", _ip), ("diffus", _ip),
                ("diffdir", _ip), ("tdust", _dp), ("vcell", _dp), ("ravearr", _dp),
-               ("Ldint", _dp), ("hdisk", _dp)]
+               ("Ldint", _dp), ("hdisk", _dp), ("vrarr", _dp), ("vthetarr", _dp), ("divvarr", _dp)]
 
 
 class Grid(C.Structure):

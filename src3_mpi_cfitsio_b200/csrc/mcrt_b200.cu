@@ -118,6 +118,12 @@ struct mcrt_ctx {
   double *d_dens_thermal = nullptr;   // [ncell] density of the thermal component (tfinal)
   int32_t *d_idust3 = nullptr;        // [ncell] its opacity species (0 = none)
   int32_t *d_diffus = nullptr;
+  // gas velocity field (tfinal's adiabatic and advective terms)
+  bool have_vel = false;
+  double *d_vel = nullptr;            // [3][ncell] vrarr, vthetarr, divvarr
+  int32_t *d_tflag = nullptr;         // [ncell] bit 0: disk ids 1/2/9, bit 1: ids 4/10 (tfinal's gradient rules)
+  double *d_rave = nullptr;           // [nrg] cell-centre radii (ravearr or the wall midpoints)
+  std::vector<int32_t> h_diffus;      // diffusion flags (convergence statistics)
   // tables
   int32_t *d_nlambda = nullptr;
   double *d_tabs = nullptr;
@@ -203,18 +209,39 @@ namespace mcrt {
 __device__ __forceinline__ double p4(double x) { double x2 = x * x; return x2 * x2; }
 
 // dusttemp (dusttemp_5.f90:8-152) for a zero velocity field
+// The emission side of dusttemp's balance at table temperature i:
+// Tint^4 kappa_P plus, with a gas velocity field, the adiabatic term
+// (k/4/sigt/2.3/mH)/kappa_V/11605^3 * Tint*divv/rstar/rsol and the advective
+// term (3k/8/sigt/2.3/mH)/kappa_V/11605^3 * (vr gradtr + vthet gradtt)/
+// rstar/rsol (dusttemp_5.f90:42-53), in the reference's left-to-right order.
+struct DustVel {
+  double divv, adv;          // divv; vr*gradtr + vthet*gradtt
+  bool on;
+};
+__device__ __forceinline__ double kappa_T(const double* Tint, const double* kp, int i, double kv, double rstar,
+                                          const DustVel& v) {
+  const double emi = __dmul_rn(p4(Tint[i]), kp[i]);
+  if (!v.on) return emi;
+  constexpr double kB = 1.3806503e-16, sigt = 5.670400e-5, mH = 1.67262158e-24, rsol = 6.9598e10;
+  const double p3 = 11605.0 * 11605.0 * 11605.0;
+  const double c1 = kB / 4.0 / sigt / 2.3 / mH, c2 = kB * 3.0 / 8.0 / sigt / 2.3 / mH;
+  const double adi = __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c1, kv), p3), Tint[i]), v.divv), rstar), rsol);
+  const double adv = __ddiv_rn(__ddiv_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c2, kv), p3), v.adv), rstar), rsol);
+  return __dadd_rn(__dadd_rn(emi, adi), adv);
+}
+
 __device__ double dusttemp_dev(const double* Tint, const double* kp, int nT, double kv, double na, int nphot,
-                               double mcell, double rstar, double tstar) {
+                               double mcell, double rstar, double tstar, const DustVel& v = DustVel{0.0, 0.0, false}) {
   const double Tmax = 199999.0, T01 = 0.1 / 11605.0;
   double Td = T01;
   if (!(mcell > 0.0)) return Td;
   double abs_ = p4(tstar) * (na * 3.1415926535897932384626433 * rstar * rstar) / ((double)nphot * kv);
   abs_ = abs_ * (6.9598e10 * 6.9598e10) / p4(mcell);
   if (na == 0.0) return T01;
-  double minkap = p4(Tint[0]) * kp[0], maxkap = minkap;
+  double minkap = kappa_T(Tint, kp, 0, kv, rstar, v), maxkap = minkap;
   int mini = 1, maxi = 1;
   for (int i = 1; i <= nT; ++i) {
-    const double k = p4(Tint[i - 1]) * kp[i - 1];
+    const double k = kappa_T(Tint, kp, i - 1, kv, rstar, v);
     if (minkap > k) { minkap = k; mini = i; }
     if (maxkap < k) { maxkap = k; maxi = i; }
   }
@@ -222,7 +249,7 @@ __device__ double dusttemp_dev(const double* Tint, const double* kp, int nT, dou
   if (minkap > abs_) Td = fmax(fmin(Tint[mini - 1], Tmax / 11605.0), T01);
   if (mini < maxi) {
     for (int i = mini; i <= maxi - 1; ++i) {
-      const double kl = p4(Tint[i - 1]) * kp[i - 1], ku = p4(Tint[i]) * kp[i];
+      const double kl = kappa_T(Tint, kp, i - 1, kv, rstar, v), ku = kappa_T(Tint, kp, i, kv, rstar, v);
       if (kl < abs_ && ku >= abs_) {
         const double Tl = Tint[i - 1], Tu = Tint[i];
         Td = Tl + (Tu - Tl) / (ku - kl) * (abs_ - kl);
@@ -231,7 +258,7 @@ __device__ double dusttemp_dev(const double* Tint, const double* kp, int nT, dou
     }
   } else {
     for (int i = maxi; i <= mini - 1; ++i) {
-      const double kl = p4(Tint[i - 1]) * kp[i - 1], ku = p4(Tint[i]) * kp[i];
+      const double kl = kappa_T(Tint, kp, i - 1, kv, rstar, v), ku = kappa_T(Tint, kp, i, kv, rstar, v);
       if (kl > abs_ && ku <= abs_) {
         const double Tl = Tint[i - 1], Tu = Tint[i];
         Td = Tl + (Tu - Tl) / (ku - kl) * (abs_ - kl);
@@ -250,6 +277,14 @@ struct TfinalArgs {
   const double *told;   // tdave of the previous iteration
   double *tnew;         // scratch: new upper-hemisphere values
   double *tdave;        // result
+  // gas velocity field (null vr: at rest) and the pass scratch of its
+  // temperature gradients
+  const double *vr, *vth, *divv;        // [ncell]
+  const double *rarr, *thetarr, *rave;  // walls; cell-centre radii [nrg-1]
+  const int32_t *tflag;                 // [ncell] bit 0: densarr ids 1, 2 or 9 > 0; bit 1: ids 4 or 10 > 0
+  double *tsm;                          // [nrg*ntg] smoothed temperature (phi slice 1)
+  double *gtr, *gtt, *gtr2, *gtt2;      // [nrg*ntg] gradients, raw and smoothed
+  double *acc;                          // [ncell] sum of passes 11..maxii
 };
 
 // tfinal_5_test1.f90:206-256: upper-hemisphere cells of phi slice 1.  The
@@ -308,6 +343,165 @@ __global__ void tfinal_mirror(TfinalArgs a) {
   }
 }
 
+// ---- tfinal with a gas velocity field: the passes of tfinal_5_test1.f90
+// (maxii of them, averaged over passes 11..maxii when maxii > 10).  Every
+// pass smooths the temperature over 31 x 31 cells, forms the radial and
+// polar gradients, smooths them over 31 radial cells, and solves dusttemp
+// with the adiabatic and advective terms cell by cell.  The kernels work on
+// phi slice 1 (the model is axisymmetric in this part of the reference).
+
+// Box limits of the reference (width w each side, clipped to 1..n-1).
+__device__ __forceinline__ void tf_box(int i, int w, int n, int& lo, int& hi) {
+  if (i > w && i < n - w) { lo = i - w; hi = i + w; }
+  else if (i <= w) { lo = 1; hi = i + w; }
+  else { lo = i - w; hi = n - 1; }
+}
+
+// tfinal_5_test1.f90:65-106: smoothed temperature of every cell.
+__global__ void tfv_smooth(TfinalArgs a) {
+  const double T01 = 0.1 / 11605.0;
+  const int64_t n = (int64_t)a.nrg * a.ntg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1, it = (int)(k / a.nrg) + 1;
+    if (ir > a.nrg - 1 || it > a.ntg - 1) { a.tsm[k] = 0.0; continue; }
+    int r1, r2, t1, t2;
+    tf_box(ir, 15, a.nrg, r1, r2);
+    tf_box(it, 15, a.ntg, t1, t2);
+    double tot = 0.0;
+    int nsm = 0;
+    for (int iir = r1; iir <= r2; ++iir)
+      for (int iit = t1; iit <= t2; ++iit) {
+        const double v = a.tdave[(iir - 1) + (int64_t)a.nrg * (iit - 1)];
+        if (v > T01) { ++nsm; tot = __dadd_rn(tot, v); }
+      }
+    if (nsm > 0) tot = __ddiv_rn(tot, (double)nsm);
+    if (a.tdave[(ir - 1) + (int64_t)a.nrg * (it - 1)] == T01) tot = T01;
+    a.tsm[k] = tot;
+  }
+}
+
+// tfinal_5_test1.f90:108-135: the raw gradients of cell (ir,it) before the
+// outer-edge copy; zero in disk cells.
+__device__ __forceinline__ void tfv_grad_cell(const TfinalArgs& a, int ir, int it, double& gr, double& gt) {
+  const int nrg = a.nrg;
+  auto T = [&](int i, int j) { return a.tsm[(i - 1) + (int64_t)nrg * (j - 1)]; };
+  const double rad = a.rave[ir - 1];
+  const double dr = __dsub_rn(a.rarr[ir], a.rarr[ir - 1]);
+  const double dt = __dsub_rn(a.thetarr[it], a.thetarr[it - 1]);
+  gr = __ddiv_rn(__dsub_rn(T(ir + 1, it), T(ir, it)), dr);
+  if (it <= 15) gr = __ddiv_rn(__dsub_rn(T(ir + 1, 16), T(ir, 16)), dr);
+  gt = __ddiv_rn(__ddiv_rn(__dsub_rn(T(ir, it + 1), T(ir, it)), dt), rad);
+  if (it <= 15) gt = __ddiv_rn(__ddiv_rn(__dsub_rn(T(ir, 17), T(ir, 16)), rad), __dsub_rn(a.thetarr[16], a.thetarr[15]));
+}
+
+__global__ void tfv_grad(TfinalArgs a, int first_pass) {
+  const int64_t n = (int64_t)a.nrg * a.ntg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1, it = (int)(k / a.nrg) + 1;
+    double gr = 0.0, gt = 0.0;
+    if (!first_pass && ir <= a.nrg - 1 && it <= a.ntg - 1) {
+      const int src = a.nrg - 17;               // ir >= nrg-widthr-1 copies row nrg-widthr-2 (its final value)
+      if (ir >= a.nrg - 16) {
+        tfv_grad_cell(a, src, it, gr, gt);
+        if (a.tflag[(src - 1) + (int64_t)a.nrg * (it - 1)] & 1) { gr = 0.0; gt = 0.0; }
+      } else {
+        tfv_grad_cell(a, ir, it, gr, gt);
+      }
+      if (a.tflag[k] & 1) { gr = 0.0; gt = 0.0; }
+    }
+    a.gtr[k] = gr;
+    a.gtt[k] = gt;
+  }
+}
+
+// tfinal_5_test1.f90:145-194: gradients smoothed over 31 radial cells; in
+// cells of densarr ids 4/10 the radial one is the mean of the negative ones.
+__global__ void tfv_smooth_grad(TfinalArgs a) {
+  const int64_t n = (int64_t)a.nrg * a.ntg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1, it = (int)(k / a.nrg) + 1;
+    double gr = 0.0, gt = 0.0;
+    if (ir <= a.nrg - 1 && it <= a.ntg - 1) {
+      int r1, r2;
+      tf_box(ir, 15, a.nrg, r1, r2);
+      const int64_t row = (int64_t)a.nrg * (it - 1);
+      if (a.tflag[k] & 2) {
+        int nsm = 0;
+        for (int iir = r1; iir <= r2; ++iir) {
+          const double v = a.gtr[(iir - 1) + row];
+          if (v < 0.0) { ++nsm; gr = __dadd_rn(gr, v); }
+        }
+        if (nsm > 0) gr = __ddiv_rn(gr, (double)nsm);
+      } else {
+        for (int iir = r1; iir <= r2; ++iir) gr = __dadd_rn(gr, a.gtr[(iir - 1) + row]);
+        gr = __ddiv_rn(__ddiv_rn(gr, (double)(r2 - r1 + 1)), 1.0);
+      }
+      for (int iir = r1; iir <= r2; ++iir) gt = __dadd_rn(gt, a.gtt[(iir - 1) + row]);
+      gt = __ddiv_rn(__ddiv_rn(gt, (double)(r2 - r1 + 1)), 1.0);
+    }
+    a.gtr2[k] = gr;
+    a.gtt2[k] = gt;
+  }
+}
+
+// tfinal_5_test1.f90:206-243 with the velocity terms: the upper-hemisphere
+// cells of slice 1, in place in tdave (each reads only its own cells).
+__global__ void tfv_cells(TfinalArgs a) {
+  const int nu = (a.ntg - 1) / 2;
+  const int64_t n = (int64_t)(a.nrg - 1) * nu;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % (a.nrg - 1)) + 1;
+    const int it = (int)(k / (a.nrg - 1)) + 1;
+    const int itm = a.ntg - it;
+    const int64_t c = (ir - 1) + (int64_t)a.nrg * (it - 1);
+    const int64_t cm = (ir - 1) + (int64_t)a.nrg * (itm - 1);
+    double td = 0.1 / 11605.0;
+    const int sp = a.idust3[c];
+    if (sp > 0) {
+      if (!a.diffus[c]) {
+        const double dm = (a.idust3[cm] == sp) ? a.dens[cm] : 0.0;
+        const double m1 = pow(a.dens[c] * a.vcell[c], 0.25);
+        const double m2 = pow(dm * a.vcell[c], 0.25);
+        const double* kp = a.kappap + (int64_t)a.nT * (sp - 1);
+        const double gr = a.gtr2[c], gt = a.gtt2[c];
+        DustVel v1{a.divv[c], __dadd_rn(__dmul_rn(a.vr[c], gr), __dmul_rn(a.vth[c], gt)), true};
+        DustVel v2{a.divv[cm], __dadd_rn(__dmul_rn(a.vr[cm], gr), __dmul_rn(a.vth[cm], gt)), true};
+        const double t1 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[c], a.nphot, m1, a.rstar, a.tstar, v1);
+        const double t2 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[cm], a.nphot, m2, a.rstar, a.tstar, v2);
+        td = (t1 + t2) / 2.0;
+      } else {
+        td = (a.tdust[c] + a.tdust[cm]) / 2.0;
+      }
+      if (td * 11605.0 >= 199999.0) td = 199999.0 / 11605.0;
+    }
+    a.tdave[c] = td;
+  }
+}
+
+// tfinal_5_test1.f90:267-288: mirror to the lower hemisphere and the other
+// phi slices (in place), and the pass sum of passes 11..maxii.
+__global__ void tfv_mirror(TfinalArgs a, int accumulate, int first_acc) {
+  const int64_t n = (int64_t)a.nrg * a.ntg * a.npg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1;
+    const int it = (int)((k / a.nrg) % a.ntg) + 1;
+    const int ip = (int)(k / ((int64_t)a.nrg * a.ntg)) + 1;
+    double v = a.tdave[k];
+    if (ir <= a.nrg - 1 && it <= a.ntg - 1 && (ip == 1 || (a.npg > 2 && ip <= a.npg - 1))) {
+      const int src_it = (it >= (a.ntg + 1) / 2) ? a.ntg - it : it;
+      if (src_it != it || ip != 1) v = a.tdave[(ir - 1) + (int64_t)a.nrg * (src_it - 1)];
+    }
+    if (ip != 1 || it >= (a.ntg + 1) / 2) a.tdave[k] = v;      // upper cells of slice 1 are the sources
+    if (accumulate) a.acc[k] = first_acc ? v : __dadd_rn(a.acc[k], v);
+  }
+}
+
+__global__ void tfv_average(TfinalArgs a, int passes) {
+  const int64_t n = (int64_t)a.nrg * a.ntg * a.npg;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    a.tdave[k] = a.acc[k] / (double)passes;
+}
+
 // gridset_5_model13new.f90:1855-1866: tdust for the next iteration
 __global__ void tdust_from_tdave(int64_t n, const double* tdave, const int32_t* diffus, const int32_t* idust3,
                                  const CellRec* cells, double* tdust) {
@@ -321,7 +515,7 @@ __global__ void tdust_from_tdave(int64_t n, const double* tdave, const int32_t* 
 // Convergence sums of tfinal_5_test1.f90:307-332 accumulated on the device:
 // out[0..2] sums of |dT/T|, out[3..5] sums of (dT/T)^2, out[6..8] counts.
 __global__ void tfinal_stats(int nrg, int ntg, const double* told, const double* tnew, const double* rarr,
-                             double autors, double* out) {
+                             double autors, const int32_t* diffus, double* out) {
   const int nu = (ntg - 1) / 2;
   const int64_t n = (int64_t)(nrg - 1) * nu;
   const double T01 = 0.1 / 11605.0;
@@ -333,7 +527,7 @@ __global__ void tfinal_stats(int nrg, int ntg, const double* told, const double*
     const double to = told[c], tn = tnew[c];
     const double d = (tn - to) / tn;
     if (tn != to && tn > T01 && to > T01) { a[0] += fabs(d); a[3] += d * d; a[6] += 1.0; }
-    if (tn > T01 && to > T01) { a[1] += fabs(d); a[4] += d * d; a[7] += 1.0; }
+    if (!diffus[c] && tn > T01 && to > T01) { a[1] += fabs(d); a[4] += d * d; a[7] += 1.0; }
     if (rarr[ir - 1] / autors < 5.0 && tn > T01 && to > T01) { a[2] += fabs(d); a[5] += d * d; a[8] += 1.0; }
   }
   for (int i = 0; i < 9; ++i) {
@@ -719,6 +913,34 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   CK(cudaMemcpyAsync(ctx->d_dens_thermal, dens_th.data(), ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_idust3, idust3.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_diffus, diffus.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->h_diffus = diffus;
+  // velocity field and tfinal's per-cell gradient rules
+  const bool vel = g->vrarr && g->vthetarr && g->divvarr;
+  if (!vel && (g->vrarr || g->vthetarr || g->divvarr))
+    return fail(ctx, MCRT_ERR_ARG, "mcrt_upload_grid: vrarr, vthetarr and divvarr come together (or none)");
+  if (vel) {
+    if (nrg < 19 || ntg < 18)
+      return fail(ctx, MCRT_ERR_UNSUPPORTED, "a velocity field needs nrg >= 19 and ntg >= 18 (tfinal's 15-cell windows)");
+    std::vector<int32_t> tflag(ncell, 0);
+    for (int64_t k = 0; k < ncell; ++k) {
+      auto rho = [&](int id) { return g->densarr[k + ncell * (id - 1)]; };
+      if (rho(1) + rho(2) + rho(9) > 0.0) tflag[k] |= 1;
+      if (rho(4) + rho(10) > 0.0) tflag[k] |= 2;
+    }
+    std::vector<double> rave(nrg, 0.0);
+    for (int i = 0; i < nrg - 1; ++i) rave[i] = g->ravearr ? g->ravearr[i] : 0.5 * (g->rarr[i] + g->rarr[i + 1]);
+    int rc2;
+    if (!ctx->d_vel && ((rc2 = dalloc(ctx, &ctx->d_vel, 3 * ncell)) || (rc2 = dalloc(ctx, &ctx->d_tflag, ncell)) ||
+                        (rc2 = dalloc(ctx, &ctx->d_rave, nrg))))
+      return rc2;
+    CK(cudaMemcpyAsync(ctx->d_vel, g->vrarr, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_vel + ncell, g->vthetarr, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_vel + 2 * ncell, g->divvarr, ncell * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_tflag, tflag.data(), ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->d_rave, rave.data(), nrg * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));     // the host vectors go out of scope
+  }
+  ctx->have_vel = vel;
   CK(cudaStreamSynchronize(ctx->stream));
   DevModel& m = ctx->dm;
   const double* w = ctx->d_walls;
@@ -748,7 +970,10 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
 
 int mcrt_check_grid(const mcrt_config* c, const mcrt_grid* g, char* msg, int32_t msg_len) {
   auto bad = [&](int code, const char* fmt, auto... a) {
-    if (msg && msg_len > 0) snprintf(msg, (size_t)msg_len, fmt, a...);
+    if (msg && msg_len > 0) {
+      if constexpr (sizeof...(a) == 0) snprintf(msg, (size_t)msg_len, "%s", fmt);
+      else snprintf(msg, (size_t)msg_len, fmt, a...);
+    }
     return code;
   };
   if (msg && msg_len > 0) msg[0] = 0;
@@ -774,6 +999,10 @@ int mcrt_check_grid(const mcrt_config* c, const mcrt_grid* g, char* msg, int32_t
     if (i > 0 && !(g->phiarr[i] > g->phiarr[i - 1])) return bad(MCRT_ERR_ARG, "phiarr is not increasing at %d", i + 1);
   }
   const int64_t ncell = (int64_t)nrg * ntg * npg;
+  for (const double* v : {g->vrarr, g->vthetarr, g->divvarr})
+    if (v)
+      for (int64_t k = 0; k < ncell; ++k)
+        if (!std::isfinite(v[k])) return bad(MCRT_ERR_ARG, "velocity field entry %lld is not finite", (long long)k + 1);
   for (int64_t k = 0; k < ncell; ++k) {
     bool dust = false;
     for (int id = 0; id < MCRT_NDG2; ++id) {
@@ -1717,9 +1946,10 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
   CK(cudaSetDevice(ctx->device));
   const mcrt_config& c = ctx->cfg;
   const int64_t nc = ctx->ncell;
+  const int64_t n2 = (int64_t)c.nrg * c.ntg;
   double* d_td = nullptr;
   int rc;
-  if ((rc = dalloc(ctx, &d_td, 3 * nc))) return rc;
+  if ((rc = dalloc(ctx, &d_td, 3 * nc + (ctx->have_vel ? nc + 5 * n2 : 0)))) return rc;
   CK(cudaMemcpyAsync(d_td, tdave, nc * 8, cudaMemcpyHostToDevice, ctx->stream));
   TfinalArgs a{};
   a.nrg = c.nrg; a.ntg = c.ntg; a.npg = c.npg; a.nT = c.nT; a.nphot = nphot; a.maxii = iter > 3 ? 20 : 1;
@@ -1731,8 +1961,25 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
   a.idust3 = ctx->d_idust3; a.diffus = ctx->d_diffus;
   a.told = d_td; a.tnew = d_td + nc; a.tdave = d_td + 2 * nc;
   std::vector<double> old(tdave, tdave + nc);
-  tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
-  tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
+  if (!ctx->have_vel) {
+    tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
+    tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
+  } else {
+    // the passes work in place on tdave, starting from the previous field
+    a.vr = ctx->d_vel; a.vth = ctx->d_vel + nc; a.divv = ctx->d_vel + 2 * nc;
+    a.rarr = ctx->dm.rarr; a.thetarr = ctx->dm.thetarr; a.rave = ctx->d_rave; a.tflag = ctx->d_tflag;
+    a.acc = d_td + 3 * nc;
+    a.tsm = a.acc + nc; a.gtr = a.tsm + n2; a.gtt = a.gtr + n2; a.gtr2 = a.gtt + n2; a.gtt2 = a.gtr2 + n2;
+    CK(cudaMemcpyAsync(a.tdave, d_td, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    for (int ii = 1; ii <= a.maxii; ++ii) {
+      tfv_smooth<<<256, 128, 0, ctx->stream>>>(a);
+      tfv_grad<<<256, 128, 0, ctx->stream>>>(a, ii == 1 ? 1 : 0);
+      tfv_smooth_grad<<<256, 128, 0, ctx->stream>>>(a);
+      tfv_cells<<<256, 128, 0, ctx->stream>>>(a);
+      tfv_mirror<<<512, 256, 0, ctx->stream>>>(a, (a.maxii > 10 && ii > 10) ? 1 : 0, ii == 11 ? 1 : 0);
+    }
+    if (a.maxii > 10) tfv_average<<<512, 256, 0, ctx->stream>>>(a, a.maxii - 10);
+  }
   tdust_from_tdave<<<512, 256, 0, ctx->stream>>>(nc, a.tdave, ctx->d_diffus, ctx->d_idust3, ctx->d_cells, ctx->d_tdust);
   CK(cudaMemcpyAsync(ctx->d_tdust0, ctx->d_tdust, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaGetLastError());
@@ -1749,7 +1996,7 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
       const double told = old[k], tnew = tdave[k];
       const double d = (tnew - told) / tnew;
       if (tnew != told && tnew > T01 && told > T01) { s[0] += std::fabs(d); s2[0] += d * d; n[0]++; }
-      if (tnew > T01 && told > T01) { s[1] += std::fabs(d); s2[1] += d * d; n[1]++; }
+      if (!ctx->h_diffus[k] && tnew > T01 && told > T01) { s[1] += std::fabs(d); s2[1] += d * d; n[1]++; }
       if (ctx->h_rarr[ir - 1] / c.autors < 5.0 && tnew > T01 && told > T01) { s[2] += std::fabs(d); s2[2] += d * d; n[2]++; }
     }
   }
@@ -1779,6 +2026,9 @@ int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, 
   if (nc > kNoAllocMaxCells)
     return fail(ctx, MCRT_ERR_ARG, "mcrt_update_temperature_noalloc: %lld cells exceed its fixed scratch of %lld cells",
                 (long long)nc, (long long)kNoAllocMaxCells);
+  if (ctx->have_vel)
+    return fail(ctx, MCRT_ERR_UNSUPPORTED,
+                "mcrt_update_temperature_noalloc: a gas velocity field needs the pass buffers of mcrt_update_temperature");
   CK(cudaSetDevice(ctx->device));
   // the scratch array's device address, looked up once per context with the
   // context's device current (a new context, e.g. after a device reset,
@@ -1802,7 +2052,7 @@ int mcrt_update_temperature_noalloc(mcrt_ctx* ctx, int32_t nphot, int32_t iter, 
   a.told = d_told; a.tnew = d_tnew; a.tdave = d_res;
   tfinal_cells<<<256, 128, 0, ctx->stream>>>(a);
   tfinal_mirror<<<512, 256, 0, ctx->stream>>>(a);
-  tfinal_stats<<<128, 256, 0, ctx->stream>>>(c.nrg, c.ntg, d_told, d_res, ctx->dm.rarr, c.autors, d_stats);
+  tfinal_stats<<<128, 256, 0, ctx->stream>>>(c.nrg, c.ntg, d_told, d_res, ctx->dm.rarr, c.autors, ctx->d_diffus, d_stats);
   tdust_from_tdave<<<512, 256, 0, ctx->stream>>>(nc, d_res, ctx->d_diffus, ctx->d_idust3, ctx->d_cells, ctx->d_tdust);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ctx->d_tdust0, ctx->d_tdust, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));

@@ -675,6 +675,76 @@ def with_diffusion(m: Model, iteration: int = 2) -> Model:
     return setdiffus(m, m.grid["tdust"].copy(), iteration)
 
 
+def with_velocities(m: Model) -> Model:
+    """The gas velocity field gridset gives the envelope
+    (gridset_5_model13new.f90:1372-1412, 1439-1471): Ulrich infall,
+    vfall = sqrt(G (M* + Mdisk) / r) at the cell-centre radius, on the walls
+    of theta:
+        equator, r > Rc:  vr = -vfall sqrt(2 - Rc/r),  vtheta = 0
+        equator, r <= Rc: vr = -vfall,  vtheta = vfall sqrt(1 - r/Rc)
+        else:             vr = -vfall sqrt(1 + mu/mu0),
+                          vtheta = vfall (mu0 - mu)/sin(theta) sqrt(1 + mu/mu0)
+    with mu = |cos(theta)| and mu0 the streamline root (zerod.f90); the
+    divergence from the face averages of the upper hemisphere, mirrored
+    below.  Cells of the envelope component (id 3) take these values; the
+    disk and the cavity stay at rest (this model has no disk wind and no
+    expanding outer envelope, so the reference's wind and sonic-point
+    branches do not arise).  The pole walls, where the reference's vtheta
+    is 0/0, get vtheta = 0."""
+    w = m.w
+    nrg, ntg, npg = w.nrg, w.ntg, w.npg
+    autors = m.config["autors"]
+    rarr, thetarr = m.grid["rarr"], m.grid["thetarr"]
+    rave = 0.5 * (rarr[:-1] + rarr[1:])
+    rc = w.rc_au * autors
+    vfall = np.sqrt(GN * (w.massc + w.massd) * MSOL / rave / w.rstar / RSOL)      # [nrg-1]
+    vru = np.zeros((nrg, ntg))
+    vtu = np.zeros((nrg, ntg))
+    sint = np.sin(thetarr)
+    cost = np.abs(np.cos(thetarr))
+    rx = rave / rc
+    for ir in range(nrg - 1):
+        mu0 = Model._ulrich_mu0(cost.copy(), np.full(ntg, rx[ir]))
+        vr = -vfall[ir] * np.sqrt(1.0 + cost / mu0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            vt = np.where(sint > 1e-12, vfall[ir] * (mu0 - cost) / sint * np.sqrt(1.0 + cost / mu0), 0.0)
+        ieq = (ntg + 1) // 2 - 1
+        if ntg % 2 == 1:
+            if rave[ir] > rc:
+                vr[ieq] = -vfall[ir] * math.sqrt(2.0 - rc / rave[ir])
+                vt[ieq] = 0.0
+            else:
+                vr[ieq] = -vfall[ir]
+                vt[ieq] = vfall[ir] * math.sqrt(1.0 - rave[ir] / rc)
+        vru[ir], vtu[ir] = vr, vt
+    div = np.zeros((nrg, ntg))
+    nu = (ntg - 1) // 2
+    for ir in range(nrg - 1):
+        rad, rad1, rad2 = rave[ir], rarr[ir + 1], rarr[ir]
+        dr = rad1 - rad2
+        for it in range(nu):
+            t1, t2 = thetarr[it + 1], thetarr[it]
+            th = 0.5 * (t1 + t2)
+            dt = t1 - t2
+            vr1 = 0.5 * (vru[ir + 1, it + 1] + vru[ir + 1, it])
+            vr2 = 0.5 * (vru[ir, it + 1] + vru[ir, it])
+            vt1 = 0.5 * (vtu[ir + 1, it + 1] + vtu[ir, it + 1])
+            vt2 = 0.5 * (vtu[ir + 1, it] + vtu[ir, it])
+            div[ir, it] = ((rad1 ** 2 * vr1 - rad2 ** 2 * vr2) / dr / rad ** 2
+                           + (math.sin(t1) * vt1 - math.sin(t2) * vt2) / dt / rad / math.sin(th))
+        for it in range((ntg + 1) // 2 - 1, ntg - 1):
+            div[ir, it] = div[ir, ntg - 2 - it]
+    env = m.dens4()[..., 2] > 0.0                   # id 3: envelope
+    shape = (nrg, ntg, npg)
+    vr3 = np.where(env, np.broadcast_to(vru[:, :, None], shape), 0.0)
+    vt3 = np.where(env, np.broadcast_to(vtu[:, :, None], shape), 0.0)
+    dv3 = np.where(env, np.broadcast_to(div[:, :, None], shape), 0.0)
+    m.grid["vrarr"] = np.asfortranarray(vr3).ravel(order="F")
+    m.grid["vthetarr"] = np.asfortranarray(vt3).ravel(order="F")
+    m.grid["divvarr"] = np.asfortranarray(dv3).ravel(order="F")
+    return m
+
+
 LUCY_STATE_2D = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "reference_2d_tdave.npy")
 
 

@@ -106,6 +106,38 @@ def test_tfinal_matches_oracle(warm_small, oracle_mod):
     eng.close()
 
 
+def test_tfinal_with_velocity_field_matches_oracle(oracle_mod):
+    """tfinal with the envelope's infall field on the benchmark grid (the
+    passes of tfinal_5_test1.f90: smoothed temperatures and gradients,
+    dusttemp's adiabatic and advective terms), device against oracle on the
+    same dtauabs, one pass (iteration 2) and twenty averaged over the last
+    ten (iteration 5).  The diffusion flags are cleared so that every cell
+    goes through dusttemp."""
+    import copy
+    m = model.with_velocities(model.reference_2d_converged())
+    m.grid["diffus"] = np.zeros_like(m.grid["diffus"])
+    m.grid["diffdir"] = np.zeros_like(m.grid["diffdir"])
+    rest = copy.deepcopy(m)
+    for k in ("vrarr", "vthetarr", "divvarr"):
+        del rest.grid[k]
+    n = 200000
+    eng = _engine(m)
+    eng.reset_tallies()
+    eng.run(n, ipeel=0)
+    tg = eng.download(images=False)
+    env = (m.dens4()[..., 2] > 0).ravel(order="F")
+    for it in (2, 5):
+        eng.tdave = m.grid["tdust"].copy()
+        td_g, _, sig_g = eng.update_temperature(n, it)
+        td_o, sig_o = oracle_mod.tfinal(abi.Bundle(m), tg["dtauabs"], n, it, m.grid["tdust"])
+        assert np.allclose(td_g, td_o, rtol=1e-12, atol=0), np.abs(td_g / td_o - 1).max()
+        assert np.allclose(sig_g, sig_o, rtol=1e-9, equal_nan=True)
+        td_r, _ = oracle_mod.tfinal(abi.Bundle(rest), tg["dtauabs"], n, it, m.grid["tdust"])
+        change = np.abs(td_g / td_r - 1.0)
+        assert change[env].max() > 1e-4 and change[~env].max() == 0.0
+    eng.close()
+
+
 def test_multi_launch_sharding(warm_small):
     """Packet ranges are independent: two launches over halves of the range
     give the tallies of one launch over all of it (the per-rank split of the

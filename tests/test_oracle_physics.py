@@ -318,3 +318,28 @@ def test_isrf_table_has_the_reference_layout():
     # below 1.2398/lmin eV
     top = 1.2398 / (0.0912 * (1000.0 / 0.0912) ** (1.0 / 200))
     assert abs(10 ** lfr[-1] / top - 1.0) < 1e-9 and 10 ** lfr[1] > 1.2398 / 1000.0
+
+
+def test_tfinal_velocity_field_reduces_to_the_gas_at_rest(oracle_mod):
+    """With a velocity field of zeros the passes of tfinal give the result of
+    a gas at rest bit for bit (the adiabatic and advective terms are exact
+    zeros); the envelope's infall field changes the temperature of envelope
+    cells only, by well under a percent."""
+    import copy
+    from src3_mpi_cfitsio_b200 import abi, model
+    m = model.reference_2d_converged()
+    mv = model.with_velocities(copy.deepcopy(m))
+    mz = copy.deepcopy(mv)
+    for k in ("vrarr", "vthetarr", "divvarr"):
+        mz.grid[k] = np.zeros_like(mz.grid[k])
+    n = 100000
+    tal, _ = oracle_mod.run(abi.Bundle(m), n, ipeel=0, images=False)
+    env = (m.dens4()[..., 2] > 0).ravel(order="F")
+    for it in (2, 5):
+        a, _ = oracle_mod.tfinal(abi.Bundle(m), tal["dtauabs"], n, it, m.grid["tdust"])
+        b, _ = oracle_mod.tfinal(abi.Bundle(mz), tal["dtauabs"], n, it, m.grid["tdust"])
+        c, _ = oracle_mod.tfinal(abi.Bundle(mv), tal["dtauabs"], n, it, m.grid["tdust"])
+        assert np.array_equal(a, b)
+        rel = np.abs(c / a - 1.0)
+        assert rel[~env].max() == 0.0
+        assert 1e-5 < rel[env].max() < 1e-2
