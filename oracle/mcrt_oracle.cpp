@@ -1944,13 +1944,13 @@ static double dusttemp(const mcrt_config* c, const mcrt_tables* t, double na, in
   auto p4 = [](double x) { double x2 = x * x; return x2 * x2; };
   const double p3 = 11605.0 * 11605.0 * 11605.0;
   const double c1 = KB / 4.0 / SIGT / 2.3 / MHY, c2 = KB * 3.0 / 8.0 / SIGT / 2.3 / MHY;
-  const double gr = vr * gradtr + vthet * gradtt;
+  // the factor of Tint in the adiabatic term and the advective term, formed
+  // once per cell
+  const double adi = c1 / kv / p3 * divv / rstar / RSOL;
+  const double adv = c2 / kv / p3 * (vr * gradtr + vthet * gradtt) / rstar / RSOL;
   for (int i = 0; i < nT; ++i) {
     const double emi = p4(t->Tint[i]) * kp[i];
-    if (!vel) { kappaT[i] = emi; continue; }
-    const double adi = c1 / kv / p3 * t->Tint[i] * divv / rstar / RSOL;
-    const double adv = c2 / kv / p3 * gr / rstar / RSOL;
-    kappaT[i] = emi + adi + adv;
+    kappaT[i] = vel ? emi + adi * t->Tint[i] + adv : emi;
   }
   double Td = 0.1 / 11605.0;
   if (mcell > 0.0) {

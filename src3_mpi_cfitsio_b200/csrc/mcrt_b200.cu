@@ -213,21 +213,27 @@ __device__ __forceinline__ double p4(double x) { double x2 = x * x; return x2 * 
 // Tint^4 kappa_P plus, with a gas velocity field, the adiabatic term
 // (k/4/sigt/2.3/mH)/kappa_V/11605^3 * Tint*divv/rstar/rsol and the advective
 // term (3k/8/sigt/2.3/mH)/kappa_V/11605^3 * (vr gradtr + vthet gradtt)/
-// rstar/rsol (dusttemp_5.f90:42-53), in the reference's left-to-right order.
+// rstar/rsol (dusttemp_5.f90:42-53).  The factors of Tint and the constant
+// term are formed once per cell (dust_vel); the oracle forms them the same way.
 struct DustVel {
-  double divv, adv;          // divv; vr*gradtr + vthet*gradtt
+  double adi, adv;           // adiabatic term per unit Tint; advective term
   bool on;
 };
+__device__ __forceinline__ DustVel dust_vel(double kv, double rstar, double divv, double vgrad) {
+  constexpr double kB = 1.3806503e-16, sigt = 5.670400e-5, mH = 1.67262158e-24, rsol = 6.9598e10;
+  const double p3 = 11605.0 * 11605.0 * 11605.0;
+  const double c1 = kB / 4.0 / sigt / 2.3 / mH, c2 = kB * 3.0 / 8.0 / sigt / 2.3 / mH;
+  DustVel v;
+  v.adi = __ddiv_rn(__ddiv_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c1, kv), p3), divv), rstar), rsol);
+  v.adv = __ddiv_rn(__ddiv_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c2, kv), p3), vgrad), rstar), rsol);
+  v.on = true;
+  return v;
+}
 __device__ __forceinline__ double kappa_T(const double* Tint, const double* kp, int i, double kv, double rstar,
                                           const DustVel& v) {
   const double emi = __dmul_rn(p4(Tint[i]), kp[i]);
   if (!v.on) return emi;
-  constexpr double kB = 1.3806503e-16, sigt = 5.670400e-5, mH = 1.67262158e-24, rsol = 6.9598e10;
-  const double p3 = 11605.0 * 11605.0 * 11605.0;
-  const double c1 = kB / 4.0 / sigt / 2.3 / mH, c2 = kB * 3.0 / 8.0 / sigt / 2.3 / mH;
-  const double adi = __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c1, kv), p3), Tint[i]), v.divv), rstar), rsol);
-  const double adv = __ddiv_rn(__ddiv_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c2, kv), p3), v.adv), rstar), rsol);
-  return __dadd_rn(__dadd_rn(emi, adi), adv);
+  return __dadd_rn(__dadd_rn(emi, __dmul_rn(v.adi, Tint[i])), v.adv);
 }
 
 __device__ double dusttemp_dev(const double* Tint, const double* kp, int nT, double kv, double na, int nphot,
@@ -464,8 +470,9 @@ __global__ void tfv_cells(TfinalArgs a) {
         const double m2 = pow(dm * a.vcell[c], 0.25);
         const double* kp = a.kappap + (int64_t)a.nT * (sp - 1);
         const double gr = a.gtr2[c], gt = a.gtt2[c];
-        DustVel v1{a.divv[c], __dadd_rn(__dmul_rn(a.vr[c], gr), __dmul_rn(a.vth[c], gt)), true};
-        DustVel v2{a.divv[cm], __dadd_rn(__dmul_rn(a.vr[cm], gr), __dmul_rn(a.vth[cm], gt)), true};
+        const double kv = a.kappav[sp - 1];
+        const DustVel v1 = dust_vel(kv, a.rstar, a.divv[c], __dadd_rn(__dmul_rn(a.vr[c], gr), __dmul_rn(a.vth[c], gt)));
+        const DustVel v2 = dust_vel(kv, a.rstar, a.divv[cm], __dadd_rn(__dmul_rn(a.vr[cm], gr), __dmul_rn(a.vth[cm], gt)));
         const double t1 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[c], a.nphot, m1, a.rstar, a.tstar, v1);
         const double t2 = dusttemp_dev(a.Tint, kp, a.nT, a.kappav[sp - 1], a.dtauabs[cm], a.nphot, m2, a.rstar, a.tstar, v2);
         td = (t1 + t2) / 2.0;

@@ -61,6 +61,10 @@ struct Lane {
   int peel_ctx, peelid, peel_idust2;
   double peel_si, coslp, sinlp;
   unsigned long long c_pkt, c_int, c_sca, c_geo, c_kil, c_exit, c_star, c_jobs;
+  // the integer-valued scalar tallies (MCRT_S_*), counted per lane and added
+  // once per warp when the kernel ends: every exit and first interaction
+  // otherwise adds to the same few addresses
+  unsigned long long s_cnt[MCRT_NSCALARS];
   int64_t ray_steps;
   double adjA;                      // replay: summed C of the packet's peel-offs still ahead
   int64_t adj_pos, adj_end;         // replay: the packet's next record
@@ -72,6 +76,8 @@ struct Lane {
     ev = EV_FETCH;
     status = 0;
     c_pkt = c_int = c_sca = c_geo = c_kil = c_exit = c_star = c_jobs = 0;
+#pragma unroll
+    for (int i = 0; i < MCRT_NSCALARS; ++i) s_cnt[i] = 0;
   }
 
   __device__ __forceinline__ void ray_from_packet(bool peel) {
@@ -106,7 +112,7 @@ struct Lane {
   // position has been copied from the ray.
   __device__ void star_reemit() {
     const DevModel& m = pk.m;
-    atomicAdd(pk.T.scal + MCRT_S_AFLUX, 1.0);
+    ++s_cnt[MCRT_S_AFLUX];
     ++pk.nstar;
     pk.rtot = sqrt(pk.rsq);
     pk.initpabs();
@@ -576,7 +582,7 @@ struct Lane {
             if (m.iffuv && !Packet::is_fuv(pk.nub)) { status = 2; ev = EV_FINISH; break; }
             if (iint > 10000 || ++nev > kMaxEvents) {
               atomicAdd(pk.T.killed + pk.cidx(pk.ir, pk.it, pk.ip), 1);
-              atomicAdd(pk.T.scal + MCRT_S_ABFLUX, 1.0);
+              ++s_cnt[MCRT_S_ABFLUX];
               status = 1;
               ev = EV_FINISH;
               break;
@@ -588,7 +594,7 @@ struct Lane {
           if (k < 0) { status = 3; ev = EV_FINISH; break; }
           if (P.adj.mode == 2 && adjA != 0.0)   // replay: the interaction density at the segment's end
             atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1), adjA);
-          if (first) { atomicAdd(pk.T.scal + MCRT_S_TOT, 1.0); first = 0; }
+          if (first) { ++s_cnt[MCRT_S_TOT]; first = 0; }
           const int slot = cell_slot(c.meta, k);
           const int idust2 = cell_id(c.meta, k);
           if (pk.ran() <= pk.sp.alb(slot)) {     // scattered
@@ -689,10 +695,10 @@ struct Lane {
     const double rho2 = x * x + y * y;
     const DevTallies& T = pk.T;
     if (rho2 < __ldg(m.aperture2 + m.nap - 1) * 1.0001) {
-      atomicAdd(T.scal + MCRT_S_FLUX, 1.0);
+      ++s_cnt[MCRT_S_FLUX];
       if (pk.iflag == 1) {
-        atomicAdd(T.scal + MCRT_S_SFLUX, 1.0);
-        atomicAdd(T.scal + MCRT_S_NSCAT, (double)iscat);
+        ++s_cnt[MCRT_S_SFLUX];
+        s_cnt[MCRT_S_NSCAT] += (unsigned long long)iscat;
       }
     }
     const int inub = pk.freq_bin(pk.nub);
@@ -711,9 +717,18 @@ struct Lane {
         }
       }
     }
-    if (pk.iflag == 1) atomicAdd(T.scal + MCRT_S_SCOUNT, 1.0);
+    if (pk.iflag == 1) ++s_cnt[MCRT_S_SCOUNT];
   }
 };
+
+// The lanes' integer-valued scalar tallies into the FP64 scalars, one atomic
+// per warp and scalar (integers below 2^53: the sums are exact in any order).
+__device__ __forceinline__ void flush_scalars(const LaunchParams& P, const Lane& L) {
+  for (int i = 0; i < MCRT_NSCALARS; ++i) {
+    const unsigned long long x = warp_sum(L.s_cnt[i]);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(P.t.scal + i, (double)x);
+  }
+}
 
 // Warp-scheduled persistent kernel.  All 32 lanes of a warp stay in the loop
 // until every lane is out of packets, so the warp votes are well defined.
@@ -744,6 +759,7 @@ __device__ __forceinline__ void warp_loop(Lane& L, const LaunchParams& P) {
     unsigned long long x = warp_sum(v[i]);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(P.t.cnt + i, x);
   }
+  flush_scalars(P, L);
 }
 
 // Warp-scheduled persistent kernel.

@@ -186,6 +186,7 @@ __device__ __forceinline__ void flush_counters(const LaunchParams& P, const Lane
     unsigned long long x = warp_sum(v[i]);
     if ((threadIdx.x & 31) == 0 && x) atomicAdd(P.t.cnt + i, x);
   }
+  flush_scalars(P, L);
 }
 
 // Queue position of this lane among the lanes of `mask` that push to one

@@ -134,7 +134,7 @@ def test_tfinal_with_velocity_field_matches_oracle(oracle_mod):
         assert np.allclose(sig_g, sig_o, rtol=1e-9, equal_nan=True)
         td_r, _ = oracle_mod.tfinal(abi.Bundle(rest), tg["dtauabs"], n, it, m.grid["tdust"])
         change = np.abs(td_g / td_r - 1.0)
-        assert change[env].max() > 1e-4 and change[~env].max() == 0.0
+        assert change[env].max() > 1e-4 and change[~env].max() <= 1e-12
     eng.close()
 
 
