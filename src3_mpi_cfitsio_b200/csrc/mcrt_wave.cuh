@@ -111,28 +111,6 @@ __device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int n
   }
 }
 
-__device__ __forceinline__ void wave_save_event(const Lane& L, WaveRec& R, int nslot) {
-  const Packet& k = L.pk;
-  R.ux = k.ux; R.uy = k.uy; R.uz = k.uz;
-  R.cost = k.cost; R.sint = k.sint; R.cosp = k.cosp; R.sinp = k.sinp; R.phi = k.phi;
-  R.sip = k.sip; R.sqp = k.sqp; R.sup = k.sup; R.svp = k.svp; R.nub = k.nub;
-  R.cosb = k.cosb; R.sinb = k.sinb; R.lp = k.lp;
-  R.xpold = L.xpold; R.ypold = L.ypold; R.zpold = L.zpold;
-  R.peel_si = L.peel_si; R.coslp = L.coslp; R.sinlp = L.sinlp;
-  R.nev = L.nev; R.iphot = L.iphot; R.kfetch = L.kfetch;
-  R.iflag = k.iflag; R.i_orig = k.i_orig; R.nscat = k.nscat; R.nabsev = k.nabsev;
-  R.nstar = k.nstar; R.ndiffev = k.ndiffev;
-  R.iscat = L.iscat; R.iint = L.iint; R.first = L.first; R.slot_s = L.slot_s;
-  R.prev_r = L.prev_r; R.prev_t = L.prev_t; R.prev_p = L.prev_p;
-  R.peel_ctx = L.peel_ctx; R.peelid = L.peelid; R.peel_idust2 = L.peel_idust2;
-  for (int s = 0; s < nslot; ++s) {
-    R.spec[s] = k.sp.kapd(s);
-    R.spec[kMaxSlot + s] = k.sp.alb(s);
-    R.spec[2 * kMaxSlot + s] = k.sp.g(s);
-    R.spec[3 * kMaxSlot + s] = k.sp.pl(s);
-  }
-}
-
 #ifdef MCRT_MIXED
 // The mixed walk kernel's record I/O: the walk is set up in its
 // closest-approach form straight from the record (start point, direction,
@@ -178,6 +156,89 @@ __device__ __forceinline__ void wave_save_qwalk(const Lane& L, WaveRec& R) {
   }
 }
 #endif
+
+// The event kernel loads by event: the ray geometry only for a peel-off bin
+// (every other event starts a new ray), the peel-off state only in peeled
+// iterations (it is set and used within one visit otherwise), and the
+// species columns not for a packet that exits or ends (the next packet's
+// emission sets them).  Its save writes every group a later walk or event
+// reads.
+__device__ __forceinline__ void wave_load_state(Lane& L, const WaveRec& R) {
+  Packet& k = L.pk;
+  k.tau = R.tau; k.ifuv = R.ifuv;
+  L.ray_steps = R.ray_steps;
+  k.rng.s1 = R.s1; k.rng.s2 = R.s2; k.rng.ndraws = R.ndraws;
+  L.ev = R.ev; L.status = R.status;
+  k.ncross = R.ncross; k.exitflag = R.exitflag;
+}
+
+__device__ __forceinline__ void wave_load_raygeom(Lane& L, const WaveRec& R) {
+  Ray& y = L.ray;
+  y.x = R.x; y.y = R.y; y.z = R.z; y.rs = R.rs; y.rt = R.rt;
+  y.vx = R.vx; y.vy = R.vy; y.vz = R.vz; y.tsum = R.tsum;
+  y.r = R.r; y.t = R.t; y.p = R.p;
+  y.onw = (R.rbits & 1) != 0;
+  y.peel = (R.rbits & 2) != 0;
+#ifdef MCRT_MIXED
+  y.qready = false;
+#endif
+}
+
+__device__ __forceinline__ void wave_load_core(Lane& L, const WaveRec& R) {
+  Packet& k = L.pk;
+  k.ux = R.ux; k.uy = R.uy; k.uz = R.uz;
+  k.cost = R.cost; k.sint = R.sint; k.cosp = R.cosp; k.sinp = R.sinp; k.phi = R.phi;
+  k.sip = R.sip; k.sqp = R.sqp; k.sup = R.sup; k.svp = R.svp; k.nub = R.nub;
+  L.xpold = R.xpold; L.ypold = R.ypold; L.zpold = R.zpold;
+  L.nev = R.nev; L.iphot = R.iphot; L.kfetch = R.kfetch;
+  k.iflag = R.iflag; k.i_orig = R.i_orig; k.nscat = R.nscat; k.nabsev = R.nabsev;
+  k.nstar = R.nstar; k.ndiffev = R.ndiffev;
+  L.iscat = R.iscat; L.iint = R.iint; L.first = R.first; L.slot_s = R.slot_s;
+  L.prev_r = R.prev_r; L.prev_t = R.prev_t; L.prev_p = R.prev_p;
+}
+
+__device__ __forceinline__ void wave_load_peelstate(Lane& L, const WaveRec& R) {
+  Packet& k = L.pk;
+  k.cosb = R.cosb; k.sinb = R.sinb; k.lp = R.lp;
+  L.peel_si = R.peel_si; L.coslp = R.coslp; L.sinlp = R.sinlp;
+  L.peel_ctx = R.peel_ctx; L.peelid = R.peelid; L.peel_idust2 = R.peel_idust2;
+}
+
+__device__ __forceinline__ void wave_load_spec(Lane& L, const WaveRec& R, int nslot) {
+  Packet& k = L.pk;
+  for (int s = 0; s < nslot; ++s) {
+    k.sp.kapd(s) = R.spec[s];
+    k.sp.alb(s) = R.spec[kMaxSlot + s];
+    k.sp.g(s) = R.spec[2 * kMaxSlot + s];
+    k.sp.pl(s) = R.spec[3 * kMaxSlot + s];
+  }
+}
+
+__device__ __forceinline__ void wave_save_core(const Lane& L, WaveRec& R, int nslot) {
+  const Packet& k = L.pk;
+  R.ux = k.ux; R.uy = k.uy; R.uz = k.uz;
+  R.cost = k.cost; R.sint = k.sint; R.cosp = k.cosp; R.sinp = k.sinp; R.phi = k.phi;
+  R.sip = k.sip; R.sqp = k.sqp; R.sup = k.sup; R.svp = k.svp; R.nub = k.nub;
+  R.xpold = L.xpold; R.ypold = L.ypold; R.zpold = L.zpold;
+  R.nev = L.nev; R.iphot = L.iphot; R.kfetch = L.kfetch;
+  R.iflag = k.iflag; R.i_orig = k.i_orig; R.nscat = k.nscat; R.nabsev = k.nabsev;
+  R.nstar = k.nstar; R.ndiffev = k.ndiffev;
+  R.iscat = L.iscat; R.iint = L.iint; R.first = L.first; R.slot_s = L.slot_s;
+  R.prev_r = L.prev_r; R.prev_t = L.prev_t; R.prev_p = L.prev_p;
+  for (int s = 0; s < nslot; ++s) {
+    R.spec[s] = k.sp.kapd(s);
+    R.spec[kMaxSlot + s] = k.sp.alb(s);
+    R.spec[2 * kMaxSlot + s] = k.sp.g(s);
+    R.spec[3 * kMaxSlot + s] = k.sp.pl(s);
+  }
+}
+
+__device__ __forceinline__ void wave_save_peelstate(const Lane& L, WaveRec& R) {
+  const Packet& k = L.pk;
+  R.cosb = k.cosb; R.sinb = k.sinb; R.lp = k.lp;
+  R.peel_si = L.peel_si; R.coslp = L.coslp; R.sinlp = L.sinlp;
+  R.peel_ctx = L.peel_ctx; R.peelid = L.peelid; R.peel_idust2 = L.peel_idust2;
+}
 
 __device__ __forceinline__ void flush_counters(const LaunchParams& P, const Lane& L) {
   unsigned long long v[14] = {L.c_pkt, L.pk.c_cross, L.c_int, L.c_sca, L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin,
@@ -266,15 +327,21 @@ __global__ void __launch_bounds__(kBlock, MCRT_EVENT_MIN_BLOCKS) wave_event(Laun
       slot = k < nf ? W.evq[k] : W.evq[W.slots - 1 - (int64_t)(k - nf)];
       WaveRec& R = W.recs[slot];
       const int ev = R.ev;
+      const bool peeled = P.ipeel != 0;
       if (ev != EV_FETCH) {
-        wave_load_walk(L, R, nslot);
-        wave_load_event(L, R, nslot);
+        wave_load_state(L, R);
+        if (ev == EV_PEEL_BIN) wave_load_raygeom(L, R);
+        wave_load_pos(L, R);
+        wave_load_core(L, R);
+        if (peeled) wave_load_peelstate(L, R);
+        if (ev != EV_EXIT && ev != EV_FINISH) wave_load_spec(L, R, nslot);
       }
       L.ev = ev;
       L.events(P);
       if (L.ev == EV_NONE) {
         wave_save_walk(L, R);
-        wave_save_event(L, R, nslot);
+        wave_save_core(L, R, nslot);
+        if (peeled) wave_save_peelstate(L, R);
         walk = true;
       }
     }
