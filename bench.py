@@ -484,6 +484,8 @@ def run_ours(args, rank, world):
         amx = res["mixed"]
         tmask = (a64[4] > 1.0 / 11605.0) & (amx[4] > 1.0 / 11605.0)
         terr = np.abs(amx[4][tmask] / a64[4][tmask] - 1.0)
+        c64, cmx = a64[2].counters(), amx[2].counters()
+        c64p, cmxp = a64[3].counters(), amx[3].counters()
         extra = {
             "fp64_value": P / (a64[0] / 1e3), "mixed_value": P / (amx[0] / 1e3),
             "mixed_over_fp64": a64[0] / amx[0],
@@ -500,6 +502,12 @@ def run_ours(args, rank, world):
                                     "image_q_l1": _errors(a64[3], amx[3]).get("image_m_q"),
                                     "temperature_median_rel": float(np.median(terr)) if terr.size else None,
                                     "temperature_p99_rel": float(np.quantile(terr, 0.99)) if terr.size else None,
+                                    "crossings_rel": cmx["crossings"] / c64["crossings"] - 1.0,
+                                    "interactions_rel": cmx["interactions"] / c64["interactions"] - 1.0,
+                                    "peel_crossings_rel": (cmxp["peel_cross"] / c64p["peel_cross"] - 1.0
+                                                           if c64p["peel_cross"] else None),
+                                    "geom_fail": {"mixed": cmx["geom_fail"] + cmxp["geom_fail"],
+                                                  "fp64": c64["geom_fail"] + c64p["geom_fail"]},
                                     "note": "same packets and random streams; differences are Monte Carlo "
                                             "divergence of histories after FP32 scattering"},
         }

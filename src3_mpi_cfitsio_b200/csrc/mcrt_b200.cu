@@ -208,7 +208,7 @@ namespace mcrt {
 
 __device__ __forceinline__ double p4(double x) { double x2 = x * x; return x2 * x2; }
 
-// dusttemp (dusttemp_5.f90:8-152) for a zero velocity field
+// dusttemp (dusttemp_5.f90:8-152).
 // The emission side of dusttemp's balance at table temperature i:
 // Tint^4 kappa_P plus, with a gas velocity field, the adiabatic term
 // (k/4/sigt/2.3/mH)/kappa_V/11605^3 * Tint*divv/rstar/rsol and the advective
