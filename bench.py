@@ -681,9 +681,10 @@ def main():
                     help="packets per model of each autotuner trial")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
-    # 706 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
-    # launch over 2,097,152 walks, from an ncu capture of the 8e6-packet case
-    ap.add_argument("--traffic-per-walk", type=float, default=705.9,
+    # 777.5 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
+    # launch (FP32 walk) over 2,097,152 walks, from an ncu capture of the
+    # 8e6-packet case
+    ap.add_argument("--traffic-per-walk", type=float, default=777.5,
                     help="DRAM bytes per walk of the wave_walk kernel from an ncu capture")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

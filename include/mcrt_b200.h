@@ -367,6 +367,22 @@ int mcrt_adjoint(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo, int64_t iphot_hi, 
  * models without diffusion cells can need that.  Every chunk's forward pass
  * ends with its own tail of long-lived packets, so large chunks are faster. */
 int mcrt_set_adjoint_chunk(mcrt_ctx *ctx, int64_t packets);
+/* Control variate of the adjoint's replay.  No reference counterpart.  A
+ * segment's score (delta at the interaction minus the optical depth of the
+ * segment, per cell and component) has zero mean given the segment's start,
+ * so it may be weighted by A - B instead of A, for any B fixed before the
+ * segment: the gradient stays unbiased, and its variance drops where B is
+ * close to A (the peel-off contributions still ahead of the packet).  With
+ * nfb > 0, mcrt_adjoint first replays `pilot_packets` packets of another
+ * generator (generator % 32 + 1, independent of the range) and tabulates
+ * the mean A per (cell, frequency bin, direction class); bins with fewer
+ * than `min_count` segment starts get B = 0.  Frequency bins: nfb
+ * log-uniform bins of the SED's range (numin, lnurat); direction classes
+ * (ndir = 4): radially outward or inward x moving away from or toward the
+ * midplane (ndir = 1: none).  The replay then covers every packet of the
+ * range, not only those with peel-off records.  Device memory: three
+ * arrays of ncell*nfb*ndir doubles.  nfb = 0 switches it off (default). */
+int mcrt_set_adjoint_baseline(mcrt_ctx *ctx, int32_t nfb, int32_t ndir, int64_t pilot_packets, double min_count);
 
 /* Recompute the diffusion cells' end-of-iteration temperature of the last
  * mcrt_run_iteration from the (reduced) diffusion absorption counts and the

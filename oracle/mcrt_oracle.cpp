@@ -259,6 +259,18 @@ struct Adjoint {
   std::vector<std::pair<int, double>> ev;   // (event index, C) of the packet, in event order
   size_t pos = 0;
   std::vector<std::pair<int64_t, double>> cross;   // crossings of the current peel ray: (cell, length)
+  // Control variate: a segment's score is weighted by A - B instead of A,
+  // with B = vtab[cell, frequency bin] of the segment's start state, a
+  // table fixed before the run (the score of a segment has zero mean given
+  // its start, so any such B leaves the estimate unbiased).  vsum/vcnt, if
+  // set, collect A per (cell, bin) at segment starts to build such a table.
+  const double* vtab = nullptr;
+  double* vsum = nullptr;
+  double* vcnt = nullptr;
+  int nfb = 1, ndir = 1;
+  double lnumin = 0.0, lnurat = 1.0;
+  double B = 0.0;
+  double W() const { return A - B; }
 };
 
 struct Packet {
@@ -690,10 +702,10 @@ struct Packet {
 
   void tally_abs(int ir, int it, int ip, double len) {   // tauint_3d_2_fuv.f90:83-98, 122-144
     int64_t c = m->cidx(ir, it, ip);
-    if (adj && adj->replay && adj->A != 0.0) {
+    if (adj && adj->replay && adj->W() != 0.0) {
       for (int id = 1; id <= MCRT_NDG2; ++id) {
         const double d = m->dens(ir, it, ip, id);
-        if (d > 0.0) (*adj->grad)[c + m->ncell * (id - 1)] -= adj->A * (kapd[m->fopac(ir, it, ip, id) - 1] * d * len);
+        if (d > 0.0) (*adj->grad)[c + m->ncell * (id - 1)] -= adj->W() * (kapd[m->fopac(ir, it, ip, id) - 1] * d * len);
       }
     }
     for (int id = 1; id <= MCRT_NDG2; ++id) {
@@ -1499,16 +1511,28 @@ struct Packet {
   // ------------------------------------------------------------ adjoint
   // Replay: before the walk that follows interaction k (k = nscat + nabsev;
   // 0 after the emission), drop the peel-offs of event k from A.
-  void adjoint_advance() {
+  void adjoint_advance(const int* ii) {
     if (!adj || !adj->replay) return;
     const int k = nscat + nabsev;
     while (adj->pos < adj->ev.size() && adj->ev[adj->pos].first <= k) adj->A -= adj->ev[adj->pos++].second;
+    if (adj->vtab || adj->vsum) {
+      int fb = (int)((double)adj->nfb * (std::log(nub) - adj->lnumin) / adj->lnurat);
+      fb = std::min(std::max(fb, 0), adj->nfb - 1);
+      int db = 0;
+      if (adj->ndir == 4) {     // outward / inward radially, away from / toward the midplane
+        const double ux_ = sint * cosp, uy_ = sint * sinp, uz_ = cost;
+        db = (ux_ * xp + uy_ * yp + uz_ * zp > 0.0 ? 1 : 0) + (uz_ * zp > 0.0 ? 2 : 0);
+      }
+      const int64_t v = (m->cidx(ii[0], ii[1], ii[2]) * adj->nfb + fb) * adj->ndir + db;
+      if (adj->vtab) adj->B = adj->vtab[v];
+      if (adj->vsum) { adj->vsum[v] += adj->A; adj->vcnt[v] += 1.0; }
+    }
   }
   // Replay: the interaction density kapd*rho of the selected component at
   // the end of the segment.
   void adjoint_interaction(int ir, int it, int ip, int idust2) {
-    if (!adj || !adj->replay || adj->A == 0.0) return;
-    (*adj->grad)[m->cidx(ir, it, ip) + m->ncell * (idust2 - 1)] += adj->A;
+    if (!adj || !adj->replay || adj->W() == 0.0) return;
+    (*adj->grad)[m->cidx(ir, it, ip) + m->ncell * (idust2 - 1)] += adj->W();
   }
   // Pass 1: weighted contribution of one binned peel-off and its -C*tau
   // terms along the recorded ray.
@@ -1623,7 +1647,7 @@ struct Packet {
     exitflag = 0;
     int iscat = 0, iint = 0, idust2 = 0;
     int64_t nev = 0;
-    adjoint_advance();
+    adjoint_advance(ii);
     tau = -std::log(ran());
     if (!tauint(ii[0], ii[1], ii[2])) return 3;
     int ir = ii[0], it = ii[1], ip = ii[2];
@@ -1677,7 +1701,7 @@ struct Packet {
           if (ipeel == 1 && !c.partial_peeloff) peel_all(sip, ii[0], ii[1], ii[2], idust2);
           ++iint;
         }
-        adjoint_advance();
+        adjoint_advance(ii);
         tau = -std::log(ran());
         xpold = xp; ypold = yp; zpold = zp;
         ux = sint * cosp;
@@ -2135,11 +2159,18 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
 // iteration with peel-offs, objective and dL/dlog(rho) per (cell, component
 // id) summed into grad[ncell*10] (Fortran order (nrg,ntg,npg,10)), objective
 // into *obj.  Test infrastructure: the FP64 reference of mcrt_adjoint.
-extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables* tab, int64_t np,
-                              int64_t iphot_lo, int64_t iphot_hi, int32_t iter, int32_t seed1, int32_t seed2,
-                              int32_t generator, int32_t nthreads, const double* lam_psed, const double* lam_img,
-                              double* grad, double* obj) {
-  if (iter < 1 || !lam_psed || !grad || !obj) return MCRT_ERR_ARG;
+// With `vtab` (ncell x nfb, cell-major) every segment's score is weighted
+// by A - vtab[cell, bin] (Adjoint::vtab) and every packet is replayed; with
+// `vsum`/`vcnt` (same shape) the replay adds A and 1 per segment start.  The
+// frequency bins split [numin, numin*e^lnurat] (the SED's range) into nfb
+// log-uniform bins.
+extern "C" int oracle_adjoint_cv(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables* tab, int64_t np,
+                                 int64_t iphot_lo, int64_t iphot_hi, int32_t iter, int32_t seed1, int32_t seed2,
+                                 int32_t generator, int32_t nthreads, const double* lam_psed, const double* lam_img,
+                                 double* grad, double* obj, const double* vtab, int32_t nfb, double* vsum,
+                                 double* vcnt) {
+  if (iter < 1 || !lam_psed || !grad || !obj || nfb == 0 || ((vsum != nullptr) != (vcnt != nullptr)))
+    return MCRT_ERR_ARG;
   const int64_t block0 = (int64_t)(iter - 1) * np;
   Model m;
   m.c = *cfg;
@@ -2178,6 +2209,11 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
   for (auto& t : tl) t.init(m.ncell, nsed, npsed);
   std::vector<std::vector<double>> gl(nt, std::vector<double>(m.ncell * MCRT_NDG2, 0.0));
   std::vector<double> objs(nt, 0.0);
+  const int ndir = nfb < 0 ? 4 : 1;
+  if (nfb < 0) nfb = -nfb;
+  const int64_t nv = vsum ? m.ncell * nfb * ndir : 0;
+  std::vector<std::vector<double>> vs(nt, std::vector<double>(nv, 0.0)), vc(nt, std::vector<double>(nv, 0.0));
+  const bool all = vtab || vsum;       // the control variate scores packets without peel-offs too
   std::atomic<int64_t> next(iphot_lo);
   auto worker = [&](int tid) {
     Packet p;
@@ -2185,6 +2221,12 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
     A.lam_psed = lam_psed;
     A.lam_img = cfg->output_imcube ? lam_img : nullptr;
     A.grad = &gl[tid];
+    A.vtab = vtab;
+    A.nfb = nfb;
+    A.ndir = ndir;
+    A.lnumin = std::log(cfg->numin);
+    A.lnurat = cfg->lnurat;
+    if (vsum) { A.vsum = vs[tid].data(); A.vcnt = vc[tid].data(); }
     p.m = &m; p.T = &tl[tid]; p.I = &img; p.adj = &A;
     for (auto* v : {&p.kappa, &p.albedo, &p.g, &p.pl, &p.g2, &p.onemg2, &p.g2p1, &p.twog, &p.kapd}) v->assign(cfg->nopac, 0.0);
     for (;;) {
@@ -2201,10 +2243,10 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
         p.run(iphot, np, ns, npacc, npaccstar, ips);
         double R = 0.0;
         for (const auto& e : A.ev) R += e.second;
-        if (R == 0.0) continue;
+        if (R == 0.0 && !all) continue;
         // pass 2: replay on the same stream, scoring the segments
         A.record = false; A.replay = true;
-        A.A = R; A.pos = 0;
+        A.A = R; A.pos = 0; A.B = 0.0;
         p.ipeel = 0;
         p.rng = stream(seed1, seed2, generator, block0 + iphot - 1);
         p.nscat = p.nabsev = p.ncross = p.nstar = p.ndiffev = 0;
@@ -2226,7 +2268,21 @@ extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, con
   double o = 0.0;
   for (int i = 0; i < nt; ++i) o += objs[i];
   *obj = o;
+  for (int64_t k = 0; k < nv; ++k) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < nt; ++i) { a += vs[i][k]; b += vc[i][k]; }
+    vsum[k] += a;
+    vcnt[k] += b;
+  }
   return MCRT_OK;
+}
+
+extern "C" int oracle_adjoint(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables* tab, int64_t np,
+                              int64_t iphot_lo, int64_t iphot_hi, int32_t iter, int32_t seed1, int32_t seed2,
+                              int32_t generator, int32_t nthreads, const double* lam_psed, const double* lam_img,
+                              double* grad, double* obj) {
+  return oracle_adjoint_cv(cfg, grid, tab, np, iphot_lo, iphot_hi, iter, seed1, seed2, generator, nthreads, lam_psed,
+                           lam_img, grad, obj, nullptr, 1, nullptr, nullptr);
 }
 
 // ===================================================================

@@ -81,6 +81,8 @@ def load():
                                        C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
                                        C.c_int32, C.c_int32, D, D, D, D]
         lib.oracle_adjoint.restype = C.c_int
+        lib.oracle_adjoint_cv.argtypes = lib.oracle_adjoint.argtypes + [D, C.c_int32, D, D]
+        lib.oracle_adjoint_cv.restype = C.c_int
         lib.oracle_rng.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.oracle_inczeta.argtypes = [C.POINTER(C.c_double)]
@@ -171,6 +173,39 @@ def adjoint(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img: np
     if rc != 0:
         raise RuntimeError(f"oracle_adjoint failed with code {rc}")
     return grad, obj.value
+
+
+def adjoint_cv(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img: np.ndarray | None = None,
+               lo: int = 1, hi: int | None = None, *, vtab: np.ndarray | None = None, nfb: int = 1,
+               learn: bool = False, iteration: int = 1, seeds=(12345678, 87654321), generator: int = 1,
+               threads: int | None = None):
+    """``adjoint`` with the control variate: every segment's score weighted
+    by A - vtab[cell, frequency bin] (vtab: [ncell*nfb], cell-major; None =
+    no baseline).  Returns (grad, L, vsum, vcnt); with learn=True vsum/vcnt
+    hold the summed A and the count per (cell, bin) at segment starts."""
+    lib = load()
+    hi = np_total if hi is None else hi
+    threads = threads or os.cpu_count() or 1
+    c = bundle.config
+    ncell = c.nrg * c.ntg * c.npg
+    lp = np.ascontiguousarray(lam_psed, dtype=np.float64)
+    li = None if lam_img is None else np.ascontiguousarray(lam_img, dtype=np.float64)
+    vt = None if vtab is None else np.ascontiguousarray(vtab, dtype=np.float64)
+    nv = ncell * abs(nfb) * (4 if nfb < 0 else 1)
+    if vt is not None and vt.size != nv:
+        raise ValueError("vtab must hold ncell*nfb values")
+    grad = np.zeros(ncell * 10, np.float64)
+    vs = np.zeros(nv, np.float64) if learn else None
+    vc = np.zeros(nv, np.float64) if learn else None
+    obj = C.c_double(0.0)
+    D = C.POINTER(C.c_double)
+    P = (lambda a: a.ctypes.data_as(D) if a is not None else None)
+    rc = lib.oracle_adjoint_cv(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables), np_total, lo,
+                               hi, iteration, seeds[0], seeds[1], generator, threads, lp.ctypes.data_as(D), P(li),
+                               grad.ctypes.data_as(D), C.byref(obj), P(vt), nfb, P(vs), P(vc))
+    if rc != 0:
+        raise RuntimeError(f"oracle_adjoint_cv failed with code {rc}")
+    return grad, obj.value, vs, vc
 
 
 def setemiss(nudust, kappad, adust, nlambda, nT: int = 500, nnu: int = 513, ndg: int | None = None,

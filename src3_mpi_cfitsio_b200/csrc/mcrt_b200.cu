@@ -92,6 +92,12 @@ struct mcrt_ctx {
   int64_t adj_chunk = (int64_t)1 << 25;   // packets per adjoint chunk (halved when its records reach 2^31)
   double* d_adj_sum = nullptr;        // [ncell*10 + 1] gradient and objective summed over chunks
   int64_t adj_sort_cap = 0;           // capacity of the sorted copies (skey, sc) and the sort scratch
+  // control variate of the replay (mcrt_set_adjoint_baseline)
+  int32_t cv_nfb = 0, cv_ndir = 1;
+  int64_t cv_pilot = 0;
+  double cv_min_count = 16.0;
+  int64_t cv_cap = 0;                 // entries of cv_tab / cv_sum / cv_cnt
+  double *cv_tab = nullptr, *cv_sum = nullptr, *cv_cnt = nullptr;
   bool have_grid = false, have_tables = false;
   bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
   bool have_isrf = false;             // ISRF sampling table uploaded (external-illumination packets)
@@ -1673,11 +1679,57 @@ __global__ void add_doubles(const double* src, double* dst, int64_t n) {
     dst[i] += src[i];
 }
 
+// The control variate from a learning replay: the mean A per bin, 0 where
+// fewer than min_count segments started in the bin.
+__global__ void cv_table(const double* sum, const double* cnt, double min_count, double* tab, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    tab[i] = cnt[i] >= min_count ? sum[i] / cnt[i] : 0.0;
+}
+
+// Chunks of lo..hi; with `sum` the chunk gradients and objectives are added
+// into sum[ncell*10 + 1].
+int adjoint_range(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t seed1, int32_t seed2,
+                  int32_t generator, double* sum, double* total_ms) {
+  AdjointArgs& A = ctx->adj;
+  const int64_t ncell = ctx->ncell;
+  int rc;
+  int64_t chunk = std::min<int64_t>(hi - lo + 1, ctx->adj_chunk);
+  for (int64_t c_lo = lo; c_lo <= hi;) {
+    const int64_t c_hi = std::min(hi, c_lo + chunk - 1);
+    bool too_many = false;
+    if ((rc = adjoint_chunk(ctx, np, c_lo, c_hi, iter, seed1, seed2, generator, total_ms, &too_many))) return rc;
+    if (too_many) {
+      if (c_hi == c_lo) return fail(ctx, MCRT_ERR_ARG, "adjoint: one packet with 2^31 peel-off records");
+      chunk = std::max<int64_t>(1, (c_hi - c_lo + 1) / 2);
+      continue;
+    }
+    if (sum) {
+      add_doubles<<<256, 256, 0, ctx->stream>>>(A.grad, sum, ncell * 10);
+      add_doubles<<<1, 32, 0, ctx->stream>>>(A.obj, sum + ncell * 10, 1);
+      CK(cudaGetLastError());
+    }
+    c_lo = c_hi + 1;
+  }
+  return MCRT_OK;
+}
+
 }  // namespace
 
 int mcrt_set_adjoint_chunk(mcrt_ctx* ctx, int64_t packets) {
   if (!ctx || packets < 1 || packets >= ((int64_t)1 << 31)) return MCRT_ERR_ARG;
   ctx->adj_chunk = packets;
+  return MCRT_OK;
+}
+
+int mcrt_set_adjoint_baseline(mcrt_ctx* ctx, int32_t nfb, int32_t ndir, int64_t pilot_packets, double min_count) {
+  if (!ctx) return MCRT_ERR_ARG;
+  if (nfb == 0) { ctx->cv_nfb = 0; return MCRT_OK; }
+  if (nfb < 0 || nfb > 1000 || (ndir != 1 && ndir != 4) || pilot_packets < 1 || !(min_count >= 1.0))
+    return fail(ctx, MCRT_ERR_ARG, "adjoint baseline: need 1 <= nfb <= 1000, ndir 1 or 4, pilot >= 1, min_count >= 1");
+  ctx->cv_nfb = nfb;
+  ctx->cv_ndir = ndir;
+  ctx->cv_pilot = pilot_packets;
+  ctx->cv_min_count = min_count;
   return MCRT_OK;
 }
 
@@ -1689,7 +1741,6 @@ int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter
   const mcrt_config& c = ctx->cfg;
   if (c.npeel < 1) return fail(ctx, MCRT_ERR_ARG, "the adjoint differentiates peeled outputs: npeel must be >= 1");
   if (ctx->dm.nslot > kJobSlots) return fail(ctx, MCRT_ERR_UNSUPPORTED, "adjoint needs at most %d opacity species", kJobSlots);
-  const int64_t npk = hi - lo + 1;
   CK(cudaSetDevice(ctx->device));
   const int64_t ncell = ctx->ncell;
   AdjointArgs& A = ctx->adj;
@@ -1710,25 +1761,44 @@ int mcrt_adjoint(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter
   }
   if (!ctx->d_adj_sum && (rc = dalloc(ctx, &ctx->d_adj_sum, (size_t)ncell * 10 + 1))) return rc;
   CK(cudaMemsetAsync(ctx->d_adj_sum, 0, ((size_t)ncell * 10 + 1) * 8, ctx->stream));
+  double total_ms = 0.0;
+  A.vtab = nullptr; A.vsum = nullptr; A.vcnt = nullptr; A.all = 0;
+  if (ctx->cv_nfb > 0) {
+    // Control variate: a learning replay of cv_pilot packets on another
+    // generator (independent of lo..hi) gives the mean A per bin; the
+    // replay of lo..hi then weights every segment's score by A - mean.
+    const int64_t nv = ncell * ctx->cv_nfb * ctx->cv_ndir;
+    if (ctx->cv_cap < nv) {
+      for (double* q : {ctx->cv_tab, ctx->cv_sum, ctx->cv_cnt})
+        if (q) dfree(ctx, q);
+      ctx->cv_tab = ctx->cv_sum = ctx->cv_cnt = nullptr;
+      ctx->cv_cap = 0;
+      if ((rc = dalloc(ctx, &ctx->cv_tab, nv)) || (rc = dalloc(ctx, &ctx->cv_sum, nv)) || (rc = dalloc(ctx, &ctx->cv_cnt, nv)))
+        return rc;
+      ctx->cv_cap = nv;
+    }
+    CK(cudaMemsetAsync(ctx->cv_sum, 0, (size_t)nv * 8, ctx->stream));
+    CK(cudaMemsetAsync(ctx->cv_cnt, 0, (size_t)nv * 8, ctx->stream));
+    A.nfb = ctx->cv_nfb;
+    A.ndir = ctx->cv_ndir;
+    A.lnumin = log(c.numin);
+    A.lnurat = c.lnurat;
+    A.vsum = ctx->cv_sum;
+    A.vcnt = ctx->cv_cnt;
+    A.all = 1;
+    rc = adjoint_range(ctx, ctx->cv_pilot, 1, ctx->cv_pilot, iter, seed1, seed2, generator % 32 + 1, nullptr, &total_ms);
+    A.vsum = nullptr; A.vcnt = nullptr;
+    if (rc) { A.all = 0; return rc; }
+    cv_table<<<256, 256, 0, ctx->stream>>>(ctx->cv_sum, ctx->cv_cnt, ctx->cv_min_count, ctx->cv_tab, nv);
+    CK(cudaGetLastError());
+    A.vtab = ctx->cv_tab;
+  }
   // Packets are independent here (diffusion heating is frozen), so the
   // gradient and the objective of lo..hi are the sums over chunks; a chunk
   // whose records would reach 2^31 is redone in halves.
-  double total_ms = 0.0;
-  int64_t chunk = std::min<int64_t>(npk, ctx->adj_chunk);
-  for (int64_t c_lo = lo; c_lo <= hi;) {
-    const int64_t c_hi = std::min(hi, c_lo + chunk - 1);
-    bool too_many = false;
-    if ((rc = adjoint_chunk(ctx, np, c_lo, c_hi, iter, seed1, seed2, generator, &total_ms, &too_many))) return rc;
-    if (too_many) {
-      if (c_hi == c_lo) return fail(ctx, MCRT_ERR_ARG, "adjoint: one packet with 2^31 peel-off records");
-      chunk = std::max<int64_t>(1, (c_hi - c_lo + 1) / 2);
-      continue;
-    }
-    add_doubles<<<256, 256, 0, ctx->stream>>>(A.grad, ctx->d_adj_sum, ncell * 10);
-    add_doubles<<<1, 32, 0, ctx->stream>>>(A.obj, ctx->d_adj_sum + ncell * 10, 1);
-    CK(cudaGetLastError());
-    c_lo = c_hi + 1;
-  }
+  rc = adjoint_range(ctx, np, lo, hi, iter, seed1, seed2, generator, ctx->d_adj_sum, &total_ms);
+  A.vtab = nullptr; A.all = 0;
+  if (rc) return rc;
   ctx->last_ms = total_ms;
   CK(cudaMemcpyAsync(grad, ctx->d_adj_sum, (size_t)ncell * 10 * 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(objective, ctx->d_adj_sum + ncell * 10, 8, cudaMemcpyDeviceToHost, ctx->stream));

@@ -193,6 +193,18 @@ struct AdjointArgs {
   const int64_t* end;
   const unsigned long long* skey;  // replay: sorted records
   const double* sc;
+  // Replay control variate: each segment's score is weighted by A - B with
+  // B = vtab[(cell*nfb + frequency bin)*ndir + direction class] of the
+  // segment's start state (nullptr: B = 0).  vsum/vcnt (learning replay):
+  // A and 1 added per segment start.  all != 0: every packet of the range is
+  // replayed, not only those with records (B also weights packets whose A
+  // is zero).
+  const double* vtab;
+  double* vsum;
+  double* vcnt;
+  int32_t nfb, ndir;
+  int32_t all, pad2_;
+  double lnumin, lnurat;           // frequency bins: nfb log-uniform bins of [numin, numin*exp(lnurat)]
 };
 constexpr int kAdjEvBits = 24;    // event index bits of a record key
 

@@ -67,6 +67,7 @@ struct Lane {
   unsigned long long s_cnt[MCRT_NSCALARS];
   int64_t ray_steps;
   double adjA;                      // replay: summed C of the packet's peel-offs still ahead
+  double adjB;                      // replay: the control variate of the current segment
   int64_t adj_pos, adj_end;         // replay: the packet's next record
 
   __device__ Lane(const DevModel& m, const DevTallies& t, double* sbase, float* fbase = nullptr) : pk(m, t, sbase, fbase) {
@@ -167,18 +168,19 @@ struct Lane {
     pk.cell_coefs(c, opac, absc);
     if (!R.peel) {
       const double dtau = (double)__fmul_rn(opac, (float)dt);
-      if (__dadd_rn(R.tsum, dtau) > pk.tau) {
-        const double ds = __ddiv_rn(__dsub_rn(pk.tau, R.tsum), (double)opac);
-        pk.tally_absf(ci, absc, ds);
-        if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)ds);
-        g.q = __dadd_rn(g.q, ds);
+      // The walk piece in this cell: to the interaction point if the
+      // sampled tau is reached here (tauint :69-111), else the whole crossing.
+      const bool hit = __dadd_rn(R.tsum, dtau) > pk.tau;
+      const double len = hit ? __ddiv_rn(__dsub_rn(pk.tau, R.tsum), (double)opac) : dt;
+      pk.tally_absf(ci, absc, len);
+      if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)len);
+      if (hit) {
+        g.q = __dadd_rn(g.q, len);
         R.onw = false;
         if (!kStarEvent) packet_from_ray();
         ev = EV_AFTER_WALK;
         return;
       }
-      pk.tally_absf(ci, absc, dt);
-      if (P.adj.mode == 2) adjoint_scoref(P, ci, c, (float)dt);
       R.tsum = __dadd_rn(R.tsum, dtau);
     } else {
       R.tsum = __dadd_rn(R.tsum, (double)__fmul_rn(opac, (float)dt));
@@ -223,11 +225,12 @@ struct Lane {
 
   // Replay: -A * tau of a walk piece in cell ci, per component (FP32 cell).
   __device__ __forceinline__ void adjoint_scoref(const LaunchParams& P, int64_t ci, const CellRecF& c, float len) {
-    if (adjA == 0.0) return;
+    const double w = adjA - adjB;
+    if (w == 0.0) return;
     const int n = cell_n(c.meta);
     for (int k = 0; k < n; ++k) {
       const int id = cell_id(c.meta, k);
-      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(adjA * (double)(pk.kf(cell_slot(c.meta, k)) * c.rho[k] * len)));
+      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(w * (double)(pk.kf(cell_slot(c.meta, k)) * c.rho[k] * len)));
     }
   }
 #else
@@ -303,11 +306,12 @@ struct Lane {
   // ------------------------------------------------------------ adjoint
   // Replay: -A * tau of a walk piece of length len in cell ci, per component.
   __device__ __forceinline__ void adjoint_score(const LaunchParams& P, int64_t ci, const CellRec& c, double len) {
-    if (adjA == 0.0) return;
+    const double w = adjA - adjB;
+    if (w == 0.0) return;
     const int n = cell_n(c.meta);
     for (int k = 0; k < n; ++k) {
       const int id = cell_id(c.meta, k);
-      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(adjA * (pk.sp.kapd(cell_slot(c.meta, k)) * c.rho[k] * len)));
+      atomicAdd(P.adj.grad + ci + pk.m.ncell * (id - 1), -(w * (pk.sp.kapd(cell_slot(c.meta, k)) * c.rho[k] * len)));
     }
   }
   // Replay: before the walk that follows event k (0 = emission, else the
@@ -317,6 +321,18 @@ struct Lane {
     const unsigned long long k = (unsigned long long)(pk.nscat + pk.nabsev);
     const unsigned long long mask = (1ull << kAdjEvBits) - 1ull;
     while (adj_pos < adj_end && (P.adj.skey[adj_pos] & mask) <= k) adjA -= P.adj.sc[adj_pos++];
+    if (P.adj.vtab || P.adj.vsum) {   // the control variate's (cell, frequency, direction) bin
+      int fb = (int)((double)P.adj.nfb * (log(pk.nub) - P.adj.lnumin) / P.adj.lnurat);
+      fb = min(max(fb, 0), P.adj.nfb - 1);
+      int db = 0;
+      if (P.adj.ndir == 4) {          // outward / inward radially, away from / toward the midplane
+        const double ux = pk.sint * pk.cosp, uy = pk.sint * pk.sinp, uz = pk.cost;
+        db = (ux * pk.xp + uy * pk.yp + uz * pk.zp > 0.0 ? 1 : 0) + (uz * pk.zp > 0.0 ? 2 : 0);
+      }
+      const int64_t v = (pk.cidx(pk.ir, pk.it, pk.ip) * P.adj.nfb + fb) * P.adj.ndir + db;
+      if (P.adj.vtab) adjB = P.adj.vtab[v];
+      if (P.adj.vsum) { atomicAdd(P.adj.vsum + v, adjA); atomicAdd(P.adj.vcnt + v, 1.0); }
+    }
   }
 
   // Queue a peel-off job for the peel kernel; false if the queue is full
@@ -444,12 +460,13 @@ struct Lane {
         case EV_FETCH: {
           if (P.fetch_off) { ev = EV_DONE; return; }
           const unsigned long long k = atomicAdd(P.next, 1ull);
-          if (P.adj.mode == 2) {          // replay: the packets that have peel-off records
-            if ((int64_t)k >= P.adj.nlist) { ev = EV_DONE; return; }
-            kfetch = P.adj.list[k];
+          if (P.adj.mode == 2) {          // replay: the packets that have peel-off records (or all)
+            if ((int64_t)k >= (P.adj.all ? P.hi - P.lo + 1 : P.adj.nlist)) { ev = EV_DONE; return; }
+            kfetch = P.adj.all ? (int64_t)k : (int64_t)P.adj.list[k];
             adj_pos = P.adj.start[kfetch];
             adj_end = P.adj.end[kfetch];
             adjA = 0.0;
+            adjB = 0.0;
             for (int64_t r = adj_pos; r < adj_end; ++r) adjA += P.adj.sc[r];
           } else {
             if ((int64_t)k >= P.hi - P.lo + 1) { ev = EV_DONE; return; }
@@ -592,8 +609,8 @@ struct Lane {
           const CellRec c = m.cells[ci];
           const int k = pk.select_dust(c);
           if (k < 0) { status = 3; ev = EV_FINISH; break; }
-          if (P.adj.mode == 2 && adjA != 0.0)   // replay: the interaction density at the segment's end
-            atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1), adjA);
+          if (P.adj.mode == 2 && adjA != adjB)   // replay: the interaction density at the segment's end
+            atomicAdd(P.adj.grad + ci + m.ncell * (cell_id(c.meta, k) - 1), adjA - adjB);
           if (first) { ++s_cnt[MCRT_S_TOT]; first = 0; }
           const int slot = cell_slot(c.meta, k);
           const int idust2 = cell_id(c.meta, k);

@@ -655,6 +655,9 @@ struct Packet {
     if (p == m.npg) p = 1;
   }
 
+#ifndef MCRT_TALLY_WARP_AGG
+#define MCRT_TALLY_WARP_AGG 0
+#endif
 #ifdef MCRT_MIXED
   // ------------------------------------------------ FP32 walk (QRay)
   // FP32 opacity columns of the walk: kapd and kapd*(1-albedo) per slot.
@@ -682,7 +685,23 @@ struct Packet {
     }
   }
   __device__ __forceinline__ void tally_absf(int64_t ci, float absc, double len) {
+#if MCRT_TALLY_WARP_AGG
+    // Lanes of the warp that tally the same cell add their pieces first and
+    // one of them issues the atomic (the sum order differs from one atomic
+    // per lane only in rounding).
+    const double v = absc > 0.0f ? __dmul_rn(len, (double)absc) : 0.0;
+    const unsigned grp = __match_any_sync(__activemask(), (unsigned long long)ci);
+    const int lane = threadIdx.x & 31;
+    if (grp == (1u << lane)) {
+      if (v != 0.0) atomicAdd(T.dtauabs + ci, v);
+    } else {
+      double sum = 0.0;
+      for (unsigned b = grp; b; b &= b - 1u) sum = __dadd_rn(sum, __shfl_sync(grp, v, __ffs(b) - 1));
+      if (lane == __ffs(grp) - 1 && sum != 0.0) atomicAdd(T.dtauabs + ci, sum);
+    }
+#else
     if (absc > 0.0f) atomicAdd(T.dtauabs + ci, __dmul_rn(len, (double)absc));
+#endif
     if (m.iffuv) atomicAdd(T.fuvmean + ci, len * (m.rstar * RSOL) * ifuv / __ldg(m.vcell + ci));
   }
 

@@ -85,6 +85,7 @@ def load_library(path: str = LIB_PATH):
                                        P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double),
                                        P(C.c_double)]
     lib.mcrt_set_adjoint_chunk.argtypes = [C.c_void_p, C.c_int64]
+    lib.mcrt_set_adjoint_baseline.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_double]
     lib.mcrt_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_double),
                                   P(C.c_double), P(C.c_double), C.c_int32, C.c_int32, P(C.c_double), P(C.c_double),
                                   P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int64),
@@ -106,7 +107,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
                  "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
-                 "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_model_density"):
+                 "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_set_adjoint_baseline", "mcrt_model_density"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -360,6 +361,16 @@ class Engine:
         """Packets per adjoint chunk (forward, sort and replay per chunk;
         gradients and objective summed)."""
         self._check(self.lib.mcrt_set_adjoint_chunk(self.ctx, int(packets)))
+
+    def set_adjoint_baseline(self, nfb: int = 10, ndir: int = 4, pilot_packets: int = 1_000_000,
+                             min_count: float = 16.0):
+        """Control variate of the adjoint's replay (C ABI
+        ``mcrt_set_adjoint_baseline``): the mean future contribution per
+        (cell, frequency bin, direction class), learned from a pilot replay
+        of `pilot_packets` packets on another generator, is subtracted from
+        each segment's weight.  ``nfb=0`` switches it off."""
+        self._check(self.lib.mcrt_set_adjoint_baseline(self.ctx, int(nfb), int(ndir), int(pilot_packets),
+                                                       float(min_count)))
 
     def refresh_diffusion(self):
         """Diffusion-cell temperatures of the last run from the (reduced) counts."""

@@ -551,6 +551,35 @@ def test_adjoint_matches_oracle(warm_small, oracle_mod, diffusion):
         assert abs(a - b) <= 2e-2 * np.abs(g_or.reshape((ncell, 10), order="F")[:, comp]).sum() + 1e-12, comp
 
 
+def test_adjoint_control_variate_matches_oracle(warm_small, oracle_mod):
+    """mcrt_adjoint with the replay's control variate (pilot replay on
+    generator 2, mean future contribution per cell x 5 frequency bins x 4
+    direction classes) against the oracle doing the same two steps: the
+    pilot's counts and the baseline table follow from the same packets, so
+    the gradients agree as closely as the plain replay's do."""
+    m = model.with_diffusion(warm_small)
+    lam, img = _adjoint_weights(m)
+    n, pilot = 4000, 3000
+    eng = _engine(m)
+    eng.set_adjoint_baseline(nfb=5, ndir=4, pilot_packets=pilot, min_count=4.0)
+    g_gpu, L_gpu = eng.adjoint(n, lam, img)
+    eng.set_adjoint_baseline(nfb=0)
+    g_plain, _ = eng.adjoint(n, lam, img)
+    eng.close()
+    b = abi.Bundle(m)
+    _, _, vs, vc = oracle_mod.adjoint_cv(b, pilot, lam, img, nfb=-5, learn=True, generator=2)
+    V = np.where(vc >= 4.0, vs / np.maximum(vc, 1.0), 0.0)
+    g_or, L_or, _, _ = oracle_mod.adjoint_cv(b, n, lam, img, vtab=V, nfb=-5)
+    assert L_gpu > 0 and abs(L_gpu - L_or) <= 1e-3 * abs(L_or)
+    assert np.abs(g_gpu - g_or).sum() <= 2e-2 * np.abs(g_or).sum()
+    assert np.abs(g_gpu - g_plain).sum() > 1e-3 * np.abs(g_plain).sum()   # the baseline took effect
+    ncell = m.config["nrg"] * m.config["ntg"] * m.config["npg"]
+    for comp in range(10):
+        a = g_gpu.reshape((ncell, 10), order="F")[:, comp].sum()
+        o = g_or.reshape((ncell, 10), order="F")[:, comp]
+        assert abs(a - o.sum()) <= 2e-2 * np.abs(o).sum() + 1e-12, comp
+
+
 def test_adjoint_mixed_precision_and_repeatability(warm_small):
     m = model.with_diffusion(warm_small)
     lam, img = _adjoint_weights(m)

@@ -343,3 +343,31 @@ def test_tfinal_velocity_field_reduces_to_the_gas_at_rest(oracle_mod):
         rel = np.abs(c / a - 1.0)
         assert rel[~env].max() == 0.0
         assert 1e-5 < rel[env].max() < 1e-2
+
+
+def test_oracle_adjoint_control_variate(oracle_mod):
+    """The replay's control variate (each segment's score weighted by A - B):
+    B = 0 everywhere reproduces the plain replay exactly (the extra packets
+    without peel-off records then add nothing), and a learning replay
+    counts one segment start per packet plus one per interaction."""
+    m = model.with_diffusion(model.warm(model.small_2d()))
+    b = abi.Bundle(m)
+    lam = _adjoint_weights(m)
+    c = m.config
+    ncell = c["nrg"] * c["ntg"] * c["npg"]
+    n = 3000
+    g0, L0 = oracle_mod.adjoint(b, n, lam, threads=4)
+    for nfb in (5, -5):                       # -5: five frequency bins x four direction classes
+        nv = ncell * 5 * (4 if nfb < 0 else 1)
+        g1, L1, _, _ = oracle_mod.adjoint_cv(b, n, lam, vtab=np.zeros(nv), nfb=nfb, threads=4)
+        assert abs(L1 - L0) <= 1e-12 * L0      # threads take packets in any order
+        assert np.allclose(g1, g0, rtol=1e-12, atol=1e-12 * np.abs(g0).max())
+    # without diffusion cells the replay's paths are those of an ordinary run
+    b = abi.Bundle(model.warm(model.small_2d()))
+    _, L2, vs, vc = oracle_mod.adjoint_cv(b, n, lam, nfb=-5, learn=True, threads=4)
+    assert L2 > 0
+    _, log = oracle_mod.run(b, n, ipeel=0, nlog=n, threads=4)
+    events = abi.packet_log_to_numpy(log)
+    segments = n + int(events["nscat"].sum() + events["nabs"].sum())
+    assert vc.sum() == segments
+    assert (vc >= 0).all() and np.isfinite(vs).all() and vs.sum() > 0
