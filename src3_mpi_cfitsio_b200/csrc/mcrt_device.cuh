@@ -15,6 +15,7 @@
 // by the download) and are updated with atomics.
 #pragma once
 #include <cstdint>
+#include <cstddef>
 
 #include "../../include/mcrt_b200.h"
 
@@ -126,29 +127,41 @@ struct __align__(16) PeelJob {
 };
 
 // Wavefront schedule: one in-flight packet per pool slot, kept in HBM
-// between the walk kernel and the event kernel.  The walk part (first 200
-// bytes) is what the walk kernel reads and writes; the event kernel moves the
-// whole record.  `spec` holds the species columns kapd, alb, g, pl, kap
-// (kMaxSlot each) of the packet's current frequency.
+// between the walk kernel and the event kernel.  Fields come in 16-byte
+// groups (two doubles, or four 32-bit integers) that one kernel reads or
+// writes together, so every record access is a 16-byte vector load or
+// store.  The walk part (first 208 bytes) is what the walk kernels read and
+// write.  `spec` holds per species slot the columns kapd, albedo, g, pl of
+// the packet's current frequency.
 struct __align__(16) WaveRec {
   // walk part
-  double x, y, z, rs, rt, vx, vy, vz, tsum;   // ray
-  double tau, ifuv;
+  double x, y, z, rs, rt, vx, vy, vz;                 // ray start point and direction
+  double tsum, tau;
+  double ifuv;
   int64_t ray_steps;
-  int32_t r, t, p, rbits;                     // rbits: ray onw | ray peel << 1
-  int32_t s1, s2, ndraws, ev;
-  int32_t status, ncross, exitflag, on_wall;
-  int32_t ir, it, ip, pad0;
-  double xp, yp, zp, rsq, rtot;
+  int32_t r, t, p, rbits;                             // ray cell; rbits: onw | peel << 1
+  int32_t ev, status, ncross, exitflag;
+  int32_t s1, s2, ndraws, pad0;                       // random stream
+  int32_t ir, it, ip, on_wall;                        // packet cell
+  double xp, yp, zp, rsq, rtot, pad1;                 // packet position
   // event part
-  double ux, uy, uz, cost, sint, cosp, sinp, phi, sip, sqp, sup, svp, nub, cosb, sinb, lp;
-  double xpold, ypold, zpold, peel_si, coslp, sinlp;
-  int64_t nev, iphot, kfetch;
-  int32_t iflag, i_orig, nscat, nabsev, nstar, ndiffev, iscat, iint;
-  int32_t first, slot_s, prev_r, prev_t, prev_p, peel_ctx, peelid, peel_idust2;
-  double spec[5 * kMaxSlot];
+  double ux, uy, uz, cost, sint, cosp, sinp, phi;
+  double sip, sqp, sup, svp, nub, xpold, ypold, zpold;
+  int64_t nev, iphot, kfetch, pad2;
+  int32_t iflag, i_orig, nscat, nabsev;
+  int32_t nstar, ndiffev, iscat, iint;
+  int32_t first, slot_s, prev_r, prev_t;
+  int32_t prev_p, peel_ctx, peelid, peel_idust2;
+  double cosb, sinb, lp, peel_si, coslp, sinlp;       // peel-off state
+  double spec[4 * kMaxSlot];                          // [slot][kapd, albedo, g, pl]
 };
 static_assert(sizeof(WaveRec) % 16 == 0, "WaveRec must keep 16-byte alignment");
+static_assert(offsetof(WaveRec, tsum) % 16 == 0 && offsetof(WaveRec, ifuv) % 16 == 0 && offsetof(WaveRec, r) % 16 == 0 &&
+                  offsetof(WaveRec, s1) % 16 == 0 && offsetof(WaveRec, xp) % 16 == 0 && offsetof(WaveRec, ux) % 16 == 0 &&
+                  offsetof(WaveRec, sip) % 16 == 0 && offsetof(WaveRec, nev) % 16 == 0 &&
+                  offsetof(WaveRec, iflag) % 16 == 0 && offsetof(WaveRec, cosb) % 16 == 0 &&
+                  offsetof(WaveRec, spec) % 16 == 0,
+              "WaveRec groups must start on 16-byte boundaries");
 
 // Queue counters of the wavefront loop.  The event queue is filled from both
 // ends by the walk kernel: interactions from the front, every other event

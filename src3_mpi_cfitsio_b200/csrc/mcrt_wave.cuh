@@ -26,59 +26,87 @@
 namespace mcrt {
 
 // ------------------------------------------------------------ record I/O
-// The walk kernel reads the ray part only: every way a packet walk ends
-// (interaction point, exit, stellar surface, geometry failure) first copies
-// the ray into the packet position (packet_from_ray), and a peel-off walk
-// never changes it, so the packet position is written back after packet
-// walks and never read by the walk kernel.
-__device__ __forceinline__ void wave_load_ray(Lane& L, const WaveRec& R, int nslot) {
-  Ray& y = L.ray;
-  y.x = R.x; y.y = R.y; y.z = R.z; y.rs = R.rs; y.rt = R.rt;
-  y.vx = R.vx; y.vy = R.vy; y.vz = R.vz; y.tsum = R.tsum;
-  y.r = R.r; y.t = R.t; y.p = R.p;
-  y.onw = (R.rbits & 1) != 0;
-  y.peel = (R.rbits & 2) != 0;
-#ifdef MCRT_MIXED
-  y.qready = false;                 // every loaded walk sets up its own closest-approach form
-#endif
+// Every access is a 16-byte vector load or store of one group of WaveRec.
+__device__ __forceinline__ double2 rd2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void wr2(double* p, double a, double b) { *reinterpret_cast<double2*>(p) = make_double2(a, b); }
+__device__ __forceinline__ int4 rd4(const int32_t* p) { return *reinterpret_cast<const int4*>(p); }
+__device__ __forceinline__ void wr4(int32_t* p, int a, int b, int c, int d) {
+  *reinterpret_cast<int4*>(p) = make_int4(a, b, c, d);
+}
+
+// The ray cell, the walk state and the random stream.
+__device__ __forceinline__ void wave_load_state(Lane& L, const WaveRec& R) {
   Packet& k = L.pk;
-  k.tau = R.tau; k.ifuv = R.ifuv;
-  L.ray_steps = R.ray_steps;
-  k.rng.s1 = R.s1; k.rng.s2 = R.s2; k.rng.ndraws = R.ndraws;
-  L.ev = R.ev; L.status = R.status;
-  k.ncross = R.ncross; k.exitflag = R.exitflag;
-  for (int s = 0; s < nslot; ++s) {
-    k.sp.kapd(s) = R.spec[s];
-    k.sp.alb(s) = R.spec[kMaxSlot + s];
-  }
+  const double2 tt = rd2(&R.tsum);
+  L.ray.tsum = tt.x;
+  k.tau = tt.y;
+  const double2 fs = rd2(&R.ifuv);
+  k.ifuv = fs.x;
+  L.ray_steps = __double_as_longlong(fs.y);
+  const int4 e = rd4(&R.ev);
+  L.ev = e.x; L.status = e.y; k.ncross = e.z; k.exitflag = e.w;
+  const int4 g = rd4(&R.s1);
+  k.rng.s1 = g.x; k.rng.s2 = g.y; k.rng.ndraws = g.z;
+}
+
+__device__ __forceinline__ void wave_load_raygeom(Lane& L, const WaveRec& R) {
+  Ray& y = L.ray;
+  double2 a = rd2(&R.x), b = rd2(&R.z), c = rd2(&R.rt), d = rd2(&R.vy);
+  y.x = a.x; y.y = a.y; y.z = b.x; y.rs = b.y; y.rt = c.x; y.vx = c.y; y.vy = d.x; y.vz = d.y;
+  const int4 q = rd4(&R.r);
+  y.r = q.x; y.t = q.y; y.p = q.z;
+  y.onw = (q.w & 1) != 0;
+  y.peel = (q.w & 2) != 0;
+#ifdef MCRT_MIXED
+  y.qready = false;
+#endif
 }
 
 __device__ __forceinline__ void wave_load_pos(Lane& L, const WaveRec& R) {
   Packet& k = L.pk;
-  k.on_wall = R.on_wall != 0;
-  k.ir = R.ir; k.it = R.it; k.ip = R.ip;
-  k.xp = R.xp; k.yp = R.yp; k.zp = R.zp; k.rsq = R.rsq; k.rtot = R.rtot;
-}
-
-__device__ __forceinline__ void wave_save_ray(const Lane& L, WaveRec& R) {
-  const Ray& y = L.ray;
-  R.x = y.x; R.y = y.y; R.z = y.z; R.rs = y.rs; R.rt = y.rt;
-  R.vx = y.vx; R.vy = y.vy; R.vz = y.vz; R.tsum = y.tsum;
-  R.r = y.r; R.t = y.t; R.p = y.p;
-  R.rbits = (y.onw ? 1 : 0) | (y.peel ? 2 : 0);
-  const Packet& k = L.pk;
-  R.tau = k.tau; R.ifuv = k.ifuv;
-  R.ray_steps = L.ray_steps;
-  R.s1 = k.rng.s1; R.s2 = k.rng.s2; R.ndraws = k.rng.ndraws;
-  R.ev = L.ev; R.status = L.status;
-  R.ncross = k.ncross; R.exitflag = k.exitflag;
+  const int4 c = rd4(&R.ir);
+  k.ir = c.x; k.it = c.y; k.ip = c.z;
+  k.on_wall = c.w != 0;
+  const double2 a = rd2(&R.xp), b = rd2(&R.zp), d = rd2(&R.rtot);
+  k.xp = a.x; k.yp = a.y; k.zp = b.x; k.rsq = b.y; k.rtot = d.x;
 }
 
 __device__ __forceinline__ void wave_save_pos(const Lane& L, WaveRec& R) {
   const Packet& k = L.pk;
-  R.on_wall = k.on_wall ? 1 : 0;
-  R.ir = k.ir; R.it = k.it; R.ip = k.ip;
-  R.xp = k.xp; R.yp = k.yp; R.zp = k.zp; R.rsq = k.rsq; R.rtot = k.rtot;
+  wr4(&R.ir, k.ir, k.it, k.ip, k.on_wall ? 1 : 0);
+  wr2(&R.xp, k.xp, k.yp);
+  wr2(&R.zp, k.zp, k.rsq);
+  wr2(&R.rtot, k.rtot, 0.0);
+}
+
+// The walk kernel of the FP64 build reads the ray part only: every way a
+// packet walk ends (interaction point, exit, stellar surface, geometry
+// failure) first copies the ray into the packet position (packet_from_ray),
+// and a peel-off walk never changes it, so the packet position is written
+// back after packet walks and never read by the walk kernel.
+__device__ __forceinline__ void wave_load_ray(Lane& L, const WaveRec& R, int nslot) {
+  wave_load_raygeom(L, R);
+  wave_load_state(L, R);
+  Packet& k = L.pk;
+  for (int s = 0; s < nslot; ++s) {
+    const double2 a = rd2(&R.spec[4 * s]);
+    k.sp.kapd(s) = a.x;
+    k.sp.alb(s) = a.y;
+  }
+}
+
+__device__ __forceinline__ void wave_save_ray(const Lane& L, WaveRec& R) {
+  const Ray& y = L.ray;
+  const Packet& k = L.pk;
+  wr2(&R.x, y.x, y.y);
+  wr2(&R.z, y.z, y.rs);
+  wr2(&R.rt, y.rt, y.vx);
+  wr2(&R.vy, y.vy, y.vz);
+  wr2(&R.tsum, y.tsum, k.tau);
+  wr2(&R.ifuv, k.ifuv, __longlong_as_double(L.ray_steps));
+  wr4(&R.r, y.r, y.t, y.p, (y.onw ? 1 : 0) | (y.peel ? 2 : 0));
+  wr4(&R.ev, L.ev, L.status, k.ncross, k.exitflag);
+  wr4(&R.s1, k.rng.s1, k.rng.s2, k.rng.ndraws, 0);
 }
 
 __device__ __forceinline__ void wave_load_walk(Lane& L, const WaveRec& R, int nslot) {
@@ -91,24 +119,83 @@ __device__ __forceinline__ void wave_save_walk(const Lane& L, WaveRec& R) {
   wave_save_pos(L, R);
 }
 
-__device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int nslot) {
+// Direction, Stokes vector, frequency, the event bookkeeping.
+__device__ __forceinline__ void wave_load_core(Lane& L, const WaveRec& R) {
   Packet& k = L.pk;
-  k.ux = R.ux; k.uy = R.uy; k.uz = R.uz;
-  k.cost = R.cost; k.sint = R.sint; k.cosp = R.cosp; k.sinp = R.sinp; k.phi = R.phi;
-  k.sip = R.sip; k.sqp = R.sqp; k.sup = R.sup; k.svp = R.svp; k.nub = R.nub;
-  k.cosb = R.cosb; k.sinb = R.sinb; k.lp = R.lp;
-  L.xpold = R.xpold; L.ypold = R.ypold; L.zpold = R.zpold;
-  L.peel_si = R.peel_si; L.coslp = R.coslp; L.sinlp = R.sinlp;
-  L.nev = R.nev; L.iphot = R.iphot; L.kfetch = R.kfetch;
-  k.iflag = R.iflag; k.i_orig = R.i_orig; k.nscat = R.nscat; k.nabsev = R.nabsev;
-  k.nstar = R.nstar; k.ndiffev = R.ndiffev;
-  L.iscat = R.iscat; L.iint = R.iint; L.first = R.first; L.slot_s = R.slot_s;
-  L.prev_r = R.prev_r; L.prev_t = R.prev_t; L.prev_p = R.prev_p;
-  L.peel_ctx = R.peel_ctx; L.peelid = R.peelid; L.peel_idust2 = R.peel_idust2;
+  double2 a = rd2(&R.ux), b = rd2(&R.uz), c = rd2(&R.sint), d = rd2(&R.sinp);
+  k.ux = a.x; k.uy = a.y; k.uz = b.x; k.cost = b.y; k.sint = c.x; k.cosp = c.y; k.sinp = d.x; k.phi = d.y;
+  a = rd2(&R.sip); b = rd2(&R.sup); c = rd2(&R.nub); d = rd2(&R.ypold);
+  k.sip = a.x; k.sqp = a.y; k.sup = b.x; k.svp = b.y; k.nub = c.x; L.xpold = c.y; L.ypold = d.x; L.zpold = d.y;
+  const longlong2 n0 = *reinterpret_cast<const longlong2*>(&R.nev);
+  const longlong2 n1 = *reinterpret_cast<const longlong2*>(&R.kfetch);
+  L.nev = n0.x; L.iphot = n0.y; L.kfetch = n1.x;
+  int4 q = rd4(&R.iflag);
+  k.iflag = q.x; k.i_orig = q.y; k.nscat = q.z; k.nabsev = q.w;
+  q = rd4(&R.nstar);
+  k.nstar = q.x; k.ndiffev = q.y; L.iscat = q.z; L.iint = q.w;
+  q = rd4(&R.first);
+  L.first = q.x; L.slot_s = q.y; L.prev_r = q.z; L.prev_t = q.w;
+  q = rd4(&R.prev_p);
+  L.prev_p = q.x; L.peel_ctx = q.y; L.peelid = q.z; L.peel_idust2 = q.w;
+}
+
+__device__ __forceinline__ void wave_load_peelstate(Lane& L, const WaveRec& R) {
+  Packet& k = L.pk;
+  const double2 a = rd2(&R.cosb), b = rd2(&R.lp), c = rd2(&R.coslp);
+  k.cosb = a.x; k.sinb = a.y; k.lp = b.x; L.peel_si = b.y; L.coslp = c.x; L.sinlp = c.y;
+}
+
+__device__ __forceinline__ void wave_load_spec(Lane& L, const WaveRec& R, int nslot) {
+  Packet& k = L.pk;
   for (int s = 0; s < nslot; ++s) {
-    k.sp.g(s) = R.spec[2 * kMaxSlot + s];
-    k.sp.pl(s) = R.spec[3 * kMaxSlot + s];
+    const double2 a = rd2(&R.spec[4 * s]), b = rd2(&R.spec[4 * s + 2]);
+    k.sp.kapd(s) = a.x;
+    k.sp.alb(s) = a.y;
+    k.sp.g(s) = b.x;
+    k.sp.pl(s) = b.y;
   }
+}
+
+// The event part as the tail kernel resumes it (the walk part comes with
+// wave_load_walk): core, peel-off state, and the g and pl columns.
+__device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int nslot) {
+  wave_load_core(L, R);
+  wave_load_peelstate(L, R);
+  Packet& k = L.pk;
+  for (int s = 0; s < nslot; ++s) {
+    const double2 b = rd2(&R.spec[4 * s + 2]);
+    k.sp.g(s) = b.x;
+    k.sp.pl(s) = b.y;
+  }
+}
+
+__device__ __forceinline__ void wave_save_core(const Lane& L, WaveRec& R, int nslot) {
+  const Packet& k = L.pk;
+  wr2(&R.ux, k.ux, k.uy);
+  wr2(&R.uz, k.uz, k.cost);
+  wr2(&R.sint, k.sint, k.cosp);
+  wr2(&R.sinp, k.sinp, k.phi);
+  wr2(&R.sip, k.sip, k.sqp);
+  wr2(&R.sup, k.sup, k.svp);
+  wr2(&R.nub, k.nub, L.xpold);
+  wr2(&R.ypold, L.ypold, L.zpold);
+  *reinterpret_cast<longlong2*>(&R.nev) = make_longlong2(L.nev, L.iphot);
+  *reinterpret_cast<longlong2*>(&R.kfetch) = make_longlong2(L.kfetch, 0);
+  wr4(&R.iflag, k.iflag, k.i_orig, k.nscat, k.nabsev);
+  wr4(&R.nstar, k.nstar, k.ndiffev, L.iscat, L.iint);
+  wr4(&R.first, L.first, L.slot_s, L.prev_r, L.prev_t);
+  wr4(&R.prev_p, L.prev_p, L.peel_ctx, L.peelid, L.peel_idust2);
+  for (int s = 0; s < nslot; ++s) {
+    wr2(&R.spec[4 * s], k.sp.kapd(s), k.sp.alb(s));
+    wr2(&R.spec[4 * s + 2], k.sp.g(s), k.sp.pl(s));
+  }
+}
+
+__device__ __forceinline__ void wave_save_peelstate(const Lane& L, WaveRec& R) {
+  const Packet& k = L.pk;
+  wr2(&R.cosb, k.cosb, k.sinb);
+  wr2(&R.lp, k.lp, L.peel_si);
+  wr2(&R.coslp, L.coslp, L.sinlp);
 }
 
 #ifdef MCRT_MIXED
@@ -121,38 +208,43 @@ __device__ __forceinline__ void wave_load_event(Lane& L, const WaveRec& R, int n
 __device__ __forceinline__ void wave_load_qwalk(Lane& L, const WaveRec& R, int nslot) {
   Ray& y = L.ray;
   Packet& k = L.pk;
-  y.r = R.r; y.t = R.t; y.p = R.p;
-  y.onw = (R.rbits & 1) != 0;
-  y.peel = (R.rbits & 2) != 0;
-  y.tsum = R.tsum;
+  const int4 q = rd4(&R.r);
+  y.r = q.x; y.t = q.y; y.p = q.z;
+  y.onw = (q.w & 1) != 0;
+  y.peel = (q.w & 2) != 0;
+  const double2 tt = rd2(&R.tsum);
+  y.tsum = tt.x;
+  k.tau = tt.y;
   y.qready = true;
-  k.tau = R.tau; k.ifuv = R.ifuv;
-  L.ray_steps = R.ray_steps;
-  L.ev = R.ev; L.status = R.status;
-  k.ncross = R.ncross; k.exitflag = R.exitflag;
+  const double2 fs = rd2(&R.ifuv);
+  k.ifuv = fs.x;
+  L.ray_steps = __double_as_longlong(fs.y);
+  const int4 e = rd4(&R.ev);
+  L.ev = e.x; L.status = e.y; k.ncross = e.z; k.exitflag = e.w;
   for (int s = 0; s < nslot; ++s) {
-    const double kd = R.spec[s];
-    k.kf(s) = (float)kd;
-    k.kaf(s) = (float)__dmul_rn(kd, __dsub_rn(1.0, R.spec[kMaxSlot + s]));
+    const double2 a = rd2(&R.spec[4 * s]);
+    k.kf(s) = (float)a.x;
+    k.kaf(s) = (float)__dmul_rn(a.x, __dsub_rn(1.0, a.y));
   }
-  k.qbegin(y.g, R.x, R.y, R.z, R.vx, R.vy, R.vz, y.r, y.t, y.p);
+  const double2 a = rd2(&R.x), b = rd2(&R.z), c = rd2(&R.rt), d = rd2(&R.vy);
+  k.qbegin(y.g, a.x, a.y, b.x, c.y, d.x, d.y, y.r, y.t, y.p);
 }
 
 __device__ __forceinline__ void wave_save_qwalk(const Lane& L, WaveRec& R) {
   const Ray& y = L.ray;
   const Packet& k = L.pk;
-  R.tsum = y.tsum;
-  R.r = y.r; R.t = y.t; R.p = y.p;
-  R.rbits = (y.onw ? 1 : 0) | (y.peel ? 2 : 0);
-  R.ray_steps = L.ray_steps;
-  R.ev = L.ev; R.status = L.status;
-  R.ncross = k.ncross; R.exitflag = k.exitflag;
+  wr2(&R.tsum, y.tsum, k.tau);
+  wr2(&R.ifuv, k.ifuv, __longlong_as_double(L.ray_steps));
+  wr4(&R.r, y.r, y.t, y.p, (y.onw ? 1 : 0) | (y.peel ? 2 : 0));
+  wr4(&R.ev, L.ev, L.status, k.ncross, k.exitflag);
   if (!y.peel) {
+    const double2 a = rd2(&R.x), b = rd2(&R.z), c = rd2(&R.rt), d = rd2(&R.vy);
     double x, yy, z, rs, rt;
-    Packet::qpos(R.x, R.y, R.z, R.vx, R.vy, R.vz, y.g.q, y.g.q0, x, yy, z, rs, rt);
-    R.xp = x; R.yp = yy; R.zp = z; R.rsq = rs; R.rtot = rt;
-    R.on_wall = y.onw ? 1 : 0;
-    R.ir = y.r; R.it = y.t; R.ip = y.p;
+    Packet::qpos(a.x, a.y, b.x, c.y, d.x, d.y, y.g.q, y.g.q0, x, yy, z, rs, rt);
+    wr4(&R.ir, y.r, y.t, y.p, y.onw ? 1 : 0);
+    wr2(&R.xp, x, yy);
+    wr2(&R.zp, z, rs);
+    wr2(&R.rtot, rt, 0.0);
   }
 }
 #endif
@@ -163,82 +255,6 @@ __device__ __forceinline__ void wave_save_qwalk(const Lane& L, WaveRec& R) {
 // species columns not for a packet that exits or ends (the next packet's
 // emission sets them).  Its save writes every group a later walk or event
 // reads.
-__device__ __forceinline__ void wave_load_state(Lane& L, const WaveRec& R) {
-  Packet& k = L.pk;
-  k.tau = R.tau; k.ifuv = R.ifuv;
-  L.ray_steps = R.ray_steps;
-  k.rng.s1 = R.s1; k.rng.s2 = R.s2; k.rng.ndraws = R.ndraws;
-  L.ev = R.ev; L.status = R.status;
-  k.ncross = R.ncross; k.exitflag = R.exitflag;
-}
-
-__device__ __forceinline__ void wave_load_raygeom(Lane& L, const WaveRec& R) {
-  Ray& y = L.ray;
-  y.x = R.x; y.y = R.y; y.z = R.z; y.rs = R.rs; y.rt = R.rt;
-  y.vx = R.vx; y.vy = R.vy; y.vz = R.vz; y.tsum = R.tsum;
-  y.r = R.r; y.t = R.t; y.p = R.p;
-  y.onw = (R.rbits & 1) != 0;
-  y.peel = (R.rbits & 2) != 0;
-#ifdef MCRT_MIXED
-  y.qready = false;
-#endif
-}
-
-__device__ __forceinline__ void wave_load_core(Lane& L, const WaveRec& R) {
-  Packet& k = L.pk;
-  k.ux = R.ux; k.uy = R.uy; k.uz = R.uz;
-  k.cost = R.cost; k.sint = R.sint; k.cosp = R.cosp; k.sinp = R.sinp; k.phi = R.phi;
-  k.sip = R.sip; k.sqp = R.sqp; k.sup = R.sup; k.svp = R.svp; k.nub = R.nub;
-  L.xpold = R.xpold; L.ypold = R.ypold; L.zpold = R.zpold;
-  L.nev = R.nev; L.iphot = R.iphot; L.kfetch = R.kfetch;
-  k.iflag = R.iflag; k.i_orig = R.i_orig; k.nscat = R.nscat; k.nabsev = R.nabsev;
-  k.nstar = R.nstar; k.ndiffev = R.ndiffev;
-  L.iscat = R.iscat; L.iint = R.iint; L.first = R.first; L.slot_s = R.slot_s;
-  L.prev_r = R.prev_r; L.prev_t = R.prev_t; L.prev_p = R.prev_p;
-}
-
-__device__ __forceinline__ void wave_load_peelstate(Lane& L, const WaveRec& R) {
-  Packet& k = L.pk;
-  k.cosb = R.cosb; k.sinb = R.sinb; k.lp = R.lp;
-  L.peel_si = R.peel_si; L.coslp = R.coslp; L.sinlp = R.sinlp;
-  L.peel_ctx = R.peel_ctx; L.peelid = R.peelid; L.peel_idust2 = R.peel_idust2;
-}
-
-__device__ __forceinline__ void wave_load_spec(Lane& L, const WaveRec& R, int nslot) {
-  Packet& k = L.pk;
-  for (int s = 0; s < nslot; ++s) {
-    k.sp.kapd(s) = R.spec[s];
-    k.sp.alb(s) = R.spec[kMaxSlot + s];
-    k.sp.g(s) = R.spec[2 * kMaxSlot + s];
-    k.sp.pl(s) = R.spec[3 * kMaxSlot + s];
-  }
-}
-
-__device__ __forceinline__ void wave_save_core(const Lane& L, WaveRec& R, int nslot) {
-  const Packet& k = L.pk;
-  R.ux = k.ux; R.uy = k.uy; R.uz = k.uz;
-  R.cost = k.cost; R.sint = k.sint; R.cosp = k.cosp; R.sinp = k.sinp; R.phi = k.phi;
-  R.sip = k.sip; R.sqp = k.sqp; R.sup = k.sup; R.svp = k.svp; R.nub = k.nub;
-  R.xpold = L.xpold; R.ypold = L.ypold; R.zpold = L.zpold;
-  R.nev = L.nev; R.iphot = L.iphot; R.kfetch = L.kfetch;
-  R.iflag = k.iflag; R.i_orig = k.i_orig; R.nscat = k.nscat; R.nabsev = k.nabsev;
-  R.nstar = k.nstar; R.ndiffev = k.ndiffev;
-  R.iscat = L.iscat; R.iint = L.iint; R.first = L.first; R.slot_s = L.slot_s;
-  R.prev_r = L.prev_r; R.prev_t = L.prev_t; R.prev_p = L.prev_p;
-  for (int s = 0; s < nslot; ++s) {
-    R.spec[s] = k.sp.kapd(s);
-    R.spec[kMaxSlot + s] = k.sp.alb(s);
-    R.spec[2 * kMaxSlot + s] = k.sp.g(s);
-    R.spec[3 * kMaxSlot + s] = k.sp.pl(s);
-  }
-}
-
-__device__ __forceinline__ void wave_save_peelstate(const Lane& L, WaveRec& R) {
-  const Packet& k = L.pk;
-  R.cosb = k.cosb; R.sinb = k.sinb; R.lp = k.lp;
-  R.peel_si = L.peel_si; R.coslp = L.coslp; R.sinlp = L.sinlp;
-  R.peel_ctx = L.peel_ctx; R.peelid = L.peelid; R.peel_idust2 = L.peel_idust2;
-}
 
 __device__ __forceinline__ void flush_counters(const LaunchParams& P, const Lane& L) {
   unsigned long long v[14] = {L.c_pkt, L.pk.c_cross, L.c_int, L.c_sca, L.pk.c_peel, L.pk.c_pcross, L.pk.c_pbin,

@@ -1,12 +1,24 @@
 """Path-replay adjoint against central finite differences on the 2-D bench
-model (nr=100, ntheta=99, diffusion on) at 4e7 packets per evaluation, the
-scale at which its Monte Carlo error is below the 2 % target.
+model (nr=100, ntheta=99, diffusion on) at 4e7 packets per evaluation, and
+against the FP64 build's replay.
 
-Scaling one density component everywhere by exp(+-eps) changes the objective
-(the peeled SED plus the 3.6/24/70 um images) by 2 eps * sum(grad[:, comp]).
-Both sides use the same seeds (common random numbers), so the test is
-deterministic up to the order of FP64 atomic sums.  The envelope and cavity
-components are checked.  The optically thick disk is not: its estimate
+Scaling one density component in a set of cells by exp(+-eps) changes the
+objective (the peeled SED plus the 3.6/24/70 um images) by
+2 eps * sum(grad[cells, comp]).  Both sides use the same seeds (common
+random numbers), so the tests are deterministic up to the order of FP64
+atomic sums.
+
+Step size.  With common random numbers a finite difference is exact for the
+packets whose discrete decisions (interaction cell, scatter or absorb,
+escape) do not change with the step, and carries the whole contribution of
+every packet whose decision flips.  The flips shrink more slowly than the
+step, so their share grows as eps falls: measured on this model, the
+envelope's central difference moves from the adjoint by 0.2 % at eps = 5e-2,
+0.5 % at 1e-2 and 11 % at 1e-3 (the cavity: 0.6 %, 1.2 %, 1.6 %).  The
+tests use eps = 1e-2, where the difference is below the 2 % target and the
+truncation error (eps^2) is 1e-4.
+
+The optically thick disk is not held to 2 % per evaluation: its estimate
 scatters by ~6 % from seed to seed on both sides at this size.
 """
 import numpy as np
@@ -17,28 +29,98 @@ from src3_mpi_cfitsio_b200 import model
 
 pytestmark = pytest.mark.gpu
 
+N = 40_000_000
+EPS = 1e-2
+SEEDS = (12345678, 87654321)
 
-def test_adjoint_within_two_percent_of_central_differences():
+
+@pytest.fixture(scope="module")
+def bench_adjoint():
+    """The mixed engine on the bench model and its adjoint at N packets."""
     from src3_mpi_cfitsio_b200.engine import Engine
     base = model.with_diffusion(model.warm(model.reference_2d()))
     lam, img = madj.sed_image_weights(base)
     c = base.config
     ncell = c["nrg"] * c["ntg"] * c["npg"]
     dens0 = base.grid["densarr"].reshape((ncell, 10), order="F").copy()
-    n, eps, seeds = 40_000_000, 0.05, (12345678, 87654321)
     eng = Engine(base, precision="mixed")
-    g, L = eng.adjoint(n, lam, img, seeds=seeds)
-    G = g.reshape((ncell, 10), order="F")
-    assert L > 0
-    for comp in (2, 3):                       # 0-based columns: envelope (id 3) and cavity (id 4)
-        vals = []
-        for sgn in (1, -1):
-            d = dens0.copy()
-            d[:, comp] *= np.exp(sgn * eps)
-            base.grid["densarr"] = d.ravel(order="F")
-            eng.upload_grid()
-            vals.append(eng.adjoint(n, lam, img, seeds=seeds)[1])
-        fd = (vals[0] - vals[1]) / (2 * eps)
-        adj = G[:, comp].sum()
-        assert abs(adj - fd) <= 0.02 * abs(fd), (comp + 1, adj, fd)
+    g, L = eng.adjoint(N, lam, img, seeds=SEEDS)
+    yield dict(base=base, lam=lam, img=img, ncell=ncell, dens0=dens0, eng=eng,
+               G=g.reshape((ncell, 10), order="F"), L=L)
+    base.grid["densarr"] = dens0.ravel(order="F")
     eng.close()
+
+
+def _central_difference(A, mask, comp, eps=EPS):
+    """(L(rho e^eps) - L(rho e^-eps)) / (2 eps) for component `comp` in the
+    cells of `mask`, same seeds; the grid is restored afterwards."""
+    eng, base, dens0 = A["eng"], A["base"], A["dens0"]
+    vals = []
+    for sgn in (1, -1):
+        d = dens0.copy()
+        d[mask, comp] *= np.exp(sgn * eps)
+        base.grid["densarr"] = d.ravel(order="F")
+        eng.upload_grid()
+        vals.append(eng.adjoint(N, A["lam"], A["img"], seeds=SEEDS)[1])
+    base.grid["densarr"] = dens0.ravel(order="F")
+    eng.upload_grid()
+    return (vals[0] - vals[1]) / (2 * eps)
+
+
+def test_adjoint_within_two_percent_of_central_differences(bench_adjoint):
+    """Envelope (id 3) and cavity (id 4) everywhere: measured 0.5 % and 1.2 %."""
+    A = bench_adjoint
+    assert A["L"] > 0
+    every = np.ones(A["ncell"], bool)
+    for comp in (2, 3):                       # 0-based columns: envelope (id 3) and cavity (id 4)
+        fd = _central_difference(A, every, comp)
+        adj = A["G"][:, comp].sum()
+        assert abs(adj - fd) <= 0.02 * abs(fd), (comp + 1, adj, fd)
+
+
+def test_adjoint_per_cell_gradient_on_radial_shells(bench_adjoint):
+    """The per-cell gradient, summed over four radial shells of the envelope
+    (equal numbers of envelope cells), against the central difference of
+    scaling the envelope in that shell alone.  Measured: -0.6, -1.1, +3.4 and
+    +1.0 % (the shells hold 4.0e6 ... 1.3e6 of the 1.46e7 total)."""
+    A = bench_adjoint
+    nrg = A["base"].config["nrg"]
+    ir = np.arange(A["ncell"]) % nrg
+    env = A["dens0"][:, 2] > 0
+    q = np.percentile(ir[env], [25, 50, 75])
+    edges = [0, *[int(v) for v in q], nrg]
+    total = A["G"][env, 2].sum()
+    for a, b in zip(edges[:-1], edges[1:]):
+        shell = env & (ir >= a) & (ir < b)
+        adj = A["G"][shell, 2].sum()
+        assert abs(adj) >= 0.05 * abs(total)          # every shell carries a real share
+        fd = _central_difference(A, shell, 2)
+        assert abs(adj - fd) <= 0.05 * abs(fd), (a, b, adj, fd)
+
+
+def test_mixed_adjoint_agrees_with_fp64_replay():
+    """The mixed build's gradient against the FP64 build's path replay on the
+    bench model, same packets and seeds (1e7): the objective, the envelope,
+    cavity and disk component sums and the disk-parameter gradients.  The two
+    builds' histories part after FP32 scattering in a few packets; measured
+    differences are 0.02-0.2 %."""
+    from src3_mpi_cfitsio_b200.engine import Engine
+    base = model.with_diffusion(model.warm(model.reference_2d()))
+    lam, img = madj.sed_image_weights(base)
+    c = base.config
+    ncell = c["nrg"] * c["ntg"] * c["npg"]
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng = Engine(base, precision=prec)
+        g, L = eng.adjoint(10_000_000, lam, img, seeds=SEEDS)
+        eng.close()
+        G = g.reshape((ncell, 10), order="F")
+        out[prec] = dict(L=L, comp=[G[:, k].sum() for k in (1, 2, 3)], par=madj.parameter_gradient(base, g))
+    a, b = out["fp64"], out["mixed"]
+    assert abs(b["L"] - a["L"]) <= 1e-3 * a["L"]
+    for x, y in zip(a["comp"], b["comp"]):
+        assert abs(y - x) <= 0.01 * abs(x), (x, y)
+    for name in ("massd", "h100_au"):
+        assert abs(b["par"][name] - a["par"][name]) <= 0.02 * abs(a["par"][name]), name
+    # the flaring-index gradient is a small difference of large terms
+    assert abs(b["par"]["b_exp"] - a["par"]["b_exp"]) <= 0.05 * abs(a["par"]["massd"]) + 0.02 * abs(a["par"]["b_exp"])
