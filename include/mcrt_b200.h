@@ -125,6 +125,15 @@ typedef struct mcrt_grid {
   const double  *vrarr;       /* [nrg,ntg,npg] cm/s                         */
   const double  *vthetarr;    /* [nrg,ntg,npg] cm/s                         */
   const double  *divvarr;     /* [nrg,ntg,npg] cm/s per stellar radius      */
+  /* Small-grain (VSG/PAH) emission level per cell, optional: the row of the
+   * Draine emissivity table (mcrt_tables.draine) a small grain absorbing in
+   * the cell re-emits from, the reference's imean (int_mean.f90:67-80).
+   * Iteration 1 uses row 2 whatever imean holds, as the reference's first
+   * iteration does (emit_common_2.f90:35-39).  NULL: row 1 afterwards, which
+   * is what the reference's int_mean gives: its jmean tally is switched off
+   * (usejmean = .False., tauint_3d_2_fuv.f90:27), so every cell's intensity
+   * ratio is 0 and locates below uratio_arr(1). */
+  const int32_t *imean;       /* [nrg,ntg,npg], 1..nemit                    */
 } mcrt_grid;
 
 /*
@@ -159,6 +168,15 @@ typedef struct mcrt_tables {
    * routine sets it: cdf 0, log cdf -99, log freq 0).  NULL when unused. */
   const double  *isrf;
   int32_t        nisrf, pad_isrf;
+  /* Small-grain (VSG/PAH) emission spectra, needed when a cell holds a
+   * small-grain component (ids 5-8): the tables draine_cdf.f90 leaves in
+   * draine_mod, concatenated as cdf_d(nemit,ndraine), logcdf_d(nemit,ndraine)
+   * and logfreq_d(ndraine), frequencies ascending in eV (the first entries
+   * as that routine sets them: cdf 0, log cdf -10, log freq 0).  A small
+   * grain re-emits from row imean of the cell (rep_draine_new.f90).  NULL
+   * when the model has no small grains. */
+  const double  *draine;
+  int32_t        nemit, ndraine;
 } mcrt_tables;
 
 /*

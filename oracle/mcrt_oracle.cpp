@@ -106,6 +106,32 @@ struct Rng {
   }
 };
 
+// rep_draine_new.f90: a small-grain re-emission frequency from row im of the
+// Draine spectra: locate3 (bisection over the columns of row im, in the
+// direction the row runs), then linear in log10 cdf and log10 nu.  The
+// tables: cdf_d(nemit,ndraine), logcdf_d(nemit,ndraine), logfreq_d(ndraine).
+double rep_draine(const mcrt_tables* t, int im, Rng& rng) {
+  const double xran = rng.ran();
+  const int ne = t->nemit, nd = t->ndraine;
+  const double* cdf = t->draine;
+  const double* lcdf = cdf + (int64_t)ne * nd;
+  const double* lfrq = cdf + 2 * (int64_t)ne * nd;
+  auto at = [&](const double* a, int j) { return a[(im - 1) + (int64_t)ne * (j - 1)]; };
+  int jl = 0, ju = nd + 1;
+  while (ju - jl > 1) {                           // locate3.f90:8-22
+    const int jm = (ju + jl) / 2;
+    if ((at(cdf, nd) > at(cdf, 1)) == (xran > at(cdf, jm))) jl = jm;
+    else ju = jm;
+  }
+  int ifreq = jl;
+  if (ifreq == nd) ifreq = ifreq - 1;
+  if (ifreq == 0) ifreq = 1;
+  const double logfreq = (std::log10(xran) - at(lcdf, ifreq)) / (at(lcdf, ifreq + 1) - at(lcdf, ifreq)) *
+                             (lfrq[ifreq] - lfrq[ifreq - 1]) +
+                         lfrq[ifreq - 1];
+  return std::pow(10.0, logfreq);
+}
+
 // set_all_seeds (ecuyer_cote_mod.f90:350-395) for `generator`, then `block`
 // applications of reinitialize_current_generator(1).
 Rng stream(int32_t seed1, int32_t seed2, int32_t generator, int64_t block) {
@@ -195,6 +221,7 @@ struct Model {
   std::atomic<int32_t>* ndiff = nullptr;
   double nphot_diff = 1.0;
   std::vector<double> sintarr;
+  int iter = 1;              // the iteration (small grains re-emit from Draine row 2 in the first)
 
   int64_t cidx(int ir, int it, int ip) const {
     return (int64_t)(ir - 1) + (int64_t)nrg * ((it - 1) + (int64_t)ntg * (ip - 1));
@@ -1675,7 +1702,22 @@ struct Packet {
           else if (idust2 == 3 || idust2 == 7) i_orig = 3;
           else i_orig = 4;
           if (!m->g->diffus[cc]) T->nabs[cc]++;
-          if (!m->g->diffus[cc]) {
+          if (!m->g->diffus[cc] && m->is_sg[idust2 - 1]) {
+            // emit_common, small grains (emit_common_2.f90:32-50): a frequency
+            // from the Draine spectrum of the cell's intensity level, then
+            // emit_sg.f90; the opacset there is repeated below
+            const int im = m->iter == 1 ? 2 : (m->g->imean ? m->g->imean[cc] : 1);
+            nub = rep_draine(m->t, im, rng);
+            sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+            cost = 1.0 - 2.0 * ran();
+            sint = std::sqrt(1.0 - cost * cost);
+            phi = R2P * ran();
+            cosp = std::cos(phi);
+            sinp = std::sin(phi);
+            uy = sint * sinp;
+            ux = sint * cosp;
+            uz = cost;
+          } else if (!m->g->diffus[cc]) {
             // emit_common, non-diffusion thermal branch (emit_common_2.f90:52-81)
             double tave = m->g->tdust[cc];
             // reemit.f90
@@ -1785,6 +1827,7 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   const int64_t block0 = (int64_t)(iter - 1) * np;
   Model m;
   m.c = *cfg;
+  m.iter = iter;
   m.g = grid;
   m.t = tab;
   m.nrg = cfg->nrg; m.ntg = cfg->ntg; m.npg = cfg->npg;
@@ -2174,6 +2217,7 @@ extern "C" int oracle_adjoint_cv(const mcrt_config* cfg, const mcrt_grid* grid, 
   const int64_t block0 = (int64_t)(iter - 1) * np;
   Model m;
   m.c = *cfg;
+  m.iter = iter;
   m.g = grid;
   m.t = tab;
   m.nrg = cfg->nrg; m.ntg = cfg->ntg; m.npg = cfg->npg;
@@ -2463,4 +2507,14 @@ extern "C" int oracle_setemiss(int32_t nopac, int32_t ndg, int32_t nlammax, cons
   for (auto v : miss) m += v;
   if (qsimp_misses) *qsimp_misses = m;
   return 0;
+}
+
+// rep_draine on its own: n frequencies from row im of the Draine spectra,
+// drawn from block 0 of generator 1 of (seed1, seed2).  Test infrastructure.
+extern "C" int oracle_rep_draine(const mcrt_tables* tab, int32_t im, int64_t n, int32_t seed1, int32_t seed2,
+                                 double* out) {
+  if (!tab || !tab->draine || im < 1 || im > tab->nemit || tab->ndraine < 2 || !out) return MCRT_ERR_ARG;
+  Rng rng = stream(seed1, seed2, 1, 0);
+  for (int64_t i = 0; i < n; ++i) out[i] = rep_draine(tab, im, rng);
+  return MCRT_OK;
 }

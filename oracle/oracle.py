@@ -83,6 +83,8 @@ def load():
         lib.oracle_adjoint.restype = C.c_int
         lib.oracle_adjoint_cv.argtypes = lib.oracle_adjoint.argtypes + [D, C.c_int32, D, D]
         lib.oracle_adjoint_cv.restype = C.c_int
+        lib.oracle_rep_draine.argtypes = [C.POINTER(abi.Tables), C.c_int32, C.c_int64, C.c_int32, C.c_int32, D]
+        lib.oracle_rep_draine.restype = C.c_int
         lib.oracle_rng.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32,
                                    C.POINTER(C.c_double), C.POINTER(C.c_int32)]
         lib.oracle_inczeta.argtypes = [C.POINTER(C.c_double)]
@@ -206,6 +208,18 @@ def adjoint_cv(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img:
     if rc != 0:
         raise RuntimeError(f"oracle_adjoint_cv failed with code {rc}")
     return grad, obj.value, vs, vc
+
+
+def rep_draine(bundle: abi.Bundle, im: int, n: int, seeds=(12345678, 87654321)) -> np.ndarray:
+    """n small-grain re-emission frequencies [eV] from row `im` of the
+    Draine spectra (rep_draine_new.f90), one random stream."""
+    lib = load()
+    out = np.empty(n, np.float64)
+    rc = lib.oracle_rep_draine(C.byref(bundle.tables), im, n, seeds[0], seeds[1],
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rep_draine failed with code {rc}")
+    return out
 
 
 def setemiss(nudust, kappad, adust, nlambda, nT: int = 500, nnu: int = 513, ndg: int | None = None,

@@ -46,7 +46,8 @@ GRID_FIELDS = [("rarr", _dp), ("r2arr", _dp), ("thetarr", _dp), ("costarr", _dp)
                ("sintarr", _dp), ("tan2arr", _dp), ("phiarr", _dp), ("aarr", _dp),
                ("barr", _dp), ("densarr", _dp), ("findopac", _ip), ("diffus", _ip),
                ("diffdir", _ip), ("tdust", _dp), ("vcell", _dp), ("ravearr", _dp),
-               ("Ldint", _dp), ("hdisk", _dp), ("vrarr", _dp), ("vthetarr", _dp), ("divvarr", _dp)]
+               ("Ldint", _dp), ("hdisk", _dp), ("vrarr", _dp), ("vthetarr", _dp), ("divvarr", _dp),
+               ("imean", _ip)]
 
 
 class Grid(C.Structure):
@@ -60,7 +61,8 @@ TABLE_FIELDS = [("nlambda", _ip), ("nudust", _dp), ("kappad", _dp), ("adust", _d
                 ("loghnu", _dp), ("aperture2", _dp), ("u", _dp), ("coste_arr", _dp),
                 ("sinte_arr", _dp), ("cospe_arr", _dp), ("sinpe_arr", _dp),
                 ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32),
-                ("isrf", _dp), ("nisrf", C.c_int32), ("pad_isrf", C.c_int32)]
+                ("isrf", _dp), ("nisrf", C.c_int32), ("pad_isrf", C.c_int32),
+                ("draine", _dp), ("nemit", C.c_int32), ("ndraine", C.c_int32)]
 
 
 class Tables(C.Structure):

@@ -101,6 +101,10 @@ struct mcrt_ctx {
   bool have_grid = false, have_tables = false;
   bool have_acc = false;              // ravearr / Ldint / hdisk uploaded (accretion packets)
   bool have_isrf = false;             // ISRF sampling table uploaded (external-illumination packets)
+  bool have_draine = false;           // small-grain emission spectra uploaded
+  bool have_sg = false;               // the grid holds small-grain components (ids 5-8)
+  int32_t imean_max = 0;              // largest imean of the grid (0: none given)
+  int32_t *d_imean = nullptr;
   std::string err;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -811,6 +815,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
   std::vector<int> slot_species;
   std::vector<double> dens_th(ncell, 0.0);
   std::vector<int32_t> idust3(ncell, 0), diffus(ncell, 0);
+  bool has_sg = false;
   for (int64_t k = 0; k < ncell; ++k) {
     CellRec& r = cells[k];
     std::memset(&r, 0, sizeof r);
@@ -821,7 +826,6 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
       if (!(rho > 0.0)) continue;
       const int sp = g->findopac[k + ncell * (id - 1)];
       if (id > 8) return fail(ctx, MCRT_ERR_UNSUPPORTED, "gas-opacity component %d is outside the built scope", id);
-      if (kIsSg[id - 1]) return fail(ctx, MCRT_ERR_UNSUPPORTED, "small-grain component %d needs rep_draine (out of scope)", id);
       if (sp != id) return fail(ctx, MCRT_ERR_UNSUPPORTED, "findopac(.,%d)=%d: dust components must map to their own species", id, sp);
       if (sp < 1 || sp > c.nopac) return fail(ctx, MCRT_ERR_ARG, "findopac out of range");
       if (n >= kMaxComp) return fail(ctx, MCRT_ERR_UNSUPPORTED, "more than %d non-zero density components in a cell", kMaxComp);
@@ -836,7 +840,7 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
       r.meta |= (uint32_t)s << (2 + 7 * n);
       r.meta |= (uint32_t)(id - 1) << (5 + 7 * n);
       ++n;
-      if (!kIsSg[id - 1]) { ++nth; dens_th[k] = rho; idust3[k] = id; }
+      if (!kIsSg[id - 1]) { ++nth; dens_th[k] = rho; idust3[k] = id; } else has_sg = true;
     }
     r.meta |= (uint32_t)n;
     if (nth > 1) return fail(ctx, MCRT_ERR_UNSUPPORTED, "cell with %d thermal components (tfinal allows one)", nth);
@@ -954,8 +958,23 @@ int mcrt_upload_grid(mcrt_ctx* ctx, const mcrt_grid* g) {
     CK(cudaStreamSynchronize(ctx->stream));     // the host vectors go out of scope
   }
   ctx->have_vel = vel;
+  // small-grain emission level per cell (imean), optional
+  int32_t imax = 0;
+  if (g->imean) {
+    for (int64_t k = 0; k < ncell; ++k) {
+      if (g->imean[k] < 1) return fail(ctx, MCRT_ERR_ARG, "imean(%lld) = %d: rows of the Draine table start at 1",
+                                       (long long)k, g->imean[k]);
+      imax = std::max(imax, g->imean[k]);
+    }
+    int rc3;
+    if (!ctx->d_imean && (rc3 = dalloc(ctx, &ctx->d_imean, ncell))) return rc3;
+    CK(cudaMemcpyAsync(ctx->d_imean, g->imean, ncell * 4, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->imean_max = imax;
+  ctx->have_sg = has_sg;
   CK(cudaStreamSynchronize(ctx->stream));
   DevModel& m = ctx->dm;
+  m.imean = g->imean ? ctx->d_imean : nullptr;
   const double* w = ctx->d_walls;
   m.rarr = w; w += nrg + 1;
   m.r2arr = w; w += nrg + 1;
@@ -1105,6 +1124,18 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
       if (!(t->isrf[i] >= t->isrf[i - 1])) return fail(ctx, MCRT_ERR_ARG, "isrf cdf must be non-decreasing");
     add(t->isrf, 3 * (int64_t)t->nisrf);
   }
+  // small-grain emission spectra (draine_cdf.f90): cdf_d, logcdf_d
+  // (nemit x ndraine) and logfreq_d (ndraine), as draine_mod holds them
+  const bool draine = t->draine != nullptr && t->nemit > 0 && t->ndraine > 0;
+  const int draine_at = draine ? (int)off.size() : -1;
+  if (draine) {
+    if (t->nemit > 1000 || t->ndraine < 2 || t->ndraine > 1000000)
+      return fail(ctx, MCRT_ERR_ARG, "nemit must be 1..1000 and ndraine 2..1e6");
+    const int64_t nn = 2 * (int64_t)t->nemit * t->ndraine + t->ndraine;
+    for (int64_t i = 0; i < nn; ++i)
+      if (!std::isfinite(t->draine[i])) return fail(ctx, MCRT_ERR_ARG, "draine table entry %lld is not finite", (long long)i);
+    add(t->draine, nn);
+  }
   // jump tables a^(2^30 * 2^k)
   std::vector<int64_t> jump(128);
   int64_t j1 = 1033780774, j2 = 1494757890;   // a1w, a2w (ecuyer_cote_mod.f90:14-15)
@@ -1153,6 +1184,12 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.isrf_logcdf = isrf ? m.isrf_cdf + t->nisrf : nullptr;
   m.isrf_logfreq = isrf ? m.isrf_cdf + 2 * (int64_t)t->nisrf : nullptr;
   ctx->have_isrf = isrf;
+  m.nemit = draine ? t->nemit : 0;
+  m.ndraine = draine ? t->ndraine : 0;
+  m.draine_cdf = draine ? b + off[draine_at] : nullptr;
+  m.draine_logcdf = draine ? m.draine_cdf + (int64_t)t->nemit * t->ndraine : nullptr;
+  m.draine_logfreq = draine ? m.draine_cdf + 2 * (int64_t)t->nemit * t->ndraine : nullptr;
+  ctx->have_draine = draine;
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;
@@ -1259,6 +1296,10 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   if (nsum != np) ns = ns + np - nsum;
   if (npacc > 1 && !ctx->have_acc)
     return fail(ctx, MCRT_ERR_ARG, "accretion packets (accfrac > 0) need ravearr, Ldint and hdisk in mcrt_upload_grid");
+  if (ctx->have_sg && !ctx->have_draine)
+    return fail(ctx, MCRT_ERR_UNSUPPORTED, "the grid has small-grain components (ids 5-8): upload the Draine spectra (mcrt_tables.draine)");
+  if (ctx->have_sg && std::max(ctx->imean_max, 2) > ctx->dm.nemit)
+    return fail(ctx, MCRT_ERR_ARG, "imean selects Draine row %d of %d", std::max(ctx->imean_max, 2), ctx->dm.nemit);
   if (npout > 0 && !ctx->have_isrf)
     return fail(ctx, MCRT_ERR_ARG, "external-illumination packets (isrf_frac > 0) need the isrf table in mcrt_upload_tables");
   // generator seeds (set_all_seeds)

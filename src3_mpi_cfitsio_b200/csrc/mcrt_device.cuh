@@ -96,6 +96,12 @@ struct DevModel {
   // external illumination: the ISRF sampling table (isrf_mod after isrf_cdf.f90)
   const double *isrf_cdf, *isrf_logcdf, *isrf_logfreq;
   int nisrf;
+  // small-grain emission: the Draine spectra (draine_mod after
+  // draine_cdf.f90), [nemit][ndraine] Fortran order, and the per-cell row
+  // (imean; nullptr: row 2 in the first iteration, row 1 afterwards)
+  const double *draine_cdf, *draine_logcdf, *draine_logfreq;
+  int nemit, ndraine;
+  const int32_t *imean;
   // star
   const double *atmosnu, *hnuint, *lognu, *loghnu, *limb_prob;
   const double *inczeta;                     // [MCRT_IZMAX]

@@ -462,6 +462,31 @@ struct Packet {
     nub = pow(10.0, lg);
   }
 
+  // Small-grain re-emission frequency (rep_draine_new.f90): locate3 in row
+  // im of the cumulative spectra (bisection over the columns, in the
+  // direction the row runs), then linear in log10 cdf and log10 nu between
+  // the bracketing columns.
+  __device__ double rep_draine(int im) {
+    const double xran = ran();
+    const int ne = m.nemit, nd = m.ndraine;
+    const double* cd = m.draine_cdf + (im - 1);
+    auto cdf = [&](int j) { return __ldg(cd + (int64_t)(j - 1) * ne); };
+    const bool asc = cdf(nd) > cdf(1);
+    int jl = 0, ju = nd + 1;
+    while (ju - jl > 1) {
+      const int jm = (ju + jl) >> 1;
+      if (asc == (xran > cdf(jm))) jl = jm; else ju = jm;
+    }
+    int i = jl;
+    if (i == nd) i = i - 1;
+    if (i == 0) i = 1;
+    const double* lc = m.draine_logcdf + (im - 1);
+    const double* lf = m.draine_logfreq;
+    const double c0 = __ldg(lc + (int64_t)(i - 1) * ne), c1 = __ldg(lc + (int64_t)i * ne);
+    const double lg = (log10(xran) - c0) / (c1 - c0) * (__ldg(lf + i) - __ldg(lf + i - 1)) + __ldg(lf + i - 1);
+    return pow(10.0, lg);
+  }
+
   __device__ void initpabs() {                     // initpabs.f90:1-44
     sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
     cosb = zp / rtot;
@@ -1674,6 +1699,26 @@ struct Packet {
   // diffusion cell, emission from the diffusion surface.  false = geometry
   // failure.
   __device__ bool emit_common(const LaunchParams& P, int64_t ci, const CellRec& c, int slot) {
+    const int id = m.slot_species[slot];    // dust components use their own species (findopacid_5.f90)
+    if (!cell_diffus(c.flags) && id >= 5 && id <= 8) {
+      // small grains (emit_common_2.f90:32-50): a frequency from the Draine
+      // spectrum of the cell's intensity level, then emit_sg.f90 (an
+      // unpolarised packet in a random direction).  The opacset the
+      // reference calls here is repeated by propagate right after.
+      const bool first = (P.block0_dev ? *P.block0_dev : P.block0) == 0;   // iteration 1
+      const int im = first ? 2 : (m.imean ? __ldg(m.imean + ci) : 1);
+      nub = rep_draine(im);
+      sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;
+      cost = 1.0 - 2.0 * ran();
+      sint = sqrt(1.0 - cost * cost);
+      phi = R2P * ran();
+      cosp = cos(phi);
+      sinp = sin(phi);
+      uy = sint * sinp;
+      ux = sint * cosp;
+      uz = cost;
+      return true;
+    }
     if (!cell_diffus(c.flags)) {
       const double tave = __ldg(m.tdust + ci);
       sip = 1.0; sqp = 0.0; sup = 0.0; svp = 0.0;    // reemit.f90

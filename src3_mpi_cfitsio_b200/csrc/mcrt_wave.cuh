@@ -430,15 +430,19 @@ __global__ void __launch_bounds__(kBlock, MCRT_WALK_MIN_BLOCKS) wave_walk(Launch
 #endif
       }
     }
-    const bool front = done && L.ev == EV_AFTER_WALK;
-    const bool back = done && !front;
-    const unsigned mf = __ballot_sync(FULL, front);
-    const unsigned mb = __ballot_sync(FULL, back);
-    const unsigned long long pf = warp_push(mf, front, &W.ctl->n_front);
-    const unsigned long long pb = warp_push(mb, back, &W.ctl->n_back);
-    if (front) W.evq[pf] = slot;
-    if (back) W.evq[W.slots - 1 - (int64_t)pb] = slot;
-    if (done) have = false;
+    // queue the ended walks (about half of the steps end none: a walk
+    // averages ~44 crossings)
+    if (__any_sync(FULL, done)) {
+      const bool front = done && L.ev == EV_AFTER_WALK;
+      const bool back = done && !front;
+      const unsigned mf = __ballot_sync(FULL, front);
+      const unsigned mb = __ballot_sync(FULL, back);
+      const unsigned long long pf = warp_push(mf, front, &W.ctl->n_front);
+      const unsigned long long pb = warp_push(mb, back, &W.ctl->n_back);
+      if (front) W.evq[pf] = slot;
+      if (back) W.evq[W.slots - 1 - (int64_t)pb] = slot;
+      if (done) have = false;
+    }
   }
   {
     const unsigned long long x = warp_sum(L.pk.c_cross);

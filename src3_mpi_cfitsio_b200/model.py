@@ -946,3 +946,74 @@ def with_isrf(m: Model, frac: float = 0.2, **kw) -> Model:
     m.tables["nisrf"] = t.size // 3
     m.config["isrf_frac"] = frac
     return m
+
+
+def draine_table(nemit: int = 18, ndraine: int = 1000, lmin_um: float = 1.0, lmax_um: float = 1000.0) -> np.ndarray:
+    """Small-grain (VSG/PAH) emission spectra in the layout draine_cdf.f90
+    leaves in draine_mod: cdf_d(nemit,ndraine), logcdf_d(nemit,ndraine) and
+    logfreq_d(ndraine), concatenated (Fortran order), frequencies ascending
+    in eV.  The reference reads Draine's emissivities at 18 intensity ratios
+    (uratio_arr 0.5 ... 1e7) from files that are not present; here row j is
+    a synthetic spectrum with the aromatic bands (3.3, 6.2, 7.7, 8.6, 11.3,
+    12.7, 17 um, Lorentzian profiles) over a modified-blackbody continuum
+    whose temperature rises with the intensity ratio (T = 40 K U^(1/6)), the
+    continuum's share growing with U.  The table itself follows
+    draine_cdf.f90 step for step: the wavelength grid reversed into
+    ascending frequency, trapezoidal cumulative sums in frequency, the rows
+    normalised, cdf 0 / log cdf -10 / log freq 0 in the first column."""
+    uratio = np.array([0.5, 1.0, 2.0, 5.0, 10.0, 20.0, 30.0, 1e2, 3e2, 1e3, 3e3, 1e4, 3e4, 1e5, 3e5, 1e6, 3e6, 1e7])
+    uratio = uratio[:nemit] if nemit <= uratio.size else np.logspace(-0.3, 7.0, nemit)
+    lam = np.logspace(math.log10(lmin_um), math.log10(lmax_um), ndraine)       # file order: increasing lambda
+    bands = [(3.3, 0.04, 0.3), (6.2, 0.15, 1.0), (7.7, 0.4, 2.0), (8.6, 0.3, 0.8), (11.3, 0.25, 1.5),
+             (12.7, 0.3, 0.6), (17.0, 1.0, 0.4)]
+    pdf = np.zeros((nemit, ndraine))
+    for j, U in enumerate(uratio):
+        T = 40.0 * U ** (1.0 / 6.0)
+        x = 14387.77 / (lam * T)
+        with np.errstate(over="ignore"):
+            cont = lam ** -5 / np.expm1(np.minimum(x, 700.0)) * lam ** -1.5
+        cont = cont / cont.max()
+        aro = sum(a / (1.0 + ((lam - l0) / w) ** 2) for l0, w, a in bands)
+        mix = 0.2 + 0.7 * (math.log10(U) + 0.3) / 7.3
+        pdf[j] = (1.0 - mix) * aro / aro.max() + mix * cont
+    freq = (1.2398 / lam)[::-1]                                  # draine_cdf.f90: freq_d(ndraine-i+1)
+    pdf_d = pdf[:, ::-1]
+    cdf = np.zeros((nemit, ndraine))
+    cdf[:, 1:] = np.cumsum(0.5 * (pdf_d[:, 1:] + pdf_d[:, :-1]) * (freq[1:] - freq[:-1])[None, :], axis=1)
+    cdf[:, 1:] = cdf[:, 1:] / cdf[:, -1:]
+    cdf[:, 0] = 0.0
+    logcdf = np.empty_like(cdf)
+    logcdf[:, 0] = -10.0
+    logcdf[:, 1:] = np.log10(cdf[:, 1:])
+    logfreq = np.empty(ndraine)
+    logfreq[0] = 0.0
+    logfreq[1:] = np.log10(freq[1:])
+    F = lambda a: np.asfortranarray(a).ravel(order="F")
+    return np.concatenate([F(cdf), F(logcdf), logfreq])
+
+
+def with_small_grains(m: Model, fsg: float = 0.2, sg_cavity: bool = True, **kw) -> Model:
+    """Small grains (VSG/PAH, component ids 5-8, grid_mod_5.f90:20): a
+    fraction `fsg` of the disk's and the envelope's dust mass moves to their
+    small-grain components (ids 6 and 7), and with `sg_cavity` the cavity's
+    dust becomes small grains only (id 8).  The reference's select_dust
+    (select_dust_2.f90:20-33) picks the one thermal component of a cell
+    whenever there is exactly one, so small grains absorb and re-emit (from
+    the Draine spectra, ``draine_table``) only in cells without thermal dust,
+    here the cavity.  Species 5-8 use the dust law of the others."""
+    w = m.w
+    d = m.dens4().copy()
+    d[..., 5] = fsg * d[..., 1]
+    d[..., 1] = (1.0 - fsg) * d[..., 1]
+    d[..., 6] = fsg * d[..., 2]
+    d[..., 2] = (1.0 - fsg) * d[..., 2]
+    if sg_cavity:
+        d[..., 7] = d[..., 3]
+        d[..., 3] = 0.0
+    m.grid["densarr"] = np.asfortranarray(d).ravel(order="F")
+    t = draine_table(**kw)
+    m.tables["draine"] = t
+    nemit = kw.get("nemit", 18)
+    m.tables["nemit"] = nemit
+    m.tables["ndraine"] = t.size // (2 * nemit + 1)
+    return m

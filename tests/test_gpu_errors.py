@@ -12,7 +12,7 @@ from src3_mpi_cfitsio_b200 import model
 
 pytestmark = pytest.mark.gpu
 
-ERR_ARG, ERR_GEOM, ERR_TIMEOUT = 1, 4, 5
+ERR_ARG, ERR_UNSUPPORTED, ERR_GEOM, ERR_TIMEOUT = 1, 3, 4, 5
 
 
 def _engine(m, precision="fp64"):
@@ -86,4 +86,33 @@ def test_wave_limit_times_out_and_the_next_run_is_whole():
     assert eng.download(images=False).counters()["packets"] < 20000
     eng.set_limits()
     _normal_run(eng, 20000)
+    eng.close()
+
+
+def test_small_grains_without_draine_spectra_are_refused():
+    """A grid with small-grain components but no Draine spectra uploads, and
+    the run refuses it with MCRT_ERR_UNSUPPORTED before any launch; a Draine
+    row beyond the table (imean) is MCRT_ERR_ARG; with the spectra the run
+    goes through."""
+    from src3_mpi_cfitsio_b200.engine import MCRTError
+    m = model.with_small_grains(model.warm(model.small_2d()))
+    tables = dict(m.tables)
+    bare = copy.deepcopy(m)
+    for k in ("draine", "nemit", "ndraine"):
+        bare.tables.pop(k)
+    eng = _engine(bare)
+    with pytest.raises(MCRTError) as e:
+        eng.run(1000, ipeel=0)
+    assert e.value.code == ERR_UNSUPPORTED
+    eng.close()
+    over = copy.deepcopy(m)
+    c = over.config
+    over.grid["imean"] = np.full(c["nrg"] * c["ntg"] * c["npg"], tables["nemit"] + 1, np.int32)
+    eng = _engine(over)
+    with pytest.raises(MCRTError) as e:
+        eng.run(1000, ipeel=0)
+    assert e.value.code == ERR_ARG
+    eng.close()
+    eng = _engine(m)
+    _normal_run(eng)
     eng.close()

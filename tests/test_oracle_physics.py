@@ -371,3 +371,43 @@ def test_oracle_adjoint_control_variate(oracle_mod):
     segments = n + int(events["nscat"].sum() + events["nabs"].sum())
     assert vc.sum() == segments
     assert (vc >= 0).all() and np.isfinite(vs).all() and vs.sum() > 0
+
+
+def test_rep_draine_samples_the_draine_spectrum(oracle_mod):
+    """rep_draine (oracle restatement) draws frequencies whose distribution
+    is the row's cumulative spectrum: the fraction of draws below each
+    column frequency matches cdf_d at that column (Kolmogorov distance of
+    2e5 draws below 5e-3, where the sampling error is ~2e-3); rows of
+    higher intensity ratio emit bluer."""
+    m = model.with_small_grains(model.warm(model.small_2d()))
+    b = abi.Bundle(m)
+    ne, nd = m.tables["nemit"], m.tables["ndraine"]
+    t = m.tables["draine"]
+    cdf = t[:ne * nd].reshape((ne, nd), order="F")
+    freq = 10.0 ** t[2 * ne * nd:]
+    medians = []
+    for im in (1, 2, 9, 18):
+        nu = np.sort(oracle_mod.rep_draine(b, im, 200000))
+        assert np.isfinite(nu).all() and (nu > 0).all()
+        emp = np.searchsorted(nu, freq[1:], side="right") / nu.size
+        assert np.abs(emp - cdf[im - 1, 1:]).max() < 5e-3, im
+        medians.append(np.median(nu))
+    assert medians[-1] > medians[0]
+
+
+def test_small_grains_reemit_in_cells_without_thermal_dust(oracle_mod):
+    """With small grains in the disk and envelope and a small-grain-only
+    cavity, absorptions by small grains (dsg) occur only in cells without
+    thermal dust (select_dust's one-thermal-component rule), every packet
+    is accounted for, and the first and a later iteration (Draine rows 2
+    and 1) both run."""
+    m = model.with_small_grains(model.warm(model.small_2d()))
+    d = m.dens4()
+    thermal = (d[..., [0, 1, 2, 3, 8, 9]] > 0).any(axis=-1)
+    n = 20000
+    for it in (1, 2):
+        tal, _ = oracle_mod.run(abi.Bundle(m), n, ipeel=0, iteration=it, threads=4)
+        dsg = tal["dsg"].reshape(d.shape[:3], order="F")
+        assert dsg.sum() > 0 and dsg[thermal].sum() == 0
+        c = tal.counters()
+        assert c["packets"] == n and c["exited"] + c["killed"] + c["geom_fail"] == n
