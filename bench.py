@@ -434,6 +434,22 @@ def run_ours(args, rank, world):
         abytes = algorithmic_bytes(counters)
         kname = f"transport_sched ({args.precision})"
     achieved = abytes / (kms / 1e3) / 1e9
+    # The timed steps run the wavefront loop as one graph launch per
+    # iteration, whose walk times are %globaltimer stamps between the loop's
+    # launches.  One more iteration with the host-driven loop times every
+    # walk launch with CUDA events on the engine's stream, as a cross-check.
+    event_check = None
+    if args.schedule == "wave":
+        eng.set_wave_loop(False)
+        eng.reset_tallies()
+        eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
+        wh = eng.wave_stats()
+        eng.set_wave_loop(True)
+        reduce_ranks(eng)
+        event_check = {"walk_ms_per_launch": wh["walk_ms"] / max(wh["walk_launches"], 1),
+                       "achieved_gbs": 16.0 * wh["walk_crossings"] / max(wh["walk_launches"], 1)
+                       / (wh["walk_ms"] / max(wh["walk_launches"], 1) / 1e3) / 1e9,
+                       "how": "host-driven loop, CUDA events around each walk launch, one iteration after the timed steps"}
     # secondary (compute) roofline of the same launches: ~100 FP64 operations
     # per cell crossing (the face quadratics with their square roots and
     # divisions, the compares, the move), against the nominal FP64 vector
@@ -554,13 +570,15 @@ def run_ours(args, rank, world):
                   "frac": achieved / peak, "traffic": traffic,
                   "peak_source": "measured" if not peaks.get("_fallback") else "fallback",
                   "kernel": kname, "kernel_ms_per_launch": kms, "algorithmic_bytes_per_launch": abytes,
-                  "note": "cell walk: L2-resident grid, issue/latency-bound; 16 B per crossing is the "
+                  "timing": "device-driven loop: %globaltimer stamps between the launches of the timed steps",
+                  "cuda_event_check": event_check,
+                  "note": "cell walk: L2-resident grid, issue-bound; 16 B per crossing is the "
                           "algorithmic HBM-equivalent traffic"},
         roofline_compute={"achieved": fp64_tflops, "peak": fp64_peak, "unit": "TFLOP/s (FP64)",
                           "frac": fp64_tflops / fp64_peak, "peak_source": "nominal",
                           "flops_per_crossing": 100,
                           "note": "neither HBM nor the FP64 pipe bounds the walk: ncu shows instruction issue "
-                                  "on ~49 % of cycles with fixed-latency FP64 dependencies as the main stall"},
+                                  "on ~68 % of cycles at 32 warps/SM, half of each warp's lanes active"},
         kernels_ms_last_step=kernels,
         # kernels of the last timed step (transport launches counted by the
         # engine, plus tfinal_cells / tfinal_mirror / tfinal_stats /

@@ -385,6 +385,18 @@ int mcrt_adjoint(mcrt_ctx *ctx, int64_t np, int64_t iphot_lo, int64_t iphot_hi, 
  * models without diffusion cells can need that.  Every chunk's forward pass
  * ends with its own tail of long-lived packets, so large chunks are faster. */
 int mcrt_set_adjoint_chunk(mcrt_ctx *ctx, int64_t packets);
+/* Who drives the wavefront loop of mcrt_run_iteration.  No reference
+ * counterpart.  1 (default): the device, as one CUDA-graph launch per
+ * iteration whose WHILE node runs the event and walk launches and decides
+ * on the device when to hand over to the tail launch; the host waits once.
+ * It applies to iterations without peel-off jobs and outside the adjoint;
+ * the graph is captured on the first such call and again whenever the
+ * launch parameters change (packet range, seeds, grid or table uploads,
+ * schedule settings), so the first call after a change also pays the
+ * capture.  0: the host reads the queue sizes after every walk launch (as
+ * peeled iterations and the adjoint always do).  Results do not depend on
+ * it. */
+int mcrt_set_wave_loop(mcrt_ctx *ctx, int32_t device_loop);
 /* Control variate of the adjoint's replay.  No reference counterpart.  A
  * segment's score (delta at the interaction minus the optical depth of the
  * segment, per cell and component) has zero mean given the segment's start,

@@ -71,6 +71,18 @@ struct mcrt_ctx {
   int64_t wave_pool = 1 << 21;
   int64_t wave_jobs = 0;              // peel-off job queue capacity asked for (0: default)
   int64_t wave_tail = -1;             // tail launch at <= this many live packets (<0: 8 per tail lane, 0: never)
+  // device-driven wavefront loop (mcrt_set_wave_loop): the graph captured
+  // for the last packet range and the launch parameters it was captured with
+  int32_t wave_device_loop = 1;
+  cudaGraph_t wl_graph = nullptr;
+  cudaGraphExec_t wl_exec = nullptr;
+  cudaStream_t wl_body = nullptr;
+  LaunchParams wl_params;
+  WaveArgs wl_w;
+  unsigned long long wl_tail = 0, wl_max = 0;
+  int64_t wl_npk = 0;
+  int64_t *d_block0 = nullptr, *h_block0 = nullptr;   // the iteration's first random block, read by the graph
+  WaveCtl* h_ctl = nullptr;
   int64_t wave_cap = 0;
   WaveRec *d_recs = nullptr;
   int32_t *d_walkq = nullptr, *d_evq = nullptr;
@@ -599,17 +611,35 @@ __global__ void add_counters(unsigned long long* cnt, unsigned long long waves, 
 // Device-driven wavefront loop (a CUDA-graph WHILE node whose body is event
 // launch, wave_loop_mid, walk launch, wave_loop_cond): the decisions the
 // host loop of run_iteration_impl takes after each walk launch.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The loop kernels also time the launches between them: each adds the time
+// since the previous stamp to its kernel class (the launch gaps included).
+__global__ void wave_loop_start(WaveCtl* c) { c->t_last = global_ns(); }
+
 __global__ void wave_loop_mid(WaveCtl* c) {
+  const unsigned long long t = global_ns();
+  c->ev_ns += t - c->t_last;
+  c->t_last = t;
   c->n_front = 0;
   c->n_back = 0;
   c->walk_fetch = 0;
 }
 
-// pad1 counts waves, pad2 flags a loop stopped by the wave limit.  Ends the
+// pad1 counts waves, pad2 flags a loop stopped by the wave limit (its
+// packets in flight are abandoned: the tail launch finds none).  Ends the
 // loop when no packet is live, or hands the rest to the tail launch once
 // every packet has started and at most tail_live are live.
 __global__ void wave_loop_cond(WaveCtl* c, const unsigned long long* next, int64_t npk, unsigned long long tail_live,
                                unsigned long long max_waves, cudaGraphConditionalHandle h) {
+  const unsigned long long t = global_ns();
+  c->walk_ns += t - c->t_last;
+  c->t_last = t;
+  c->walks += c->n_walk;
   const unsigned long long live = c->n_front + c->n_back;
   const unsigned long long waves = c->pad1 + 1;
   c->pad1 = waves;
@@ -620,13 +650,72 @@ __global__ void wave_loop_cond(WaveCtl* c, const unsigned long long* next, int64
   if (go && waves >= max_waves) {
     go = false;
     c->pad2 = 1;
+    c->n_front = 0;
+    c->n_back = 0;
   }
   cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
-__global__ void wave_loop_finish(unsigned long long* cnt, const WaveCtl* c) {
+__global__ void wave_loop_finish(unsigned long long* cnt, WaveCtl* c) {
+  c->tail_ns += global_ns() - c->t_last;
   cnt[MCRT_C_WAVES] += c->pad1;
-  cnt[MCRT_C_LAUNCHES] += 4 * c->pad1 + 4;    // + wave_init, tail, diffusion_finalize, this
+  cnt[MCRT_C_LAUNCHES] += 4 * c->pad1 + 5;    // + wave_init, wave_loop_start, tail, diffusion_finalize, this
+}
+
+// Captures on stream s (in capture mode) the device-driven wavefront loop of
+// one packet range: loop reset, wave_init, the WHILE node whose body (event
+// launch, wave_loop_mid, walk launch, wave_loop_cond) is captured on stream
+// bs, the tail launch (no work when the loop ended with no live packet) and
+// wave_loop_finish.  The kernels' arguments are fixed at capture.
+cudaError_t capture_wave_loop(const LaunchParams& P, const WaveArgs& W, unsigned long long* next,
+                              unsigned long long* cnt, int64_t npk, unsigned long long tail_live,
+                              unsigned long long max_waves, bool mixed, int nsm, cudaStream_t s, cudaStream_t bs) {
+  const int egrid = nsm * (mixed ? wave_event_mixed_blocks_per_sm() : wave_event_fp64_blocks_per_sm());
+  const int wgrid = nsm * (mixed ? wave_walk_mixed_blocks_per_sm() : wave_walk_fp64_blocks_per_sm());
+  const int tgrid = nsm * (mixed ? wave_tail_mixed_blocks_per_sm() : wave_tail_fp64_blocks_per_sm());
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(next, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(W.ctl, 0, sizeof(WaveCtl), s)) != cudaSuccess) return e;
+  if ((e = launch_wave_init(W, s)) != cudaSuccess) return e;
+  wave_loop_start<<<1, 1, 0, s>>>(W.ctl);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn;
+  if ((e = cudaGraphAddNode(&cn, g, deps, nd, &cp)) != cudaSuccess) return e;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return e;
+  cudaError_t eb = mixed ? launch_wave_event_mixed(P, W, egrid, bs) : launch_wave_event_fp64(P, W, egrid, bs);
+  if (eb == cudaSuccess) {
+    wave_loop_mid<<<1, 1, 0, bs>>>(W.ctl);
+    eb = cudaGetLastError();
+  }
+  if (eb == cudaSuccess) eb = mixed ? launch_wave_walk_mixed(P, W, wgrid, bs) : launch_wave_walk_fp64(P, W, wgrid, bs);
+  if (eb == cudaSuccess) {
+    wave_loop_cond<<<1, 1, 0, bs>>>(W.ctl, next, npk, tail_live, max_waves, h);
+    eb = cudaGetLastError();
+  }
+  cudaGraph_t bout = nullptr;
+  e = cudaStreamEndCapture(bs, &bout);
+  if (eb != cudaSuccess) return eb;
+  if (e != cudaSuccess) return e;
+  if ((e = cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess) return e;
+  LaunchParams T = P;
+  T.fetch_off = 1;
+  if ((e = mixed ? launch_wave_tail_mixed(T, W, tgrid, s) : launch_wave_tail_fp64(T, W, tgrid, s)) != cudaSuccess) return e;
+  wave_loop_finish<<<1, 1, 0, s>>>(cnt, W.ctl);
+  return cudaGetLastError();
 }
 
 // diskflux (flux_test.f90:14-82) on the REAL arrays the download produces
@@ -758,6 +847,11 @@ void mcrt_destroy(mcrt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->wl_exec) cudaGraphExecDestroy(ctx->wl_exec);
+  if (ctx->wl_graph) cudaGraphDestroy(ctx->wl_graph);
+  if (ctx->wl_body) cudaStreamDestroy(ctx->wl_body);
+  if (ctx->h_block0) cudaFreeHost(ctx->h_block0);
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   if (ctx->h_wctl) cudaFreeHost(ctx->h_wctl);
   if (ctx->h_geom) cudaFreeHost(ctx->h_geom);
   for (auto& p : ctx->kt_ev)
@@ -1305,7 +1399,7 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;
   for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }
-  P = LaunchParams{};
+  std::memset(&P, 0, sizeof P);
   P.m = ctx->dm;
   DevModel& m = P.m;
   m.nrg = c.nrg; m.ntg = c.ntg; m.npg = c.npg; m.nopac = c.nopac; m.nlammax = c.nlammax; m.nT = c.nT; m.nnu = c.nnu;
@@ -1344,9 +1438,75 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   return MCRT_OK;
 }
 
+// The wavefront loop of one packet range as one graph launch (no peel-off
+// queue, no adjoint): the loop's decisions run on the device
+// (capture_wave_loop), so the host waits once instead of after every walk
+// launch.  The graph is captured again when the launch parameters change;
+// the iteration enters through block0_dev, which the graph's first node
+// copies from pinned host memory.  Kernel times come from the loop's own
+// %globaltimer stamps.
+static int run_wave_device_loop(mcrt_ctx* ctx, const LaunchParams& P, const WaveArgs& W, int64_t npk,
+                                unsigned long long tail_live, bool mixed) {
+  if (!ctx->d_block0) {
+    int rc = dalloc(ctx, &ctx->d_block0, 1);
+    if (rc) return rc;
+    CK(cudaHostAlloc((void**)&ctx->h_block0, sizeof(int64_t), cudaHostAllocDefault));
+    CK(cudaHostAlloc((void**)&ctx->h_ctl, sizeof(WaveCtl), cudaHostAllocDefault));
+    CK(cudaStreamCreateWithFlags(&ctx->wl_body, cudaStreamNonBlocking));
+  }
+  LaunchParams K = P;
+  K.block0 = 0;
+  K.block0_dev = ctx->d_block0;
+  const unsigned long long max_waves = (unsigned long long)ctx->wave_limit;
+  const bool same = ctx->wl_exec && std::memcmp(&K, &ctx->wl_params, sizeof K) == 0 &&
+                    std::memcmp(&W, &ctx->wl_w, sizeof W) == 0 && ctx->wl_tail == tail_live &&
+                    ctx->wl_max == max_waves && ctx->wl_npk == npk;
+  if (!same) {
+    if (ctx->wl_exec) cudaGraphExecDestroy(ctx->wl_exec);
+    if (ctx->wl_graph) cudaGraphDestroy(ctx->wl_graph);
+    ctx->wl_exec = nullptr;
+    ctx->wl_graph = nullptr;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ec = cudaMemcpyAsync(ctx->d_block0, ctx->h_block0, sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
+    if (ec == cudaSuccess)
+      ec = capture_wave_loop(K, W, ctx->d_next, ctx->dt.cnt, npk, tail_live, max_waves, mixed, ctx->nsm, ctx->stream,
+                             ctx->wl_body);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &gr);
+    if (ec != cudaSuccess || ee != cudaSuccess) {
+      if (gr) cudaGraphDestroy(gr);
+      return fail(ctx, MCRT_ERR_CUDA, "wave loop graph capture: %s", cudaGetErrorString(ec != cudaSuccess ? ec : ee));
+    }
+    ctx->wl_graph = gr;
+    CK(cudaGraphInstantiate(&ctx->wl_exec, gr, 0));
+    ctx->wl_params = K;
+    ctx->wl_w = W;
+    ctx->wl_tail = tail_live;
+    ctx->wl_max = max_waves;
+    ctx->wl_npk = npk;
+  }
+  *ctx->h_block0 = P.block0;
+  CK(cudaGraphLaunch(ctx->wl_exec, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_wctl, sizeof(WaveCtl), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const WaveCtl& c = *ctx->h_ctl;
+  ctx->last_waves = (int64_t)c.pad1;
+  ctx->kt_ms[0] = 1e-6 * (double)c.walk_ns;      // walk, event, tail (kernel classes of wave_stats)
+  ctx->kt_ms[1] = 1e-6 * (double)c.ev_ns;
+  ctx->kt_ms[2] = 1e-6 * (double)c.tail_ns;
+  ctx->kt_launch[0] = ctx->kt_launch[1] = (int64_t)c.pad1;
+  ctx->kt_launch[2] = 1;
+  ctx->kt_walks = (int64_t)c.walks;
+  ctx->h_wctl[5] = c.walk_cross;
+  if (c.pad2)                          // the packets in flight were abandoned; the context stays usable
+    return fail(ctx, MCRT_ERR_TIMEOUT, "wavefront loop stopped after %llu waves with packets in flight", c.pad1);
+  return MCRT_OK;
+}
+
 static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t iter, int32_t ipeel,
                               int32_t seed1, int32_t seed2, int32_t generator, int adj_mode) {
-  LaunchParams P{};
+  LaunchParams P;
+  std::memset(&P, 0, sizeof P);         // padding too: the device loop compares launch parameters bytewise
   {
     const int rc0 = make_params(ctx, np, lo, hi, iter, ipeel, seed1, seed2, generator, P);
     if (rc0) return rc0;
@@ -1408,6 +1568,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
   P.job_cap = ctx->job_cap;
   const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
   int64_t launches = 0;                     // kernels this call launches (MCRT_C_LAUNCHES)
+  bool devloop = false;                     // the wavefront loop ran as one graph launch
   // device time per kernel class (wavefront schedule): events around each
   // launch, read back at the next host synchronisation
   enum { KT_WALK = 0, KT_EVENT = 1, KT_TAIL = 2, KT_PEEL = 3 };
@@ -1482,6 +1643,11 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     const unsigned long long tail_live = adj_mode ? 0ull
                                          : ctx->wave_tail < 0 ? (unsigned long long)tgrid * kTransportBlock * 8ull
                                                               : (unsigned long long)ctx->wave_tail;
+    devloop = ctx->wave_device_loop != 0 && !queue && adj_mode == 0;
+    if (devloop) {
+      int rc = run_wave_device_loop(ctx, P, W, npk, tail_live, mixed);
+      if (rc) return rc;
+    } else {
     CK(cudaMemsetAsync(ctx->d_next, 0, 4 * sizeof(unsigned long long), ctx->stream));
     cudaError_t e = launch_wave_init(W, ctx->stream);
     if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "wave init: %s", cudaGetErrorString(e));
@@ -1548,6 +1714,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     CK(cudaMemcpyAsync(h + 5, &ctx->d_wctl->walk_cross, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        ctx->stream));
     ctx->last_waves = waves;
+    }
   }
   int per_sm = wave ? 1 : ctx->precision == MCRT_PREC_FP64
                               ? (warp ? transport_sched_fp64_blocks_per_sm() : transport_fp64_blocks_per_sm())
@@ -1576,8 +1743,10 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   cudaError_t ef = launch_diffusion_finalize(P.m, ctx->dt.ndiff, ctx->d_tdust0, ctx->d_tdust, P.nphot_diff, ctx->stream);
   if (ef != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion finalize: %s", cudaGetErrorString(ef));
-  launches += 2;                              // diffusion_finalize and add_counters
-  add_counters<<<1, 1, 0, ctx->stream>>>(ctx->dt.cnt, (unsigned long long)(wave ? ctx->last_waves : 0),
+  // diffusion_finalize and add_counters (the graph's wave_loop_finish
+  // counts its waves and launches, diffusion_finalize included)
+  launches += devloop ? 1 : 2;
+  add_counters<<<1, 1, 0, ctx->stream>>>(ctx->dt.cnt, (unsigned long long)(wave && !devloop ? ctx->last_waves : 0),
                                          (unsigned long long)launches);
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(ctx->h_geom + 1, ctx->dt.cnt + MCRT_C_GEOM_FAIL, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -1759,6 +1928,12 @@ int adjoint_range(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_t ite
 int mcrt_set_adjoint_chunk(mcrt_ctx* ctx, int64_t packets) {
   if (!ctx || packets < 1 || packets >= ((int64_t)1 << 31)) return MCRT_ERR_ARG;
   ctx->adj_chunk = packets;
+  return MCRT_OK;
+}
+
+int mcrt_set_wave_loop(mcrt_ctx* ctx, int32_t device_loop) {
+  if (!ctx || (device_loop != 0 && device_loop != 1)) return MCRT_ERR_ARG;
+  ctx->wave_device_loop = device_loop;
   return MCRT_OK;
 }
 
@@ -2302,56 +2477,16 @@ cudaError_t batch_capture_wave_branch(mcrt_batch* b, int i, int64_t npk, cudaStr
   W.ctl = w.ctl;
   W.slots = std::min<int64_t>(b->wave_slots, npk);
   W.walk_batch = c->wave_batch > 0 ? c->wave_batch : 8;
-  const int egrid = b->nsm * (mixed ? wave_event_mixed_blocks_per_sm() : wave_event_fp64_blocks_per_sm());
-  const int wgrid = b->nsm * (mixed ? wave_walk_mixed_blocks_per_sm() : wave_walk_fp64_blocks_per_sm());
   const int tgrid = b->nsm * (mixed ? wave_tail_mixed_blocks_per_sm() : wave_tail_fp64_blocks_per_sm());
   const unsigned long long tail_live = (unsigned long long)tgrid * kTransportBlock * 8ull;
   cudaError_t e;
   if ((e = cudaMemsetAsync(c->d_tally, 0, c->tally_bytes, s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(w.next, 0, 4 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(w.ctl, 0, sizeof(WaveCtl), s)) != cudaSuccess) return e;
-  if ((e = launch_wave_init(W, s)) != cudaSuccess) return e;
-  cudaStreamCaptureStatus st;
-  cudaGraph_t g = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t nd = 0;
-  if ((e = cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd)) != cudaSuccess) return e;
-  cudaGraphConditionalHandle h;
-  if ((e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
-  cudaGraphNodeParams cp{};
-  cp.type = cudaGraphNodeTypeConditional;
-  cp.conditional.handle = h;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t cn;
-  if ((e = cudaGraphAddNode(&cn, g, deps, nd, &cp)) != cudaSuccess) return e;
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  cudaStream_t bs = b->body_stream;
-  if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+  // the tail launch takes over once every packet has started, so the loop
+  // needs a few thousand waves at most; the limit only bounds a fault
+  if ((e = capture_wave_loop(P, W, w.next, c->dt.cnt, npk, tail_live, 1000000ull, mixed, b->nsm, s, b->body_stream)) !=
+      cudaSuccess)
     return e;
-  cudaError_t eb = mixed ? launch_wave_event_mixed(P, W, egrid, bs) : launch_wave_event_fp64(P, W, egrid, bs);
-  if (eb == cudaSuccess) {
-    wave_loop_mid<<<1, 1, 0, bs>>>(w.ctl);
-    eb = cudaGetLastError();
-  }
-  if (eb == cudaSuccess) eb = mixed ? launch_wave_walk_mixed(P, W, wgrid, bs) : launch_wave_walk_fp64(P, W, wgrid, bs);
-  if (eb == cudaSuccess) {
-    // the tail launch takes over once every packet has started, so the loop
-    // needs a few thousand waves at most; the limit only bounds a fault
-    wave_loop_cond<<<1, 1, 0, bs>>>(w.ctl, w.next, npk, tail_live, 1000000ull, h);
-    eb = cudaGetLastError();
-  }
-  cudaGraph_t bout = nullptr;
-  e = cudaStreamEndCapture(bs, &bout);
-  if (eb != cudaSuccess) return eb;
-  if (e != cudaSuccess) return e;
-  if ((e = cudaStreamUpdateCaptureDependencies(s, &cn, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess) return e;
-  LaunchParams T = P;
-  T.fetch_off = 1;
-  if ((e = mixed ? launch_wave_tail_mixed(T, W, tgrid, s) : launch_wave_tail_fp64(T, W, tgrid, s)) != cudaSuccess) return e;
-  if ((e = launch_diffusion_finalize(P.m, c->dt.ndiff, c->d_tdust0, c->d_tdust, P.nphot_diff, s)) != cudaSuccess) return e;
-  wave_loop_finish<<<1, 1, 0, s>>>(c->dt.cnt, w.ctl);
-  return cudaGetLastError();
+  return launch_diffusion_finalize(P.m, c->dt.ndiff, c->d_tdust0, c->d_tdust, P.nphot_diff, s);
 }
 
 int batch_build_wave(mcrt_batch* b, const int64_t* np) {

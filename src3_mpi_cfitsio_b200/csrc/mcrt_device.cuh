@@ -176,6 +176,10 @@ struct WaveCtl {
   unsigned long long n_front, n_back, walk_fetch;         // zeroed before each walk launch
   unsigned long long walk_cross;                          // crossings stepped by walk launches (whole loop)
   unsigned long long n_walk, ev_fetch, pad1, pad2;        // zeroed before each event launch
+  // device-driven loop (CUDA-graph WHILE node): %globaltimer stamp of the
+  // last loop kernel, device time of the event launches, walk launches and
+  // the tail [ns], walks queued over the loop
+  unsigned long long t_last, ev_ns, walk_ns, tail_ns, walks, pad3, pad4, pad5;
 };
 
 struct WaveArgs {

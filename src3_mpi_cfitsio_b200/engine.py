@@ -86,6 +86,7 @@ def load_library(path: str = LIB_PATH):
                                        P(C.c_double)]
     lib.mcrt_set_adjoint_chunk.argtypes = [C.c_void_p, C.c_int64]
     lib.mcrt_set_adjoint_baseline.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.c_double]
+    lib.mcrt_set_wave_loop.argtypes = [C.c_void_p, C.c_int32]
     lib.mcrt_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_double),
                                   P(C.c_double), P(C.c_double), C.c_int32, C.c_int32, P(C.c_double), P(C.c_double),
                                   P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int64),
@@ -107,7 +108,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
                  "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
-                 "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_set_adjoint_baseline", "mcrt_model_density"):
+                 "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_set_adjoint_baseline", "mcrt_set_wave_loop", "mcrt_model_density"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -270,6 +271,12 @@ class Engine:
         queue capacity (0: default) and the live-packet count at which one
         tail launch finishes the iteration (<0: default, 0: never)."""
         self._check(self.lib.mcrt_set_wave_pool(self.ctx, int(slots), int(peel_jobs), int(tail_packets)))
+
+    def set_wave_loop(self, device: bool = True):
+        """Wavefront loop driven by the device (one graph launch per
+        iteration) or by the host (a synchronisation after every walk
+        launch); C ABI ``mcrt_set_wave_loop``."""
+        self._check(self.lib.mcrt_set_wave_loop(self.ctx, 1 if device else 0))
 
     def upload_grid(self):
         self.bundle = abi.Bundle(self.model)

@@ -262,6 +262,46 @@ def test_schedules_agree_bitwise(warm_small, batch):
         assert np.array_equal(a[k], b[k]), k
 
 
+@pytest.mark.parametrize("precision,pool,tail", [("fp64", 1 << 21, -1), ("mixed", 2048, -1), ("mixed", 1024, 0)])
+def test_device_wave_loop_matches_host_loop(warm_small, precision, pool, tail):
+    """The wavefront loop as one graph launch (the device decides on the
+    next wave and on the tail launch) runs the same packets as the
+    host-driven loop: packet logs bit for bit, counters exactly, tallies up
+    to FP64 summation order; a second iteration reuses the captured graph
+    with the iteration's random blocks, and the loop's own timings account
+    for every wave."""
+    n = 20000
+    out = []
+    for device in (False, True):
+        eng = _engine(warm_small, precision=precision)
+        eng.set_schedule("wave")
+        eng.set_wave_pool(pool, 0, tail)
+        eng.set_wave_loop(device)
+        eng.enable_packet_log(n)
+        logs, tals, stats = [], [], []
+        for it in (1, 2):
+            eng.reset_tallies()
+            eng.run(n, ipeel=0, iteration=it)
+            logs.append(abi.packet_log_to_numpy(eng.packet_log(n)))
+            tals.append(eng.download(images=False))
+            stats.append(eng.wave_stats())
+        eng.close()
+        out.append((logs, tals, stats))
+    (lh, th, sh), (ld, td, sd) = out
+    for it in range(2):
+        for k in lh[it]:
+            assert np.array_equal(lh[it][k], ld[it][k]), (it, k)
+        ch, cd = th[it].counters(), td[it].counters()
+        for k in ("packets", "crossings", "interactions", "scatters", "killed", "exited", "starhits", "waves"):
+            assert ch[k] == cd[k], (it, k)
+        assert np.allclose(th[it]["dtauabs"], td[it]["dtauabs"], rtol=1e-10, atol=1e-12 * th[it]["dtauabs"].max())
+        assert np.array_equal(th[it]["nabs"], td[it]["nabs"])
+        assert sd[it]["walk_launches"] == sh[it]["walk_launches"] == ch["waves"]
+        assert sd[it]["walks"] == sh[it]["walks"] and sd[it]["walk_crossings"] == sh[it]["walk_crossings"]
+        assert sd[it]["walk_ms"] > 0 and sd[it]["event_ms"] > 0
+    assert not np.array_equal(ld[0]["ndraws"], ld[1]["ndraws"])       # the second iteration drew other blocks
+
+
 @pytest.mark.parametrize("precision,pool,batch,tail", [("fp64", 1 << 21, 8, -1), ("fp64", 96, 1, 0),
                                                        ("fp64", 512, 32, 200), ("mixed", 1 << 21, 8, -1),
                                                        ("mixed", 256, 8, 0)])
