@@ -337,7 +337,13 @@ def run_ours(args, rank, world):
             mdist.allreduce_device_tallies(e, device=dev)
             e.refresh_diffusion()
 
+    # gridset reruns setdiffus at the start of every iteration
+    # (gridset_5_model13new.f90:1842-1866): the diffusion region follows tdave
+    diffusion = bool(m.config.get("diffusion"))
+
     def step(it, e, precision=None):
+        if diffusion:
+            e.setdiffus(it)
         e.reset_tallies()
         e.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
         kms = e.kernel_ms()
@@ -357,6 +363,8 @@ def run_ours(args, rank, world):
         eng.mark(0)
         for s in range(args.steps):
             it = args.warmup + s + 1
+            if diffusion:
+                eng.setdiffus(it)
             eng.reset_tallies()
             eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
             kernel_ms.append(eng.kernel_ms())
@@ -396,6 +404,8 @@ def run_ours(args, rank, world):
         t0 = time.perf_counter()
         eng.mark(4)
         eng.upload_grid()
+        if diffusion:
+            eng.setdiffus(it)
         eng.reset_tallies()
         eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
         reduce_ranks(eng)
@@ -406,6 +416,9 @@ def run_ours(args, rank, world):
         e2e_steps.append(max(eng.elapsed_ms(4, 5), (time.perf_counter() - t0) * 1e3))
     e2e_ms = sum(e2e_steps) / len(e2e_steps)
     d2h = sum(a.nbytes for a in tl.arrays.values()) + td.nbytes
+    if diffusion:   # setdiffus: tdave up, the packed flags (int32 per cell) down
+        h2d += eng.tdave.nbytes
+        d2h += 4 * eng.tdave.size
     e2e_ms = float(allreduce(np.array([e2e_ms]), "max")[0])
     e2e = np_total / (e2e_ms / 1e3)
 

@@ -421,6 +421,26 @@ int mcrt_set_adjoint_baseline(mcrt_ctx *ctx, int32_t nfb, int32_t ndir, int64_t 
  * counts, as each MPI rank heats a private copy in the reference. */
 int mcrt_refresh_diffusion(mcrt_ctx *ctx);
 
+/* The diffusion region of the next iteration: setdiffus(iter)
+ * (setdiffus_5.f90:1-132, called from gridset_5_model13new.f90:1842 at the
+ * start of every iteration) followed by gridset's temperature reset
+ * (gridset_5_model13new.f90:1855-1866), on the device.  For each radius from
+ * the dust radius out to rmaxd [R*], each theta cell of the upper hemisphere
+ * marches toward the pole summing kappav*R* x chiR(tdave) x rho x dtheta x r
+ * over its thermal components (tdave floored at 50 K when iter < 2); a cell
+ * whose march reaches tau = 1 within h/20 (hdisk) of photon path starts a
+ * diffusion run down to the midplane (diffdir -2), mirrored below it (+2) and
+ * copied to every phi slice.  massd <= 0 (no disk) clears the region.  The
+ * context's cell flags and start-of-iteration tdust are rewritten (tdust =
+ * tdave, 0.1 K in diffusion and empty cells) for the next mcrt_run_iteration.
+ * Needs mcrt_grid.hdisk and mcrt_tables.kappar.  tdave [nrg,ntg,npg] (every
+ * entry positive) is read; diffus, diffdir [nrg,ntg,npg] and dcount (the
+ * reference's count of diffusion cells) may be NULL.  Cells without a thermal
+ * component are never flagged (diffusion emission needs a temperature). */
+int mcrt_setdiffus(mcrt_ctx *ctx, int32_t iter, double massd, double rmaxd,
+                   const double *tdave, int32_t *diffus, int32_t *diffdir,
+                   int64_t *dcount);
+
 /* Lucy temperature update on the device: tfinal(nphot,iter,converge)
  * (tfinal_5_test1.f90:1-447) with dusttemp (dusttemp_5.f90:8-152).
  * tdave [nrg,ntg,npg] is read (previous iteration) and overwritten.

@@ -2195,6 +2195,93 @@ int oracle_tfinal(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t
   return MCRT_OK;
 }
 
+// setdiffus (setdiffus_5.f90:1-132) as the reference writes it: clear the
+// flags; for ir from nr0 while rarr(ir) < rmaxd (and ir <= nrg-1), for it =
+// (ntg-1)/2 down to 2, march toward the pole over slice 1 summing
+// kapd(V) x chiR(tt) x densarr x dtheta x rad of the thermal components
+// (tt = tdave, floored at 50 K when iter < 2) until tau reaches 1; if
+// tau >= 1 and the path to tau = 1 is below hdisk/20, flag it..(ntg-1)/2
+// with diffdir -2.  Mirror into the lower hemisphere (diffdir +2), copy slice
+// 1 to the other phi slices, then gridset's reset (gridset_5_model13new.f90:
+// 1855-1866): tdust = tdave, 0.1 K in diffusion cells and in empty cells.
+// kapd holds kappav x R* (setup_wave.f90:50).  chiR (dust_5.f90:112-141)
+// clamps an index outside the table to its end intervals where the
+// reference stops.  Cells without a thermal component are left unflagged.
+int oracle_setdiffus(const mcrt_config* c, const mcrt_grid* g, const mcrt_tables* t, int32_t iter, double massd,
+                     double rmaxd, const double* tdave, int32_t* diffus, int32_t* diffdir, double* tdust) {
+  const int nrg = c->nrg, ntg = c->ntg, npg = c->npg, nT = c->nT;
+  const int64_t ncell = (int64_t)nrg * ntg * npg;
+  auto ci = [&](int ir, int it, int ip) { return (int64_t)(ir - 1) + (int64_t)nrg * ((it - 1) + (int64_t)ntg * (ip - 1)); };
+  auto dens = [&](int ir, int it, int ip, int id) { return g->densarr[ci(ir, it, ip) + ncell * (id - 1)]; };
+  auto fop = [&](int ir, int it, int ip, int id) { return g->findopac[ci(ir, it, ip) + ncell * (id - 1)]; };
+  const bool thermal[MCRT_NDG2] = {true, true, true, true, false, false, false, false, true, true};
+  auto chiR = [&](double T, int sp) {
+    const double lT = std::log(T);
+    int k = (int)((double)(nT - 1) * (lT - t->lTint[0]) / (t->lTint[nT - 1] - t->lTint[0])) + 1;
+    k = std::min(std::max(k, 1), nT - 1);
+    const double f = (lT - t->lTint[k - 1]) / (t->lTint[k] - t->lTint[k - 1]);
+    const double* kr = t->kappar + (int64_t)nT * (sp - 1);
+    return (1.0 - f) * kr[k - 1] + f * kr[k];
+  };
+  const double rmincgs = c->rstar * 6.9598e10;
+  std::fill(diffus, diffus + ncell, 0);
+  std::fill(diffdir, diffdir + ncell, 0);
+  if (massd > 0.0) {
+    const int nr0 = (c->rddust == g->rarr[0]) ? 1 : 3;
+    int ir = nr0;
+    double rad = g->rarr[ir - 1];
+    while (rad < rmaxd && ir <= nrg - 1) {
+      const double zmr = g->hdisk[ir - 1];
+      for (int it = (ntg - 1) / 2; it >= 2; --it) {
+        double tau = 0.0, tau1 = 0.0;
+        int itt = it;
+        while (tau < 1.0 && itt > 1) {
+          const double dt = g->thetarr[itt] - g->thetarr[itt - 1];
+          tau1 = tau;
+          double tt = tdave[ci(ir, itt, 1)];
+          if (iter < 2) tt = std::max(tt, 50.0 / 11605.0);
+          for (int id = 1; id <= MCRT_NDG2; ++id) {
+            if (!thermal[id - 1] || !(dens(ir, itt, 1, id) > 0.0)) continue;
+            const int sp = fop(ir, itt, 1, id);
+            tau = tau + (t->kappav[sp - 1] * rmincgs) * chiR(tt, sp) * dens(ir, itt, 1, id) * dt * rad;
+          }
+          itt = itt - 1;
+        }
+        double lmfp1;
+        if (tau > 1.0) lmfp1 = rad * (g->thetarr[itt + 1] - g->thetarr[itt]) / (tau - tau1) * (1.0 - tau1);
+        else lmfp1 = rad * (g->thetarr[itt + 1] - g->thetarr[itt]);
+        const double lmfp = rad * (g->thetarr[it] - g->thetarr[itt + 1]) + lmfp1;
+        if (tau >= 1.0 && lmfp < zmr / 20.0)
+          for (int it1 = it; it1 <= (ntg - 1) / 2; ++it1) { diffus[ci(ir, it1, 1)] = 1; diffdir[ci(ir, it1, 1)] = -2; }
+      }
+      ir = ir + 1;
+      rad = g->rarr[ir - 1];
+    }
+    for (int ir2 = 1; ir2 <= nrg - 1; ++ir2)
+      for (int it = (ntg + 1) / 2; it <= ntg - 1; ++it) {
+        diffus[ci(ir2, it, 1)] = diffus[ci(ir2, ntg - it, 1)];
+        diffdir[ci(ir2, it, 1)] = -diffdir[ci(ir2, ntg - it, 1)];
+      }
+    if (npg > 2)
+      for (int ir2 = 1; ir2 <= nrg - 1; ++ir2)
+        for (int it = 1; it <= ntg - 1; ++it)
+          for (int ip = 2; ip <= npg - 1; ++ip) {
+            diffus[ci(ir2, it, ip)] = diffus[ci(ir2, it, 1)];
+            diffdir[ci(ir2, it, ip)] = diffdir[ci(ir2, it, 1)];
+          }
+  }
+  for (int64_t k = 0; k < ncell; ++k) {
+    bool th = false, any = false;
+    for (int id = 1; id <= MCRT_NDG2; ++id) {
+      const double rho = g->densarr[k + ncell * (id - 1)];
+      if (rho > 0.0) { any = true; if (thermal[id - 1]) th = true; }
+    }
+    if (!th) { diffus[k] = 0; diffdir[k] = 0; }
+    tdust[k] = (diffus[k] || !any) ? 0.1 / 11605.0 : tdave[k];
+  }
+  return 0;
+}
+
 }  // extern "C"
 
 

@@ -92,6 +92,10 @@ def load():
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int32, C.c_int32,
                                       C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.oracle_tfinal.restype = C.c_int
+        lib.oracle_setdiffus.argtypes = [C.POINTER(abi.Config), C.POINTER(abi.Grid), C.POINTER(abi.Tables),
+                                         C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        lib.oracle_setdiffus.restype = C.c_int
         D = C.POINTER(C.c_double)
         lib.oracle_setemiss.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32), D, D, D, C.c_int32,
                                         C.c_int32, D, D, D, D, D, D, C.POINTER(C.c_int64), C.c_int32]
@@ -150,6 +154,25 @@ def tfinal(bundle: abi.Bundle, dtauabs: np.ndarray, nphot: int, iteration: int, 
     if rc != 0:
         raise RuntimeError(f"oracle_tfinal failed with code {rc}")
     return td, sig
+
+
+def setdiffus(bundle: abi.Bundle, iteration: int, massd: float, rmaxd: float, tdave: np.ndarray):
+    """setdiffus (setdiffus_5.f90:1-132) and gridset's tdust reset
+    (gridset_5_model13new.f90:1855-1866): returns (diffus, diffdir, tdust),
+    Fortran-order flat arrays."""
+    lib = load()
+    td = np.ascontiguousarray(tdave, dtype=np.float64)
+    n = td.size
+    dif = np.zeros(n, np.int32)
+    ddir = np.zeros(n, np.int32)
+    tdust = np.zeros(n, np.float64)
+    I = C.POINTER(C.c_int32)
+    rc = lib.oracle_setdiffus(C.byref(bundle.config), C.byref(bundle.grid), C.byref(bundle.tables), iteration,
+                              float(massd), float(rmaxd), td.ctypes.data_as(C.POINTER(C.c_double)),
+                              dif.ctypes.data_as(I), ddir.ctypes.data_as(I), tdust.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(f"oracle_setdiffus failed with code {rc}")
+    return dif, ddir, tdust
 
 
 def adjoint(bundle: abi.Bundle, np_total: int, lam_psed: np.ndarray, lam_img: np.ndarray | None = None,

@@ -164,6 +164,10 @@ struct mcrt_ctx {
   cudaEvent_t marks[16] = {};
   void *d_flush = nullptr;
   int64_t off_Tint = 0, off_kappap = 0;   // offsets of Tint/kappap in d_tabs (tfinal)
+  int64_t off_kappar = -1;              // offset of kappar in d_tabs (setdiffus), -1 when not uploaded
+  double *d_sd_tdave = nullptr;         // setdiffus: [ncell] tdave, [nrg*ntg] marks, [ncell] flags out
+  uint8_t *d_sd_mark = nullptr;
+  int32_t *d_sd_out = nullptr;
   std::vector<double> h_rarr;
   std::vector<int32_t> species_grid;  // per species: first species with a bit-identical wavelength column
   double* noalloc_scratch = nullptr;   // device address of g_tfinal_scratch (mcrt_update_temperature_noalloc)
@@ -538,6 +542,107 @@ __global__ void tdust_from_tdave(int64_t n, const double* tdave, const int32_t* 
     double t = diffus[k] ? 0.1 / 11605.0 : tdave[k];
     if (cell_n(cells[k].meta) == 0) t = 0.1 / 11605.0;
     tdust[k] = t;
+  }
+}
+
+// ---- setdiffus (setdiffus_5.f90:1-132) -------------------------------------
+struct SetdiffusArgs {
+  int nrg, ntg, npg, nT, iter;
+  int nr0, nr1;                 // radii ir = nr0..nr1 are marched (rarr(ir) < rmaxd, ir <= nrg-1)
+  double rmincgs;
+  const double *rarr, *thetarr, *hdisk, *kappav, *kappar, *lTint;
+  const double* tdave;          // [ncell] temperature of the last tfinal
+  const CellRec* cells;
+  uint8_t* mark;                // [nrg*ntg] theta cell it of radius ir starts a diffusion run
+};
+
+// chiR (dust_5.f90:112-141): the Rosseland table of species sp interpolated
+// in log T; an index outside the table is clamped to its end intervals.
+__device__ double chiR_dev(const double* lTint, const double* kappar, int nT, double T, int sp) {
+  const double lT = log(T);
+  int k = (int)__ddiv_rn(__dmul_rn((double)(nT - 1), __dsub_rn(lT, lTint[0])), __dsub_rn(lTint[nT - 1], lTint[0])) + 1;
+  k = min(max(k, 1), nT - 1);
+  const double f = __ddiv_rn(__dsub_rn(lT, lTint[k - 1]), __dsub_rn(lTint[k], lTint[k - 1]));
+  const double* kr = kappar + (int64_t)nT * (sp - 1);
+  return __dadd_rn(__dmul_rn(__dsub_rn(1.0, f), kr[k - 1]), __dmul_rn(f, kr[k]));
+}
+
+// One thread per (ir, it) of the upper hemisphere: the march toward the
+// pole (setdiffus_5.f90:57-94) that sums the Rosseland optical depth of the
+// thermal components of slice ip = 1 until it reaches 1, then the mean-free
+// path test against h/20.  mark = 1 where cell it starts a diffusion run.
+__global__ void setdiffus_mark(SetdiffusArgs a) {
+  const int nt = (a.ntg - 1) / 2 - 1;          // it = 2..(ntg-1)/2
+  const int64_t n = (int64_t)(a.nr1 - a.nr0 + 1) * (nt > 0 ? nt : 0);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = a.nr0 + (int)(q / nt);
+    const int it = 2 + (int)(q % nt);
+    const double rad = a.rarr[ir - 1];
+    const double zmr = a.hdisk[ir - 1];
+    double tau = 0.0, tau1 = 0.0;
+    int itt = it;
+    while (tau < 1.0 && itt > 1) {
+      const double dt = __dsub_rn(a.thetarr[itt], a.thetarr[itt - 1]);
+      tau1 = tau;
+      const int64_t c = (ir - 1) + (int64_t)a.nrg * (itt - 1);
+      double tt = a.tdave[c];
+      if (a.iter < 2) tt = fmax(tt, 50.0 / 11605.0);
+      const CellRec r = a.cells[c];
+      for (int k = 0; k < cell_n(r.meta); ++k) {
+        const int id = cell_id(r.meta, k);      // findopac(.,id) = id
+        if ((id >= 5 && id <= 8) || !(r.rho[k] > 0.0)) continue;   // small grains are not thermal
+        double t = __dmul_rn(a.kappav[id - 1], a.rmincgs);
+        t = __dmul_rn(t, chiR_dev(a.lTint, a.kappar, a.nT, tt, id));
+        t = __dmul_rn(__dmul_rn(__dmul_rn(t, r.rho[k]), dt), rad);
+        tau = __dadd_rn(tau, t);
+      }
+      itt = itt - 1;
+    }
+    double lmfp1;
+    if (tau > 1.0)
+      lmfp1 = __dmul_rn(__ddiv_rn(__dmul_rn(rad, __dsub_rn(a.thetarr[itt + 1], a.thetarr[itt])), __dsub_rn(tau, tau1)),
+                        __dsub_rn(1.0, tau1));
+    else
+      lmfp1 = __dmul_rn(rad, __dsub_rn(a.thetarr[itt + 1], a.thetarr[itt]));
+    const double lmfp = __dadd_rn(__dmul_rn(rad, __dsub_rn(a.thetarr[it], a.thetarr[itt + 1])), lmfp1);
+    a.mark[(ir - 1) + (int64_t)a.nrg * (it - 1)] = (tau >= 1.0 && lmfp < zmr / 20.0) ? 1 : 0;
+  }
+}
+
+// One thread per cell: a marked cell flags itself and every cell between it
+// and the midplane (setdiffus_5.f90:96-101, diffdir -2), the lower
+// hemisphere mirrors the upper one with diffdir +2 (:106-111), slice 1 is
+// copied to every phi slice (:113-121); cells without a thermal component
+// stay off (they have no temperature to diffuse).  Then gridset's reset
+// (gridset_5_model13new.f90:1855-1866): tdust = tdave, 0.1 K in diffusion
+// cells and in empty cells.  The cell records' flag bits, the flag array and
+// both tdust copies are rewritten; out (optional) receives diffus | diffdir << 8.
+__global__ void setdiffus_apply(SetdiffusArgs a, int massd_pos, CellRec* cells, int32_t* diffus, double* tdust,
+                                double* tdust0, int32_t* out) {
+  const int64_t n = (int64_t)a.nrg * a.ntg * a.npg;
+  const int half = (a.ntg - 1) / 2;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int ir = (int)(k % a.nrg) + 1;
+    const int it = (int)((k / a.nrg) % a.ntg) + 1;
+    const int ip = (int)(k / ((int64_t)a.nrg * a.ntg)) + 1;
+    int on = 0, dd = 0;
+    if (massd_pos && ir <= a.nrg - 1 && it <= a.ntg - 1 && ip <= (a.npg > 2 ? a.npg - 1 : 1)) {
+      int src = it, sgn = -2;
+      if (it >= (a.ntg + 1) / 2) { src = a.ntg - it; sgn = 2; }
+      if (src >= 2 && src <= half)
+        for (int j = 2; j <= src && !on; ++j) on = a.mark[(ir - 1) + (int64_t)a.nrg * (j - 1)];
+      dd = on ? sgn : 0;
+    }
+    CellRec r = cells[k];
+    if (!cell_thermal(r.flags)) { on = 0; dd = 0; }
+    r.flags = (r.flags & ~31u) | (uint32_t)on | ((uint32_t)(dd + 8) << 1);
+    cells[k].flags = r.flags;
+    diffus[k] = on;
+    double t = on ? 0.1 / 11605.0 : a.tdave[k];
+    if (cell_n(r.meta) == 0) t = 0.1 / 11605.0;
+    tdust[k] = t;
+    tdust0[k] = t;
+    if (out) out[k] = on | (dd << 8);
   }
 }
 
@@ -1188,6 +1293,9 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   add(c.npeel ? t->coste_arr : pz.data(), np); add(c.npeel ? t->sinte_arr : pz.data(), np);            // 18-19
   add(c.npeel ? t->cospe_arr : pz.data(), np); add(c.npeel ? t->sinpe_arr : pz.data(), np);            // 20-21
   add(t->Tint, c.nT); add(t->kappap, (int64_t)c.nT * c.nopac);                                          // 22-23
+  // Rosseland table (setdiffus), optional
+  const int kappar_at = t->kappar ? (int)off.size() : -1;
+  if (t->kappar) add(t->kappar, (int64_t)c.nT * c.nopac);
   // tabulated scattering matrices: the table and, per (species, wavelength)
   // row, the rejection bound max(S11 + |S12|) over the cosine bins, which
   // bounds the sampling probability (S11 I + S12 (cos2i Q +- sin2i U)) / I
@@ -1303,6 +1411,7 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   ctx->have_tables = true;
   ctx->off_Tint = off[22];
   ctx->off_kappap = off[23];
+  ctx->off_kappar = kappar_at >= 0 ? off[kappar_at] : -1;
   return MCRT_OK;
 }
 
@@ -2229,6 +2338,59 @@ int mcrt_refresh_diffusion(mcrt_ctx* ctx) {
                                             std::max(ctx->last_ns, 1.0), ctx->stream);
   if (e != cudaSuccess) return fail(ctx, MCRT_ERR_CUDA, "diffusion refresh: %s", cudaGetErrorString(e));
   CK(cudaStreamSynchronize(ctx->stream));
+  return MCRT_OK;
+}
+
+int mcrt_setdiffus(mcrt_ctx* ctx, int32_t iter, double massd, double rmaxd, const double* tdave, int32_t* diffus,
+                   int32_t* diffdir, int64_t* dcount) {
+  if (!ctx || !tdave) return MCRT_ERR_ARG;
+  if (!ctx->have_grid || !ctx->have_tables) return fail(ctx, MCRT_ERR_STATE, "upload the grid and tables first");
+  if (!ctx->have_acc) return fail(ctx, MCRT_ERR_STATE, "mcrt_setdiffus needs the disk scale heights (mcrt_grid.hdisk)");
+  if (ctx->off_kappar < 0) return fail(ctx, MCRT_ERR_STATE, "mcrt_setdiffus needs the Rosseland table (mcrt_tables.kappar)");
+  if (!std::isfinite(massd) || !std::isfinite(rmaxd)) return fail(ctx, MCRT_ERR_ARG, "massd and rmaxd must be finite");
+  const mcrt_config& c = ctx->cfg;
+  const int64_t nc = ctx->ncell;
+  for (int64_t k = 0; k < nc; ++k)
+    if (!(tdave[k] > 0.0) || !std::isfinite(tdave[k]))
+      return fail(ctx, MCRT_ERR_ARG, "tdave(%lld) = %g is not a positive temperature", (long long)k + 1, tdave[k]);
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if (!ctx->d_sd_tdave) {
+    if ((rc = dalloc(ctx, &ctx->d_sd_tdave, nc))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_sd_mark, (size_t)c.nrg * c.ntg))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_sd_out, nc))) return rc;
+  }
+  SetdiffusArgs a{};
+  a.nrg = c.nrg; a.ntg = c.ntg; a.npg = c.npg; a.nT = c.nT; a.iter = iter;
+  // the march starts at the first dust cell, or two cells further out when
+  // the grid starts at the star rather than at the dust radius (setdiffus_5.f90:44-48)
+  a.nr0 = (c.rddust == ctx->h_rarr[0]) ? 1 : 3;
+  int ir = a.nr0;
+  while (ir <= c.nrg - 1 && ctx->h_rarr[ir - 1] < rmaxd) ++ir;
+  a.nr1 = ir - 1;
+  a.rmincgs = c.rstar * 6.9598e10;
+  a.rarr = ctx->dm.rarr; a.thetarr = ctx->dm.thetarr; a.hdisk = ctx->dm.hdisk;
+  a.kappav = ctx->dm.kappav; a.kappar = ctx->d_tabs + ctx->off_kappar; a.lTint = ctx->dm.lTint;
+  a.tdave = ctx->d_sd_tdave; a.cells = ctx->d_cells; a.mark = ctx->d_sd_mark;
+  CK(cudaMemcpyAsync(ctx->d_sd_tdave, tdave, nc * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_sd_mark, 0, (size_t)c.nrg * c.ntg, ctx->stream));
+  const bool disk = massd > 0.0;
+  if (disk && a.nr1 >= a.nr0 && (c.ntg - 1) / 2 >= 2) setdiffus_mark<<<148, 128, 0, ctx->stream>>>(a);
+  setdiffus_apply<<<512, 256, 0, ctx->stream>>>(a, disk ? 1 : 0, ctx->d_cells, ctx->d_diffus, ctx->d_tdust,
+                                                ctx->d_tdust0, ctx->d_sd_out);
+  CK(cudaGetLastError());
+  std::vector<int32_t> out(nc);
+  CK(cudaMemcpyAsync(out.data(), ctx->d_sd_out, nc * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  int64_t cnt = 0;
+  for (int64_t k = 0; k < nc; ++k) {
+    const int on = out[k] & 1;
+    ctx->h_diffus[k] = on;
+    cnt += on;
+    if (diffus) diffus[k] = on;
+    if (diffdir) diffdir[k] = out[k] >> 8;
+  }
+  if (dcount) *dcount = cnt;
   return MCRT_OK;
 }
 

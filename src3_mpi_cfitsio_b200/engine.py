@@ -69,6 +69,8 @@ def load_library(path: str = LIB_PATH):
     lib.mcrt_wave_stats.argtypes = [C.c_void_p, P(C.c_double), P(C.c_int64)]
     lib.mcrt_device_tallies_view.argtypes = [C.c_void_p, P(abi.DeviceTallies)]
     lib.mcrt_refresh_diffusion.argtypes = [C.c_void_p]
+    lib.mcrt_setdiffus.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, P(C.c_double), P(C.c_int32),
+                                   P(C.c_int32), P(C.c_int64)]
     D = P(C.c_double)
     lib.mcrt_adjoint.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
                                  C.c_int32, D, D, D, D]
@@ -105,7 +107,7 @@ def load_library(path: str = LIB_PATH):
                  "mcrt_set_wave_pool", "mcrt_reset_tallies", "mcrt_run_iteration", "mcrt_download_tallies",
                  "mcrt_accumulate_tallies", "mcrt_update_temperature", "mcrt_enable_packet_log",
                  "mcrt_download_packet_log", "mcrt_last_kernel_ms", "mcrt_wave_stats", "mcrt_mark", "mcrt_elapsed_ms",
-                 "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_adjoint",
+                 "mcrt_device_tallies_view", "mcrt_refresh_diffusion", "mcrt_setdiffus", "mcrt_adjoint",
                  "mcrt_flush_l2", "mcrt_synchronize", "mcrt_batch_create", "mcrt_batch_run_iteration",
                  "mcrt_batch_tune", "mcrt_batch_set_schedule", "mcrt_batch_set_tuning", "mcrt_batch_last_ms",
                  "mcrt_setemiss", "mcrt_set_adjoint_chunk", "mcrt_set_adjoint_baseline", "mcrt_set_wave_loop", "mcrt_model_density"):
@@ -383,6 +385,24 @@ class Engine:
         """Diffusion-cell temperatures of the last run from the (reduced) counts."""
         self._check(self.lib.mcrt_refresh_diffusion(self.ctx))
 
+    def setdiffus(self, iteration: int, tdave=None):
+        """setdiffus(iter) and gridset's tdust reset on the device
+        (mcrt_setdiffus), from ``tdave`` (default: the engine's current
+        temperature); returns (diffus, diffdir, dcount) as Fortran-order
+        flat arrays.  The disk mass and outer radius come from the model."""
+        w = self.model.w
+        td = np.ascontiguousarray(self.tdave if tdave is None else tdave, dtype=np.float64)
+        n = td.size
+        dif = np.zeros(n, np.int32)
+        ddir = np.zeros(n, np.int32)
+        cnt = C.c_int64(0)
+        I = C.POINTER(C.c_int32)
+        self._check(self.lib.mcrt_setdiffus(self.ctx, iteration, float(w.massd),
+                                            float(w.rmaxd_au * self.model.config["autors"]),
+                                            td.ctypes.data_as(C.POINTER(C.c_double)), dif.ctypes.data_as(I),
+                                            ddir.ctypes.data_as(I), C.byref(cnt)))
+        return dif, ddir, int(cnt.value)
+
     def enable_packet_log(self, n: int):
         self._check(self.lib.mcrt_enable_packet_log(self.ctx, n))
 
@@ -409,8 +429,13 @@ class Engine:
 
         Runs np_total packets (the packet loop), leaves the reduced tallies in
         ``self.tallies`` and updates the temperature with ``tfinal``;
-        returns the new ``converge`` ('yes'/'no').
+        returns the new ``converge`` ('yes'/'no').  A model with the
+        diffusion treatment first recomputes its diffusion region from the
+        current temperature, as gridset does every iteration
+        (gridset_5_model13new.f90:1842-1866, ``setdiffus``).
         """
+        if self.model.config.get("diffusion") and iteration >= 1:
+            self.setdiffus(iteration)
         self.reset_tallies()
         self.run(np_total, iteration=iteration, ipeel=ipeel, seeds=(12345678 - i1 if i1 else 12345678, 87654321),
                  generator=generator)

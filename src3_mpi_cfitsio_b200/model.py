@@ -667,6 +667,7 @@ def setdiffus(m: Model, tdave: np.ndarray, iteration: int) -> Model:
     T = np.where(diffus > 0, 0.1 / 11605.0, td)
     T = np.where(dens.sum(axis=-1) > 0, T, 0.1 / 11605.0)
     m.grid["tdust"] = np.asfortranarray(T).ravel(order="F")
+    m.config["diffusion"] = True      # gridset reruns setdiffus every iteration (mctherm.par DIFFUSION)
     return m
 
 
