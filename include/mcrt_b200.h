@@ -57,7 +57,7 @@ extern "C" {
 
 /* ---- arithmetic of the transport kernels ---- */
 #define MCRT_PREC_FP64   0   /* everything in FP64 (event-for-event with the oracle) */
-#define MCRT_PREC_MIXED  1   /* FP32 scattering; FP64 division-free walk, tau sums, tallies */
+#define MCRT_PREC_MIXED  1   /* FP32 walk and scattering; FP64 sphere roots, tau sums, tallies */
 
 /*
  * Run configuration: the scalars of tts_mod/grid_mod/dust_mod/spot_mod that
@@ -99,6 +99,11 @@ typedef struct mcrt_config {
   double cspot1, sspot1, scspot1, ssspot1;
   double cspot2, sspot2, scspot2, ssspot2;
   double csprad;
+  /* Filter-band images (output_imfilt, peeloff_3d_2_test.f90:245-285): the
+   * number of filter curves nfilt (the reference's nbnd, tts_mod_5.f90:62)
+   * and the leading dimension nwfiltmax of mcrt_tables.filtwave/filtphi
+   * (filt_mod.f90:10-14).  output_imfilt = 0 leaves the images off. */
+  int32_t output_imfilt, nfilt, nwfiltmax, pad_filt;
 } mcrt_config;
 
 /*
@@ -177,6 +182,13 @@ typedef struct mcrt_tables {
    * when the model has no small grains. */
   const double  *draine;
   int32_t        nemit, ndraine;
+  /* Filter curves of the filter-band images (filt_mod.f90, read by
+   * filt_nu.f90), needed when output_imfilt = 1: filtwave(nwfiltmax,nfilt)
+   * frequencies in Hz, ascending within each curve, filtphi(nwfiltmax,nfilt)
+   * the normalised responses, and nwfilt(nfilt) the reference's line counts
+   * (a curve uses its first nwfilt-1 points, filt_nu.f90:30). */
+  const int32_t *nwfilt;
+  const double  *filtwave, *filtphi;
 } mcrt_tables;
 
 /*
@@ -191,6 +203,11 @@ typedef struct mcrt_tallies {
   float   *image_m_i, *image_m_q, *image_m_u, *image_m_v;             /* [npeel,nxhst,nxhst,nfreq] */
   double  *scalars;   /* [MCRT_NSCALARS], see MCRT_S_* below                 */
   int64_t *counters;  /* [MCRT_NCOUNTERS], see MCRT_C_* below                */
+  /* Filter-band images (output_imfilt = 1): Stokes I, Q, U, V and Stokes I
+   * by origin (d disk, s star, e envelope, o outflow: i_orig 2, 1, 3, 4),
+   * tts_mod_5.f90:67-68 */
+  float   *image_b_i, *image_b_q, *image_b_u, *image_b_v;             /* [npeel,nxhst,nxhst,nfilt] */
+  float   *image_b_d, *image_b_s, *image_b_e, *image_b_o;             /* [npeel,nxhst,nxhst,nfilt] */
 } mcrt_tallies;
 
 /* scalars[] of one iteration (the reference's module scalars) */

@@ -258,6 +258,7 @@ struct Tally {
 
 struct Images {       // shared across threads, atomic adds
   std::vector<double> im[4];
+  std::vector<double> imb[8];   // filter-band images: I Q U V, then I by origin d s e o
 };
 
 void atomic_add(double& x, double v) {
@@ -1310,6 +1311,35 @@ struct Packet {
         atomic_add(I->im[3][k], q_v);
       }
     }
+    // filter-band images (peeloff_3d_2_test.f90:242-285): freq = 2.9979e14/wave,
+    // wave = 1.2398/nub; a filter whose open range (filtwave(1), filtwave(nf))
+    // holds freq adds the Stokes vector times filtphi at the last point below
+    // freq, found by the reference's linear scan; I also goes to the image of
+    // the packet's origin (s star, d disk, e envelope, o outflow)
+    if (c.output_imfilt && !I->imb[0].empty() && vx > -1.0e9 && vx < 1.0e9 && vy > -1.0e9 && vy < 1.0e9) {
+      int ix = (int)vx + 1, iy = (int)vy + 1;
+      if (ix <= c.nxhst && iy <= c.nxhst && ix > 0 && iy > 0) {
+        const double wave = 1.2398 / nub;
+        const double freq = 2.9979e14 / wave;
+        for (int ifilt = 1; ifilt <= c.nfilt; ++ifilt) {
+          const int nf = t->nwfilt[ifilt - 1] - 1;
+          const double* fw = t->filtwave + (int64_t)c.nwfiltmax * (ifilt - 1);
+          if (freq > fw[0] && freq < fw[nf - 1]) {
+            int iw = 1;
+            while (freq > fw[iw - 1]) iw = iw + 1;
+            iw = iw - 1;
+            const double wt = t->filtphi[(int64_t)c.nwfiltmax * (ifilt - 1) + iw - 1];
+            const int64_t k = (int64_t)(peelid - 1) + (int64_t)c.npeel * ((ix - 1) + (int64_t)c.nxhst * ((iy - 1) + (int64_t)c.nxhst * (ifilt - 1)));
+            atomic_add(I->imb[0][k], q_i * wt);
+            atomic_add(I->imb[1][k], q_q * wt);
+            atomic_add(I->imb[2][k], q_u * wt);
+            atomic_add(I->imb[3][k], q_v * wt);
+            const int oi = i_orig == 1 ? 5 : (i_orig == 2 ? 4 : (i_orig == 3 ? 6 : (i_orig == 4 ? 7 : -1)));
+            if (oi >= 0) atomic_add(I->imb[oi][k], q_i * wt);
+          }
+        }
+      }
+    }
     int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
     int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= c.nap; ++ia) {
@@ -1866,6 +1896,9 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   const int64_t nimg = (int64_t)cfg->npeel * cfg->nxhst * cfg->nxhst * cfg->nfreq;
   Images img;
   for (auto& v : img.im) v.assign(cfg->output_imcube ? nimg : 0, 0.0);
+  const int64_t nimgb = (int64_t)cfg->npeel * cfg->nxhst * cfg->nxhst * cfg->nfilt;
+  if (cfg->output_imfilt && (cfg->nfilt < 1 || !tab->nwfilt || !tab->filtwave || !tab->filtphi)) return MCRT_ERR_ARG;
+  for (auto& v : img.imb) v.assign(cfg->output_imfilt ? nimgb : 0, 0.0);
   int nt = std::max(1, (int)nthreads);
   std::vector<Tally> tl(nt);
   for (auto& t : tl) t.init(m.ncell, nsed, npsed);
@@ -1924,6 +1957,9 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
     for (int k = 0; k < 9; ++k) put(pd[k], S.psed[k]);
     float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
     for (int k = 0; k < 4; ++k) put(im[k], img.im[k]);
+    float* ib[8] = {out->image_b_i, out->image_b_q, out->image_b_u, out->image_b_v,
+                    out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
+    for (int k = 0; k < 8; ++k) put(ib[k], img.imb[k]);
     if (out->scalars) for (int k = 0; k < MCRT_NSCALARS; ++k) out->scalars[k] = S.scal[k];
     if (out->counters) for (int k = 0; k < MCRT_NCOUNTERS; ++k) out->counters[k] = S.cnt[k];
   }

@@ -39,7 +39,7 @@ class Config(C.Structure):
         "rstar", "tstar", "tstarave", "tshock", "fspot", "accfrac", "accfrac2",
         "isrf_frac", "rddust", "rmaxi", "numin", "lnurat", "autors", "ifuv_ori",
         "cspot1", "sspot1", "scspot1", "ssspot1", "cspot2", "sspot2", "scspot2",
-        "ssspot2", "csprad")]
+        "ssspot2", "csprad")] + [(n, C.c_int32) for n in ("output_imfilt", "nfilt", "nwfiltmax", "pad_filt")]
 
 
 GRID_FIELDS = [("rarr", _dp), ("r2arr", _dp), ("thetarr", _dp), ("costarr", _dp),
@@ -62,7 +62,8 @@ TABLE_FIELDS = [("nlambda", _ip), ("nudust", _dp), ("kappad", _dp), ("adust", _d
                 ("sinte_arr", _dp), ("cospe_arr", _dp), ("sinpe_arr", _dp),
                 ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32),
                 ("isrf", _dp), ("nisrf", C.c_int32), ("pad_isrf", C.c_int32),
-                ("draine", _dp), ("nemit", C.c_int32), ("ndraine", C.c_int32)]
+                ("draine", _dp), ("nemit", C.c_int32), ("ndraine", C.c_int32),
+                ("nwfilt", _ip), ("filtwave", _dp), ("filtphi", _dp)]
 
 
 class Tables(C.Structure):
@@ -74,12 +75,14 @@ CELL_D = ["dtauabs", "fuvmean"]
 SED = ["si", "sq", "su", "sv", "si2", "sq2", "su2", "sv2", "nums", "aveinc"]
 PSED = ["ti", "tq", "tu", "tv", "ti2", "tq2", "tu2", "tv2", "numt"]
 IMG = ["image_m_i", "image_m_q", "image_m_u", "image_m_v"]
+IMGB = ["image_b_i", "image_b_q", "image_b_u", "image_b_v", "image_b_d", "image_b_s", "image_b_e", "image_b_o"]
 
 
 class Tallies(C.Structure):
     _fields_ = ([(n, _ip) for n in CELL_I] + [(n, _dp) for n in CELL_D] +
                 [(n, _fp) for n in SED] + [(n, _fp) for n in PSED] +
-                [(n, _fp) for n in IMG] + [("scalars", _dp), ("counters", _lp)])
+                [(n, _fp) for n in IMG] + [("scalars", _dp), ("counters", _lp)] +
+                [(n, _fp) for n in IMGB])
 
 
 class PacketLog(C.Structure):
@@ -163,6 +166,10 @@ class TallyArrays:
         if images and cfg.output_imcube:
             for n in IMG:
                 self.arrays[n] = np.zeros(nimg, np.float32)
+        if images and cfg.output_imfilt:
+            nimgb = cfg.npeel * cfg.nxhst * cfg.nxhst * cfg.nfilt
+            for n in IMGB:
+                self.arrays[n] = np.zeros(nimgb, np.float32)
         self.arrays["scalars"] = np.zeros(MCRT_NSCALARS, np.float64)
         self.arrays["counters"] = np.zeros(MCRT_NCOUNTERS, np.int64)
         t = Tallies()
@@ -204,6 +211,8 @@ class TallyArrays:
             return a.reshape((c.nfreq, c.npeel, c.nap, MCRT_NO), order="F")
         if name in IMG:
             return a.reshape((c.npeel, c.nxhst, c.nxhst, c.nfreq), order="F")
+        if name in IMGB:
+            return a.reshape((c.npeel, c.nxhst, c.nxhst, c.nfilt), order="F")
         return a
 
 

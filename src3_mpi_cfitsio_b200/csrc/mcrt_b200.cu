@@ -156,6 +156,10 @@ struct mcrt_ctx {
   unsigned long long *d_next = nullptr;    // [0] packets, [1] peel jobs, [2] peel items
   PeelJob *d_jobs = nullptr;
   int64_t job_cap = 0;
+  double *d_job_nub = nullptr;        // [job_cap] packet frequency per job (filter-band images)
+  int64_t job_nub_cap = 0;
+  int64_t nimgb = 0;                  // filter-band image size (0: off)
+  int32_t *d_nfpts = nullptr;         // [nfilt] points per filter curve
   int64_t chunk_packets = 1 << 20;
   int32_t *d_err = nullptr;
   mcrt_packet_log *d_log = nullptr;
@@ -918,9 +922,15 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   ctx->nsed = (int64_t)c.nfreq * c.nmu * c.nph * c.nap * MCRT_NO;
   ctx->npsed = (int64_t)c.nfreq * c.npeel * c.nap * MCRT_NO;
   ctx->nimg = c.output_imcube ? (int64_t)c.npeel * c.nxhst * c.nxhst * c.nfreq : 0;
-  // one tally allocation: cell ints, cell doubles, SED, peeled SED, images, scalars, counters
+  if (c.output_imfilt && (c.nfilt < 1 || c.nfilt > 4096 || c.nwfiltmax < 2)) {
+    *out = ctx;
+    return fail(ctx, MCRT_ERR_ARG, "output_imfilt needs 1 <= nfilt <= 4096 and nwfiltmax >= 2");
+  }
+  ctx->nimgb = c.output_imfilt ? (int64_t)c.npeel * c.nxhst * c.nxhst * c.nfilt : 0;
+  // one tally allocation: cell ints, cell doubles, SED, peeled SED, images,
+  // filter-band images, scalars, counters
   const int64_t n_int = 5 * ctx->ncell;
-  const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + MCRT_NSCALARS;
+  const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + MCRT_NSCALARS;
   ctx->tally_bytes = (size_t)n_dbl * 8 + (size_t)MCRT_NCOUNTERS * 8 + (size_t)((n_int * 4 + 7) / 8) * 8;
   int rc = dalloc(ctx, (char**)&ctx->d_tally, ctx->tally_bytes);
   if (rc) { *out = ctx; return rc; }
@@ -932,6 +942,7 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   t.sed = d; d += 10 * ctx->nsed;
   t.psed = d; d += 9 * ctx->npsed;
   t.img = d; d += 4 * ctx->nimg;
+  t.imgb = d; d += 8 * ctx->nimgb;
   t.scal = d; d += MCRT_NSCALARS;
   t.cnt = (unsigned long long*)d;
   int32_t* ip = (int32_t*)(t.cnt + MCRT_NCOUNTERS);
@@ -1293,9 +1304,6 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   add(c.npeel ? t->coste_arr : pz.data(), np); add(c.npeel ? t->sinte_arr : pz.data(), np);            // 18-19
   add(c.npeel ? t->cospe_arr : pz.data(), np); add(c.npeel ? t->sinpe_arr : pz.data(), np);            // 20-21
   add(t->Tint, c.nT); add(t->kappap, (int64_t)c.nT * c.nopac);                                          // 22-23
-  // Rosseland table (setdiffus), optional
-  const int kappar_at = t->kappar ? (int)off.size() : -1;
-  if (t->kappar) add(t->kappar, (int64_t)c.nT * c.nopac);
   // tabulated scattering matrices: the table and, per (species, wavelength)
   // row, the rejection bound max(S11 + |S12|) over the cosine bins, which
   // bounds the sampling probability (S11 I + S12 (cos2i Q +- sin2i U)) / I
@@ -1338,6 +1346,30 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
       if (!std::isfinite(t->draine[i])) return fail(ctx, MCRT_ERR_ARG, "draine table entry %lld is not finite", (long long)i);
     add(t->draine, nn);
   }
+  // filter curves of the filter-band images (filt_nu.f90): filtwave and
+  // filtphi per filter over nwfiltmax points, of which nwfilt-1 are used
+  const bool filt = c.output_imfilt && t->nwfilt && t->filtwave && t->filtphi;
+  if (c.output_imfilt && !filt) return fail(ctx, MCRT_ERR_ARG, "output_imfilt needs nwfilt, filtwave and filtphi");
+  const int filt_at = filt ? (int)off.size() : -1;
+  std::vector<int32_t> nfpts;
+  if (filt) {
+    for (int f = 0; f < c.nfilt; ++f) {
+      const int nf = t->nwfilt[f] - 1;
+      if (nf < 1 || nf > c.nwfiltmax) return fail(ctx, MCRT_ERR_ARG, "nwfilt(%d) = %d: a curve needs 1..nwfiltmax points", f + 1, t->nwfilt[f]);
+      const double* fw = t->filtwave + (int64_t)c.nwfiltmax * f;
+      const double* fp = t->filtphi + (int64_t)c.nwfiltmax * f;
+      for (int i = 0; i < nf; ++i) {
+        if (!std::isfinite(fw[i]) || !std::isfinite(fp[i])) return fail(ctx, MCRT_ERR_ARG, "filter %d holds a non-finite value", f + 1);
+        if (i > 0 && fw[i] < fw[i - 1]) return fail(ctx, MCRT_ERR_ARG, "filtwave of filter %d must be non-decreasing in frequency", f + 1);
+      }
+      nfpts.push_back(nf);
+    }
+    add(t->filtwave, (int64_t)c.nwfiltmax * c.nfilt);
+    add(t->filtphi, (int64_t)c.nwfiltmax * c.nfilt);
+  }
+  // Rosseland table (setdiffus), optional; after the blocks read by fixed index
+  const int kappar_at = t->kappar ? (int)off.size() : -1;
+  if (t->kappar) add(t->kappar, (int64_t)c.nT * c.nopac);
   // jump tables a^(2^30 * 2^k)
   std::vector<int64_t> jump(128);
   int64_t j1 = 1033780774, j2 = 1494757890;   // a1w, a2w (ecuyer_cote_mod.f90:14-15)
@@ -1362,6 +1394,11 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   }
   int rc;
   if (ctx->have_tables) { dfree(ctx, ctx->d_tabs); dfree(ctx, ctx->d_nlambda); dfree(ctx, ctx->d_jump); }
+  if (ctx->d_nfpts) { dfree(ctx, ctx->d_nfpts); ctx->d_nfpts = nullptr; }
+  if (filt) {
+    if ((rc = dalloc(ctx, &ctx->d_nfpts, nfpts.size()))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_nfpts, nfpts.data(), nfpts.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  }
   if ((rc = dalloc(ctx, &ctx->d_tabs, tab.size()))) return rc;
   if ((rc = dalloc(ctx, &ctx->d_nlambda, c.nopac))) return rc;
   if ((rc = dalloc(ctx, &ctx->d_jump, jump.size()))) return rc;
@@ -1392,6 +1429,9 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.draine_logcdf = draine ? m.draine_cdf + (int64_t)t->nemit * t->ndraine : nullptr;
   m.draine_logfreq = draine ? m.draine_cdf + 2 * (int64_t)t->nemit * t->ndraine : nullptr;
   ctx->have_draine = draine;
+  m.nfpts = filt ? ctx->d_nfpts : nullptr;
+  m.filtwave = filt ? b + off[filt_at] : nullptr;
+  m.filtphi = filt ? b + off[filt_at + 1] : nullptr;
   m.nlambda = ctx->d_nlambda;
   m.jump1 = ctx->d_jump;
   m.jump2 = ctx->d_jump + 64;
@@ -1505,6 +1545,8 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     return fail(ctx, MCRT_ERR_ARG, "imean selects Draine row %d of %d", std::max(ctx->imean_max, 2), ctx->dm.nemit);
   if (npout > 0 && !ctx->have_isrf)
     return fail(ctx, MCRT_ERR_ARG, "external-illumination packets (isrf_frac > 0) need the isrf table in mcrt_upload_tables");
+  if (c.output_imfilt && ipeel == 1 && !ctx->dm.filtwave)
+    return fail(ctx, MCRT_ERR_ARG, "filter-band images (output_imfilt) need nwfilt, filtwave and filtphi in mcrt_upload_tables");
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;
   for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }
@@ -1516,6 +1558,7 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   m.output_imcube = c.output_imcube; m.partial_peeloff = c.partial_peeloff; m.limb = c.limb; m.iplanckst = c.iplanckst;
   m.idust = c.idust; m.iffuv = c.iffuv; m.ispot = c.ispot; m.nspot = c.nspot;
   m.ncell = ctx->ncell; m.nsed = ctx->nsed; m.npsed = ctx->npsed; m.nimg = ctx->nimg;
+  m.output_imfilt = c.output_imfilt ? 1 : 0; m.nfilt = c.nfilt; m.nwfiltmax = c.nwfiltmax; m.nimgb = ctx->nimgb;
   m.rstar = c.rstar; m.rmincgs = c.rstar * 6.9598e10; m.tstar = c.tstar; m.tshock = c.tshock; m.fspot = c.fspot;
   m.rmaxi = c.rmaxi; m.fractxh = 2.0 * c.rmaxi / (double)c.nxhst; m.numin = c.numin; m.lnurat = c.lnurat;
   m.ifuv_ori = c.ifuv_ori;
@@ -1652,6 +1695,14 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
       if (rc) return rc;
       ctx->job_cap = want;
     }
+    if (ctx->cfg.output_imfilt && ctx->job_nub_cap != ctx->job_cap) {   // the frequency of each job
+      if (ctx->d_job_nub) dfree(ctx, ctx->d_job_nub);
+      ctx->d_job_nub = nullptr;
+      ctx->job_nub_cap = 0;
+      int rc = dalloc(ctx, &ctx->d_job_nub, (size_t)ctx->job_cap);
+      if (rc) return rc;
+      ctx->job_nub_cap = ctx->job_cap;
+    }
   }
   if (wave && ctx->wave_cap < wave_slots) {
     if (ctx->d_recs) dfree(ctx, ctx->d_recs);
@@ -1673,6 +1724,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
       for (auto& e : p) CK(cudaEventCreate(&e));
   }
   P.jobs = queue ? ctx->d_jobs : nullptr;
+  P.job_nub = (queue && ctx->cfg.output_imfilt) ? ctx->d_job_nub : nullptr;
   P.njobs = ctx->d_next + 1;
   P.job_cap = ctx->job_cap;
   const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
@@ -2201,13 +2253,16 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
   float* sed[10] = {out->si, out->sq, out->su, out->sv, out->si2, out->sq2, out->su2, out->sv2, out->nums, out->aveinc};
   float* ps[9] = {out->ti, out->tq, out->tu, out->tv, out->ti2, out->tq2, out->tu2, out->tv2, out->numt};
   float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
-  int64_t nmax = std::max(ctx->nsed, std::max(ctx->npsed, ctx->nimg));
+  float* ib[8] = {out->image_b_i, out->image_b_q, out->image_b_u, out->image_b_v,
+                  out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
+  int64_t nmax = std::max(std::max(ctx->nsed, ctx->nimgb), std::max(ctx->npsed, ctx->nimg));
   float* d_f = nullptr;
   if ((rc = dalloc(ctx, &d_f, nmax))) return rc;
   std::vector<std::pair<float*, std::pair<const double*, int64_t>>> jobs;
   for (int k = 0; k < 10; ++k) jobs.push_back({sed[k], {t.sed + k * ctx->nsed, ctx->nsed}});
   for (int k = 0; k < 9; ++k) jobs.push_back({ps[k], {t.psed + k * ctx->npsed, ctx->npsed}});
   for (int k = 0; k < 4; ++k) jobs.push_back({im[k], {t.img + k * ctx->nimg, ctx->nimg}});
+  for (int k = 0; k < 8; ++k) jobs.push_back({ib[k], {t.imgb + k * ctx->nimgb, ctx->nimgb}});
   for (auto& j : jobs) {
     if (!j.first || j.second.second == 0) continue;
     const int64_t n = j.second.second;
@@ -2228,7 +2283,9 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
   mcrt_tallies rest = *out;
   for (float** f : {&rest.si, &rest.sq, &rest.su, &rest.sv, &rest.si2, &rest.sq2, &rest.su2, &rest.sv2, &rest.nums,
                     &rest.aveinc, &rest.ti, &rest.tq, &rest.tu, &rest.tv, &rest.ti2, &rest.tq2, &rest.tu2, &rest.tv2,
-                    &rest.numt, &rest.image_m_i, &rest.image_m_q, &rest.image_m_u, &rest.image_m_v})
+                    &rest.numt, &rest.image_m_i, &rest.image_m_q, &rest.image_m_u, &rest.image_m_v,
+                    &rest.image_b_i, &rest.image_b_q, &rest.image_b_u, &rest.image_b_v,
+                    &rest.image_b_d, &rest.image_b_s, &rest.image_b_e, &rest.image_b_o})
     *f = nullptr;
   int rc = mcrt_download_tallies(ctx, &rest);
   if (rc) return rc;
@@ -2238,8 +2295,9 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
   const float inorm = (float)(rnp / ltot_lsol);
   const bool peel = ipeel == 1;
   const int64_t nsed = ctx->nsed, npsed = ctx->npsed, nimg = (peel && c.output_imcube) ? ctx->nimg : 0;
+  const int64_t nimgb = (peel && c.output_imfilt) ? ctx->nimgb : 0;
   float* d_f = nullptr;
-  if ((rc = dalloc(ctx, &d_f, std::max<int64_t>({10 * nsed, 9 * npsed, 4 * nimg, 1})))) return rc;
+  if ((rc = dalloc(ctx, &d_f, std::max<int64_t>({10 * nsed, 9 * npsed, 4 * nimg, nimgb, 1})))) return rc;
   auto grid = [](int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); };
   auto get = [&](float* dst, const float* src, int64_t n) -> int {
     if (!dst) return MCRT_OK;
@@ -2250,6 +2308,8 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
   float* sed[10] = {out->si, out->sq, out->su, out->sv, out->si2, out->sq2, out->su2, out->sv2, out->nums, out->aveinc};
   float* ps[9] = {out->ti, out->tq, out->tu, out->tv, out->ti2, out->tq2, out->tu2, out->tv2, out->numt};
   float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
+  float* ib[8] = {out->image_b_i, out->image_b_q, out->image_b_u, out->image_b_v,
+                  out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
   diskflux_sed<<<grid(nsed), 256, 0, ctx->stream>>>(t.sed, nsed, rnorm, d_f);
   for (int a = 0; a < 10 && !rc; ++a) rc = get(sed[a], d_f + a * nsed, nsed);
   if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
@@ -2262,12 +2322,21 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
       rc = get(im[a], d_f, nimg);
       if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
     }
+    for (int a = 0; a < 8 && !rc && nimgb > 0; ++a) {      // flux_test.f90:64-73
+      if (!ib[a]) continue;
+      diskflux_img<<<grid(nimgb), 256, 0, ctx->stream>>>(t.imgb + a * nimgb, nimgb, inorm, d_f);
+      rc = get(ib[a], d_f, nimgb);
+      if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MCRT_OK : fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux sync");
+    }
   } else if (!rc) {                          // ipeel /= 1: the peeled arrays as downloaded (flux_test.f90:44)
     mcrt_tallies pe{};
     pe.ti = out->ti; pe.tq = out->tq; pe.tu = out->tu; pe.tv = out->tv;
     pe.ti2 = out->ti2; pe.tq2 = out->tq2; pe.tu2 = out->tu2; pe.tv2 = out->tv2; pe.numt = out->numt;
     pe.image_m_i = out->image_m_i; pe.image_m_q = out->image_m_q;
     pe.image_m_u = out->image_m_u; pe.image_m_v = out->image_m_v;
+    pe.image_b_i = out->image_b_i; pe.image_b_q = out->image_b_q; pe.image_b_u = out->image_b_u;
+    pe.image_b_v = out->image_b_v; pe.image_b_d = out->image_b_d; pe.image_b_s = out->image_b_s;
+    pe.image_b_e = out->image_b_e; pe.image_b_o = out->image_b_o;
     rc = mcrt_download_tallies(ctx, &pe);
   }
   cudaError_t le = cudaGetLastError();
@@ -2281,7 +2350,7 @@ int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
   CK(cudaSetDevice(ctx->device));
   const DevTallies& t = ctx->dt;
   const int64_t nc = ctx->ncell;
-  const int64_t nmax = std::max<int64_t>(std::max<int64_t>(nc, MCRT_NCOUNTERS),
+  const int64_t nmax = std::max<int64_t>(std::max<int64_t>(std::max<int64_t>(nc, MCRT_NCOUNTERS), ctx->nimgb),
                                          std::max(ctx->nsed, std::max(ctx->npsed, ctx->nimg)));
   void* d_in = nullptr;
   int rc = dalloc(ctx, (char**)&d_in, (size_t)nmax * 8);
@@ -2314,6 +2383,9 @@ int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
   for (int k = 0; k < 10 && !rc; ++k) rc = add(sed[k], 2, t.sed + k * ctx->nsed, ctx->nsed);
   for (int k = 0; k < 9 && !rc; ++k) rc = add(ps[k], 2, t.psed + k * ctx->npsed, ctx->npsed);
   for (int k = 0; k < 4 && !rc; ++k) rc = add(im[k], 2, t.img + k * ctx->nimg, ctx->nimg);
+  const float* ib[8] = {in->image_b_i, in->image_b_q, in->image_b_u, in->image_b_v,
+                        in->image_b_d, in->image_b_s, in->image_b_e, in->image_b_o};
+  for (int k = 0; k < 8 && !rc; ++k) rc = add(ib[k], 2, t.imgb + k * ctx->nimgb, ctx->nimgb);
   dfree(ctx, d_in);
   return rc;
 }
@@ -2322,7 +2394,7 @@ int mcrt_device_tallies_view(mcrt_ctx* ctx, mcrt_device_tallies* out) {
   if (!ctx || !out) return MCRT_ERR_ARG;
   const int64_t nc = ctx->ncell;
   out->f64 = ctx->dt.dtauabs;                 // first member of the allocation
-  out->n_f64 = 2 * nc + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + MCRT_NSCALARS;
+  out->n_f64 = 2 * nc + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + MCRT_NSCALARS;
   out->u64 = (uint64_t*)ctx->dt.cnt;
   out->n_u64 = MCRT_NCOUNTERS;
   out->i32 = ctx->dt.nabs;

@@ -55,6 +55,7 @@ struct DevTallies {
   double *sed;                             // [10][nsed]
   double *psed;                            // [9][npsed]
   double *img;                             // [4][nimg]
+  double *imgb;                            // [8][nimgb] filter-band images: I Q U V, I by origin d s e o
   double *scal;                            // [MCRT_NSCALARS]
   unsigned long long *cnt;                 // [MCRT_NCOUNTERS]
   int32_t *ndiff;                          // [ncell] diffusion absorptions per surface cell
@@ -113,6 +114,13 @@ struct DevModel {
   // multiplications
   const int64_t *jump1, *jump2;
   const int64_t *jdig1, *jdig2;
+  // filter-band images (output_imfilt): per filter the number of points
+  // used (nwfilt - 1) and the curves filtwave (Hz, non-decreasing), filtphi
+  // [nfilt][nwfiltmax]
+  int output_imfilt, nfilt, nwfiltmax;
+  int64_t nimgb;
+  const int32_t *nfpts;
+  const double *filtwave, *filtphi;
 };
 
 // One peel-off request: the packet's state at an emission, scattering or
@@ -268,6 +276,7 @@ struct LaunchParams {
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter
   PeelJob *jobs;                // peel-off job queue (nullptr: peel inline)
+  double *job_nub;              // [job_cap] packet frequency per job (filter-band images only)
   unsigned long long *njobs;    // jobs queued
   int64_t job_cap;
   mcrt_packet_log *log;

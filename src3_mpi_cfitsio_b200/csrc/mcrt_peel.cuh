@@ -25,6 +25,7 @@ struct PeelLane {
   double si;        // I weight of this direction
   int64_t steps;
   PeelJob J;
+  double nub;       // the packet's frequency (filter-band images only)
   double adjC;      // adjoint forward pass: weighted contribution of the binned ray
   Rng rng0;         // stream state at the walk's start (the re-walk repeats it)
 
@@ -42,6 +43,7 @@ struct PeelLane {
     const unsigned long long jid = k / (unsigned long long)m.npeel;
     dir = (int)(k % (unsigned long long)m.npeel) + 1;
     J = P.jobs[jid];
+    nub = P.job_nub ? P.job_nub[jid] : 0.0;
     const double cospe = __ldg(m.cospe + dir - 1), sinpe = __ldg(m.sinpe + dir - 1);
     const double coste = __ldg(m.coste + dir - 1), sinte = __ldg(m.sinte + dir - 1);
     if (J.bits & 4u) {             // direct stellar peel-off (newdisktherm_5_fuv.f90:378-411)
@@ -228,6 +230,7 @@ struct PeelLane {
         atomicAdd(T.img + 3 * m.nimg + k, qv);
       }
     }
+    bin_filters(m, T, id, vx, vy, nub, i_orig, qi, qq, qu, qv);
     const int i_inter = scattered ? 2 : ((i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

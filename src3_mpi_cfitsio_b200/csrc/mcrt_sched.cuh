@@ -365,6 +365,7 @@ struct Lane {
     J.bits = (pk.on_wall ? 1u : 0u) | ((pk.iflag == 1 ? 1u : 0u) << 1) | ((ctx == PC_DIRECT ? 1u : 0u) << 2) |
              ((uint32_t)pk.i_orig << 3) | ((uint32_t)(pk.freq_bin(pk.nub) - 1) << 8);
     P.jobs[j] = J;
+    if (P.job_nub) P.job_nub[j] = pk.nub;
     ++c_jobs;
     return true;
   }
@@ -433,6 +434,7 @@ struct Lane {
         atomicAdd(pk.T.img + 3 * m.nimg + k, qv);
       }
     }
+    bin_filters(m, pk.T, id, vx, vy, pk.nub, pk.i_orig, qi, qq, qu, qv);
     const int i_inter = (pk.iflag == 1) ? 2 : ((pk.i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + pk.i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

@@ -177,6 +177,41 @@ struct SpecState {
 
 enum KapdOrder { KAPD_DISK = 0, KAPD_PROPAGATE = 1, KAPD_TAUINT = 2 };
 
+// Filter-band images (peeloff_3d_2_test.f90:242-285) of one peel-off that
+// reached image coordinates (vx, vy) (pixel units from the image corner):
+// freq = 2.9979e14 / wave with wave = 1.2398 / nub, as the reference forms
+// them; every filter whose open range (filtwave(1), filtwave(nf)) holds freq
+// adds the Stokes vector times filtphi(iw), iw the last point below freq
+// (the reference's linear scan; a binary search finds the same point on a
+// non-decreasing curve), and Stokes I to the image of the packet's origin
+// (i_orig 1 star, 2 disk, 3 envelope, 4 outflow).
+__device__ __forceinline__ void bin_filters(const DevModel& m, const DevTallies& T, int id, double vx, double vy,
+                                            double nub, int i_orig, double qi, double qq, double qu, double qv) {
+  if (!m.output_imfilt || !(vx > -1.0e9 && vx < 1.0e9 && vy > -1.0e9 && vy < 1.0e9)) return;
+  const int ix = (int)vx + 1, iy = (int)vy + 1;
+  if (ix > m.nxhst || iy > m.nxhst || ix <= 0 || iy <= 0) return;
+  const double wave = 1.2398 / nub;
+  const double freq = 2.9979e14 / wave;
+  const int oi = i_orig == 1 ? 5 : (i_orig == 2 ? 4 : (i_orig == 3 ? 6 : (i_orig == 4 ? 7 : -1)));
+  for (int f = 0; f < m.nfilt; ++f) {
+    const int nf = __ldg(m.nfpts + f);
+    const double* fw = m.filtwave + (int64_t)m.nwfiltmax * f;
+    if (!(freq > __ldg(fw) && freq < __ldg(fw + nf - 1))) continue;
+    int lo = 0, hi = nf - 1;                 // first point with fw >= freq lies in (0, nf-1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(fw + mid) >= freq) hi = mid; else lo = mid;
+    }
+    const double wt = __ldg(m.filtphi + (int64_t)m.nwfiltmax * f + hi - 1);
+    const int64_t k = (int64_t)(id - 1) + (int64_t)m.npeel * ((ix - 1) + (int64_t)m.nxhst * ((iy - 1) + (int64_t)m.nxhst * f));
+    atomicAdd(T.imgb + k, qi * wt);
+    atomicAdd(T.imgb + m.nimgb + k, qq * wt);
+    atomicAdd(T.imgb + 2 * m.nimgb + k, qu * wt);
+    atomicAdd(T.imgb + 3 * m.nimgb + k, qv * wt);
+    if (oi >= 0) atomicAdd(T.imgb + oi * m.nimgb + k, qi * wt);
+  }
+}
+
 struct Packet {
   const DevModel& m;
   const DevTallies& T;
@@ -1546,6 +1581,7 @@ struct Packet {
         atomicAdd(T.img + 3 * m.nimg + k, qv);
       }
     }
+    bin_filters(m, T, peelid, vx, vy, nub, i_orig, qi, qq, qu, qv);
     const int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

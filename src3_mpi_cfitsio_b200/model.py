@@ -949,6 +949,48 @@ def with_isrf(m: Model, frac: float = 0.2, **kw) -> Model:
     return m
 
 
+def filter_table(bands_um=(3.6, 24.0, 70.0), rel_width: float = 0.25, npts: int = 60, nwfiltmax: int = 64):
+    """Filter curves in the layout filt_nu.f90 leaves in filt_mod: per
+    filter, frequencies in Hz (2.9979e14 / lambda[um]) ascending over its
+    points, responses normalised by their trapezoidal integral over
+    frequency (filt_nu.f90:50-103), padded to nwfiltmax points; nwfilt
+    counts the points plus the file's header line, as the reference does.
+    The reference reads its 49 curves (2MASS, IRAC, MIPS, ...) from files that
+    are not present; here band b is a Gaussian in log wavelength centred on
+    bands_um[b] with relative width rel_width, sampled out to 2.5 widths.
+    Returns (nwfilt, filtwave, filtphi), the last two Fortran-ordered
+    (nwfiltmax, nfilt)."""
+    nf = len(bands_um)
+    if npts > nwfiltmax:
+        raise ValueError("npts must fit in nwfiltmax")
+    nwfilt = np.full(nf, npts + 1, np.int32)
+    fw = np.zeros((nwfiltmax, nf))
+    fp = np.zeros((nwfiltmax, nf))
+    for b, lam0 in enumerate(bands_um):
+        x = np.linspace(-2.5, 2.5, npts)
+        lam = lam0 * np.exp(x * rel_width)[::-1]             # decreasing wavelength: ascending frequency
+        f = 2.9979e14 / lam
+        phi = np.exp(-0.5 * ((np.log(lam / lam0)) / rel_width) ** 2)
+        fint = np.sum(0.5 * (phi[1:] + phi[:-1]) * (f[1:] - f[:-1]))
+        fw[:npts, b] = f
+        fp[:npts, b] = phi / fint
+        fw[npts:, b] = f[-1]
+    F = lambda a: np.asfortranarray(a).ravel(order="F")
+    return nwfilt, F(fw), F(fp)
+
+
+def with_filters(m: Model, **kw) -> Model:
+    """Filter-band images (output_imfilt): the curves of ``filter_table``."""
+    nwfilt, fw, fp = filter_table(**kw)
+    m.tables["nwfilt"] = nwfilt
+    m.tables["filtwave"] = fw
+    m.tables["filtphi"] = fp
+    m.config["output_imfilt"] = 1
+    m.config["nfilt"] = int(nwfilt.size)
+    m.config["nwfiltmax"] = int(fw.size // nwfilt.size)
+    return m
+
+
 def draine_table(nemit: int = 18, ndraine: int = 1000, lmin_um: float = 1.0, lmax_um: float = 1000.0) -> np.ndarray:
     """Small-grain (VSG/PAH) emission spectra in the layout draine_cdf.f90
     leaves in draine_mod: cdf_d(nemit,ndraine), logcdf_d(nemit,ndraine) and
