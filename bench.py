@@ -343,7 +343,7 @@ def run_ours(args, rank, world):
 
     def step(it, e, precision=None):
         if diffusion:
-            e.setdiffus(it)
+            e.setdiffus(it, outputs=False)
         e.reset_tallies()
         e.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
         kms = e.kernel_ms()
@@ -364,7 +364,7 @@ def run_ours(args, rank, world):
         for s in range(args.steps):
             it = args.warmup + s + 1
             if diffusion:
-                eng.setdiffus(it)
+                eng.setdiffus(it, outputs=False)
             eng.reset_tallies()
             eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
             kernel_ms.append(eng.kernel_ms())
@@ -405,7 +405,7 @@ def run_ours(args, rank, world):
         eng.mark(4)
         eng.upload_grid()
         if diffusion:
-            eng.setdiffus(it)
+            eng.setdiffus(it, outputs=False)
         eng.reset_tallies()
         eng.run(np_total, lo, hi, iteration=it, ipeel=args.ipeel)
         reduce_ranks(eng)
@@ -712,10 +712,10 @@ def main():
                     help="packets per model of each autotuner trial")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
-    # 777.5 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
-    # launch (FP32 walk) over 2,097,152 walks, from an ncu capture of the
-    # 8e6-packet case
-    ap.add_argument("--traffic-per-walk", type=float, default=777.5,
+    # 691.1 B: dram__bytes_read.sum + dram__bytes_write.sum of one wave_walk
+    # launch (FP32 walk, record in 16-byte groups) over 2,097,152 walks, from
+    # an ncu capture of the 8e6-packet case
+    ap.add_argument("--traffic-per-walk", type=float, default=691.1,
                     help="DRAM bytes per walk of the wave_walk kernel from an ncu capture")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

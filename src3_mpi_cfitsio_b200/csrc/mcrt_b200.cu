@@ -146,6 +146,9 @@ struct mcrt_ctx {
   int32_t *d_tflag = nullptr;         // [ncell] bit 0: disk ids 1/2/9, bit 1: ids 4/10 (tfinal's gradient rules)
   double *d_rave = nullptr;           // [nrg] cell-centre radii (ravearr or the wall midpoints)
   std::vector<int32_t> h_diffus;      // diffusion flags (convergence statistics)
+  bool h_diffus_stale = false;        // mcrt_setdiffus changed d_diffus without copying it here
+  void *d_scratch = nullptr;          // grow-only scratch of the per-iteration calls (tfinal, download)
+  size_t scratch_bytes = 0;
   // tables
   int32_t *d_nlambda = nullptr;
   double *d_tabs = nullptr;
@@ -215,6 +218,26 @@ void dfree(mcrt_ctx* ctx, void* p) {
   auto it = std::find(ctx->allocs.begin(), ctx->allocs.end(), p);
   if (it != ctx->allocs.end()) ctx->allocs.erase(it);
   cudaFree(p);
+}
+
+// Scratch of the calls a driver makes every iteration (the temperature
+// update, the tally download): one buffer that only grows, so after the
+// first iteration they allocate and free nothing (cudaFree would also wait
+// for the whole device).  One user at a time: each call finishes with it
+// before it returns.
+template <class T>
+int scratch(mcrt_ctx* ctx, T** p, size_t n) {
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  if (ctx->scratch_bytes < bytes) {
+    if (ctx->d_scratch) dfree(ctx, ctx->d_scratch);
+    ctx->d_scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    const int rc = dalloc(ctx, (char**)&ctx->d_scratch, bytes);
+    if (rc) return rc;
+    ctx->scratch_bytes = bytes;
+  }
+  *p = static_cast<T*>(ctx->d_scratch);
+  return MCRT_OK;
 }
 
 int64_t mulmod_h(int64_t a, int64_t b, int64_t m) {
@@ -2257,7 +2280,7 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
                   out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
   int64_t nmax = std::max(std::max(ctx->nsed, ctx->nimgb), std::max(ctx->npsed, ctx->nimg));
   float* d_f = nullptr;
-  if ((rc = dalloc(ctx, &d_f, nmax))) return rc;
+  if ((rc = scratch(ctx, &d_f, nmax))) return rc;
   std::vector<std::pair<float*, std::pair<const double*, int64_t>>> jobs;
   for (int k = 0; k < 10; ++k) jobs.push_back({sed[k], {t.sed + k * ctx->nsed, ctx->nsed}});
   for (int k = 0; k < 9; ++k) jobs.push_back({ps[k], {t.psed + k * ctx->npsed, ctx->npsed}});
@@ -2267,11 +2290,10 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
     if (!j.first || j.second.second == 0) continue;
     const int64_t n = j.second.second;
     to_float<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, ctx->stream>>>(j.second.first, d_f, n);
-    if ((rc = cp(j.first, d_f, n * 4))) { dfree(ctx, d_f); return rc; }
+    if ((rc = cp(j.first, d_f, n * 4))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
   }
   CK(cudaStreamSynchronize(ctx->stream));
-  dfree(ctx, d_f);
   return MCRT_OK;
 }
 
@@ -2451,6 +2473,10 @@ int mcrt_setdiffus(mcrt_ctx* ctx, int32_t iter, double massd, double rmaxd, cons
   setdiffus_apply<<<512, 256, 0, ctx->stream>>>(a, disk ? 1 : 0, ctx->d_cells, ctx->d_diffus, ctx->d_tdust,
                                                 ctx->d_tdust0, ctx->d_sd_out);
   CK(cudaGetLastError());
+  if (!diffus && !diffdir && !dcount) {     // nothing to return: no wait; tfinal copies the flags it needs
+    ctx->h_diffus_stale = true;
+    return MCRT_OK;
+  }
   std::vector<int32_t> out(nc);
   CK(cudaMemcpyAsync(out.data(), ctx->d_sd_out, nc * 4, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -2462,6 +2488,7 @@ int mcrt_setdiffus(mcrt_ctx* ctx, int32_t iter, double massd, double rmaxd, cons
     if (diffus) diffus[k] = on;
     if (diffdir) diffdir[k] = out[k] >> 8;
   }
+  ctx->h_diffus_stale = false;
   if (dcount) *dcount = cnt;
   return MCRT_OK;
 }
@@ -2476,7 +2503,7 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
   const int64_t n2 = (int64_t)c.nrg * c.ntg;
   double* d_td = nullptr;
   int rc;
-  if ((rc = dalloc(ctx, &d_td, 3 * nc + (ctx->have_vel ? nc + 5 * n2 : 0)))) return rc;
+  if ((rc = scratch(ctx, &d_td, 3 * nc + (ctx->have_vel ? nc + 5 * n2 : 0)))) return rc;
   CK(cudaMemcpyAsync(d_td, tdave, nc * 8, cudaMemcpyHostToDevice, ctx->stream));
   TfinalArgs a{};
   a.nrg = c.nrg; a.ntg = c.ntg; a.npg = c.npg; a.nT = c.nT; a.nphot = nphot; a.maxii = iter > 3 ? 20 : 1;
@@ -2511,8 +2538,11 @@ int mcrt_update_temperature(mcrt_ctx* ctx, int32_t nphot, int32_t iter, double* 
   CK(cudaMemcpyAsync(ctx->d_tdust0, ctx->d_tdust, nc * 8, cudaMemcpyDeviceToDevice, ctx->stream));
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(tdave, a.tdave, nc * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->h_diffus_stale) {           // the flags of the last mcrt_setdiffus, for the statistics below
+    CK(cudaMemcpyAsync(ctx->h_diffus.data(), ctx->d_diffus, nc * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->h_diffus_stale = false;
+  }
   CK(cudaStreamSynchronize(ctx->stream));
-  dfree(ctx, d_td);
   // convergence statistics (tfinal_5_test1.f90:307-348)
   const double T01 = 0.1 / 11605.0;
   double s[3] = {0, 0, 0}, s2[3] = {0, 0, 0};

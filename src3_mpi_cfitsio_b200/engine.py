@@ -385,22 +385,26 @@ class Engine:
         """Diffusion-cell temperatures of the last run from the (reduced) counts."""
         self._check(self.lib.mcrt_refresh_diffusion(self.ctx))
 
-    def setdiffus(self, iteration: int, tdave=None):
+    def setdiffus(self, iteration: int, tdave=None, outputs: bool = True):
         """setdiffus(iter) and gridset's tdust reset on the device
         (mcrt_setdiffus), from ``tdave`` (default: the engine's current
         temperature); returns (diffus, diffdir, dcount) as Fortran-order
-        flat arrays.  The disk mass and outer radius come from the model."""
+        flat arrays, or None with ``outputs=False`` (the call then returns
+        without waiting for the device).  The disk mass and outer radius
+        come from the model."""
         w = self.model.w
         td = np.ascontiguousarray(self.tdave if tdave is None else tdave, dtype=np.float64)
         n = td.size
+        I = C.POINTER(C.c_int32)
+        args = (self.ctx, iteration, float(w.massd), float(w.rmaxd_au * self.model.config["autors"]),
+                td.ctypes.data_as(C.POINTER(C.c_double)))
+        if not outputs:
+            self._check(self.lib.mcrt_setdiffus(*args, None, None, None))
+            return None
         dif = np.zeros(n, np.int32)
         ddir = np.zeros(n, np.int32)
         cnt = C.c_int64(0)
-        I = C.POINTER(C.c_int32)
-        self._check(self.lib.mcrt_setdiffus(self.ctx, iteration, float(w.massd),
-                                            float(w.rmaxd_au * self.model.config["autors"]),
-                                            td.ctypes.data_as(C.POINTER(C.c_double)), dif.ctypes.data_as(I),
-                                            ddir.ctypes.data_as(I), C.byref(cnt)))
+        self._check(self.lib.mcrt_setdiffus(*args, dif.ctypes.data_as(I), ddir.ctypes.data_as(I), C.byref(cnt)))
         return dif, ddir, int(cnt.value)
 
     def enable_packet_log(self, n: int):
@@ -435,7 +439,7 @@ class Engine:
         (gridset_5_model13new.f90:1842-1866, ``setdiffus``).
         """
         if self.model.config.get("diffusion") and iteration >= 1:
-            self.setdiffus(iteration)
+            self.setdiffus(iteration, outputs=False)
         self.reset_tallies()
         self.run(np_total, iteration=iteration, ipeel=ipeel, seeds=(12345678 - i1 if i1 else 12345678, 87654321),
                  generator=generator)

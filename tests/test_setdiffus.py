@@ -134,3 +134,32 @@ def test_runs_after_device_setdiffus_equal_runs_on_the_generated_region(precisio
     assert (a["pad"] != 0).sum() == (b["pad"] != 0).sum()
     for k in a:
         assert np.array_equal(a[k][nodiff], b[k][nodiff]), k
+
+
+@pytest.mark.gpu
+def test_setdiffus_without_outputs_feeds_the_convergence_statistics(oracle_mod):
+    """mcrt_setdiffus with no output arrays returns without waiting; the
+    flags reach tfinal's convergence statistics (which leave diffusion cells
+    out) through the temperature update.  Same tallies, same result as the
+    call that returns the flags, and as an engine given the region at
+    upload."""
+    from src3_mpi_cfitsio_b200.engine import Engine
+    base = model.warm(model.small_2d())
+    td = base.grid["tdust"].copy()
+    ref = model.setdiffus(model.warm(model.small_2d()), td, 2)
+    tal, _ = oracle_mod.run(abi.Bundle(ref), 20000, ipeel=0, threads=8, images=False)
+    res = []
+    for m, outputs in ((base, True), (base, False), (ref, None)):
+        eng = Engine(m, precision="fp64")
+        if outputs is not None:
+            eng.setdiffus(2, td, outputs=outputs)
+        eng.reset_tallies()
+        eng.accumulate(tal)
+        eng.tdave = td.copy()
+        t, conv, sig = eng.update_temperature(20000, 2)
+        res.append((t, sig))
+        eng.close()
+    assert np.isfinite(res[0][1]).all()
+    for t, sig in res[1:]:
+        assert np.array_equal(t, res[0][0])
+        assert np.array_equal(sig, res[0][1])
