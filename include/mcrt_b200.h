@@ -104,6 +104,15 @@ typedef struct mcrt_config {
    * and the leading dimension nwfiltmax of mcrt_tables.filtwave/filtphi
    * (filt_mod.f90:10-14).  output_imfilt = 0 leaves the images off. */
   int32_t output_imfilt, nfilt, nwfiltmax, pad_filt;
+  /* Multi-wavelength nested ("sparse") images (output_imsparse,
+   * peeloff_3d_2_test.f90:302-309, type_nested_image.f90:75-101): per
+   * inclination and Stokes parameter, sparse_nlev nested square images of
+   * sparse_dim^2 pixels (half sizes mcrt_tables.sparse_levels) times
+   * sparse_nnu bins in log10(frequency [Hz]) from sparse_lognu_min to
+   * sparse_lognu_max -- the values nested_image_setup receives
+   * (initarr_2_new.f90:170-190), in the reference's single precision. */
+  int32_t output_imsparse, sparse_dim, sparse_nlev, sparse_nnu;
+  float   sparse_lognu_min, sparse_lognu_max;
 } mcrt_config;
 
 /*
@@ -189,6 +198,10 @@ typedef struct mcrt_tables {
    * (a curve uses its first nwfilt-1 points, filt_nu.f90:30). */
   const int32_t *nwfilt;
   const double  *filtwave, *filtphi;
+  /* Half sizes of the nested images [R*], ascending, as find_levels
+   * (type_nested_image.f90:62-73) leaves them in image%levels; needed when
+   * output_imsparse = 1. */
+  const float   *sparse_levels;                                     /* [sparse_nlev] */
 } mcrt_tables;
 
 /*
@@ -208,6 +221,11 @@ typedef struct mcrt_tallies {
    * tts_mod_5.f90:67-68 */
   float   *image_b_i, *image_b_q, *image_b_u, *image_b_v;             /* [npeel,nxhst,nxhst,nfilt] */
   float   *image_b_d, *image_b_s, *image_b_e, *image_b_o;             /* [npeel,nxhst,nxhst,nfilt] */
+  /* Nested images (output_imsparse = 1), image_ms_i..v of tts_mod_5.f90:76
+   * held dense: [sparse_dim, sparse_dim, sparse_nnu, sparse_nlev, npeel]
+   * (pixel ix fastest); the driver inserts the non-zero pixels into its
+   * smart images for nested_image_write. */
+  float   *image_ms_i, *image_ms_q, *image_ms_u, *image_ms_v;
 } mcrt_tallies;
 
 /* scalars[] of one iteration (the reference's module scalars) */
@@ -452,7 +470,8 @@ int mcrt_refresh_diffusion(mcrt_ctx *ctx);
  * tdave, 0.1 K in diffusion and empty cells) for the next mcrt_run_iteration.
  * Needs mcrt_grid.hdisk and mcrt_tables.kappar.  tdave [nrg,ntg,npg] (every
  * entry positive) is read; diffus, diffdir [nrg,ntg,npg] and dcount (the
- * reference's count of diffusion cells) may be NULL.  Cells without a thermal
+ * reference's count of diffusion cells) may be NULL; with all three NULL the
+ * call returns without waiting for the device.  Cells without a thermal
  * component are never flagged (diffusion emission needs a temperature). */
 int mcrt_setdiffus(mcrt_ctx *ctx, int32_t iter, double massd, double rmaxd,
                    const double *tdave, int32_t *diffus, int32_t *diffdir,

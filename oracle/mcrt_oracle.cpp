@@ -259,7 +259,37 @@ struct Tally {
 struct Images {       // shared across threads, atomic adds
   std::vector<double> im[4];
   std::vector<double> imb[8];   // filter-band images: I Q U V, then I by origin d s e o
+  std::vector<double> ims[4];   // nested images, I Q U V, dense [dim,dim,nnu,nlev,npeel]
 };
+
+// math_binning.f90 ipos_sp: bin of x among nbin equal bins of [xmin,xmax]
+// in single precision; 0 below the range, nbin+1 above it.
+int ipos_sp(float xmin, float xmax, float x, int nbin) {
+  if (xmax > xmin) {
+    if (x < xmin) return 0;
+    if (x > xmax) return nbin + 1;
+  } else {
+    if (x < xmax) return 0;
+    if (x > xmin) return nbin + 1;
+  }
+  const float frac = (x - xmin) / (xmax - xmin);
+  return (int)(frac * (float)nbin) + 1;
+}
+
+// math_binning.f90 locate_sp: jl with xx(jl) <= x < xx(jl+1) (1-based) by
+// bisection, 1 at xx(1), n-1 at xx(n), -1 outside the table.
+int locate_sp(const float* xx, int n, float x) {
+  const bool ascnd = xx[n - 1] >= xx[0];
+  int jl = 0, ju = n + 1;
+  while (ju - jl > 1) {
+    const int jm = (ju + jl) / 2;
+    if (ascnd == (x >= xx[jm - 1])) jl = jm; else ju = jm;
+  }
+  if (x == xx[0]) return 1;
+  if (x == xx[n - 1]) return n - 1;
+  if (x > xx[n - 1] || x < xx[0]) return -1;
+  return jl;
+}
 
 void atomic_add(double& x, double v) {
   std::atomic_ref<double> a(x);
@@ -1340,6 +1370,33 @@ struct Packet {
         }
       }
     }
+    // nested images (peeloff_3d_2_test.f90:302-309 -> nested_image_bin,
+    // type_nested_image.f90:75-101): single-precision position and
+    // log10(frequency); the level is the smallest whose half size exceeds
+    // max(|x|,|y|); a pixel outside the image (only at a level's exact edge)
+    // is dropped
+    if (c.output_imsparse && !I->ims[0].empty()) {
+      const float xr = (float)ximage, yr = (float)yimage;
+      const float lnu = (float)std::log10(2.9979e14 / (1.2398 / nub));
+      const float* lev = t->sparse_levels;
+      const int nl = c.sparse_nlev;
+      const float r = std::max(std::fabs(xr), std::fabs(yr));
+      if (!(r > lev[nl - 1])) {
+        int l = locate_sp(lev, nl, r);
+        l = (l < 0) ? 1 : l + 1;
+        const int ix = ipos_sp(-lev[l - 1], lev[l - 1], xr, c.sparse_dim);
+        const int iy = ipos_sp(-lev[l - 1], lev[l - 1], yr, c.sparse_dim);
+        const int inu = ipos_sp(c.sparse_lognu_min, c.sparse_lognu_max, lnu, c.sparse_nnu);
+        if (inu >= 1 && inu <= c.sparse_nnu && ix >= 1 && ix <= c.sparse_dim && iy >= 1 && iy <= c.sparse_dim) {
+          const int64_t k = (int64_t)(ix - 1) + (int64_t)c.sparse_dim * ((iy - 1) + (int64_t)c.sparse_dim *
+                            ((inu - 1) + (int64_t)c.sparse_nnu * ((l - 1) + (int64_t)nl * (peelid - 1))));
+          atomic_add(I->ims[0][k], q_i);
+          atomic_add(I->ims[1][k], q_q);
+          atomic_add(I->ims[2][k], q_u);
+          atomic_add(I->ims[3][k], q_v);
+        }
+      }
+    }
     int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
     int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= c.nap; ++ia) {
@@ -1899,6 +1956,10 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
   const int64_t nimgb = (int64_t)cfg->npeel * cfg->nxhst * cfg->nxhst * cfg->nfilt;
   if (cfg->output_imfilt && (cfg->nfilt < 1 || !tab->nwfilt || !tab->filtwave || !tab->filtphi)) return MCRT_ERR_ARG;
   for (auto& v : img.imb) v.assign(cfg->output_imfilt ? nimgb : 0, 0.0);
+  const int64_t nims = (int64_t)cfg->sparse_dim * cfg->sparse_dim * cfg->sparse_nnu * cfg->sparse_nlev * cfg->npeel;
+  if (cfg->output_imsparse && (cfg->sparse_dim < 1 || cfg->sparse_nnu < 1 || cfg->sparse_nlev < 1 || !tab->sparse_levels))
+    return MCRT_ERR_ARG;
+  for (auto& v : img.ims) v.assign(cfg->output_imsparse ? nims : 0, 0.0);
   int nt = std::max(1, (int)nthreads);
   std::vector<Tally> tl(nt);
   for (auto& t : tl) t.init(m.ncell, nsed, npsed);
@@ -1960,6 +2021,8 @@ int oracle_run(const mcrt_config* cfg, const mcrt_grid* grid, const mcrt_tables*
     float* ib[8] = {out->image_b_i, out->image_b_q, out->image_b_u, out->image_b_v,
                     out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
     for (int k = 0; k < 8; ++k) put(ib[k], img.imb[k]);
+    float* is[4] = {out->image_ms_i, out->image_ms_q, out->image_ms_u, out->image_ms_v};
+    for (int k = 0; k < 4; ++k) put(is[k], img.ims[k]);
     if (out->scalars) for (int k = 0; k < MCRT_NSCALARS; ++k) out->scalars[k] = S.scal[k];
     if (out->counters) for (int k = 0; k < MCRT_NCOUNTERS; ++k) out->counters[k] = S.cnt[k];
   }

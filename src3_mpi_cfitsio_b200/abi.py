@@ -39,7 +39,10 @@ class Config(C.Structure):
         "rstar", "tstar", "tstarave", "tshock", "fspot", "accfrac", "accfrac2",
         "isrf_frac", "rddust", "rmaxi", "numin", "lnurat", "autors", "ifuv_ori",
         "cspot1", "sspot1", "scspot1", "ssspot1", "cspot2", "sspot2", "scspot2",
-        "ssspot2", "csprad")] + [(n, C.c_int32) for n in ("output_imfilt", "nfilt", "nwfiltmax", "pad_filt")]
+        "ssspot2", "csprad")] + [(n, C.c_int32) for n in ("output_imfilt", "nfilt", "nwfiltmax", "pad_filt",
+                                                           "output_imsparse", "sparse_dim", "sparse_nlev",
+                                                           "sparse_nnu")] + [
+        (n, C.c_float) for n in ("sparse_lognu_min", "sparse_lognu_max")]
 
 
 GRID_FIELDS = [("rarr", _dp), ("r2arr", _dp), ("thetarr", _dp), ("costarr", _dp),
@@ -63,7 +66,7 @@ TABLE_FIELDS = [("nlambda", _ip), ("nudust", _dp), ("kappad", _dp), ("adust", _d
                 ("limb_prob", _dp), ("mueller", _dp), ("narr", C.c_int32), ("pad_mueller", C.c_int32),
                 ("isrf", _dp), ("nisrf", C.c_int32), ("pad_isrf", C.c_int32),
                 ("draine", _dp), ("nemit", C.c_int32), ("ndraine", C.c_int32),
-                ("nwfilt", _ip), ("filtwave", _dp), ("filtphi", _dp)]
+                ("nwfilt", _ip), ("filtwave", _dp), ("filtphi", _dp), ("sparse_levels", _fp)]
 
 
 class Tables(C.Structure):
@@ -76,13 +79,14 @@ SED = ["si", "sq", "su", "sv", "si2", "sq2", "su2", "sv2", "nums", "aveinc"]
 PSED = ["ti", "tq", "tu", "tv", "ti2", "tq2", "tu2", "tv2", "numt"]
 IMG = ["image_m_i", "image_m_q", "image_m_u", "image_m_v"]
 IMGB = ["image_b_i", "image_b_q", "image_b_u", "image_b_v", "image_b_d", "image_b_s", "image_b_e", "image_b_o"]
+IMGS = ["image_ms_i", "image_ms_q", "image_ms_u", "image_ms_v"]
 
 
 class Tallies(C.Structure):
     _fields_ = ([(n, _ip) for n in CELL_I] + [(n, _dp) for n in CELL_D] +
                 [(n, _fp) for n in SED] + [(n, _fp) for n in PSED] +
                 [(n, _fp) for n in IMG] + [("scalars", _dp), ("counters", _lp)] +
-                [(n, _fp) for n in IMGB])
+                [(n, _fp) for n in IMGB] + [(n, _fp) for n in IMGS])
 
 
 class PacketLog(C.Structure):
@@ -134,9 +138,15 @@ class Bundle:
             if ptype is C.c_int32:          # scalar member
                 setattr(s, name, int(a))
                 continue
+            if ptype is C.c_float:          # scalar member
+                setattr(s, name, float(a))
+                continue
             if ptype is _ip:
                 a = np.ascontiguousarray(a, dtype=np.int32)
                 ct = C.c_int32
+            elif ptype is _fp:
+                a = np.ascontiguousarray(a, dtype=np.float32)
+                ct = C.c_float
             else:
                 a = np.ascontiguousarray(a, dtype=np.float64)
                 ct = C.c_double
@@ -170,6 +180,10 @@ class TallyArrays:
             nimgb = cfg.npeel * cfg.nxhst * cfg.nxhst * cfg.nfilt
             for n in IMGB:
                 self.arrays[n] = np.zeros(nimgb, np.float32)
+        if images and cfg.output_imsparse:
+            nims = cfg.sparse_dim * cfg.sparse_dim * cfg.sparse_nnu * cfg.sparse_nlev * cfg.npeel
+            for n in IMGS:
+                self.arrays[n] = np.zeros(nims, np.float32)
         self.arrays["scalars"] = np.zeros(MCRT_NSCALARS, np.float64)
         self.arrays["counters"] = np.zeros(MCRT_NCOUNTERS, np.int64)
         t = Tallies()
@@ -213,6 +227,8 @@ class TallyArrays:
             return a.reshape((c.npeel, c.nxhst, c.nxhst, c.nfreq), order="F")
         if name in IMGB:
             return a.reshape((c.npeel, c.nxhst, c.nxhst, c.nfilt), order="F")
+        if name in IMGS:
+            return a.reshape((c.sparse_dim, c.sparse_dim, c.sparse_nnu, c.sparse_nlev, c.npeel), order="F")
         return a
 
 

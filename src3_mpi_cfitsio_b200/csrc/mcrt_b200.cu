@@ -162,6 +162,8 @@ struct mcrt_ctx {
   double *d_job_nub = nullptr;        // [job_cap] packet frequency per job (filter-band images)
   int64_t job_nub_cap = 0;
   int64_t nimgb = 0;                  // filter-band image size (0: off)
+  int64_t nims = 0;                   // nested image size per Stokes parameter (0: off)
+  float *d_levels = nullptr;          // [sparse_nlev] nested image half sizes
   int32_t *d_nfpts = nullptr;         // [nfilt] points per filter curve
   int64_t chunk_packets = 1 << 20;
   int32_t *d_err = nullptr;
@@ -950,10 +952,18 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
     return fail(ctx, MCRT_ERR_ARG, "output_imfilt needs 1 <= nfilt <= 4096 and nwfiltmax >= 2");
   }
   ctx->nimgb = c.output_imfilt ? (int64_t)c.npeel * c.nxhst * c.nxhst * c.nfilt : 0;
+  if (c.output_imsparse && (c.sparse_dim < 1 || c.sparse_nnu < 1 || c.sparse_nlev < 1 || c.sparse_nlev > 64 ||
+                            !(c.sparse_lognu_max > c.sparse_lognu_min))) {
+    *out = ctx;
+    return fail(ctx, MCRT_ERR_ARG, "output_imsparse needs sparse_dim, sparse_nnu >= 1, 1 <= sparse_nlev <= 64 "
+                                   "and sparse_lognu_max > sparse_lognu_min");
+  }
+  ctx->nims = c.output_imsparse ? (int64_t)c.sparse_dim * c.sparse_dim * c.sparse_nnu * c.sparse_nlev * c.npeel : 0;
   // one tally allocation: cell ints, cell doubles, SED, peeled SED, images,
   // filter-band images, scalars, counters
   const int64_t n_int = 5 * ctx->ncell;
-  const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + MCRT_NSCALARS;
+  const int64_t n_dbl = 2 * ctx->ncell + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + 4 * ctx->nims +
+                        MCRT_NSCALARS;
   ctx->tally_bytes = (size_t)n_dbl * 8 + (size_t)MCRT_NCOUNTERS * 8 + (size_t)((n_int * 4 + 7) / 8) * 8;
   int rc = dalloc(ctx, (char**)&ctx->d_tally, ctx->tally_bytes);
   if (rc) { *out = ctx; return rc; }
@@ -966,6 +976,7 @@ int mcrt_create(const mcrt_config* cfg, int device, mcrt_ctx** out) {
   t.psed = d; d += 9 * ctx->npsed;
   t.img = d; d += 4 * ctx->nimg;
   t.imgb = d; d += 8 * ctx->nimgb;
+  t.ims = d; d += 4 * ctx->nims;
   t.scal = d; d += MCRT_NSCALARS;
   t.cnt = (unsigned long long*)d;
   int32_t* ip = (int32_t*)(t.cnt + MCRT_NCOUNTERS);
@@ -1418,6 +1429,16 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   int rc;
   if (ctx->have_tables) { dfree(ctx, ctx->d_tabs); dfree(ctx, ctx->d_nlambda); dfree(ctx, ctx->d_jump); }
   if (ctx->d_nfpts) { dfree(ctx, ctx->d_nfpts); ctx->d_nfpts = nullptr; }
+  if (ctx->d_levels) { dfree(ctx, ctx->d_levels); ctx->d_levels = nullptr; }
+  if (c.output_imsparse) {
+    if (!t->sparse_levels) return fail(ctx, MCRT_ERR_ARG, "output_imsparse needs sparse_levels");
+    for (int l = 0; l < c.sparse_nlev; ++l)
+      if (!(t->sparse_levels[l] > 0.0f) || !std::isfinite(t->sparse_levels[l]) ||
+          (l > 0 && !(t->sparse_levels[l] > t->sparse_levels[l - 1])))
+        return fail(ctx, MCRT_ERR_ARG, "sparse_levels must be positive and ascending");
+    if ((rc = dalloc(ctx, &ctx->d_levels, (size_t)c.sparse_nlev))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_levels, t->sparse_levels, (size_t)c.sparse_nlev * 4, cudaMemcpyHostToDevice, ctx->stream));
+  }
   if (filt) {
     if ((rc = dalloc(ctx, &ctx->d_nfpts, nfpts.size()))) return rc;
     CK(cudaMemcpyAsync(ctx->d_nfpts, nfpts.data(), nfpts.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -1453,6 +1474,7 @@ int mcrt_upload_tables(mcrt_ctx* ctx, const mcrt_tables* t) {
   m.draine_logfreq = draine ? m.draine_cdf + 2 * (int64_t)t->nemit * t->ndraine : nullptr;
   ctx->have_draine = draine;
   m.nfpts = filt ? ctx->d_nfpts : nullptr;
+  m.sparse_levels = c.output_imsparse ? ctx->d_levels : nullptr;
   m.filtwave = filt ? b + off[filt_at] : nullptr;
   m.filtphi = filt ? b + off[filt_at + 1] : nullptr;
   m.nlambda = ctx->d_nlambda;
@@ -1570,6 +1592,8 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
     return fail(ctx, MCRT_ERR_ARG, "external-illumination packets (isrf_frac > 0) need the isrf table in mcrt_upload_tables");
   if (c.output_imfilt && ipeel == 1 && !ctx->dm.filtwave)
     return fail(ctx, MCRT_ERR_ARG, "filter-band images (output_imfilt) need nwfilt, filtwave and filtphi in mcrt_upload_tables");
+  if (c.output_imsparse && ipeel == 1 && !ctx->dm.sparse_levels)
+    return fail(ctx, MCRT_ERR_ARG, "nested images (output_imsparse) need sparse_levels in mcrt_upload_tables");
   // generator seeds (set_all_seeds)
   int64_t g1 = seed1, g2 = seed2;
   for (int g = 2; g <= generator; ++g) { g1 = mulmod_h(2082007225, g1, 2147483563); g2 = mulmod_h(784306273, g2, 2147483399); }
@@ -1582,6 +1606,9 @@ static int make_params(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi, int32_
   m.idust = c.idust; m.iffuv = c.iffuv; m.ispot = c.ispot; m.nspot = c.nspot;
   m.ncell = ctx->ncell; m.nsed = ctx->nsed; m.npsed = ctx->npsed; m.nimg = ctx->nimg;
   m.output_imfilt = c.output_imfilt ? 1 : 0; m.nfilt = c.nfilt; m.nwfiltmax = c.nwfiltmax; m.nimgb = ctx->nimgb;
+  m.output_imsparse = c.output_imsparse ? 1 : 0; m.sparse_dim = c.sparse_dim; m.sparse_nlev = c.sparse_nlev;
+  m.sparse_nnu = c.sparse_nnu; m.sparse_lognu_min = c.sparse_lognu_min; m.sparse_lognu_max = c.sparse_lognu_max;
+  m.nims = ctx->nims;
   m.rstar = c.rstar; m.rmincgs = c.rstar * 6.9598e10; m.tstar = c.tstar; m.tshock = c.tshock; m.fspot = c.fspot;
   m.rmaxi = c.rmaxi; m.fractxh = 2.0 * c.rmaxi / (double)c.nxhst; m.numin = c.numin; m.lnurat = c.lnurat;
   m.ifuv_ori = c.ifuv_ori;
@@ -1718,7 +1745,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
       if (rc) return rc;
       ctx->job_cap = want;
     }
-    if (ctx->cfg.output_imfilt && ctx->job_nub_cap != ctx->job_cap) {   // the frequency of each job
+    if ((ctx->cfg.output_imfilt || ctx->cfg.output_imsparse) && ctx->job_nub_cap != ctx->job_cap) {   // each job's frequency
       if (ctx->d_job_nub) dfree(ctx, ctx->d_job_nub);
       ctx->d_job_nub = nullptr;
       ctx->job_nub_cap = 0;
@@ -1747,7 +1774,7 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
       for (auto& e : p) CK(cudaEventCreate(&e));
   }
   P.jobs = queue ? ctx->d_jobs : nullptr;
-  P.job_nub = (queue && ctx->cfg.output_imfilt) ? ctx->d_job_nub : nullptr;
+  P.job_nub = (queue && (ctx->cfg.output_imfilt || ctx->cfg.output_imsparse)) ? ctx->d_job_nub : nullptr;
   P.njobs = ctx->d_next + 1;
   P.job_cap = ctx->job_cap;
   const int peel_grid = ctx->nsm * (mixed ? peel_mixed_blocks_per_sm() : peel_fp64_blocks_per_sm());
@@ -1761,7 +1788,15 @@ static int run_iteration_impl(mcrt_ctx* ctx, int64_t np, int64_t lo, int64_t hi,
     ctx->kt_walks = ctx->kt_walk_cross = 0;
   }
   auto kt_begin = [&](int k) -> int {
-    if (wave) CK(cudaEventRecord(ctx->kt_ev[k][0], ctx->stream));
+    if (!wave) return MCRT_OK;
+    if (ctx->kt_pending[k]) {             // the class ran again before a host synchronisation: keep its time
+      float f = 0.f;
+      CK(cudaEventSynchronize(ctx->kt_ev[k][1]));
+      CK(cudaEventElapsedTime(&f, ctx->kt_ev[k][0], ctx->kt_ev[k][1]));
+      ctx->kt_ms[k] += f;
+      ctx->kt_pending[k] = false;
+    }
+    CK(cudaEventRecord(ctx->kt_ev[k][0], ctx->stream));
     return MCRT_OK;
   };
   auto kt_end = [&](int k) -> int {
@@ -2278,7 +2313,7 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
   float* im[4] = {out->image_m_i, out->image_m_q, out->image_m_u, out->image_m_v};
   float* ib[8] = {out->image_b_i, out->image_b_q, out->image_b_u, out->image_b_v,
                   out->image_b_d, out->image_b_s, out->image_b_e, out->image_b_o};
-  int64_t nmax = std::max(std::max(ctx->nsed, ctx->nimgb), std::max(ctx->npsed, ctx->nimg));
+  int64_t nmax = std::max(std::max(std::max(ctx->nsed, ctx->nimgb), ctx->nims), std::max(ctx->npsed, ctx->nimg));
   float* d_f = nullptr;
   if ((rc = scratch(ctx, &d_f, nmax))) return rc;
   std::vector<std::pair<float*, std::pair<const double*, int64_t>>> jobs;
@@ -2286,6 +2321,8 @@ int mcrt_download_tallies(mcrt_ctx* ctx, mcrt_tallies* out) {
   for (int k = 0; k < 9; ++k) jobs.push_back({ps[k], {t.psed + k * ctx->npsed, ctx->npsed}});
   for (int k = 0; k < 4; ++k) jobs.push_back({im[k], {t.img + k * ctx->nimg, ctx->nimg}});
   for (int k = 0; k < 8; ++k) jobs.push_back({ib[k], {t.imgb + k * ctx->nimgb, ctx->nimgb}});
+  float* is[4] = {out->image_ms_i, out->image_ms_q, out->image_ms_u, out->image_ms_v};
+  for (int k = 0; k < 4; ++k) jobs.push_back({is[k], {t.ims + k * ctx->nims, ctx->nims}});
   for (auto& j : jobs) {
     if (!j.first || j.second.second == 0) continue;
     const int64_t n = j.second.second;
@@ -2307,7 +2344,8 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
                     &rest.aveinc, &rest.ti, &rest.tq, &rest.tu, &rest.tv, &rest.ti2, &rest.tq2, &rest.tu2, &rest.tv2,
                     &rest.numt, &rest.image_m_i, &rest.image_m_q, &rest.image_m_u, &rest.image_m_v,
                     &rest.image_b_i, &rest.image_b_q, &rest.image_b_u, &rest.image_b_v,
-                    &rest.image_b_d, &rest.image_b_s, &rest.image_b_e, &rest.image_b_o})
+                    &rest.image_b_d, &rest.image_b_s, &rest.image_b_e, &rest.image_b_o,
+                    &rest.image_ms_i, &rest.image_ms_q, &rest.image_ms_u, &rest.image_ms_v})
     *f = nullptr;
   int rc = mcrt_download_tallies(ctx, &rest);
   if (rc) return rc;
@@ -2361,6 +2399,12 @@ int mcrt_diskflux(mcrt_ctx* ctx, int64_t np, double ltot_lsol, int32_t ipeel, mc
     pe.image_b_e = out->image_b_e; pe.image_b_o = out->image_b_o;
     rc = mcrt_download_tallies(ctx, &pe);
   }
+  if (!rc && (out->image_ms_i || out->image_ms_q || out->image_ms_u || out->image_ms_v)) {
+    mcrt_tallies ms{};                       // nested images: not normalised by flux_test.f90
+    ms.image_ms_i = out->image_ms_i; ms.image_ms_q = out->image_ms_q;
+    ms.image_ms_u = out->image_ms_u; ms.image_ms_v = out->image_ms_v;
+    rc = mcrt_download_tallies(ctx, &ms);
+  }
   cudaError_t le = cudaGetLastError();
   if (!rc && le != cudaSuccess) rc = fail(ctx, MCRT_ERR_CUDA, "mcrt_diskflux: %s", cudaGetErrorString(le));
   dfree(ctx, d_f);
@@ -2372,7 +2416,8 @@ int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
   CK(cudaSetDevice(ctx->device));
   const DevTallies& t = ctx->dt;
   const int64_t nc = ctx->ncell;
-  const int64_t nmax = std::max<int64_t>(std::max<int64_t>(std::max<int64_t>(nc, MCRT_NCOUNTERS), ctx->nimgb),
+  const int64_t nmax = std::max<int64_t>(std::max<int64_t>(std::max<int64_t>(nc, MCRT_NCOUNTERS),
+                                                            std::max(ctx->nimgb, ctx->nims)),
                                          std::max(ctx->nsed, std::max(ctx->npsed, ctx->nimg)));
   void* d_in = nullptr;
   int rc = dalloc(ctx, (char**)&d_in, (size_t)nmax * 8);
@@ -2408,6 +2453,8 @@ int mcrt_accumulate_tallies(mcrt_ctx* ctx, const mcrt_tallies* in) {
   const float* ib[8] = {in->image_b_i, in->image_b_q, in->image_b_u, in->image_b_v,
                         in->image_b_d, in->image_b_s, in->image_b_e, in->image_b_o};
   for (int k = 0; k < 8 && !rc; ++k) rc = add(ib[k], 2, t.imgb + k * ctx->nimgb, ctx->nimgb);
+  const float* is[4] = {in->image_ms_i, in->image_ms_q, in->image_ms_u, in->image_ms_v};
+  for (int k = 0; k < 4 && !rc; ++k) rc = add(is[k], 2, t.ims + k * ctx->nims, ctx->nims);
   dfree(ctx, d_in);
   return rc;
 }
@@ -2416,7 +2463,7 @@ int mcrt_device_tallies_view(mcrt_ctx* ctx, mcrt_device_tallies* out) {
   if (!ctx || !out) return MCRT_ERR_ARG;
   const int64_t nc = ctx->ncell;
   out->f64 = ctx->dt.dtauabs;                 // first member of the allocation
-  out->n_f64 = 2 * nc + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + MCRT_NSCALARS;
+  out->n_f64 = 2 * nc + 10 * ctx->nsed + 9 * ctx->npsed + 4 * ctx->nimg + 8 * ctx->nimgb + 4 * ctx->nims + MCRT_NSCALARS;
   out->u64 = (uint64_t*)ctx->dt.cnt;
   out->n_u64 = MCRT_NCOUNTERS;
   out->i32 = ctx->dt.nabs;

@@ -56,6 +56,7 @@ struct DevTallies {
   double *psed;                            // [9][npsed]
   double *img;                             // [4][nimg]
   double *imgb;                            // [8][nimgb] filter-band images: I Q U V, I by origin d s e o
+  double *ims;                             // [4][nims] nested images I Q U V, [dim,dim,nnu,nlev,npeel]
   double *scal;                            // [MCRT_NSCALARS]
   unsigned long long *cnt;                 // [MCRT_NCOUNTERS]
   int32_t *ndiff;                          // [ncell] diffusion absorptions per surface cell
@@ -121,6 +122,13 @@ struct DevModel {
   int64_t nimgb;
   const int32_t *nfpts;
   const double *filtwave, *filtphi;
+  // nested images (output_imsparse): sparse_nlev square images of
+  // sparse_dim^2 pixels with half sizes sparse_levels (ascending), sparse_nnu
+  // bins in log10(frequency) over [lognu_min, lognu_max]
+  int output_imsparse, sparse_dim, sparse_nlev, sparse_nnu;
+  float sparse_lognu_min, sparse_lognu_max;
+  int64_t nims;
+  const float *sparse_levels;
 };
 
 // One peel-off request: the packet's state at an emission, scattering or
@@ -276,7 +284,7 @@ struct LaunchParams {
   int32_t g1, g2;               // generator initial seeds
   unsigned long long *next;     // dynamic packet counter
   PeelJob *jobs;                // peel-off job queue (nullptr: peel inline)
-  double *job_nub;              // [job_cap] packet frequency per job (filter-band images only)
+  double *job_nub;              // [job_cap] packet frequency per job (filter-band and nested images only)
   unsigned long long *njobs;    // jobs queued
   int64_t job_cap;
   mcrt_packet_log *log;

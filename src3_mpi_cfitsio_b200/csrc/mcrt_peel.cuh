@@ -231,6 +231,7 @@ struct PeelLane {
       }
     }
     bin_filters(m, T, id, vx, vy, nub, i_orig, qi, qq, qu, qv);
+    bin_nested(m, T, id, ximage, yimage, nub, qi, qq, qu, qv);
     const int i_inter = scattered ? 2 : ((i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

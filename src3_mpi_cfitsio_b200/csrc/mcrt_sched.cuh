@@ -435,6 +435,7 @@ struct Lane {
       }
     }
     bin_filters(m, pk.T, id, vx, vy, pk.nub, pk.i_orig, qi, qq, qu, qv);
+    bin_nested(m, pk.T, id, ximage, yimage, pk.nub, qi, qq, qu, qv);
     const int i_inter = (pk.iflag == 1) ? 2 : ((pk.i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + pk.i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

@@ -212,6 +212,62 @@ __device__ __forceinline__ void bin_filters(const DevModel& m, const DevTallies&
   }
 }
 
+// math_binning.f90 ipos_sp / locate_sp in single precision, each rounding
+// explicit so that the bins are the reference's bit for bit.
+__device__ __forceinline__ int ipos_sp(float xmin, float xmax, float x, int nbin) {
+  if (xmax > xmin) {
+    if (x < xmin) return 0;
+    if (x > xmax) return nbin + 1;
+  } else {
+    if (x < xmax) return 0;
+    if (x > xmin) return nbin + 1;
+  }
+  const float frac = __fdiv_rn(__fsub_rn(x, xmin), __fsub_rn(xmax, xmin));
+  return (int)__fmul_rn(frac, (float)nbin) + 1;
+}
+__device__ __forceinline__ int locate_sp(const float* xx, int n, float x) {
+  const bool ascnd = __ldg(xx + n - 1) >= __ldg(xx);
+  int jl = 0, ju = n + 1;
+  while (ju - jl > 1) {
+    const int jm = (ju + jl) >> 1;
+    if (ascnd == (x >= __ldg(xx + jm - 1))) jl = jm; else ju = jm;
+  }
+  if (x == __ldg(xx)) return 1;
+  if (x == __ldg(xx + n - 1)) return n - 1;
+  if (x > __ldg(xx + n - 1) || x < __ldg(xx)) return -1;
+  return jl;
+}
+
+// Nested multi-wavelength images (peeloff_3d_2_test.f90:302-309 calling
+// nested_image_bin, type_nested_image.f90:75-101) of one peel-off at image
+// position (ximage, yimage): position and log10(frequency) in single
+// precision as the reference passes them; the level is the smallest whose
+// half size exceeds max(|x|,|y|); the four Stokes images share the pixel.
+// A pixel beyond the image (a position exactly on a level's edge, where
+// ipos gives dim+1) is dropped.
+__device__ __forceinline__ void bin_nested(const DevModel& m, const DevTallies& T, int id, double ximage,
+                                           double yimage, double nub, double qi, double qq, double qu, double qv) {
+  if (!m.output_imsparse) return;
+  const float xr = (float)ximage, yr = (float)yimage;
+  const float* lev = m.sparse_levels;
+  const int nl = m.sparse_nlev;
+  const float r = fmaxf(fabsf(xr), fabsf(yr));
+  if (r > __ldg(lev + nl - 1)) return;
+  int l = locate_sp(lev, nl, r);
+  l = (l < 0) ? 1 : l + 1;
+  const float h = __ldg(lev + l - 1);
+  const int ix = ipos_sp(-h, h, xr, m.sparse_dim), iy = ipos_sp(-h, h, yr, m.sparse_dim);
+  const float lnu = (float)log10(2.9979e14 / (1.2398 / nub));
+  const int inu = ipos_sp(m.sparse_lognu_min, m.sparse_lognu_max, lnu, m.sparse_nnu);
+  if (inu < 1 || inu > m.sparse_nnu || ix < 1 || ix > m.sparse_dim || iy < 1 || iy > m.sparse_dim) return;
+  const int64_t k = (int64_t)(ix - 1) + (int64_t)m.sparse_dim * ((iy - 1) + (int64_t)m.sparse_dim *
+                    ((inu - 1) + (int64_t)m.sparse_nnu * ((l - 1) + (int64_t)nl * (id - 1))));
+  atomicAdd(T.ims + k, qi);
+  atomicAdd(T.ims + m.nims + k, qq);
+  atomicAdd(T.ims + 2 * m.nims + k, qu);
+  atomicAdd(T.ims + 3 * m.nims + k, qv);
+}
+
 struct Packet {
   const DevModel& m;
   const DevTallies& T;
@@ -1582,6 +1638,7 @@ struct Packet {
       }
     }
     bin_filters(m, T, peelid, vx, vy, nub, i_orig, qi, qq, qu, qv);
+    bin_nested(m, T, peelid, ximage, yimage, nub, qi, qq, qu, qv);
     const int i_inter = (iflag == 1) ? 2 : ((i_orig == 1) ? 1 : 3);
     const int indx[3] = {1, 1 + i_orig, 5 + i_inter};
     for (int ia = 1; ia <= m.nap; ++ia) {

@@ -991,6 +991,43 @@ def with_filters(m: Model, **kw) -> Model:
     return m
 
 
+def nested_levels(l_max: float, l_min: float, factor: int):
+    """Half sizes of the nested images, ascending, as find_levels
+    (type_nested_image.f90:62-73) computes them in single precision:
+    n = ceiling(log10(l_max/l_min) / log10(factor)) + 1 and
+    levels(n+1-l) = l_max / factor**(l-1)."""
+    f32 = np.float32
+    lmax, lmin, fac = f32(l_max), f32(l_min), f32(factor)
+    n = int(math.ceil(float(np.log10(lmax / lmin) / np.log10(fac)))) + 1
+    lev = np.zeros(n, np.float32)
+    for l in range(1, n + 1):
+        lev[n - l] = lmax / fac ** f32(l - 1)
+    return lev
+
+
+def with_nested_images(m: Model, dim: int = 64, rmax_au: float | None = None, rmin: float = 50.0,
+                       factor: int = 4) -> Model:
+    """Nested multi-wavelength images (output_imsparse): the setup of
+    initarr_2_new.f90:170-190 -- half sizes from rmax_au [AU] (default: the
+    image half size) down to rmin [R*], nfreq bins in log10(frequency [Hz])
+    over the SED range, both computed in single precision as there."""
+    if dim % factor or (dim // 2) % 2:
+        raise ValueError("dim must be a multiple of factor and dim/2 even (nested_image_setup)")
+    c = m.config
+    autors = c["autors"]
+    rmax = (m.w.rmaxi_au if rmax_au is None else rmax_au)
+    f32 = np.float32
+    numin = f32(c["numin"])
+    numax = f32(c["numin"] * math.exp(c["lnurat"]))
+    c.update(output_imsparse=1, sparse_dim=dim, sparse_nnu=c["nfreq"],
+             sparse_lognu_min=float(np.log10(numin * f32(2.9979e14) / f32(1.2398))),
+             sparse_lognu_max=float(np.log10(numax * f32(2.9979e14) / f32(1.2398))))
+    lev = nested_levels(f32(rmax) * f32(autors), rmin, factor)
+    c["sparse_nlev"] = int(lev.size)
+    m.tables["sparse_levels"] = lev
+    return m
+
+
 def draine_table(nemit: int = 18, ndraine: int = 1000, lmin_um: float = 1.0, lmax_um: float = 1000.0) -> np.ndarray:
     """Small-grain (VSG/PAH) emission spectra in the layout draine_cdf.f90
     leaves in draine_mod: cdf_d(nemit,ndraine), logcdf_d(nemit,ndraine) and

@@ -32,12 +32,12 @@ def test_library_exports_all_symbols():
 
 
 def test_struct_sizes_match_header():
-    # mirrored ctypes layouts: 24 int32 + 23 double + 4 int32 config, pointer-only structs
+    # mirrored ctypes layouts: 24 int32 + 23 double + 8 int32 + 2 float config, pointer-only structs
     from src3_mpi_cfitsio_b200 import abi
-    assert ctypes.sizeof(abi.Config) == 24 * 4 + 23 * 8 + 4 * 4
+    assert ctypes.sizeof(abi.Config) == 24 * 4 + 23 * 8 + 8 * 4 + 2 * 4
     assert ctypes.sizeof(abi.Grid) == 22 * 8
-    assert ctypes.sizeof(abi.Tables) == 30 * 8 + 6 * 4
-    assert ctypes.sizeof(abi.Tallies) == (4 + 2 + 10 + 9 + 4 + 2 + 8) * 8
+    assert ctypes.sizeof(abi.Tables) == 31 * 8 + 6 * 4
+    assert ctypes.sizeof(abi.Tallies) == (4 + 2 + 10 + 9 + 4 + 2 + 8 + 4) * 8
     assert ctypes.sizeof(abi.PacketLog) == 8 + 12 * 4 + 10 * 8
 
 
