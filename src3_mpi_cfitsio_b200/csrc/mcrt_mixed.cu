@@ -22,6 +22,15 @@
 #ifndef MCRT_WALK_MIN_BLOCKS
 #define MCRT_WALK_MIN_BLOCKS 8
 #endif
+// The peel-off kernel at 4 blocks (16 warps) per SM, <= 128 registers: the
+// phase-matrix and binning code spills about 200 B to local memory, but the
+// FP32 walk it shares the kernel with runs a third more warps.  B200, mixed,
+// peeled iterations: 2-D 1e7 packets 1141 -> 824 ms, 3-D clumpy 2e6 packets
+// 1118 -> 950 ms (interleaved on one box); 5 blocks (<= 102 registers,
+// ~600 B spilled) was slower than 3.
+#ifndef MCRT_PEEL_MIN_BLOCKS
+#define MCRT_PEEL_MIN_BLOCKS 4
+#endif
 #define mcrt mcrt_mixed
 #include "mcrt_sched.cuh"
 #include "mcrt_peel.cuh"

@@ -252,7 +252,10 @@ struct PeelLane {
 
 // Persistent peel-off kernel over the (job, inclination) items queued by the
 // preceding transport launch (the job count is read on the device).
-__global__ void __launch_bounds__(kBlock) peel_sched(LaunchParams P, unsigned long long* next_item) {
+#ifndef MCRT_PEEL_MIN_BLOCKS
+#define MCRT_PEEL_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(kBlock, MCRT_PEEL_MIN_BLOCKS) peel_sched(LaunchParams P, unsigned long long* next_item) {
   __shared__ double spec[5 * kMaxSlot * kBlock];
   PeelLane L(P.m, P.t, spec);
   const unsigned FULL = 0xffffffffu;
