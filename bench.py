@@ -4,10 +4,12 @@ Workload (the configuration the headline metric is quoted on): the 2-D disk +
 Ulrich envelope + bipolar cavity model (nr=100 x ntheta=99 x nphi=1 cells,
 4000 K / 2 Rsun star, Mdisk=0.01 Msun, 100 log wavelengths 0.1-3000 um),
 run as Lucy iterations of the reference's ``disk`` routine.  One step is one
-iteration: the packet loop over ``--packets`` packets per GPU (emission, cell
-walk, scattering, absorption + Lucy reemission, exit binning) plus the
-device temperature update (``tfinal``).  Inputs are synthetic (seeded
-generator, no reference parameter files exist here).
+iteration: the diffusion region of the current temperature (``setdiffus``,
+as gridset reruns it every iteration), the packet loop over ``--packets``
+packets per GPU (emission, cell walk, scattering, absorption + Lucy
+reemission, exit binning) and the device temperature update (``tfinal``).
+Inputs are synthetic (seeded generator, no reference parameter files exist
+here).
 
 value : packets/s of the whole job (all ranks), device-timed between CUDA
         events on the engine's stream, max over ranks;
