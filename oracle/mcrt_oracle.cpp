@@ -1383,7 +1383,7 @@ struct Packet {
       const float r = std::max(std::fabs(xr), std::fabs(yr));
       if (!(r > lev[nl - 1])) {
         int l = locate_sp(lev, nl, r);
-        l = (l < 0) ? 1 : l + 1;
+        l = (l < 0) ? 1 : std::min(l + 1, nl);   // a single level met exactly at its edge stays that level
         const int ix = ipos_sp(-lev[l - 1], lev[l - 1], xr, c.sparse_dim);
         const int iy = ipos_sp(-lev[l - 1], lev[l - 1], yr, c.sparse_dim);
         const int inu = ipos_sp(c.sparse_lognu_min, c.sparse_lognu_max, lnu, c.sparse_nnu);

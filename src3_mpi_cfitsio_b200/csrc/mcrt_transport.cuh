@@ -254,7 +254,7 @@ __device__ __forceinline__ void bin_nested(const DevModel& m, const DevTallies& 
   const float r = fmaxf(fabsf(xr), fabsf(yr));
   if (r > __ldg(lev + nl - 1)) return;
   int l = locate_sp(lev, nl, r);
-  l = (l < 0) ? 1 : l + 1;
+  l = (l < 0) ? 1 : min(l + 1, nl);     // a single level met exactly at its edge stays that level
   const float h = __ldg(lev + l - 1);
   const int ix = ipos_sp(-h, h, xr, m.sparse_dim), iy = ipos_sp(-h, h, yr, m.sparse_dim);
   const float lnu = (float)log10(2.9979e14 / (1.2398 / nub));
