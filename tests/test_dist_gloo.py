@@ -25,12 +25,18 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _model():
+    """The reduced 2-D model with every peel-off output on: image cubes,
+    filter-band images and nested images."""
+    return model.with_nested_images(model.with_filters(model.warm(model.small_2d())))
+
+
 def _rank_main(rank, world, port, out_dir):
     import torch.distributed as tdist
     from oracle import oracle
     tdist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
-        m = model.warm(model.small_2d())
+        m = _model()
         lo, hi = dist.shard_range(N_PACKETS, rank, world)
         tal, _ = oracle.run(abi.Bundle(m), N_PACKETS, lo, hi, ipeel=1, threads=2)
         dist.allreduce_host_tallies(tal)
@@ -60,7 +66,7 @@ def test_two_gloo_ranks_reduce_to_the_single_run(oracle_mod):
         mp.start_processes(_rank_main, args=(world, _free_port(), d), nprocs=world, join=True,
                            start_method="spawn")
         red = dict(np.load(os.path.join(d, "reduced.npz")))
-    m = model.warm(model.small_2d())
+    m = _model()
     one, _ = oracle_mod.run(abi.Bundle(m), N_PACKETS, ipeel=1, threads=2)
     ints = [k for k, a in one.arrays.items() if a.dtype in (np.int32, np.int64)]
     assert {"nabs", "dbig", "killed", "counters"} <= set(ints)
@@ -73,6 +79,7 @@ def test_two_gloo_ranks_reduce_to_the_single_run(oracle_mod):
         if a.dtype == np.float32:
             assert np.allclose(red[k], a, rtol=2e-6, atol=1e-6 * max(1e-30, float(np.abs(a).max()))), k
     assert one["ti"].sum() > 0 and one["nums"].sum() > 0
+    assert one["image_b_i"].sum() > 0 and one["image_ms_i"].sum() > 0
 
 
 @pytest.mark.parametrize("world", [1, 2, 3, 8])
