@@ -339,8 +339,9 @@ int mcrt_set_precision(mcrt_ctx *ctx, int32_t mode);
 int mcrt_set_schedule(mcrt_ctx *ctx, int32_t schedule, int32_t event_batch);
 
 /* Wavefront schedule sizes.  `slots`: in-flight packet slots (default
- * 2,097,152; 784 bytes of device memory each).  `peel_jobs`: capacity of the
- * peel-off job queue in jobs (176 bytes each; 0 = default, 16 x slots
+ * 2,097,152; 744 bytes of device memory each).  `peel_jobs`: capacity of the
+ * peel-off job queue in jobs (192 bytes each, 200 with filter-band or nested
+ * images; 0 = default, 16 x slots
  * within [8,388,608, 67,108,864]; else at least 2 x slots); the loop runs
  * the peel-off kernel whenever fewer than `slots` free jobs remain and
  * before the tail launch, whose peel-offs beyond the capacity are walked
