@@ -281,6 +281,7 @@ struct Packet {
   int iflag, i_orig, exitflag;
   int nscat, nabsev, ncross, nstar, ndiffev;
   unsigned long long c_cross, c_peel, c_pcross, c_pbin, c_reset;
+  bool spec_dirty = false;      // opacset rewrote the species columns (the wavefront event kernel saves them then)
 
   // sbase: kSpecCols columns of kMaxSlot doubles per thread (the species
   // state and, in the mixed build, the FP32 walk columns in the last one);
@@ -306,6 +307,7 @@ struct Packet {
   // interpolation weight of the first such slot: the same search over the
   // same values gives the same result.
   __device__ void opacset(double nu, int order) {
+    spec_dirty = true;
     int a = 0, b = 0, have = -1;
     double f = 0.0;
     for (int s = 0; s < m.nslot; ++s) {

@@ -353,10 +353,13 @@ __global__ void __launch_bounds__(kBlock, MCRT_EVENT_MIN_BLOCKS) wave_event(Laun
         if (ev != EV_EXIT && ev != EV_FINISH) wave_load_spec(L, R, nslot);
       }
       L.ev = ev;
+      L.pk.spec_dirty = false;
       L.events(P);
       if (L.ev == EV_NONE) {
         wave_save_walk(L, R);
-        wave_save_core(L, R, nslot);
+        // the species columns change only with the frequency (opacset):
+        // a scattering or a peel-off event leaves the record's copy valid
+        wave_save_core(L, R, L.pk.spec_dirty ? nslot : 0);
         if (peeled) wave_save_peelstate(L, R);
         walk = true;
       }
